@@ -1,0 +1,360 @@
+#!/usr/bin/env python3
+"""Headline benchmark: 2048^2 scalar band-limited ASM propagations per second.
+
+Workload (one "step" = a batch of --batch propagations of distinct fields):
+  2048 x 2048 grid, dx = 2 um, lambda = 632.8 nm, z = 5 cm, complex64 pipeline
+  (FP64 transfer-function argument), device-resident fields propagated in place
+  through the C ABI (wos_propagate_dev).  Inputs: a seeded unit-amplitude
+  random-phase field (excites every frequency bin) in 16 rotating 32 MiB
+  buffers (512 MiB working set, > 4x the 126 MB L2).
+Also reported: the FP64 (complex128) kernel on the same workload, the
+end-to-end rate through the host API (complex128 host buffers, H2D + D2H in
+the timed region), the roofline of the dominant kernel from live per-launch
+CUDA events, and the oracle's CPU rate on this host.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Multi-GPU: replicas (one independent propagation stream per rank); value is
+the job-wide rate = all ranks' propagations / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "2048² ASM props/s, FP32 vs FP64 GPU at rel-L2≤1e-5; % HBM roofline"
+N = 2048
+DX = 2e-6
+WL = 632.8e-9
+ZPROP = 0.05
+POOL = 16
+
+
+def workload_config(batch: int) -> dict:
+    return {"workload": f"asm {N}x{N} scalar, complex64, dx=2um, lambda=632.8nm, z=5cm",
+            "grid": [N, N], "method": "asm", "fields_per_step": batch,
+            "input": "unit-amplitude random phase (seed 1)",
+            "l2_flush": f"inputs larger than L2: {POOL} rotating {N * N * 8 >> 20} MiB fields",
+            "parallelism": "replicas"}
+
+
+def measured_peaks() -> tuple:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def input_field(seed: int = 1) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    return np.exp(1j * rng.uniform(0, 2 * np.pi, (N, N))).astype(np.complex128)
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(sample_props: int = 3) -> dict:
+    """The FP64 oracle (C restatement of the reference's Go CPU path) on this host."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # noqa: E402  (CPU-baseline leg only)
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    ex = input_field()
+    t_total = 0.0
+    done = 0
+    for _ in range(sample_props):
+        f = O.Field(ex.copy(), DX)
+        c = O.Context(wavelength=WL)
+        t0 = time.perf_counter()
+        O.propagate(f, ZPROP, "asm", c)
+        t_total += time.perf_counter() - t0
+        done += 1
+        if t_total > 30:
+            break
+    return {"value": done / t_total, "unit": "props/s", "cores": cores, "kind": "port",
+            "sample": f"{done} propagation(s) of the {N}x{N} workload, FP64 C oracle, {cores} threads "
+                      "(parFor semantics of optics/fft.go:91-122, Warnings enabled)",
+            "seconds": t_total}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # noqa: E402  (reference arm: the reference algorithm on the host cores)
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    ex = input_field()
+    for _ in range(args.warmup):
+        f = O.Field(ex.copy(), DX)
+        O.propagate(f, ZPROP, "asm", O.Context(wavelength=WL))
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        f = O.Field(ex.copy(), DX)
+        O.propagate(f, ZPROP, "asm", O.Context(wavelength=WL))
+    dt = time.perf_counter() - t0
+    v = args.steps / dt
+    line = {"metric": METRIC, "value": v, "unit": "props/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference", "config": workload_config(1),
+            "cpu_baseline": {"value": v, "unit": "props/s", "cores": cores, "kind": "port",
+                             "sample": f"one {N}x{N} propagation per step, FP64 C oracle "
+                                       "(restatement of optics/fft.go + optics/propagate.go), "
+                                       f"{cores} threads"},
+            "e2e": {"value": v, "unit": "props/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def time_device(g, torch, bufs, steps, warmup, batch, ctx, stream, profile=False):
+    """Device-resident timed region: steps x batch in-place propagations."""
+    n = 0
+    for _ in range(warmup * batch):
+        b = bufs[n % len(bufs)]
+        g.propagate_dev(N, N, DX, 1, b.data_ptr(), b.data_ptr(), ZPROP, "asm", ctx)
+        n += 1
+    if profile:
+        g.synchronize()
+        g.profile_reset()
+        g.set_profiling(True)
+    launches0 = g.launch_count()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps * batch):
+        b = bufs[n % len(bufs)]
+        g.propagate_dev(N, N, DX, 1, b.data_ptr(), b.data_ptr(), ZPROP, "asm", ctx)
+        n += 1
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = g.launch_count() - launches0
+    prof = g.profile() if profile else {}
+    if profile:
+        g.set_profiling(False)
+    return e0.elapsed_time(e1), launches, prof
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=64)
+    ap.add_argument("--impl", default="ours")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    wos = importlib.import_module("tetsuhiro-wos_b200")
+
+    stream = torch.cuda.Stream()
+    g32 = wos.GPU(wos.FP32, device=local)
+    g32.set_stream(stream.cuda_stream)
+    g64 = wos.GPU(wos.FP64, device=local)
+    g64.set_stream(stream.cuda_stream)
+    ctx = wos.Context(wavelength=WL, warnings_enabled=False)
+
+    ex = input_field()
+    with torch.cuda.stream(stream):
+        base32 = torch.from_numpy(ex.astype(np.complex64)).cuda()
+        bufs = [base32.clone() for _ in range(POOL)]
+    torch.cuda.synchronize()
+
+    # ---- correctness of this exact workload: FP32 vs FP64 GPU kernels
+    with torch.cuda.stream(stream):
+        a32 = base32.clone()
+        a64 = torch.from_numpy(ex).cuda()
+    torch.cuda.synchronize()
+    g32.propagate_dev(N, N, DX, 1, a32.data_ptr(), a32.data_ptr(), ZPROP, "asm", ctx)
+    g64.propagate_dev(N, N, DX, 1, a64.data_ptr(), a64.data_ptr(), ZPROP, "asm", ctx)
+    torch.cuda.synchronize()
+    r64 = a64.cpu().numpy()
+    rel32 = float(np.sqrt(np.sum(np.abs(a32.cpu().numpy().astype(np.complex128) - r64) ** 2) /
+                          np.sum(np.abs(r64) ** 2)))
+    del a32, a64
+
+    # ---- FP64 kernel on the same workload (reported beside the headline)
+    with torch.cuda.stream(stream):
+        bufs64 = [torch.from_numpy(ex).cuda() for _ in range(8)]
+    torch.cuda.synchronize()
+    s64 = max(2, args.steps // 5)
+    ms64, _, _ = time_device(g64, torch, bufs64, s64, 2, args.batch // 4 or 1, ctx, stream)
+    fp64_rate = s64 * (args.batch // 4 or 1) / (ms64 / 1e3)
+    del bufs64
+    torch.cuda.empty_cache()
+
+    # ---- headline: device-resident FP32, with live per-launch profile
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    ms, launches, prof = time_device(g32, torch, bufs, args.steps, args.warmup, args.batch, ctx, stream,
+                                     profile=True)
+    clk = clocks.stop()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    props = args.steps * args.batch * world
+    value = props / (ms_max / 1e3)
+
+    # roofline of the dominant kernel: algorithmic bytes per launch / mean launch time
+    peak, peak_kind = measured_peaks()
+    per_launch_bytes = {"row_fwd": 16 * N * N, "col_fused": 16 * N * N, "row_inv": 16 * N * N}
+    dom = max(prof, key=lambda k: prof[k][0]) if prof else None
+    roof = None
+    if dom:
+        tot_ms, cnt = prof[dom]
+        avg_s = tot_ms / cnt / 1e3
+        ach = per_launch_bytes.get(dom, 16 * N * N) / avg_s / 1e9
+        roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                "frac": ach / peak, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": None, "algorithmic_bytes_per_launch": per_launch_bytes.get(dom),
+                "mean_launch_us": avg_s * 1e6,
+                "per_kernel_us": {k: v[0] / v[1] * 1e3 for k, v in prof.items()},
+                "whole_propagation": {"algorithmic_bytes": 48 * N * N,
+                                      "achieved_gbs": 48 * N * N * value / world / 1e9,
+                                      "frac": 48 * N * N * value / world / 1e9 / peak}}
+    traffic_file = os.path.join(ROOT, "profiles", "traffic_asm2048_c64.json")
+    if roof and os.path.exists(traffic_file):
+        try:
+            with open(traffic_file) as fh:
+                roof["traffic"] = json.load(fh).get(dom)
+        except Exception:
+            pass
+
+    # ---- end to end through the host API (complex128 host buffers, pinned)
+    e2e = None
+    if not args.no_e2e:
+        host = torch.from_numpy(ex).pin_memory()
+        hnp = host.numpy()
+        f = wos.Field(hnp, DX)
+        f.ex = hnp  # the pinned buffer itself (no copy)
+        nsteps = max(3, args.steps // 5)
+        for _ in range(2):
+            g32.propagate(f, ZPROP, "asm", wos.Context(wavelength=WL))
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(nsteps):
+            g32.propagate(f, ZPROP, "asm", wos.Context(wavelength=WL))
+        t1.record(stream)
+        torch.cuda.synchronize()
+        e_ms = t0.elapsed_time(t1)
+        te = torch.tensor([e_ms], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e = {"value": nsteps * world / (float(te.item()) / 1e3), "unit": "props/s",
+               "h2d_bytes_per_step": N * N * 16, "d2h_bytes_per_step": N * N * 16,
+               "api": "wos_propagate (host complex128 Field, Warnings enabled)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_baseline()
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "props/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": workload_config(args.batch), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clk,
+                "fp64": {"value": fp64_rate, "unit": "props/s", "dtype": "f64",
+                         "fp32_speedup": value / world / fp64_rate},
+                "parity": {"rel_l2_fp32_vs_fp64_gpu": rel32, "tolerance": 1e-5}}
+        print(json.dumps(line), flush=True)
+    g32.close()
+    g64.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

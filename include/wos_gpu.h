@@ -1,0 +1,250 @@
+/*
+ * wos_gpu.h -- C ABI of libwosgpu.so, the B200 (sm_100a) propagation backend
+ * for the Tetsuhiro-WOS `optics` package.
+ *
+ * The reference's GPU seam is per FFT: fft2D / fft1DAny call gpuFFT2D /
+ * gpuFFT1D (optics/fft.go:135-142,209-216), which copy the whole array to the
+ * device and back around one cuFFT Z2Z call (optics/gpu.go:173-207).  This
+ * library moves the seam up to the propagation call itself: one entry point
+ * per reference function of the hot path, each crossing PCIe once per field.
+ *
+ * Conventions
+ *  - All signatures are plain C: pointers, sizes, doubles, ints.
+ *  - A field component is row-major ny x nx (index y*nx + x), exactly the Go
+ *    Field.Ex / Field.Ey layout (optics/field.go:14-22) with ny = nx = N.
+ *    Host buffers are complex128 (wos_c128 = Go complex128 = C double _Complex).
+ *  - Device-resident entry points (suffix _dev) take device pointers whose
+ *    element type is the context precision: complex64 (float2) for WOS_FP32,
+ *    complex128 (double2) for WOS_FP64.
+ *  - Every call returns a wos_status; on failure wos_last_error() returns a
+ *    thread-local message.  There is no CPU fallback: an error is reported to
+ *    the caller, never hidden.
+ *  - A context owns one CUDA stream, its device workspace and its plans.  It
+ *    may be used by one host thread at a time (calls serialise on an internal
+ *    lock); use one context per concurrent caller.
+ */
+#ifndef WOS_GPU_H
+#define WOS_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WOS_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define WOS_API __attribute__((visibility("default")))
+#else
+#define WOS_API
+#endif
+
+typedef struct { double re, im; } wos_c128;
+typedef struct wos_ctx_s* wos_ctx;
+
+/* Status codes (replace the cufftResult / cudaError_t strings of optics/gpu.go:51-79). */
+enum wos_status {
+    WOS_OK = 0,
+    WOS_INVALID_ARG = 1,
+    WOS_UNSUPPORTED_SIZE = 2,
+    WOS_OOM = 3,
+    WOS_CUDA_ERROR = 4,
+    WOS_TIMEOUT = 5,
+    WOS_NOT_INITIALISED = 6,
+    WOS_UNKNOWN_METHOD = 7
+};
+
+/* Method ids: the Method constants of optics/propagate.go:40-50. */
+enum wos_method {
+    WOS_ASM = 1,
+    WOS_ASM_PAD = 2,
+    WOS_ASM_SHIFT = 3,
+    WOS_ASM_SHIFT_PAD = 4,
+    WOS_FRESNEL_TF = 5,
+    WOS_FRESNEL_IR = 6,
+    WOS_FRAUNHOFER = 7
+};
+
+enum wos_precision { WOS_FP64 = 0, WOS_FP32 = 1 };
+
+/* Warning bits: the Warnings.Add codes of the hot path (optics/propagate.go:203-264,515,586,654). */
+enum wos_warn_bit {
+    WOS_W_EVANESCENT_FILTERED = 0,
+    WOS_W_BACKWARD_REGULARIZED = 1,
+    WOS_W_BACKWARD_EVANESCENT = 2,
+    WOS_W_ASM_ALIAS_WRAP = 3,
+    WOS_W_FRESNEL_TF_ALIAS = 4,
+    WOS_W_FRESNEL_IR_ALIAS = 5,
+    WOS_W_FRAUNHOFER_NEARFIELD = 6,
+    WOS_W_COUNT = 7
+};
+
+/* optics.Context (optics/field.go:237-254), the fields the hot path reads. */
+typedef struct {
+    double wavelength;        /* m */
+    int evanescent_zero;      /* Evanescent == "zero" */
+    double evanescent_limit;  /* nepers, 0 = off */
+    int backward_regularize;  /* BackwardRegularize */
+    double tikhonov_alpha;    /* <= 0 -> 1e-3 */
+    int diagnostics;          /* 1 when ctx.Warnings != nil: compute what the warnings need */
+} wos_context;
+
+/* Scalars behind the reference's warnings, plus the warnings themselves
+ * (count and value per code, as Warnings.Add would record them). */
+typedef struct {
+    double p_in, p_out;           /* Field.Power() before / after (W), compensated FP64 sums */
+    double centroid_fx, centroid_fy; /* spectral centroid (asm_shift*), 1/m */
+    int carrier_applied;          /* 1 when the carrier shift branch ran */
+    int wrap_checked;             /* 1 when spectralRadius ran */
+    double spectral_radius;       /* f_sig: 90 % spectral power radius, 1/m */
+    double rms_radius_in;         /* fraunhofer input support D, m */
+    double dx_out;                /* output pixel pitch (fraunhofer changes it), m */
+    int warn_count[WOS_W_COUNT];
+    double warn_value[WOS_W_COUNT];
+} wos_diag;
+
+/* Host field: optics.Field (optics/field.go:14-22), generalised to ny x nx. */
+typedef struct {
+    int ny, nx;
+    double dx;
+    int polarized;       /* 1: ey is propagated too */
+    wos_c128* ex;
+    wos_c128* ey;
+} wos_field;
+
+/* Parametric refractive index n(x,y,z) of a split-step medium (the IndexFunc
+ * closure of optics/medium.go:8 cannot cross the ABI; this descriptor covers
+ * uniform, stratified, graded-core, z-modulated and absorbing-border media):
+ *   Re n = re0(z) + core_dn * exp(-((x-x0)^2+(y-y0)^2)/core_w^2)
+ *                 * (1 + zmod_amp * sin(2 pi z / zmod_period + zmod_phase))
+ *   Im n = im0(z) + border_strength * ((border_px - d)/border_px)^border_order, d < border_px
+ * where d is the pixel distance to the nearest window edge and (re0, im0)(z)
+ * is layer k for the first k with z < layer_z[k], else (re_bg, im_bg). */
+typedef struct {
+    double re_bg, im_bg;
+    double core_dn, core_x0, core_y0, core_w;
+    double zmod_amp, zmod_period, zmod_phase;
+    int border_px;
+    int border_order;
+    double border_strength;
+    int n_layers;
+    double layer_z[8];
+    double layer_re[8];
+    double layer_im[8];
+} wos_index_desc;
+
+/* ---- device and context (replaces gpuInit / GPUAvailable / GPUBackendInfo,
+ *      optics/gpu.go:106-143) ---- */
+WOS_API int wos_device_count(void);
+WOS_API int wos_device_name(int device, char* buf, int buflen);
+WOS_API int wos_ctx_create(int device, int precision, wos_ctx* out);
+WOS_API int wos_ctx_destroy(wos_ctx ctx);
+/* Use the caller's CUDA stream (cudaStream_t) instead of the context's own. */
+WOS_API int wos_ctx_set_stream(wos_ctx ctx, void* stream);
+WOS_API void* wos_ctx_get_stream(wos_ctx ctx);
+WOS_API int wos_ctx_precision(wos_ctx ctx);
+/* Columns per CTA of the fused column pass (power of two; 0 = automatic). */
+WOS_API int wos_ctx_set_col_width(wos_ctx ctx, int w);
+WOS_API int wos_ctx_synchronize(wos_ctx ctx);
+/* Per-launch CUDA-event profile on the context stream (no counterpart in the
+ * reference, whose only timers are Result.ElapsedMS and Go benchmarks).
+ * kind: 0 row forward, 1 row inverse, 2 row inverse.screen.forward,
+ * 3 row inverse.accumulate, 4 column fused (FFT.H.IFFT), 5 column Fraunhofer,
+ * 6 column reduction, 7 column FFT.  Reading synchronises outstanding events. */
+WOS_API int wos_ctx_set_profiling(wos_ctx ctx, int on);
+WOS_API int wos_ctx_profile(wos_ctx ctx, int kind, double* total_ms, long long* launches);
+WOS_API int wos_ctx_profile_reset(wos_ctx ctx);
+/* Number of sweep kernels this context has launched since the last reset. */
+WOS_API long long wos_ctx_launch_count(wos_ctx ctx);
+/* The specialised power-of-two ASM sweeps (default on); off forces the general
+ * sweeps, which compute the same transform. */
+WOS_API int wos_ctx_set_fast_path(wos_ctx ctx, int enabled);
+/* Autotuner of the specialised sweeps (no counterpart in the reference): times
+ * every (row elements/thread, column elements/thread, columns/CTA) launch
+ * configuration for an ny x nx grid on this device and keeps the fastest for
+ * the context; wos_ctx_set_tune installs a configuration from a cache. */
+WOS_API int wos_autotune(wos_ctx ctx, int ny, int nx, int* row_e, int* col_e, int* col_w);
+WOS_API int wos_ctx_set_tune(wos_ctx ctx, int ny, int nx, int row_e, int col_e, int col_w);
+WOS_API const char* wos_status_string(int status);
+WOS_API const char* wos_last_error(void);
+WOS_API const char* wos_backend_info(void);
+
+/* ---- FFT users outside the propagators (fft2D / fft1DAny callers,
+ *      optics/fft.go:135-142,209-216; gpuFFT2D / gpuFFT1D, optics/gpu.go:275-304).
+ *      Host complex128 in place; inverse scales by 1/n per axis like fft1D. ---- */
+WOS_API int wos_fft2d(wos_ctx ctx, int ny, int nx, wos_c128* a, int inverse);
+WOS_API int wos_fft1d(wos_ctx ctx, int n, wos_c128* a, int inverse);
+WOS_API int wos_fft2d_dev(wos_ctx ctx, int ny, int nx, int batch, void* a, int inverse);
+
+/* ---- Propagate (optics/propagate.go:65-102): the host Field in place. ---- */
+WOS_API int wos_propagate(wos_ctx ctx, wos_field* f, double z, int method, const wos_context* c,
+                  wos_diag* diag /* may be NULL */);
+
+/* Device-resident variant: in/out hold ncomp components [ncomp][ny][nx] in the
+ * context precision; in == out is allowed.  dx_out returns the output pitch
+ * through diag. */
+WOS_API int wos_propagate_dev(wos_ctx ctx, int ny, int nx, double dx, int ncomp, const void* in, void* out,
+                      double z, int method, const wos_context* c, wos_diag* diag);
+
+/* Device-resident variant with complex128 device I/O in either precision
+ * (the FP32 pipeline converts inside its first and last sweep). */
+WOS_API int wos_propagate_dev_c128(wos_ctx ctx, int ny, int nx, double dx, int ncomp, const void* in,
+                           void* out, double z, int method, const wos_context* c, wos_diag* diag);
+
+/* ---- PropagateSplitStep (optics/medium.go:22-45) with a parametric medium. ---- */
+WOS_API int wos_splitstep(wos_ctx ctx, wos_field* f, double z, const wos_index_desc* n, int steps,
+                  const wos_context* c, wos_diag* diag);
+WOS_API int wos_splitstep_dev(wos_ctx ctx, int ny, int nx, double dx, int ncomp, void* field, double z,
+                      const wos_index_desc* n, int steps, const wos_context* c, wos_diag* diag);
+/* Sampled medium: n_re / n_im are host FP64 maps [nmaps][ny][nx]; nmaps == 1
+ * for a z-independent medium, else nmaps == steps (slice s uses map s). */
+WOS_API int wos_splitstep_maps(wos_ctx ctx, wos_field* f, double z, const double* n_re, const double* n_im,
+                       int nmaps, int steps, const wos_context* c, wos_diag* diag);
+
+/* ---- PropagatePolychromatic (optics/polychromatic.go:18-44): out[ny*nx] FP64
+ *      intensity sum_k weight_k |U_k|^2; the input field is not modified.
+ *      The batch entry points accumulate the warnings of every unit into diag
+ *      (the reference's shared ctx.Warnings). ---- */
+WOS_API int wos_polychromatic(wos_ctx ctx, const wos_field* f, double z, const double* wavelengths,
+                      const double* weights, int nsamples, int method, const wos_context* base,
+                      double* out, wos_diag* diag /* may be NULL */);
+
+/* ---- Propagate3D (optics/volume.go:8-18): out = nz * ncomp * ny*nx complex128,
+ *      plane q is the input propagated to zs[q] (zs[q] == 0 copies the input). ---- */
+WOS_API int wos_volume(wos_ctx ctx, const wos_field* f, const double* zs, int nz, int method,
+               const wos_context* c, wos_c128* out, wos_diag* diag);
+
+/* ---- GenerateSchellRealizations + PropagatePartiallyCoherent + AverageIntensity
+ *      (optics/coherence.go:22-116).  noise holds m*n*n complex values that take
+ *      the place of complex(rng.NormFloat64(), rng.NormFloat64())/sqrt2. ---- */
+WOS_API int wos_schell_modes(wos_ctx ctx, int n, double dx, double width, double coherence, int m,
+                     const wos_c128* noise, wos_c128* modes_out);
+WOS_API int wos_partially_coherent(wos_ctx ctx, int n, double dx, double width, double coherence, int m,
+                           const wos_c128* noise, double z, int method, const wos_context* c,
+                           double* out, wos_diag* diag);
+
+/* ---- thin-element multiply (optics/elements.go:128-141,195-221,288-313,488-532). ---- */
+WOS_API int wos_apply_lens(wos_ctx ctx, wos_field* f, double wavelength, double focal, double aperture,
+                   double x0, double y0);
+WOS_API int wos_apply_aperture_circle(wos_ctx ctx, wos_field* f, double radius, double x0, double y0,
+                              double edge_sigma);
+/* kind: 0 amplitude_sin, 1 amplitude_binary, 2 phase_sin, 3 phase_binary, 4 blazed */
+WOS_API int wos_apply_grating(wos_ctx ctx, wos_field* f, int kind, double period, double modulation,
+                      double duty, double blaze_depth, double rotation, double offset);
+WOS_API int wos_apply_phase_mask(wos_ctx ctx, wos_field* f, const double* phi, double amp);
+
+/* ---- inverse design (no counterpart in the reference): ASM forward / adjoint.
+ *      u = ASM_z(a * exp(i phi)), L = sum (|u|^2 - T)^2, grad = dL/dphi. ---- */
+WOS_API int wos_asm_forward_loss(wos_ctx ctx, int ny, int nx, double dx, double z, const wos_context* c,
+                         const wos_c128* a, const double* phi, const double* target, double* loss);
+WOS_API int wos_asm_loss_grad(wos_ctx ctx, int ny, int nx, double dx, double z, const wos_context* c,
+                      const wos_c128* a, const double* phi, const double* target, double* loss,
+                      double* grad);
+/* Adjoint operator A^H = F^-1 diag(conj H) F of an ASM step, host field in place. */
+WOS_API int wos_asm_adjoint(wos_ctx ctx, wos_field* f, double z, const wos_context* c);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

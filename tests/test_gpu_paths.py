@@ -1,0 +1,56 @@
+"""The specialised power-of-two ASM sweeps agree with the general sweeps and
+with the oracle, for every launch configuration the autotuner may pick."""
+import numpy as np
+import pytest
+
+import oracle as O
+from gpu_util import rel_l2, tol, wos
+
+pytestmark = pytest.mark.gpu
+
+
+def field(n, seed=3):
+    rng = np.random.default_rng(seed)
+    return np.exp(1j * rng.uniform(0, 2 * np.pi, (n, n)))
+
+
+@pytest.mark.parametrize("prec", [wos.FP64, wos.FP32], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("n", [256, 512, 1024, 2048])
+def test_fast_equals_general(prec, n):
+    dx, wl, z = 2e-6, 632.8e-9, 3e-3
+    ex = field(n)
+    with wos.GPU(prec) as g:
+        a = wos.Field(ex.copy(), dx)
+        ca = wos.Context(wavelength=wl)
+        g.propagate(a, z, "asm", ca)
+        g.set_fast_path(False)
+        b = wos.Field(ex.copy(), dx)
+        cb = wos.Context(wavelength=wl)
+        g.propagate(b, z, "asm", cb)
+    assert rel_l2(a.ex, b.ex) <= tol(prec)
+    assert ca.warnings.keys() == cb.warnings.keys()
+    if n <= 512:
+        o = O.Field(ex.copy(), dx)
+        O.propagate(o, z, "asm", O.Context(wavelength=wl))
+        assert rel_l2(a.ex, o.ex) <= tol(prec)
+
+
+@pytest.mark.parametrize("prec", [wos.FP64, wos.FP32], ids=["fp64", "fp32"])
+def test_every_launch_configuration(prec):
+    n, dx, wl, z = 512, 1e-6, 5e-7, 2e-4
+    ex = field(n, 4)
+    o = O.Field(ex.copy(), dx)
+    O.propagate(o, z, "asm", O.Context(wavelength=wl))
+    with wos.GPU(prec) as g:
+        best = g.autotune(n, n)
+        assert best[0] in (8, 16) and best[1] in (8, 16) and best[2] >= 1
+        for re in (8, 16):
+            for ce in (8, 16):
+                for w in (1, 2, 4, 8):
+                    try:
+                        g.set_tune(n, n, re, ce, w)
+                    except wos.WosError:
+                        continue
+                    f = wos.Field(ex.copy(), dx)
+                    g.propagate(f, z, "asm", wos.Context(wavelength=wl))
+                    assert rel_l2(f.ex, o.ex) <= tol(prec), (re, ce, w)

@@ -1,0 +1,2274 @@
+// wos_api.cu -- the C ABI of libwosgpu.so (include/wos_gpu.h).
+//
+// Each entry point restates one function of the reference's Go `optics`
+// package as a sequence of sm_100a sweeps (wos_kernels.cu).  Host-visible
+// behaviour (z == 0 early return, nil-context defaults, evanescent policy,
+// warning codes and values) follows the cited reference lines; the numerics
+// run on the device, with no CPU fallback.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/wos_gpu.h"
+#include "wos_fast.cuh"
+#include "wos_kernels.cuh"
+
+using namespace wos;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int st, const std::string& msg) {
+    g_err = msg;
+    return st;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            return fail(e_ == cudaErrorMemoryAllocation ? WOS_OOM : WOS_CUDA_ERROR,           \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+        }                                                                                     \
+    } while (0)
+
+#define TRY(x)                  \
+    do {                        \
+        int rc_ = (x);          \
+        if (rc_ != WOS_OK) return rc_; \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t n = 0;
+};
+
+int ensure(DevBuf& b, size_t bytes) {
+    if (b.n >= bytes && b.p) return WOS_OK;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.n = 0;
+    if (bytes == 0) return WOS_OK;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(WOS_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    b.n = bytes;
+    return WOS_OK;
+}
+
+bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+int next_pow2(int n) {
+    int m = 1;
+    while (m < n) m <<= 1;
+    return m;
+}
+
+// Everything needed to transform a line of logical length n in one precision.
+struct Axis {
+    int n = 0, L = 0, blue = 0;
+    void* tw = nullptr;
+    void* chirp = nullptr;
+    void* bf = nullptr;
+    void* bi = nullptr;
+};
+
+constexpr int kMaxL32 = 8192;  // largest line held on chip (threads x elements)
+constexpr int kMaxL64 = 8192;
+
+// Launch configuration of the specialised sweeps for one grid: elements per
+// thread of the row and column passes, columns per CTA.
+struct Tune {
+    int rowE, colE, colW;
+};
+long long tune_key(int fp64, int ny, int nx) { return ((long long)fp64 << 62) | ((long long)ny << 31) | nx; }
+
+}  // namespace
+
+struct wos_ctx_s {
+    int device = 0;
+    int fp64 = 0;
+    cudaStream_t st = nullptr;
+    bool own_stream = false;
+    std::mutex mu;
+    std::map<int, Axis> axes[2];  // [fp64][n]
+    DevBuf stage, scratch, scratch2, scratch3, red, redout, tmp, maps, params, vol, accum, aux;
+    double* hred = nullptr;  // pinned mirror of redout
+    size_t hred_n = 0;
+    int colw = 0;
+    bool no_fast = false;               // force the general sweeps (tests compare both)
+    std::map<long long, Tune> tune;     // autotuned launch configurations
+    size_t csz() const { return fp64 ? 16 : 8; }
+    // per-launch CUDA-event profile (wos_ctx_set_profiling): a ring of event
+    // pairs; a slot's elapsed time is folded into its kind when it is reused
+    // or read, by which time the pair has long completed.
+    static constexpr int kRing = 1024;
+    bool prof_on = false, prof_made = false;
+    cudaEvent_t ev0[kRing], ev1[kRing];
+    int ev_kind[kRing];
+    bool ev_used[kRing];
+    int ev_head = 0;
+    double prof_ms[8] = {0};
+    long long prof_n[8] = {0};
+    long long launches = 0;
+};
+
+namespace {
+
+int set_device(wos_ctx c) {
+    CK(cudaSetDevice(c->device));
+    return WOS_OK;
+}
+
+void prof_fold(wos_ctx c, int slot) {
+    if (!c->ev_used[slot]) return;
+    float ms = 0;
+    if (cudaEventSynchronize(c->ev1[slot]) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, c->ev0[slot], c->ev1[slot]) == cudaSuccess) {
+        c->prof_ms[c->ev_kind[slot]] += ms;
+        c->prof_n[c->ev_kind[slot]] += 1;
+    }
+    cudaGetLastError();
+    c->ev_used[slot] = false;
+}
+
+// Kinds: 0..3 row modes (fwd, inv, inv.screen.fwd, inv.accumulate), 4..7 column
+// modes (fused, fraunhofer, reduce, fft).
+template <typename F>
+cudaError_t timed_launch(wos_ctx c, int kind, F&& launch) {
+    c->launches++;
+    if (!c->prof_on) return launch();
+    const int slot = c->ev_head;
+    prof_fold(c, slot);
+    cudaEventRecord(c->ev0[slot], c->st);
+    cudaError_t e = launch();
+    cudaEventRecord(c->ev1[slot], c->st);
+    c->ev_kind[slot] = kind;
+    c->ev_used[slot] = true;
+    c->ev_head = (slot + 1) % wos_ctx_s::kRing;
+    return e;
+}
+cudaError_t prof_rows(wos_ctx c, int fp64, const RowArgs& a) {
+    return timed_launch(c, a.mode & 3, [&] { return launch_rows(fp64, a, c->st); });
+}
+cudaError_t prof_cols(wos_ctx c, int fp64, const ColArgs& a) {
+    return timed_launch(c, 4 + (a.mode & 3), [&] { return launch_cols(fp64, a, c->st); });
+}
+
+int get_axis(wos_ctx c, int n, int fp64, Axis** out);
+
+int build_axis(wos_ctx c, int n, int fp64, Axis& ax) {
+    const size_t cs = fp64 ? 16 : 8;
+    ax.n = n;
+    ax.blue = is_pow2(n) ? 0 : 1;
+    ax.L = ax.blue ? next_pow2(2 * n - 1) : n;
+    if (n < 2) return fail(WOS_UNSUPPORTED_SIZE, "line length must be >= 2");
+    if (ax.L > (fp64 ? kMaxL64 : kMaxL32))
+        return fail(WOS_UNSUPPORTED_SIZE, "line length " + std::to_string(n) + " exceeds the on-chip limit (" +
+                                              std::to_string(fp64 ? kMaxL64 : kMaxL32) + " transform points)");
+    CK(cudaMalloc(&ax.tw, cs * ax.L));
+    CK(launch_twiddles(fp64, ax.tw, ax.L, c->st));
+    if (!ax.blue) return WOS_OK;
+    CK(cudaMalloc(&ax.chirp, cs * n));
+    CK(cudaMalloc(&ax.bf, cs * ax.L));
+    CK(cudaMalloc(&ax.bi, cs * ax.L));
+    // b0 kernels in FP64, transformed with the FP64 power-of-two axis of M
+    Axis* m64 = nullptr;
+    TRY(get_axis(c, ax.L, 1, &m64));
+    double2* b0 = nullptr;
+    CK(cudaMalloc(&b0, sizeof(double2) * 2 * ax.L));
+    CK(launch_chirp_b0(fp64, ax.chirp, b0, b0 + ax.L, n, ax.L, c->st));
+    RowArgs r{};
+    r.mode = ROW_FWD;
+    r.rows = 2;
+    r.L = ax.L;
+    r.ny_grid = 2;
+    r.nx_grid = ax.L;
+    r.dx = 1;
+    r.in = b0;
+    r.in_ld = ax.L;
+    r.in_off = 0;
+    r.in_n = ax.L;
+    r.out = b0;
+    r.out_ld = ax.L;
+    r.out_off = 0;
+    r.out_n = ax.L;
+    r.out_scale = 1;
+    r.tw = m64->tw;
+    r.batch = 1;
+    CK(prof_rows(c, 1, r));
+    CK(launch_bhat_finish(fp64, ax.bf, ax.bi, b0, b0 + ax.L, ax.L, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    cudaFree(b0);
+    return WOS_OK;
+}
+
+int get_axis(wos_ctx c, int n, int fp64, Axis** out) {
+    auto& m = c->axes[fp64];
+    auto it = m.find(n);
+    if (it != m.end()) {
+        *out = &it->second;
+        return WOS_OK;
+    }
+    Axis ax;
+    int rc = build_axis(c, n, fp64, ax);
+    if (rc != WOS_OK) {
+        if (ax.tw) cudaFree(ax.tw);
+        if (ax.chirp) cudaFree(ax.chirp);
+        if (ax.bf) cudaFree(ax.bf);
+        if (ax.bi) cudaFree(ax.bi);
+        return rc;
+    }
+    auto res = m.emplace(n, ax);
+    *out = &res.first->second;
+    return WOS_OK;
+}
+
+void fill_axis(RowArgs& r, const Axis* a) {
+    r.L = a->L;
+    r.blue_n = a->blue ? a->n : 0;
+    r.tw = a->tw;
+    r.chirp = a->chirp;
+    r.bhat_f = a->bf;
+    r.bhat_i = a->bi;
+}
+void fill_axis(ColArgs& r, const Axis* a) {
+    r.L = a->L;
+    r.blue_n = a->blue ? a->n : 0;
+    r.tw = a->tw;
+    r.chirp = a->chirp;
+    r.bhat_f = a->bf;
+    r.bhat_i = a->bi;
+}
+
+RowArgs row_defaults(int ny, int nx, double dx) {
+    RowArgs r{};
+    r.ny_grid = ny;
+    r.nx_grid = nx;
+    r.dx = dx;
+    r.out_scale = 1.0;
+    r.pre_amp = 1.0;
+    r.weight = 1.0;
+    r.batch = 1;
+    return r;
+}
+ColArgs col_defaults(wos_ctx c, double dx) {
+    ColArgs a{};
+    a.h.scale = 1.0;
+    a.h.dx = dx;
+    a.h.c_re = 1.0;
+    a.h.exact = c->fp64;
+    a.hist_dx = dx;
+    a.out_scale = 1.0;
+    a.batch = 1;
+    a.W = c->colw;
+    return a;
+}
+
+// Columns per CTA of the fused pass.  Adjacent columns give 64 B row segments
+// (8 x complex64, 4 x complex128) while the tile stays within shared memory.
+int auto_colw_p(wos_ctx c, int fp64, int L) {
+    if (c->colw > 0) return c->colw;
+    const int E = pick_E(fp64, L);
+    const int T = L / E;
+    const int maxt = max_threads_for(fp64, E);
+    int W = fp64 ? 4 : 8;
+    while (W > 1 && (W * T > maxt || col_smem_bytes(fp64, L, W) > 200 * 1024)) W >>= 1;
+    return W;
+}
+int auto_colw(wos_ctx c, int L) { return auto_colw_p(c, c->fp64, L); }
+
+// ---- reductions: partial region r, finished into redout[r]
+constexpr int kRegions = 8;
+struct Red {
+    wos_ctx c;
+    size_t per_region = 0;  // doubles per region
+};
+
+int red_prepare(wos_ctx c, size_t max_blocks) {
+    const size_t per = max_blocks * RS_COUNT;
+    TRY(ensure(c->red, per * kRegions * sizeof(double)));
+    TRY(ensure(c->redout, (size_t)kRegions * RS_COUNT * sizeof(double) * 1));
+    if (!c->hred || c->hred_n < (size_t)kRegions * RS_COUNT) {
+        if (c->hred) cudaFreeHost(c->hred);
+        CK(cudaMallocHost(&c->hred, sizeof(double) * kRegions * RS_COUNT));
+        c->hred_n = kRegions * RS_COUNT;
+    }
+    return WOS_OK;
+}
+double* red_region(wos_ctx c, int r) {
+    const size_t per = c->red.n / sizeof(double) / kRegions;
+    return reinterpret_cast<double*>(c->red.p) + per * r;
+}
+size_t red_region_blocks(wos_ctx c) { return c->red.n / sizeof(double) / kRegions / RS_COUNT; }
+double* redout_region(wos_ctx c, int r) { return reinterpret_cast<double*>(c->redout.p) + (size_t)RS_COUNT * r; }
+
+// blocks of a row launch (mirrors launch_rows_t) and of a column launch
+size_t row_blocks(int fp64, int L, int rows, int batch) {
+    const int E = pick_E(fp64, L);
+    const int T = L / E;
+    int lines = 1;
+    while (lines * 2 * T <= 256 && lines * 2 <= rows) lines *= 2;
+    while (lines * T < 32) lines *= 2;
+    return (size_t)((rows + lines - 1) / lines) * std::max(batch, 1);
+}
+size_t col_blocks(int fp64, int L, int W, int ncols, int batch) {
+    const int E = pick_E(fp64, L);
+    const int T = L / E;
+    const int maxt = max_threads_for(fp64, E);
+    while (W * T < 32) W *= 2;
+    while (W > 1 && W * T > maxt) W /= 2;
+    return (size_t)((ncols + W - 1) / W) * std::max(batch, 1);
+}
+
+// ---- evanescent policy (optics/propagate.go:186-199)
+struct Policy {
+    int zero = 0, reg = 0;
+    double alpha = 0, limit = 0;
+};
+Policy ev_policy(const wos_context& c, double z) {
+    Policy p;
+    p.limit = c.evanescent_limit;
+    if (z < 0) {
+        if (c.backward_regularize) {
+            p.alpha = c.tikhonov_alpha;
+            if (p.alpha <= 0) p.alpha = 1e-3;
+            p.reg = 1;
+            return p;
+        }
+        p.zero = 1;
+        return p;
+    }
+    p.zero = c.evanescent_zero;
+    return p;
+}
+
+void warn_add(wos_diag* d, int bit, double value) {
+    if (!d) return;
+    d->warn_count[bit]++;
+    if (value != 0) d->warn_value[bit] = value;
+}
+
+// asmWarn (optics/propagate.go:203-218)
+void asm_warn(wos_diag* d, double z, double pin, double pout, const Policy& p) {
+    if (pin > 0 && pout < pin * (1 - 1e-8) && z > 0)
+        warn_add(d, WOS_W_EVANESCENT_FILTERED, (pin - pout) / pin);
+    if (z < 0) {
+        if (p.reg) warn_add(d, WOS_W_BACKWARD_REGULARIZED, 0);
+        else if (p.zero) warn_add(d, WOS_W_BACKWARD_EVANESCENT, 0);
+    }
+}
+
+// spectralRadius tail (optics/propagate.go:309-319) from the 97-bin histogram
+double spectral_radius_from_hist(const double* hist, double dx, double frac) {
+    const int bins = 96;
+    const double fnyq = 1 / (2 * dx);
+    double tot = 0;
+    for (int b = 0; b <= bins; b++) tot += hist[b];
+    if (tot <= 0) return 0;
+    double run = 0;
+    for (int b = 0; b <= bins; b++) {
+        run += hist[b];
+        if (run >= frac * tot) return (double)b / bins * fnyq;
+    }
+    return fnyq;
+}
+
+// asmWrapWarn decision (optics/propagate.go:247-264); carry = min(nx,ny)*dx
+bool wrap_needed(const wos_context& c, int ny, int nx, double dx, double z) {
+    const double carry = (double)std::min(nx, ny) * dx;
+    if (!c.diagnostics || z == 0 || carry <= 0) return false;
+    return std::fabs(z) * c.wavelength / (2 * dx) > carry;
+}
+void wrap_finish(wos_diag* d, const wos_context& c, int ny, int nx, double dx, double z, const double* hist) {
+    const double carry = (double)std::min(nx, ny) * dx;
+    const double fsig = spectral_radius_from_hist(hist, dx, 0.90);
+    if (d) {
+        d->wrap_checked = 1;
+        d->spectral_radius = fsig;
+    }
+    if (fsig <= 0) return;
+    const double walk = std::fabs(z) * c.wavelength * fsig;
+    if (walk > carry) warn_add(d, WOS_W_ASM_ALIAS_WRAP, walk / carry);
+}
+
+// ---------------------------------------------------------------- pipeline
+struct Prop {
+    int ny, nx;
+    double dx;
+    int ncomp;
+    const void* in;
+    int in_c128;
+    void* out;
+    int out_c128;
+    double z;
+    int method;
+    wos_context c;
+    wos_diag* diag;
+};
+
+// Fetch finished reduction regions [0, n) to the host (one synchronisation).
+int fetch_red(wos_ctx c, int nreg) {
+    CK(cudaMemcpyAsync(c->hred, c->redout.p, sizeof(double) * RS_COUNT * nreg, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+HArgs asm_h(wos_ctx c, const wos_context& cc, double z, const Policy& p, double dx, int lfx, int lfy) {
+    HArgs h{};
+    h.kind = H_ASM;
+    h.exact = c->fp64;
+    h.wl = cc.wavelength;
+    h.k = 2 * M_PI / cc.wavelength;
+    h.z = z;
+    h.kz = h.k * z;
+    h.kaz = h.k * std::fabs(z);
+    h.zero_ev = p.zero;
+    h.reg = p.reg;
+    h.alpha = p.alpha;
+    h.limit = p.limit;
+    h.dx = dx;
+    h.lfx = lfx;
+    h.lfy = lfy;
+    h.scale = 1.0 / ((double)lfx * (double)lfy);
+    h.c_re = 1;
+    return h;
+}
+
+// Forward row pass of an unpadded field into `dst` (native), plus a column
+// reduction: spectral centroid sums and/or the radial histogram.
+int spectrum_stats(wos_ctx c, const Prop& p, void* dst, bool centroid, bool hist, int shift, double fxc,
+                   double fyc, int region, int* blocks_out) {
+    Axis *ax, *ay;
+    TRY(get_axis(c, p.nx, c->fp64, &ax));
+    TRY(get_axis(c, p.ny, c->fp64, &ay));
+    const long long np = (long long)p.ny * p.nx;
+    RowArgs r = row_defaults(p.ny, p.nx, p.dx);
+    r.mode = ROW_FWD;
+    r.rows = p.ny;
+    fill_axis(r, ax);
+    r.in = p.in;
+    r.in_c128 = p.in_c128;
+    r.in_ld = p.nx;
+    r.in_bstride = np;
+    r.in_off = 0;
+    r.in_n = p.nx;
+    r.out = dst;
+    r.out_ld = p.nx;
+    r.out_bstride = np;
+    r.out_off = 0;
+    r.out_n = p.nx;
+    r.pre_shift = shift;
+    r.fxc = fxc;
+    r.fyc = fyc;
+    r.batch = p.ncomp;
+    const int W = auto_colw(c, ay->L);
+    const size_t nbc = col_blocks(c->fp64, ay->L, W, p.nx, p.ncomp);
+    TRY(red_prepare(c, nbc));
+    CK(prof_rows(c, c->fp64, r));
+    ColArgs a = col_defaults(c, p.dx);
+    a.mode = COL_REDUCE;
+    a.ncols = p.nx;
+    fill_axis(a, ay);
+    a.W = W;
+    a.src = dst;
+    a.src_ld = p.nx;
+    a.src_bstride = np;
+    a.in_off = 0;
+    a.in_n = p.ny;
+    a.red = red_region(c, region);
+    a.red_spec = centroid;
+    a.red_hist = hist;
+    a.hist_lx = p.nx;
+    a.hist_ly = p.ny;
+    a.hist_dx = p.dx;
+    a.batch = p.ncomp;
+    CK(prof_cols(c, c->fp64, a));
+    const int nb = (int)nbc;
+    if (centroid) CK(launch_reduce_finish(a.red, nb, 1, RS_SW, 3, redout_region(c, region), c->st));
+    if (hist) CK(launch_reduce_finish(a.red, nb, 1, RS_HIST, 97, redout_region(c, region), c->st));
+    if (blocks_out) *blocks_out = nb;
+    return WOS_OK;
+}
+
+// The three-sweep propagator shared by asm / asm_shift / asm_pad /
+// asm_shift_pad / fresnel_tf / fresnel_ir:
+//   rows:  in (ny x nx) -> scratch rows, forward transform over mx points
+//   cols:  forward over my points, H, inverse, keep rows [offy, offy+ny)
+//   rows:  inverse over mx points, keep columns [offx, offx+nx) -> out
+// pad = 1 doubles both axes (zero-padded linear convolution,
+// optics/propagate.go:346-387); the padding is folded into addressing.
+struct Sweep3 {
+    int pad = 0;
+    int shift = 0;
+    double fxc = 0, fyc = 0;
+    HArgs h{};
+    bool red_pin = false, red_pout = false, hist = false;
+    bool red_loss = false;  // spectral power-loss sums of the H_ASM step (region 1)
+    bool fast = false;      // set when the specialised sweeps ran (no crop sums)
+};
+
+int env_int(const char* name, int def) {
+    const char* v = std::getenv(name);
+    return (v && *v) ? std::atoi(v) : def;
+}
+
+Tune get_tune(wos_ctx c, int ny, int nx) {
+    auto it = c->tune.find(tune_key(c->fp64, ny, nx));
+    if (it != c->tune.end()) return it->second;
+    Tune t;
+    t.rowE = env_int("WOS_ROWE", c->fp64 ? (nx >= 8192 ? 16 : 8) : 16);
+    t.colE = env_int("WOS_COLE", c->fp64 ? (ny >= 8192 ? 16 : 8) : 16);
+    t.colW = env_int("WOS_COLW", c->fp64 ? 2 : 4);
+    if (c->colw > 0) t.colW = c->colw;
+    return t;
+}
+
+size_t fast_row_blocks(int L, int E, int rows, int batch) {
+    const int T = L / E;
+    int lines = 1;
+    while (lines * 2 * T <= 256 && lines * 2 <= rows) lines *= 2;
+    while (lines * T < 32) lines *= 2;
+    return (size_t)((rows + lines - 1) / lines) * std::max(batch, 1);
+}
+size_t fast_col_blocks(int fp64, int L, int E, int W, int ncols, int batch) {
+    const int T = L / E;
+    const int maxt = (E >= 16 || fp64) ? 512 : 1024;
+    while (W * T < 32) W *= 2;
+    while (W > 1 && W * T > maxt) W /= 2;
+    return (size_t)((ncols + W - 1) / W) * std::max(batch, 1);
+}
+
+// Plain band-limited ASM on power-of-two grids through the specialised
+// sweeps.  Returns -1 when the grid is not covered (the general sweeps run).
+int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
+    if (!is_pow2(p.nx) || !is_pow2(p.ny)) return -1;
+    const Tune t = get_tune(c, p.ny, p.nx);
+    if (!fast_supported(c->fp64, p.nx, t.rowE) || !fast_supported(c->fp64, p.ny, t.colE)) return -1;
+    Axis *ax, *ay;
+    TRY(get_axis(c, p.nx, c->fp64, &ax));
+    TRY(get_axis(c, p.ny, c->fp64, &ay));
+    const long long np = (long long)p.ny * p.nx;
+    void* S;
+    if (!p.out_c128) {
+        S = p.out;
+    } else {
+        TRY(ensure(c->scratch, (size_t)np * p.ncomp * c->csz()));
+        S = c->scratch.p;
+    }
+    const size_t nbr = fast_row_blocks(p.nx, t.rowE, p.ny, p.ncomp);
+    const size_t nbc = fast_col_blocks(c->fp64, p.ny, t.colE, t.colW, p.nx, p.ncomp);
+    if (s.red_pin || s.red_pout || s.red_loss) TRY(red_prepare(c, std::max(nbr, nbc)));
+    int nb = 0;
+    FastRows r{};
+    r.rows = p.ny;
+    r.in = p.in;
+    r.in_c128 = p.in_c128;
+    r.in_ld = p.nx;
+    r.in_bstride = np;
+    r.out = S;
+    r.out_ld = p.nx;
+    r.out_bstride = np;
+    r.tw = ax->tw;
+    r.out_scale = 1.0;
+    r.red = s.red_pin ? red_region(c, 0) + RS_P : nullptr;
+    r.red_stride = RS_COUNT;
+    r.batch = p.ncomp;
+    CK(timed_launch(c, 0, [&] { return fast_rows(c->fp64, p.nx, t.rowE, false, r, c->st, &nb); }));
+    if (s.red_pin) CK(launch_reduce_finish(red_region(c, 0), (int)nbr, 1, RS_P, 1, redout_region(c, 0), c->st));
+    FastCols k{};
+    k.ncols = p.nx;
+    k.W = t.colW;
+    k.data = S;
+    k.ld = p.nx;
+    k.bstride = np;
+    k.tw = ay->tw;
+    k.batch = p.ncomp;
+    k.wl = s.h.wl;
+    k.dx = s.h.dx;
+    k.kz = s.h.kz;
+    k.kaz = s.h.kaz;
+    k.scale = s.h.scale;
+    k.alpha = s.h.alpha;
+    k.limit = s.h.limit;
+    k.zero_ev = s.h.zero_ev;
+    k.reg = s.h.reg;
+    k.backward = s.h.z < 0;
+    k.conj = s.h.conj;
+    k.red = s.red_loss ? red_region(c, 1) + RS_SW : nullptr;
+    k.red_stride = RS_COUNT;
+    CK(timed_launch(c, 4, [&] { return fast_cols(c->fp64, p.ny, t.colE, k, c->st, &nb); }));
+    if (s.red_loss) CK(launch_reduce_finish(red_region(c, 1), (int)nbc, 1, RS_SW, 2, redout_region(c, 1), c->st));
+    FastRows q{};
+    q.rows = p.ny;
+    q.in = S;
+    q.in_ld = p.nx;
+    q.in_bstride = np;
+    q.out = p.out;
+    q.out_c128 = p.out_c128;
+    q.out_ld = p.nx;
+    q.out_bstride = np;
+    q.tw = ax->tw;
+    q.out_scale = 1.0;
+    q.red = s.red_pout ? red_region(c, 2) + RS_P : nullptr;
+    q.red_stride = RS_COUNT;
+    q.batch = p.ncomp;
+    CK(timed_launch(c, 1, [&] { return fast_rows(c->fp64, p.nx, t.rowE, true, q, c->st, &nb); }));
+    if (s.red_pout) CK(launch_reduce_finish(red_region(c, 2), (int)nbr, 1, RS_P, 1, redout_region(c, 2), c->st));
+    s.fast = true;
+    return WOS_OK;
+}
+
+int run_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
+    if (!s.pad && !s.shift && s.h.kind == H_ASM && !s.hist && s.h.fxoff == 0 && s.h.fyoff == 0 &&
+        !c->no_fast) {
+        const int rc = try_fast_sweep3(c, p, s);
+        if (rc != -1) return rc;
+    }
+    const int mx = s.pad ? 2 * p.nx : p.nx;
+    const int my = s.pad ? 2 * p.ny : p.ny;
+    const int offx = s.pad ? p.nx / 2 : 0, offy = s.pad ? p.ny / 2 : 0;
+    Axis *ax, *ay;
+    TRY(get_axis(c, mx, c->fp64, &ax));
+    TRY(get_axis(c, my, c->fp64, &ay));
+    const long long np_in = (long long)p.ny * p.nx;
+    const long long np_s = (long long)p.ny * mx;
+    // scratch: the output buffer itself when it is native and unpadded
+    void* S;
+    if (!s.pad && !p.out_c128) {
+        S = p.out;
+    } else {
+        TRY(ensure(c->scratch, (size_t)np_s * p.ncomp * c->csz()));
+        S = c->scratch.p;
+    }
+    const int W = auto_colw(c, ay->L);
+    const size_t nbr = row_blocks(c->fp64, ax->L, p.ny, p.ncomp);
+    const size_t nbc = col_blocks(c->fp64, ay->L, W, mx, p.ncomp);
+    TRY(red_prepare(c, std::max(nbr, nbc)));
+
+    RowArgs r = row_defaults(p.ny, p.nx, p.dx);
+    r.mode = ROW_FWD;
+    r.rows = p.ny;
+    fill_axis(r, ax);
+    r.in = p.in;
+    r.in_c128 = p.in_c128;
+    r.in_ld = p.nx;
+    r.in_bstride = np_in;
+    r.in_off = offx;
+    r.in_n = p.nx;
+    r.out = S;
+    r.out_ld = mx;
+    r.out_bstride = np_s;
+    r.out_off = 0;
+    r.out_n = ax->n;
+    r.pre_shift = s.shift;
+    r.fxc = s.fxc;
+    r.fyc = s.fyc;
+    r.batch = p.ncomp;
+    if (s.red_pin) {
+        r.red = red_region(c, 0);
+        r.red_pre = 1;
+    }
+    CK(prof_rows(c, c->fp64, r));
+    if (s.red_pin) CK(launch_reduce_finish(r.red, (int)nbr, 1, RS_P, 1, redout_region(c, 0), c->st));
+
+    ColArgs a = col_defaults(c, p.dx);
+    a.mode = COL_FUSED;
+    a.ncols = mx;
+    fill_axis(a, ay);
+    a.W = W;
+    a.src = S;
+    a.src_ld = mx;
+    a.src_bstride = np_s;
+    a.in_off = offy;
+    a.in_n = p.ny;
+    a.dst = S;
+    a.dst_ld = mx;
+    a.dst_bstride = np_s;
+    a.out_off = offy;
+    a.out_n = p.ny;
+    a.h = s.h;
+    a.batch = p.ncomp;
+    if (s.hist || s.red_loss) a.red = red_region(c, 1);
+    if (s.hist) {
+        a.red_hist = 1;
+        a.hist_lx = p.nx;
+        a.hist_ly = p.ny;
+        a.hist_dx = p.dx;
+    }
+    a.red_bpm = s.red_loss;
+    CK(prof_cols(c, c->fp64, a));
+    if (s.hist) CK(launch_reduce_finish(a.red, (int)nbc, 1, RS_HIST, 97, redout_region(c, 1), c->st));
+    if (s.red_loss) CK(launch_reduce_finish(a.red, (int)nbc, 1, RS_SW, 4, redout_region(c, 1), c->st));
+
+    RowArgs q = row_defaults(p.ny, p.nx, p.dx);
+    q.mode = ROW_INV;
+    q.rows = p.ny;
+    fill_axis(q, ax);
+    q.in = S;
+    q.in_c128 = 0;
+    q.in_ld = mx;
+    q.in_bstride = np_s;
+    q.in_off = 0;
+    q.in_n = ax->n;
+    q.out = p.out;
+    q.out_c128 = p.out_c128;
+    q.out_ld = p.nx;
+    q.out_bstride = np_in;
+    q.out_off = offx;
+    q.out_n = p.nx;
+    q.post_shift = s.shift;
+    q.fxc = s.fxc;
+    q.fyc = s.fyc;
+    q.batch = p.ncomp;
+    if (s.red_pout) {
+        q.red = red_region(c, 2);
+        q.red_post = 1;
+    }
+    CK(prof_rows(c, c->fp64, q));
+    if (s.red_pout) CK(launch_reduce_finish(q.red, (int)nbr, 1, RS_P, 2, redout_region(c, 2), c->st));
+    return WOS_OK;
+}
+
+int copy_field(wos_ctx c, const Prop& p) {
+    // z == 0: Propagate returns the field unchanged (optics/propagate.go:66-68)
+    const long long n = (long long)p.ny * p.nx * p.ncomp;
+    if (p.in == p.out && p.in_c128 == p.out_c128) return WOS_OK;
+    if (p.in_c128 == p.out_c128) {
+        CK(cudaMemcpyAsync(p.out, p.in, n * (p.in_c128 ? 16 : c->csz()), cudaMemcpyDeviceToDevice, c->st));
+        return WOS_OK;
+    }
+    if (c->fp64) {
+        CK(cudaMemcpyAsync(p.out, p.in, n * 16, cudaMemcpyDeviceToDevice, c->st));
+        return WOS_OK;
+    }
+    CK(launch_convert(p.out_c128, p.in, p.out, n, c->st));
+    return WOS_OK;
+}
+
+int run_propagate(wos_ctx c, const Prop& p0) {
+    Prop p = p0;
+    wos_diag* d = p.diag;
+    if (d) {
+        std::memset(d, 0, sizeof(*d));
+        d->dx_out = p.dx;
+    }
+    if (p.ny < 2 || p.nx < 2 || p.ncomp < 1 || p.ncomp > 2 || !(p.dx > 0))
+        return fail(WOS_INVALID_ARG, "invalid field geometry");
+    if (!p.in || !p.out) return fail(WOS_INVALID_ARG, "null field pointer");
+    if (p.z == 0) return copy_field(c, p);
+    if (!(p.c.wavelength > 0) && p.method != WOS_FRESNEL_IR)
+        return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    const bool diag = d != nullptr;
+    const Policy pol = ev_policy(p.c, p.z);
+    const double z = p.z;
+    const double dx = p.dx;
+    switch (p.method) {
+    case WOS_ASM:
+    case WOS_ASM_SHIFT:
+    case WOS_ASM_PAD:
+    case WOS_ASM_SHIFT_PAD: {
+        const bool shift_m = (p.method == WOS_ASM_SHIFT || p.method == WOS_ASM_SHIFT_PAD);
+        const bool pad_m = (p.method == WOS_ASM_PAD || p.method == WOS_ASM_SHIFT_PAD);
+        const bool wrap = wrap_needed(p.c, p.ny, p.nx, dx, z);
+        Sweep3 s;
+        s.pad = pad_m;
+        if (shift_m) {
+            // spectralCentroid (optics/propagate.go:391-416) over all components
+            const long long np = (long long)p.ny * p.nx;
+            TRY(ensure(c->scratch2, (size_t)np * p.ncomp * c->csz()));
+            const bool hist_here = wrap && p.method == WOS_ASM_SHIFT;
+            TRY(spectrum_stats(c, p, c->scratch2.p, true, hist_here, 0, 0, 0, 3, nullptr));
+            TRY(fetch_red(c, 4));
+            const double* rr = c->hred + RS_COUNT * 3;
+            double fxc = 0, fyc = 0;
+            if (rr[RS_SW] > 0) {
+                fxc = rr[RS_SFX] / rr[RS_SW];
+                fyc = rr[RS_SFY] / rr[RS_SW];
+            }
+            if (d) {
+                d->centroid_fx = fxc;
+                d->centroid_fy = fyc;
+            }
+            const double fbx = 1 / ((double)p.nx * dx), fby = 1 / ((double)p.ny * dx);
+            if (!(std::fabs(fxc) < 0.5 * fbx && std::fabs(fyc) < 0.5 * fby)) {
+                s.shift = 1;
+                s.fxc = fxc;
+                s.fyc = fyc;
+                if (d) d->carrier_applied = 1;
+                if (wrap) {
+                    if (p.method == WOS_ASM_SHIFT) {
+                        std::vector<double> h(c->hred + RS_COUNT * 3 + RS_HIST, c->hred + RS_COUNT * 3 + RS_HIST + 97);
+                        wrap_finish(d, p.c, p.ny, p.nx, dx, z, h.data());
+                    } else {
+                        // propASMPadCore checks the carrier-free field
+                        TRY(spectrum_stats(c, p, c->scratch2.p, false, true, 1, fxc, fyc, 3, nullptr));
+                        TRY(fetch_red(c, 4));
+                        std::vector<double> h(c->hred + RS_COUNT * 3 + RS_HIST, c->hred + RS_COUNT * 3 + RS_HIST + 97);
+                        wrap_finish(d, p.c, p.ny, p.nx, dx, z, h.data());
+                    }
+                }
+            }
+        }
+        const int mx = pad_m ? 2 * p.nx : p.nx, my = pad_m ? 2 * p.ny : p.ny;
+        s.h = asm_h(c, p.c, z, pol, dx, mx, my);
+        s.h.fxoff = s.fxc;
+        s.h.fyoff = s.fyc;
+        s.red_pin = diag;
+        s.red_pout = diag;
+        s.red_loss = diag;
+        // wrap check when no carrier branch ran: the plain field's spectrum
+        if (wrap && !s.shift) {
+            if (!pad_m) {
+                s.hist = true;
+            } else {
+                TRY(ensure(c->scratch2, (size_t)p.ny * p.nx * p.ncomp * c->csz()));
+                TRY(spectrum_stats(c, p, c->scratch2.p, false, true, 0, 0, 0, 3, nullptr));
+                TRY(fetch_red(c, 4));
+                std::vector<double> h(c->hred + RS_COUNT * 3 + RS_HIST, c->hred + RS_COUNT * 3 + RS_HIST + 97);
+                wrap_finish(d, p.c, p.ny, p.nx, dx, z, h.data());
+            }
+        }
+        TRY(run_sweep3(c, p, s));
+        if (diag) {
+            TRY(fetch_red(c, 3));
+            const double pin = c->hred[RS_P] * dx * dx;
+            d->p_in = pin;
+            d->p_out = c->hred[2 * RS_COUNT + RS_P] * dx * dx;
+            if (s.hist) wrap_finish(d, p.c, p.ny, p.nx, dx, z, c->hred + RS_COUNT + RS_HIST);
+            // loss fraction of the step, from sums of positive terms only:
+            // spectral sum |F|^2 (1 - |H|^2) / sum |F|^2, plus the energy the
+            // zero-padded methods crop away in the column (mx * Dy) and row (Dx) passes
+            const double p0 = c->hred[RS_COUNT + RS_SW], l1 = c->hred[RS_COUNT + RS_SW + 1];
+            const double dy = s.fast ? 0.0 : c->hred[RS_COUNT + RS_SW + 3];
+            const double dxr = s.fast ? 0.0 : c->hred[2 * RS_COUNT + RS_P + 1];
+            const double pin_sp = c->hred[RS_P];
+            const int mx = pad_m ? 2 * p.nx : p.nx;
+            double frac = p0 > 0 ? l1 / p0 : 0.0;
+            if (pin_sp > 0) frac += ((double)mx * dy + dxr) / pin_sp;
+            asm_warn(d, z, pin, pin - pin * frac, pol);
+        }
+        return WOS_OK;
+    }
+    case WOS_FRESNEL_TF: {
+        // propFresnelTF (optics/propagate.go:507-519)
+        Sweep3 s;
+        s.h = asm_h(c, p.c, z, pol, dx, p.nx, p.ny);
+        s.h.kind = H_FRESNEL_TF;
+        const double kz = (2 * M_PI / p.c.wavelength) * z;
+        s.h.c_re = std::cos(kz);
+        s.h.c_im = std::sin(kz);
+        s.red_pin = diag;
+        s.red_pout = diag;
+        TRY(run_sweep3(c, p, s));
+        if (diag) {
+            TRY(fetch_red(c, 3));
+            d->p_in = c->hred[RS_P] * dx * dx;
+            d->p_out = c->hred[2 * RS_COUNT + RS_P] * dx * dx;
+        }
+        const int n = std::min(p.nx, p.ny);
+        if (std::fabs(z) > (double)n * dx * dx / p.c.wavelength) warn_add(d, WOS_W_FRESNEL_TF_ALIAS, 0);
+        return WOS_OK;
+    }
+    case WOS_FRESNEL_IR: {
+        // propFresnelIR (optics/propagate.go:533-590): FFT2D of the 2N chirp
+        // kernel is separable, FFT(hx) (x) FFT(hy), built in FP64 per axis.
+        const double wl = p.c.wavelength;
+        if (!(wl > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+        const int mx = 2 * p.nx, my = 2 * p.ny;
+        Axis *ax64, *ay64;
+        TRY(get_axis(c, mx, 1, &ax64));
+        TRY(get_axis(c, my, 1, &ay64));
+        TRY(ensure(c->tmp, sizeof(double2) * (size_t)(mx + my) + c->csz() * (size_t)(mx + my)));
+        double2* hx = reinterpret_cast<double2*>(c->tmp.p);
+        double2* hy = hx + mx;
+        void* tx = hy + my;
+        void* ty = reinterpret_cast<char*>(tx) + c->csz() * mx;
+        CK(launch_fresnel_ir_axis(hx, mx, dx, wl, z, c->st));
+        CK(launch_fresnel_ir_axis(hy, my, dx, wl, z, c->st));
+        for (int ax = 0; ax < 2; ax++) {
+            Axis* A = ax ? ay64 : ax64;
+            RowArgs r = row_defaults(1, A->n, dx);
+            r.mode = ROW_FWD;
+            r.rows = 1;
+            fill_axis(r, A);
+            r.in = ax ? hy : hx;
+            r.in_ld = A->n;
+            r.in_n = A->n;
+            r.out = ax ? hy : hx;
+            r.out_ld = A->n;
+            r.out_n = A->n;
+            CK(prof_rows(c, 1, r));
+        }
+        CK(launch_scale_copy(c->fp64, hx, tx, mx, 1.0, 0.0, c->st));
+        CK(launch_scale_copy(c->fp64, hy, ty, my, 1.0, 0.0, c->st));
+        Sweep3 s;
+        s.pad = 1;
+        s.h = asm_h(c, p.c, z, pol, dx, mx, my);
+        s.h.kind = H_TABLE_XY;
+        s.h.tx = tx;
+        s.h.ty = ty;
+        // pre = complex(0, -1/(wl z)) * cexpI(k z) * complex(dx^2, 0)
+        const double k = 2 * M_PI / wl;
+        const double a0 = -1 / (wl * z);
+        const double cr = std::cos(k * z), ci = std::sin(k * z);
+        const double pr = -a0 * ci, pi_ = a0 * cr;  // (0 + i a0)(cr + i ci)
+        s.h.c_re = pr * (dx * dx);
+        s.h.c_im = pi_ * (dx * dx);
+        s.red_pin = diag;
+        s.red_pout = diag;
+        TRY(run_sweep3(c, p, s));
+        if (diag) {
+            TRY(fetch_red(c, 3));
+            d->p_in = c->hred[RS_P] * dx * dx;
+            d->p_out = c->hred[2 * RS_COUNT + RS_P] * dx * dx;
+        }
+        const int n = std::max(p.nx, p.ny);
+        if (std::fabs(z) < (double)n * dx * dx / wl) warn_add(d, WOS_W_FRESNEL_IR_ALIAS, 0);
+        return WOS_OK;
+    }
+    case WOS_FRAUNHOFER: {
+        // propFraunhofer (optics/propagate.go:603-662), square grids
+        if (p.nx != p.ny) return fail(WOS_UNSUPPORTED_SIZE, "fraunhofer needs a square grid (nx == ny)");
+        const int n = p.nx;
+        const double wl = p.c.wavelength;
+        const double k = 2 * M_PI / wl;
+        const double dxout = wl * std::fabs(z) / ((double)n * dx);
+        Axis* A;
+        TRY(get_axis(c, n, c->fp64, &A));
+        const long long np = (long long)n * n;
+        TRY(ensure(c->scratch, (size_t)np * p.ncomp * c->csz()));
+        void* S = c->scratch.p;
+        void* O = p.out;
+        if (p.out_c128 && !c->fp64) {
+            TRY(ensure(c->scratch3, (size_t)np * p.ncomp * c->csz()));
+            O = c->scratch3.p;
+        }
+        const size_t nbr = row_blocks(c->fp64, A->L, n, p.ncomp);
+        TRY(red_prepare(c, nbr));
+        RowArgs r = row_defaults(n, n, dx);
+        r.mode = ROW_FWD;
+        r.rows = n;
+        fill_axis(r, A);
+        r.in = p.in;
+        r.in_c128 = p.in_c128;
+        r.in_ld = n;
+        r.in_bstride = np;
+        r.in_n = n;
+        r.out = S;
+        r.out_ld = n;
+        r.out_bstride = np;
+        r.out_n = n;
+        r.batch = p.ncomp;
+        if (diag) {
+            r.red = red_region(c, 0);
+            r.red_pre = 1;
+            r.red_moments = 1;
+        }
+        CK(prof_rows(c, c->fp64, r));
+        if (diag) CK(launch_reduce_finish(r.red, (int)nbr, 1, RS_P, 4, redout_region(c, 0), c->st));
+        ColArgs a = col_defaults(c, dx);
+        a.mode = COL_FRAUNHOFER;
+        a.ncols = n;
+        fill_axis(a, A);
+        a.W = auto_colw(c, A->L);
+        a.src = S;
+        a.src_ld = n;
+        a.src_bstride = np;
+        a.in_n = n;
+        a.dst = O;
+        a.dst_ld = n;
+        a.dst_bstride = np;
+        a.h.k = k;
+        a.h.z = z;
+        a.h.wl = wl;
+        // cexpI(k z) * complex(0, -1/(wl z)), times the dx^2 of the transform
+        const double cr = std::cos(k * z), ci = std::sin(k * z);
+        const double a0 = -1 / (wl * z);
+        a.fr_c_re = (-a0 * ci) * (dx * dx);
+        a.fr_c_im = (a0 * cr) * (dx * dx);
+        a.fr_dxout = dxout;
+        a.fr_n = n;
+        a.batch = p.ncomp;
+        CK(prof_cols(c, c->fp64, a));
+        if (O != p.out) CK(launch_convert(1, O, p.out, np * p.ncomp, c->st));
+        if (d) {
+            d->dx_out = dxout;
+            TRY(fetch_red(c, 1));
+            const double* m = c->hred;
+            const double pw = m[RS_P];
+            double din = 0;
+            if (pw > 0) {
+                const double cx = m[RS_PX] / pw, cy = m[RS_PY] / pw;
+                double vr = m[RS_PR2] - pw * (cx * cx + cy * cy);
+                if (vr < 0) vr = 0;
+                din = 2 * std::sqrt(vr / pw);
+            }
+            d->rms_radius_in = din;
+            d->p_in = pw * dx * dx;
+            if (din > 0) {
+                const double nf = din * din / (wl * std::fabs(z));
+                if (nf > 0.5) warn_add(d, WOS_W_FRAUNHOFER_NEARFIELD, nf);
+            }
+        }
+        return WOS_OK;
+    }
+    default:
+        return fail(WOS_UNKNOWN_METHOD, "unknown propagation method " + std::to_string(p.method));
+    }
+}
+
+// Host field staging: [ncomp][ny][nx] complex128 in c->stage.
+int stage_in(wos_ctx c, const wos_field* f, int ncomp) {
+    const size_t np = (size_t)f->ny * f->nx;
+    TRY(ensure(c->stage, np * ncomp * 16));
+    CK(cudaMemcpyAsync(c->stage.p, f->ex, np * 16, cudaMemcpyHostToDevice, c->st));
+    if (ncomp == 2)
+        CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->stage.p) + np * 16, f->ey, np * 16, cudaMemcpyHostToDevice, c->st));
+    return WOS_OK;
+}
+int stage_out(wos_ctx c, wos_field* f, int ncomp) {
+    const size_t np = (size_t)f->ny * f->nx;
+    CK(cudaMemcpyAsync(f->ex, c->stage.p, np * 16, cudaMemcpyDeviceToHost, c->st));
+    if (ncomp == 2)
+        CK(cudaMemcpyAsync(f->ey, reinterpret_cast<char*>(c->stage.p) + np * 16, np * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+int check_field(const wos_field* f) {
+    if (!f || !f->ex || f->ny < 2 || f->nx < 2 || !(f->dx > 0) || (f->polarized && !f->ey))
+        return fail(WOS_INVALID_ARG, "invalid wos_field");
+    return WOS_OK;
+}
+
+wos_context default_context() {
+    // nil *Context -> &Context{Evanescent: "decay"} (optics/propagate.go:72-74)
+    wos_context c{};
+    return c;
+}
+
+// fft2DCPU semantics (optics/fft.go:219-242): rows then columns, inverse
+// scaled by 1/n per axis; `a` holds `batch` arrays in precision fp64.
+int fft2d_impl(wos_ctx c, int fp64, int ny, int nx, int batch, void* a, int inverse) {
+    Axis *ax, *ay;
+    TRY(get_axis(c, nx, fp64, &ax));
+    TRY(get_axis(c, ny, fp64, &ay));
+    const long long np = (long long)ny * nx;
+    RowArgs r = row_defaults(ny, nx, 1.0);
+    r.mode = inverse ? ROW_INV : ROW_FWD;
+    r.rows = ny;
+    fill_axis(r, ax);
+    r.in = a;
+    r.in_ld = nx;
+    r.in_bstride = np;
+    r.in_n = nx;
+    r.out = a;
+    r.out_ld = nx;
+    r.out_bstride = np;
+    r.out_n = nx;
+    r.out_scale = inverse ? 1.0 / (double)nx : 1.0;
+    r.batch = batch;
+    CK(prof_rows(c, fp64, r));
+    ColArgs k = col_defaults(c, 1.0);
+    k.h.exact = fp64;
+    k.mode = COL_FFT;
+    k.col_inverse = inverse;
+    k.ncols = nx;
+    fill_axis(k, ay);
+    k.W = auto_colw_p(c, fp64, ay->L);
+    k.src = a;
+    k.src_ld = nx;
+    k.src_bstride = np;
+    k.in_n = ny;
+    k.dst = a;
+    k.dst_ld = nx;
+    k.dst_bstride = np;
+    k.out_n = ny;
+    k.out_scale = inverse ? 1.0 / (double)ny : 1.0;
+    k.batch = batch;
+    CK(prof_cols(c, fp64, k));
+    return WOS_OK;
+}
+
+}  // namespace
+
+// ====================================================================== ABI
+extern "C" {
+
+const char* wos_status_string(int s) {
+    switch (s) {
+    case WOS_OK: return "ok";
+    case WOS_INVALID_ARG: return "invalid argument";
+    case WOS_UNSUPPORTED_SIZE: return "unsupported size";
+    case WOS_OOM: return "out of device memory";
+    case WOS_CUDA_ERROR: return "CUDA error";
+    case WOS_TIMEOUT: return "timeout";
+    case WOS_NOT_INITIALISED: return "not initialised";
+    case WOS_UNKNOWN_METHOD: return "unknown method";
+    }
+    return "unknown status";
+}
+
+const char* wos_last_error(void) { return g_err.c_str(); }
+
+const char* wos_backend_info(void) { return "B200 native (sm_100a): hand-written Stockham/Bluestein FFT, fused ASM sweeps"; }
+
+int wos_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+int wos_device_name(int device, char* buf, int buflen) {
+    if (!buf || buflen <= 0) return fail(WOS_INVALID_ARG, "null buffer");
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device));
+    std::snprintf(buf, (size_t)buflen, "%s", prop.name);
+    return WOS_OK;
+}
+
+int wos_ctx_create(int device, int precision, wos_ctx* out) {
+    if (!out) return fail(WOS_INVALID_ARG, "null out");
+    *out = nullptr;
+    if (precision != WOS_FP32 && precision != WOS_FP64) return fail(WOS_INVALID_ARG, "precision");
+    int n = wos_device_count();
+    if (n <= 0) return fail(WOS_NOT_INITIALISED, "no CUDA device");
+    if (device < 0 || device >= n) return fail(WOS_INVALID_ARG, "device index");
+    wos_ctx c = new wos_ctx_s();
+    c->device = device;
+    c->fp64 = precision == WOS_FP64;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(WOS_CUDA_ERROR, std::string("context creation: ") + cudaGetErrorString(e));
+    }
+    c->own_stream = true;
+    *out = c;
+    return WOS_OK;
+}
+
+int wos_ctx_destroy(wos_ctx c) {
+    if (!c) return WOS_OK;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        cudaSetDevice(c->device);
+        cudaStreamSynchronize(c->st);
+        for (int pr = 0; pr < 2; pr++)
+            for (auto& kv : c->axes[pr]) {
+                cudaFree(kv.second.tw);
+                if (kv.second.chirp) cudaFree(kv.second.chirp);
+                if (kv.second.bf) cudaFree(kv.second.bf);
+                if (kv.second.bi) cudaFree(kv.second.bi);
+            }
+        DevBuf* bufs[] = {&c->stage, &c->scratch, &c->scratch2, &c->scratch3, &c->red, &c->redout, &c->tmp,
+                          &c->maps, &c->params, &c->vol, &c->accum, &c->aux};
+        for (DevBuf* b : bufs)
+            if (b->p) cudaFree(b->p);
+        if (c->hred) cudaFreeHost(c->hred);
+        if (c->prof_made)
+            for (int i = 0; i < wos_ctx_s::kRing; i++) {
+                cudaEventDestroy(c->ev0[i]);
+                cudaEventDestroy(c->ev1[i]);
+            }
+        if (c->own_stream) cudaStreamDestroy(c->st);
+    }
+    delete c;
+    return WOS_OK;
+}
+
+int wos_ctx_set_stream(wos_ctx c, void* stream) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (c->own_stream) {
+        cudaStreamSynchronize(c->st);
+        cudaStreamDestroy(c->st);
+        c->own_stream = false;
+    }
+    c->st = reinterpret_cast<cudaStream_t>(stream);
+    return WOS_OK;
+}
+
+void* wos_ctx_get_stream(wos_ctx c) { return c ? reinterpret_cast<void*>(c->st) : nullptr; }
+
+int wos_ctx_precision(wos_ctx c) { return c ? (c->fp64 ? WOS_FP64 : WOS_FP32) : -1; }
+
+int wos_ctx_set_col_width(wos_ctx c, int w) {
+    if (!c || w < 0 || (w > 0 && (w & (w - 1)))) return fail(WOS_INVALID_ARG, "column width must be 0 or a power of two");
+    c->colw = w;
+    return WOS_OK;
+}
+
+int wos_ctx_set_profiling(wos_ctx c, int on) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (on && !c->prof_made) {
+        CK(cudaSetDevice(c->device));
+        for (int i = 0; i < wos_ctx_s::kRing; i++) {
+            CK(cudaEventCreate(&c->ev0[i]));
+            CK(cudaEventCreate(&c->ev1[i]));
+            c->ev_used[i] = false;
+        }
+        c->prof_made = true;
+    }
+    c->prof_on = on != 0;
+    return WOS_OK;
+}
+
+int wos_ctx_profile(wos_ctx c, int kind, double* total_ms, long long* launches) {
+    if (!c || kind < 0 || kind > 7) return fail(WOS_INVALID_ARG, "profile kind");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (c->prof_made)
+        for (int i = 0; i < wos_ctx_s::kRing; i++) prof_fold(c, i);
+    if (total_ms) *total_ms = c->prof_ms[kind];
+    if (launches) *launches = c->prof_n[kind];
+    return WOS_OK;
+}
+
+int wos_ctx_profile_reset(wos_ctx c) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (c->prof_made)
+        for (int i = 0; i < wos_ctx_s::kRing; i++) prof_fold(c, i);
+    for (int k = 0; k < 8; k++) {
+        c->prof_ms[k] = 0;
+        c->prof_n[k] = 0;
+    }
+    c->launches = 0;
+    return WOS_OK;
+}
+
+long long wos_ctx_launch_count(wos_ctx c) { return c ? c->launches : -1; }
+
+int wos_ctx_synchronize(wos_ctx c) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+// ---- FFTs for the remaining fft2D / fft1DAny users
+int wos_fft2d_dev(wos_ctx c, int ny, int nx, int batch, void* a, int inverse) {
+    if (!c || !a || ny < 2 || nx < 2 || batch < 1) return fail(WOS_INVALID_ARG, "fft2d_dev arguments");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    return fft2d_impl(c, c->fp64, ny, nx, batch, a, inverse);
+}
+
+int wos_fft2d(wos_ctx c, int ny, int nx, wos_c128* a, int inverse) {
+    if (!c || !a || ny < 2 || nx < 2) return fail(WOS_INVALID_ARG, "fft2d arguments");
+    const size_t np = (size_t)ny * nx;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        TRY(set_device(c));
+        TRY(ensure(c->stage, np * 16));
+        if (!c->fp64) TRY(ensure(c->scratch, np * 8));
+        CK(cudaMemcpyAsync(c->stage.p, a, np * 16, cudaMemcpyHostToDevice, c->st));
+        if (!c->fp64) CK(launch_convert(0, c->stage.p, c->scratch.p, (long long)np, c->st));
+    }
+    void* buf = c->fp64 ? c->stage.p : c->scratch.p;
+    TRY(wos_fft2d_dev(c, ny, nx, 1, buf, inverse));
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (!c->fp64) CK(launch_convert(1, c->scratch.p, c->stage.p, (long long)np, c->st));
+    CK(cudaMemcpyAsync(a, c->stage.p, np * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+int wos_fft1d(wos_ctx c, int n, wos_c128* a, int inverse) {
+    if (!c || !a || n < 2) return fail(WOS_INVALID_ARG, "fft1d arguments");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    Axis* ax;
+    TRY(get_axis(c, n, c->fp64, &ax));
+    TRY(ensure(c->stage, (size_t)n * 16));
+    CK(cudaMemcpyAsync(c->stage.p, a, (size_t)n * 16, cudaMemcpyHostToDevice, c->st));
+    RowArgs r = row_defaults(1, n, 1.0);
+    r.mode = inverse ? ROW_INV : ROW_FWD;
+    r.rows = 1;
+    fill_axis(r, ax);
+    r.in = c->stage.p;
+    r.in_c128 = 1;
+    r.in_ld = n;
+    r.in_n = n;
+    r.out = c->stage.p;
+    r.out_c128 = 1;
+    r.out_ld = n;
+    r.out_n = n;
+    r.out_scale = inverse ? 1.0 / (double)n : 1.0;
+    CK(prof_rows(c, c->fp64, r));
+    CK(cudaMemcpyAsync(a, c->stage.p, (size_t)n * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+// ---- Propagate
+int wos_propagate_dev(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* in, void* out, double z,
+                      int method, const wos_context* cc, wos_diag* diag) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    Prop p{ny, nx, dx, ncomp, in, 0, out, 0, z, method, cc ? *cc : default_context(), diag};
+    return run_propagate(c, p);
+}
+
+int wos_propagate_dev_c128(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* in, void* out, double z,
+                           int method, const wos_context* cc, wos_diag* diag) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    Prop p{ny, nx, dx, ncomp, in, 1, out, 1, z, method, cc ? *cc : default_context(), diag};
+    return run_propagate(c, p);
+}
+
+int wos_propagate(wos_ctx c, wos_field* f, double z, int method, const wos_context* cc, wos_diag* diag) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    TRY(check_field(f));
+    if (method < WOS_ASM || method > WOS_FRAUNHOFER) return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
+    if (z == 0) {
+        if (diag) {
+            std::memset(diag, 0, sizeof(*diag));
+            diag->dx_out = f->dx;
+        }
+        return WOS_OK;
+    }
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const int ncomp = f->polarized ? 2 : 1;
+    TRY(stage_in(c, f, ncomp));
+    Prop p{f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, c->stage.p, 1, z, method, cc ? *cc : default_context(), diag};
+    wos_diag local;
+    if (!p.diag && method == WOS_FRAUNHOFER) p.diag = &local;  // the new pitch is needed below
+    TRY(run_propagate(c, p));
+    TRY(stage_out(c, f, ncomp));
+    if (method == WOS_FRAUNHOFER) f->dx = p.diag->dx_out;
+    return WOS_OK;
+}
+
+}  // extern "C"
+
+// ================================================= split-step, batches, elements
+namespace {
+
+void diag_merge(wos_diag* into, const wos_diag& d) {
+    if (!into) return;
+    for (int b = 0; b < WOS_W_COUNT; b++) {
+        into->warn_count[b] += d.warn_count[b];
+        if (d.warn_count[b] && d.warn_value[b] != 0) into->warn_value[b] = d.warn_value[b];
+    }
+}
+
+struct ScreenSrc {
+    int kind = 1;  // 1 parametric, 2 maps
+    wos_index_desc desc{};
+    const double* nre = nullptr;
+    const double* nim = nullptr;
+    int nmaps = 1;
+};
+
+void fill_screen(ScreenArgs& s, const ScreenSrc& src, int slice, long long np, double k, double dz, double zc) {
+    s = ScreenArgs{};
+    s.kind = src.kind;
+    s.k = k;
+    s.dz = dz;
+    s.zc = zc;
+    if (src.kind == 1) {
+        const wos_index_desc& d = src.desc;
+        s.re_bg = d.re_bg;
+        s.im_bg = d.im_bg;
+        s.core_dn = d.core_dn;
+        s.core_x0 = d.core_x0;
+        s.core_y0 = d.core_y0;
+        s.core_w = d.core_w;
+        s.zmod_amp = d.zmod_amp;
+        s.zmod_period = d.zmod_period;
+        s.zmod_phase = d.zmod_phase;
+        s.border_px = d.border_px;
+        s.border_order = d.border_order;
+        s.border_strength = d.border_strength;
+        s.n_layers = d.n_layers < 0 ? 0 : (d.n_layers > 8 ? 8 : d.n_layers);
+        for (int i = 0; i < 8; i++) {
+            s.layer_z[i] = d.layer_z[i];
+            s.layer_re[i] = d.layer_re[i];
+            s.layer_im[i] = d.layer_im[i];
+        }
+    } else {
+        const int m = src.nmaps == 1 ? 0 : slice;
+        s.nre = src.nre + (long long)m * np;
+        s.nim = src.nim + (long long)m * np;
+    }
+}
+
+// PropagateSplitStep (optics/medium.go:22-45) with merged half steps:
+//   rows fwd | cols H(dz/2) | rows inv.M0.fwd | cols H(dz/2)^2 | ... | rows inv.M(S-1).fwd
+//   | cols H(dz/2) | rows inv
+// The power around every ASM half step (for the evanescent_filtered /
+// backward_* warnings of each Propagate(dz/2) call) comes from Parseval sums in
+// the column pass, one finished record per pass.
+int run_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* in, int in_c128, void* out,
+                  int out_c128, double z, const ScreenSrc& src, int steps, const wos_context& cc, wos_diag* d) {
+    if (d) {
+        std::memset(d, 0, sizeof(*d));
+        d->dx_out = dx;
+    }
+    if (ny < 2 || nx < 2 || ncomp < 1 || ncomp > 2 || !(dx > 0) || !in || !out)
+        return fail(WOS_INVALID_ARG, "invalid field geometry");
+    if (z == 0) {
+        Prop p{ny, nx, dx, ncomp, in, in_c128, out, out_c128, 0.0, WOS_ASM, cc, nullptr};
+        return copy_field(c, p);
+    }
+    if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    if (steps <= 0) steps = 1;
+    const double dz = z / (double)steps;
+    const double k = 2 * M_PI / cc.wavelength;
+    const double hz = dz / 2;
+    const Policy pol = ev_policy(cc, hz);
+    Axis *ax, *ay;
+    TRY(get_axis(c, nx, c->fp64, &ax));
+    TRY(get_axis(c, ny, c->fp64, &ay));
+    const long long np = (long long)ny * nx;
+    void* S;
+    if (!out_c128) {
+        S = out;
+    } else {
+        TRY(ensure(c->scratch, (size_t)np * ncomp * c->csz()));
+        S = c->scratch.p;
+    }
+    const int W = auto_colw(c, ay->L);
+    const size_t nbr = row_blocks(c->fp64, ax->L, ny, ncomp);
+    const size_t nbc = col_blocks(c->fp64, ay->L, W, nx, ncomp);
+    TRY(red_prepare(c, std::max(nbr, nbc)));
+    const bool diag = d != nullptr;
+    const bool wrap = wrap_needed(cc, ny, nx, dx, hz);
+    const int npass = steps + 1;
+    if (diag) TRY(ensure(c->tmp, sizeof(double) * RS_COUNT * (size_t)npass));
+    double* passes = reinterpret_cast<double*>(c->tmp.p);
+
+    RowArgs r = row_defaults(ny, nx, dx);
+    r.mode = ROW_FWD;
+    r.rows = ny;
+    fill_axis(r, ax);
+    r.in = in;
+    r.in_c128 = in_c128;
+    r.in_ld = nx;
+    r.in_bstride = np;
+    r.in_n = nx;
+    r.out = S;
+    r.out_ld = nx;
+    r.out_bstride = np;
+    r.out_n = nx;
+    r.batch = ncomp;
+    if (diag) {
+        r.red = red_region(c, 0);
+        r.red_pre = 1;
+    }
+    CK(prof_rows(c, c->fp64, r));
+    if (diag) CK(launch_reduce_finish(r.red, (int)nbr, 1, RS_P, 1, redout_region(c, 0), c->st));
+
+    for (int s = 0; s <= steps; s++) {
+        ColArgs a = col_defaults(c, dx);
+        a.mode = COL_FUSED;
+        a.ncols = nx;
+        fill_axis(a, ay);
+        a.W = W;
+        a.src = S;
+        a.src_ld = nx;
+        a.src_bstride = np;
+        a.in_n = ny;
+        a.dst = S;
+        a.dst_ld = nx;
+        a.dst_bstride = np;
+        a.out_n = ny;
+        a.h = asm_h(c, cc, hz, pol, dx, nx, ny);
+        a.h.kind = (s == 0 || s == steps) ? H_ASM : H_ASM_HALF2;
+        a.batch = ncomp;
+        if (diag) {
+            a.red = red_region(c, 1);
+            a.red_bpm = 1;
+            if (wrap) {
+                a.red_hist = 1;
+                a.hist_lx = nx;
+                a.hist_ly = ny;
+                a.hist_dx = dx;
+            }
+        }
+        CK(prof_cols(c, c->fp64, a));
+        if (diag) {
+            CK(launch_reduce_finish(a.red, (int)nbc, 1, RS_SW, 3, passes + (size_t)s * RS_COUNT, c->st));
+            if (wrap) CK(launch_reduce_finish(a.red, (int)nbc, 1, RS_HIST, 97, passes + (size_t)s * RS_COUNT, c->st));
+        }
+        if (s < steps) {
+            RowArgs q = row_defaults(ny, nx, dx);
+            q.mode = ROW_INV_FWD;
+            q.rows = ny;
+            fill_axis(q, ax);
+            q.in = S;
+            q.in_ld = nx;
+            q.in_bstride = np;
+            q.in_n = nx;
+            q.out = S;
+            q.out_ld = nx;
+            q.out_bstride = np;
+            q.out_n = nx;
+            q.batch = ncomp;
+            const double zc = z * (double)s / (double)steps + dz / 2;
+            fill_screen(q.scr, src, s, np, k, dz, zc);
+            CK(prof_rows(c, c->fp64, q));
+        }
+    }
+    RowArgs q = row_defaults(ny, nx, dx);
+    q.mode = ROW_INV;
+    q.rows = ny;
+    fill_axis(q, ax);
+    q.in = S;
+    q.in_ld = nx;
+    q.in_bstride = np;
+    q.in_n = nx;
+    q.out = out;
+    q.out_c128 = out_c128;
+    q.out_ld = nx;
+    q.out_bstride = np;
+    q.out_n = nx;
+    q.batch = ncomp;
+    if (diag) {
+        q.red = red_region(c, 2);
+        q.red_post = 1;
+    }
+    CK(prof_rows(c, c->fp64, q));
+    if (diag) {
+        CK(launch_reduce_finish(q.red, (int)nbr, 1, RS_P, 1, redout_region(c, 2), c->st));
+        TRY(fetch_red(c, 3));
+        d->p_in = c->hred[RS_P] * dx * dx;
+        d->p_out = c->hred[2 * RS_COUNT + RS_P] * dx * dx;
+        std::vector<double> h((size_t)npass * RS_COUNT);
+        CK(cudaMemcpy(h.data(), passes, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
+        for (int s = 0; s <= steps; s++) {
+            const double* rr = h.data() + (size_t)s * RS_COUNT;
+            const double p0 = rr[RS_SW], l1 = rr[RS_SW + 1], l2 = rr[RS_SW + 2];
+            // half step(s) of this pass: P0 -> P0-L1 and, for merged passes, P0-L1 -> P0-L1-L2
+            const int nh = (s == 0 || s == steps) ? 1 : 2;
+            for (int hh = 0; hh < nh; hh++) {
+                if (wrap) wrap_finish(d, cc, ny, nx, dx, hz, rr + RS_HIST);
+                if (hh == 0) asm_warn(d, hz, p0, p0 - l1, pol);
+                else asm_warn(d, hz, p0 - l1, (p0 - l1) - l2, pol);
+            }
+        }
+    }
+    return WOS_OK;
+}
+
+// FFT2D of a complex128 device array in FP64, whatever the context precision
+// (one-time source synthesis).
+int fft2d_fp64(wos_ctx c, int n, int batch, double2* a, int inverse) {
+    return fft2d_impl(c, 1, n, n, batch, a, inverse);
+}
+
+// GenerateSchellRealizations (optics/coherence.go:22-80) into modes (device, complex128)
+int schell_generate(wos_ctx c, int n, double dx, double width, double coh, int m, const wos_c128* noise,
+                    double2* modes) {
+    const long long nn = (long long)n * n;
+    TRY(ensure(c->aux, (size_t)nn * (16 + 8)));
+    double2* mu = reinterpret_cast<double2*>(c->aux.p);
+    double* sqs = reinterpret_cast<double*>(mu + nn);
+    CK(launch_schell_mu(mu, n, dx, coh, c->st));
+    TRY(fft2d_fp64(c, n, 1, mu, 0));
+    CK(launch_sqrt_re(sqs, mu, nn, c->st));
+    CK(cudaMemcpyAsync(modes, noise, (size_t)nn * m * 16, cudaMemcpyHostToDevice, c->st));
+    CK(launch_mul_map(modes, sqs, nn, m, c->st));
+    TRY(fft2d_fp64(c, n, m, modes, 1));
+    CK(launch_schell_env(modes, n, dx, width, m, c->st));
+    return WOS_OK;
+}
+
+// Batched ASM over units that share a geometry (polychromatic wavelengths,
+// volume distances, coherent modes): one row sweep per unit set, one column
+// launch per chunk with gridDim.y = units, then either a batched inverse row
+// sweep (planes out) or an accumulating one (intensity out).
+struct Batch {
+    int ny, nx, ncomp;
+    double dx;
+    const void* in;       // complex128 device input [ncomp or units][ny][nx]
+    long long in_unit_stride;  // elements between units of the input (0: shared input)
+    int units;
+    const double* wl_dev;  // per-unit wavelength (device) or null
+    const double* z_dev;   // per-unit z (device) or null
+    std::vector<double> wl, z;  // host copies
+    const double* w_dev;   // per-unit intensity weight (device) or null
+    double* out_int;       // device [ny][nx] FP64 intensity accumulation, or null
+    void* out_planes;      // device complex128 [units][ncomp][ny][nx], or null
+    wos_context cc;
+    wos_diag* diag;
+};
+
+int run_batch_asm(wos_ctx c, Batch& b) {
+    const int ny = b.ny, nx = b.nx, ncomp = b.ncomp;
+    const double dx = b.dx;
+    const long long np = (long long)ny * nx;
+    Axis *ax, *ay;
+    TRY(get_axis(c, nx, c->fp64, &ax));
+    TRY(get_axis(c, ny, c->fp64, &ay));
+    const int W = auto_colw(c, ay->L);
+    const bool shared_in = b.in_unit_stride == 0;
+    // chunk the units so the per-chunk spectra stay within ~4 GiB
+    const size_t per = (size_t)np * c->csz();
+    int B = (int)std::max<size_t>(1, ((size_t)4 << 30) / per);
+    B = std::min(B, b.units);
+    B = std::min(B, 65535);
+    const size_t nbr1 = row_blocks(c->fp64, ax->L, ny, shared_in ? 1 : B);
+    const size_t nbc1 = col_blocks(c->fp64, ay->L, W, nx, 1);
+    TRY(red_prepare(c, std::max(nbr1, nbc1 * (size_t)B)));
+    const bool diag = b.diag != nullptr;
+    // spectral sums per unit and component, plus a histogram per unit
+    std::vector<double> sums((size_t)b.units * RS_COUNT * ncomp, 0.0);
+    if (diag) TRY(ensure(c->tmp, sizeof(double) * RS_COUNT * (size_t)B));
+    TRY(ensure(c->scratch, (size_t)(shared_in ? 1 : B) * per));
+    TRY(ensure(c->scratch2, (size_t)B * per));
+    void* S0 = c->scratch.p;
+    void* S1 = c->scratch2.p;
+    const Policy pol = ev_policy(b.cc, b.z.empty() ? 1.0 : b.z[0]);
+    double pin_total = 0;
+    std::vector<double> pin_unit(b.units, 0.0);
+    for (int comp = 0; comp < ncomp; comp++) {
+        for (int k0 = 0; k0 < b.units; k0 += B) {
+            const int nb = std::min(B, b.units - k0);
+            // rows forward (the shared input once per component, else per unit)
+            if (k0 == 0 || !shared_in) {
+                RowArgs r = row_defaults(ny, nx, dx);
+                r.mode = ROW_FWD;
+                r.rows = ny;
+                fill_axis(r, ax);
+                r.in = reinterpret_cast<const double2*>(b.in) +
+                       (shared_in ? comp * np : ((long long)k0 * ncomp + comp) * np);
+                r.in_c128 = 1;
+                r.in_ld = nx;
+                r.in_bstride = shared_in ? 0 : ncomp * np;
+                r.in_n = nx;
+                r.out = S0;
+                r.out_ld = nx;
+                r.out_bstride = np;
+                r.out_n = nx;
+                r.batch = shared_in ? 1 : nb;
+                if (diag) {
+                    r.red = red_region(c, 0);
+                    r.red_pre = 1;
+                }
+                CK(prof_rows(c, c->fp64, r));
+                if (diag) {
+                    const int nbr = (int)row_blocks(c->fp64, ax->L, ny, 1);
+                    CK(launch_reduce_finish(r.red, nbr, r.batch, RS_P, 1, reinterpret_cast<double*>(c->tmp.p), c->st));
+                    std::vector<double> h((size_t)r.batch * RS_COUNT);
+                    CK(cudaMemcpyAsync(h.data(), c->tmp.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+                    CK(cudaStreamSynchronize(c->st));
+                    for (int u = 0; u < r.batch; u++) {
+                        const double p = h[(size_t)u * RS_COUNT + RS_P] * dx * dx;
+                        if (shared_in) pin_total += p;
+                        else pin_unit[k0 + u] += p;
+                    }
+                }
+            }
+            ColArgs a = col_defaults(c, dx);
+            a.mode = COL_FUSED;
+            a.ncols = nx;
+            fill_axis(a, ay);
+            a.W = W;
+            a.src = S0;
+            a.src_ld = nx;
+            a.src_bstride = np;
+            a.src_shared = shared_in;
+            a.in_n = ny;
+            a.dst = S1;
+            a.dst_ld = nx;
+            a.dst_bstride = np;
+            a.out_n = ny;
+            a.h = asm_h(c, b.cc, b.z.empty() ? 0.0 : b.z[0], pol, dx, nx, ny);
+            a.h.wl = -1;  // per-unit k, k z, k |z| are formed on the device from wl and z
+            a.batch_wl = b.wl_dev ? b.wl_dev + k0 : nullptr;
+            a.batch_z = b.z_dev ? b.z_dev + k0 : nullptr;
+            if (!b.wl_dev) a.h.wl = b.cc.wavelength, a.h.k = 2 * M_PI / b.cc.wavelength;
+            a.batch = nb;
+            if (diag) {
+                a.red = red_region(c, 1);
+                a.red_bpm = 1;
+                a.red_hist = 1;
+                a.hist_lx = nx;
+                a.hist_ly = ny;
+                a.hist_dx = dx;
+            }
+            CK(prof_cols(c, c->fp64, a));
+            if (diag) {
+                double* o = reinterpret_cast<double*>(c->tmp.p);
+                CK(launch_reduce_finish(a.red, (int)nbc1, nb, RS_SW, 3, o, c->st));
+                CK(launch_reduce_finish(a.red, (int)nbc1, nb, RS_HIST, 97, o, c->st));
+                std::vector<double> h((size_t)nb * RS_COUNT);
+                CK(cudaMemcpyAsync(h.data(), o, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+                CK(cudaStreamSynchronize(c->st));
+                for (int u = 0; u < nb; u++)
+                    for (int sl = RS_SW; sl < RS_COUNT; sl++)
+                        sums[((size_t)(k0 + u) * ncomp + comp) * RS_COUNT + sl] = h[(size_t)u * RS_COUNT + sl];
+            }
+            RowArgs q = row_defaults(ny, nx, dx);
+            q.rows = ny;
+            fill_axis(q, ax);
+            q.in = S1;
+            q.in_ld = nx;
+            q.in_bstride = np;
+            q.in_n = nx;
+            q.out_ld = nx;
+            q.out_n = nx;
+            if (b.out_int) {
+                q.mode = ROW_INV_ACC;
+                q.acc_nb = nb;
+                q.acc_weight = b.w_dev ? b.w_dev + k0 : nullptr;
+                q.acc_add = 1;
+                q.out = b.out_int;
+                q.out_accum_int = 2;
+                q.out_bstride = 0;
+                q.batch = 1;
+            } else {
+                q.mode = ROW_INV;
+                q.out = reinterpret_cast<double2*>(b.out_planes) + ((long long)k0 * ncomp + comp) * np;
+                q.out_c128 = 1;
+                q.out_bstride = ncomp * np;
+                q.batch = nb;
+            }
+            CK(prof_rows(c, c->fp64, q));
+        }
+    }
+    if (diag) {
+        // per unit, in order: asmWrapWarn then asmWarn (optics/propagate.go:325-332)
+        for (int u = 0; u < b.units; u++) {
+            wos_context cu = b.cc;
+            if (!b.wl.empty()) cu.wavelength = b.wl[u];
+            const double zu = b.z.empty() ? 0.0 : b.z[u];
+            if (zu == 0) continue;
+            double sw = 0, s1 = 0, hist[97] = {0};
+            for (int comp = 0; comp < ncomp; comp++) {
+                const double* rr = &sums[((size_t)u * ncomp + comp) * RS_COUNT];
+                sw += rr[RS_SW];
+                s1 += rr[RS_SW + 1];
+                for (int k = 0; k < 97; k++) hist[k] += rr[RS_HIST + k];
+            }
+            if (wrap_needed(cu, ny, nx, dx, zu)) wrap_finish(b.diag, cu, ny, nx, dx, zu, hist);
+            const double pin = shared_in ? pin_total : pin_unit[u];
+            const double frac = sw > 0 ? s1 / sw : 0.0;  // spectral loss fraction of the step
+            asm_warn(b.diag, zu, pin, pin - pin * frac, ev_policy(cu, zu));
+        }
+    }
+    return WOS_OK;
+}
+
+int upload_params(wos_ctx c, const std::vector<double>& a, const std::vector<double>& b2,
+                  const std::vector<double>& c3, double** pa, double** pb, double** pc) {
+    const size_t n = a.size() + b2.size() + c3.size();
+    TRY(ensure(c->params, sizeof(double) * std::max<size_t>(n, 1)));
+    double* p = reinterpret_cast<double*>(c->params.p);
+    std::vector<double> all;
+    all.insert(all.end(), a.begin(), a.end());
+    all.insert(all.end(), b2.begin(), b2.end());
+    all.insert(all.end(), c3.begin(), c3.end());
+    if (n) CK(cudaMemcpyAsync(p, all.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+    *pa = p;
+    *pb = p + a.size();
+    *pc = p + a.size() + b2.size();
+    return WOS_OK;
+}
+
+int element_begin(wos_ctx c, wos_field* f) {
+    TRY(check_field(f));
+    TRY(set_device(c));
+    return stage_in(c, f, f->polarized ? 2 : 1);
+}
+double2* stage_ex(wos_ctx c) { return reinterpret_cast<double2*>(c->stage.p); }
+double2* stage_ey(wos_ctx c, const wos_field* f) { return stage_ex(c) + (size_t)f->ny * f->nx; }
+
+// Inverse design on a host problem: forward (and adjoint) of one ASM step.
+int asm_loss_grad_impl(wos_ctx c, int ny, int nx, double dx, double z, const wos_context* cc, const wos_c128* a,
+                       const double* phi, const double* target, double* loss, double* grad) {
+    if (!cc || !a || !phi || !target || !loss || ny < 2 || nx < 2 || !(dx > 0))
+        return fail(WOS_INVALID_ARG, "inverse-design arguments");
+    if (!(cc->wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    const long long np = (long long)ny * nx;
+    TRY(set_device(c));
+    TRY(ensure(c->stage, (size_t)np * 16));
+    TRY(ensure(c->maps, (size_t)np * 8 * 3));
+    TRY(ensure(c->scratch, (size_t)np * c->csz()));
+    TRY(ensure(c->scratch2, (size_t)np * c->csz()));
+    double* phid = reinterpret_cast<double*>(c->maps.p);
+    double* Td = phid + np;
+    double* gd = Td + np;
+    CK(cudaMemcpyAsync(c->stage.p, a, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(phid, phi, (size_t)np * 8, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(Td, target, (size_t)np * 8, cudaMemcpyHostToDevice, c->st));
+    Axis *ax, *ay;
+    TRY(get_axis(c, nx, c->fp64, &ax));
+    TRY(get_axis(c, ny, c->fp64, &ay));
+    const Policy pol = ev_policy(*cc, z);
+    const int W = auto_colw(c, ay->L);
+    void* S = c->scratch.p;
+    void* U = c->scratch2.p;
+    const int nres = (int)((np + 255) / 256);
+    TRY(red_prepare(c, (size_t)nres));
+    auto rows = [&](int mode, const void* in, int in_c128, void* out, const double* pphi) -> int {
+        RowArgs r = row_defaults(ny, nx, dx);
+        r.mode = mode;
+        r.rows = ny;
+        fill_axis(r, ax);
+        r.in = in;
+        r.in_c128 = in_c128;
+        r.in_ld = nx;
+        r.in_n = nx;
+        r.out = out;
+        r.out_ld = nx;
+        r.out_n = nx;
+        r.pre_phi = pphi;
+        CK(prof_rows(c, c->fp64, r));
+        return WOS_OK;
+    };
+    auto cols = [&](int conj) -> int {
+        ColArgs k = col_defaults(c, dx);
+        k.mode = COL_FUSED;
+        k.ncols = nx;
+        fill_axis(k, ay);
+        k.W = W;
+        k.src = S;
+        k.src_ld = nx;
+        k.in_n = ny;
+        k.dst = S;
+        k.dst_ld = nx;
+        k.out_n = ny;
+        k.h = asm_h(c, *cc, z, pol, dx, nx, ny);
+        k.h.conj = conj;
+        CK(prof_cols(c, c->fp64, k));
+        return WOS_OK;
+    };
+    // forward: u = A (a exp(i phi))
+    TRY(rows(ROW_FWD, c->stage.p, 1, S, phid));
+    TRY(cols(0));
+    TRY(rows(ROW_INV, S, 0, U, nullptr));
+    // residual r = 4 (|u|^2 - T) u, loss = sum (|u|^2 - T)^2
+    int nb = 0;
+    CK(launch_residual(c->fp64, U, Td, S, np, red_region(c, 0), &nb, c->st));
+    CK(launch_reduce_finish(red_region(c, 0), nb, 1, RS_P, 1, redout_region(c, 0), c->st));
+    if (grad) {
+        // adjoint: b = A^H r = F^-1 diag(conj H) F r; grad = Re(conj(b) i t a)
+        TRY(rows(ROW_FWD, S, 0, S, nullptr));
+        TRY(cols(1));
+        TRY(rows(ROW_INV, S, 0, S, nullptr));
+        CK(launch_grad(c->fp64, S, reinterpret_cast<const double2*>(c->stage.p), phid, gd, np, c->st));
+        CK(cudaMemcpyAsync(grad, gd, (size_t)np * 8, cudaMemcpyDeviceToHost, c->st));
+    }
+    TRY(fetch_red(c, 1));
+    *loss = c->hred[RS_P];
+    return WOS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int wos_splitstep(wos_ctx c, wos_field* f, double z, const wos_index_desc* n, int steps, const wos_context* cc,
+                  wos_diag* diag) {
+    if (!c || !n) return fail(WOS_INVALID_ARG, "null argument");
+    TRY(check_field(f));
+    if (diag) {
+        std::memset(diag, 0, sizeof(*diag));
+        diag->dx_out = f->dx;
+    }
+    if (z == 0) return WOS_OK;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const int ncomp = f->polarized ? 2 : 1;
+    TRY(stage_in(c, f, ncomp));
+    ScreenSrc src;
+    src.kind = 1;
+    src.desc = *n;
+    TRY(run_splitstep(c, f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, c->stage.p, 1, z, src, steps,
+                      cc ? *cc : default_context(), diag));
+    return stage_out(c, f, ncomp);
+}
+
+int wos_splitstep_dev(wos_ctx c, int ny, int nx, double dx, int ncomp, void* field, double z,
+                      const wos_index_desc* n, int steps, const wos_context* cc, wos_diag* diag) {
+    if (!c || !n) return fail(WOS_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    ScreenSrc src;
+    src.kind = 1;
+    src.desc = *n;
+    return run_splitstep(c, ny, nx, dx, ncomp, field, 0, field, 0, z, src, steps, cc ? *cc : default_context(), diag);
+}
+
+int wos_splitstep_maps(wos_ctx c, wos_field* f, double z, const double* n_re, const double* n_im, int nmaps,
+                       int steps, const wos_context* cc, wos_diag* diag) {
+    if (!c || !n_re || !n_im) return fail(WOS_INVALID_ARG, "null argument");
+    TRY(check_field(f));
+    if (diag) {
+        std::memset(diag, 0, sizeof(*diag));
+        diag->dx_out = f->dx;
+    }
+    if (z == 0) return WOS_OK;
+    const int st = steps <= 0 ? 1 : steps;
+    if (nmaps != 1 && nmaps != st) return fail(WOS_INVALID_ARG, "nmaps must be 1 or steps");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const long long np = (long long)f->ny * f->nx;
+    TRY(ensure(c->maps, sizeof(double) * 2 * np * nmaps));
+    double* re = reinterpret_cast<double*>(c->maps.p);
+    double* im = re + np * nmaps;
+    CK(cudaMemcpyAsync(re, n_re, sizeof(double) * np * nmaps, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(im, n_im, sizeof(double) * np * nmaps, cudaMemcpyHostToDevice, c->st));
+    const int ncomp = f->polarized ? 2 : 1;
+    TRY(stage_in(c, f, ncomp));
+    ScreenSrc src;
+    src.kind = 2;
+    src.nre = re;
+    src.nim = im;
+    src.nmaps = nmaps;
+    TRY(run_splitstep(c, f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, c->stage.p, 1, z, src, st,
+                      cc ? *cc : default_context(), diag));
+    return stage_out(c, f, ncomp);
+}
+
+int wos_polychromatic(wos_ctx c, const wos_field* f, double z, const double* wavelengths, const double* weights,
+                      int nsamples, int method, const wos_context* base, double* out, wos_diag* diag) {
+    if (!c || !wavelengths || !weights || !out) return fail(WOS_INVALID_ARG, "null argument");
+    TRY(check_field(f));
+    if (nsamples <= 0) return fail(WOS_INVALID_ARG, "polychromatic: no wavelength samples");
+    for (int s = 0; s < nsamples; s++)
+        if (!(wavelengths[s] > 0)) return fail(WOS_INVALID_ARG, "polychromatic: wavelength must be > 0");
+    if (method < WOS_ASM || method > WOS_FRAUNHOFER) return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
+    if (diag) {
+        std::memset(diag, 0, sizeof(*diag));
+        diag->dx_out = f->dx;
+    }
+    // a nil base context means Context{Evanescent: "decay", Warnings: &Warnings{}}
+    wos_context cc = base ? *base : default_context();
+    if (!base) cc.diagnostics = 1;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const int ncomp = f->polarized ? 2 : 1;
+    const long long np = (long long)f->ny * f->nx;
+    TRY(stage_in(c, const_cast<wos_field*>(f), ncomp));
+    TRY(ensure(c->accum, sizeof(double) * np));
+    double* acc = reinterpret_cast<double*>(c->accum.p);
+    CK(cudaMemsetAsync(acc, 0, sizeof(double) * np, c->st));
+    wos_diag* dp = (cc.diagnostics && diag) ? diag : nullptr;
+    if (z == 0) {
+        for (int s = 0; s < nsamples; s++) CK(launch_accum_int(1, acc, c->stage.p, ncomp, np, weights[s], c->st));
+    } else if (method == WOS_ASM) {
+        std::vector<double> wl(wavelengths, wavelengths + nsamples), w(weights, weights + nsamples);
+        double *wl_d, *w_d, *unused;
+        TRY(upload_params(c, wl, w, {}, &wl_d, &w_d, &unused));
+        Batch b{f->ny, f->nx, ncomp, f->dx, c->stage.p, 0, nsamples, wl_d, nullptr, wl,
+                std::vector<double>(nsamples, z), w_d, acc, nullptr, cc, dp};
+        TRY(run_batch_asm(c, b));
+    } else {
+        TRY(ensure(c->scratch3, (size_t)np * ncomp * c->csz()));
+        void* O = c->scratch3.p;
+        for (int s = 0; s < nsamples; s++) {
+            wos_context cs = cc;
+            cs.wavelength = wavelengths[s];
+            wos_diag ds;
+            Prop p{f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, O, 0, z, method, cs, dp ? &ds : nullptr};
+            TRY(run_propagate(c, p));
+            if (dp) diag_merge(dp, ds);
+            CK(launch_accum_int(c->fp64, acc, O, ncomp, np, weights[s], c->st));
+        }
+    }
+    CK(cudaMemcpyAsync(out, acc, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+int wos_volume(wos_ctx c, const wos_field* f, const double* zs, int nz, int method, const wos_context* cci,
+               wos_c128* out, wos_diag* diag) {
+    if (!c || (nz > 0 && (!zs || !out)) || nz < 0) return fail(WOS_INVALID_ARG, "null argument");
+    TRY(check_field(f));
+    if (method < WOS_ASM || method > WOS_FRAUNHOFER) return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
+    if (diag) {
+        std::memset(diag, 0, sizeof(*diag));
+        diag->dx_out = f->dx;
+    }
+    if (nz == 0) return WOS_OK;
+    const wos_context cc = cci ? *cci : default_context();
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const int ncomp = f->polarized ? 2 : 1;
+    const long long np = (long long)f->ny * f->nx;
+    TRY(stage_in(c, const_cast<wos_field*>(f), ncomp));
+    TRY(ensure(c->vol, sizeof(double2) * (size_t)np * ncomp * nz));
+    double2* O = reinterpret_cast<double2*>(c->vol.p);
+    bool batched = method == WOS_ASM;
+    std::vector<double> zb;
+    std::vector<int> idx;
+    for (int q = 0; q < nz; q++) {
+        if (zs[q] != 0) {
+            zb.push_back(zs[q]);
+            idx.push_back(q);
+            if (zs[q] < 0) batched = false;
+        }
+    }
+    wos_diag* dp = diag;
+    if (batched && !zb.empty()) {
+        // the batch writes its planes compactly, then they move to their slots
+        TRY(ensure(c->scratch3, sizeof(double2) * (size_t)np * ncomp * zb.size()));
+        double2* Ob = reinterpret_cast<double2*>(c->scratch3.p);
+        double *z_d, *u1, *u2;
+        TRY(upload_params(c, zb, {}, {}, &z_d, &u1, &u2));
+        Batch b{f->ny, f->nx, ncomp, f->dx, c->stage.p, 0, (int)zb.size(), nullptr, z_d, {}, zb, nullptr, nullptr,
+                Ob, cc, (cc.diagnostics && dp) ? dp : nullptr};
+        TRY(run_batch_asm(c, b));
+        for (size_t u = 0; u < zb.size(); u++)
+            CK(cudaMemcpyAsync(O + (size_t)idx[u] * ncomp * np, Ob + u * ncomp * np, sizeof(double2) * ncomp * np,
+                               cudaMemcpyDeviceToDevice, c->st));
+    } else {
+        for (size_t u = 0; u < zb.size(); u++) {
+            wos_diag ds;
+            Prop p{f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, O + (size_t)idx[u] * ncomp * np, 1, zb[u], method, cc,
+                   (cc.diagnostics && dp) ? &ds : nullptr};
+            TRY(run_propagate(c, p));
+            if (cc.diagnostics && dp) diag_merge(dp, ds);
+        }
+    }
+    // z == 0 returns the input unchanged (optics/propagate.go:66-68)
+    for (int q = 0; q < nz; q++)
+        if (zs[q] == 0)
+            CK(cudaMemcpyAsync(O + (size_t)q * ncomp * np, c->stage.p, sizeof(double2) * ncomp * np,
+                               cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(out, O, sizeof(double2) * (size_t)np * ncomp * nz, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+int wos_schell_modes(wos_ctx c, int n, double dx, double width, double coherence, int m, const wos_c128* noise,
+                     wos_c128* modes_out) {
+    if (!c || !noise || !modes_out || n < 2 || !(dx > 0)) return fail(WOS_INVALID_ARG, "null argument");
+    if (!(width > 0) || !(coherence > 0)) return fail(WOS_INVALID_ARG, "schell: width and coherence must be > 0");
+    if (m <= 0) m = 1;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const long long nn = (long long)n * n;
+    TRY(ensure(c->vol, sizeof(double2) * (size_t)nn * m));
+    double2* modes = reinterpret_cast<double2*>(c->vol.p);
+    TRY(schell_generate(c, n, dx, width, coherence, m, noise, modes));
+    CK(cudaMemcpyAsync(modes_out, modes, sizeof(double2) * (size_t)nn * m, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+int wos_partially_coherent(wos_ctx c, int n, double dx, double width, double coherence, int m,
+                           const wos_c128* noise, double z, int method, const wos_context* cci, double* out,
+                           wos_diag* diag) {
+    if (!c || !noise || !out || n < 2 || !(dx > 0)) return fail(WOS_INVALID_ARG, "null argument");
+    if (!(width > 0) || !(coherence > 0)) return fail(WOS_INVALID_ARG, "schell: width and coherence must be > 0");
+    if (method < WOS_ASM || method > WOS_FRAUNHOFER) return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
+    if (m <= 0) m = 1;
+    if (diag) {
+        std::memset(diag, 0, sizeof(*diag));
+        diag->dx_out = dx;
+    }
+    const wos_context cc = cci ? *cci : default_context();
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const long long nn = (long long)n * n;
+    TRY(ensure(c->vol, sizeof(double2) * (size_t)nn * m));
+    double2* modes = reinterpret_cast<double2*>(c->vol.p);
+    TRY(schell_generate(c, n, dx, width, coherence, m, noise, modes));
+    TRY(ensure(c->accum, sizeof(double) * nn));
+    double* acc = reinterpret_cast<double*>(c->accum.p);
+    CK(cudaMemsetAsync(acc, 0, sizeof(double) * nn, c->st));
+    const double inv = 1 / (double)m;
+    wos_diag* dp = (cc.diagnostics && diag) ? diag : nullptr;
+    if (z == 0) {
+        for (int q = 0; q < m; q++) CK(launch_accum_int(1, acc, modes + q * nn, 1, nn, inv, c->st));
+    } else if (method == WOS_ASM) {
+        std::vector<double> w(m, inv);
+        double *w_d, *u1, *u2;
+        TRY(upload_params(c, w, {}, {}, &w_d, &u1, &u2));
+        Batch b{n, n, 1, dx, modes, nn, m, nullptr, nullptr, {}, std::vector<double>(m, z), w_d, acc, nullptr, cc, dp};
+        TRY(run_batch_asm(c, b));
+    } else {
+        TRY(ensure(c->scratch3, (size_t)nn * c->csz()));
+        void* O = c->scratch3.p;
+        for (int q = 0; q < m; q++) {
+            wos_diag ds;
+            Prop p{n, n, dx, 1, modes + q * nn, 1, O, 0, z, method, cc, dp ? &ds : nullptr};
+            TRY(run_propagate(c, p));
+            if (dp) diag_merge(dp, ds);
+            CK(launch_accum_int(c->fp64, acc, O, 1, nn, inv, c->st));
+        }
+    }
+    CK(cudaMemcpyAsync(out, acc, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+int wos_apply_lens(wos_ctx c, wos_field* f, double wavelength, double focal, double aperture, double x0, double y0) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    if (focal == 0) return fail(WOS_INVALID_ARG, "lens: focal length f must be non-zero");
+    if (!(wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(element_begin(c, f));
+    const double k = 2 * M_PI / wavelength;
+    const double cc = -k / (2 * focal);
+    CK(launch_lens(stage_ex(c), stage_ey(c, f), f->polarized, f->ny, f->nx, f->dx, cc, aperture, x0, y0, c->st));
+    return stage_out(c, f, f->polarized ? 2 : 1);
+}
+
+int wos_apply_aperture_circle(wos_ctx c, wos_field* f, double radius, double x0, double y0, double edge_sigma) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(element_begin(c, f));
+    CK(launch_aperture_circle(stage_ex(c), stage_ey(c, f), f->polarized, f->ny, f->nx, f->dx, radius, x0, y0,
+                              edge_sigma, c->st));
+    return stage_out(c, f, f->polarized ? 2 : 1);
+}
+
+int wos_apply_grating(wos_ctx c, wos_field* f, int kind, double period, double modulation, double duty,
+                      double blaze_depth, double rotation, double offset) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    if (!(period > 0)) return fail(WOS_INVALID_ARG, "grating: period must be > 0");
+    if (duty < 0 || duty > 1) return fail(WOS_INVALID_ARG, "grating: duty must be in [0,1]");
+    if (kind < 0 || kind > 4) return fail(WOS_INVALID_ARG, "grating: unknown kind");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(element_begin(c, f));
+    CK(launch_grating(stage_ex(c), stage_ey(c, f), f->polarized, f->ny, f->nx, f->dx, kind, period, modulation, duty,
+                      blaze_depth, rotation, offset, c->st));
+    return stage_out(c, f, f->polarized ? 2 : 1);
+}
+
+int wos_apply_phase_mask(wos_ctx c, wos_field* f, const double* phi, double amp) {
+    if (!c || !phi) return fail(WOS_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(element_begin(c, f));
+    const long long np = (long long)f->ny * f->nx;
+    TRY(ensure(c->maps, sizeof(double) * np));
+    CK(cudaMemcpyAsync(c->maps.p, phi, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+    CK(launch_phase_mask(stage_ex(c), stage_ey(c, f), f->polarized, np, reinterpret_cast<double*>(c->maps.p), amp,
+                         c->st));
+    return stage_out(c, f, f->polarized ? 2 : 1);
+}
+
+int wos_asm_forward_loss(wos_ctx c, int ny, int nx, double dx, double z, const wos_context* cc, const wos_c128* a,
+                         const double* phi, const double* target, double* loss) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    return asm_loss_grad_impl(c, ny, nx, dx, z, cc, a, phi, target, loss, nullptr);
+}
+
+int wos_asm_loss_grad(wos_ctx c, int ny, int nx, double dx, double z, const wos_context* cc, const wos_c128* a,
+                      const double* phi, const double* target, double* loss, double* grad) {
+    if (!c || !grad) return fail(WOS_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    return asm_loss_grad_impl(c, ny, nx, dx, z, cc, a, phi, target, loss, grad);
+}
+
+int wos_ctx_set_fast_path(wos_ctx c, int enabled) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->no_fast = !enabled;
+    return WOS_OK;
+}
+
+int wos_ctx_set_tune(wos_ctx c, int ny, int nx, int row_e, int col_e, int col_w) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    if (!fast_supported(c->fp64, nx, row_e) || !fast_supported(c->fp64, ny, col_e) || col_w < 1 ||
+        (col_w & (col_w - 1)))
+        return fail(WOS_INVALID_ARG, "unsupported launch configuration");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->tune[tune_key(c->fp64, ny, nx)] = Tune{row_e, col_e, col_w};
+    return WOS_OK;
+}
+
+// Times every launch configuration of the specialised ASM sweeps for an
+// ny x nx grid on this device (in-place propagations of a scratch field,
+// CUDA events on the context stream) and keeps the fastest for the context.
+int wos_autotune(wos_ctx c, int ny, int nx, int* row_e, int* col_e, int* col_w) {
+    if (!c || ny < 2 || nx < 2) return fail(WOS_INVALID_ARG, "autotune arguments");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const long long key = tune_key(c->fp64, ny, nx);
+    c->tune.erase(key);
+    const Tune def = get_tune(c, ny, nx);
+    if (!is_pow2(nx) || !is_pow2(ny)) {
+        if (row_e) *row_e = def.rowE;
+        if (col_e) *col_e = def.colE;
+        if (col_w) *col_w = def.colW;
+        return WOS_OK;
+    }
+    const long long np = (long long)ny * nx;
+    TRY(ensure(c->aux, (size_t)np * c->csz()));
+    CK(cudaMemsetAsync(c->aux.p, 0, (size_t)np * c->csz(), c->st));
+    wos_context cc = default_context();
+    cc.wavelength = 0.5e-6;
+    Prop p{ny, nx, 1e-6, 1, c->aux.p, 0, c->aux.p, 0, 1e-3, WOS_ASM, cc, nullptr};
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    Tune bt = def;
+    const int es[2] = {8, 16};
+    for (int re : es)
+        for (int ce : es)
+            for (int w = 1; w <= 16; w <<= 1) {
+                if (!fast_supported(c->fp64, nx, re) || !fast_supported(c->fp64, ny, ce)) continue;
+                const int T = ny / ce;
+                const int maxt = (ce >= 16 || c->fp64) ? 512 : 1024;
+                if ((w * T > maxt && w > 1) || col_smem_bytes(c->fp64, ny, w) > 220 * 1024) continue;
+                c->tune[key] = Tune{re, ce, w};
+                bool ok = true;
+                for (int it = 0; it < 2 && ok; it++) ok = run_propagate(c, p) == WOS_OK;
+                if (!ok) {
+                    cudaGetLastError();
+                    continue;
+                }
+                cudaEventRecord(e0, c->st);
+                for (int it = 0; it < 5 && ok; it++) ok = run_propagate(c, p) == WOS_OK;
+                cudaEventRecord(e1, c->st);
+                cudaEventSynchronize(e1);
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ok && ms < best) {
+                    best = ms;
+                    bt = Tune{re, ce, w};
+                }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c->tune[key] = bt;
+    if (row_e) *row_e = bt.rowE;
+    if (col_e) *col_e = bt.colE;
+    if (col_w) *col_w = bt.colW;
+    return WOS_OK;
+}
+
+int wos_asm_adjoint(wos_ctx c, wos_field* f, double z, const wos_context* cci) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    TRY(check_field(f));
+    const wos_context cc = cci ? *cci : default_context();
+    if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const int ncomp = f->polarized ? 2 : 1;
+    TRY(stage_in(c, f, ncomp));
+    Prop p{f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, c->stage.p, 1, z, WOS_ASM, cc, nullptr};
+    Sweep3 s;
+    s.h = asm_h(c, cc, z, ev_policy(cc, z), f->dx, f->nx, f->ny);
+    s.h.conj = 1;
+    TRY(run_sweep3(c, p, s));
+    return stage_out(c, f, ncomp);
+}
+
+}  // extern "C"

@@ -1,0 +1,251 @@
+// wos_elem.cu -- pointwise kernels: thin-element transmissions, Gaussian
+// Schell-model mode synthesis, intensity accumulation and the inverse-design
+// residual / gradient.  All element arithmetic is FP64 on complex128 fields,
+// formed in the reference's operation order (no FMA contraction) so that the
+// FP64 path reproduces optics/elements.go and optics/coherence.go.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "wos_fft.cuh"
+#include "wos_kernels.cuh"
+
+namespace wos {
+
+namespace {
+__device__ __forceinline__ double dm(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double da(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double ds(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dd(double a, double b) { return __ddiv_rn(a, b); }
+// Go complex128 product (ac - bd, ad + bc) without contraction
+__device__ __forceinline__ double2 gmul(double2 a, double2 b) {
+    return make_double2(ds(dm(a.x, b.x), dm(a.y, b.y)), da(dm(a.x, b.y), dm(a.y, b.x)));
+}
+__device__ __forceinline__ double2 gexpi(double phi) {
+    double s, c;
+    sincos(phi, &s, &c);
+    return make_double2(c, s);
+}
+__device__ __forceinline__ double coord(int i, int n, double dx) { return dm(ds((double)i, (double)n / 2), dx); }
+__device__ __forceinline__ double ghypot(double p, double q) {
+    p = fabs(p);
+    q = fabs(q);
+    if (p < q) { double t = p; p = q; q = t; }
+    if (p == 0) return 0;
+    q = dd(q, p);
+    return dm(p, __dsqrt_rn(da(1.0, dm(q, q))));
+}
+__device__ __forceinline__ void apply2(double2* ex, double2* ey, int pol, long long idx, double2 t) {
+    ex[idx] = gmul(ex[idx], t);
+    if (pol) ey[idx] = gmul(ey[idx], t);
+}
+}  // namespace
+
+// lensEl.Apply (optics/elements.go:195-221); c = -k/(2f) formed by the caller
+__global__ void k_lens(double2* ex, double2* ey, int pol, int ny, int nx, double dx, double c, double ap,
+                       double x0, double y0) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)ny * nx) return;
+    const int j = (int)(idx / nx), i = (int)(idx % nx);
+    const double dy = ds(coord(j, ny, dx), y0);
+    const double dxx = ds(coord(i, nx, dx), x0);
+    const double r2 = da(dm(dxx, dxx), dm(dy, dy));
+    if (ap > 0 && r2 > dm(ap, ap)) {
+        ex[idx] = make_double2(0, 0);
+        if (pol) ey[idx] = make_double2(0, 0);
+        return;
+    }
+    apply2(ex, ey, pol, idx, gexpi(dm(c, r2)));
+}
+
+// apertureEl.Apply with the circle outline (elements.go:288-313, shape.go:163-169)
+__global__ void k_aperture_circle(double2* ex, double2* ey, int pol, int ny, int nx, double dx, double radius,
+                                  double x0, double y0, double sig) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)ny * nx) return;
+    const int j = (int)(idx / nx), i = (int)(idx % nx);
+    const double dy = ds(coord(j, ny, dx), y0);
+    const double dxx = ds(coord(i, nx, dx), x0);
+    const double d = ds(radius, ghypot(dxx, dy));
+    double t;
+    if (sig > 0) t = dm(0.5, da(1.0, erf(dd(d, dm(M_SQRT2, sig)))));
+    else t = d >= 0 ? 1.0 : 0.0;
+    apply2(ex, ey, pol, idx, make_double2(t, 0));
+}
+
+// gratingEl.Apply (elements.go:488-532)
+__global__ void k_grating(double2* ex, double2* ey, int pol, int ny, int nx, double dx, int kind, double period,
+                          double modulation, double duty, double blaze, double rotation, double off) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)ny * nx) return;
+    const int j = (int)(idx / nx), i = (int)(idx % nx);
+    const double c = cos(rotation), s = sin(rotation);
+    const double uu = da(dm(c, coord(i, nx, dx)), dm(s, coord(j, ny, dx)));
+    const double ph = dd(dm(2 * M_PI, uu), period);
+    double2 t = make_double2(0, 0);
+    switch (kind) {
+    case 0: t = make_double2(dm(0.5, da(1.0, dm(modulation, cos(da(ph, off))))), 0); break;
+    case 1: if (cos(da(ph, off)) >= cos(dm(M_PI, duty))) t = make_double2(1, 0); break;
+    case 2: t = gexpi(dm(dd(modulation, 2.0), sin(da(ph, off)))); break;
+    case 3: t = (cos(da(ph, off)) >= 0) ? gexpi(modulation) : make_double2(1, 0); break;
+    default: {
+        double fr = fmod(dd(uu, period), 1.0);
+        if (fr < 0) fr = da(fr, 1.0);
+        t = gexpi(dm(blaze, fr));
+    } break;
+    }
+    apply2(ex, ey, pol, idx, t);
+}
+
+// applyMask with t = amp * exp(i phi) (elements.go:128-141)
+__global__ void k_phase_mask(double2* ex, double2* ey, int pol, long long n, const double* phi, double amp) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    apply2(ex, ey, pol, idx, gmul(make_double2(amp, 0), gexpi(phi[idx])));
+}
+
+// ---- Gaussian Schell-model synthesis (optics/coherence.go:32-77)
+__global__ void k_schell_mu(double2* a, int n, double dx, double coh) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * n) return;
+    const int j = (int)(idx / n), i = (int)(idx % n);
+    const double dy = (j <= n / 2) ? dm((double)j, dx) : dm((double)(j - n), dx);
+    const double d = (i <= n / 2) ? dm((double)i, dx) : dm((double)(i - n), dx);
+    const double mu = exp(dd(-da(dm(d, d), dm(dy, dy)), dm(dm(2.0, coh), coh)));
+    a[idx] = make_double2(mu, 0);
+}
+__global__ void k_sqrt_re(double* s, const double2* a, long long nn) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= nn) return;
+    double v = a[idx].x;
+    if (v < 0) v = 0;
+    s[idx] = sqrt(v);
+}
+__global__ void k_mul_map(double2* a, const double* s, long long nn, int batches) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= nn * batches) return;
+    a[idx] = gmul(a[idx], make_double2(s[idx % nn], 0));
+}
+__global__ void k_schell_env(double2* a, int n, double dx, double width, int batches) {
+    const long long nn = (long long)n * n;
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= nn * batches) return;
+    const long long p = idx % nn;
+    const int j = (int)(p / n), i = (int)(p % n);
+    const double x = coord(i, n, dx), y = coord(j, n, dx);
+    const double I = exp(dd(dm(-2.0, da(dm(x, x), dm(y, y))), dm(width, width)));
+    a[idx] = gmul(a[idx], make_double2(sqrt(I), 0));
+}
+
+// out[i] += w * sum_c |f[c][i]|^2  (PropagatePolychromatic / AverageIntensity)
+template <typename C>
+__global__ void k_accum_int(double* out, const C* f, int ncomp, long long np, double w) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= np) return;
+    double p = 0;
+    for (int c = 0; c < ncomp; c++) {
+        const C v = f[c * np + idx];
+        p += (double)v.x * v.x + (double)v.y * v.y;
+    }
+    out[idx] += w * p;
+}
+
+// r = 4 (|u|^2 - T) u and per-CTA partial sums of (|u|^2 - T)^2
+template <typename C>
+__global__ void k_residual(const C* u, const double* T, C* r, long long n, double* partials) {
+    __shared__ double sm[32];
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    double l = 0;
+    if (idx < n) {
+        const C v = u[idx];
+        const double d = (double)v.x * v.x + (double)v.y * v.y - T[idx];
+        l = d * d;
+        r[idx] = mkc<C>((decltype(C::x))(4 * d * (double)v.x), (decltype(C::x))(4 * d * (double)v.y));
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_down_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = l;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += sm[w];
+        partials[(long long)blockIdx.x * RS_COUNT + RS_P] = s;
+    }
+}
+
+// g = Re(conj(b) * i * t * a), t = exp(i phi)
+template <typename C>
+__global__ void k_grad(const C* b, const double2* a, const double* phi, double* g, long long n) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    double s, c;
+    sincos(phi[idx], &s, &c);
+    const double2 av = a[idx];
+    const double tar = c * av.x - s * av.y, tai = c * av.y + s * av.x;  // t*a
+    const double ir = -tai, ii = tar;                                  // i*t*a
+    const C bv = b[idx];
+    g[idx] = (double)bv.x * ir + (double)bv.y * ii;
+}
+
+// ---------------------------------------------------------------- launchers
+static inline unsigned nblk(long long n, int b = 256) { return (unsigned)((n + b - 1) / b); }
+
+cudaError_t launch_lens(double2* ex, double2* ey, int pol, int ny, int nx, double dx, double c, double ap, double x0,
+                        double y0, cudaStream_t st) {
+    k_lens<<<nblk((long long)ny * nx), 256, 0, st>>>(ex, ey, pol, ny, nx, dx, c, ap, x0, y0);
+    return cudaGetLastError();
+}
+cudaError_t launch_aperture_circle(double2* ex, double2* ey, int pol, int ny, int nx, double dx, double radius,
+                                   double x0, double y0, double sig, cudaStream_t st) {
+    k_aperture_circle<<<nblk((long long)ny * nx), 256, 0, st>>>(ex, ey, pol, ny, nx, dx, radius, x0, y0, sig);
+    return cudaGetLastError();
+}
+cudaError_t launch_grating(double2* ex, double2* ey, int pol, int ny, int nx, double dx, int kind, double period,
+                           double modulation, double duty, double blaze, double rotation, double off,
+                           cudaStream_t st) {
+    k_grating<<<nblk((long long)ny * nx), 256, 0, st>>>(ex, ey, pol, ny, nx, dx, kind, period, modulation, duty, blaze,
+                                                       rotation, off);
+    return cudaGetLastError();
+}
+cudaError_t launch_phase_mask(double2* ex, double2* ey, int pol, long long n, const double* phi, double amp,
+                              cudaStream_t st) {
+    k_phase_mask<<<nblk(n), 256, 0, st>>>(ex, ey, pol, n, phi, amp);
+    return cudaGetLastError();
+}
+cudaError_t launch_schell_mu(double2* a, int n, double dx, double coh, cudaStream_t st) {
+    k_schell_mu<<<nblk((long long)n * n), 256, 0, st>>>(a, n, dx, coh);
+    return cudaGetLastError();
+}
+cudaError_t launch_sqrt_re(double* s, const double2* a, long long nn, cudaStream_t st) {
+    k_sqrt_re<<<nblk(nn), 256, 0, st>>>(s, a, nn);
+    return cudaGetLastError();
+}
+cudaError_t launch_mul_map(double2* a, const double* s, long long nn, int batches, cudaStream_t st) {
+    k_mul_map<<<nblk(nn * batches), 256, 0, st>>>(a, s, nn, batches);
+    return cudaGetLastError();
+}
+cudaError_t launch_schell_env(double2* a, int n, double dx, double width, int batches, cudaStream_t st) {
+    k_schell_env<<<nblk((long long)n * n * batches), 256, 0, st>>>(a, n, dx, width, batches);
+    return cudaGetLastError();
+}
+cudaError_t launch_accum_int(int fp64, double* out, const void* f, int ncomp, long long np, double w,
+                             cudaStream_t st) {
+    if (fp64) k_accum_int<double2><<<nblk(np), 256, 0, st>>>(out, reinterpret_cast<const double2*>(f), ncomp, np, w);
+    else k_accum_int<float2><<<nblk(np), 256, 0, st>>>(out, reinterpret_cast<const float2*>(f), ncomp, np, w);
+    return cudaGetLastError();
+}
+cudaError_t launch_residual(int fp64, const void* u, const double* T, void* r, long long n, double* partials,
+                            int* nblocks, cudaStream_t st) {
+    *nblocks = (int)nblk(n);
+    if (fp64)
+        k_residual<double2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<const double2*>(u), T, reinterpret_cast<double2*>(r), n, partials);
+    else
+        k_residual<float2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<const float2*>(u), T, reinterpret_cast<float2*>(r), n, partials);
+    return cudaGetLastError();
+}
+cudaError_t launch_grad(int fp64, const void* b, const double2* a, const double* phi, double* g, long long n,
+                        cudaStream_t st) {
+    if (fp64) k_grad<double2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<const double2*>(b), a, phi, g, n);
+    else k_grad<float2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<const float2*>(b), a, phi, g, n);
+    return cudaGetLastError();
+}
+
+}  // namespace wos

@@ -1,0 +1,411 @@
+// wos_fast.cu -- compile-time specialised sweeps of the band-limited ASM hot
+// path (power-of-two lines): the transform length L and the elements per
+// thread E are template parameters, so every pass radix, Stockham stride and
+// twiddle step is a compile-time constant and the passes unroll completely.
+//
+//   k_rows_fast<Real, L, E, INV>: one row per T = L/E threads; coalesced
+//       loads straight into registers, optional complex128 I/O conversion,
+//       optional |E|^2 reduction, coalesced stores.
+//   k_cols_fast<Real, L, E>: W adjacent columns per CTA; forward column
+//       FFT, H(fx, fy) of asmTF (optics/propagate.go:159-181) generated on the
+//       fly from an FP64 argument, inverse column FFT; optional spectral
+//       power-loss sums.  Three sweeps per propagation in total.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "wos_fast.cuh"
+#include "wos_fft.cuh"
+
+namespace wos {
+
+template <int N> struct Log2 { static constexpr int v = 1 + Log2<N / 2>::v; };
+template <> struct Log2<1> { static constexpr int v = 0; };
+
+template <int L, int E> struct FPlan {
+    static constexpr int LG = Log2<L>::v, LE = Log2<E>::v;
+    static constexpr int P = (LG + LE - 1) / LE;                       // passes
+    static constexpr int RS = (LG % LE) ? (1 << (LG % LE)) : E;        // the odd radix (E if none)
+    static constexpr int T = L / E;                                    // threads per line
+};
+template <int L, int E, bool INV, int p> struct FRadix {
+    static constexpr int v = INV ? (p == FPlan<L, E>::P - 1 ? FPlan<L, E>::RS : E) : (p == 0 ? FPlan<L, E>::RS : E);
+};
+
+// One Stockham DIT pass, radix R, sub-transform length NS (compile time).
+template <int R, int E, int L, int NS, bool INV, typename C>
+__device__ __forceinline__ void fpass(C* v, int tt, const C* __restrict__ tw) {
+    constexpr int T = L / E;
+#pragma unroll
+    for (int b = 0; b < E / R; b++) {
+        if constexpr (NS > 1) {
+            const int j = tt + b * T;
+            const int k = j & (NS - 1);
+            constexpr int step = L / (NS * R);
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                C w = __ldg(tw + r * k * step);
+                if (INV) w.y = -w.y;
+                v[b * R + r] = cmul(v[b * R + r], w);
+            }
+        }
+        dft<R, INV>(v + b * R);
+    }
+}
+
+template <int R, int E, int L, int NS, typename C, typename IDX>
+__device__ __forceinline__ void fstore(const C* v, C* sm, const IDX& ix, int line, int tt) {
+    constexpr int T = L / E;
+#pragma unroll
+    for (int b = 0; b < E / R; b++) {
+        const int j = tt + b * T;
+        const int k = j & (NS - 1);
+        const int base = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) sm[ix(line, base + r * NS)] = v[b * R + r];
+    }
+}
+
+template <int R, int E, int L, typename C, typename IDX>
+__device__ __forceinline__ void fload(C* v, const C* sm, const IDX& ix, int line, int tt) {
+    constexpr int T = L / E;
+#pragma unroll
+    for (int b = 0; b < E / R; b++)
+#pragma unroll
+        for (int r = 0; r < R; r++) v[b * R + r] = sm[ix(line, tt + b * T + r * (L / R))];
+}
+
+// All passes from p on (template recursion, fully unrolled).
+template <int L, int E, bool INV, int p, int NS, typename C, typename IDX>
+__device__ __forceinline__ void fpasses(C* v, C* sm, const IDX& ix, int line, int tt, const C* __restrict__ tw) {
+    using PL = FPlan<L, E>;
+    if constexpr (p < PL::P) {
+        constexpr int R = FRadix<L, E, INV, p>::v;
+        fpass<R, E, L, NS, INV>(v, tt, tw);
+        if constexpr (p < PL::P - 1) {
+            constexpr int R2 = FRadix<L, E, INV, p + 1>::v;
+            __syncthreads();
+            fstore<R, E, L, NS>(v, sm, ix, line, tt);
+            __syncthreads();
+            fload<R2, E, L>(v, sm, ix, line, tt);
+            fpasses<L, E, INV, p + 1, NS * R>(v, sm, ix, line, tt, tw);
+        }
+    }
+}
+
+// position of register slot s under the natural mapping of radix R
+template <int R, int E, int L>
+__device__ __forceinline__ int fpos(int s, int tt) {
+    return tt + (s / R) * (L / E) + (s % R) * (L / R);
+}
+
+template <typename Real, int E> struct FMaxT { static constexpr int v = (E >= 16 || sizeof(Real) == 8) ? 512 : 1024; };
+
+// ------------------------------------------------------------------- rows
+template <typename Real, int L, int E, bool INV>
+__global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows a) {
+    using C = typename CT<Real>::t;
+    using PL = FPlan<L, E>;
+    constexpr int T = PL::T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int lines = blockDim.x / T;
+    const int line = threadIdx.x / T, tt = threadIdx.x - line * T;
+    const int r = blockIdx.x * lines + line;
+    const bool act = r < a.rows;
+    const RowIdx ix{row_line_stride(L)};
+    const C* tw = reinterpret_cast<const C*>(a.tw);
+    constexpr int R1 = INV ? E : PL::RS;
+    constexpr int RO = INV ? PL::RS : E;
+    const long long ib = (long long)blockIdx.y * a.in_bstride + (long long)r * a.in_ld;
+    const long long ob = (long long)blockIdx.y * a.out_bstride + (long long)r * a.out_ld;
+    C v[E];
+    double pw = 0;
+    if (act) {
+        if (a.in_c128) {
+            const double2* in = reinterpret_cast<const double2*>(a.in) + ib;
+#pragma unroll
+            for (int s = 0; s < E; s++) {
+                const double2 d = in[fpos<R1, E, L>(s, tt)];
+                v[s] = mkc<C>((Real)d.x, (Real)d.y);
+            }
+        } else {
+            const C* in = reinterpret_cast<const C*>(a.in) + ib;
+#pragma unroll
+            for (int s = 0; s < E; s++) v[s] = in[fpos<R1, E, L>(s, tt)];
+        }
+        if (a.red) {
+#pragma unroll
+            for (int s = 0; s < E; s++) pw += (double)v[s].x * v[s].x + (double)v[s].y * v[s].y;
+        }
+    } else {
+#pragma unroll
+        for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
+    }
+    fpasses<L, E, INV, 0, 1>(v, sm, ix, line, tt, tw);
+    if (act) {
+        if (a.out_scale != 1.0) {
+#pragma unroll
+            for (int s = 0; s < E; s++) v[s] = cscale(v[s], (Real)a.out_scale);
+        }
+        if (a.red && INV) {
+            pw = 0;
+#pragma unroll
+            for (int s = 0; s < E; s++) pw += (double)v[s].x * v[s].x + (double)v[s].y * v[s].y;
+        }
+        if (a.out_c128) {
+            double2* out = reinterpret_cast<double2*>(a.out) + ob;
+#pragma unroll
+            for (int s = 0; s < E; s++) out[fpos<RO, E, L>(s, tt)] = make_double2(v[s].x, v[s].y);
+        } else {
+            C* out = reinterpret_cast<C*>(a.out) + ob;
+#pragma unroll
+            for (int s = 0; s < E; s++) out[fpos<RO, E, L>(s, tt)] = v[s];
+        }
+    }
+    if (a.red) {
+        // per-CTA partial of sum |E|^2 (slot 0 of a RS_COUNT record)
+        __shared__ double rsm[32];
+        for (int o = 16; o > 0; o >>= 1) pw += __shfl_down_sync(0xffffffffu, pw, o);
+        if ((threadIdx.x & 31) == 0) rsm[threadIdx.x >> 5] = pw;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += rsm[w];
+            a.red[((long long)blockIdx.y * gridDim.x + blockIdx.x) * a.red_stride] = t;
+        }
+    }
+}
+
+// ------------------------------------------------------------------- cols
+__device__ __forceinline__ float fast_reduce_2pi(double arg) {
+    const double inv2pi = 0.15915494309189533577;
+    const double p2hi = 6.283185307179586232;
+    const double p2lo = 2.4492935982947064e-16;
+    const double n = rint(arg * inv2pi);
+    double r = fma(-n, p2hi, arg);
+    r = fma(-n, p2lo, r);
+    return (float)r;
+}
+
+template <typename Real, int L, int E>
+__global__ void __launch_bounds__(FMaxT<Real, E>::v) k_cols_fast(const FastCols a) {
+    using C = typename CT<Real>::t;
+    using PL = FPlan<L, E>;
+    constexpr int T = PL::T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int W = a.W;
+    const int w = threadIdx.x & (W - 1);
+    const int tt = threadIdx.x / W;
+    const int col = blockIdx.x * W + w;
+    const bool act = col < a.ncols;
+    const ColIdx ix{W};
+    const C* tw = reinterpret_cast<const C*>(a.tw);
+    C* base = reinterpret_cast<C*>(a.data) + (long long)blockIdx.y * a.bstride;
+    C v[E];
+    constexpr int R1 = PL::RS;
+#pragma unroll
+    for (int s = 0; s < E; s++)
+        v[s] = act ? base[(long long)fpos<R1, E, L>(s, tt) * a.ld + col] : mkc<C>(0, 0);
+    fpasses<L, E, false, 0, 1>(v, sm, ix, w, tt, tw);
+
+    // transfer function on the natural radix-E mapping: q = tt + s*T
+    const double wl = a.wl;
+    const double fx = (col <= a.ncols / 2 ? (double)col : (double)(col - a.ncols)) / ((double)a.ncols * a.dx);
+    double p0 = 0, l1 = 0;
+    if constexpr (sizeof(Real) == 4) {
+        // FP32 pipeline: FP64 argument kz*sqrt(1 - (wl fx)^2 - (wl fy)^2),
+        // reduced to [-pi, pi] in FP64, sin/cos in FP32
+        const double ax = wl * fx;
+        const double cx = fma(-ax, ax, 1.0);
+        const double g = wl / ((double)L * a.dx);
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int q = tt + s * T;
+            const double qq = (q <= L / 2) ? (double)q : (double)(q - L);
+            const double ay = qq * g;
+            const double sq = fma(-ay, ay, cx);
+            float hr, hi;
+            double m2 = 1.0;
+            if (sq >= 0) {
+                sincosf(fast_reduce_2pi(a.kz * sqrt(sq)), &hi, &hr);
+            } else {
+                const double decay = a.kaz * sqrt(-sq);
+                double amp;
+                if (a.zero_ev || (a.limit > 0 && decay > a.limit)) amp = 0;
+                else if (a.backward) amp = a.reg ? exp(decay) / (1.0 + a.alpha * a.alpha * exp(2 * decay)) : exp(decay);
+                else amp = exp(-decay);
+                hr = (float)amp;
+                hi = 0.f;
+                m2 = amp * amp;
+            }
+            if (a.red) {
+                const double pp = (double)v[s].x * v[s].x + (double)v[s].y * v[s].y;
+                p0 += pp;
+                l1 += pp * (1.0 - m2);
+            }
+            const float sc = (float)a.scale;
+            v[s] = cmul(v[s], make_float2(hr * sc, (a.conj ? -hi : hi) * sc));
+        }
+    } else {
+        // FP64 pipeline: the reference's operation sequence, uncontracted
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int q = tt + s * T;
+            const double den = __dmul_rn((double)L, a.dx);
+            const double fy = (q <= L / 2) ? __ddiv_rn((double)q, den) : __ddiv_rn((double)(q - L), den);
+            const double fxe = (col <= a.ncols / 2) ? __ddiv_rn((double)col, __dmul_rn((double)a.ncols, a.dx))
+                                                    : __ddiv_rn((double)(col - a.ncols), __dmul_rn((double)a.ncols, a.dx));
+            double p = fabs(__dmul_rn(wl, fxe)), qv = fabs(__dmul_rn(wl, fy));
+            if (p < qv) { const double t = p; p = qv; qv = t; }
+            double rho = 0;
+            if (p != 0) {
+                const double qq = __ddiv_rn(qv, p);
+                rho = __dmul_rn(p, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(qq, qq))));
+            }
+            double hr, hi, m2 = 1.0;
+            if (rho <= 1.0) {
+                sincos(__dmul_rn(a.kz, __dsqrt_rn(__dmul_rn(__dsub_rn(1.0, rho), __dadd_rn(1.0, rho)))), &hi, &hr);
+            } else {
+                const double decay = __dmul_rn(a.kaz, __dsqrt_rn(__dmul_rn(__dsub_rn(rho, 1.0), __dadd_rn(rho, 1.0))));
+                double amp;
+                if (a.zero_ev || (a.limit > 0 && decay > a.limit)) amp = 0;
+                else if (a.backward) {
+                    if (a.reg) {
+                        const double e = exp(decay);
+                        amp = __ddiv_rn(e, __dadd_rn(1.0, __dmul_rn(__dmul_rn(__dmul_rn(a.alpha, a.alpha), e), e)));
+                    } else {
+                        amp = exp(decay);
+                    }
+                } else {
+                    amp = exp(-decay);
+                }
+                hr = amp;
+                hi = 0;
+                m2 = amp * amp;
+            }
+            if (a.red) {
+                const double pp = v[s].x * v[s].x + v[s].y * v[s].y;
+                p0 += pp;
+                l1 += pp * (1.0 - m2);
+            }
+            v[s] = cmul(v[s], make_double2(hr * a.scale, (a.conj ? -hi : hi) * a.scale));
+        }
+    }
+    if (!act) {
+#pragma unroll
+        for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
+        p0 = 0;
+        l1 = 0;
+    }
+    fpasses<L, E, true, 0, 1>(v, sm, ix, w, tt, tw);
+    if (act) {
+        constexpr int RO = PL::RS;
+#pragma unroll
+        for (int s = 0; s < E; s++) base[(long long)fpos<RO, E, L>(s, tt) * a.ld + col] = v[s];
+    }
+    if (a.red) {
+        __shared__ double rsm[32][2];
+        for (int o = 16; o > 0; o >>= 1) {
+            p0 += __shfl_down_sync(0xffffffffu, p0, o);
+            l1 += __shfl_down_sync(0xffffffffu, l1, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            rsm[threadIdx.x >> 5][0] = p0;
+            rsm[threadIdx.x >> 5][1] = l1;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t0 = 0, t1 = 0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
+                t0 += rsm[k][0];
+                t1 += rsm[k][1];
+            }
+            double* o = a.red + ((long long)blockIdx.y * gridDim.x + blockIdx.x) * a.red_stride;
+            o[0] = t0;
+            o[1] = t1;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ launch
+template <typename Real, int L, int E, bool INV>
+static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
+    constexpr int T = L / E;
+    int lines = 1;
+    while (lines * 2 * T <= 256 && lines * 2 <= a.rows) lines *= 2;
+    while (lines * T < 32) lines *= 2;
+    const size_t smem = (size_t)row_line_stride(L) * lines * sizeof(typename CT<Real>::t);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_rows_fast<Real, L, E, INV>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((a.rows + lines - 1) / lines, a.batch > 0 ? a.batch : 1);
+    if (nblocks) *nblocks = (int)grid.x;
+    k_rows_fast<Real, L, E, INV><<<grid, lines * T, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename Real, int L, int E>
+static cudaError_t go_cols(const FastCols& a0, cudaStream_t st, int* nblocks) {
+    constexpr int T = L / E;
+    FastCols a = a0;
+    while (a.W * T < 32) a.W *= 2;
+    while (a.W > 1 && a.W * T > FMaxT<Real, E>::v) a.W /= 2;
+    const size_t smem = (size_t)col_tile_elems(L, a.W) * sizeof(typename CT<Real>::t);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_cols_fast<Real, L, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((a.ncols + a.W - 1) / a.W, a.batch > 0 ? a.batch : 1);
+    if (nblocks) *nblocks = (int)grid.x;
+    k_cols_fast<Real, L, E><<<grid, a.W * T, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+#define WOS_FAST_L(X) X(256) X(512) X(1024) X(2048) X(4096) X(8192)
+
+cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaStream_t st, int* nblocks) {
+#define CASE_R(LL)                                                                       \
+    case LL:                                                                             \
+        if (fp64) {                                                                      \
+            if (E == 8 && LL <= 4096) return inv ? go_rows<double, LL, 8, true>(a, st, nblocks) \
+                                                 : go_rows<double, LL, 8, false>(a, st, nblocks); \
+            if (E == 16 && LL >= 8192) return inv ? go_rows<double, LL, 16, true>(a, st, nblocks) \
+                                                  : go_rows<double, LL, 16, false>(a, st, nblocks); \
+        } else {                                                                         \
+            if (E == 8 && LL <= 4096) return inv ? go_rows<float, LL, 8, true>(a, st, nblocks) \
+                                                 : go_rows<float, LL, 8, false>(a, st, nblocks); \
+            if (E == 16) return inv ? go_rows<float, LL, 16, true>(a, st, nblocks)       \
+                                    : go_rows<float, LL, 16, false>(a, st, nblocks);     \
+        }                                                                                \
+        break;
+    switch (L) { WOS_FAST_L(CASE_R) }
+#undef CASE_R
+    return cudaErrorNotSupported;
+}
+
+cudaError_t fast_cols(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks) {
+#define CASE_C(LL)                                                                  \
+    case LL:                                                                        \
+        if (fp64) {                                                                 \
+            if (E == 8 && LL <= 4096) return go_cols<double, LL, 8>(a, st, nblocks); \
+            if (E == 16 && LL >= 8192) return go_cols<double, LL, 16>(a, st, nblocks); \
+        } else {                                                                    \
+            if (E == 8 && LL <= 4096) return go_cols<float, LL, 8>(a, st, nblocks); \
+            if (E == 16) return go_cols<float, LL, 16>(a, st, nblocks);             \
+        }                                                                           \
+        break;
+    switch (L) { WOS_FAST_L(CASE_C) }
+#undef CASE_C
+    return cudaErrorNotSupported;
+}
+
+bool fast_supported(int fp64, int L, int E) {
+    if (L < 256 || L > 8192 || (L & (L - 1))) return false;
+    if (fp64) return (E == 8 && L <= 4096) || (E == 16 && L >= 8192);
+    return E == 16 || (E == 8 && L <= 4096);
+}
+
+}  // namespace wos

@@ -1,0 +1,275 @@
+// wos_fft.cuh -- CTA-cooperative Stockham line FFT for sm_100a.
+//
+// A "line" is one row or one column of a field (length L, a power of two; for
+// Bluestein lines L is the padded convolution length M).  A group of T = L/E
+// threads owns a line; every thread keeps E complex values in registers.  Each
+// pass is a radix-R decimation-in-time Stockham butterfly (R = E, plus at most
+// one smaller pass), with twiddles from an FP64-generated table, and passes
+// exchange data through shared memory.  The forward radix order is
+// (rs, E, ..., E) and the inverse order is its reverse, so that the values a
+// thread holds after a forward FFT are exactly the inputs of its first inverse
+// pass (and vice versa): a fused FFT . pointwise . IFFT never round-trips
+// shared memory at the junction.
+//
+// Register mapping of a radix-R pass (the "natural" mapping):
+//   v[b*R + r] = x[j_b + r*(L/R)],  j_b = tt + b*T,  b < E/R
+// which, for the first and last pass, is also a coalesced global mapping.
+//
+// Transforms are unnormalised: forward uses exp(-2 pi i k n / L), inverse uses
+// exp(+2 pi i k n / L); 1/L factors are folded into the pointwise stages.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace wos {
+
+template <typename R> struct CT;
+template <> struct CT<float> { using t = float2; };
+template <> struct CT<double> { using t = double2; };
+
+template <typename C> __device__ __forceinline__ C mkc(decltype(C::x) a, decltype(C::x) b) { C r; r.x = a; r.y = b; return r; }
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mkc<C>(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mkc<C>(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+    return mkc<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename C> __device__ __forceinline__ C cmulc(C a, C b) {  // a * conj(b)
+    return mkc<C>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+template <typename C> __device__ __forceinline__ C cscale(C a, decltype(C::x) s) { return mkc<C>(a.x * s, a.y * s); }
+template <typename C> __device__ __forceinline__ C cconj(C a) { return mkc<C>(a.x, -a.y); }
+// multiply by -i (forward) or +i (inverse)
+template <bool INV, typename C> __device__ __forceinline__ C mul_mi(C a) {
+    return INV ? mkc<C>(-a.y, a.x) : mkc<C>(a.y, -a.x);
+}
+
+template <typename C> __device__ __forceinline__ C ldg_c(const C* p) { return __ldg(p); }
+
+// ---------------------------------------------------------------- small DFTs
+template <bool INV, typename C>
+__device__ __forceinline__ void dft2(C& a, C& b) {
+    C t = a;
+    a = cadd(t, b);
+    b = csub(t, b);
+}
+
+template <bool INV, typename C>
+__device__ __forceinline__ void dft4(C& v0, C& v1, C& v2, C& v3) {
+    C a0 = cadd(v0, v2), a1 = csub(v0, v2);
+    C a2 = cadd(v1, v3), a3 = mul_mi<INV>(csub(v1, v3));
+    v0 = cadd(a0, a2);
+    v2 = csub(a0, a2);
+    v1 = cadd(a1, a3);
+    v3 = csub(a1, a3);
+}
+
+template <typename C> struct K;
+template <> struct K<float2> {
+    static constexpr float S2 = 0.70710678118654752440f;
+    static constexpr float C8 = 0.92387953251128675613f;
+    static constexpr float S8 = 0.38268343236508977173f;
+};
+template <> struct K<double2> {
+    static constexpr double S2 = 0.70710678118654752440;
+    static constexpr double C8 = 0.92387953251128675613;
+    static constexpr double S8 = 0.38268343236508977173;
+};
+
+// w8^k * x for k = 1, 3 (forward: w = exp(-i pi/4))
+template <bool INV, typename C> __device__ __forceinline__ C w8_1(C x) {
+    const auto s = K<C>::S2;
+    return INV ? mkc<C>((x.x - x.y) * s, (x.x + x.y) * s) : mkc<C>((x.x + x.y) * s, (x.y - x.x) * s);
+}
+template <bool INV, typename C> __device__ __forceinline__ C w8_3(C x) {
+    const auto s = K<C>::S2;
+    return INV ? mkc<C>(-(x.x + x.y) * s, (x.x - x.y) * s) : mkc<C>((x.y - x.x) * s, -(x.x + x.y) * s);
+}
+
+template <bool INV, typename C>
+__device__ __forceinline__ void dft8(C* v) {
+    // even / odd radix-4 then combine
+    C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4<INV>(e0, e1, e2, e3);
+    dft4<INV>(o0, o1, o2, o3);
+    o1 = w8_1<INV>(o1);
+    o2 = mul_mi<INV>(o2);
+    o3 = w8_3<INV>(o3);
+    v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+    v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+    v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+    v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+}
+
+// multiply by w16^k (forward w16 = exp(-2 pi i/16)), k = 0..7
+template <int k, bool INV, typename C>
+__device__ __forceinline__ C w16(C x) {
+    using T = decltype(C::x);
+    if (k == 0) return x;
+    if (k == 4) return mul_mi<INV>(x);
+    if (k == 2) return w8_1<INV>(x);
+    if (k == 6) return w8_3<INV>(x);
+    T c, s;  // w = c - i s (forward)
+    if (k == 1) { c = K<C>::C8; s = K<C>::S8; }
+    else if (k == 3) { c = K<C>::S8; s = K<C>::C8; }
+    else if (k == 5) { c = -K<C>::S8; s = K<C>::C8; }
+    else { c = -K<C>::C8; s = K<C>::S8; }  // k == 7
+    if (INV) s = -s;
+    return mkc<C>(x.x * c + x.y * s, x.y * c - x.x * s);
+}
+
+template <bool INV, typename C>
+__device__ __forceinline__ void dft16(C* v) {
+    C e[8], o[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) { e[i] = v[2 * i]; o[i] = v[2 * i + 1]; }
+    dft8<INV>(e);
+    dft8<INV>(o);
+    o[1] = w16<1, INV>(o[1]); o[2] = w16<2, INV>(o[2]); o[3] = w16<3, INV>(o[3]);
+    o[4] = w16<4, INV>(o[4]); o[5] = w16<5, INV>(o[5]); o[6] = w16<6, INV>(o[6]);
+    o[7] = w16<7, INV>(o[7]);
+#pragma unroll
+    for (int i = 0; i < 8; i++) { v[i] = cadd(e[i], o[i]); v[i + 8] = csub(e[i], o[i]); }
+}
+
+template <int R, bool INV, typename C>
+__device__ __forceinline__ void dft(C* v) {
+    if (R == 2) dft2<INV>(v[0], v[1]);
+    else if (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
+    else if (R == 8) dft8<INV>(v);
+    else if (R == 16) dft16<INV>(v);
+}
+
+// ------------------------------------------------------------- shared layouts
+// Line-contiguous layout (rows): line l at l*S, one pad slot per 16 elements.
+struct RowIdx {
+    int S;
+    __device__ __forceinline__ int operator()(int line, int p) const { return line * S + p + (p >> 4); }
+};
+__host__ __device__ inline int row_line_stride(int L) { return L + (L >> 4) + 1; }
+
+// Interleaved layout (columns): element (line w, position p) at p*W + w, padded.
+struct ColIdx {
+    int W;
+    __device__ __forceinline__ int operator()(int line, int p) const {
+        int i = p * W + line;
+        return i + (i >> 4);
+    }
+};
+__host__ __device__ inline int col_tile_elems(int L, int W) { int n = L * W; return n + (n >> 4) + 1; }
+
+// ------------------------------------------------------------- pass pieces
+template <int R, int E, bool INV, typename C>
+__device__ __forceinline__ void pass_compute(C* v, int tt, int T, int Ns, int L, const C* __restrict__ tw) {
+#pragma unroll
+    for (int b = 0; b < E / R; b++) {
+        if (Ns > 1) {
+            const int j = tt + b * T;
+            const int k = j & (Ns - 1);
+            const int step = L / (Ns * R);
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                C w = ldg_c(tw + r * k * step);
+                if (INV) w.y = -w.y;
+                v[b * R + r] = cmul(v[b * R + r], w);
+            }
+        }
+        dft<R, INV>(v + b * R);
+    }
+}
+
+template <int R, int E, typename C, typename IDX>
+__device__ __forceinline__ void sm_store(const C* v, C* sm, const IDX& ix, int line, int tt, int T, int Ns) {
+#pragma unroll
+    for (int b = 0; b < E / R; b++) {
+        const int j = tt + b * T;
+        const int k = j & (Ns - 1);
+        const int base = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) sm[ix(line, base + r * Ns)] = v[b * R + r];
+    }
+}
+
+template <int R, int E, typename C, typename IDX>
+__device__ __forceinline__ void sm_load(C* v, const C* sm, const IDX& ix, int line, int tt, int T, int L) {
+    const int LR = L / R;
+#pragma unroll
+    for (int b = 0; b < E / R; b++) {
+        const int j = tt + b * T;
+#pragma unroll
+        for (int r = 0; r < R; r++) v[b * R + r] = sm[ix(line, j + r * LR)];
+    }
+}
+
+// Runtime radix dispatch helpers (R <= E, both powers of two).
+#define WOS_DISPATCH_R(R_, E_, BODY)                    \
+    do {                                                \
+        switch (R_) {                                   \
+        case 2: { constexpr int RR = 2; BODY; } break;  \
+        case 4: { constexpr int RR = 4; BODY; } break;  \
+        case 8: { constexpr int RR = 8; BODY; } break;  \
+        default: { constexpr int RR = 16; BODY; } break; \
+        }                                               \
+    } while (0)
+
+// Radix of pass p of a P-pass transform: forward (rs, E, ..., E), inverse reversed.
+__device__ __forceinline__ int pass_radix(bool inv, int p, int P, int rs, int E) {
+    if (rs > 1) {
+        if (!inv && p == 0) return rs;
+        if (inv && p == P - 1) return rs;
+    }
+    return E;
+}
+
+// Plan of a line transform: number of passes and the small radix.
+struct LinePlan {
+    int L;    // length (power of two)
+    int P;    // passes
+    int rs;   // small radix (1 if none)
+};
+__host__ __device__ inline LinePlan make_line_plan(int L, int E) {
+    int lg = 0;
+    while ((1 << lg) < L) lg++;
+    int le = 0;
+    while ((1 << le) < E) le++;
+    LinePlan p;
+    p.L = L;
+    p.P = lg / le + ((lg % le) ? 1 : 0);
+    p.rs = (lg % le) ? (1 << (lg % le)) : 1;
+    return p;
+}
+__host__ __device__ inline int first_radix(const LinePlan& lp, bool inv, int E) {
+    return (!inv && lp.rs > 1) ? lp.rs : E;
+}
+__host__ __device__ inline int last_radix(const LinePlan& lp, bool inv, int E) {
+    return (inv && lp.rs > 1) ? lp.rs : E;
+}
+
+// Full line transform.  On entry v holds the natural mapping for the first
+// pass radix; on exit v holds the natural mapping for the last pass radix.
+// Must be called by every thread of the CTA (it synchronises).
+template <int E, bool INV, typename C, typename IDX>
+__device__ __forceinline__ void line_fft(C* v, C* sm, const IDX& ix, int line, int tt, int T,
+                                         const LinePlan& lp, const C* __restrict__ tw) {
+    int Ns = 1;
+    for (int p = 0; p < lp.P; p++) {
+        const int R = pass_radix(INV, p, lp.P, lp.rs, E);
+        WOS_DISPATCH_R(R, E, (pass_compute<RR, E, INV>(v, tt, T, Ns, lp.L, tw)));
+        if (p < lp.P - 1) {
+            const int R2 = pass_radix(INV, p + 1, lp.P, lp.rs, E);
+            __syncthreads();
+            WOS_DISPATCH_R(R, E, (sm_store<RR, E>(v, sm, ix, line, tt, T, Ns)));
+            __syncthreads();
+            WOS_DISPATCH_R(R2, E, (sm_load<RR, E>(v, sm, ix, line, tt, T, lp.L)));
+        }
+        Ns *= R;
+    }
+}
+
+// Position held by register slot s (= b*R + r) under the natural mapping of radix R.
+__device__ __forceinline__ int nat_pos(int s, int R, int tt, int T, int L) {
+    const int b = s / R, r = s % R;
+    return tt + b * T + r * (L / R);
+}
+
+}  // namespace wos

@@ -1,0 +1,462 @@
+"""ctypes binding of libwosgpu.so (include/wos_gpu.h) and a host mirror of the
+reference `optics` interface for the propagation hot path.
+
+The names follow the Go package: Context (optics/field.go:237-254), Field
+(optics/field.go:14-22), propagate (optics/propagate.go:65-102),
+propagate_split_step (optics/medium.go:22-45), propagate_polychromatic
+(optics/polychromatic.go:18-44), propagate_3d (optics/volume.go:8-18),
+generate_schell_realizations / propagate_partially_coherent
+(optics/coherence.go:22-116).  Errors raise WosError; there is no CPU path:
+if the shared library or a CUDA device is missing, calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field as dfield
+from typing import Dict, Optional, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libwosgpu.so")
+
+METHODS = {"asm": 1, "auto": 1, "": 1, "asm_pad": 2, "asm_shift": 3, "asm_shift_pad": 4,
+           "fresnel_tf": 5, "fresnel_ir": 6, "fraunhofer": 7}
+FP64, FP32 = 0, 1
+WARN_CODES = ["evanescent_filtered", "backward_regularized", "backward_evanescent",
+              "asm_alias_wrap", "fresnel_tf_alias", "fresnel_ir_alias", "fraunhofer_nearfield"]
+GRATING_KINDS = {"amplitude_sin": 0, "amplitude_binary": 1, "phase_sin": 2, "phase_binary": 3,
+                 "blazed": 4}
+
+# Every entry point of include/wos_gpu.h.
+EXPORTS = [
+    "wos_device_count", "wos_device_name", "wos_ctx_create", "wos_ctx_destroy",
+    "wos_ctx_set_stream", "wos_ctx_get_stream", "wos_ctx_precision", "wos_ctx_set_col_width",
+    "wos_ctx_synchronize", "wos_ctx_set_profiling", "wos_ctx_profile", "wos_ctx_profile_reset",
+    "wos_ctx_launch_count", "wos_ctx_set_fast_path", "wos_autotune", "wos_ctx_set_tune", "wos_status_string", "wos_last_error", "wos_backend_info",
+    "wos_fft2d", "wos_fft1d", "wos_fft2d_dev", "wos_propagate", "wos_propagate_dev",
+    "wos_propagate_dev_c128", "wos_splitstep", "wos_splitstep_dev", "wos_splitstep_maps",
+    "wos_polychromatic", "wos_volume", "wos_schell_modes", "wos_partially_coherent",
+    "wos_apply_lens", "wos_apply_aperture_circle", "wos_apply_grating", "wos_apply_phase_mask",
+    "wos_asm_forward_loss", "wos_asm_loss_grad", "wos_asm_adjoint",
+]
+
+
+class WosError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"wos status {status}: {msg}")
+        self.status = status
+
+
+class CContext(C.Structure):
+    _fields_ = [("wavelength", C.c_double), ("evanescent_zero", C.c_int),
+                ("evanescent_limit", C.c_double), ("backward_regularize", C.c_int),
+                ("tikhonov_alpha", C.c_double), ("diagnostics", C.c_int)]
+
+
+class CDiag(C.Structure):
+    _fields_ = [("p_in", C.c_double), ("p_out", C.c_double), ("centroid_fx", C.c_double),
+                ("centroid_fy", C.c_double), ("carrier_applied", C.c_int),
+                ("wrap_checked", C.c_int), ("spectral_radius", C.c_double),
+                ("rms_radius_in", C.c_double), ("dx_out", C.c_double),
+                ("warn_count", C.c_int * 7), ("warn_value", C.c_double * 7)]
+
+
+class CField(C.Structure):
+    _fields_ = [("ny", C.c_int), ("nx", C.c_int), ("dx", C.c_double), ("polarized", C.c_int),
+                ("ex", C.c_void_p), ("ey", C.c_void_p)]
+
+
+class IndexDesc(C.Structure):
+    """wos_index_desc: parametric n(x,y,z) of a split-step medium."""
+    _fields_ = [
+        ("re_bg", C.c_double), ("im_bg", C.c_double),
+        ("core_dn", C.c_double), ("core_x0", C.c_double), ("core_y0", C.c_double),
+        ("core_w", C.c_double), ("zmod_amp", C.c_double), ("zmod_period", C.c_double),
+        ("zmod_phase", C.c_double), ("border_px", C.c_int), ("border_order", C.c_int),
+        ("border_strength", C.c_double), ("n_layers", C.c_int),
+        ("layer_z", C.c_double * 8), ("layer_re", C.c_double * 8), ("layer_im", C.c_double * 8),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load libwosgpu.so; raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise WosError(6, f"{LIB_PATH} is missing: run tetsuhiro-wos_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        vp, i, d = C.c_void_p, C.c_int, C.c_double
+        P = C.POINTER
+        sig = {
+            "wos_device_count": ([], i), "wos_device_name": ([i, C.c_char_p, i], i),
+            "wos_ctx_create": ([i, i, P(vp)], i), "wos_ctx_destroy": ([vp], i),
+            "wos_ctx_set_stream": ([vp, vp], i), "wos_ctx_get_stream": ([vp], vp),
+            "wos_ctx_precision": ([vp], i), "wos_ctx_set_col_width": ([vp, i], i),
+            "wos_ctx_synchronize": ([vp], i), "wos_status_string": ([i], C.c_char_p),
+            "wos_ctx_set_profiling": ([vp, i], i),
+            "wos_ctx_profile": ([vp, i, P(d), P(C.c_longlong)], i),
+            "wos_ctx_profile_reset": ([vp], i), "wos_ctx_launch_count": ([vp], C.c_longlong),
+            "wos_ctx_set_fast_path": ([vp, i], i),
+            "wos_autotune": ([vp, i, i, P(i), P(i), P(i)], i),
+            "wos_ctx_set_tune": ([vp, i, i, i, i, i], i),
+            "wos_last_error": ([], C.c_char_p), "wos_backend_info": ([], C.c_char_p),
+            "wos_fft2d": ([vp, i, i, vp, i], i), "wos_fft1d": ([vp, i, vp, i], i),
+            "wos_fft2d_dev": ([vp, i, i, i, vp, i], i),
+            "wos_propagate": ([vp, vp, d, i, vp, vp], i),
+            "wos_propagate_dev": ([vp, i, i, d, i, vp, vp, d, i, vp, vp], i),
+            "wos_propagate_dev_c128": ([vp, i, i, d, i, vp, vp, d, i, vp, vp], i),
+            "wos_splitstep": ([vp, vp, d, vp, i, vp, vp], i),
+            "wos_splitstep_dev": ([vp, i, i, d, i, vp, d, vp, i, vp, vp], i),
+            "wos_splitstep_maps": ([vp, vp, d, vp, vp, i, i, vp, vp], i),
+            "wos_polychromatic": ([vp, vp, d, vp, vp, i, i, vp, vp, vp], i),
+            "wos_volume": ([vp, vp, vp, i, i, vp, vp, vp], i),
+            "wos_schell_modes": ([vp, i, d, d, d, i, vp, vp], i),
+            "wos_partially_coherent": ([vp, i, d, d, d, i, vp, d, i, vp, vp, vp], i),
+            "wos_apply_lens": ([vp, vp, d, d, d, d, d], i),
+            "wos_apply_aperture_circle": ([vp, vp, d, d, d, d], i),
+            "wos_apply_grating": ([vp, vp, i, d, d, d, d, d, d], i),
+            "wos_apply_phase_mask": ([vp, vp, vp, d], i),
+            "wos_asm_forward_loss": ([vp, i, i, d, d, vp, vp, vp, vp, vp], i),
+            "wos_asm_loss_grad": ([vp, i, i, d, d, vp, vp, vp, vp, vp, vp], i),
+            "wos_asm_adjoint": ([vp, vp, d, vp], i),
+        }
+        for name, (args, res) in sig.items():
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise WosError(rc, lib().wos_last_error().decode(errors="replace"))
+
+
+def _ptr(a: np.ndarray):
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def device_count() -> int:
+    return lib().wos_device_count()
+
+
+def backend_info() -> str:
+    """GPUBackendInfo (optics/gpu.go:139-143)."""
+    return lib().wos_backend_info().decode()
+
+
+@dataclass
+class Context:
+    """optics.Context (field.go:237-254) with its Warnings list (code -> (count, value))."""
+    wavelength: float
+    evanescent: str = "decay"
+    evanescent_limit: float = 0.0
+    backward_regularize: bool = False
+    tikhonov_alpha: float = 0.0
+    warnings_enabled: bool = True
+    warnings: Dict[str, Tuple[int, float]] = dfield(default_factory=dict)
+
+    def c(self) -> CContext:
+        cc = CContext()
+        cc.wavelength = self.wavelength
+        cc.evanescent_zero = 1 if self.evanescent == "zero" else 0
+        cc.evanescent_limit = self.evanescent_limit
+        cc.backward_regularize = 1 if self.backward_regularize else 0
+        cc.tikhonov_alpha = self.tikhonov_alpha
+        cc.diagnostics = 1 if self.warnings_enabled else 0
+        return cc
+
+    def absorb(self, d: CDiag) -> None:
+        """Warnings.Add for every warning the call raised (field.go:322-338)."""
+        if not self.warnings_enabled:
+            return
+        for b, code in enumerate(WARN_CODES):
+            n = d.warn_count[b]
+            if n <= 0:
+                continue
+            cnt, val = self.warnings.get(code, (0, 0.0))
+            v = d.warn_value[b]
+            self.warnings[code] = (cnt + n, v if v != 0 else val)
+
+
+class Field:
+    """optics.Field (field.go:14-22): ex/ey complex128 (ny, nx), row-major."""
+
+    def __init__(self, ex: np.ndarray, dx: float, ey: Optional[np.ndarray] = None):
+        self.ex = np.ascontiguousarray(ex, dtype=np.complex128)
+        self.ny, self.nx = self.ex.shape
+        self.dx = float(dx)
+        self.polarized = ey is not None
+        self.ey = (np.ascontiguousarray(ey, dtype=np.complex128) if ey is not None
+                   else np.zeros_like(self.ex))
+
+    def clone(self) -> "Field":
+        return Field(self.ex.copy(), self.dx, self.ey.copy() if self.polarized else None)
+
+    def c(self) -> CField:
+        f = CField()
+        f.ny, f.nx, f.dx, f.polarized = self.ny, self.nx, self.dx, int(self.polarized)
+        f.ex, f.ey = _ptr(self.ex), _ptr(self.ey)
+        return f
+
+    def x(self, i):
+        """X (field.go:59): centred column coordinate."""
+        return (np.asarray(i, dtype=np.float64) - self.nx / 2) * self.dx
+
+    def y(self, j):
+        """Y (field.go:62): centred row coordinate."""
+        return (np.asarray(j, dtype=np.float64) - self.ny / 2) * self.dx
+
+    def intensity(self) -> np.ndarray:
+        p = np.abs(self.ex) ** 2
+        if self.polarized:
+            p = p + np.abs(self.ey) ** 2
+        return p
+
+    def power(self) -> float:
+        return float(self.intensity().sum() * self.dx * self.dx)
+
+
+class GPU:
+    """One wos_ctx: a device, a precision (FP32 / FP64) and a CUDA stream."""
+
+    def __init__(self, precision: int = FP32, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().wos_ctx_create(device, precision, C.byref(h)))
+        self.h = h
+        self.precision = precision
+
+    def close(self) -> None:
+        if self.h:
+            lib().wos_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return lib().wos_ctx_get_stream(self.h) or 0
+
+    def set_stream(self, stream_ptr: int) -> None:
+        _check(lib().wos_ctx_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def set_col_width(self, w: int) -> None:
+        _check(lib().wos_ctx_set_col_width(self.h, w))
+
+    def synchronize(self) -> None:
+        _check(lib().wos_ctx_synchronize(self.h))
+
+    PROFILE_KINDS = ["row_fwd", "row_inv", "row_inv_screen_fwd", "row_inv_accumulate",
+                     "col_fused", "col_fraunhofer", "col_reduce", "col_fft"]
+
+    def set_profiling(self, on: bool) -> None:
+        _check(lib().wos_ctx_set_profiling(self.h, int(on)))
+
+    def profile(self) -> dict:
+        """{kind: (total_ms, launches)} of the per-launch CUDA-event profile."""
+        out = {}
+        for k, name in enumerate(self.PROFILE_KINDS):
+            ms, n = C.c_double(), C.c_longlong()
+            _check(lib().wos_ctx_profile(self.h, k, C.byref(ms), C.byref(n)))
+            if n.value:
+                out[name] = (ms.value, n.value)
+        return out
+
+    def profile_reset(self) -> None:
+        _check(lib().wos_ctx_profile_reset(self.h))
+
+    def launch_count(self) -> int:
+        return int(lib().wos_ctx_launch_count(self.h))
+
+    # ---- fft2D / fft1DAny users
+    def fft2d(self, a: np.ndarray, inverse: bool = False) -> np.ndarray:
+        a = np.ascontiguousarray(a, dtype=np.complex128).copy()
+        _check(lib().wos_fft2d(self.h, a.shape[0], a.shape[1], _ptr(a), int(inverse)))
+        return a
+
+    def fft1d(self, a: np.ndarray, inverse: bool = False) -> np.ndarray:
+        a = np.ascontiguousarray(a, dtype=np.complex128).copy()
+        _check(lib().wos_fft1d(self.h, a.size, _ptr(a), int(inverse)))
+        return a
+
+    def fft2d_dev(self, ptr: int, ny: int, nx: int, batch: int = 1, inverse: bool = False) -> None:
+        _check(lib().wos_fft2d_dev(self.h, ny, nx, batch, C.c_void_p(ptr), int(inverse)))
+
+    # ---- Propagate
+    def propagate(self, f: Field, z: float, method: str = "asm", ctx: Optional[Context] = None) -> CDiag:
+        """optics.Propagate on a host field, in place (propagate.go:65-102)."""
+        d = CDiag()
+        cf = f.c()
+        if method not in METHODS:
+            raise WosError(7, f"unknown propagation method {method!r}")
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_propagate(self.h, C.byref(cf), z, METHODS[method],
+                                   C.byref(cc) if cc is not None else None, C.byref(d)))
+        if method == "fraunhofer" and z != 0:
+            f.dx = d.dx_out
+        if ctx is not None:
+            ctx.absorb(d)
+        return d
+
+    def propagate_dev(self, ny: int, nx: int, dx: float, ncomp: int, in_ptr: int, out_ptr: int, z: float,
+                      method: str, ctx: Optional[Context], diag: bool = False, c128: bool = False):
+        d = CDiag() if diag else None
+        cc = ctx.c() if ctx is not None else None
+        fn = lib().wos_propagate_dev_c128 if c128 else lib().wos_propagate_dev
+        _check(fn(self.h, ny, nx, dx, ncomp, C.c_void_p(in_ptr), C.c_void_p(out_ptr), z, METHODS[method],
+                  C.byref(cc) if cc is not None else None, C.byref(d) if d is not None else None))
+        if d is not None and ctx is not None:
+            ctx.absorb(d)
+        return d
+
+    # ---- PropagateSplitStep
+    def split_step(self, f: Field, z: float, desc: IndexDesc, steps: int, ctx: Optional[Context]) -> CDiag:
+        d = CDiag()
+        cf = f.c()
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_splitstep(self.h, C.byref(cf), z, C.byref(desc), steps,
+                                   C.byref(cc) if cc is not None else None, C.byref(d)))
+        if ctx is not None:
+            ctx.absorb(d)
+        return d
+
+    def split_step_maps(self, f: Field, z: float, n_re: np.ndarray, n_im: np.ndarray, steps: int,
+                        ctx: Optional[Context]) -> CDiag:
+        n_re = np.ascontiguousarray(n_re, dtype=np.float64)
+        n_im = np.ascontiguousarray(n_im, dtype=np.float64)
+        nmaps = 1 if n_re.ndim == 2 else n_re.shape[0]
+        d = CDiag()
+        cf = f.c()
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_splitstep_maps(self.h, C.byref(cf), z, _ptr(n_re), _ptr(n_im), nmaps, steps,
+                                        C.byref(cc) if cc is not None else None, C.byref(d)))
+        if ctx is not None:
+            ctx.absorb(d)
+        return d
+
+    def split_step_dev(self, ny, nx, dx, ncomp, ptr, z, desc, steps, ctx, diag=False):
+        d = CDiag() if diag else None
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_splitstep_dev(self.h, ny, nx, dx, ncomp, C.c_void_p(ptr), z, C.byref(desc), steps,
+                                       C.byref(cc) if cc is not None else None,
+                                       C.byref(d) if d is not None else None))
+        return d
+
+    # ---- batches (warnings of every unit accumulate into ctx, like the shared ctx.Warnings)
+    def polychromatic(self, f: Field, z: float, wavelengths, weights, method: str = "asm",
+                      ctx: Optional[Context] = None) -> np.ndarray:
+        """PropagatePolychromatic (polychromatic.go:18-44)."""
+        wl = np.ascontiguousarray(wavelengths, dtype=np.float64)
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        out = np.zeros((f.ny, f.nx))
+        d = CDiag()
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_polychromatic(self.h, C.byref(f.c()), z, _ptr(wl), _ptr(w), wl.size, METHODS[method],
+                                       C.byref(cc) if cc is not None else None, _ptr(out), C.byref(d)))
+        if ctx is not None:
+            ctx.absorb(d)
+        return out
+
+    def volume(self, f: Field, zs, method: str = "asm", ctx: Optional[Context] = None) -> np.ndarray:
+        """Propagate3D (volume.go:8-18): (nz, ncomp, ny, nx) complex128."""
+        zz = np.ascontiguousarray(zs, dtype=np.float64)
+        ncomp = 2 if f.polarized else 1
+        out = np.zeros((zz.size, ncomp, f.ny, f.nx), dtype=np.complex128)
+        d = CDiag()
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_volume(self.h, C.byref(f.c()), _ptr(zz), zz.size, METHODS[method],
+                                C.byref(cc) if cc is not None else None, _ptr(out), C.byref(d)))
+        if ctx is not None:
+            ctx.absorb(d)
+        return out
+
+    def schell_modes(self, n: int, dx: float, width: float, coherence: float, noise: np.ndarray) -> np.ndarray:
+        """GenerateSchellRealizations (coherence.go:22-80) with caller noise."""
+        noise = np.ascontiguousarray(noise, dtype=np.complex128)
+        m = noise.shape[0]
+        out = np.zeros((m, n, n), dtype=np.complex128)
+        _check(lib().wos_schell_modes(self.h, n, dx, width, coherence, m, _ptr(noise), _ptr(out)))
+        return out
+
+    def partially_coherent(self, n: int, dx: float, width: float, coherence: float, noise: np.ndarray,
+                           z: float, method: str = "asm", ctx: Optional[Context] = None) -> np.ndarray:
+        """PropagatePartiallyCoherent (coherence.go:105-116)."""
+        noise = np.ascontiguousarray(noise, dtype=np.complex128)
+        m = noise.shape[0]
+        out = np.zeros((n, n))
+        d = CDiag()
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_partially_coherent(self.h, n, dx, width, coherence, m, _ptr(noise), z, METHODS[method],
+                                            C.byref(cc) if cc is not None else None, _ptr(out), C.byref(d)))
+        if ctx is not None:
+            ctx.absorb(d)
+        return out
+
+    # ---- launch configuration
+    def set_fast_path(self, on: bool) -> None:
+        _check(lib().wos_ctx_set_fast_path(self.h, int(on)))
+
+    def autotune(self, ny: int, nx: int) -> tuple:
+        r, c, w = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().wos_autotune(self.h, ny, nx, C.byref(r), C.byref(c), C.byref(w)))
+        return r.value, c.value, w.value
+
+    def set_tune(self, ny: int, nx: int, row_e: int, col_e: int, col_w: int) -> None:
+        _check(lib().wos_ctx_set_tune(self.h, ny, nx, row_e, col_e, col_w))
+
+    # ---- thin elements
+    def apply_lens(self, f: Field, wl, focal, aperture=0.0, x0=0.0, y0=0.0):
+        _check(lib().wos_apply_lens(self.h, C.byref(f.c()), wl, focal, aperture, x0, y0))
+
+    def apply_aperture_circle(self, f: Field, radius, x0=0.0, y0=0.0, edge_sigma=0.0):
+        _check(lib().wos_apply_aperture_circle(self.h, C.byref(f.c()), radius, x0, y0, edge_sigma))
+
+    def apply_grating(self, f: Field, kind, period, modulation=1.0, duty=0.5, blaze_depth=np.pi,
+                      rotation=0.0, offset=0.0):
+        _check(lib().wos_apply_grating(self.h, C.byref(f.c()), GRATING_KINDS[kind], period, modulation, duty,
+                                       blaze_depth, rotation, offset))
+
+    def apply_phase_mask(self, f: Field, phi: np.ndarray, amp=1.0):
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        _check(lib().wos_apply_phase_mask(self.h, C.byref(f.c()), _ptr(phi), amp))
+
+    # ---- inverse design
+    def asm_loss_grad(self, a: np.ndarray, phi: np.ndarray, target: np.ndarray, dx: float, z: float,
+                      ctx: Context, want_grad: bool = True):
+        a = np.ascontiguousarray(a, dtype=np.complex128)
+        phi = np.ascontiguousarray(phi, dtype=np.float64)
+        target = np.ascontiguousarray(target, dtype=np.float64)
+        ny, nx = a.shape
+        loss = C.c_double()
+        cc = ctx.c()
+        if want_grad:
+            grad = np.zeros((ny, nx))
+            _check(lib().wos_asm_loss_grad(self.h, ny, nx, dx, z, C.byref(cc), _ptr(a), _ptr(phi), _ptr(target),
+                                           C.byref(loss), _ptr(grad)))
+            return loss.value, grad
+        _check(lib().wos_asm_forward_loss(self.h, ny, nx, dx, z, C.byref(cc), _ptr(a), _ptr(phi), _ptr(target),
+                                          C.byref(loss)))
+        return loss.value, None
+
+    def asm_adjoint(self, f: Field, z: float, ctx: Context) -> None:
+        cc = ctx.c()
+        _check(lib().wos_asm_adjoint(self.h, C.byref(f.c()), z, C.byref(cc)))
