@@ -236,6 +236,9 @@ def main() -> None:
     g64 = wos.GPU(wos.FP64, device=local)
     g64.set_stream(stream.cuda_stream)
     ctx = wos.Context(wavelength=WL, warnings_enabled=False)
+    # launch configuration of the specialised sweeps: timed on this device
+    tune32 = g32.autotune(N, N)
+    tune64 = g64.autotune(N, N)
 
     ex = input_field()
     with torch.cuda.stream(stream):
@@ -343,7 +346,10 @@ def main() -> None:
         line = {"metric": METRIC, "value": value, "unit": "props/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": workload_config(args.batch), "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+                "config": dict(workload_config(args.batch),
+                               autotune={"fp32": {"row_e": tune32[0], "col_e": tune32[1], "col_w": tune32[2]},
+                                         "fp64": {"row_e": tune64[0], "col_e": tune64[1], "col_w": tune64[2]}}),
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clk,
                 "fp64": {"value": fp64_rate, "unit": "props/s", "dtype": "f64",
                          "fp32_speedup": value / world / fp64_rate},

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from gpu_util import rel_l2, tol, wos
+from gpu_util import TOL_FP64_SCHELL, rel_l2, tol, tol_case, wos
 from wos_testutil import complex_normal, waist_radius
 
 pytestmark = pytest.mark.gpu
@@ -173,7 +173,7 @@ def test_volume_matches_oracle(gpu, method):
     out = gpu.volume(wos.Field(ex.copy(), dx), zs, method, wos.Context(wavelength=wl))
     assert np.array_equal(out[0, 0], ex)   # z == 0 returns the input unchanged
     for q in range(len(zs)):
-        assert rel_l2(out[q], ref[q]) <= tol(gpu.precision), q
+        assert rel_l2(out[q], ref[q]) <= tol_case(gpu.precision, method, n, n), q
 
 
 # ------------------------------------------------------------------ Schell
@@ -182,7 +182,7 @@ def test_schell_modes_match_oracle(gpu):
     noise = complex_normal(3, (m, n, n))
     ref = O.schell_realizations(n, dx, w0, sigc, noise)
     got = gpu.schell_modes(n, dx, w0, sigc, noise)
-    assert rel_l2(got, ref) <= 1e-12   # synthesis runs in FP64 in both precisions
+    assert rel_l2(got, ref) <= TOL_FP64_SCHELL   # synthesis runs in FP64 in both precisions
 
 
 def test_schell_source_coherence_kat(gpu):
@@ -209,7 +209,7 @@ def test_partially_coherent_matches_oracle(gpu, method):
         outs.append(f.ex)
     ref = O.average_intensity(np.array(outs))
     got = gpu.partially_coherent(n, dx, w0, sigc, noise, z, method, wos.Context(wavelength=wl))
-    assert rel_l2(got, ref) <= tol(gpu.precision)
+    assert rel_l2(got, ref) <= max(tol(gpu.precision), TOL_FP64_SCHELL)
 
 
 # ---------------------------------------------------------------- elements

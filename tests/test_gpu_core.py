@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from gpu_util import TOL_FP32, TOL_FP64, rel_l2, tol, wos
+from gpu_util import TOL_FP32, TOL_FP64, rel_l2, tol, tol_case, wos
 from wos_testutil import (SimpleRNG, analytic_gaussian_fresnel, centroid_x, ref_field,
                           single_bin_plane_wave)
 
@@ -153,7 +153,7 @@ def test_propagate_matches_oracle(gpu, method, case, polarized):
     gf = wos.Field(ex.copy(), dx, None if ey is None else ey.copy())
     gc = wos.Context(wavelength=wl)
     gpu.propagate(gf, z, method, gc)
-    t = tol(gpu.precision)
+    t = tol_case(gpu.precision, method, ny, nx)
     err = rel_l2(gf.ex, of.ex)
     assert err <= t, (err, gc.warnings, oc.warnings)
     if polarized:

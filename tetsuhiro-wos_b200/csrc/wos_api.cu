@@ -80,6 +80,7 @@ struct Axis {
     void* chirp = nullptr;
     void* bf = nullptr;
     void* bi = nullptr;
+    void* ftw[2] = {nullptr, nullptr};  // per-pass twiddles of the specialised sweeps (E = 8, 16)
 };
 
 constexpr int kMaxL32 = 8192;  // largest line held on chip (threads x elements)
@@ -548,6 +549,18 @@ size_t fast_col_blocks(int fp64, int L, int E, int W, int ncols, int batch) {
     return (size_t)((ncols + W - 1) / W) * std::max(batch, 1);
 }
 
+// Per-pass twiddle table of the specialised sweeps for a power-of-two axis.
+int fast_tw(wos_ctx c, Axis* a, int E, const void** out) {
+    const int slot = E == 16 ? 1 : 0;
+    if (!a->ftw[slot]) {
+        const size_t bytes = (size_t)fast_table_len(a->L, E) * c->csz();
+        CK(cudaMalloc(&a->ftw[slot], bytes));
+        CK(fast_build_twiddles(c->fp64, a->L, E, a->ftw[slot], c->st));
+    }
+    *out = a->ftw[slot];
+    return WOS_OK;
+}
+
 // Plain band-limited ASM on power-of-two grids through the specialised
 // sweeps.  Returns -1 when the grid is not covered (the general sweeps run).
 int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
@@ -557,6 +570,9 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     Axis *ax, *ay;
     TRY(get_axis(c, p.nx, c->fp64, &ax));
     TRY(get_axis(c, p.ny, c->fp64, &ay));
+    const void *twx, *twy;
+    TRY(fast_tw(c, ax, t.rowE, &twx));
+    TRY(fast_tw(c, ay, t.colE, &twy));
     const long long np = (long long)p.ny * p.nx;
     void* S;
     if (!p.out_c128) {
@@ -578,7 +594,7 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     r.out = S;
     r.out_ld = p.nx;
     r.out_bstride = np;
-    r.tw = ax->tw;
+    r.tw = twx;
     r.out_scale = 1.0;
     r.red = s.red_pin ? red_region(c, 0) + RS_P : nullptr;
     r.red_stride = RS_COUNT;
@@ -591,7 +607,7 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     k.data = S;
     k.ld = p.nx;
     k.bstride = np;
-    k.tw = ay->tw;
+    k.tw = twy;
     k.batch = p.ncomp;
     k.wl = s.h.wl;
     k.dx = s.h.dx;
@@ -617,7 +633,7 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     q.out_c128 = p.out_c128;
     q.out_ld = p.nx;
     q.out_bstride = np;
-    q.tw = ax->tw;
+    q.tw = twx;
     q.out_scale = 1.0;
     q.red = s.red_pout ? red_region(c, 2) + RS_P : nullptr;
     q.red_stride = RS_COUNT;
@@ -1173,6 +1189,8 @@ int wos_ctx_destroy(wos_ctx c) {
                 if (kv.second.chirp) cudaFree(kv.second.chirp);
                 if (kv.second.bf) cudaFree(kv.second.bf);
                 if (kv.second.bi) cudaFree(kv.second.bi);
+                for (void* t : kv.second.ftw)
+                    if (t) cudaFree(t);
             }
         DevBuf* bufs[] = {&c->stage, &c->scratch, &c->scratch2, &c->scratch3, &c->red, &c->redout, &c->tmp,
                           &c->maps, &c->params, &c->vol, &c->accum, &c->aux};
@@ -2226,7 +2244,7 @@ int wos_autotune(wos_ctx c, int ny, int nx, int* row_e, int* col_e, int* col_w) 
                 if (!fast_supported(c->fp64, nx, re) || !fast_supported(c->fp64, ny, ce)) continue;
                 const int T = ny / ce;
                 const int maxt = (ce >= 16 || c->fp64) ? 512 : 1024;
-                if ((w * T > maxt && w > 1) || col_smem_bytes(c->fp64, ny, w) > 220 * 1024) continue;
+                if ((w * T > maxt && w > 1) || fast_col_smem(c->fp64, ny, w) > 220 * 1024) continue;
                 c->tune[key] = Tune{re, ce, w};
                 bool ok = true;
                 for (int it = 0; it < 2 && ok; it++) ok = run_propagate(c, p) == WOS_OK;

@@ -1,15 +1,20 @@
 // wos_fast.cu -- compile-time specialised sweeps of the band-limited ASM hot
-// path (power-of-two lines): the transform length L and the elements per
-// thread E are template parameters, so every pass radix, Stockham stride and
-// twiddle step is a compile-time constant and the passes unroll completely.
+// path (power-of-two lines).  The transform length L and the elements per
+// thread E are template parameters, so every pass radix, Stockham stride,
+// shared-memory offset and twiddle offset is a compile-time constant:
+//  * shared memory is padded (one slot per 2^SH positions) so that each
+//    exchange is conflict-free and every address is a per-thread base plus an
+//    immediate (the padding commutes with the pass strides, see padq below);
+//  * twiddles come from per-pass tables W_{NS R}^{r k} laid out [r][k]
+//    (generated in FP64, rounded once), so the threads of a warp read
+//    consecutive entries and each load is base + immediate.
 //
-//   k_rows_fast<Real, L, E, INV>: one row per T = L/E threads; coalesced
-//       loads straight into registers, optional complex128 I/O conversion,
-//       optional |E|^2 reduction, coalesced stores.
-//   k_cols_fast<Real, L, E>: W adjacent columns per CTA; forward column
-//       FFT, H(fx, fy) of asmTF (optics/propagate.go:159-181) generated on the
-//       fly from an FP64 argument, inverse column FFT; optional spectral
-//       power-loss sums.  Three sweeps per propagation in total.
+//   k_rows_fast<Real, L, E, INV>: one row per T = L/E threads, coalesced
+//       loads straight into registers, optional complex128 conversion and
+//       sum |E|^2, coalesced stores.
+//   k_cols_fast<Real, L, E>: W adjacent columns per CTA; forward column FFT,
+//       H(fx, fy) of asmTF (optics/propagate.go:159-181) generated on the fly
+//       from an FP64 argument, inverse column FFT, optional spectral loss sums.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -23,27 +28,48 @@ template <> struct Log2<1> { static constexpr int v = 0; };
 
 template <int L, int E> struct FPlan {
     static constexpr int LG = Log2<L>::v, LE = Log2<E>::v;
-    static constexpr int P = (LG + LE - 1) / LE;                       // passes
-    static constexpr int RS = (LG % LE) ? (1 << (LG % LE)) : E;        // the odd radix (E if none)
-    static constexpr int T = L / E;                                    // threads per line
+    static constexpr int P = (LG + LE - 1) / LE;                 // passes
+    static constexpr int RS = (LG % LE) ? (1 << (LG % LE)) : E;  // the odd radix (E if none)
+    static constexpr int T = L / E;                              // threads per line
 };
-template <int L, int E, bool INV, int p> struct FRadix {
-    static constexpr int v = INV ? (p == FPlan<L, E>::P - 1 ? FPlan<L, E>::RS : E) : (p == 0 ? FPlan<L, E>::RS : E);
-};
+// radix and sub-transform length NS of pass p (forward order (RS, E, ..), inverse reversed)
+__host__ __device__ constexpr int fp_radix(int P, int RS, int E, bool inv, int p) {
+    return inv ? (p == P - 1 ? RS : E) : (p == 0 ? RS : E);
+}
+__host__ __device__ constexpr int fp_ns(int P, int RS, int E, bool inv, int p) {
+    int ns = 1;
+    for (int q = 0; q < p; q++) ns *= fp_radix(P, RS, E, inv, q);
+    return ns;
+}
+// offset of pass p's table: forward passes first, then inverse passes;
+// pass p holds NS*(R-1) entries (pass 0 has NS = 1 and needs none)
+__host__ __device__ constexpr int fp_twoff(int P, int RS, int E, bool inv, int p) {
+    int off = 0;
+    for (int d = 0; d < 2; d++) {
+        const bool dinv = d == 1;
+        for (int q = 1; q < P; q++) {
+            if (dinv == inv && q == p) return off;
+            off += fp_ns(P, RS, E, dinv, q) * (fp_radix(P, RS, E, dinv, q) - 1);
+        }
+    }
+    return off;
+}
 
-// One Stockham DIT pass, radix R, sub-transform length NS (compile time).
-template <int R, int E, int L, int NS, bool INV, typename C>
-__device__ __forceinline__ void fpass(C* v, int tt, const C* __restrict__ tw) {
+// padded slot of position q: one pad slot every 2^SH positions
+template <int SH> __device__ __forceinline__ int padq(int q) { return q + (q >> SH); }
+
+// One Stockham DIT pass, radix R, sub-transform length NS.
+template <int R, int E, int L, int NS, int TWOFF, bool INV, typename C>
+__device__ __forceinline__ void fpass(C* v, int tt, const C* __restrict__ twp) {
     constexpr int T = L / E;
 #pragma unroll
     for (int b = 0; b < E / R; b++) {
         if constexpr (NS > 1) {
-            const int j = tt + b * T;
-            const int k = j & (NS - 1);
-            constexpr int step = L / (NS * R);
+            const int k = (tt + b * T) & (NS - 1);
+            const C* tk = twp + TWOFF + k;
 #pragma unroll
             for (int r = 1; r < R; r++) {
-                C w = __ldg(tw + r * k * step);
+                C w = __ldg(tk + (r - 1) * NS);
                 if (INV) w.y = -w.y;
                 v[b * R + r] = cmul(v[b * R + r], w);
             }
@@ -52,42 +78,54 @@ __device__ __forceinline__ void fpass(C* v, int tt, const C* __restrict__ tw) {
     }
 }
 
-template <int R, int E, int L, int NS, typename C, typename IDX>
-__device__ __forceinline__ void fstore(const C* v, C* sm, const IDX& ix, int line, int tt) {
+// Exchange stores / loads on a line whose element q lives at
+// sm[line_base + STR * padq<SH>(q)] (STR = W for interleaved columns).
+template <int R, int E, int L, int NS, int SH, int STR, typename C>
+__device__ __forceinline__ void fstore(const C* v, C* smb, int tt) {
     constexpr int T = L / E;
+    static_assert(NS >= (1 << SH) || NS == 1 || NS * R >= (1 << SH), "padding does not commute with this pass");
 #pragma unroll
     for (int b = 0; b < E / R; b++) {
         const int j = tt + b * T;
         const int k = j & (NS - 1);
         const int base = (j - k) * R + k;
+        int tb;
+        if constexpr (NS >= (1 << SH)) tb = padq<SH>(base);
+        else tb = base + ((base - k) >> SH);
+        C* p = smb + STR * tb;
 #pragma unroll
-        for (int r = 0; r < R; r++) sm[ix(line, base + r * NS)] = v[b * R + r];
+        for (int r = 0; r < R; r++) p[STR * (r * NS + ((r * NS) >> SH))] = v[b * R + r];
     }
 }
 
-template <int R, int E, int L, typename C, typename IDX>
-__device__ __forceinline__ void fload(C* v, const C* sm, const IDX& ix, int line, int tt) {
+template <int R, int E, int L, int SH, int STR, typename C>
+__device__ __forceinline__ void fload(C* v, const C* smb, int tt) {
     constexpr int T = L / E;
+    constexpr int LR = L / R;
+    static_assert(LR % (1 << SH) == 0, "load stride must be a multiple of the pad period");
 #pragma unroll
-    for (int b = 0; b < E / R; b++)
+    for (int b = 0; b < E / R; b++) {
+        const C* p = smb + STR * padq<SH>(tt + b * T);
 #pragma unroll
-        for (int r = 0; r < R; r++) v[b * R + r] = sm[ix(line, tt + b * T + r * (L / R))];
+        for (int r = 0; r < R; r++) v[b * R + r] = p[STR * (r * (LR + (LR >> SH)))];
+    }
 }
 
-// All passes from p on (template recursion, fully unrolled).
-template <int L, int E, bool INV, int p, int NS, typename C, typename IDX>
-__device__ __forceinline__ void fpasses(C* v, C* sm, const IDX& ix, int line, int tt, const C* __restrict__ tw) {
+template <int L, int E, bool INV, int p, int SH, int STR, typename C>
+__device__ __forceinline__ void fpasses(C* v, C* smb, int tt, const C* __restrict__ twp) {
     using PL = FPlan<L, E>;
     if constexpr (p < PL::P) {
-        constexpr int R = FRadix<L, E, INV, p>::v;
-        fpass<R, E, L, NS, INV>(v, tt, tw);
+        constexpr int R = fp_radix(PL::P, PL::RS, E, INV, p);
+        constexpr int NS = fp_ns(PL::P, PL::RS, E, INV, p);
+        constexpr int TWOFF = fp_twoff(PL::P, PL::RS, E, INV, p);
+        fpass<R, E, L, NS, TWOFF, INV>(v, tt, twp);
         if constexpr (p < PL::P - 1) {
-            constexpr int R2 = FRadix<L, E, INV, p + 1>::v;
+            constexpr int R2 = fp_radix(PL::P, PL::RS, E, INV, p + 1);
             __syncthreads();
-            fstore<R, E, L, NS>(v, sm, ix, line, tt);
+            fstore<R, E, L, NS, SH, STR>(v, smb, tt);
             __syncthreads();
-            fload<R2, E, L>(v, sm, ix, line, tt);
-            fpasses<L, E, INV, p + 1, NS * R>(v, sm, ix, line, tt, tw);
+            fload<R2, E, L, SH, STR>(v, smb, tt);
+            fpasses<L, E, INV, p + 1, SH, STR>(v, smb, tt, twp);
         }
     }
 }
@@ -100,6 +138,11 @@ __device__ __forceinline__ int fpos(int s, int tt) {
 
 template <typename Real, int E> struct FMaxT { static constexpr int v = (E >= 16 || sizeof(Real) == 8) ? 512 : 1024; };
 
+constexpr int kRowSH = 4;  // row layout: one pad slot per 16
+constexpr int kColSH = 3;  // column tile: one pad row per 8 (W-interleaved)
+__host__ __device__ constexpr int frow_stride(int L) { return L + (L >> kRowSH) + 2; }
+__host__ __device__ constexpr int fcol_elems(int L, int W) { return W * (L + (L >> kColSH)) + 2; }
+
 // ------------------------------------------------------------------- rows
 template <typename Real, int L, int E, bool INV>
 __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows a) {
@@ -107,13 +150,12 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
     using PL = FPlan<L, E>;
     constexpr int T = PL::T;
     extern __shared__ __align__(16) unsigned char smraw[];
-    C* sm = reinterpret_cast<C*>(smraw);
     const int lines = blockDim.x / T;
     const int line = threadIdx.x / T, tt = threadIdx.x - line * T;
+    C* smb = reinterpret_cast<C*>(smraw) + line * frow_stride(L);
     const int r = blockIdx.x * lines + line;
     const bool act = r < a.rows;
-    const RowIdx ix{row_line_stride(L)};
-    const C* tw = reinterpret_cast<const C*>(a.tw);
+    const C* twp = reinterpret_cast<const C*>(a.tw);
     constexpr int R1 = INV ? E : PL::RS;
     constexpr int RO = INV ? PL::RS : E;
     const long long ib = (long long)blockIdx.y * a.in_bstride + (long long)r * a.in_ld;
@@ -122,18 +164,18 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
     double pw = 0;
     if (act) {
         if (a.in_c128) {
-            const double2* in = reinterpret_cast<const double2*>(a.in) + ib;
+            const double2* in = reinterpret_cast<const double2*>(a.in) + ib + tt;
 #pragma unroll
             for (int s = 0; s < E; s++) {
-                const double2 d = in[fpos<R1, E, L>(s, tt)];
+                const double2 d = in[fpos<R1, E, L>(s, 0)];
                 v[s] = mkc<C>((Real)d.x, (Real)d.y);
             }
         } else {
-            const C* in = reinterpret_cast<const C*>(a.in) + ib;
+            const C* in = reinterpret_cast<const C*>(a.in) + ib + tt;
 #pragma unroll
-            for (int s = 0; s < E; s++) v[s] = in[fpos<R1, E, L>(s, tt)];
+            for (int s = 0; s < E; s++) v[s] = in[fpos<R1, E, L>(s, 0)];
         }
-        if (a.red) {
+        if (a.red && !INV) {
 #pragma unroll
             for (int s = 0; s < E; s++) pw += (double)v[s].x * v[s].x + (double)v[s].y * v[s].y;
         }
@@ -141,29 +183,28 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
 #pragma unroll
         for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
     }
-    fpasses<L, E, INV, 0, 1>(v, sm, ix, line, tt, tw);
+    fpasses<L, E, INV, 0, kRowSH, 1>(v, smb, tt, twp);
     if (act) {
         if (a.out_scale != 1.0) {
 #pragma unroll
             for (int s = 0; s < E; s++) v[s] = cscale(v[s], (Real)a.out_scale);
         }
         if (a.red && INV) {
-            pw = 0;
 #pragma unroll
             for (int s = 0; s < E; s++) pw += (double)v[s].x * v[s].x + (double)v[s].y * v[s].y;
         }
         if (a.out_c128) {
-            double2* out = reinterpret_cast<double2*>(a.out) + ob;
+            double2* out = reinterpret_cast<double2*>(a.out) + ob + tt;
 #pragma unroll
-            for (int s = 0; s < E; s++) out[fpos<RO, E, L>(s, tt)] = make_double2(v[s].x, v[s].y);
+            for (int s = 0; s < E; s++) out[fpos<RO, E, L>(s, 0)] = make_double2(v[s].x, v[s].y);
         } else {
-            C* out = reinterpret_cast<C*>(a.out) + ob;
+            C* out = reinterpret_cast<C*>(a.out) + ob + tt;
 #pragma unroll
-            for (int s = 0; s < E; s++) out[fpos<RO, E, L>(s, tt)] = v[s];
+            for (int s = 0; s < E; s++) out[fpos<RO, E, L>(s, 0)] = v[s];
         }
     }
     if (a.red) {
-        // per-CTA partial of sum |E|^2 (slot 0 of a RS_COUNT record)
+        // per-CTA partial of sum |E|^2 (slot 0 of a record of stride red_stride)
         __shared__ double rsm[32];
         for (int o = 16; o > 0; o >>= 1) pw += __shfl_down_sync(0xffffffffu, pw, o);
         if ((threadIdx.x & 31) == 0) rsm[threadIdx.x >> 5] = pw;
@@ -177,14 +218,21 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
 }
 
 // ------------------------------------------------------------------- cols
-__device__ __forceinline__ float fast_reduce_2pi(double arg) {
+__device__ __forceinline__ double fast_reduce_2pi_d(double arg) {
     const double inv2pi = 0.15915494309189533577;
     const double p2hi = 6.283185307179586232;
     const double p2lo = 2.4492935982947064e-16;
     const double n = rint(arg * inv2pi);
     double r = fma(-n, p2hi, arg);
-    r = fma(-n, p2lo, r);
-    return (float)r;
+    return fma(-n, p2lo, r);
+}
+
+// sqrt of s in (0, 1] to ~1e-14 relative: single-precision reciprocal square
+// root seed refined by one Newton step in FP64 (s in FP32 range here).
+__device__ __forceinline__ double fast_sqrt_d(double s) {
+    const double r0 = (double)rsqrtf((float)s);
+    const double y0 = s * r0;
+    return fma(0.5 * r0, fma(-y0, y0, s), y0);
 }
 
 template <typename Real, int L, int E>
@@ -193,42 +241,55 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_cols_fast(const FastCols 
     using PL = FPlan<L, E>;
     constexpr int T = PL::T;
     extern __shared__ __align__(16) unsigned char smraw[];
-    C* sm = reinterpret_cast<C*>(smraw);
     const int W = a.W;
     const int w = threadIdx.x & (W - 1);
     const int tt = threadIdx.x / W;
+    C* smb = reinterpret_cast<C*>(smraw) + w;
     const int col = blockIdx.x * W + w;
     const bool act = col < a.ncols;
-    const ColIdx ix{W};
-    const C* tw = reinterpret_cast<const C*>(a.tw);
-    C* base = reinterpret_cast<C*>(a.data) + (long long)blockIdx.y * a.bstride;
+    const C* twp = reinterpret_cast<const C*>(a.tw);
+    C* base = reinterpret_cast<C*>(a.data) + (long long)blockIdx.y * a.bstride + col;
     C v[E];
     constexpr int R1 = PL::RS;
+    if (act) {
+        const C* src = base + (long long)tt * a.ld;
 #pragma unroll
-    for (int s = 0; s < E; s++)
-        v[s] = act ? base[(long long)fpos<R1, E, L>(s, tt) * a.ld + col] : mkc<C>(0, 0);
-    fpasses<L, E, false, 0, 1>(v, sm, ix, w, tt, tw);
+        for (int s = 0; s < E; s++) v[s] = src[(long long)fpos<R1, E, L>(s, 0) * a.ld];
+    } else {
+#pragma unroll
+        for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
+    }
+    // interleaved tile: stride W between consecutive positions of a column
+    switch (W) {
+    case 1: fpasses<L, E, false, 0, kColSH, 1>(v, smb, tt, twp); break;
+    case 2: fpasses<L, E, false, 0, kColSH, 2>(v, smb, tt, twp); break;
+    case 4: fpasses<L, E, false, 0, kColSH, 4>(v, smb, tt, twp); break;
+    case 8: fpasses<L, E, false, 0, kColSH, 8>(v, smb, tt, twp); break;
+    default: fpasses<L, E, false, 0, kColSH, 16>(v, smb, tt, twp); break;
+    }
 
-    // transfer function on the natural radix-E mapping: q = tt + s*T
+    // transfer function on the radix-E natural mapping: q = tt + s*T
     const double wl = a.wl;
-    const double fx = (col <= a.ncols / 2 ? (double)col : (double)(col - a.ncols)) / ((double)a.ncols * a.dx);
     double p0 = 0, l1 = 0;
     if constexpr (sizeof(Real) == 4) {
         // FP32 pipeline: FP64 argument kz*sqrt(1 - (wl fx)^2 - (wl fy)^2),
-        // reduced to [-pi, pi] in FP64, sin/cos in FP32
+        // reduced to [-pi, pi] in FP64, sin/cos in single precision
+        const double fx = (col <= a.ncols / 2 ? (double)col : (double)(col - a.ncols)) / ((double)a.ncols * a.dx);
         const double ax = wl * fx;
         const double cx = fma(-ax, ax, 1.0);
         const double g = wl / ((double)L * a.dx);
+        const float sc = (float)a.scale;
+        const float sgn = a.conj ? -1.f : 1.f;
 #pragma unroll
         for (int s = 0; s < E; s++) {
             const int q = tt + s * T;
-            const double qq = (q <= L / 2) ? (double)q : (double)(q - L);
-            const double ay = qq * g;
+            const double ay = (double)(q <= L / 2 ? q : q - L) * g;
             const double sq = fma(-ay, ay, cx);
             float hr, hi;
             double m2 = 1.0;
-            if (sq >= 0) {
-                sincosf(fast_reduce_2pi(a.kz * sqrt(sq)), &hi, &hr);
+            if (sq >= 0) {  // rho <= 1: propagating
+                const double sr = sq > 0 ? fast_sqrt_d(sq) : 0.0;
+                __sincosf((float)fast_reduce_2pi_d(a.kz * sr), &hi, &hr);
             } else {
                 const double decay = a.kaz * sqrt(-sq);
                 double amp;
@@ -244,19 +305,19 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_cols_fast(const FastCols 
                 p0 += pp;
                 l1 += pp * (1.0 - m2);
             }
-            const float sc = (float)a.scale;
-            v[s] = cmul(v[s], make_float2(hr * sc, (a.conj ? -hi : hi) * sc));
+            v[s] = cmul(v[s], make_float2(hr * sc, sgn * hi * sc));
         }
     } else {
         // FP64 pipeline: the reference's operation sequence, uncontracted
+        const double fxe = (col <= a.ncols / 2) ? __ddiv_rn((double)col, __dmul_rn((double)a.ncols, a.dx))
+                                                : __ddiv_rn((double)(col - a.ncols), __dmul_rn((double)a.ncols, a.dx));
+        const double den = __dmul_rn((double)L, a.dx);
+        const double px = fabs(__dmul_rn(wl, fxe));
 #pragma unroll
         for (int s = 0; s < E; s++) {
             const int q = tt + s * T;
-            const double den = __dmul_rn((double)L, a.dx);
             const double fy = (q <= L / 2) ? __ddiv_rn((double)q, den) : __ddiv_rn((double)(q - L), den);
-            const double fxe = (col <= a.ncols / 2) ? __ddiv_rn((double)col, __dmul_rn((double)a.ncols, a.dx))
-                                                    : __ddiv_rn((double)(col - a.ncols), __dmul_rn((double)a.ncols, a.dx));
-            double p = fabs(__dmul_rn(wl, fxe)), qv = fabs(__dmul_rn(wl, fy));
+            double p = px, qv = fabs(__dmul_rn(wl, fy));
             if (p < qv) { const double t = p; p = qv; qv = t; }
             double rho = 0;
             if (p != 0) {
@@ -293,16 +354,21 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_cols_fast(const FastCols 
         }
     }
     if (!act) {
-#pragma unroll
-        for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
         p0 = 0;
         l1 = 0;
     }
-    fpasses<L, E, true, 0, 1>(v, sm, ix, w, tt, tw);
+    switch (W) {
+    case 1: fpasses<L, E, true, 0, kColSH, 1>(v, smb, tt, twp); break;
+    case 2: fpasses<L, E, true, 0, kColSH, 2>(v, smb, tt, twp); break;
+    case 4: fpasses<L, E, true, 0, kColSH, 4>(v, smb, tt, twp); break;
+    case 8: fpasses<L, E, true, 0, kColSH, 8>(v, smb, tt, twp); break;
+    default: fpasses<L, E, true, 0, kColSH, 16>(v, smb, tt, twp); break;
+    }
     if (act) {
         constexpr int RO = PL::RS;
+        C* dst = base + (long long)tt * a.ld;
 #pragma unroll
-        for (int s = 0; s < E; s++) base[(long long)fpos<RO, E, L>(s, tt) * a.ld + col] = v[s];
+        for (int s = 0; s < E; s++) dst[(long long)fpos<RO, E, L>(s, 0) * a.ld] = v[s];
     }
     if (a.red) {
         __shared__ double rsm[32][2];
@@ -328,6 +394,46 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_cols_fast(const FastCols 
     }
 }
 
+// ------------------------------------------------------------------ tables
+// Per-pass twiddles W_{NS R}^{r k} (forward sign), [r-1][k], FP64 -> pipeline type.
+template <typename C>
+__global__ void k_pass_twiddles(C* out, int off, int NS, int R) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= NS * (R - 1)) return;
+    const int r = i / NS + 1, k = i % NS;
+    double s, c;
+    sincospi(-2.0 * (double)r * (double)k / ((double)NS * (double)R), &s, &c);
+    out[off + i] = mkc<C>((decltype(C::x))c, (decltype(C::x))s);
+}
+
+int fast_table_len(int L, int E) {
+    int LG = 0, LE = 0;
+    while ((1 << LG) < L) LG++;
+    while ((1 << LE) < E) LE++;
+    const int P = (LG + LE - 1) / LE;
+    const int RS = (LG % LE) ? (1 << (LG % LE)) : E;
+    return fp_twoff(P, RS, E, true, P) + 1;  // past the last inverse pass
+}
+
+cudaError_t fast_build_twiddles(int fp64, int L, int E, void* out, cudaStream_t st) {
+    int LG = 0, LE = 0;
+    while ((1 << LG) < L) LG++;
+    while ((1 << LE) < E) LE++;
+    const int P = (LG + LE - 1) / LE;
+    const int RS = (LG % LE) ? (1 << (LG % LE)) : E;
+    for (int d = 0; d < 2; d++) {
+        const bool inv = d == 1;
+        for (int p = 1; p < P; p++) {
+            const int NS = fp_ns(P, RS, E, inv, p), R = fp_radix(P, RS, E, inv, p);
+            const int off = fp_twoff(P, RS, E, inv, p);
+            const int n = NS * (R - 1);
+            if (fp64) k_pass_twiddles<double2><<<(n + 255) / 256, 256, 0, st>>>(reinterpret_cast<double2*>(out), off, NS, R);
+            else k_pass_twiddles<float2><<<(n + 255) / 256, 256, 0, st>>>(reinterpret_cast<float2*>(out), off, NS, R);
+        }
+    }
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ launch
 template <typename Real, int L, int E, bool INV>
 static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
@@ -335,7 +441,7 @@ static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
     int lines = 1;
     while (lines * 2 * T <= 256 && lines * 2 <= a.rows) lines *= 2;
     while (lines * T < 32) lines *= 2;
-    const size_t smem = (size_t)row_line_stride(L) * lines * sizeof(typename CT<Real>::t);
+    const size_t smem = (size_t)frow_stride(L) * lines * sizeof(typename CT<Real>::t);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_rows_fast<Real, L, E, INV>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -353,7 +459,8 @@ static cudaError_t go_cols(const FastCols& a0, cudaStream_t st, int* nblocks) {
     FastCols a = a0;
     while (a.W * T < 32) a.W *= 2;
     while (a.W > 1 && a.W * T > FMaxT<Real, E>::v) a.W /= 2;
-    const size_t smem = (size_t)col_tile_elems(L, a.W) * sizeof(typename CT<Real>::t);
+    if (a.W > 16) return cudaErrorInvalidConfiguration;
+    const size_t smem = (size_t)fcol_elems(L, a.W) * sizeof(typename CT<Real>::t);
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(k_cols_fast<Real, L, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -367,19 +474,19 @@ static cudaError_t go_cols(const FastCols& a0, cudaStream_t st, int* nblocks) {
 #define WOS_FAST_L(X) X(256) X(512) X(1024) X(2048) X(4096) X(8192)
 
 cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaStream_t st, int* nblocks) {
-#define CASE_R(LL)                                                                       \
-    case LL:                                                                             \
-        if (fp64) {                                                                      \
-            if (E == 8 && LL <= 4096) return inv ? go_rows<double, LL, 8, true>(a, st, nblocks) \
-                                                 : go_rows<double, LL, 8, false>(a, st, nblocks); \
-            if (E == 16 && LL >= 8192) return inv ? go_rows<double, LL, 16, true>(a, st, nblocks) \
+#define CASE_R(LL)                                                                                  \
+    case LL:                                                                                        \
+        if (fp64) {                                                                                 \
+            if (E == 8 && LL <= 4096) return inv ? go_rows<double, LL, 8, true>(a, st, nblocks)     \
+                                                 : go_rows<double, LL, 8, false>(a, st, nblocks);   \
+            if (E == 16 && LL >= 8192) return inv ? go_rows<double, LL, 16, true>(a, st, nblocks)   \
                                                   : go_rows<double, LL, 16, false>(a, st, nblocks); \
-        } else {                                                                         \
-            if (E == 8 && LL <= 4096) return inv ? go_rows<float, LL, 8, true>(a, st, nblocks) \
-                                                 : go_rows<float, LL, 8, false>(a, st, nblocks); \
-            if (E == 16) return inv ? go_rows<float, LL, 16, true>(a, st, nblocks)       \
-                                    : go_rows<float, LL, 16, false>(a, st, nblocks);     \
-        }                                                                                \
+        } else {                                                                                    \
+            if (E == 8 && LL <= 4096) return inv ? go_rows<float, LL, 8, true>(a, st, nblocks)      \
+                                                 : go_rows<float, LL, 8, false>(a, st, nblocks);    \
+            if (E == 16) return inv ? go_rows<float, LL, 16, true>(a, st, nblocks)                  \
+                                    : go_rows<float, LL, 16, false>(a, st, nblocks);                \
+        }                                                                                           \
         break;
     switch (L) { WOS_FAST_L(CASE_R) }
 #undef CASE_R
@@ -387,15 +494,15 @@ cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaS
 }
 
 cudaError_t fast_cols(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks) {
-#define CASE_C(LL)                                                                  \
-    case LL:                                                                        \
-        if (fp64) {                                                                 \
-            if (E == 8 && LL <= 4096) return go_cols<double, LL, 8>(a, st, nblocks); \
+#define CASE_C(LL)                                                                     \
+    case LL:                                                                           \
+        if (fp64) {                                                                    \
+            if (E == 8 && LL <= 4096) return go_cols<double, LL, 8>(a, st, nblocks);   \
             if (E == 16 && LL >= 8192) return go_cols<double, LL, 16>(a, st, nblocks); \
-        } else {                                                                    \
-            if (E == 8 && LL <= 4096) return go_cols<float, LL, 8>(a, st, nblocks); \
-            if (E == 16) return go_cols<float, LL, 16>(a, st, nblocks);             \
-        }                                                                           \
+        } else {                                                                       \
+            if (E == 8 && LL <= 4096) return go_cols<float, LL, 8>(a, st, nblocks);    \
+            if (E == 16) return go_cols<float, LL, 16>(a, st, nblocks);                \
+        }                                                                              \
         break;
     switch (L) { WOS_FAST_L(CASE_C) }
 #undef CASE_C
@@ -407,5 +514,7 @@ bool fast_supported(int fp64, int L, int E) {
     if (fp64) return (E == 8 && L <= 4096) || (E == 16 && L >= 8192);
     return E == 16 || (E == 8 && L <= 4096);
 }
+
+size_t fast_col_smem(int fp64, int L, int W) { return (size_t)fcol_elems(L, W) * (fp64 ? 16 : 8); }
 
 }  // namespace wos

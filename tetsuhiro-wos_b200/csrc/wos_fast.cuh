@@ -35,3 +35,10 @@ cudaError_t fast_cols(int fp64, int L, int E, const FastCols& a, cudaStream_t st
 bool fast_supported(int fp64, int L, int E);
 
 }  // namespace wos
+
+namespace wos {
+// per-pass twiddle tables of the specialised sweeps (forward passes, then inverse)
+int fast_table_len(int L, int E);
+cudaError_t fast_build_twiddles(int fp64, int L, int E, void* out, cudaStream_t st);
+size_t fast_col_smem(int fp64, int L, int W);
+}  // namespace wos
