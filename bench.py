@@ -211,6 +211,8 @@ def main() -> None:
     ap.add_argument("--impl", default="ours")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="use the default (or WOS_ROWE/WOS_COLE/WOS_COLW) launch configuration")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -237,8 +239,11 @@ def main() -> None:
     g64.set_stream(stream.cuda_stream)
     ctx = wos.Context(wavelength=WL, warnings_enabled=False)
     # launch configuration of the specialised sweeps: timed on this device
-    tune32 = g32.autotune(N, N)
-    tune64 = g64.autotune(N, N)
+    if args.no_autotune:
+        tune32 = tune64 = ("default",) * 3
+    else:
+        tune32 = g32.autotune(N, N)
+        tune64 = g64.autotune(N, N)
 
     ex = input_field()
     with torch.cuda.stream(stream):

@@ -244,6 +244,25 @@ WOS_API int wos_asm_loss_grad(wos_ctx ctx, int ny, int nx, double dx, double z, 
 /* Adjoint operator A^H = F^-1 diag(conj H) F of an ASM step, host field in place. */
 WOS_API int wos_asm_adjoint(wos_ctx ctx, wos_field* f, double z, const wos_context* c);
 
+/* ---- zero-padded ASM that allocates no device memory (no counterpart in the
+ *      reference).  For callers that cannot call cudaMalloc: processes that
+ *      reserve all device memory up front behind their own allocator, or
+ *      pipelines that cannot afford the device-wide synchronisation of
+ *      cudaFree.  Same result as wos_propagate_dev(..., WOS_ASM_PAD, ...) on a
+ *      WOS_FP32 context, without diagnostics.  in / out: device complex64
+ *      [ny][nx] (in == out allowed); ny and nx powers of two, 4..1024, larger
+ *      sizes return WOS_UNSUPPORTED_SIZE.  Work space: file-scope device arrays
+ *      (a 1024 x 2048 complex64 intermediate, 16 MiB, plus 32 KiB of
+ *      twiddles) that every GPU loading the library holds until exit.  The
+ *      first call on a device resolves their addresses and fills the twiddles
+ *      (a kernel and a synchronisation of `stream`): make that first call
+ *      before any stream capture.  All calls share the arrays, so calls that
+ *      overlap on the GPU (different streams or threads) race; serialise them.
+ *      Nothing needs clearing between calls: each call writes every scratch
+ *      element it reads.  stream: a cudaStream_t (NULL = legacy default). ---- */
+WOS_API int wos_asm_pad_c64_noalloc(const void* in, void* out, int ny, int nx, double dx, double z,
+                                    const wos_context* c, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1136,6 +1136,14 @@ const char* wos_status_string(int s) {
 }
 
 const char* wos_last_error(void) { return g_err.c_str(); }
+}  // extern "C"
+
+namespace wos {
+// error text of entry points defined in other translation units
+void set_last_error(const char* msg) { g_err = msg; }
+}  // namespace wos
+
+extern "C" {
 
 const char* wos_backend_info(void) { return "B200 native (sm_100a): hand-written Stockham/Bluestein FFT, fused ASM sweeps"; }
 

@@ -39,7 +39,7 @@ EXPORTS = [
     "wos_propagate_dev_c128", "wos_splitstep", "wos_splitstep_dev", "wos_splitstep_maps",
     "wos_polychromatic", "wos_volume", "wos_schell_modes", "wos_partially_coherent",
     "wos_apply_lens", "wos_apply_aperture_circle", "wos_apply_grating", "wos_apply_phase_mask",
-    "wos_asm_forward_loss", "wos_asm_loss_grad", "wos_asm_adjoint",
+    "wos_asm_forward_loss", "wos_asm_loss_grad", "wos_asm_adjoint", "wos_asm_pad_c64_noalloc",
 ]
 
 
@@ -124,6 +124,7 @@ def lib():
             "wos_asm_forward_loss": ([vp, i, i, d, d, vp, vp, vp, vp, vp], i),
             "wos_asm_loss_grad": ([vp, i, i, d, d, vp, vp, vp, vp, vp, vp], i),
             "wos_asm_adjoint": ([vp, vp, d, vp], i),
+            "wos_asm_pad_c64_noalloc": ([vp, vp, i, i, d, d, vp, vp], i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name, None)
