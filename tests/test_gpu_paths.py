@@ -54,3 +54,31 @@ def test_every_launch_configuration(prec):
                     f = wos.Field(ex.copy(), dx)
                     g.propagate(f, z, "asm", wos.Context(wavelength=wl))
                     assert rel_l2(f.ex, o.ex) <= tol(prec), (re, ce, w)
+
+
+@pytest.mark.parametrize("prec", [wos.FP64, wos.FP32], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("n", [256, 1024, 2048])
+def test_wrap_histogram_fast_equals_general(prec, n):
+    """asmWrapWarn's spectral radius (optics/propagate.go:247-310) from the
+    histogram binned inside the specialised column sweep equals the general
+    sweep's and the oracle's, bin for bin at the 90 % crossing."""
+    dx, wl = 2e-6, 632.8e-9
+    z = 3.0 * n * dx * 2 * dx / wl      # walk-off test active: z wl / (2 dx) > n dx
+    rng = np.random.default_rng(n)
+    x = (np.arange(n) - n / 2) * dx
+    env = np.exp(-(x[None, :] ** 2 + x[:, None] ** 2) / (n * dx / 5) ** 2)
+    ex = env * np.exp(1j * rng.uniform(0, 0.6, (n, n)))
+    res = []
+    with wos.GPU(prec) as g:
+        for fast in (True, False):
+            g.set_fast_path(fast)
+            f = wos.Field(ex.copy(), dx)
+            c = wos.Context(wavelength=wl)
+            d = g.propagate(f, z, "asm", c)
+            assert d.wrap_checked == 1
+            res.append((d.spectral_radius, dict(c.warnings), f.ex))
+    assert res[0][0] == res[1][0]
+    assert res[0][1].keys() == res[1][1].keys()
+    assert rel_l2(res[0][2], res[1][2]) <= tol(prec)
+    o = O.Field(ex.copy(), dx)
+    assert res[0][0] == O.spectral_radius(o, 0.90)

@@ -542,10 +542,8 @@ size_t fast_row_blocks(int L, int E, int rows, int batch) {
     return (size_t)((rows + lines - 1) / lines) * std::max(batch, 1);
 }
 size_t fast_col_blocks(int fp64, int L, int E, int W, int ncols, int batch) {
-    const int T = L / E;
-    const int maxt = (E >= 16 || fp64) ? 512 : 1024;
-    while (W * T < 32) W *= 2;
-    while (W > 1 && W * T > maxt) W /= 2;
+    W = fast_col_width(fp64, L, E, W);
+    if (W < 1) W = 1;
     return (size_t)((ncols + W - 1) / W) * std::max(batch, 1);
 }
 
@@ -583,7 +581,7 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     }
     const size_t nbr = fast_row_blocks(p.nx, t.rowE, p.ny, p.ncomp);
     const size_t nbc = fast_col_blocks(c->fp64, p.ny, t.colE, t.colW, p.nx, p.ncomp);
-    if (s.red_pin || s.red_pout || s.red_loss) TRY(red_prepare(c, std::max(nbr, nbc)));
+    if (s.red_pin || s.red_pout || s.red_loss || s.hist) TRY(red_prepare(c, std::max(nbr, nbc)));
     int nb = 0;
     FastRows r{};
     r.rows = p.ny;
@@ -620,10 +618,17 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     k.reg = s.h.reg;
     k.backward = s.h.z < 0;
     k.conj = s.h.conj;
+    k.krev = s.h.kz / (2 * M_PI);
+    k.rev_phase = std::fabs(k.krev) < 268435456.0;  // 2^28 revolutions
     k.red = s.red_loss ? red_region(c, 1) + RS_SW : nullptr;
     k.red_stride = RS_COUNT;
+    if (s.hist) {
+        k.hist = red_region(c, 1) + RS_HIST;
+        k.hist_dx = p.dx;
+    }
     CK(timed_launch(c, 4, [&] { return fast_cols(c->fp64, p.ny, t.colE, k, c->st, &nb); }));
     if (s.red_loss) CK(launch_reduce_finish(red_region(c, 1), (int)nbc, 1, RS_SW, 2, redout_region(c, 1), c->st));
+    if (s.hist) CK(launch_reduce_finish(red_region(c, 1), (int)nbc, 1, RS_HIST, 97, redout_region(c, 1), c->st));
     FastRows q{};
     q.rows = p.ny;
     q.in = S;
@@ -645,8 +650,7 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
 }
 
 int run_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
-    if (!s.pad && !s.shift && s.h.kind == H_ASM && !s.hist && s.h.fxoff == 0 && s.h.fyoff == 0 &&
-        !c->no_fast) {
+    if (!s.pad && !s.shift && s.h.kind == H_ASM && s.h.fxoff == 0 && s.h.fyoff == 0 && !c->no_fast) {
         const int rc = try_fast_sweep3(c, p, s);
         if (rc != -1) return rc;
     }
@@ -2250,9 +2254,7 @@ int wos_autotune(wos_ctx c, int ny, int nx, int* row_e, int* col_e, int* col_w) 
         for (int ce : es)
             for (int w = 1; w <= 16; w <<= 1) {
                 if (!fast_supported(c->fp64, nx, re) || !fast_supported(c->fp64, ny, ce)) continue;
-                const int T = ny / ce;
-                const int maxt = (ce >= 16 || c->fp64) ? 512 : 1024;
-                if ((w * T > maxt && w > 1) || fast_col_smem(c->fp64, ny, w) > 220 * 1024) continue;
+                if (fast_col_width(c->fp64, ny, ce, w) != w || fast_col_smem(c->fp64, ny, ce, w) > 220 * 1024) continue;
                 c->tune[key] = Tune{re, ce, w};
                 bool ok = true;
                 for (int it = 0; it < 2 && ok; it++) ok = run_propagate(c, p) == WOS_OK;

@@ -111,7 +111,11 @@ __device__ __forceinline__ void fload(C* v, const C* smb, int tt) {
     }
 }
 
-template <int L, int E, bool INV, int p, int SH, int STR, typename C>
+// All passes from p on.  Each exchange has its own padding period, the radix
+// of the pass that stores (SH = log2 R): for every power-of-two line stride W
+// that makes the store of each pass conflict-free, and the natural-order load
+// of the next pass stays a per-thread base plus immediates.
+template <int L, int E, bool INV, int p, int STR, typename C>
 __device__ __forceinline__ void fpasses(C* v, C* smb, int tt, const C* __restrict__ twp) {
     using PL = FPlan<L, E>;
     if constexpr (p < PL::P) {
@@ -121,13 +125,32 @@ __device__ __forceinline__ void fpasses(C* v, C* smb, int tt, const C* __restric
         fpass<R, E, L, NS, TWOFF, INV>(v, tt, twp);
         if constexpr (p < PL::P - 1) {
             constexpr int R2 = fp_radix(PL::P, PL::RS, E, INV, p + 1);
+            constexpr int SH = Log2<R>::v;
             __syncthreads();
             fstore<R, E, L, NS, SH, STR>(v, smb, tt);
             __syncthreads();
             fload<R2, E, L, SH, STR>(v, smb, tt);
-            fpasses<L, E, INV, p + 1, SH, STR>(v, smb, tt, twp);
+            fpasses<L, E, INV, p + 1, STR>(v, smb, tt, twp);
         }
     }
+}
+
+// padded length of a line: the largest padq over the exchanges of both directions
+__host__ __device__ constexpr int fp_padded_len(int L, int E) {
+    int LG = 0, LE = 0;
+    while ((1 << LG) < L) LG++;
+    while ((1 << LE) < E) LE++;
+    const int P = (LG + LE - 1) / LE;
+    const int RS = (LG % LE) ? (1 << (LG % LE)) : E;
+    int m = L;
+    for (int d = 0; d < 2; d++)
+        for (int p = 0; p < P - 1; p++) {
+            int R = fp_radix(P, RS, E, d == 1, p), sh = 0;
+            while ((1 << sh) < R) sh++;
+            const int len = (L - 1) + ((L - 1) >> sh) + 1;
+            if (len > m) m = len;
+        }
+    return m;
 }
 
 // position of register slot s under the natural mapping of radix R
@@ -137,11 +160,17 @@ __device__ __forceinline__ int fpos(int s, int tt) {
 }
 
 template <typename Real, int E> struct FMaxT { static constexpr int v = (E >= 16 || sizeof(Real) == 8) ? 512 : 1024; };
+// column kernels: 256-thread CTAs for lines of up to 256 threads, three
+// resident per SM for FP32 radix-8 lines (<= 85 registers), two otherwise
+// (<= 128, which 16 complex64 or 8 complex128 values per thread fit without
+// spilling); longer lines keep 512-thread CTAs
+template <typename Real, int L, int E> struct FColB {
+    static constexpr int maxt = (L / E <= 256) ? 256 : 512;
+    static constexpr int minb = (L / E <= 256) ? ((sizeof(Real) == 4 && E == 8) ? 3 : 2) : 1;
+};
 
-constexpr int kRowSH = 4;  // row layout: one pad slot per 16
-constexpr int kColSH = 3;  // column tile: one pad row per 8 (W-interleaved)
-__host__ __device__ constexpr int frow_stride(int L) { return L + (L >> kRowSH) + 2; }
-__host__ __device__ constexpr int fcol_elems(int L, int W) { return W * (L + (L >> kColSH)) + 2; }
+__host__ __device__ constexpr int frow_stride(int L, int E) { return fp_padded_len(L, E) + 2; }
+__host__ __device__ constexpr int fcol_elems(int L, int E, int W) { return W * fp_padded_len(L, E) + 2; }
 
 // ------------------------------------------------------------------- rows
 template <typename Real, int L, int E, bool INV>
@@ -152,7 +181,7 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
     extern __shared__ __align__(16) unsigned char smraw[];
     const int lines = blockDim.x / T;
     const int line = threadIdx.x / T, tt = threadIdx.x - line * T;
-    C* smb = reinterpret_cast<C*>(smraw) + line * frow_stride(L);
+    C* smb = reinterpret_cast<C*>(smraw) + line * frow_stride(L, E);
     const int r = blockIdx.x * lines + line;
     const bool act = r < a.rows;
     const C* twp = reinterpret_cast<const C*>(a.tw);
@@ -183,7 +212,7 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
 #pragma unroll
         for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
     }
-    fpasses<L, E, INV, 0, kRowSH, 1>(v, smb, tt, twp);
+    fpasses<L, E, INV, 0, 1>(v, smb, tt, twp);
     if (act) {
         if (a.out_scale != 1.0) {
 #pragma unroll
@@ -235,13 +264,40 @@ __device__ __forceinline__ double fast_sqrt_d(double s) {
     return fma(0.5 * r0, fma(-y0, y0, s), y0);
 }
 
-template <typename Real, int L, int E>
-__global__ void __launch_bounds__(FMaxT<Real, E>::v) k_cols_fast(const FastCols a) {
+// sqrt of s in [2^-100, 1] to ~1e-13 relative without FP64<->FP32 conversion
+// instructions: the single-precision seed is assembled from the double's bit
+// fields (exponent rebias 1023 -> 127, mantissa truncated to 23 bits), its
+// reciprocal square root is taken in single precision, widened back by the
+// same rebias, and refined by one Newton step in FP64.
+__device__ __forceinline__ double fast_sqrt_bits(double s) {
+    const int hi = __double2hiint(s), lo = __double2loint(s);
+    const float sf = __int_as_float(__funnelshift_l(lo, hi - 0x38000000, 3));
+    const int rb = __float_as_int(rsqrtf(sf));
+    const double r0 = __hiloint2double((rb >> 3) + 0x38000000, (int)((unsigned)rb << 29));
+    const double y0 = s * r0;
+    return fma(0.5 * r0, fma(-y0, y0, s), y0);
+}
+
+// exp(2 pi i t) for |t| < 2^28 revolutions in single precision.  Adding
+// 1.5 * 2^29 rounds t to a multiple of 2^-23 and leaves that multiple, modulo
+// 2^23, in the low mantissa bits; sign-extending 23 of them gives the
+// fractional part in [-1/2, 1/2) as an integer, converted exactly through the
+// 1.5 * 2^23 float pattern, then scaled to radians.
+__device__ __forceinline__ float2 cexp_rev(double t) {
+    const double u = t + 805306368.0;  // 1.5 * 2^29
+    const int s23 = (int)((unsigned)__double2loint(u) << 9) >> 9;
+    const float f = __int_as_float(0x4b400000 + s23) - 12582912.0f;
+    float sn, cs;
+    __sincosf(f * 7.490140565847857e-07f, &sn, &cs);  // 2 pi / 2^23
+    return make_float2(cs, sn);
+}
+
+template <typename Real, int L, int E, int W>
+__global__ void __launch_bounds__(FColB<Real, L, E>::maxt, FColB<Real, L, E>::minb) k_cols_fast(const FastCols a) {
     using C = typename CT<Real>::t;
     using PL = FPlan<L, E>;
     constexpr int T = PL::T;
     extern __shared__ __align__(16) unsigned char smraw[];
-    const int W = a.W;
     const int w = threadIdx.x & (W - 1);
     const int tt = threadIdx.x / W;
     C* smb = reinterpret_cast<C*>(smraw) + w;
@@ -260,12 +316,53 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_cols_fast(const FastCols 
         for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
     }
     // interleaved tile: stride W between consecutive positions of a column
-    switch (W) {
-    case 1: fpasses<L, E, false, 0, kColSH, 1>(v, smb, tt, twp); break;
-    case 2: fpasses<L, E, false, 0, kColSH, 2>(v, smb, tt, twp); break;
-    case 4: fpasses<L, E, false, 0, kColSH, 4>(v, smb, tt, twp); break;
-    case 8: fpasses<L, E, false, 0, kColSH, 8>(v, smb, tt, twp); break;
-    default: fpasses<L, E, false, 0, kColSH, 16>(v, smb, tt, twp); break;
+    fpasses<L, E, false, 0, W>(v, smb, tt, twp);
+
+    // radial histogram of the spectrum (before H) for the alias-wrap check
+    __shared__ double hsm[97];
+    if (a.hist) {
+        double* P = reinterpret_cast<double*>(smraw);  // [q][w], W*L doubles: inside the tile
+        __syncthreads();  // the tile is free once every thread has loaded its last pass
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int q = tt + s * T;
+            P[q * W + w] = act ? (double)v[s].x * v[s].x + (double)v[s].y * v[s].y : 0.0;
+        }
+        for (int k = threadIdx.x; k < 97; k += blockDim.x) hsm[k] = 0;
+        __syncthreads();
+        // |q| = j and L - j share a bin; each warp takes 32 consecutive j of one column
+        constexpr int NJ = (L / 2 + 1 + 31) / 32 * 32;
+        const double fnyq = 1.0 / (2.0 * a.hist_dx);
+        const double den = __dmul_rn((double)L, a.hist_dx);
+        const double dnx = __dmul_rn((double)a.ncols, a.hist_dx);
+        for (int idx = threadIdx.x; idx < W * NJ; idx += blockDim.x) {
+            const int wc = idx / NJ, j = idx - wc * NJ;
+            const int c2 = blockIdx.x * W + wc;
+            double pw = 0;
+            int b = 0;
+            if (j <= L / 2 && c2 < a.ncols) {
+                pw = P[j * W + wc];
+                if (j > 0 && j < L / 2) pw += P[(L - j) * W + wc];
+                const double hfx = (c2 <= a.ncols / 2) ? __ddiv_rn((double)c2, dnx) : __ddiv_rn((double)(c2 - a.ncols), dnx);
+                const double fy = __ddiv_rn((double)j, den);
+                double hp = fabs(hfx), hq = fabs(fy);
+                if (hp < hq) { const double t = hp; hp = hq; hq = t; }
+                double hy = 0;
+                if (hp != 0) {
+                    const double r = __ddiv_rn(hq, hp);
+                    hy = __dmul_rn(hp, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(r, r))));
+                }
+                b = (int)__dmul_rn(__ddiv_rn(hy, fnyq), 96.0);
+                b = b > 96 ? 96 : (b < 0 ? 0 : b);
+            }
+            const int b0 = __shfl_sync(0xffffffffu, b, 0);
+            if (__all_sync(0xffffffffu, b == b0 || pw == 0)) {
+                for (int o = 16; o > 0; o >>= 1) pw += __shfl_down_sync(0xffffffffu, pw, o);
+                if ((threadIdx.x & 31) == 0 && pw != 0) atomicAdd(&hsm[b0], pw);
+            } else if (pw != 0) {
+                atomicAdd(&hsm[b], pw);
+            }
+        }
     }
 
     // transfer function on the radix-E natural mapping: q = tt + s*T
@@ -273,23 +370,32 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_cols_fast(const FastCols 
     double p0 = 0, l1 = 0;
     if constexpr (sizeof(Real) == 4) {
         // FP32 pipeline: FP64 argument kz*sqrt(1 - (wl fx)^2 - (wl fy)^2),
-        // reduced to [-pi, pi] in FP64, sin/cos in single precision
+        // reduced modulo one period in FP64, sin/cos in single precision
         const double fx = (col <= a.ncols / 2 ? (double)col : (double)(col - a.ncols)) / ((double)a.ncols * a.dx);
         const double ax = wl * fx;
         const double cx = fma(-ax, ax, 1.0);
         const double g = wl / ((double)L * a.dx);
+        const double tg = (double)T * g, ay0 = (double)tt * g;
         const float sc = (float)a.scale;
         const float sgn = a.conj ? -1.f : 1.f;
 #pragma unroll
         for (int s = 0; s < E; s++) {
-            const int q = tt + s * T;
-            const double ay = (double)(q <= L / 2 ? q : q - L) * g;
+            // signed position of q = tt + s*T is q - L from s = E/2 on (q = L/2
+            // itself has the same |fy| either way)
+            const double ay = fma((double)(s < E / 2 ? s : s - E), tg, ay0);
             const double sq = fma(-ay, ay, cx);
             float hr, hi;
             double m2 = 1.0;
             if (sq >= 0) {  // rho <= 1: propagating
-                const double sr = sq > 0 ? fast_sqrt_d(sq) : 0.0;
-                __sincosf((float)fast_reduce_2pi_d(a.kz * sr), &hi, &hr);
+                if (a.rev_phase) {
+                    const double sr = sq > 0x1p-100 ? fast_sqrt_bits(sq) : 0.0;
+                    const float2 e = cexp_rev(a.krev * sr);
+                    hr = e.x;
+                    hi = e.y;
+                } else {
+                    const double sr = sq > 0 ? fast_sqrt_d(sq) : 0.0;
+                    __sincosf((float)fast_reduce_2pi_d(a.kz * sr), &hi, &hr);
+                }
             } else {
                 const double decay = a.kaz * sqrt(-sq);
                 double amp;
@@ -357,13 +463,7 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_cols_fast(const FastCols 
         p0 = 0;
         l1 = 0;
     }
-    switch (W) {
-    case 1: fpasses<L, E, true, 0, kColSH, 1>(v, smb, tt, twp); break;
-    case 2: fpasses<L, E, true, 0, kColSH, 2>(v, smb, tt, twp); break;
-    case 4: fpasses<L, E, true, 0, kColSH, 4>(v, smb, tt, twp); break;
-    case 8: fpasses<L, E, true, 0, kColSH, 8>(v, smb, tt, twp); break;
-    default: fpasses<L, E, true, 0, kColSH, 16>(v, smb, tt, twp); break;
-    }
+    fpasses<L, E, true, 0, W>(v, smb, tt, twp);
     if (act) {
         constexpr int RO = PL::RS;
         C* dst = base + (long long)tt * a.ld;
@@ -391,6 +491,11 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_cols_fast(const FastCols 
             o[0] = t0;
             o[1] = t1;
         }
+    }
+    if (a.hist) {
+        __syncthreads();
+        double* o = a.hist + ((long long)blockIdx.y * gridDim.x + blockIdx.x) * a.red_stride;
+        for (int k = threadIdx.x; k < 97; k += blockDim.x) o[k] = hsm[k];
     }
 }
 
@@ -441,8 +546,8 @@ static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
     int lines = 1;
     while (lines * 2 * T <= 256 && lines * 2 <= a.rows) lines *= 2;
     while (lines * T < 32) lines *= 2;
-    const size_t smem = (size_t)frow_stride(L) * lines * sizeof(typename CT<Real>::t);
-    if (smem > 48 * 1024) {
+    const size_t smem = (size_t)frow_stride(L, E) * lines * sizeof(typename CT<Real>::t);
+    if (smem > kSmemNoOptIn) {
         cudaError_t e = cudaFuncSetAttribute(k_rows_fast<Real, L, E, INV>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
@@ -453,22 +558,35 @@ static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
     return cudaGetLastError();
 }
 
-template <typename Real, int L, int E>
-static cudaError_t go_cols(const FastCols& a0, cudaStream_t st, int* nblocks) {
+template <typename Real, int L, int E, int W>
+static cudaError_t go_cols_w(const FastCols& a, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
-    FastCols a = a0;
-    while (a.W * T < 32) a.W *= 2;
-    while (a.W > 1 && a.W * T > FMaxT<Real, E>::v) a.W /= 2;
-    if (a.W > 16) return cudaErrorInvalidConfiguration;
-    const size_t smem = (size_t)fcol_elems(L, a.W) * sizeof(typename CT<Real>::t);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_cols_fast<Real, L, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
+    if constexpr (W * T < 32 || W * T > FColB<Real, L, E>::maxt) {
+        return cudaErrorInvalidConfiguration;
+    } else {
+        const size_t smem = (size_t)fcol_elems(L, E, W) * sizeof(typename CT<Real>::t);
+        if (smem > kSmemNoOptIn) {
+            cudaError_t e = cudaFuncSetAttribute(k_cols_fast<Real, L, E, W>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
+        dim3 grid((a.ncols + W - 1) / W, a.batch > 0 ? a.batch : 1);
+        if (nblocks) *nblocks = (int)grid.x;
+        k_cols_fast<Real, L, E, W><<<grid, W * T, smem, st>>>(a);
+        return cudaGetLastError();
     }
-    dim3 grid((a.ncols + a.W - 1) / a.W, a.batch > 0 ? a.batch : 1);
-    if (nblocks) *nblocks = (int)grid.x;
-    k_cols_fast<Real, L, E><<<grid, a.W * T, smem, st>>>(a);
-    return cudaGetLastError();
+}
+
+template <typename Real, int L, int E>
+static cudaError_t go_cols(const FastCols& a, cudaStream_t st, int* nblocks) {
+    switch (fast_col_width(sizeof(Real) == 8, L, E, a.W)) {
+    case 1: return go_cols_w<Real, L, E, 1>(a, st, nblocks);
+    case 2: return go_cols_w<Real, L, E, 2>(a, st, nblocks);
+    case 4: return go_cols_w<Real, L, E, 4>(a, st, nblocks);
+    case 8: return go_cols_w<Real, L, E, 8>(a, st, nblocks);
+    case 16: return go_cols_w<Real, L, E, 16>(a, st, nblocks);
+    default: return cudaErrorInvalidConfiguration;
+    }
 }
 
 #define WOS_FAST_L(X) X(256) X(512) X(1024) X(2048) X(4096) X(8192)
@@ -477,13 +595,18 @@ cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaS
 #define CASE_R(LL)                                                                                  \
     case LL:                                                                                        \
         if (fp64) {                                                                                 \
-            if (E == 8 && LL <= 4096) return inv ? go_rows<double, LL, 8, true>(a, st, nblocks)     \
-                                                 : go_rows<double, LL, 8, false>(a, st, nblocks);   \
-            if (E == 16 && LL >= 8192) return inv ? go_rows<double, LL, 16, true>(a, st, nblocks)   \
-                                                  : go_rows<double, LL, 16, false>(a, st, nblocks); \
+            if constexpr (LL <= 4096) {                                                             \
+                if (E == 8) return inv ? go_rows<double, LL, 8, true>(a, st, nblocks)               \
+                                       : go_rows<double, LL, 8, false>(a, st, nblocks);             \
+            } else {                                                                                \
+                if (E == 16) return inv ? go_rows<double, LL, 16, true>(a, st, nblocks)             \
+                                        : go_rows<double, LL, 16, false>(a, st, nblocks);           \
+            }                                                                                       \
         } else {                                                                                    \
-            if (E == 8 && LL <= 4096) return inv ? go_rows<float, LL, 8, true>(a, st, nblocks)      \
-                                                 : go_rows<float, LL, 8, false>(a, st, nblocks);    \
+            if constexpr (LL <= 4096) {                                                             \
+                if (E == 8) return inv ? go_rows<float, LL, 8, true>(a, st, nblocks)                \
+                                       : go_rows<float, LL, 8, false>(a, st, nblocks);              \
+            }                                                                                       \
             if (E == 16) return inv ? go_rows<float, LL, 16, true>(a, st, nblocks)                  \
                                     : go_rows<float, LL, 16, false>(a, st, nblocks);                \
         }                                                                                           \
@@ -494,19 +617,38 @@ cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaS
 }
 
 cudaError_t fast_cols(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks) {
-#define CASE_C(LL)                                                                     \
-    case LL:                                                                           \
-        if (fp64) {                                                                    \
-            if (E == 8 && LL <= 4096) return go_cols<double, LL, 8>(a, st, nblocks);   \
-            if (E == 16 && LL >= 8192) return go_cols<double, LL, 16>(a, st, nblocks); \
-        } else {                                                                       \
-            if (E == 8 && LL <= 4096) return go_cols<float, LL, 8>(a, st, nblocks);    \
-            if (E == 16) return go_cols<float, LL, 16>(a, st, nblocks);                \
-        }                                                                              \
+#define CASE_C(LL)                                                                  \
+    case LL:                                                                        \
+        if (fp64) {                                                                 \
+            if constexpr (LL <= 4096) {                                             \
+                if (E == 8) return go_cols<double, LL, 8>(a, st, nblocks);          \
+            } else {                                                                \
+                if (E == 16) return go_cols<double, LL, 16>(a, st, nblocks);        \
+            }                                                                       \
+        } else {                                                                    \
+            if constexpr (LL <= 4096) {                                             \
+                if (E == 8) return go_cols<float, LL, 8>(a, st, nblocks);           \
+            }                                                                       \
+            if (E == 16) return go_cols<float, LL, 16>(a, st, nblocks);             \
+        }                                                                           \
         break;
     switch (L) { WOS_FAST_L(CASE_C) }
 #undef CASE_C
     return cudaErrorNotSupported;
+}
+
+// Columns per CTA actually launched for a requested width W: raised until a CTA
+// holds a full warp, lowered until it fits the kernel's thread bound; 0 if
+// no width fits.
+int fast_col_width(int fp64, int L, int E, int W) {
+    const int T = L / E;
+    const int maxt = (T <= 256) ? 256 : 512;
+    if (W < 1) W = 1;
+    while (W * T < 32) W *= 2;
+    while (W > 1 && W * T > maxt) W /= 2;
+    if (W > 16 || W * T > maxt || W * T < 32) return 0;
+    (void)fp64;
+    return W;
 }
 
 bool fast_supported(int fp64, int L, int E) {
@@ -515,6 +657,6 @@ bool fast_supported(int fp64, int L, int E) {
     return E == 16 || (E == 8 && L <= 4096);
 }
 
-size_t fast_col_smem(int fp64, int L, int W) { return (size_t)fcol_elems(L, W) * (fp64 ? 16 : 8); }
+size_t fast_col_smem(int fp64, int L, int E, int W) { return (size_t)fcol_elems(L, E, W) * (fp64 ? 16 : 8); }
 
 }  // namespace wos

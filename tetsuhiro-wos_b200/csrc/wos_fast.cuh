@@ -26,8 +26,15 @@ struct FastCols {
     double wl, dx, kz, kaz, scale, alpha, limit;
     int zero_ev, reg, backward;
     int conj;             // adjoint: multiply by conj(H)
+    double krev;          // kz / (2 pi): the propagating phase in revolutions
+    int rev_phase;        // FP32: reduce the phase in revolutions (|krev| < 2^28)
     double* red;          // per-CTA [sum |F|^2, sum |F|^2 (1-|H|^2)], or null
     long long red_stride;
+    // radial histogram of |F|^2 for the alias-wrap check (97 bins of
+    // hypot(fx, fy) / f_Nyquist, optics/propagate.go:203-245), per CTA at
+    // hist + block * red_stride, or null
+    double* hist;
+    double hist_dx;
 };
 
 cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaStream_t st, int* nblocks);
@@ -40,5 +47,6 @@ namespace wos {
 // per-pass twiddle tables of the specialised sweeps (forward passes, then inverse)
 int fast_table_len(int L, int E);
 cudaError_t fast_build_twiddles(int fp64, int L, int E, void* out, cudaStream_t st);
-size_t fast_col_smem(int fp64, int L, int W);
+size_t fast_col_smem(int fp64, int L, int E, int W);
+int fast_col_width(int fp64, int L, int E, int W);
 }  // namespace wos

@@ -23,6 +23,12 @@
 
 namespace wos {
 
+// Dynamic shared memory above which a kernel must opt in: the 48 KiB default
+// limit covers dynamic plus static shared memory, and the sweeps keep up to
+// 2 KiB of static reduction scratch.
+constexpr size_t kSmemNoOptIn = 46 * 1024;
+
+
 template <typename R> struct CT;
 template <> struct CT<float> { using t = float2; };
 template <> struct CT<double> { using t = double2; };

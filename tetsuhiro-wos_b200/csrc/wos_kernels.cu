@@ -759,7 +759,7 @@ static cudaError_t launch_rows_t(const RowArgs& a, cudaStream_t st) {
     while (lines * 2 * T <= 256 && lines * 2 <= a.rows) lines *= 2;
     while (lines * T < 32) lines *= 2;  // whole warps (idle lines are inactive)
     const size_t smem = (size_t)row_line_stride(a.L) * lines * sizeof(typename CT<Real>::t);
-    if (smem > 48 * 1024) {
+    if (smem > kSmemNoOptIn) {
         cudaError_t e = cudaFuncSetAttribute(k_rows<Real, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
@@ -778,7 +778,7 @@ static cudaError_t launch_cols_t(const ColArgs& a, cudaStream_t st) {
     while (b.W > 1 && b.W * T > maxt) b.W /= 2;
     if (b.W * T > maxt) return cudaErrorInvalidConfiguration;
     const size_t smem = (size_t)col_tile_elems(b.L, b.W) * sizeof(typename CT<Real>::t);
-    if (smem > 48 * 1024) {
+    if (smem > kSmemNoOptIn) {
         cudaError_t e = cudaFuncSetAttribute(k_cols<Real, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
