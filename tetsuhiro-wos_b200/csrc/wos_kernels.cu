@@ -686,19 +686,42 @@ __global__ void k_bhat_finish(C* df, C* di, const double2* bf, const double2* bi
 // Neumaier-compensated sum of the per-CTA partials of slots [s0, s0+ns) for
 // batch group blockIdx.x (nblocks partials each), one thread per slot, blocks
 // summed in a fixed order (deterministic).
-__global__ void k_reduce_finish(const double* partials, int nblocks, int s0, int ns, double* out) {
-    const int k = threadIdx.x;
-    if (k >= ns) return;
-    const double* p = partials + (long long)blockIdx.x * nblocks * RS_COUNT;
+// Compensated sum of slot s0 + blockIdx.y over the nblocks per-CTA records of
+// batch blockIdx.x.  Each thread keeps a Neumaier pair (sum, compensation)
+// over a fixed stride of records; the pairs are combined in a fixed tree, so
+// the result is deterministic and carries the compensation of every term.
+__device__ __forceinline__ void neumaier_add(double& s, double& c, double x) {
+    const double t = s + x;
+    if (fabs(s) >= fabs(x)) c += (s - t) + x;
+    else c += (x - t) + s;
+    s = t;
+}
+
+__global__ void __launch_bounds__(256) k_reduce_finish(const double* partials, int nblocks, int s0, double* out) {
+    const int k = blockIdx.y;
+    const double* p = partials + (long long)blockIdx.x * nblocks * RS_COUNT + s0 + k;
     double s = 0, c = 0;
-    for (int b = 0; b < nblocks; b++) {
-        const double x = p[(long long)b * RS_COUNT + s0 + k];
-        const double t = s + x;
-        if (fabs(s) >= fabs(x)) c += (s - t) + x;
-        else c += (x - t) + s;
-        s = t;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) neumaier_add(s, c, p[(long long)b * RS_COUNT]);
+    for (int o = 16; o > 0; o >>= 1) {
+        const double s2 = __shfl_down_sync(0xffffffffu, s, o);
+        const double c2 = __shfl_down_sync(0xffffffffu, c, o);
+        c += c2;
+        neumaier_add(s, c, s2);
     }
-    out[(long long)blockIdx.x * RS_COUNT + s0 + k] = s + c;
+    __shared__ double ws[8][2];
+    if ((threadIdx.x & 31) == 0) {
+        ws[threadIdx.x >> 5][0] = s;
+        ws[threadIdx.x >> 5][1] = c;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double ts = 0, tc = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            tc += ws[w][1];
+            neumaier_add(ts, tc, ws[w][0]);
+        }
+        out[(long long)blockIdx.x * RS_COUNT + s0 + k] = ts + tc;
+    }
 }
 
 __global__ void k_convert(int to_c128, const void* src, void* dst, long long n) {
@@ -849,7 +872,8 @@ cudaError_t launch_bhat_finish(int fp64, void* df, void* di, const double2* bf, 
 
 cudaError_t launch_reduce_finish(const double* partials, int nblocks, int nbatch, int s0, int ns,
                                  double* out, cudaStream_t st) {
-    k_reduce_finish<<<nbatch, 128, 0, st>>>(partials, nblocks, s0, ns, out);
+    if (ns <= 0 || nbatch <= 0) return cudaSuccess;
+    k_reduce_finish<<<dim3(nbatch, ns), 256, 0, st>>>(partials, nblocks, s0, out);
     return cudaGetLastError();
 }
 
