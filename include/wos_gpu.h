@@ -157,8 +157,13 @@ WOS_API int wos_ctx_profile(wos_ctx ctx, int kind, double* total_ms, long long* 
 WOS_API int wos_ctx_profile_reset(wos_ctx ctx);
 /* Number of sweep kernels this context has launched since the last reset. */
 WOS_API long long wos_ctx_launch_count(wos_ctx ctx);
-/* The specialised power-of-two ASM sweeps (default on); off forces the general
- * sweeps, which compute the same transform. */
+/* Sweep selection for the power-of-two ASM path, all computing the same
+ * transform: 1 (default) the specialised sweeps, the column sweep (and the
+ * FP64 row sweep) as persistent TMA-pipelined kernels where the layout and
+ * shared memory allow; 3 both row and column sweeps pipelined; 2 the
+ * specialised one-shot kernels only; 0 the general sweeps.  The pipelined kernels bound every wait on a copy; a wait
+ * that expired is reported as WOS_TIMEOUT by the next call that synchronises
+ * (host-buffer entry points, wos_ctx_synchronize). */
 WOS_API int wos_ctx_set_fast_path(wos_ctx ctx, int enabled);
 /* Autotuner of the specialised sweeps (no counterpart in the reference): times
  * every (row elements/thread, column elements/thread, columns/CTA) launch

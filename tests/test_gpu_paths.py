@@ -82,3 +82,82 @@ def test_wrap_histogram_fast_equals_general(prec, n):
     assert rel_l2(res[0][2], res[1][2]) <= tol(prec)
     o = O.Field(ex.copy(), dx)
     assert res[0][0] == O.spectral_radius(o, 0.90)
+
+
+def _dev_propagate(g, prec, ex, ey, dx, z, wl, mode):
+    """propagate_dev on device buffers of the context precision (the layout the
+    pipelined sweeps take), returning the fields and the diagnostics."""
+    import torch
+    g.set_fast_path(mode)
+    dt = torch.complex128 if prec == wos.FP64 else torch.complex64
+    comps = [ex] if ey is None else [ex, ey]
+    buf = torch.from_numpy(np.stack(comps)).to(dt).cuda().contiguous()
+    torch.cuda.synchronize()  # the context's stream does not wait for torch's
+    ny, nx = ex.shape
+    c = wos.Context(wavelength=wl)
+    d = g.propagate_dev(ny, nx, dx, len(comps), buf.data_ptr(), buf.data_ptr(), z, "asm", c, diag=True)
+    g.synchronize()
+    return buf.cpu().numpy().astype(np.complex128), d, c
+
+
+@pytest.mark.parametrize("prec", [wos.FP64, wos.FP32], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("shape", [(256, 256), (512, 512), (1024, 1024), (2048, 2048), (256, 1024), (1024, 256)])
+@pytest.mark.parametrize("ncomp", [1, 2])
+@pytest.mark.parametrize("mode", [1, 3])
+def test_pipelined_equals_one_shot(prec, shape, ncomp, mode):
+    """The persistent TMA-pipelined sweeps (mode 1: columns, mode 3: rows and
+    columns) compute exactly what the one-shot specialised sweeps (mode 2)
+    compute, element for element; the diagnostics differ only in the grouping
+    of their partial sums."""
+    ny, nx = shape
+    dx, wl, z = 2e-6, 632.8e-9, 2e-3
+    rng = np.random.default_rng(ny * 7 + nx + ncomp)
+    ex = np.exp(1j * rng.uniform(0, 2 * np.pi, (ny, nx)))
+    ey = 0.5 * np.exp(1j * rng.uniform(0, 2 * np.pi, (ny, nx))) if ncomp == 2 else None
+    with wos.GPU(prec) as g:
+        a, da, ca = _dev_propagate(g, prec, ex, ey, dx, z, wl, mode)
+        b, db, cb = _dev_propagate(g, prec, ex, ey, dx, z, wl, 2)
+    assert np.array_equal(a, b)
+    p_exact = ny * nx * dx * dx * (1.25 if ncomp == 2 else 1.0)
+    for d in (da, db):
+        assert abs(d.p_in - p_exact) <= 1e-6 * p_exact
+    assert abs(da.p_in - db.p_in) <= 1e-12 * db.p_in
+    assert abs(da.p_out - db.p_out) <= 1e-12 * db.p_out
+    assert ca.warnings.keys() == cb.warnings.keys()
+    if ny == nx <= 512:
+        o = O.Field(ex.copy(), dx)
+        O.propagate(o, z, "asm", O.Context(wavelength=wl))
+        assert rel_l2(a[0], o.ex) <= tol(prec)
+
+
+@pytest.mark.parametrize("prec", [wos.FP64, wos.FP32], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("mode", [1, 3])
+def test_pipelined_wrap_histogram(prec, mode):
+    """The alias-wrap histogram accumulated across the tiles of a persistent
+    column CTA gives the one-shot kernels' spectral radius and warnings."""
+    n, dx, wl = 1024, 2e-6, 632.8e-9
+    z = 3.0 * n * dx * 2 * dx / wl
+    x = (np.arange(n) - n / 2) * dx
+    ex = np.exp(-(x[None, :] ** 2 + x[:, None] ** 2) / (n * dx / 5) ** 2).astype(np.complex128)
+    with wos.GPU(prec) as g:
+        a, da, ca = _dev_propagate(g, prec, ex, None, dx, z, wl, mode)
+        b, db, cb = _dev_propagate(g, prec, ex, None, dx, z, wl, 2)
+    assert da.wrap_checked == 1 and db.wrap_checked == 1
+    assert da.spectral_radius == db.spectral_radius
+    assert ca.warnings.keys() == cb.warnings.keys()
+    assert np.array_equal(a, b)
+
+
+def test_fp32_phase_beyond_revolution_range_uses_general_sweep():
+    """|z / lambda| >= 2^28 revolutions: the FP32 specialised column sweep
+    declines (its exact revolution reduction needs fewer), the general sweep
+    with its FP64 Cody-Waite reduction propagates, and the result still meets
+    the FP32 tolerance against the oracle."""
+    n, dx, wl, z = 256, 40e-6, 500e-9, 150.0  # z / wl = 3e8 > 2^28
+    ex = field(n, 9)
+    o = O.Field(ex.copy(), dx)
+    O.propagate(o, z, "asm", O.Context(wavelength=wl))
+    with wos.GPU(wos.FP32) as g:
+        f = wos.Field(ex.copy(), dx)
+        g.propagate(f, z, "asm", wos.Context(wavelength=wl))
+    assert rel_l2(f.ex, o.ex) <= tol(wos.FP32)

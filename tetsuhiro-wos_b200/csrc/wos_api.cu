@@ -18,6 +18,7 @@
 
 #include "../../include/wos_gpu.h"
 #include "wos_fast.cuh"
+#include "wos_pipe.cuh"
 #include "wos_kernels.cuh"
 
 using namespace wos;
@@ -107,6 +108,9 @@ struct wos_ctx_s {
     size_t hred_n = 0;
     int colw = 0;
     bool no_fast = false;               // force the general sweeps (tests compare both)
+    int sweep_mode = 1;                 // wos_ctx_set_fast_path: 1, 2 or 3 (0 is no_fast)
+    unsigned* err_dev = nullptr;        // error word of the pipelined kernels (device)
+    unsigned* err_host = nullptr;       // pinned mirror, read where the host synchronises
     std::map<long long, Tune> tune;     // autotuned launch configurations
     size_t csz() const { return fp64 ? 16 : 8; }
     // per-launch CUDA-event profile (wos_ctx_set_profiling): a ring of event
@@ -128,6 +132,18 @@ namespace {
 int set_device(wos_ctx c) {
     CK(cudaSetDevice(c->device));
     return WOS_OK;
+}
+
+// The pipelined sweeps bound every wait on a copy; one that expired left a bit
+// in the context's error word.  Read after a synchronisation that copied the
+// word to its pinned mirror; the word is cleared for the calls that follow.
+int check_err_word(wos_ctx c) {
+    const unsigned w = *c->err_host;
+    if (w == 0) return WOS_OK;
+    *c->err_host = 0;
+    cudaMemsetAsync(c->err_dev, 0, sizeof(unsigned), c->st);
+    return fail(WOS_TIMEOUT, "a pipelined sweep gave up waiting for a bulk copy (device error word " +
+                                 std::to_string(w) + "); its output is incomplete");
 }
 
 void prof_fold(wos_ctx c, int slot) {
@@ -529,7 +545,7 @@ Tune get_tune(wos_ctx c, int ny, int nx) {
     Tune t;
     t.rowE = env_int("WOS_ROWE", c->fp64 ? (nx >= 8192 ? 16 : 8) : 16);
     t.colE = env_int("WOS_COLE", c->fp64 ? (ny >= 8192 ? 16 : 8) : 16);
-    t.colW = env_int("WOS_COLW", c->fp64 ? 2 : 4);
+    t.colW = env_int("WOS_COLW", c->fp64 ? 2 : 8);
     if (c->colw > 0) t.colW = c->colw;
     return t;
 }
@@ -561,8 +577,34 @@ int fast_tw(wos_ctx c, Axis* a, int E, const void** out) {
 
 // Plain band-limited ASM on power-of-two grids through the specialised
 // sweeps.  Returns -1 when the grid is not covered (the general sweeps run).
+// One specialised sweep: the pipelined kernel where the sweep mode asks for it
+// and it accepts the layout, else the one-shot kernel; *nb receives the number
+// of per-CTA records.  By default FP32 rows are one-shot (four resident
+// register-bound CTAs beat three pipelined ones), FP64 rows and all columns
+// pipelined where the tile fits two stages.
+cudaError_t sweep_rows(wos_ctx c, int L, int E, bool inv, const FastRows& a, int* nb) {
+    if (c->sweep_mode == 3 || (c->sweep_mode == 1 && c->fp64)) {
+        FastRows b = a;
+        b.err = c->err_dev;
+        const cudaError_t e = pipe_rows(c->fp64, L, E, inv, b, c->st, nb);
+        if (e != cudaErrorNotSupported) return e;
+    }
+    return fast_rows(c->fp64, L, E, inv, a, c->st, nb);
+}
+cudaError_t sweep_cols(wos_ctx c, int L, int E, const FastCols& a, int* nb) {
+    if (c->sweep_mode != 2) {
+        FastCols b = a;
+        b.err = c->err_dev;
+        const cudaError_t e = pipe_cols(c->fp64, L, E, b, c->st, nb);
+        if (e != cudaErrorNotSupported) return e;
+    }
+    return fast_cols(c->fp64, L, E, a, c->st, nb);
+}
+
 int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     if (!is_pow2(p.nx) || !is_pow2(p.ny)) return -1;
+    // the FP32 column sweep reduces the phase in revolutions: |kz / 2 pi| < 2^28
+    if (!c->fp64 && !(std::fabs(s.h.kz / (2 * M_PI)) < 268435456.0)) return -1;
     const Tune t = get_tune(c, p.ny, p.nx);
     if (!fast_supported(c->fp64, p.nx, t.rowE) || !fast_supported(c->fp64, p.ny, t.colE)) return -1;
     Axis *ax, *ay;
@@ -597,8 +639,8 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     r.red = s.red_pin ? red_region(c, 0) + RS_P : nullptr;
     r.red_stride = RS_COUNT;
     r.batch = p.ncomp;
-    CK(timed_launch(c, 0, [&] { return fast_rows(c->fp64, p.nx, t.rowE, false, r, c->st, &nb); }));
-    if (s.red_pin) CK(launch_reduce_finish(red_region(c, 0), (int)nbr, 1, RS_P, 1, redout_region(c, 0), c->st));
+    CK(timed_launch(c, 0, [&] { return sweep_rows(c, p.nx, t.rowE, false, r, &nb); }));
+    if (s.red_pin) CK(launch_reduce_finish(red_region(c, 0), nb, 1, RS_P, 1, redout_region(c, 0), c->st));
     FastCols k{};
     k.ncols = p.nx;
     k.W = t.colW;
@@ -619,16 +661,15 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     k.backward = s.h.z < 0;
     k.conj = s.h.conj;
     k.krev = s.h.kz / (2 * M_PI);
-    k.rev_phase = std::fabs(k.krev) < 268435456.0;  // 2^28 revolutions
     k.red = s.red_loss ? red_region(c, 1) + RS_SW : nullptr;
     k.red_stride = RS_COUNT;
     if (s.hist) {
         k.hist = red_region(c, 1) + RS_HIST;
         k.hist_dx = p.dx;
     }
-    CK(timed_launch(c, 4, [&] { return fast_cols(c->fp64, p.ny, t.colE, k, c->st, &nb); }));
-    if (s.red_loss) CK(launch_reduce_finish(red_region(c, 1), (int)nbc, 1, RS_SW, 2, redout_region(c, 1), c->st));
-    if (s.hist) CK(launch_reduce_finish(red_region(c, 1), (int)nbc, 1, RS_HIST, 97, redout_region(c, 1), c->st));
+    CK(timed_launch(c, 4, [&] { return sweep_cols(c, p.ny, t.colE, k, &nb); }));
+    if (s.red_loss) CK(launch_reduce_finish(red_region(c, 1), nb, 1, RS_SW, 2, redout_region(c, 1), c->st));
+    if (s.hist) CK(launch_reduce_finish(red_region(c, 1), nb, 1, RS_HIST, 97, redout_region(c, 1), c->st));
     FastRows q{};
     q.rows = p.ny;
     q.in = S;
@@ -643,8 +684,8 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     q.red = s.red_pout ? red_region(c, 2) + RS_P : nullptr;
     q.red_stride = RS_COUNT;
     q.batch = p.ncomp;
-    CK(timed_launch(c, 1, [&] { return fast_rows(c->fp64, p.nx, t.rowE, true, q, c->st, &nb); }));
-    if (s.red_pout) CK(launch_reduce_finish(red_region(c, 2), (int)nbr, 1, RS_P, 1, redout_region(c, 2), c->st));
+    CK(timed_launch(c, 1, [&] { return sweep_rows(c, p.nx, t.rowE, true, q, &nb); }));
+    if (s.red_pout) CK(launch_reduce_finish(red_region(c, 2), nb, 1, RS_P, 1, redout_region(c, 2), c->st));
     s.fast = true;
     return WOS_OK;
 }
@@ -1061,8 +1102,9 @@ int stage_out(wos_ctx c, wos_field* f, int ncomp) {
     CK(cudaMemcpyAsync(f->ex, c->stage.p, np * 16, cudaMemcpyDeviceToHost, c->st));
     if (ncomp == 2)
         CK(cudaMemcpyAsync(f->ey, reinterpret_cast<char*>(c->stage.p) + np * 16, np * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(c->err_host, c->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
-    return WOS_OK;
+    return check_err_word(c);
 }
 
 int check_field(const wos_field* f) {
@@ -1185,6 +1227,16 @@ int wos_ctx_create(int device, int precision, wos_ctx* out) {
         return fail(WOS_CUDA_ERROR, std::string("context creation: ") + cudaGetErrorString(e));
     }
     c->own_stream = true;
+    e = cudaMalloc(&c->err_dev, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemset(c->err_dev, 0, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMallocHost(&c->err_host, sizeof(unsigned));
+    if (e != cudaSuccess) {
+        if (c->err_dev) cudaFree(c->err_dev);
+        cudaStreamDestroy(c->st);
+        delete c;
+        return fail(WOS_CUDA_ERROR, std::string("context creation: ") + cudaGetErrorString(e));
+    }
+    *c->err_host = 0;
     *out = c;
     return WOS_OK;
 }
@@ -1209,6 +1261,8 @@ int wos_ctx_destroy(wos_ctx c) {
         for (DevBuf* b : bufs)
             if (b->p) cudaFree(b->p);
         if (c->hred) cudaFreeHost(c->hred);
+        if (c->err_dev) cudaFree(c->err_dev);
+        if (c->err_host) cudaFreeHost(c->err_host);
         if (c->prof_made)
             for (int i = 0; i < wos_ctx_s::kRing; i++) {
                 cudaEventDestroy(c->ev0[i]);
@@ -1285,8 +1339,11 @@ long long wos_ctx_launch_count(wos_ctx c) { return c ? c->launches : -1; }
 
 int wos_ctx_synchronize(wos_ctx c) {
     if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    CK(cudaMemcpyAsync(c->err_host, c->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
-    return WOS_OK;
+    return check_err_word(c);
 }
 
 // ---- FFTs for the remaining fft2D / fft1DAny users
@@ -2207,8 +2264,10 @@ int wos_asm_loss_grad(wos_ctx c, int ny, int nx, double dx, double z, const wos_
 
 int wos_ctx_set_fast_path(wos_ctx c, int enabled) {
     if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    if (enabled < 0 || enabled > 3) return fail(WOS_INVALID_ARG, "fast path mode is 0, 1, 2 or 3");
     std::lock_guard<std::mutex> lk(c->mu);
-    c->no_fast = !enabled;
+    c->no_fast = enabled == 0;
+    c->sweep_mode = enabled == 0 ? 1 : enabled;
     return WOS_OK;
 }
 

@@ -15,162 +15,9 @@
 //   k_cols_fast<Real, L, E>: W adjacent columns per CTA; forward column FFT,
 //       H(fx, fy) of asmTF (optics/propagate.go:159-181) generated on the fly
 //       from an FP64 argument, inverse column FFT, optional spectral loss sums.
-#include <cuda_runtime.h>
-#include <math.h>
-
-#include "wos_fast.cuh"
-#include "wos_fft.cuh"
+#include "wos_fast_dev.cuh"
 
 namespace wos {
-
-template <int N> struct Log2 { static constexpr int v = 1 + Log2<N / 2>::v; };
-template <> struct Log2<1> { static constexpr int v = 0; };
-
-template <int L, int E> struct FPlan {
-    static constexpr int LG = Log2<L>::v, LE = Log2<E>::v;
-    static constexpr int P = (LG + LE - 1) / LE;                 // passes
-    static constexpr int RS = (LG % LE) ? (1 << (LG % LE)) : E;  // the odd radix (E if none)
-    static constexpr int T = L / E;                              // threads per line
-};
-// radix and sub-transform length NS of pass p (forward order (RS, E, ..), inverse reversed)
-__host__ __device__ constexpr int fp_radix(int P, int RS, int E, bool inv, int p) {
-    return inv ? (p == P - 1 ? RS : E) : (p == 0 ? RS : E);
-}
-__host__ __device__ constexpr int fp_ns(int P, int RS, int E, bool inv, int p) {
-    int ns = 1;
-    for (int q = 0; q < p; q++) ns *= fp_radix(P, RS, E, inv, q);
-    return ns;
-}
-// offset of pass p's table: forward passes first, then inverse passes;
-// pass p holds NS*(R-1) entries (pass 0 has NS = 1 and needs none)
-__host__ __device__ constexpr int fp_twoff(int P, int RS, int E, bool inv, int p) {
-    int off = 0;
-    for (int d = 0; d < 2; d++) {
-        const bool dinv = d == 1;
-        for (int q = 1; q < P; q++) {
-            if (dinv == inv && q == p) return off;
-            off += fp_ns(P, RS, E, dinv, q) * (fp_radix(P, RS, E, dinv, q) - 1);
-        }
-    }
-    return off;
-}
-
-// padded slot of position q: one pad slot every 2^SH positions
-template <int SH> __device__ __forceinline__ int padq(int q) { return q + (q >> SH); }
-
-// One Stockham DIT pass, radix R, sub-transform length NS.
-template <int R, int E, int L, int NS, int TWOFF, bool INV, typename C>
-__device__ __forceinline__ void fpass(C* v, int tt, const C* __restrict__ twp) {
-    constexpr int T = L / E;
-#pragma unroll
-    for (int b = 0; b < E / R; b++) {
-        if constexpr (NS > 1) {
-            const int k = (tt + b * T) & (NS - 1);
-            const C* tk = twp + TWOFF + k;
-#pragma unroll
-            for (int r = 1; r < R; r++) {
-                C w = __ldg(tk + (r - 1) * NS);
-                if (INV) w.y = -w.y;
-                v[b * R + r] = cmul(v[b * R + r], w);
-            }
-        }
-        dft<R, INV>(v + b * R);
-    }
-}
-
-// Exchange stores / loads on a line whose element q lives at
-// sm[line_base + STR * padq<SH>(q)] (STR = W for interleaved columns).
-template <int R, int E, int L, int NS, int SH, int STR, typename C>
-__device__ __forceinline__ void fstore(const C* v, C* smb, int tt) {
-    constexpr int T = L / E;
-    static_assert(NS >= (1 << SH) || NS == 1 || NS * R >= (1 << SH), "padding does not commute with this pass");
-#pragma unroll
-    for (int b = 0; b < E / R; b++) {
-        const int j = tt + b * T;
-        const int k = j & (NS - 1);
-        const int base = (j - k) * R + k;
-        int tb;
-        if constexpr (NS >= (1 << SH)) tb = padq<SH>(base);
-        else tb = base + ((base - k) >> SH);
-        C* p = smb + STR * tb;
-#pragma unroll
-        for (int r = 0; r < R; r++) p[STR * (r * NS + ((r * NS) >> SH))] = v[b * R + r];
-    }
-}
-
-template <int R, int E, int L, int SH, int STR, typename C>
-__device__ __forceinline__ void fload(C* v, const C* smb, int tt) {
-    constexpr int T = L / E;
-    constexpr int LR = L / R;
-    static_assert(LR % (1 << SH) == 0, "load stride must be a multiple of the pad period");
-#pragma unroll
-    for (int b = 0; b < E / R; b++) {
-        const C* p = smb + STR * padq<SH>(tt + b * T);
-#pragma unroll
-        for (int r = 0; r < R; r++) v[b * R + r] = p[STR * (r * (LR + (LR >> SH)))];
-    }
-}
-
-// All passes from p on.  Each exchange has its own padding period, the radix
-// of the pass that stores (SH = log2 R): for every power-of-two line stride W
-// that makes the store of each pass conflict-free, and the natural-order load
-// of the next pass stays a per-thread base plus immediates.
-template <int L, int E, bool INV, int p, int STR, typename C>
-__device__ __forceinline__ void fpasses(C* v, C* smb, int tt, const C* __restrict__ twp) {
-    using PL = FPlan<L, E>;
-    if constexpr (p < PL::P) {
-        constexpr int R = fp_radix(PL::P, PL::RS, E, INV, p);
-        constexpr int NS = fp_ns(PL::P, PL::RS, E, INV, p);
-        constexpr int TWOFF = fp_twoff(PL::P, PL::RS, E, INV, p);
-        fpass<R, E, L, NS, TWOFF, INV>(v, tt, twp);
-        if constexpr (p < PL::P - 1) {
-            constexpr int R2 = fp_radix(PL::P, PL::RS, E, INV, p + 1);
-            constexpr int SH = Log2<R>::v;
-            __syncthreads();
-            fstore<R, E, L, NS, SH, STR>(v, smb, tt);
-            __syncthreads();
-            fload<R2, E, L, SH, STR>(v, smb, tt);
-            fpasses<L, E, INV, p + 1, STR>(v, smb, tt, twp);
-        }
-    }
-}
-
-// padded length of a line: the largest padq over the exchanges of both directions
-__host__ __device__ constexpr int fp_padded_len(int L, int E) {
-    int LG = 0, LE = 0;
-    while ((1 << LG) < L) LG++;
-    while ((1 << LE) < E) LE++;
-    const int P = (LG + LE - 1) / LE;
-    const int RS = (LG % LE) ? (1 << (LG % LE)) : E;
-    int m = L;
-    for (int d = 0; d < 2; d++)
-        for (int p = 0; p < P - 1; p++) {
-            int R = fp_radix(P, RS, E, d == 1, p), sh = 0;
-            while ((1 << sh) < R) sh++;
-            const int len = (L - 1) + ((L - 1) >> sh) + 1;
-            if (len > m) m = len;
-        }
-    return m;
-}
-
-// position of register slot s under the natural mapping of radix R
-template <int R, int E, int L>
-__device__ __forceinline__ int fpos(int s, int tt) {
-    return tt + (s / R) * (L / E) + (s % R) * (L / R);
-}
-
-template <typename Real, int E> struct FMaxT { static constexpr int v = (E >= 16 || sizeof(Real) == 8) ? 512 : 1024; };
-// column kernels: 256-thread CTAs for lines of up to 256 threads, three
-// resident per SM for FP32 radix-8 lines (<= 85 registers), two otherwise
-// (<= 128, which 16 complex64 or 8 complex128 values per thread fit without
-// spilling); longer lines keep 512-thread CTAs
-template <typename Real, int L, int E> struct FColB {
-    static constexpr int maxt = (L / E <= 256) ? 256 : 512;
-    static constexpr int minb = (L / E <= 256) ? ((sizeof(Real) == 4 && E == 8) ? 3 : 2) : 1;
-};
-
-__host__ __device__ constexpr int frow_stride(int L, int E) { return fp_padded_len(L, E) + 2; }
-__host__ __device__ constexpr int fcol_elems(int L, int E, int W) { return W * fp_padded_len(L, E) + 2; }
 
 // ------------------------------------------------------------------- rows
 template <typename Real, int L, int E, bool INV>
@@ -202,7 +49,7 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
         } else {
             const C* in = reinterpret_cast<const C*>(a.in) + ib + tt;
 #pragma unroll
-            for (int s = 0; s < E; s++) v[s] = in[fpos<R1, E, L>(s, 0)];
+            for (int s = 0; s < E; s++) v[s] = __ldcs(in + fpos<R1, E, L>(s, 0));
         }
         if (a.red && !INV) {
 #pragma unroll
@@ -246,57 +93,11 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
     }
 }
 
-// ------------------------------------------------------------------- cols
-__device__ __forceinline__ double fast_reduce_2pi_d(double arg) {
-    const double inv2pi = 0.15915494309189533577;
-    const double p2hi = 6.283185307179586232;
-    const double p2lo = 2.4492935982947064e-16;
-    const double n = rint(arg * inv2pi);
-    double r = fma(-n, p2hi, arg);
-    return fma(-n, p2lo, r);
-}
-
-// sqrt of s in (0, 1] to ~1e-14 relative: single-precision reciprocal square
-// root seed refined by one Newton step in FP64 (s in FP32 range here).
-__device__ __forceinline__ double fast_sqrt_d(double s) {
-    const double r0 = (double)rsqrtf((float)s);
-    const double y0 = s * r0;
-    return fma(0.5 * r0, fma(-y0, y0, s), y0);
-}
-
-// sqrt of s in [2^-100, 1] to ~1e-13 relative without FP64<->FP32 conversion
-// instructions: the single-precision seed is assembled from the double's bit
-// fields (exponent rebias 1023 -> 127, mantissa truncated to 23 bits), its
-// reciprocal square root is taken in single precision, widened back by the
-// same rebias, and refined by one Newton step in FP64.
-__device__ __forceinline__ double fast_sqrt_bits(double s) {
-    const int hi = __double2hiint(s), lo = __double2loint(s);
-    const float sf = __int_as_float(__funnelshift_l(lo, hi - 0x38000000, 3));
-    const int rb = __float_as_int(rsqrtf(sf));
-    const double r0 = __hiloint2double((rb >> 3) + 0x38000000, (int)((unsigned)rb << 29));
-    const double y0 = s * r0;
-    return fma(0.5 * r0, fma(-y0, y0, s), y0);
-}
-
-// exp(2 pi i t) for |t| < 2^28 revolutions in single precision.  Adding
-// 1.5 * 2^29 rounds t to a multiple of 2^-23 and leaves that multiple, modulo
-// 2^23, in the low mantissa bits; sign-extending 23 of them gives the
-// fractional part in [-1/2, 1/2) as an integer, converted exactly through the
-// 1.5 * 2^23 float pattern, then scaled to radians.
-__device__ __forceinline__ float2 cexp_rev(double t) {
-    const double u = t + 805306368.0;  // 1.5 * 2^29
-    const int s23 = (int)((unsigned)__double2loint(u) << 9) >> 9;
-    const float f = __int_as_float(0x4b400000 + s23) - 12582912.0f;
-    float sn, cs;
-    __sincosf(f * 7.490140565847857e-07f, &sn, &cs);  // 2 pi / 2^23
-    return make_float2(cs, sn);
-}
-
 template <typename Real, int L, int E, int W>
-__global__ void __launch_bounds__(FColB<Real, L, E>::maxt, FColB<Real, L, E>::minb) k_cols_fast(const FastCols a) {
+__global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, E, W>::minb)
+    k_cols_fast(const FastCols a) {
     using C = typename CT<Real>::t;
     using PL = FPlan<L, E>;
-    constexpr int T = PL::T;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int w = threadIdx.x & (W - 1);
     const int tt = threadIdx.x / W;
@@ -305,12 +106,15 @@ __global__ void __launch_bounds__(FColB<Real, L, E>::maxt, FColB<Real, L, E>::mi
     const bool act = col < a.ncols;
     const C* twp = reinterpret_cast<const C*>(a.tw);
     C* base = reinterpret_cast<C*>(a.data) + (long long)blockIdx.y * a.bstride + col;
+    __shared__ double hsm[97];
+    if (a.hist)
+        for (int k = threadIdx.x; k < 97; k += blockDim.x) hsm[k] = 0;
     C v[E];
     constexpr int R1 = PL::RS;
     if (act) {
         const C* src = base + (long long)tt * a.ld;
 #pragma unroll
-        for (int s = 0; s < E; s++) v[s] = src[(long long)fpos<R1, E, L>(s, 0) * a.ld];
+        for (int s = 0; s < E; s++) v[s] = __ldcs(src + (long long)fpos<R1, E, L>(s, 0) * a.ld);
     } else {
 #pragma unroll
         for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
@@ -318,151 +122,8 @@ __global__ void __launch_bounds__(FColB<Real, L, E>::maxt, FColB<Real, L, E>::mi
     // interleaved tile: stride W between consecutive positions of a column
     fpasses<L, E, false, 0, W>(v, smb, tt, twp);
 
-    // radial histogram of the spectrum (before H) for the alias-wrap check
-    __shared__ double hsm[97];
-    if (a.hist) {
-        double* P = reinterpret_cast<double*>(smraw);  // [q][w], W*L doubles: inside the tile
-        __syncthreads();  // the tile is free once every thread has loaded its last pass
-#pragma unroll
-        for (int s = 0; s < E; s++) {
-            const int q = tt + s * T;
-            P[q * W + w] = act ? (double)v[s].x * v[s].x + (double)v[s].y * v[s].y : 0.0;
-        }
-        for (int k = threadIdx.x; k < 97; k += blockDim.x) hsm[k] = 0;
-        __syncthreads();
-        // |q| = j and L - j share a bin; each warp takes 32 consecutive j of one column
-        constexpr int NJ = (L / 2 + 1 + 31) / 32 * 32;
-        const double fnyq = 1.0 / (2.0 * a.hist_dx);
-        const double den = __dmul_rn((double)L, a.hist_dx);
-        const double dnx = __dmul_rn((double)a.ncols, a.hist_dx);
-        for (int idx = threadIdx.x; idx < W * NJ; idx += blockDim.x) {
-            const int wc = idx / NJ, j = idx - wc * NJ;
-            const int c2 = blockIdx.x * W + wc;
-            double pw = 0;
-            int b = 0;
-            if (j <= L / 2 && c2 < a.ncols) {
-                pw = P[j * W + wc];
-                if (j > 0 && j < L / 2) pw += P[(L - j) * W + wc];
-                const double hfx = (c2 <= a.ncols / 2) ? __ddiv_rn((double)c2, dnx) : __ddiv_rn((double)(c2 - a.ncols), dnx);
-                const double fy = __ddiv_rn((double)j, den);
-                double hp = fabs(hfx), hq = fabs(fy);
-                if (hp < hq) { const double t = hp; hp = hq; hq = t; }
-                double hy = 0;
-                if (hp != 0) {
-                    const double r = __ddiv_rn(hq, hp);
-                    hy = __dmul_rn(hp, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(r, r))));
-                }
-                b = (int)__dmul_rn(__ddiv_rn(hy, fnyq), 96.0);
-                b = b > 96 ? 96 : (b < 0 ? 0 : b);
-            }
-            const int b0 = __shfl_sync(0xffffffffu, b, 0);
-            if (__all_sync(0xffffffffu, b == b0 || pw == 0)) {
-                for (int o = 16; o > 0; o >>= 1) pw += __shfl_down_sync(0xffffffffu, pw, o);
-                if ((threadIdx.x & 31) == 0 && pw != 0) atomicAdd(&hsm[b0], pw);
-            } else if (pw != 0) {
-                atomicAdd(&hsm[b], pw);
-            }
-        }
-    }
-
-    // transfer function on the radix-E natural mapping: q = tt + s*T
-    const double wl = a.wl;
     double p0 = 0, l1 = 0;
-    if constexpr (sizeof(Real) == 4) {
-        // FP32 pipeline: FP64 argument kz*sqrt(1 - (wl fx)^2 - (wl fy)^2),
-        // reduced modulo one period in FP64, sin/cos in single precision
-        const double fx = (col <= a.ncols / 2 ? (double)col : (double)(col - a.ncols)) / ((double)a.ncols * a.dx);
-        const double ax = wl * fx;
-        const double cx = fma(-ax, ax, 1.0);
-        const double g = wl / ((double)L * a.dx);
-        const double tg = (double)T * g, ay0 = (double)tt * g;
-        const float sc = (float)a.scale;
-        const float sgn = a.conj ? -1.f : 1.f;
-#pragma unroll
-        for (int s = 0; s < E; s++) {
-            // signed position of q = tt + s*T is q - L from s = E/2 on (q = L/2
-            // itself has the same |fy| either way)
-            const double ay = fma((double)(s < E / 2 ? s : s - E), tg, ay0);
-            const double sq = fma(-ay, ay, cx);
-            float hr, hi;
-            double m2 = 1.0;
-            if (sq >= 0) {  // rho <= 1: propagating
-                if (a.rev_phase) {
-                    const double sr = sq > 0x1p-100 ? fast_sqrt_bits(sq) : 0.0;
-                    const float2 e = cexp_rev(a.krev * sr);
-                    hr = e.x;
-                    hi = e.y;
-                } else {
-                    const double sr = sq > 0 ? fast_sqrt_d(sq) : 0.0;
-                    __sincosf((float)fast_reduce_2pi_d(a.kz * sr), &hi, &hr);
-                }
-            } else {
-                const double decay = a.kaz * sqrt(-sq);
-                double amp;
-                if (a.zero_ev || (a.limit > 0 && decay > a.limit)) amp = 0;
-                else if (a.backward) amp = a.reg ? exp(decay) / (1.0 + a.alpha * a.alpha * exp(2 * decay)) : exp(decay);
-                else amp = exp(-decay);
-                hr = (float)amp;
-                hi = 0.f;
-                m2 = amp * amp;
-            }
-            if (a.red) {
-                const double pp = (double)v[s].x * v[s].x + (double)v[s].y * v[s].y;
-                p0 += pp;
-                l1 += pp * (1.0 - m2);
-            }
-            v[s] = cmul(v[s], make_float2(hr * sc, sgn * hi * sc));
-        }
-    } else {
-        // FP64 pipeline: the reference's operation sequence, uncontracted
-        const double fxe = (col <= a.ncols / 2) ? __ddiv_rn((double)col, __dmul_rn((double)a.ncols, a.dx))
-                                                : __ddiv_rn((double)(col - a.ncols), __dmul_rn((double)a.ncols, a.dx));
-        const double den = __dmul_rn((double)L, a.dx);
-        const double px = fabs(__dmul_rn(wl, fxe));
-#pragma unroll
-        for (int s = 0; s < E; s++) {
-            const int q = tt + s * T;
-            const double fy = (q <= L / 2) ? __ddiv_rn((double)q, den) : __ddiv_rn((double)(q - L), den);
-            double p = px, qv = fabs(__dmul_rn(wl, fy));
-            if (p < qv) { const double t = p; p = qv; qv = t; }
-            double rho = 0;
-            if (p != 0) {
-                const double qq = __ddiv_rn(qv, p);
-                rho = __dmul_rn(p, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(qq, qq))));
-            }
-            double hr, hi, m2 = 1.0;
-            if (rho <= 1.0) {
-                sincos(__dmul_rn(a.kz, __dsqrt_rn(__dmul_rn(__dsub_rn(1.0, rho), __dadd_rn(1.0, rho)))), &hi, &hr);
-            } else {
-                const double decay = __dmul_rn(a.kaz, __dsqrt_rn(__dmul_rn(__dsub_rn(rho, 1.0), __dadd_rn(rho, 1.0))));
-                double amp;
-                if (a.zero_ev || (a.limit > 0 && decay > a.limit)) amp = 0;
-                else if (a.backward) {
-                    if (a.reg) {
-                        const double e = exp(decay);
-                        amp = __ddiv_rn(e, __dadd_rn(1.0, __dmul_rn(__dmul_rn(__dmul_rn(a.alpha, a.alpha), e), e)));
-                    } else {
-                        amp = exp(decay);
-                    }
-                } else {
-                    amp = exp(-decay);
-                }
-                hr = amp;
-                hi = 0;
-                m2 = amp * amp;
-            }
-            if (a.red) {
-                const double pp = v[s].x * v[s].x + v[s].y * v[s].y;
-                p0 += pp;
-                l1 += pp * (1.0 - m2);
-            }
-            v[s] = cmul(v[s], make_double2(hr * a.scale, (a.conj ? -hi : hi) * a.scale));
-        }
-    }
-    if (!act) {
-        p0 = 0;
-        l1 = 0;
-    }
+    col_spectral_stage<Real, L, E, W>(v, reinterpret_cast<C*>(smraw), hsm, blockIdx.x * W, a, p0, l1);
     fpasses<L, E, true, 0, W>(v, smb, tt, twp);
     if (act) {
         constexpr int RO = PL::RS;
@@ -470,33 +131,7 @@ __global__ void __launch_bounds__(FColB<Real, L, E>::maxt, FColB<Real, L, E>::mi
 #pragma unroll
         for (int s = 0; s < E; s++) dst[(long long)fpos<RO, E, L>(s, 0) * a.ld] = v[s];
     }
-    if (a.red) {
-        __shared__ double rsm[32][2];
-        for (int o = 16; o > 0; o >>= 1) {
-            p0 += __shfl_down_sync(0xffffffffu, p0, o);
-            l1 += __shfl_down_sync(0xffffffffu, l1, o);
-        }
-        if ((threadIdx.x & 31) == 0) {
-            rsm[threadIdx.x >> 5][0] = p0;
-            rsm[threadIdx.x >> 5][1] = l1;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double t0 = 0, t1 = 0;
-            for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
-                t0 += rsm[k][0];
-                t1 += rsm[k][1];
-            }
-            double* o = a.red + ((long long)blockIdx.y * gridDim.x + blockIdx.x) * a.red_stride;
-            o[0] = t0;
-            o[1] = t1;
-        }
-    }
-    if (a.hist) {
-        __syncthreads();
-        double* o = a.hist + ((long long)blockIdx.y * gridDim.x + blockIdx.x) * a.red_stride;
-        for (int k = threadIdx.x; k < 97; k += blockDim.x) o[k] = hsm[k];
-    }
+    col_write_red(a, (long long)blockIdx.y * gridDim.x + blockIdx.x, p0, l1, hsm);
 }
 
 // ------------------------------------------------------------------ tables
@@ -553,7 +188,7 @@ static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
         if (e != cudaSuccess) return e;
     }
     dim3 grid((a.rows + lines - 1) / lines, a.batch > 0 ? a.batch : 1);
-    if (nblocks) *nblocks = (int)grid.x;
+    if (nblocks) *nblocks = (int)(grid.x * grid.y);
     k_rows_fast<Real, L, E, INV><<<grid, lines * T, smem, st>>>(a);
     return cudaGetLastError();
 }
@@ -561,7 +196,7 @@ static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
 template <typename Real, int L, int E, int W>
 static cudaError_t go_cols_w(const FastCols& a, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
-    if constexpr (W * T < 32 || W * T > FColB<Real, L, E>::maxt) {
+    if constexpr (W * T < 32 || W * T > fcol_max_threads(sizeof(Real) == 8, T)) {
         return cudaErrorInvalidConfiguration;
     } else {
         const size_t smem = (size_t)fcol_elems(L, E, W) * sizeof(typename CT<Real>::t);
@@ -571,7 +206,7 @@ static cudaError_t go_cols_w(const FastCols& a, cudaStream_t st, int* nblocks) {
             if (e != cudaSuccess) return e;
         }
         dim3 grid((a.ncols + W - 1) / W, a.batch > 0 ? a.batch : 1);
-        if (nblocks) *nblocks = (int)grid.x;
+        if (nblocks) *nblocks = (int)(grid.x * grid.y);
         k_cols_fast<Real, L, E, W><<<grid, W * T, smem, st>>>(a);
         return cudaGetLastError();
     }
@@ -642,12 +277,11 @@ cudaError_t fast_cols(int fp64, int L, int E, const FastCols& a, cudaStream_t st
 // no width fits.
 int fast_col_width(int fp64, int L, int E, int W) {
     const int T = L / E;
-    const int maxt = (T <= 256) ? 256 : 512;
+    const int maxt = fcol_max_threads(fp64 != 0, T);
     if (W < 1) W = 1;
     while (W * T < 32) W *= 2;
     while (W > 1 && W * T > maxt) W /= 2;
     if (W > 16 || W * T > maxt || W * T < 32) return 0;
-    (void)fp64;
     return W;
 }
 

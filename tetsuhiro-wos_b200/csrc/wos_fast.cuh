@@ -13,6 +13,7 @@ struct FastRows {
     double* red;          // per-CTA sum |E|^2 (record stride red_stride), or null
     long long red_stride;
     int batch;
+    unsigned* err;        // device error word of the pipelined kernels (bit 0: a bounded wait expired)
 };
 
 struct FastCols {
@@ -26,8 +27,7 @@ struct FastCols {
     double wl, dx, kz, kaz, scale, alpha, limit;
     int zero_ev, reg, backward;
     int conj;             // adjoint: multiply by conj(H)
-    double krev;          // kz / (2 pi): the propagating phase in revolutions
-    int rev_phase;        // FP32: reduce the phase in revolutions (|krev| < 2^28)
+    double krev;          // kz / (2 pi): the propagating phase in revolutions (FP32: |krev| < 2^28)
     double* red;          // per-CTA [sum |F|^2, sum |F|^2 (1-|H|^2)], or null
     long long red_stride;
     // radial histogram of |F|^2 for the alias-wrap check (97 bins of
@@ -35,6 +35,7 @@ struct FastCols {
     // hist + block * red_stride, or null
     double* hist;
     double hist_dx;
+    unsigned* err;        // device error word of the pipelined kernels (bit 0: a bounded wait expired)
 };
 
 cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaStream_t st, int* nblocks);

@@ -1,0 +1,475 @@
+// wos_fast_dev.cuh -- device building blocks of the compile-time specialised
+// power-of-two sweeps (pass plan, padded exchanges, transfer function,
+// histogram and loss sums), shared by the one-shot and the pipelined kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "wos_fast.cuh"
+#include "wos_fft.cuh"
+
+namespace wos {
+
+template <int N> struct Log2 { static constexpr int v = 1 + Log2<N / 2>::v; };
+template <> struct Log2<1> { static constexpr int v = 0; };
+
+template <int L, int E> struct FPlan {
+    static constexpr int LG = Log2<L>::v, LE = Log2<E>::v;
+    static constexpr int P = (LG + LE - 1) / LE;                 // passes
+    static constexpr int RS = (LG % LE) ? (1 << (LG % LE)) : E;  // the odd radix (E if none)
+    static constexpr int T = L / E;                              // threads per line
+};
+// radix and sub-transform length NS of pass p (forward order (RS, E, ..), inverse reversed)
+__host__ __device__ constexpr int fp_radix(int P, int RS, int E, bool inv, int p) {
+    return inv ? (p == P - 1 ? RS : E) : (p == 0 ? RS : E);
+}
+__host__ __device__ constexpr int fp_ns(int P, int RS, int E, bool inv, int p) {
+    int ns = 1;
+    for (int q = 0; q < p; q++) ns *= fp_radix(P, RS, E, inv, q);
+    return ns;
+}
+// offset of pass p's table: forward passes first, then inverse passes;
+// pass p holds NS*(R-1) entries (pass 0 has NS = 1 and needs none)
+__host__ __device__ constexpr int fp_twoff(int P, int RS, int E, bool inv, int p) {
+    int off = 0;
+    for (int d = 0; d < 2; d++) {
+        const bool dinv = d == 1;
+        for (int q = 1; q < P; q++) {
+            if (dinv == inv && q == p) return off;
+            off += fp_ns(P, RS, E, dinv, q) * (fp_radix(P, RS, E, dinv, q) - 1);
+        }
+    }
+    return off;
+}
+
+// padded slot of position q: one pad slot every 2^SH positions
+template <int SH> __device__ __forceinline__ int padq(int q) { return q + (q >> SH); }
+
+// Read-only load that asks L1 to keep the line (twiddle tables are re-read by
+// every line of a sweep while the field streams through).
+__device__ __forceinline__ float2 ldg_keep(const float2* p) {
+    float2 r;
+    asm("ld.global.nc.L1::evict_last.v2.f32 {%0, %1}, [%2];" : "=f"(r.x), "=f"(r.y) : "l"(p));
+    return r;
+}
+__device__ __forceinline__ double2 ldg_keep(const double2* p) {
+    double2 r;
+    asm("ld.global.nc.L1::evict_last.v2.f64 {%0, %1}, [%2];" : "=d"(r.x), "=d"(r.y) : "l"(p));
+    return r;
+}
+
+// Twiddles of one Stockham DIT pass (radix R, sub-transform length NS) for
+// this thread's E/R butterflies, [b][r-1]; none when NS == 1.
+template <int R, int E, int L, int NS, int TWOFF, typename C>
+__device__ __forceinline__ void ftw_load(C* w, int tt, const C* __restrict__ twp) {
+    constexpr int T = L / E;
+    if constexpr (NS > 1) {
+#pragma unroll
+        for (int b = 0; b < E / R; b++) {
+            const C* tk = twp + TWOFF + ((tt + b * T) & (NS - 1));
+#pragma unroll
+            for (int r = 1; r < R; r++) w[b * (R - 1) + r - 1] = ldg_keep(tk + (r - 1) * NS);
+        }
+    }
+}
+
+// One Stockham DIT pass on registers, its twiddles already loaded.
+template <int R, int E, int NS, bool INV, typename C>
+__device__ __forceinline__ void fpass_tw(C* v, const C* w) {
+#pragma unroll
+    for (int b = 0; b < E / R; b++) {
+        if constexpr (NS > 1) {
+#pragma unroll
+            for (int r = 1; r < R; r++) {
+                C t = w[b * (R - 1) + r - 1];
+                if (INV) t.y = -t.y;
+                v[b * R + r] = cmul(v[b * R + r], t);
+            }
+        }
+        dft<R, INV>(v + b * R);
+    }
+}
+
+// Exchange stores / loads on a line whose element q lives at
+// sm[line_base + STR * padq<SH>(q)] (STR = W for interleaved columns).
+template <int R, int E, int L, int NS, int SH, int STR, typename C>
+__device__ __forceinline__ void fstore(const C* v, C* smb, int tt) {
+    constexpr int T = L / E;
+    static_assert(NS >= (1 << SH) || NS == 1 || NS * R >= (1 << SH), "padding does not commute with this pass");
+#pragma unroll
+    for (int b = 0; b < E / R; b++) {
+        const int j = tt + b * T;
+        const int k = j & (NS - 1);
+        const int base = (j - k) * R + k;
+        int tb;
+        if constexpr (NS >= (1 << SH)) tb = padq<SH>(base);
+        else tb = base + ((base - k) >> SH);
+        C* p = smb + STR * tb;
+#pragma unroll
+        for (int r = 0; r < R; r++) p[STR * (r * NS + ((r * NS) >> SH))] = v[b * R + r];
+    }
+}
+
+template <int R, int E, int L, int SH, int STR, typename C>
+__device__ __forceinline__ void fload(C* v, const C* smb, int tt) {
+    constexpr int T = L / E;
+    constexpr int LR = L / R;
+    static_assert(LR % (1 << SH) == 0, "load stride must be a multiple of the pad period");
+#pragma unroll
+    for (int b = 0; b < E / R; b++) {
+        const C* p = smb + STR * padq<SH>(tt + b * T);
+#pragma unroll
+        for (int r = 0; r < R; r++) v[b * R + r] = p[STR * (r * (LR + (LR >> SH)))];
+    }
+}
+
+// All passes from p on; wcur holds pass p's twiddles.  Each exchange has its
+// own padding period, the radix of the pass that stores (SH = log2 R): for
+// every power-of-two line stride W that makes the store of each pass
+// conflict-free, and the natural-order load of the next pass stays a
+// per-thread base plus immediates.  The next pass's twiddles are requested
+// once this thread's stores are issued (the data registers are free then), so
+// their latency runs under the barrier.
+template <int L, int E, bool INV, int p, int STR, typename C>
+__device__ __forceinline__ void fpasses_from(C* v, C* smb, int tt, const C* __restrict__ twp, const C* wcur) {
+    using PL = FPlan<L, E>;
+    if constexpr (p < PL::P) {
+        constexpr int R = fp_radix(PL::P, PL::RS, E, INV, p);
+        constexpr int NS = fp_ns(PL::P, PL::RS, E, INV, p);
+        fpass_tw<R, E, NS, INV>(v, wcur);
+        if constexpr (p < PL::P - 1) {
+            constexpr int R2 = fp_radix(PL::P, PL::RS, E, INV, p + 1);
+            constexpr int NS2 = fp_ns(PL::P, PL::RS, E, INV, p + 1);
+            constexpr int TWOFF2 = fp_twoff(PL::P, PL::RS, E, INV, p + 1);
+            constexpr int SH = Log2<R>::v;
+            C wn[(E / R2) * (R2 - 1)];
+            __syncthreads();
+            fstore<R, E, L, NS, SH, STR>(v, smb, tt);
+            ftw_load<R2, E, L, NS2, TWOFF2>(wn, tt, twp);
+            __syncthreads();
+            fload<R2, E, L, SH, STR>(v, smb, tt);
+            fpasses_from<L, E, INV, p + 1, STR>(v, smb, tt, twp, wn);
+        }
+    }
+}
+
+// A whole line transform (the first pass has NS == 1: no twiddles).
+template <int L, int E, bool INV, int p, int STR, typename C>
+__device__ __forceinline__ void fpasses(C* v, C* smb, int tt, const C* __restrict__ twp) {
+    static_assert(p == 0, "a line transform starts at pass 0");
+    fpasses_from<L, E, INV, 0, STR>(v, smb, tt, twp, static_cast<const C*>(nullptr));
+}
+
+// padded length of a line: the largest padq over the exchanges of both directions
+__host__ __device__ constexpr int fp_padded_len(int L, int E) {
+    int LG = 0, LE = 0;
+    while ((1 << LG) < L) LG++;
+    while ((1 << LE) < E) LE++;
+    const int P = (LG + LE - 1) / LE;
+    const int RS = (LG % LE) ? (1 << (LG % LE)) : E;
+    int m = L;
+    for (int d = 0; d < 2; d++)
+        for (int p = 0; p < P - 1; p++) {
+            int R = fp_radix(P, RS, E, d == 1, p), sh = 0;
+            while ((1 << sh) < R) sh++;
+            const int len = (L - 1) + ((L - 1) >> sh) + 1;
+            if (len > m) m = len;
+        }
+    return m;
+}
+
+// position of register slot s under the natural mapping of radix R
+template <int R, int E, int L>
+__device__ __forceinline__ int fpos(int s, int tt) {
+    return tt + (s / R) * (L / E) + (s % R) * (L / R);
+}
+
+template <typename Real, int E> struct FMaxT { static constexpr int v = (E >= 16 || sizeof(Real) == 8) ? 512 : 1024; };
+// Column kernels: a CTA holds W columns of T = L/E threads.  A tile row of W
+// complex64 values is one global-memory segment, so wide tiles (W*8 bytes >=
+// one 32-byte sector) are what keep the strided column access efficient:
+// FP32 CTAs go up to 1024 threads, with three resident per SM at 256 threads
+// (<= 84 registers), two at 512 and one at 1024 (<= 64 registers: the line's
+// values and the transfer function never share the registers, H is applied
+// in shared memory); FP64 CTAs keep 256 threads (two per SM, <= 128 registers) unless a
+// line needs more.
+__host__ __device__ constexpr int fcol_max_threads(bool fp64, int T) { return fp64 ? (T <= 256 ? 256 : 512) : 1024; }
+template <typename Real, int L, int E, int W> struct FColB {
+    static constexpr int threads = W * (L / E);
+    // resident CTAs per SM: FP32 <= 84 registers per thread up to 256 threads
+    // (three 256-thread CTAs), two 512-thread CTAs; FP64 <= 128 registers
+    static constexpr int minb = sizeof(Real) == 4 ? (threads <= 256 ? 65536 / (threads * 84) : 65536 / (threads * 64))
+                                                  : (threads <= 512 ? 65536 / (threads * 128) : 1);
+};
+
+__host__ __device__ constexpr int frow_stride(int L, int E) { return fp_padded_len(L, E) + 2; }
+__host__ __device__ constexpr int fcol_elems(int L, int E, int W) { return W * fp_padded_len(L, E) + 2; }
+
+// ------------------------------------------------------------------- cols
+// sqrt of s in [2^-100, 1] to ~1e-13 relative without FP64<->FP32 conversion
+// instructions: the single-precision seed is assembled from the double's bit
+// fields (exponent rebias 1023 -> 127, mantissa truncated to 23 bits), its
+// reciprocal square root is taken in single precision, widened back by the
+// same rebias, and refined by one Newton step in FP64.
+__device__ __forceinline__ double fast_sqrt_bits(double s) {
+    const int hi = __double2hiint(s), lo = __double2loint(s);
+    const float sf = __int_as_float(__funnelshift_l(lo, hi - 0x38000000, 3));
+    const int rb = __float_as_int(rsqrtf(sf));
+    const double r0 = __hiloint2double((rb >> 3) + 0x38000000, (int)((unsigned)rb << 29));
+    const double y0 = s * r0;
+    return fma(0.5 * r0, fma(-y0, y0, s), y0);
+}
+
+// exp(2 pi i t) for |t| < 2^28 revolutions in single precision.  Adding
+// 1.5 * 2^29 rounds t to a multiple of 2^-23 and leaves that multiple, modulo
+// 2^23, in the low mantissa bits; sign-extending 23 of them gives the
+// fractional part in [-1/2, 1/2) as an integer, converted exactly through the
+// 1.5 * 2^23 float pattern, then scaled to radians.
+__device__ __forceinline__ float2 cexp_rev(double t) {
+    const double u = t + 805306368.0;  // 1.5 * 2^29
+    const int s23 = (int)((unsigned)__double2loint(u) << 9) >> 9;
+    const float f = __int_as_float(0x4b400000 + s23) - 12582912.0f;
+    float sn, cs;
+    __sincosf(f * 7.490140565847857e-07f, &sn, &cs);  // 2 pi / 2^23
+    return make_float2(cs, sn);
+}
+
+// Radial histogram of |F|^2 (the spectrum before H) for the alias-wrap check
+// (spectralRadius, optics/propagate.go:270-310), added into hsm (97 bins,
+// zeroed by the caller) from the W columns held dense in the tile ([q][w]):
+// |q| = j and L - j share a bin; each warp takes 32 consecutive j of one
+// column.  Out of line: it runs only for the alias-wrap check and keeps the
+// unrolled sweep code compact.
+template <typename C>
+__device__ __noinline__ void col_hist_bin(const C* tile, double* hsm, int col0, int L, int W, int ncols,
+                                          double hist_dx) {
+    const int NJ = (L / 2 + 1 + 31) / 32 * 32;
+    const double fnyq = 1.0 / (2.0 * hist_dx);
+    const double den = __dmul_rn((double)L, hist_dx);
+    const double dnx = __dmul_rn((double)ncols, hist_dx);
+    for (int idx = threadIdx.x; idx < W * NJ; idx += blockDim.x) {
+        const int wc = idx / NJ, j = idx - wc * NJ;
+        const int c2 = col0 + wc;
+        double pw = 0;
+        int b = 0;
+        if (j <= L / 2 && c2 < ncols) {
+            const C x = tile[j * W + wc];
+            pw = (double)x.x * x.x + (double)x.y * x.y;
+            if (j > 0 && j < L / 2) {
+                const C y = tile[(L - j) * W + wc];
+                pw += (double)y.x * y.x + (double)y.y * y.y;
+            }
+            const double hfx = (c2 <= ncols / 2) ? __ddiv_rn((double)c2, dnx) : __ddiv_rn((double)(c2 - ncols), dnx);
+            const double fy = __ddiv_rn((double)j, den);
+            double hp = fabs(hfx), hq = fabs(fy);
+            if (hp < hq) { const double t = hp; hp = hq; hq = t; }
+            double hy = 0;
+            if (hp != 0) {
+                const double r = __ddiv_rn(hq, hp);
+                hy = __dmul_rn(hp, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(r, r))));
+            }
+            b = (int)__dmul_rn(__ddiv_rn(hy, fnyq), 96.0);
+            b = b > 96 ? 96 : (b < 0 ? 0 : b);
+        }
+        const int b0 = __shfl_sync(0xffffffffu, b, 0);
+        if (__all_sync(0xffffffffu, b == b0 || pw == 0)) {
+            for (int o = 16; o > 0; o >>= 1) pw += __shfl_down_sync(0xffffffffu, pw, o);
+            if ((threadIdx.x & 31) == 0 && pw != 0) atomicAdd(&hsm[b0], pw);
+        } else if (pw != 0) {
+            atomicAdd(&hsm[b], pw);
+        }
+    }
+}
+
+// Evanescent amplitude of asmTF (optics/propagate.go:168-180) for the FP32
+// pipeline (sq = 1 - rho^2 < 0); out of line, it is rarely taken.
+static __device__ __noinline__ double ev_amp_f(double sq, double kaz, int zero_ev, double limit, int backward, int reg,
+                                        double alpha) {
+    const double decay = kaz * sqrt(-sq);
+    if (zero_ev || (limit > 0 && decay > limit)) return 0;
+    if (backward) return reg ? exp(decay) / (1.0 + alpha * alpha * exp(2 * decay)) : exp(decay);
+    return exp(-decay);
+}
+
+// The same in the reference's operation sequence (FP64 pipeline), rho > 1.
+static __device__ __noinline__ double ev_amp_d(double rho, double kaz, int zero_ev, double limit, int backward, int reg,
+                                        double alpha) {
+    const double decay = __dmul_rn(kaz, __dsqrt_rn(__dmul_rn(__dsub_rn(rho, 1.0), __dadd_rn(rho, 1.0))));
+    if (zero_ev || (limit > 0 && decay > limit)) return 0;
+    if (backward) {
+        if (reg) {
+            const double e = exp(decay);
+            return __ddiv_rn(e, __dadd_rn(1.0, __dmul_rn(__dmul_rn(__dmul_rn(alpha, alpha), e), e)));
+        }
+        return exp(decay);
+    }
+    return exp(-decay);
+}
+
+// H(fx, fy) of asmTF (optics/propagate.go:159-181) times `scale` (conj(H)
+// for the adjoint) and |H|^2, FP32 pipeline: cx = 1 - (wl fx)^2 of the
+// column, ay = wl fy; the FP64 argument kz sqrt(1 - rho^2) is taken in
+// revolutions (|kz / 2 pi| < 2^28, checked by the host) and reduced exactly.
+__device__ __forceinline__ float2 h_f32(const FastCols& a, double cx, double ay, double& m2) {
+    const double sq = fma(-ay, ay, cx);
+    float hr, hi;
+    m2 = 1.0;
+    if (sq >= 0) {  // rho <= 1: propagating
+        const double sr = sq > 0x1p-100 ? fast_sqrt_bits(sq) : 0.0;
+        const float2 e = cexp_rev(a.krev * sr);
+        hr = e.x;
+        hi = e.y;
+    } else {
+        const double amp = ev_amp_f(sq, a.kaz, a.zero_ev, a.limit, a.backward, a.reg, a.alpha);
+        hr = (float)amp;
+        hi = 0.f;
+        m2 = amp * amp;
+    }
+    const float sc = (float)a.scale;
+    return make_float2(hr * sc, (a.conj ? -hi : hi) * sc);
+}
+
+// The same in the FP64 pipeline, with the reference's operation sequence
+// (uncontracted): px = |wl fx| of the column, fy = freq(q).
+__device__ __forceinline__ double2 h_f64(const FastCols& a, double px, double fy, double& m2) {
+    double p = px, qv = fabs(__dmul_rn(a.wl, fy));
+    if (p < qv) { const double t = p; p = qv; qv = t; }
+    double rho = 0;
+    if (p != 0) {
+        const double qq = __ddiv_rn(qv, p);
+        rho = __dmul_rn(p, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(qq, qq))));
+    }
+    double hr, hi;
+    m2 = 1.0;
+    if (rho <= 1.0) {
+        sincos(__dmul_rn(a.kz, __dsqrt_rn(__dmul_rn(__dsub_rn(1.0, rho), __dadd_rn(1.0, rho)))), &hi, &hr);
+    } else {
+        const double amp = ev_amp_d(rho, a.kaz, a.zero_ev, a.limit, a.backward, a.reg, a.alpha);
+        hr = amp;
+        hi = 0;
+        m2 = amp * amp;
+    }
+    return make_double2(hr * a.scale, (a.conj ? -hi : hi) * a.scale);
+}
+
+// Multiply the spectrum of the W columns held dense in the tile ([q][w],
+// W*L values) by H, once per pair (q, L - q): |fy| and so H are the same for
+// both.  Thread (tt, w) takes q = tt + i*T for i < E/2, i.e. q < L/2; the
+// thread with q = 0 also takes the Nyquist row L/2.  p0 += |F|^2 and
+// l1 += |F|^2 (1 - |H|^2) when the loss sums are requested.  Every thread of
+// the CTA calls this between two barriers.
+template <typename Real, int L, int E, int W, typename C>
+__device__ __forceinline__ void col_tile_h(C* tile, int col0, const FastCols& a, double& p0, double& l1) {
+    constexpr int T = L / E;
+    const int w = threadIdx.x & (W - 1);
+    const int tt = threadIdx.x / W;
+    const int col = col0 + w;
+    if (col >= a.ncols) return;  // zero columns stay zero
+    const bool red = a.red != nullptr;
+    auto apply = [&](int q, const C h, double m2) {
+        C x = tile[q * W + w];
+        if (red) {
+            const double pp = (double)x.x * x.x + (double)x.y * x.y;
+            p0 += pp;
+            l1 += pp * (1.0 - m2);
+        }
+        tile[q * W + w] = cmul(x, h);
+    };
+    if constexpr (sizeof(Real) == 4) {
+        const double fx = (col <= a.ncols / 2 ? (double)col : (double)(col - a.ncols)) / ((double)a.ncols * a.dx);
+        const double ax = a.wl * fx;
+        const double cx = fma(-ax, ax, 1.0);
+        const double g = a.wl / ((double)L * a.dx);
+        const double tg = (double)T * g, ay0 = (double)tt * g;
+#pragma unroll
+        for (int i = 0; i < E / 2; i++) {
+            const int q = tt + i * T;
+            double m2;
+            const float2 h = h_f32(a, cx, fma((double)i, tg, ay0), m2);
+            apply(q, h, m2);
+            if (q != 0) apply(L - q, h, m2);
+        }
+        if (tt == 0) {
+            double m2;
+            const float2 h = h_f32(a, cx, (double)(L / 2) * g, m2);
+            apply(L / 2, h, m2);
+        }
+    } else {
+        const double fxe = (col <= a.ncols / 2) ? __ddiv_rn((double)col, __dmul_rn((double)a.ncols, a.dx))
+                                                : __ddiv_rn((double)(col - a.ncols), __dmul_rn((double)a.ncols, a.dx));
+        const double den = __dmul_rn((double)L, a.dx);
+        const double px = fabs(__dmul_rn(a.wl, fxe));
+#pragma unroll
+        for (int i = 0; i < E / 2; i++) {
+            const int q = tt + i * T;
+            double m2;
+            const double2 h = h_f64(a, px, __ddiv_rn((double)q, den), m2);
+            apply(q, h, m2);
+            if (q != 0) apply(L - q, h, m2);
+        }
+        if (tt == 0) {
+            double m2;
+            const double2 h = h_f64(a, px, __ddiv_rn((double)(L / 2), den), m2);
+            apply(L / 2, h, m2);
+        }
+    }
+}
+
+// The column part of one band-limited ASM step on registers v (the tile's
+// forward transform is done, natural order q = tt + s*T): the spectrum goes
+// to the tile, the alias-wrap histogram and H are applied there, and v is
+// reloaded in the natural order of the inverse transform's first pass.
+template <typename Real, int L, int E, int W, typename C>
+__device__ __forceinline__ void col_spectral_stage(C* v, C* tile, double* hsm, int col0, const FastCols& a,
+                                                   double& p0, double& l1) {
+    constexpr int T = L / E;
+    const int w = threadIdx.x & (W - 1);
+    const int tt = threadIdx.x / W;
+    __syncthreads();  // every thread has loaded its last forward pass
+#pragma unroll
+    for (int s = 0; s < E; s++) tile[(tt + s * T) * W + w] = v[s];
+    __syncthreads();
+    if (a.hist) {
+        col_hist_bin(tile, hsm, col0, L, W, a.ncols, a.hist_dx);
+        __syncthreads();
+    }
+    col_tile_h<Real, L, E, W>(tile, col0, a, p0, l1);
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < E; s++) v[s] = tile[(tt + s * T) * W + w];
+}
+
+// Per-CTA record blk of the loss sums [sum |F|^2, sum |F|^2 (1 - |H|^2)] and
+// of the histogram; every thread of the CTA calls this.
+__device__ __forceinline__ void col_write_red(const FastCols& a, long long blk, double p0, double l1,
+                                              const double* hsm) {
+    if (a.red) {
+        __shared__ double rsm[32][2];
+        for (int o = 16; o > 0; o >>= 1) {
+            p0 += __shfl_down_sync(0xffffffffu, p0, o);
+            l1 += __shfl_down_sync(0xffffffffu, l1, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            rsm[threadIdx.x >> 5][0] = p0;
+            rsm[threadIdx.x >> 5][1] = l1;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t0 = 0, t1 = 0;
+            for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
+                t0 += rsm[k][0];
+                t1 += rsm[k][1];
+            }
+            double* o = a.red + blk * a.red_stride;
+            o[0] = t0;
+            o[1] = t1;
+        }
+    }
+    if (a.hist) {
+        __syncthreads();
+        double* o = a.hist + blk * a.red_stride;
+        for (int k = threadIdx.x; k < 97; k += blockDim.x) o[k] = hsm[k];
+    }
+}
+
+}  // namespace wos

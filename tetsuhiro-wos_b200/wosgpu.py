@@ -413,7 +413,10 @@ class GPU:
         return out
 
     # ---- launch configuration
-    def set_fast_path(self, on: bool) -> None:
+    def set_fast_path(self, on) -> None:
+        """0/False: general sweeps; 1/True: specialised sweeps with the column
+        sweep pipelined where the layout allows (default); 2: specialised
+        one-shot sweeps only; 3: row and column sweeps pipelined."""
         _check(lib().wos_ctx_set_fast_path(self.h, int(on)))
 
     def autotune(self, ny: int, nx: int) -> tuple:
