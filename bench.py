@@ -202,6 +202,194 @@ def time_device(g, torch, bufs, steps, warmup, batch, ctx, stream, profile=False
     return e0.elapsed_time(e1), launches, prof
 
 
+
+# ---------------------------------------------------------------------------
+# Secondary configurations of the workload table (one JSON line each):
+#   python bench.py --config {cfg1,cfg2,cfg3,cfg4.1,cfg4.2,cfg4.3,cfg5}
+# Seeded synthetic inputs of the stated shapes stand in for the reference's
+# cases; timed through the library's public entry points with CUDA events on
+# the context's stream (host-buffer entry points include their H2D/D2H); a
+# bounded sample of the FP64 oracle on the host cores gives the CPU figure.
+def _cfg_inputs(name: str):
+    rng = np.random.default_rng(1)
+    if name == "cfg1":
+        n, dx, wl, z = 512, 2e-6, 632.8e-9, 0.05
+        x = (np.arange(n) - n / 2) * dx
+        r2 = x[None, :] ** 2 + x[:, None] ** 2
+        ex = np.exp(-r2 / (200e-6) ** 2) * np.exp(-1j * np.pi * r2 / (wl * 0.2))
+        ex[r2 > (400e-6) ** 2] = 0
+        return dict(ex=ex, dx=dx, wl=wl, z=z, method="asm", evanescent="zero")
+    if name == "cfg2":
+        ny, nx, dx, wl, z = 1000, 1500, 1e-6, 532e-9, 2e-3
+        cells = rng.uniform(0, 1, ((ny + 3) // 4, (nx + 3) // 4))
+        u = np.repeat(np.repeat(cells, 4, axis=0), 4, axis=1)[:ny, :nx]
+        x = (np.arange(nx) - nx / 2) * dx
+        ex = np.exp(2j * np.pi * u) * np.exp(1j * 2 * np.pi / wl * np.sin(np.radians(3)) * x)[None, :]
+        return dict(ex=ex, ey=0.5j * ex, dx=dx, wl=wl, z=z, method="asm_shift_pad")
+    raise ValueError(name)
+
+
+def _algorithmic_bytes(name: str, esz: int) -> float:
+    """Per-run algorithmic bytes of the workload table (complex64: esz = 8)."""
+    k = esz / 8
+    return {"cfg1": 48 * 512 ** 2 * k, "cfg2": 2 * 104 * 1.5e6 * k, "cfg3": 803 * 16 * 1024 ** 2 * k,
+            "cfg4.1": (32 + 64 * 32) * 1024 ** 2 * k, "cfg4.2": 256 * 56 * 512 ** 2 * k,
+            "cfg4.3": 32 * 768 ** 2 * 129 * k, "cfg5": 108 * 2048 ** 2 * k}[name]
+
+
+def run_config(args) -> None:
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O  # noqa: E402  (CPU-baseline leg only)
+    wos = importlib.import_module("tetsuhiro-wos_b200")
+    name = args.config
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    peak, peak_kind = measured_peaks()
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    lines = []
+
+    def timed(fn, steps, warm):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / steps  # s per run
+
+    def cpu(fn, budget=20.0):
+        t0 = time.perf_counter()
+        n = 0
+        while True:
+            fn()
+            n += 1
+            if time.perf_counter() - t0 > budget / 4 or n >= 3:
+                break
+        return (time.perf_counter() - t0) / n
+
+    for prec, pname, esz in ((wos.FP32, "f32", 8), (wos.FP64, "f64", 16)):
+        g = wos.GPU(prec)
+        g.set_stream(stream.cuda_stream)
+        rec = {"precision": pname}
+        if name in ("cfg1", "cfg2"):
+            d = _cfg_inputs(name)
+            ex, ey = d["ex"], d.get("ey")
+            ctxk = dict(wavelength=d["wl"], evanescent=d.get("evanescent", "decay"))
+            ncomp = 1 if ey is None else 2
+            dt = torch.complex128 if prec == wos.FP64 else torch.complex64
+            with torch.cuda.stream(stream):
+                dev = [torch.from_numpy(np.stack([ex] if ey is None else [ex, ey])).to(dt).cuda() for _ in range(8)]
+            torch.cuda.synchronize()
+            ny, nx = ex.shape
+            cnt = [0]
+
+            def dev_run():
+                b = dev[cnt[0] % 8]
+                cnt[0] += 1
+                g.propagate_dev(ny, nx, d["dx"], ncomp, b.data_ptr(), b.data_ptr(), d["z"], d["method"],
+                                wos.Context(warnings_enabled=False, **ctxk))
+            rec["device_s"] = timed(dev_run, args.steps, args.warmup)
+            hf = wos.Field(ex.copy(), d["dx"], None if ey is None else ey.copy())
+            rec["e2e_s"] = timed(lambda: g.propagate(hf, d["z"], d["method"], wos.Context(**ctxk)),
+                                 max(3, args.steps // 5), 2)
+            if prec == wos.FP64:
+                rec_cpu = cpu(lambda: O.propagate(O.Field(ex.copy(), d["dx"], None if ey is None else ey.copy()),
+                                                  d["z"], d["method"], O.Context(**ctxk)))
+        elif name == "cfg3":
+            n, dx, wl, slices, dz = 1024, 0.5e-6, 1.55e-6, 400, 2e-6
+            x = (np.arange(n) - n / 2) * dx
+            ex = np.exp(-((x[None, :] - 5e-6) ** 2 + x[:, None] ** 2) / (8e-6) ** 2).astype(np.complex128)
+            desc = wos.IndexDesc(re_bg=1.45, im_bg=1e-5, core_dn=0.01, core_w=25e-6, zmod_amp=0.1,
+                                 zmod_period=200e-6, border_px=32, border_order=2, border_strength=5e-3)
+            dt = torch.complex128 if prec == wos.FP64 else torch.complex64
+            with torch.cuda.stream(stream):
+                dev = torch.from_numpy(ex).to(dt).cuda()
+            torch.cuda.synchronize()
+            rec["device_s"] = timed(lambda: g.split_step_dev(n, n, dx, 1, dev.data_ptr(), slices * dz, desc, slices,
+                                                             wos.Context(wavelength=wl, warnings_enabled=False)),
+                                    max(2, args.steps // 10), 1)
+            hf = wos.Field(ex.copy(), dx)
+            rec["e2e_s"] = timed(lambda: g.split_step(hf, slices * dz, desc, slices, wos.Context(wavelength=wl)), 2, 1)
+            if prec == wos.FP64:
+                od = O.IndexDesc(re_bg=1.45, im_bg=1e-5, core_dn=0.01, core_w=25e-6, zmod_amp=0.1,
+                                 zmod_period=200e-6, border_px=32, border_order=2, border_strength=5e-3)
+                t0 = time.perf_counter()
+                O.splitstep(O.Field(ex.copy(), dx), 20 * dz, od, 20, O.Context(wavelength=wl))
+                rec_cpu = (time.perf_counter() - t0) * slices / 20  # 20 of 400 slices, scaled
+        elif name == "cfg4.1":
+            n, dx, z = 1024, 2e-6, 0.01
+            x = (np.arange(n) - n / 2) * dx
+            t = (np.cos(2 * np.pi * x / 20e-6) >= np.cos(np.pi * 0.5)).astype(np.float64)
+            ex = np.repeat(t[None, :], n, axis=0).astype(np.complex128)
+            wls = np.linspace(400e-9, 700e-9, 64)
+            hf = wos.Field(ex, dx)
+            rec["e2e_s"] = timed(lambda: g.polychromatic(hf, z, wls, np.ones(64), "asm", wos.Context(wavelength=wls[0])),
+                                 max(2, args.steps // 10), 1)
+            if prec == wos.FP64:
+                t0 = time.perf_counter()
+                O.polychromatic(O.Field(ex.copy(), dx), z, wls[:4], np.ones(4), "asm", O.Context(wavelength=wls[0]))
+                rec_cpu = (time.perf_counter() - t0) * 16  # 4 of 64 wavelengths, scaled
+        elif name == "cfg4.2":
+            n, dx, z, m = 512, 4e-6, 0.01, 256
+            noise = (rng_noise := np.random.default_rng(1)).standard_normal((m, n, n)) / np.sqrt(2) + \
+                1j * rng_noise.standard_normal((m, n, n)) / np.sqrt(2)
+            rec["e2e_s"] = timed(lambda: g.partially_coherent(n, dx, 600e-6, 50e-6, noise, z, "asm",
+                                                               wos.Context(wavelength=632.8e-9)),
+                                 max(2, args.steps // 10), 1)
+            if prec == wos.FP64:
+                t0 = time.perf_counter()
+                modes = O.schell_realizations(n, dx, 600e-6, 50e-6, noise[:8])
+                for k in range(8):
+                    O.propagate(O.Field(modes[k].copy(), dx), z, "asm", O.Context(wavelength=632.8e-9))
+                rec_cpu = (time.perf_counter() - t0) * m / 8  # 8 of 256 modes, scaled
+        elif name == "cfg4.3":
+            n, dx, wl = 768, 4e-6, 632.8e-9
+            x = (np.arange(n) - n / 2) * dx
+            ex = np.exp(-(x[None, :] ** 2 + x[:, None] ** 2) / (300e-6) ** 2).astype(np.complex128)
+            zs = np.linspace(0, 0.01, 128)
+            hf = wos.Field(ex, dx)
+            rec["e2e_s"] = timed(lambda: g.volume(hf, zs, "asm", wos.Context(wavelength=wl)), max(2, args.steps // 10), 1)
+            if prec == wos.FP64:
+                t0 = time.perf_counter()
+                O.propagate3d(O.Field(ex.copy(), dx), zs[:4], "asm", O.Context(wavelength=wl))
+                rec_cpu = (time.perf_counter() - t0) * 32  # 4 of 128 planes, scaled
+        elif name == "cfg5":
+            n, dx, wl, z = 2048, 4e-6, 633e-9, 0.1
+            r = np.random.default_rng(1)
+            phi = r.uniform(0, 2 * np.pi, (n, n))
+            x = (np.arange(n) - n / 2) * dx
+            tgt = np.zeros((n, n))
+            for cx, cy in r.uniform(-0.3, 0.3, (16, 2)) * n * dx:
+                tgt += np.exp(-((x[None, :] - cx) ** 2 + (x[:, None] - cy) ** 2) / (2 * (20e-6) ** 2))
+            a = np.ones((n, n), dtype=np.complex128)
+            rec["e2e_s"] = timed(lambda: g.asm_loss_grad(a, phi, tgt, dx, z, wos.Context(wavelength=wl)),
+                                 max(2, args.steps // 10), 1)
+            if prec == wos.FP64:
+                rec_cpu = cpu(lambda: O.asm_phase_loss_grad(a, phi, tgt, dx, z, O.Context(wavelength=wl)))
+        g.close()
+        lines.append(rec)
+
+    f32, f64 = lines
+    best = f32.get("device_s", f32["e2e_s"])
+    ab = _algorithmic_bytes(name, 8)
+    line = {"metric": f"{name} runs/s (FP32 pipeline; FP64 beside it)", "value": 1.0 / best, "unit": "runs/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": best * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": name, "timing": "device-resident" if "device_s" in f32 else "host API (H2D/D2H included)"},
+            "roofline": {"bound": "hbm", "achieved": ab / best / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": ab / best / 1e9 / peak, "algorithmic_bytes_per_run": ab,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"},
+            "fp32": f32, "fp64": f64,
+            "cpu_baseline": {"value": 1.0 / rec_cpu, "unit": "runs/s", "cores": cores, "kind": "port",
+                             "sample": "FP64 C oracle, bounded sample scaled to one run"}}
+    print(json.dumps(line), flush=True)
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -211,6 +399,8 @@ def main() -> None:
     ap.add_argument("--impl", default="ours")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--config", default="headline",
+                    help="headline (default) or one of cfg1 cfg2 cfg3 cfg4.1 cfg4.2 cfg4.3 cfg5")
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the default (or WOS_ROWE/WOS_COLE/WOS_COLW) launch configuration")
     args = ap.parse_args()
@@ -218,6 +408,9 @@ def main() -> None:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.config != "headline":
+        run_config(args)
         return
 
     import torch
