@@ -312,3 +312,67 @@ def test_adjoint_is_the_adjoint(gpu):
     lhs = np.vdot(ya, ax.ex)
     rhs = np.vdot(ahy.ex, xa)
     assert abs(lhs - rhs) / abs(lhs) <= (1e-12 if gpu.precision == wos.FP64 else 1e-5)
+
+
+def _bpm_dev(g, prec, ex, ey, dx, z, desc, steps, wl, mode):
+    """split_step_dev (no diagnostics: the specialised path is eligible) in sweep mode `mode`."""
+    import torch
+    g.set_fast_path(mode)
+    dt = torch.complex128 if prec == wos.FP64 else torch.complex64
+    comps = [ex] if ey is None else [ex, ey]
+    buf = torch.from_numpy(np.stack(comps)).to(dt).cuda().contiguous()
+    torch.cuda.synchronize()
+    n = ex.shape[0]
+    g.split_step_dev(n, n, dx, len(comps), buf.data_ptr(), z, desc, steps,
+                     wos.Context(wavelength=wl, warnings_enabled=False))
+    g.synchronize()
+    g.set_fast_path(1)
+    return buf.cpu().numpy().astype(np.complex128)
+
+
+@pytest.mark.parametrize("kind", ["uniform", "stratified", "graded", "graded_pol"])
+def test_split_step_specialised_matches_general_and_oracle(gpu, kind):
+    """The specialised split-step (screen inside the row sweep, slice constants
+    applied once, merged half steps as one column step) against the general
+    sweeps and the FP64 oracle."""
+    n, dx, wl = 128, 0.5e-6, 1.55e-6
+    x = (np.arange(n) - n / 2) * dx
+    ex = np.exp(-((x[None, :] - 5e-6) ** 2 + x[:, None] ** 2) / (8e-6) ** 2).astype(complex)
+    ey = 0.5j * ex if kind == "graded_pol" else None
+    if kind == "uniform":
+        od, gd = desc_pair(re_bg=1.45, im_bg=1e-5)
+        steps, z = 8, 16e-6
+    elif kind == "stratified":
+        od, gd = desc_pair(re_bg=1.0, im_bg=2e-5, n_layers=2, layer_z=[6e-6, 14e-6], layer_re=[1.5, 1.2],
+                           layer_im=[0.0, 1e-4])
+        steps, z = 10, 20e-6
+    else:
+        od, gd = desc_pair(re_bg=1.45, im_bg=1e-5, core_dn=0.01, core_x0=2e-6, core_y0=-3e-6, core_w=25e-6,
+                           zmod_amp=0.1, zmod_period=200e-6, zmod_phase=0.3, border_px=16, border_order=2,
+                           border_strength=5e-3)
+        steps, z = 12, 24e-6
+    fast = _bpm_dev(gpu, gpu.precision, ex, ey, dx, z, gd, steps, wl, 1)
+    gen = _bpm_dev(gpu, gpu.precision, ex, ey, dx, z, gd, steps, wl, 0)
+    of = O.Field(ex.copy(), dx, None if ey is None else ey.copy())
+    O.splitstep(of, z, od, steps, O.Context(wavelength=wl))
+    t = tol(gpu.precision) * 10
+    assert rel_l2(fast[0], of.ex) <= t
+    assert rel_l2(fast[0], gen[0]) <= t
+    if ey is not None:
+        assert rel_l2(fast[1], of.ey) <= t
+
+
+def test_split_step_specialised_cfg3_scale(gpu):
+    """1024^2, 400 slices (the BPM workload): the specialised path against the
+    general path in FP64 (both on the GPU; the oracle would take minutes)."""
+    n, dx, wl, steps, dz = 1024, 0.5e-6, 1.55e-6, 400, 2e-6
+    x = (np.arange(n) - n / 2) * dx
+    ex = np.exp(-((x[None, :] - 5e-6) ** 2 + x[:, None] ** 2) / (8e-6) ** 2).astype(complex)
+    _, gd = desc_pair(re_bg=1.45, im_bg=1e-5, core_dn=0.01, core_w=25e-6, zmod_amp=0.1, zmod_period=200e-6,
+                      border_px=32, border_order=2, border_strength=5e-3)
+    fast = _bpm_dev(gpu, gpu.precision, ex, None, dx, steps * dz, gd, steps, wl, 1)
+    with wos.GPU(wos.FP64) as g64:
+        ref = _bpm_dev(g64, wos.FP64, ex, None, dx, steps * dz, gd, steps, wl, 0)
+    err = rel_l2(fast[0], ref[0])
+    print("cfg3 rel-L2 vs FP64 general:", err)
+    assert err <= (1e-11 if gpu.precision == wos.FP64 else 1e-4)

@@ -1504,6 +1504,130 @@ void fill_screen(ScreenArgs& s, const ScreenSrc& src, int slice, long long np, d
 // The power around every ASM half step (for the evanescent_filtered /
 // backward_* warnings of each Propagate(dz/2) call) comes from Parseval sums in
 // the column pass, one finished record per pass.
+// Split-step BPM on the specialised sweeps: A(dz/2) M A(dz) M ... A(dz/2) with
+// the column sweeps of the fused ASM (the merged half steps A(dz/2)^2 are one
+// step A(dz): forward steps without an evanescent limit only) and the slice
+// screens inside the row sweeps (k_rows_bpm_fast).  The screen of a
+// parametric medium factorises as c_s * border(d) * exp(i p_s gx(x) gy(y)):
+// the slice constants c_s = exp(-k dz Im n0) exp(i k dz (Re n0 - 1)) are
+// multiplied in FP64 on the host and applied once in the last sweep.
+// Returns -1 when the case is not eligible (the general path then runs).
+int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* in, int in_c128, void* out,
+                       int out_c128, double z, const ScreenSrc& src, int steps, const wos_context& cc, bool diag) {
+    if (diag || c->no_fast || src.kind != 1 || !is_pow2(nx) || !is_pow2(ny) || !(z > 0)) return -1;
+    const double dz = z / (double)steps, hz = dz / 2;
+    const double k = 2 * M_PI / cc.wavelength;
+    const Policy pol = ev_policy(cc, hz);
+    if (pol.limit > 0 || pol.reg) return -1;
+    if (!c->fp64 && !(std::fabs(k * dz / (2 * M_PI)) < 268435456.0)) return -1;
+    const Tune t = get_tune(c, ny, nx);
+    if (!fast_supported(c->fp64, nx, t.rowE) || !fast_supported(c->fp64, ny, t.colE)) return -1;
+    const wos_index_desc& d = src.desc;
+    Axis *ax, *ay;
+    TRY(get_axis(c, nx, c->fp64, &ax));
+    TRY(get_axis(c, ny, c->fp64, &ay));
+    const void *twx, *twy;
+    TRY(fast_tw(c, ax, t.rowE, &twx));
+    TRY(fast_tw(c, ay, t.colE, &twy));
+    const long long np = (long long)ny * nx;
+    void* S;
+    if (!out_c128) {
+        S = out;
+    } else {
+        TRY(ensure(c->scratch, (size_t)np * ncomp * c->csz()));
+        S = c->scratch.p;
+    }
+    // per-run tables: gx of the graded core and the border absorption
+    const bool core = d.core_dn != 0;
+    const int bpx = (d.border_px > 0 && d.border_strength != 0) ? d.border_px : 0;
+    TRY(ensure(c->params, sizeof(double) * ((size_t)nx + (size_t)bpx + 1)));
+    std::vector<double> tab((size_t)nx + (size_t)bpx);
+    for (int i = 0; i < nx; i++) {
+        const double x = ((double)i - (double)nx / 2) * dx - d.core_x0;
+        tab[i] = core ? std::exp(-(x * x) / (d.core_w * d.core_w)) : 0.0;
+    }
+    for (int q = 0; q < bpx; q++) {
+        double p = 1;
+        const double tq = (double)(bpx - q) / (double)bpx;
+        for (int o = 0; o < d.border_order; o++) p *= tq;
+        tab[(size_t)nx + q] = std::exp(-k * d.border_strength * p * dz);
+    }
+    CK(cudaMemcpyAsync(c->params.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, c->st));
+    const double* gx = reinterpret_cast<const double*>(c->params.p);
+    int nb = 0;
+    FastRows r{};
+    r.rows = ny;
+    r.in = in;
+    r.in_c128 = in_c128;
+    r.in_ld = nx;
+    r.in_bstride = np;
+    r.out = S;
+    r.out_ld = nx;
+    r.out_bstride = np;
+    r.tw = twx;
+    r.out_scale = 1.0;
+    r.batch = ncomp;
+    CK(timed_launch(c, 0, [&] { return fast_rows(c->fp64, nx, t.rowE, false, r, c->st, &nb); }));
+    FastCols kc{};
+    kc.ncols = nx;
+    kc.W = t.colW;
+    kc.data = S;
+    kc.ld = nx;
+    kc.bstride = np;
+    kc.tw = twy;
+    kc.batch = ncomp;
+    kc.wl = cc.wavelength;
+    kc.dx = dx;
+    kc.scale = 1.0 / ((double)nx * (double)ny);
+    kc.zero_ev = pol.zero;
+    kc.precise_phase = 1;
+    FastRows m = r;
+    m.in = S;
+    m.in_c128 = 0;
+    m.bpm_gx = core ? gx : nullptr;
+    m.bpm_y0 = d.core_y0;
+    m.bpm_w2 = d.core_w * d.core_w;
+    m.bpm_dx = dx;
+    m.bpm_border = bpx ? gx + nx : nullptr;
+    m.bpm_border_px = bpx;
+    m.bpm_nx = nx;
+    double c_logamp = 0, c_phase = 0;  // product of the slice constants
+    for (int s = 0; s <= steps; s++) {
+        const double zp = (s == 0 || s == steps) ? hz : dz;
+        kc.kz = k * zp;
+        kc.kaz = k * zp;
+        kc.krev = kc.kz / (2 * M_PI);
+        CK(timed_launch(c, 4, [&] { return sweep_cols(c, ny, t.colE, kc, &nb); }));
+        if (s < steps) {
+            const double zc = z * (double)s / (double)steps + dz / 2;
+            double r0 = d.re_bg, i0 = d.im_bg;
+            for (int q = 0; q < d.n_layers && q < 8; q++)
+                if (zc < d.layer_z[q]) {
+                    r0 = d.layer_re[q];
+                    i0 = d.layer_im[q];
+                    break;
+                }
+            double mod = 1;
+            if (d.zmod_amp != 0) mod = 1.0 + d.zmod_amp * std::sin(2 * M_PI * zc / d.zmod_period + d.zmod_phase);
+            m.bpm_phase = k * d.core_dn * mod * dz;
+            c_phase += k * (r0 - 1.0) * dz;
+            c_logamp += -k * i0 * dz;
+            CK(timed_launch(c, 0, [&] { return fast_rows_bpm(c->fp64, nx, t.rowE, m, c->st, &nb); }));
+        }
+    }
+    FastRows q = r;
+    q.in = S;
+    q.in_c128 = 0;
+    q.out = out;
+    q.out_c128 = out_c128;
+    const double ca = std::exp(c_logamp), cp = std::remainder(c_phase, 2 * M_PI);
+    q.out_scale = ca * std::cos(cp);
+    q.out_scale_im = ca * std::sin(cp);
+    if (q.out_scale_im == 0.0 && q.out_scale == 1.0) q.out_scale_im = 0.0;
+    CK(timed_launch(c, 1, [&] { return fast_rows(c->fp64, nx, t.rowE, true, q, c->st, &nb); }));
+    return WOS_OK;
+}
+
 int run_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* in, int in_c128, void* out,
                   int out_c128, double z, const ScreenSrc& src, int steps, const wos_context& cc, wos_diag* d) {
     if (d) {
@@ -1518,6 +1642,11 @@ int run_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* i
     }
     if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
     if (steps <= 0) steps = 1;
+    {
+        const int rc = try_fast_splitstep(c, ny, nx, dx, ncomp, in, in_c128, out, out_c128, z, src, steps, cc,
+                                          d != nullptr);
+        if (rc != -1) return rc;
+    }
     const double dz = z / (double)steps;
     const double k = 2 * M_PI / cc.wavelength;
     const double hz = dz / 2;

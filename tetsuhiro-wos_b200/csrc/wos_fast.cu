@@ -61,7 +61,11 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
     }
     fpasses<L, E, INV, 0, 1>(v, smb, tt, twp);
     if (act) {
-        if (a.out_scale != 1.0) {
+        if (a.out_scale_im != 0.0) {
+            const C cs = mkc<C>((Real)a.out_scale, (Real)a.out_scale_im);
+#pragma unroll
+            for (int s = 0; s < E; s++) v[s] = cmul(v[s], cs);
+        } else if (a.out_scale != 1.0) {
 #pragma unroll
             for (int s = 0; s < E; s++) v[s] = cscale(v[s], (Real)a.out_scale);
         }
@@ -90,6 +94,64 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
             for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += rsm[w];
             a.red[((long long)blockIdx.y * gridDim.x + blockIdx.x) * a.red_stride] = t;
         }
+    }
+}
+
+// One split-step slice on a row (optics/medium.go:50-65 for the screen): the
+// inverse row transform, the screen t(x, y) = border[d] exp(i phase gx gy) at
+// the inverse's natural output positions, which are the forward transform's
+// natural input positions (radix rs both), and the forward row transform, all
+// in registers.  The screen is evaluated in FP64 in both pipelines.
+template <typename Real, int L, int E>
+__global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_bpm_fast(const FastRows a) {
+    using C = typename CT<Real>::t;
+    using PL = FPlan<L, E>;
+    constexpr int T = PL::T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int lines = blockDim.x / T;
+    const int line = threadIdx.x / T, tt = threadIdx.x - line * T;
+    C* smb = reinterpret_cast<C*>(smraw) + line * frow_stride(L, E);
+    const int r = blockIdx.x * lines + line;
+    const bool act = r < a.rows;
+    const C* twp = reinterpret_cast<const C*>(a.tw);
+    const long long ib = (long long)blockIdx.y * a.in_bstride + (long long)r * a.in_ld;
+    const long long ob = (long long)blockIdx.y * a.out_bstride + (long long)r * a.out_ld;
+    C v[E];
+    if (act) {
+        const C* in = reinterpret_cast<const C*>(a.in) + ib + tt;
+#pragma unroll
+        for (int s = 0; s < E; s++) v[s] = __ldcs(in + fpos<E, E, L>(s, 0));
+    } else {
+#pragma unroll
+        for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
+    }
+    fpasses<L, E, true, 0, 1>(v, smb, tt, twp);
+    if (act) {
+        const double y = ((double)r - (double)a.rows / 2) * a.bpm_dx;
+        const double gy = a.bpm_gx ? exp(-((y - a.bpm_y0) * (y - a.bpm_y0)) / a.bpm_w2) : 0.0;
+        const double pg = a.bpm_phase * gy;
+        const int dr = min(r, a.rows - 1 - r);
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int q = fpos<PL::RS, E, L>(s, tt);
+            double sn = 0, cs = 1;
+            if (a.bpm_gx) sincos(pg * __ldg(a.bpm_gx + q), &sn, &cs);
+            if (a.bpm_border) {
+                const int d = min(dr, min(q, a.bpm_nx - 1 - q));
+                if (d < a.bpm_border_px) {
+                    const double b = __ldg(a.bpm_border + d);
+                    sn *= b;
+                    cs *= b;
+                }
+            }
+            v[s] = cmul(v[s], mkc<C>((Real)cs, (Real)sn));
+        }
+    }
+    fpasses<L, E, false, 0, 1>(v, smb, tt, twp);
+    if (act) {
+        C* out = reinterpret_cast<C*>(a.out) + ob + tt;
+#pragma unroll
+        for (int s = 0; s < E; s++) out[fpos<E, E, L>(s, 0)] = v[s];
     }
 }
 
@@ -193,6 +255,24 @@ static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
     return cudaGetLastError();
 }
 
+template <typename Real, int L, int E>
+static cudaError_t go_rows_bpm(const FastRows& a, cudaStream_t st, int* nblocks) {
+    constexpr int T = L / E;
+    int lines = 1;
+    while (lines * 2 * T <= 256 && lines * 2 <= a.rows) lines *= 2;
+    while (lines * T < 32) lines *= 2;
+    const size_t smem = (size_t)frow_stride(L, E) * lines * sizeof(typename CT<Real>::t);
+    if (smem > kSmemNoOptIn) {
+        cudaError_t e = cudaFuncSetAttribute(k_rows_bpm_fast<Real, L, E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((a.rows + lines - 1) / lines, a.batch > 0 ? a.batch : 1);
+    if (nblocks) *nblocks = (int)(grid.x * grid.y);
+    k_rows_bpm_fast<Real, L, E><<<grid, lines * T, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
 template <typename Real, int L, int E, int W>
 static cudaError_t go_cols_w(const FastCols& a, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
@@ -283,6 +363,27 @@ int fast_col_width(int fp64, int L, int E, int W) {
     while (W > 1 && W * T > maxt) W /= 2;
     if (W > 16 || W * T > maxt || W * T < 32) return 0;
     return W;
+}
+
+cudaError_t fast_rows_bpm(int fp64, int L, int E, const FastRows& a, cudaStream_t st, int* nblocks) {
+#define CASE_B(LL)                                                                   \
+    case LL:                                                                         \
+        if (fp64) {                                                                  \
+            if constexpr (LL <= 4096) {                                              \
+                if (E == 8) return go_rows_bpm<double, LL, 8>(a, st, nblocks);       \
+            } else {                                                                 \
+                if (E == 16) return go_rows_bpm<double, LL, 16>(a, st, nblocks);     \
+            }                                                                        \
+        } else {                                                                     \
+            if constexpr (LL <= 4096) {                                              \
+                if (E == 8) return go_rows_bpm<float, LL, 8>(a, st, nblocks);        \
+            }                                                                        \
+            if (E == 16) return go_rows_bpm<float, LL, 16>(a, st, nblocks);          \
+        }                                                                            \
+        break;
+    switch (L) { WOS_FAST_L(CASE_B) }
+#undef CASE_B
+    return cudaErrorNotSupported;
 }
 
 bool fast_supported(int fp64, int L, int E) {

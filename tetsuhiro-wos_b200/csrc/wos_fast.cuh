@@ -14,6 +14,18 @@ struct FastRows {
     long long red_stride;
     int batch;
     unsigned* err;        // device error word of the pipelined kernels (bit 0: a bounded wait expired)
+    double out_scale_im;  // imaginary part of the output scale (complex scale when non-zero)
+    // split-step slice screen between an inverse and a forward row transform
+    // (k_rows_bpm_fast): t = border[d] * exp(i phase gx[x] gy(y)), the
+    // constant part of the slice (background index, interior absorption) being
+    // applied once per run by the caller
+    const double* bpm_gx;     // exp(-(x - x0)^2 / w^2) per column, or null (no graded core)
+    double bpm_y0, bpm_w2;    // row factor gy = exp(-(y - y0)^2 / w^2)
+    double bpm_dx;            // pixel pitch (y = (r - ny/2) dx)
+    double bpm_phase;         // k dz core_dn (1 + zmod_amp sin(2 pi zc / period + phase))
+    const double* bpm_border; // exp(-k dz strength ((px - d)/px)^order) for edge distance d < px, or null
+    int bpm_border_px;
+    int bpm_nx;               // grid width (edge distance)
 };
 
 struct FastCols {
@@ -28,6 +40,7 @@ struct FastCols {
     int zero_ev, reg, backward;
     int conj;             // adjoint: multiply by conj(H)
     double krev;          // kz / (2 pi): the propagating phase in revolutions (FP32: |krev| < 2^28)
+    int precise_phase;    // FP32: sin/cos of the phase to ~1 ulp (repeated application, e.g. split-step)
     double* red;          // per-CTA [sum |F|^2, sum |F|^2 (1-|H|^2)], or null
     long long red_stride;
     // radial histogram of |F|^2 for the alias-wrap check (97 bins of
@@ -40,6 +53,9 @@ struct FastCols {
 
 cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaStream_t st, int* nblocks);
 cudaError_t fast_cols(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks);
+// One split-step slice on rows: inverse transform, slice screen, forward
+// transform (native precision in and out, in place allowed).
+cudaError_t fast_rows_bpm(int fp64, int L, int E, const FastRows& a, cudaStream_t st, int* nblocks);
 bool fast_supported(int fp64, int L, int E);
 
 }  // namespace wos

@@ -224,13 +224,17 @@ __device__ __forceinline__ double fast_sqrt_bits(double s) {
 // 1.5 * 2^29 rounds t to a multiple of 2^-23 and leaves that multiple, modulo
 // 2^23, in the low mantissa bits; sign-extending 23 of them gives the
 // fractional part in [-1/2, 1/2) as an integer, converted exactly through the
-// 1.5 * 2^23 float pattern, then scaled to radians.
-__device__ __forceinline__ float2 cexp_rev(double t) {
+// 1.5 * 2^23 float pattern.  `precise` evaluates sin/cos of that exact fraction
+// to about 1 ulp (sincospif, for transfer functions applied hundreds of times,
+// whose errors add up); otherwise the hardware approximation (absolute error
+// about 2^-21) serves a single application.
+__device__ __forceinline__ float2 cexp_rev(double t, bool precise) {
     const double u = t + 805306368.0;  // 1.5 * 2^29
     const int s23 = (int)((unsigned)__double2loint(u) << 9) >> 9;
     const float f = __int_as_float(0x4b400000 + s23) - 12582912.0f;
     float sn, cs;
-    __sincosf(f * 7.490140565847857e-07f, &sn, &cs);  // 2 pi / 2^23
+    if (precise) sincospif(f * 2.384185791015625e-07f, &sn, &cs);  // 2^-22: half-revolutions
+    else __sincosf(f * 7.490140565847857e-07f, &sn, &cs);            // 2 pi / 2^23
     return make_float2(cs, sn);
 }
 
@@ -316,7 +320,7 @@ __device__ __forceinline__ float2 h_f32(const FastCols& a, double cx, double ay,
     m2 = 1.0;
     if (sq >= 0) {  // rho <= 1: propagating
         const double sr = sq > 0x1p-100 ? fast_sqrt_bits(sq) : 0.0;
-        const float2 e = cexp_rev(a.krev * sr);
+        const float2 e = cexp_rev(a.krev * sr, a.precise_phase != 0);
         hr = e.x;
         hi = e.y;
     } else {
