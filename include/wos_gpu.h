@@ -246,6 +246,14 @@ WOS_API int wos_asm_forward_loss(wos_ctx ctx, int ny, int nx, double dx, double 
 WOS_API int wos_asm_loss_grad(wos_ctx ctx, int ny, int nx, double dx, double z, const wos_context* c,
                       const wos_c128* a, const double* phi, const double* target, double* loss,
                       double* grad);
+/* Device-resident form of wos_asm_loss_grad for optimisation loops that keep
+ * the design on the GPU: a is a device [ny][nx] array of the context's complex
+ * type, phi and target device FP64 arrays, grad a device FP64 array (or NULL
+ * for the loss alone); the loss is returned to the host.  Power-of-two ny, nx
+ * from 256 to 8192 (else WOS_UNSUPPORTED_SIZE). */
+WOS_API int wos_asm_loss_grad_dev(wos_ctx ctx, int ny, int nx, double dx, double z, const wos_context* c,
+                                  const void* a, const double* phi, const double* target, double* loss,
+                                  double* grad);
 /* Adjoint operator A^H = F^-1 diag(conj H) F of an ASM step, host field in place. */
 WOS_API int wos_asm_adjoint(wos_ctx ctx, wos_field* f, double z, const wos_context* c);
 

@@ -376,3 +376,56 @@ def test_split_step_specialised_cfg3_scale(gpu):
     err = rel_l2(fast[0], ref[0])
     print("cfg3 rel-L2 vs FP64 general:", err)
     assert err <= (1e-11 if gpu.precision == wos.FP64 else 1e-4)
+
+
+def test_design_specialised_path_matches_oracle_general_and_fd(gpu):
+    """Power-of-two grids take the five-sweep inverse-design path (residual
+    and gradient inside the row sweeps): loss and gradient against the FP64
+    oracle and the general sweeps, and the gradient against central finite
+    differences of the oracle's forward on 16 pixels."""
+    n, dx, wl, z = 256, 4e-6, 633e-9, 5e-3
+    a, phi, T = _design(n, 3)
+    ctx = O.Context(wavelength=wl)
+    lo, go = O.asm_phase_loss_grad(a, phi, T, dx, z, ctx)
+    lf, gf = gpu.asm_loss_grad(a, phi, T, dx, z, wos.Context(wavelength=wl))
+    gpu.set_fast_path(0)
+    lg, gg = gpu.asm_loss_grad(a, phi, T, dx, z, wos.Context(wavelength=wl))
+    gpu.set_fast_path(1)
+    fp64 = gpu.precision == wos.FP64
+    assert abs(lf - lo) / lo <= (1e-11 if fp64 else 1e-5)
+    assert rel_l2(gf, go) <= (1e-11 if fp64 else 1e-4)
+    assert abs(lf - lg) / lg <= (1e-11 if fp64 else 1e-5)
+    assert rel_l2(gf, gg) <= (1e-11 if fp64 else 1e-4)
+    rng = np.random.default_rng(4)
+    scale = np.max(np.abs(gf))
+    for _ in range(16):
+        j, i = rng.integers(0, n, 2)
+        p1 = phi.copy(); p1[j, i] += 1e-6
+        p2 = phi.copy(); p2[j, i] -= 1e-6
+        l1, _ = O.asm_phase_loss_grad(a, p1, T, dx, z, ctx, want_grad=False)
+        l2, _ = O.asm_phase_loss_grad(a, p2, T, dx, z, ctx, want_grad=False)
+        assert abs((l1 - l2) / 2e-6 - gf[j, i]) <= 1e-4 * scale
+
+
+@pytest.mark.parametrize("n", [256, 2048])
+def test_design_device_entry_point_matches_host(gpu, n):
+    """wos_asm_loss_grad_dev (device arrays, as an optimisation loop keeps
+    them) returns the host entry point's loss and gradient."""
+    import torch
+    dx, wl, z = 4e-6, 633e-9, 0.1 if n == 2048 else 5e-3
+    a, phi, T = _design(n, 5)
+    lh, gh = gpu.asm_loss_grad(a, phi, T, dx, z, wos.Context(wavelength=wl))
+    dt = torch.complex128 if gpu.precision == wos.FP64 else torch.complex64
+    ad = torch.from_numpy(a).to(dt).cuda()
+    pd = torch.from_numpy(phi).cuda()
+    td = torch.from_numpy(T).cuda()
+    gd = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ld = gpu.asm_loss_grad_dev(n, n, dx, z, wos.Context(wavelength=wl), ad.data_ptr(), pd.data_ptr(), td.data_ptr(),
+                               gd.data_ptr())
+    gpu.synchronize()
+    fp64 = gpu.precision == wos.FP64
+    assert abs(ld - lh) / lh <= (1e-12 if fp64 else 1e-6)
+    assert rel_l2(gd.cpu().numpy(), gh) <= (1e-12 if fp64 else 1e-5)
+    l0 = gpu.asm_loss_grad_dev(n, n, dx, z, wos.Context(wavelength=wl), ad.data_ptr(), pd.data_ptr(), td.data_ptr())
+    assert abs(l0 - ld) <= 1e-12 * abs(ld)

@@ -97,6 +97,112 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
     }
 }
 
+// Inverse-design row stages (see DesignArgs).  Positions q of a row follow
+// the natural order of radix rs (the forward transform's input order, the
+// inverse's output order), so every pointwise step sits between two
+// transforms in registers.
+template <typename Real, int L, int E, int STAGE>
+__global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_design(const FastRows a, const DesignArgs d) {
+    using C = typename CT<Real>::t;
+    using PL = FPlan<L, E>;
+    constexpr int T = PL::T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int lines = blockDim.x / T;
+    const int line = threadIdx.x / T, tt = threadIdx.x - line * T;
+    C* smb = reinterpret_cast<C*>(smraw) + line * frow_stride(L, E);
+    const int r = blockIdx.x * lines + line;
+    const bool act = r < a.rows;
+    const C* twp = reinterpret_cast<const C*>(a.tw);
+    const long long row = (long long)r * L;
+    C v[E];
+    double loss = 0;
+    if (STAGE == 0) {
+        if (act) {
+#pragma unroll
+            for (int s = 0; s < E; s++) {
+                const int q = fpos<PL::RS, E, L>(s, tt);
+                double sn, cs;
+                sincos(__ldg(d.phi + row + q), &sn, &cs);
+                double ar, ai;
+                if (d.amp_c128) {
+                    const double2 x = reinterpret_cast<const double2*>(d.amp)[row + q];
+                    ar = x.x;
+                    ai = x.y;
+                } else {
+                    const C x = reinterpret_cast<const C*>(d.amp)[row + q];
+                    ar = x.x;
+                    ai = x.y;
+                }
+                v[s] = mkc<C>((Real)(cs * ar - sn * ai), (Real)(cs * ai + sn * ar));
+            }
+        } else {
+#pragma unroll
+            for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
+        }
+    } else {
+        if (act) {
+            const C* in = reinterpret_cast<const C*>(a.in) + row + tt;
+#pragma unroll
+            for (int s = 0; s < E; s++) v[s] = __ldcs(in + fpos<E, E, L>(s, 0));
+        } else {
+#pragma unroll
+            for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
+        }
+        fpasses<L, E, true, 0, 1>(v, smb, tt, twp);
+    }
+    if (STAGE == 1 && act) {
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int q = fpos<PL::RS, E, L>(s, tt);
+            const double ur = v[s].x, ui = v[s].y;
+            const double dd = ur * ur + ui * ui - __ldg(d.target + row + q);
+            loss += dd * dd;
+            v[s] = mkc<C>((Real)(4 * dd * ur), (Real)(4 * dd * ui));
+        }
+    }
+    if (STAGE == 2) {
+        if (act) {
+#pragma unroll
+            for (int s = 0; s < E; s++) {
+                const int q = fpos<PL::RS, E, L>(s, tt);
+                double sn, cs;
+                sincos(__ldg(d.phi + row + q), &sn, &cs);
+                double ar, ai;
+                if (d.amp_c128) {
+                    const double2 x = reinterpret_cast<const double2*>(d.amp)[row + q];
+                    ar = x.x;
+                    ai = x.y;
+                } else {
+                    const C x = reinterpret_cast<const C*>(d.amp)[row + q];
+                    ar = x.x;
+                    ai = x.y;
+                }
+                // i t a = (-Im(t a), Re(t a))
+                const double tr = cs * ar - sn * ai, ti = cs * ai + sn * ar;
+                d.grad[row + q] = (double)v[s].x * (-ti) + (double)v[s].y * tr;
+            }
+        }
+    } else {
+        fpasses<L, E, false, 0, 1>(v, smb, tt, twp);
+        if (act) {
+            C* out = reinterpret_cast<C*>(a.out) + row + tt;
+#pragma unroll
+            for (int s = 0; s < E; s++) out[fpos<E, E, L>(s, 0)] = v[s];
+        }
+    }
+    if (STAGE == 1 && a.red) {
+        __shared__ double rsm[32];
+        for (int o = 16; o > 0; o >>= 1) loss += __shfl_down_sync(0xffffffffu, loss, o);
+        if ((threadIdx.x & 31) == 0) rsm[threadIdx.x >> 5] = loss;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0;
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += rsm[w];
+            a.red[(long long)blockIdx.x * a.red_stride] = t;
+        }
+    }
+}
+
 // One split-step slice on a row (optics/medium.go:50-65 for the screen): the
 // inverse row transform, the screen t(x, y) = border[d] exp(i phase gx gy) at
 // the inverse's natural output positions, which are the forward transform's
@@ -273,6 +379,33 @@ static cudaError_t go_rows_bpm(const FastRows& a, cudaStream_t st, int* nblocks)
     return cudaGetLastError();
 }
 
+template <typename Real, int L, int E, int STAGE>
+static cudaError_t go_rows_design(const FastRows& a, const DesignArgs& d, cudaStream_t st, int* nblocks) {
+    constexpr int T = L / E;
+    int lines = 1;
+    while (lines * 2 * T <= 256 && lines * 2 <= a.rows) lines *= 2;
+    while (lines * T < 32) lines *= 2;
+    const size_t smem = (size_t)frow_stride(L, E) * lines * sizeof(typename CT<Real>::t);
+    if (smem > kSmemNoOptIn) {
+        cudaError_t e = cudaFuncSetAttribute(k_rows_design<Real, L, E, STAGE>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((a.rows + lines - 1) / lines, 1);
+    if (nblocks) *nblocks = (int)grid.x;
+    k_rows_design<Real, L, E, STAGE><<<grid, lines * T, smem, st>>>(a, d);
+    return cudaGetLastError();
+}
+
+template <typename Real, int L, int E>
+static cudaError_t go_rows_design_s(int stage, const FastRows& a, const DesignArgs& d, cudaStream_t st, int* nb) {
+    switch (stage) {
+    case 0: return go_rows_design<Real, L, E, 0>(a, d, st, nb);
+    case 1: return go_rows_design<Real, L, E, 1>(a, d, st, nb);
+    default: return go_rows_design<Real, L, E, 2>(a, d, st, nb);
+    }
+}
+
 template <typename Real, int L, int E, int W>
 static cudaError_t go_cols_w(const FastCols& a, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
@@ -383,6 +516,28 @@ cudaError_t fast_rows_bpm(int fp64, int L, int E, const FastRows& a, cudaStream_
         break;
     switch (L) { WOS_FAST_L(CASE_B) }
 #undef CASE_B
+    return cudaErrorNotSupported;
+}
+
+cudaError_t fast_rows_design(int fp64, int L, int E, int stage, const FastRows& a, const DesignArgs& d,
+                             cudaStream_t st, int* nblocks) {
+#define CASE_D(LL)                                                                                  \
+    case LL:                                                                                        \
+        if (fp64) {                                                                                 \
+            if constexpr (LL <= 4096) {                                                             \
+                if (E == 8) return go_rows_design_s<double, LL, 8>(stage, a, d, st, nblocks);       \
+            } else {                                                                                \
+                if (E == 16) return go_rows_design_s<double, LL, 16>(stage, a, d, st, nblocks);     \
+            }                                                                                       \
+        } else {                                                                                    \
+            if constexpr (LL <= 4096) {                                                             \
+                if (E == 8) return go_rows_design_s<float, LL, 8>(stage, a, d, st, nblocks);        \
+            }                                                                                       \
+            if (E == 16) return go_rows_design_s<float, LL, 16>(stage, a, d, st, nblocks);          \
+        }                                                                                           \
+        break;
+    switch (L) { WOS_FAST_L(CASE_D) }
+#undef CASE_D
     return cudaErrorNotSupported;
 }
 

@@ -53,6 +53,22 @@ struct FastCols {
 
 cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaStream_t st, int* nblocks);
 cudaError_t fast_cols(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks);
+// Inverse design on rows (ASM forward / adjoint of L = sum (|u|^2 - T)^2):
+// stage 0 loads a exp(i phi) and transforms forward; stage 1 transforms back
+// to u, forms r = 4 (|u|^2 - T) u (loss partial per CTA, slot 0 of a record of
+// red_stride) and transforms r forward; stage 2 transforms back to b = A^H r
+// and writes g = Re(conj(b) i exp(i phi) a).  Single component, row-major
+// ny x nx; a is complex128 when amp_c128, else the pipeline's complex type.
+struct DesignArgs {
+    const double* phi;
+    const double* target;
+    const void* amp;
+    int amp_c128;
+    double* grad;
+};
+cudaError_t fast_rows_design(int fp64, int L, int E, int stage, const FastRows& a, const DesignArgs& d,
+                             cudaStream_t st, int* nblocks);
+
 // One split-step slice on rows: inverse transform, slice screen, forward
 // transform (native precision in and out, in place allowed).
 cudaError_t fast_rows_bpm(int fp64, int L, int E, const FastRows& a, cudaStream_t st, int* nblocks);

@@ -39,7 +39,8 @@ EXPORTS = [
     "wos_propagate_dev_c128", "wos_splitstep", "wos_splitstep_dev", "wos_splitstep_maps",
     "wos_polychromatic", "wos_volume", "wos_schell_modes", "wos_partially_coherent",
     "wos_apply_lens", "wos_apply_aperture_circle", "wos_apply_grating", "wos_apply_phase_mask",
-    "wos_asm_forward_loss", "wos_asm_loss_grad", "wos_asm_adjoint", "wos_asm_pad_c64_noalloc",
+    "wos_asm_forward_loss", "wos_asm_loss_grad", "wos_asm_loss_grad_dev", "wos_asm_adjoint",
+    "wos_asm_pad_c64_noalloc",
 ]
 
 
@@ -123,6 +124,7 @@ def lib():
             "wos_apply_phase_mask": ([vp, vp, vp, d], i),
             "wos_asm_forward_loss": ([vp, i, i, d, d, vp, vp, vp, vp, vp], i),
             "wos_asm_loss_grad": ([vp, i, i, d, d, vp, vp, vp, vp, vp, vp], i),
+            "wos_asm_loss_grad_dev": ([vp, i, i, d, d, vp, vp, vp, vp, vp, vp], i),
             "wos_asm_adjoint": ([vp, vp, d, vp], i),
             "wos_asm_pad_c64_noalloc": ([vp, vp, i, i, d, d, vp, vp], i),
         }
@@ -460,6 +462,16 @@ class GPU:
         _check(lib().wos_asm_forward_loss(self.h, ny, nx, dx, z, C.byref(cc), _ptr(a), _ptr(phi), _ptr(target),
                                           C.byref(loss)))
         return loss.value, None
+
+    def asm_loss_grad_dev(self, ny: int, nx: int, dx: float, z: float, ctx: Context, a_ptr: int, phi_ptr: int,
+                          target_ptr: int, grad_ptr: int = 0) -> float:
+        """wos_asm_loss_grad_dev: device arrays in, loss out (grad written on the device)."""
+        loss = C.c_double()
+        cc = ctx.c()
+        _check(lib().wos_asm_loss_grad_dev(self.h, ny, nx, dx, z, C.byref(cc), C.c_void_p(a_ptr),
+                                           C.c_void_p(phi_ptr), C.c_void_p(target_ptr), C.byref(loss),
+                                           C.c_void_p(grad_ptr) if grad_ptr else None))
+        return loss.value
 
     def asm_adjoint(self, f: Field, z: float, ctx: Context) -> None:
         cc = ctx.c()
