@@ -196,6 +196,15 @@ WOS_API int wos_propagate_dev(wos_ctx ctx, int ny, int nx, double dx, int ncomp,
  * (the FP32 pipeline converts inside its first and last sweep). */
 WOS_API int wos_propagate_dev_c128(wos_ctx ctx, int ny, int nx, double dx, int ncomp, const void* in,
                            void* out, double z, int method, const wos_context* c, wos_diag* diag);
+/* A batch of independent device fields propagated with the same geometry and
+ * settings (in[i] -> out[i], each as wos_propagate_dev without diagnostics).
+ * On the power-of-two ASM path the fields run concurrently on streams forked
+ * from the context stream and joined back into it, so the kernels of one
+ * field fill the SMs that another leaves idle; otherwise they run in order.
+ * No counterpart in the reference (which propagates one field per call). */
+WOS_API int wos_propagate_batch_dev(wos_ctx ctx, int nfields, int ny, int nx, double dx, int ncomp,
+                                    const void* const* in, void* const* out, double z, int method,
+                                    const wos_context* c);
 
 /* ---- PropagateSplitStep (optics/medium.go:22-45) with a parametric medium. ---- */
 WOS_API int wos_splitstep(wos_ctx ctx, wos_field* f, double z, const wos_index_desc* n, int steps,

@@ -40,6 +40,7 @@ EXPORTS = [
     "wos_polychromatic", "wos_volume", "wos_schell_modes", "wos_partially_coherent",
     "wos_apply_lens", "wos_apply_aperture_circle", "wos_apply_grating", "wos_apply_phase_mask",
     "wos_asm_forward_loss", "wos_asm_loss_grad", "wos_asm_loss_grad_dev", "wos_asm_adjoint",
+    "wos_propagate_batch_dev",
     "wos_asm_pad_c64_noalloc",
 ]
 
@@ -125,6 +126,7 @@ def lib():
             "wos_asm_forward_loss": ([vp, i, i, d, d, vp, vp, vp, vp, vp], i),
             "wos_asm_loss_grad": ([vp, i, i, d, d, vp, vp, vp, vp, vp, vp], i),
             "wos_asm_loss_grad_dev": ([vp, i, i, d, d, vp, vp, vp, vp, vp, vp], i),
+            "wos_propagate_batch_dev": ([vp, i, i, i, d, i, vp, vp, d, i, vp], i),
             "wos_asm_adjoint": ([vp, vp, d, vp], i),
             "wos_asm_pad_c64_noalloc": ([vp, vp, i, i, d, d, vp, vp], i),
         }
@@ -330,6 +332,16 @@ class GPU:
         if d is not None and ctx is not None:
             ctx.absorb(d)
         return d
+
+    def propagate_batch_dev(self, ny: int, nx: int, dx: float, ncomp: int, in_ptrs, out_ptrs, z: float,
+                            method: str, ctx: Optional[Context]) -> None:
+        """wos_propagate_batch_dev: independent device fields, concurrently where the path allows."""
+        n = len(in_ptrs)
+        ia = (C.c_void_p * n)(*[C.c_void_p(p) for p in in_ptrs])
+        oa = (C.c_void_p * n)(*[C.c_void_p(p) for p in out_ptrs])
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_propagate_batch_dev(self.h, n, ny, nx, dx, ncomp, ia, oa, z, METHODS[method],
+                                             C.byref(cc) if cc is not None else None))
 
     # ---- PropagateSplitStep
     def split_step(self, f: Field, z: float, desc: IndexDesc, steps: int, ctx: Optional[Context]) -> CDiag:
