@@ -185,6 +185,13 @@ WOS_API int wos_fft2d_dev(wos_ctx ctx, int ny, int nx, int batch, void* a, int i
 /* ---- Propagate (optics/propagate.go:65-102): the host Field in place. ---- */
 WOS_API int wos_propagate(wos_ctx ctx, wos_field* f, double z, int method, const wos_context* c,
                   wos_diag* diag /* may be NULL */);
+/* A batch of host fields (each as wos_propagate, in place; diags may be NULL,
+ * else one per field).  Uploads, sweeps and downloads of consecutive fields
+ * overlap (separate copy streams, three device staging slots), so with
+ * page-locked host buffers a field costs about one PCIe direction instead of
+ * both.  No counterpart in the reference (one field per call). */
+WOS_API int wos_propagate_batch(wos_ctx ctx, int nfields, wos_field* fields, double z, int method,
+                                const wos_context* c, wos_diag* diags);
 
 /* Device-resident variant: in/out hold ncomp components [ncomp][ny][nx] in the
  * context precision; in == out is allowed.  dx_out returns the output pitch

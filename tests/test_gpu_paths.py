@@ -187,3 +187,30 @@ def test_batch_dev_equals_single_calls(prec, shape, nf):
         g.synchronize()
         for o, x in zip(outs, b):
             assert np.array_equal(o.cpu().numpy(), x.cpu().numpy())
+
+
+@pytest.mark.parametrize("prec", [wos.FP64, wos.FP32], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("method", ["asm", "asm_pad", "fraunhofer"])
+def test_host_batch_equals_single_calls(prec, method):
+    """wos_propagate_batch (uploads, sweeps and downloads of consecutive fields
+    overlapped) gives every field, its warnings and its output pitch exactly
+    what one wos_propagate call gives."""
+    n, dx, wl = 256, 2e-6, 632.8e-9
+    z = 0.5 if method == "fraunhofer" else 4e-3
+    rng = np.random.default_rng(21)
+    srcs = [(np.exp(1j * rng.uniform(0, 2 * np.pi, (n, n))), None if k % 2 else
+             0.3j * np.exp(1j * rng.uniform(0, 2 * np.pi, (n, n)))) for k in range(5)]
+    with wos.GPU(prec) as g:
+        batch = [wos.Field(ex.copy(), dx, None if ey is None else ey.copy()) for ex, ey in srcs]
+        cb = wos.Context(wavelength=wl)
+        diags = g.propagate_batch(batch, z, method, cb)
+        assert len(diags) == len(batch)
+        cs = wos.Context(wavelength=wl)
+        for (ex, ey), fb in zip(srcs, batch):
+            fs = wos.Field(ex.copy(), dx, None if ey is None else ey.copy())
+            g.propagate(fs, z, method, cs)
+            assert np.array_equal(fs.ex, fb.ex)
+            if ey is not None:
+                assert np.array_equal(fs.ey, fb.ey)
+            assert fs.dx == fb.dx
+        assert cb.warnings == cs.warnings

@@ -117,6 +117,13 @@ struct wos_ctx_s {
     cudaStream_t side[kMaxAux] = {};
     cudaEvent_t fork_ev = nullptr, join_ev[kMaxAux] = {};
     int naux = 0;
+    // copy pipeline of wos_propagate_batch: host-to-device and device-to-host
+    // streams, staging slots and their events
+    static constexpr int kSlots = 3;
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    DevBuf slot[kSlots];
+    cudaEvent_t in_ev[kSlots] = {}, done_ev[kSlots] = {}, free_ev[kSlots] = {};
+    bool pipe_made = false;
     std::map<long long, Tune> tune;     // autotuned launch configurations
     size_t csz() const { return fp64 ? 16 : 8; }
     // per-launch CUDA-event profile (wos_ctx_set_profiling): a ring of event
@@ -1274,6 +1281,16 @@ int wos_ctx_destroy(wos_ctx c) {
             cudaEventDestroy(c->join_ev[i]);
         }
         if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+        if (c->pipe_made) {
+            cudaStreamDestroy(c->h2d);
+            cudaStreamDestroy(c->d2h);
+            for (int i = 0; i < wos_ctx_s::kSlots; i++) {
+                if (c->slot[i].p) cudaFree(c->slot[i].p);
+                cudaEventDestroy(c->in_ev[i]);
+                cudaEventDestroy(c->done_ev[i]);
+                cudaEventDestroy(c->free_ev[i]);
+            }
+        }
         if (c->prof_made)
             for (int i = 0; i < wos_ctx_s::kRing; i++) {
                 cudaEventDestroy(c->ev0[i]);
@@ -1489,6 +1506,86 @@ int wos_propagate_batch_dev(wos_ctx c, int nfields, int ny, int nx, double dx, i
         CK(cudaStreamWaitEvent(c->st, c->join_ev[k], 0));
     }
     return rc;
+}
+
+int wos_propagate_batch(wos_ctx c, int nfields, wos_field* fields, double z, int method, const wos_context* cci,
+                        wos_diag* diags) {
+    if (!c || nfields < 0 || (nfields > 0 && !fields)) return fail(WOS_INVALID_ARG, "batch arguments");
+    if (method < WOS_ASM || method > WOS_FRAUNHOFER) return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
+    for (int i = 0; i < nfields; i++) TRY(check_field(&fields[i]));
+    if (nfields == 0) return WOS_OK;
+    const wos_context cc = cci ? *cci : default_context();
+    if (z == 0) {
+        for (int i = 0; i < nfields && diags; i++) {
+            std::memset(&diags[i], 0, sizeof(diags[i]));
+            diags[i].dx_out = fields[i].dx;
+        }
+        return WOS_OK;
+    }
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    if (!c->pipe_made) {
+        CK(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
+        for (int i = 0; i < wos_ctx_s::kSlots; i++) {
+            CK(cudaEventCreateWithFlags(&c->in_ev[i], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&c->done_ev[i], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&c->free_ev[i], cudaEventDisableTiming));
+            CK(cudaEventRecord(c->free_ev[i], c->d2h));
+        }
+        c->pipe_made = true;
+    }
+    // field i lives in slot i % kSlots from its upload to its download; the
+    // upload of the next field is queued before field i's sweeps, so the two
+    // copy directions and the sweeps overlap (the sweeps stay in order on the
+    // context stream and share its workspace)
+    auto bytes_of = [&](int i) {
+        return (size_t)fields[i].ny * fields[i].nx * 16 * (fields[i].polarized ? 2 : 1);
+    };
+    auto upload = [&](int i) -> int {
+        const int sl = i % wos_ctx_s::kSlots;
+        const wos_field& f = fields[i];
+        const size_t np = (size_t)f.ny * f.nx;
+        CK(cudaStreamWaitEvent(c->h2d, c->free_ev[sl], 0));
+        TRY(ensure(c->slot[sl], bytes_of(i)));
+        CK(cudaMemcpyAsync(c->slot[sl].p, f.ex, np * 16, cudaMemcpyHostToDevice, c->h2d));
+        if (f.polarized)
+            CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->slot[sl].p) + np * 16, f.ey, np * 16,
+                               cudaMemcpyHostToDevice, c->h2d));
+        CK(cudaEventRecord(c->in_ev[sl], c->h2d));
+        return WOS_OK;
+    };
+    int rc = upload(0);
+    for (int i = 0; i < nfields && rc == WOS_OK; i++) {
+        const int sl = i % wos_ctx_s::kSlots;
+        if (i + 1 < nfields) {
+            rc = upload(i + 1);
+            if (rc != WOS_OK) break;
+        }
+        wos_field& f = fields[i];
+        const size_t np = (size_t)f.ny * f.nx;
+        const int ncomp = f.polarized ? 2 : 1;
+        CK(cudaStreamWaitEvent(c->st, c->in_ev[sl], 0));
+        wos_diag local;
+        wos_diag* d = diags ? &diags[i] : (method == WOS_FRAUNHOFER ? &local : nullptr);
+        Prop p{f.ny, f.nx, f.dx, ncomp, c->slot[sl].p, 1, c->slot[sl].p, 1, z, method, cc, d};
+        rc = run_propagate(c, p);
+        if (rc != WOS_OK) break;
+        if (method == WOS_FRAUNHOFER) f.dx = d->dx_out;
+        CK(cudaEventRecord(c->done_ev[sl], c->st));
+        CK(cudaStreamWaitEvent(c->d2h, c->done_ev[sl], 0));
+        CK(cudaMemcpyAsync(f.ex, c->slot[sl].p, np * 16, cudaMemcpyDeviceToHost, c->d2h));
+        if (ncomp == 2)
+            CK(cudaMemcpyAsync(f.ey, reinterpret_cast<char*>(c->slot[sl].p) + np * 16, np * 16,
+                               cudaMemcpyDeviceToHost, c->d2h));
+        CK(cudaEventRecord(c->free_ev[sl], c->d2h));
+    }
+    cudaStreamSynchronize(c->h2d);
+    cudaStreamSynchronize(c->d2h);
+    CK(cudaMemcpyAsync(c->err_host, c->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (rc != WOS_OK) return rc;
+    return check_err_word(c);
 }
 
 int wos_propagate(wos_ctx c, wos_field* f, double z, int method, const wos_context* cc, wos_diag* diag) {

@@ -40,7 +40,7 @@ EXPORTS = [
     "wos_polychromatic", "wos_volume", "wos_schell_modes", "wos_partially_coherent",
     "wos_apply_lens", "wos_apply_aperture_circle", "wos_apply_grating", "wos_apply_phase_mask",
     "wos_asm_forward_loss", "wos_asm_loss_grad", "wos_asm_loss_grad_dev", "wos_asm_adjoint",
-    "wos_propagate_batch_dev",
+    "wos_propagate_batch_dev", "wos_propagate_batch",
     "wos_asm_pad_c64_noalloc",
 ]
 
@@ -127,6 +127,7 @@ def lib():
             "wos_asm_loss_grad": ([vp, i, i, d, d, vp, vp, vp, vp, vp, vp], i),
             "wos_asm_loss_grad_dev": ([vp, i, i, d, d, vp, vp, vp, vp, vp, vp], i),
             "wos_propagate_batch_dev": ([vp, i, i, i, d, i, vp, vp, d, i, vp], i),
+            "wos_propagate_batch": ([vp, i, vp, d, i, vp, vp], i),
             "wos_asm_adjoint": ([vp, vp, d, vp], i),
             "wos_asm_pad_c64_noalloc": ([vp, vp, i, i, d, d, vp, vp], i),
         }
@@ -332,6 +333,23 @@ class GPU:
         if d is not None and ctx is not None:
             ctx.absorb(d)
         return d
+
+    def propagate_batch(self, fields, z: float, method: str = "asm", ctx: Optional[Context] = None):
+        """wos_propagate_batch: host fields in place, copies and sweeps of consecutive fields overlapped."""
+        if method not in METHODS:
+            raise WosError(7, f"unknown propagation method {method!r}")
+        n = len(fields)
+        cf = (CField * n)(*[f.c() for f in fields])
+        ds = (CDiag * n)()
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_propagate_batch(self.h, n, cf, z, METHODS[method], C.byref(cc) if cc is not None else None,
+                                         ds))
+        for f, c_, d in zip(fields, cf, ds):
+            if method == "fraunhofer":
+                f.dx = c_.dx
+            if ctx is not None:
+                ctx.absorb(d)
+        return list(ds)
 
     def propagate_batch_dev(self, ny: int, nx: int, dx: float, ncomp: int, in_ptrs, out_ptrs, z: float,
                             method: str, ctx: Optional[Context]) -> None:
