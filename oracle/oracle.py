@@ -267,6 +267,8 @@ def polychromatic(f: Field, z: float, wls, weights, method: str, ctx: Optional[C
     cc = ctx._to_c() if ctx is not None else None
     rc = lib().or_polychromatic(C.byref(f._c()), z, _ptr(wl), _ptr(w), wl.size, METHODS[method],
                                 C.byref(cc) if cc is not None else None, _ptr(out))
+    if ctx is not None:
+        ctx._from_c(cc)
     if rc != 0:
         raise ValueError(f"polychromatic rc={rc}")
     return out
@@ -279,6 +281,8 @@ def propagate3d(f: Field, zs, method: str, ctx: Optional[Context]) -> np.ndarray
     cc = ctx._to_c() if ctx is not None else None
     rc = lib().or_propagate3d(C.byref(f._c()), _ptr(zz), zz.size, METHODS[method],
                               C.byref(cc) if cc is not None else None, _ptr(out))
+    if ctx is not None:
+        ctx._from_c(cc)
     if rc != 0:
         raise ValueError(f"propagate3d rc={rc}")
     return out

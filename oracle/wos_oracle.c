@@ -808,47 +808,59 @@ static or_field clone_field(const or_field *f) {
 }
 static void free_field(or_field *g) { free(g->ex); free(g->ey); }
 
-/* PropagatePolychromatic (polychromatic.go:18-44) */
+/* PropagatePolychromatic (polychromatic.go:18-44).  The samples' contexts
+ * copy the caller's, whose Warnings is a shared pointer in the reference: what
+ * every sample adds ends up in the caller's context (written back here). */
 int or_polychromatic(const or_field *f, double z, const double *wl, const double *weight, int ns,
-                     int method, const or_context *base_in, double *out) {
+                     int method, or_context *base_io, double *out) {
     if (ns <= 0) return -3;
     or_context base;
-    if (base_in) base = *base_in;
+    if (base_io) base = *base_io;
     else { memset(&base, 0, sizeof(base)); base.has_warnings = 1; }
     size_t n = npix(f);
     memset(out, 0, sizeof(double) * n);
-    for (int s = 0; s < ns; s++) {
-        if (wl[s] <= 0) return -4;
+    int rc = 0;
+    for (int s = 0; s < ns && rc == 0; s++) {
+        if (wl[s] <= 0) { rc = -4; break; }
         or_field g = clone_field(f);
         or_context c = base;
         c.wavelength = wl[s];
-        int rc = or_propagate(&g, z, method, &c);
-        /* Warnings is a shared pointer in the reference: keep what this sample added */
+        rc = or_propagate(&g, z, method, &c);
         base.n_warn = c.n_warn;
         memcpy(base.warn, c.warn, sizeof(base.warn));
-        if (rc) { free_field(&g); return rc; }
-        for (size_t i = 0; i < n; i++) out[i] += weight[s] * intensity(&g, i);
+        if (rc == 0)
+            for (size_t i = 0; i < n; i++) out[i] += weight[s] * intensity(&g, i);
         free_field(&g);
     }
-    return 0;
+    if (base_io) {
+        base_io->n_warn = base.n_warn;
+        memcpy(base_io->warn, base.warn, sizeof(base.warn));
+    }
+    return rc;
 }
 
 /* Propagate3D (volume.go:8-18) */
-int or_propagate3d(const or_field *f, const double *zs, int nz, int method, const or_context *ctx_in,
+int or_propagate3d(const or_field *f, const double *zs, int nz, int method, or_context *ctx_io,
                    oc128 *out) {
     size_t n = npix(f);
     int ncomp = f->polarized ? 2 : 1;
     or_context ctx;
-    if (ctx_in) ctx = *ctx_in; else memset(&ctx, 0, sizeof(ctx));
-    for (int q = 0; q < nz; q++) {
+    if (ctx_io) ctx = *ctx_io; else memset(&ctx, 0, sizeof(ctx));
+    int rc = 0;
+    for (int q = 0; q < nz && rc == 0; q++) {
         or_field g = clone_field(f);
-        int rc = or_propagate(&g, zs[q], method, &ctx);
-        if (rc) { free_field(&g); return rc; }
-        memcpy(out + (size_t)q * ncomp * n, g.ex, sizeof(oc128) * n);
-        if (ncomp == 2) memcpy(out + ((size_t)q * ncomp + 1) * n, g.ey, sizeof(oc128) * n);
+        rc = or_propagate(&g, zs[q], method, &ctx);
+        if (rc == 0) {
+            memcpy(out + (size_t)q * ncomp * n, g.ex, sizeof(oc128) * n);
+            if (ncomp == 2) memcpy(out + ((size_t)q * ncomp + 1) * n, g.ey, sizeof(oc128) * n);
+        }
         free_field(&g);
     }
-    return 0;
+    if (ctx_io) { /* the same Context (and Warnings) for every plane (volume.go:8-18) */
+        ctx_io->n_warn = ctx.n_warn;
+        memcpy(ctx_io->warn, ctx.warn, sizeof(ctx.warn));
+    }
+    return rc;
 }
 
 /* GenerateSchellRealizations (coherence.go:22-80) with caller noise */

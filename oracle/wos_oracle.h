@@ -116,9 +116,9 @@ int or_splitstep_fn(or_field *f, double z, or_index_fn fn, void *user, int steps
 /* ---- batches ---- */
 /* polychromatic.go:18-44; out[ny*nx] */
 int or_polychromatic(const or_field *f, double z, const double *wl, const double *weight, int ns,
-                     int method, const or_context *base, double *out);
+                     int method, or_context *base, double *out);
 /* volume.go:8-18; out = nz * ncomp * ny*nx (ncomp = 1 + polarized) */
-int or_propagate3d(const or_field *f, const double *zs, int nz, int method, const or_context *ctx,
+int or_propagate3d(const or_field *f, const double *zs, int nz, int method, or_context *ctx,
                    oc128 *out);
 /* coherence.go:22-80 with caller-supplied complex noise (m * n*n values that
  * replace complex(rng.NormFloat64()/sqrt2, rng.NormFloat64()/sqrt2)) */

@@ -429,3 +429,58 @@ def test_design_device_entry_point_matches_host(gpu, n):
     assert rel_l2(gd.cpu().numpy(), gh) <= (1e-12 if fp64 else 1e-5)
     l0 = gpu.asm_loss_grad_dev(n, n, dx, z, wos.Context(wavelength=wl), ad.data_ptr(), pd.data_ptr(), td.data_ptr())
     assert abs(l0 - ld) <= 1e-12 * abs(ld)
+
+
+def _general(gpu, fn):
+    gpu.set_fast_path(0)
+    try:
+        return fn()
+    finally:
+        gpu.set_fast_path(1)
+
+
+def test_polychromatic_specialised_batch(gpu):
+    """256^2 (power of two): the batched specialised sweeps (one shared row
+    spectrum, per-wavelength column sweep, intensity accumulated in the row
+    sweep) against the oracle and the general sweeps, warnings included."""
+    n, dx, z = 256, 2e-6, 2e-2
+    x = (np.arange(n) - n / 2) * dx
+    g = (np.cos(2 * np.pi * x / 20e-6) >= np.cos(np.pi * 0.5)).astype(float)
+    ex = np.tile(g, (n, 1)).astype(complex) * np.exp(-(x[:, None] ** 2) / (150e-6) ** 2)
+    wls = np.linspace(400e-9, 700e-9, 9)
+    ws = np.linspace(0.5, 1.5, 9)
+    oc = O.Context(wavelength=wls[0])
+    ref = O.polychromatic(O.Field(ex.copy(), dx), z, wls, ws, "asm", oc)
+    gc = wos.Context(wavelength=wls[0])
+    out = gpu.polychromatic(wos.Field(ex.copy(), dx), z, wls, ws, "asm", gc)
+    gg = wos.Context(wavelength=wls[0])
+    gen = _general(gpu, lambda: gpu.polychromatic(wos.Field(ex.copy(), dx), z, wls, ws, "asm", gg))
+    assert rel_l2(out, ref) <= tol(gpu.precision)
+    assert rel_l2(out, gen) <= tol(gpu.precision)
+    check_warnings(gc, oc, gpu.precision == wos.FP64)
+    assert gc.warnings.keys() == gg.warnings.keys()
+
+
+def test_volume_specialised_batch(gpu):
+    n, dx, wl = 256, 4e-6, 632.8e-9
+    x = (np.arange(n) - n / 2) * dx
+    ex = np.exp(-(x[None, :] ** 2 + x[:, None] ** 2) / (150e-6) ** 2).astype(complex)
+    zs = [0.0, 1e-3, 2.5e-3, 5e-3, 1e-2, 3e-2]
+    oc = O.Context(wavelength=wl)
+    ref = O.propagate3d(O.Field(ex.copy(), dx), zs, "asm", oc)
+    gc = wos.Context(wavelength=wl)
+    out = gpu.volume(wos.Field(ex.copy(), dx), zs, "asm", gc)
+    gen = _general(gpu, lambda: gpu.volume(wos.Field(ex.copy(), dx), zs, "asm", wos.Context(wavelength=wl)))
+    assert np.array_equal(out[0, 0], ex)
+    for q in range(len(zs)):
+        assert rel_l2(out[q], ref[q]) <= tol(gpu.precision), q
+        assert rel_l2(out[q], gen[q]) <= tol(gpu.precision), q
+    check_warnings(gc, oc, gpu.precision == wos.FP64)
+
+
+def test_partially_coherent_specialised_batch(gpu):
+    n, dx, w0, sigc, m, wl, z = 256, 1e-5, 6e-4, 5e-5, 12, 632.8e-9, 2e-2
+    noise = complex_normal(6, (m, n, n))
+    got = gpu.partially_coherent(n, dx, w0, sigc, noise, z, "asm", wos.Context(wavelength=wl))
+    gen = _general(gpu, lambda: gpu.partially_coherent(n, dx, w0, sigc, noise, z, "asm", wos.Context(wavelength=wl)))
+    assert rel_l2(got, gen) <= tol(gpu.precision) * 10

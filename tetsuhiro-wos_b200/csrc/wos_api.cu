@@ -1996,6 +1996,152 @@ struct Batch {
     wos_diag* diag;
 };
 
+// Batched ASM on the specialised sweeps (power-of-two grids): the forward row
+// sweep once per component for a shared input, then per chunk of units one
+// column sweep (gridDim.y = units, per-unit wavelength / distance, the shared
+// row spectrum as its source) and one row sweep that either accumulates the
+// weighted intensity of the chunk in registers or writes each unit's plane.
+// Diagnostics: per-unit spectral loss sums and histograms from the column
+// records, input power from the row records.  -1: not eligible.
+int try_fast_batch(wos_ctx c, Batch& b, std::vector<double>& sums, std::vector<double>& pin_unit,
+                   double& pin_total) {
+    const int ny = b.ny, nx = b.nx, ncomp = b.ncomp;
+    if (c->no_fast || !is_pow2(nx) || !is_pow2(ny)) return -1;
+    if (!c->fp64) {
+        for (int u = 0; u < b.units; u++) {
+            const double wl = b.wl.empty() ? b.cc.wavelength : b.wl[u];
+            const double z = b.z.empty() ? 0.0 : b.z[u];
+            if (!(std::fabs(z / wl) < 268435456.0)) return -1;
+        }
+    }
+    const Tune t = get_tune(c, ny, nx);
+    if (!fast_supported(c->fp64, nx, t.rowE) || !fast_supported(c->fp64, ny, t.colE)) return -1;
+    const double dx = b.dx;
+    const long long np = (long long)ny * nx;
+    const bool shared_in = b.in_unit_stride == 0;
+    const bool diag = b.diag != nullptr;
+    Axis *ax, *ay;
+    TRY(get_axis(c, nx, c->fp64, &ax));
+    TRY(get_axis(c, ny, c->fp64, &ay));
+    const void *twx, *twy;
+    TRY(fast_tw(c, ax, t.rowE, &twx));
+    TRY(fast_tw(c, ay, t.colE, &twy));
+    const size_t per = (size_t)np * c->csz();
+    int B = (int)std::max<size_t>(1, ((size_t)4 << 30) / per);
+    B = std::min(B, b.units);
+    B = std::min(B, 65535);
+    const size_t nbr = fast_row_blocks(nx, t.rowE, ny, shared_in ? 1 : B);
+    const size_t nbc = fast_col_blocks(c->fp64, ny, t.colE, t.colW, nx, 1);
+    TRY(red_prepare(c, std::max(nbr, nbc * (size_t)B)));
+    if (diag) TRY(ensure(c->tmp, sizeof(double) * RS_COUNT * (size_t)B));
+    TRY(ensure(c->scratch, (size_t)(shared_in ? 1 : B) * per));
+    TRY(ensure(c->scratch2, (size_t)B * per));
+    void* S0 = c->scratch.p;
+    void* S1 = c->scratch2.p;
+    const Policy pol = ev_policy(b.cc, b.z.empty() ? 1.0 : b.z[0]);
+    const HArgs h = asm_h(c, b.cc, b.z.empty() ? 0.0 : b.z[0], pol, dx, nx, ny);
+    double* o = reinterpret_cast<double*>(c->tmp.p);
+    int nb = 0;
+    for (int comp = 0; comp < ncomp; comp++) {
+        for (int k0 = 0; k0 < b.units; k0 += B) {
+            const int nu = std::min(B, b.units - k0);
+            if (k0 == 0 || !shared_in) {
+                FastRows r{};
+                r.rows = ny;
+                r.in = reinterpret_cast<const double2*>(b.in) +
+                       (shared_in ? comp * np : ((long long)k0 * ncomp + comp) * np);
+                r.in_c128 = 1;
+                r.in_ld = nx;
+                r.in_bstride = shared_in ? 0 : ncomp * np;
+                r.out = S0;
+                r.out_ld = nx;
+                r.out_bstride = np;
+                r.tw = twx;
+                r.out_scale = 1.0;
+                r.batch = shared_in ? 1 : nu;
+                if (diag) {
+                    r.red = red_region(c, 0) + RS_P;
+                    r.red_stride = RS_COUNT;
+                }
+                CK(timed_launch(c, 0, [&] { return fast_rows(c->fp64, nx, t.rowE, false, r, c->st, &nb); }));
+                if (diag) {
+                    const int per_unit = nb / r.batch;
+                    CK(launch_reduce_finish(red_region(c, 0), per_unit, r.batch, RS_P, 1, o, c->st));
+                    std::vector<double> hh((size_t)r.batch * RS_COUNT);
+                    CK(cudaMemcpyAsync(hh.data(), o, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost, c->st));
+                    CK(cudaStreamSynchronize(c->st));
+                    for (int u = 0; u < r.batch; u++) {
+                        const double p = hh[(size_t)u * RS_COUNT + RS_P] * dx * dx;
+                        if (shared_in) pin_total += p;
+                        else pin_unit[k0 + u] += p;
+                    }
+                }
+            }
+            FastCols k{};
+            k.ncols = nx;
+            k.W = t.colW;
+            k.data = S1;
+            k.ld = nx;
+            k.bstride = np;
+            k.src = S0;
+            k.src_bstride = shared_in ? 0 : np;
+            k.tw = twy;
+            k.batch = nu;
+            k.wl = b.cc.wavelength;
+            k.dx = dx;
+            k.z = b.z.empty() ? 0.0 : b.z[0];
+            k.kz = h.kz;
+            k.kaz = h.kaz;
+            k.krev = h.kz / (2 * M_PI);
+            k.batch_wl = b.wl_dev ? b.wl_dev + k0 : nullptr;
+            k.batch_z = b.z_dev ? b.z_dev + k0 : nullptr;
+            k.scale = h.scale;
+            k.alpha = h.alpha;
+            k.limit = h.limit;
+            k.zero_ev = h.zero_ev;
+            k.reg = h.reg;
+            k.backward = h.z < 0;
+            if (diag) {
+                k.red = red_region(c, 1) + RS_SW;
+                k.red_stride = RS_COUNT;
+                k.hist = red_region(c, 1) + RS_HIST;
+                k.hist_dx = dx;
+            }
+            CK(timed_launch(c, 4, [&] { return sweep_cols(c, ny, t.colE, k, &nb); }));
+            if (diag) {
+                const int per_unit = nb / nu;
+                CK(launch_reduce_finish(red_region(c, 1), per_unit, nu, RS_SW, 2, o, c->st));
+                CK(launch_reduce_finish(red_region(c, 1), per_unit, nu, RS_HIST, 97, o, c->st));
+                std::vector<double> hh((size_t)nu * RS_COUNT);
+                CK(cudaMemcpyAsync(hh.data(), o, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost, c->st));
+                CK(cudaStreamSynchronize(c->st));
+                for (int u = 0; u < nu; u++)
+                    for (int sl = RS_SW; sl < RS_COUNT; sl++)
+                        sums[((size_t)(k0 + u) * ncomp + comp) * RS_COUNT + sl] = hh[(size_t)u * RS_COUNT + sl];
+            }
+            FastRows q{};
+            q.rows = ny;
+            q.in = S1;
+            q.in_ld = nx;
+            q.in_bstride = np;
+            q.tw = twx;
+            q.out_scale = 1.0;
+            if (b.out_int) {
+                AccArgs acc{nu, b.w_dev ? b.w_dev + k0 : nullptr, b.out_int, 1};
+                CK(timed_launch(c, 1, [&] { return fast_rows_acc(c->fp64, nx, t.rowE, q, acc, c->st, &nb); }));
+            } else {
+                q.out = reinterpret_cast<double2*>(b.out_planes) + ((long long)k0 * ncomp + comp) * np;
+                q.out_c128 = 1;
+                q.out_ld = nx;
+                q.out_bstride = ncomp * np;
+                q.batch = nu;
+                CK(timed_launch(c, 1, [&] { return fast_rows(c->fp64, nx, t.rowE, true, q, c->st, &nb); }));
+            }
+        }
+    }
+    return WOS_OK;
+}
+
 int run_batch_asm(wos_ctx c, Batch& b) {
     const int ny = b.ny, nx = b.nx, ncomp = b.ncomp;
     const double dx = b.dx;
@@ -2024,7 +2170,9 @@ int run_batch_asm(wos_ctx c, Batch& b) {
     const Policy pol = ev_policy(b.cc, b.z.empty() ? 1.0 : b.z[0]);
     double pin_total = 0;
     std::vector<double> pin_unit(b.units, 0.0);
-    for (int comp = 0; comp < ncomp; comp++) {
+    const int fast = try_fast_batch(c, b, sums, pin_unit, pin_total);
+    if (fast != -1 && fast != WOS_OK) return fast;
+    for (int comp = 0; comp < ncomp && fast == -1; comp++) {
         for (int k0 = 0; k0 < b.units; k0 += B) {
             const int nb = std::min(B, b.units - k0);
             // rows forward (the shared input once per component, else per unit)
@@ -2177,7 +2325,6 @@ int element_begin(wos_ctx c, wos_field* f) {
 double2* stage_ex(wos_ctx c) { return reinterpret_cast<double2*>(c->stage.p); }
 double2* stage_ey(wos_ctx c, const wos_field* f) { return stage_ex(c) + (size_t)f->ny * f->nx; }
 
-// Inverse design on a host problem: forward (and adjoint) of one ASM step.
 // Inverse design on the specialised sweeps (power-of-two grids): five sweeps,
 // forward ASM of a exp(i phi) | residual between the inverse and the forward
 // transform of the middle row sweep | adjoint ASM | gradient in the last row
@@ -2250,6 +2397,7 @@ int asm_design_fast(wos_ctx c, int ny, int nx, double dx, double z, const wos_co
     return WOS_OK;
 }
 
+// Inverse design on a host problem: forward (and adjoint) of one ASM step.
 int asm_loss_grad_impl(wos_ctx c, int ny, int nx, double dx, double z, const wos_context* cc, const wos_c128* a,
                        const double* phi, const double* target, double* loss, double* grad) {
     if (!cc || !a || !phi || !target || !loss || ny < 2 || nx < 2 || !(dx > 0))

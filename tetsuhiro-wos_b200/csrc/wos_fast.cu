@@ -203,6 +203,50 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_design(const FastRow
     }
 }
 
+// Inverse row transforms of the nb units of a batch with their weighted
+// intensity accumulated in registers (PropagatePolychromatic /
+// AverageIntensity, optics/polychromatic.go:18-44, coherence.go:82-101); one
+// FP64 store per element.
+template <typename Real, int L, int E>
+__global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_acc_fast(const FastRows a, const AccArgs acc) {
+    using C = typename CT<Real>::t;
+    using PL = FPlan<L, E>;
+    constexpr int T = PL::T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int lines = blockDim.x / T;
+    const int line = threadIdx.x / T, tt = threadIdx.x - line * T;
+    C* smb = reinterpret_cast<C*>(smraw) + line * frow_stride(L, E);
+    const int r = blockIdx.x * lines + line;
+    const bool act = r < a.rows;
+    const C* twp = reinterpret_cast<const C*>(a.tw);
+    Real sum[E];
+#pragma unroll
+    for (int s = 0; s < E; s++) sum[s] = 0;
+    for (int u = 0; u < acc.nb; u++) {
+        C v[E];
+        if (act) {
+            const C* in = reinterpret_cast<const C*>(a.in) + (long long)u * a.in_bstride + (long long)r * a.in_ld + tt;
+#pragma unroll
+            for (int s = 0; s < E; s++) v[s] = __ldcs(in + fpos<E, E, L>(s, 0));
+        } else {
+#pragma unroll
+            for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
+        }
+        fpasses<L, E, true, 0, 1>(v, smb, tt, twp);
+        const double w = acc.weight ? acc.weight[u] : 1.0;
+#pragma unroll
+        for (int s = 0; s < E; s++) sum[s] += (Real)(w * ((double)v[s].x * v[s].x + (double)v[s].y * v[s].y));
+    }
+    if (act) {
+        double* out = acc.out + (long long)r * L + tt;
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            double* o = out + fpos<PL::RS, E, L>(s, 0);
+            *o = (acc.add ? *o : 0.0) + (double)sum[s];
+        }
+    }
+}
+
 // One split-step slice on a row (optics/medium.go:50-65 for the screen): the
 // inverse row transform, the screen t(x, y) = border[d] exp(i phase gx gy) at
 // the inverse's natural output positions, which are the forward transform's
@@ -274,13 +318,14 @@ __global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, 
     const bool act = col < a.ncols;
     const C* twp = reinterpret_cast<const C*>(a.tw);
     C* base = reinterpret_cast<C*>(a.data) + (long long)blockIdx.y * a.bstride + col;
+    const C* sbase = a.src ? reinterpret_cast<const C*>(a.src) + (long long)blockIdx.y * a.src_bstride + col : base;
     __shared__ double hsm[97];
     if (a.hist)
         for (int k = threadIdx.x; k < 97; k += blockDim.x) hsm[k] = 0;
     C v[E];
     constexpr int R1 = PL::RS;
     if (act) {
-        const C* src = base + (long long)tt * a.ld;
+        const C* src = sbase + (long long)tt * a.ld;
 #pragma unroll
         for (int s = 0; s < E; s++) v[s] = __ldcs(src + (long long)fpos<R1, E, L>(s, 0) * a.ld);
     } else {
@@ -291,7 +336,8 @@ __global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, 
     fpasses<L, E, false, 0, W>(v, smb, tt, twp);
 
     double p0 = 0, l1 = 0;
-    col_spectral_stage<Real, L, E, W>(v, reinterpret_cast<C*>(smraw), hsm, blockIdx.x * W, a, p0, l1);
+    col_spectral_stage<Real, L, E, W>(v, reinterpret_cast<C*>(smraw), hsm, blockIdx.x * W, a, h_unit(a, blockIdx.y),
+                                      p0, l1);
     fpasses<L, E, true, 0, W>(v, smb, tt, twp);
     if (act) {
         constexpr int RO = PL::RS;
@@ -376,6 +422,24 @@ static cudaError_t go_rows_bpm(const FastRows& a, cudaStream_t st, int* nblocks)
     dim3 grid((a.rows + lines - 1) / lines, a.batch > 0 ? a.batch : 1);
     if (nblocks) *nblocks = (int)(grid.x * grid.y);
     k_rows_bpm_fast<Real, L, E><<<grid, lines * T, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename Real, int L, int E>
+static cudaError_t go_rows_acc(const FastRows& a, const AccArgs& acc, cudaStream_t st, int* nblocks) {
+    constexpr int T = L / E;
+    int lines = 1;
+    while (lines * 2 * T <= 256 && lines * 2 <= a.rows) lines *= 2;
+    while (lines * T < 32) lines *= 2;
+    const size_t smem = (size_t)frow_stride(L, E) * lines * sizeof(typename CT<Real>::t);
+    if (smem > kSmemNoOptIn) {
+        cudaError_t e = cudaFuncSetAttribute(k_rows_acc_fast<Real, L, E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((a.rows + lines - 1) / lines, 1);
+    if (nblocks) *nblocks = (int)grid.x;
+    k_rows_acc_fast<Real, L, E><<<grid, lines * T, smem, st>>>(a, acc);
     return cudaGetLastError();
 }
 
@@ -516,6 +580,28 @@ cudaError_t fast_rows_bpm(int fp64, int L, int E, const FastRows& a, cudaStream_
         break;
     switch (L) { WOS_FAST_L(CASE_B) }
 #undef CASE_B
+    return cudaErrorNotSupported;
+}
+
+cudaError_t fast_rows_acc(int fp64, int L, int E, const FastRows& a, const AccArgs& acc, cudaStream_t st,
+                          int* nblocks) {
+#define CASE_A(LL)                                                                    \
+    case LL:                                                                          \
+        if (fp64) {                                                                   \
+            if constexpr (LL <= 4096) {                                               \
+                if (E == 8) return go_rows_acc<double, LL, 8>(a, acc, st, nblocks);   \
+            } else {                                                                  \
+                if (E == 16) return go_rows_acc<double, LL, 16>(a, acc, st, nblocks); \
+            }                                                                         \
+        } else {                                                                      \
+            if constexpr (LL <= 4096) {                                               \
+                if (E == 8) return go_rows_acc<float, LL, 8>(a, acc, st, nblocks);    \
+            }                                                                         \
+            if (E == 16) return go_rows_acc<float, LL, 16>(a, acc, st, nblocks);      \
+        }                                                                             \
+        break;
+    switch (L) { WOS_FAST_L(CASE_A) }
+#undef CASE_A
     return cudaErrorNotSupported;
 }
 

@@ -49,6 +49,15 @@ struct FastCols {
     double* hist;
     double hist_dx;
     unsigned* err;        // device error word of the pipelined kernels (bit 0: a bounded wait expired)
+    // batches of units (polychromatic wavelengths, volume distances): unit b =
+    // blockIdx.y reads src + b * src_bstride (src null: in place) and writes
+    // data + b * bstride; its wavelength and distance come from batch_wl[b] /
+    // batch_z[b] when given (else wl / z)
+    const void* src;
+    long long src_bstride;
+    const double* batch_wl;
+    const double* batch_z;
+    double z;
 };
 
 cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaStream_t st, int* nblocks);
@@ -68,6 +77,18 @@ struct DesignArgs {
 };
 cudaError_t fast_rows_design(int fp64, int L, int E, int stage, const FastRows& a, const DesignArgs& d,
                              cudaStream_t st, int* nblocks);
+
+// Inverse row transforms of the units of a batch, accumulated as weighted
+// intensity in one pass: out[r][x] (+)= sum_u w[u] |IFFT(in_u)[r][x]|^2, in_u =
+// in + u * in_bstride (nb units), out FP64 [rows][L].
+struct AccArgs {
+    int nb;
+    const double* weight;  // per unit, or null (1)
+    double* out;
+    int add;               // add to out instead of overwriting it
+};
+cudaError_t fast_rows_acc(int fp64, int L, int E, const FastRows& a, const AccArgs& acc, cudaStream_t st,
+                          int* nblocks);
 
 // One split-step slice on rows: inverse transform, slice screen, forward
 // transform (native precision in and out, in place allowed).

@@ -310,21 +310,35 @@ static __device__ __noinline__ double ev_amp_d(double rho, double kaz, int zero_
     return exp(-decay);
 }
 
+// Wavelength and distance of one unit of a batch (or of the single launch):
+// k = 2 pi / wl, kz = k z, k |z|, kz / 2 pi, formed as the host forms them.
+struct HUnit {
+    double wl, kz, kaz, krev;
+};
+__device__ __forceinline__ HUnit h_unit(const FastCols& a, int b) {
+    if (!a.batch_wl && !a.batch_z) return HUnit{a.wl, a.kz, a.kaz, a.krev};
+    const double wl = a.batch_wl ? a.batch_wl[b] : a.wl;
+    const double z = a.batch_z ? a.batch_z[b] : a.z;
+    const double k = 2 * M_PI / wl;
+    const double kz = k * z;
+    return HUnit{wl, kz, k * fabs(z), kz / (2 * M_PI)};
+}
+
 // H(fx, fy) of asmTF (optics/propagate.go:159-181) times `scale` (conj(H)
 // for the adjoint) and |H|^2, FP32 pipeline: cx = 1 - (wl fx)^2 of the
 // column, ay = wl fy; the FP64 argument kz sqrt(1 - rho^2) is taken in
 // revolutions (|kz / 2 pi| < 2^28, checked by the host) and reduced exactly.
-__device__ __forceinline__ float2 h_f32(const FastCols& a, double cx, double ay, double& m2) {
+__device__ __forceinline__ float2 h_f32(const FastCols& a, const HUnit& hu, double cx, double ay, double& m2) {
     const double sq = fma(-ay, ay, cx);
     float hr, hi;
     m2 = 1.0;
     if (sq >= 0) {  // rho <= 1: propagating
         const double sr = sq > 0x1p-100 ? fast_sqrt_bits(sq) : 0.0;
-        const float2 e = cexp_rev(a.krev * sr, a.precise_phase != 0);
+        const float2 e = cexp_rev(hu.krev * sr, a.precise_phase != 0);
         hr = e.x;
         hi = e.y;
     } else {
-        const double amp = ev_amp_f(sq, a.kaz, a.zero_ev, a.limit, a.backward, a.reg, a.alpha);
+        const double amp = ev_amp_f(sq, hu.kaz, a.zero_ev, a.limit, a.backward, a.reg, a.alpha);
         hr = (float)amp;
         hi = 0.f;
         m2 = amp * amp;
@@ -335,8 +349,8 @@ __device__ __forceinline__ float2 h_f32(const FastCols& a, double cx, double ay,
 
 // The same in the FP64 pipeline, with the reference's operation sequence
 // (uncontracted): px = |wl fx| of the column, fy = freq(q).
-__device__ __forceinline__ double2 h_f64(const FastCols& a, double px, double fy, double& m2) {
-    double p = px, qv = fabs(__dmul_rn(a.wl, fy));
+__device__ __forceinline__ double2 h_f64(const FastCols& a, const HUnit& hu, double px, double fy, double& m2) {
+    double p = px, qv = fabs(__dmul_rn(hu.wl, fy));
     if (p < qv) { const double t = p; p = qv; qv = t; }
     double rho = 0;
     if (p != 0) {
@@ -346,9 +360,9 @@ __device__ __forceinline__ double2 h_f64(const FastCols& a, double px, double fy
     double hr, hi;
     m2 = 1.0;
     if (rho <= 1.0) {
-        sincos(__dmul_rn(a.kz, __dsqrt_rn(__dmul_rn(__dsub_rn(1.0, rho), __dadd_rn(1.0, rho)))), &hi, &hr);
+        sincos(__dmul_rn(hu.kz, __dsqrt_rn(__dmul_rn(__dsub_rn(1.0, rho), __dadd_rn(1.0, rho)))), &hi, &hr);
     } else {
-        const double amp = ev_amp_d(rho, a.kaz, a.zero_ev, a.limit, a.backward, a.reg, a.alpha);
+        const double amp = ev_amp_d(rho, hu.kaz, a.zero_ev, a.limit, a.backward, a.reg, a.alpha);
         hr = amp;
         hi = 0;
         m2 = amp * amp;
@@ -363,7 +377,8 @@ __device__ __forceinline__ double2 h_f64(const FastCols& a, double px, double fy
 // l1 += |F|^2 (1 - |H|^2) when the loss sums are requested.  Every thread of
 // the CTA calls this between two barriers.
 template <typename Real, int L, int E, int W, typename C>
-__device__ __forceinline__ void col_tile_h(C* tile, int col0, const FastCols& a, double& p0, double& l1) {
+__device__ __forceinline__ void col_tile_h(C* tile, int col0, const FastCols& a, const HUnit& hu, double& p0,
+                                           double& l1) {
     constexpr int T = L / E;
     const int w = threadIdx.x & (W - 1);
     const int tt = threadIdx.x / W;
@@ -381,39 +396,39 @@ __device__ __forceinline__ void col_tile_h(C* tile, int col0, const FastCols& a,
     };
     if constexpr (sizeof(Real) == 4) {
         const double fx = (col <= a.ncols / 2 ? (double)col : (double)(col - a.ncols)) / ((double)a.ncols * a.dx);
-        const double ax = a.wl * fx;
+        const double ax = hu.wl * fx;
         const double cx = fma(-ax, ax, 1.0);
-        const double g = a.wl / ((double)L * a.dx);
+        const double g = hu.wl / ((double)L * a.dx);
         const double tg = (double)T * g, ay0 = (double)tt * g;
 #pragma unroll
         for (int i = 0; i < E / 2; i++) {
             const int q = tt + i * T;
             double m2;
-            const float2 h = h_f32(a, cx, fma((double)i, tg, ay0), m2);
+            const float2 h = h_f32(a, hu, cx, fma((double)i, tg, ay0), m2);
             apply(q, h, m2);
             if (q != 0) apply(L - q, h, m2);
         }
         if (tt == 0) {
             double m2;
-            const float2 h = h_f32(a, cx, (double)(L / 2) * g, m2);
+            const float2 h = h_f32(a, hu, cx, (double)(L / 2) * g, m2);
             apply(L / 2, h, m2);
         }
     } else {
         const double fxe = (col <= a.ncols / 2) ? __ddiv_rn((double)col, __dmul_rn((double)a.ncols, a.dx))
                                                 : __ddiv_rn((double)(col - a.ncols), __dmul_rn((double)a.ncols, a.dx));
         const double den = __dmul_rn((double)L, a.dx);
-        const double px = fabs(__dmul_rn(a.wl, fxe));
+        const double px = fabs(__dmul_rn(hu.wl, fxe));
 #pragma unroll
         for (int i = 0; i < E / 2; i++) {
             const int q = tt + i * T;
             double m2;
-            const double2 h = h_f64(a, px, __ddiv_rn((double)q, den), m2);
+            const double2 h = h_f64(a, hu, px, __ddiv_rn((double)q, den), m2);
             apply(q, h, m2);
             if (q != 0) apply(L - q, h, m2);
         }
         if (tt == 0) {
             double m2;
-            const double2 h = h_f64(a, px, __ddiv_rn((double)(L / 2), den), m2);
+            const double2 h = h_f64(a, hu, px, __ddiv_rn((double)(L / 2), den), m2);
             apply(L / 2, h, m2);
         }
     }
@@ -425,7 +440,7 @@ __device__ __forceinline__ void col_tile_h(C* tile, int col0, const FastCols& a,
 // reloaded in the natural order of the inverse transform's first pass.
 template <typename Real, int L, int E, int W, typename C>
 __device__ __forceinline__ void col_spectral_stage(C* v, C* tile, double* hsm, int col0, const FastCols& a,
-                                                   double& p0, double& l1) {
+                                                   const HUnit& hu, double& p0, double& l1) {
     constexpr int T = L / E;
     const int w = threadIdx.x & (W - 1);
     const int tt = threadIdx.x / W;
@@ -437,7 +452,7 @@ __device__ __forceinline__ void col_spectral_stage(C* v, C* tile, double* hsm, i
         col_hist_bin(tile, hsm, col0, L, W, a.ncols, a.hist_dx);
         __syncthreads();
     }
-    col_tile_h<Real, L, E, W>(tile, col0, a, p0, l1);
+    col_tile_h<Real, L, E, W>(tile, col0, a, hu, p0, l1);
     __syncthreads();
 #pragma unroll
     for (int s = 0; s < E; s++) v[s] = tile[(tt + s * T) * W + w];

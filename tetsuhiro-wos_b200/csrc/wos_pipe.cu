@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, 
 #pragma unroll
         for (int s = 0; s < E; s++) v[s] = stg[fpos<R1, E, L>(s, tt) * W + w];
         fpasses<L, E, false, 0, W>(v, stg + w, tt, twp);
-        col_spectral_stage<Real, L, E, W>(v, stg, hsm, c0, a, p0, l1);
+        col_spectral_stage<Real, L, E, W>(v, stg, hsm, c0, a, h_unit(a, b), p0, l1);
         fpasses<L, E, true, 0, W>(v, stg + w, tt, twp);
         if (act) {
             constexpr int RO = PL::RS;
@@ -368,6 +368,7 @@ cudaError_t go_cols_pipe_w(const FastCols& a, cudaStream_t st, int* nblocks) {
                   CP::SMEM > kMaxSmem) {
         return cudaErrorNotSupported;
     } else {
+        if (a.src) return cudaErrorNotSupported;  // the tensor map covers the in-place plane only
         const int nb = a.batch > 0 ? a.batch : 1;
         const long long bstride = nb > 1 ? a.bstride : a.ld * L;
         if (!aligned16(a.data, a.ld * esz, bstride * esz)) return cudaErrorNotSupported;

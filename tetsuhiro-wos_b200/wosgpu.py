@@ -151,6 +151,15 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
 
 
+def _out_array(out, shape, dtype):
+    """A caller-supplied output array (e.g. page-locked) after checking it, else a new one."""
+    if out is None:
+        return np.zeros(shape, dtype=dtype)
+    if out.shape != tuple(shape) or out.dtype != dtype or not out.flags["C_CONTIGUOUS"]:
+        raise WosError(1, f"output array must be C-contiguous {dtype.__name__} {tuple(shape)}")
+    return out
+
+
 def device_count() -> int:
     return lib().wos_device_count()
 
@@ -396,11 +405,11 @@ class GPU:
 
     # ---- batches (warnings of every unit accumulate into ctx, like the shared ctx.Warnings)
     def polychromatic(self, f: Field, z: float, wavelengths, weights, method: str = "asm",
-                      ctx: Optional[Context] = None) -> np.ndarray:
-        """PropagatePolychromatic (polychromatic.go:18-44)."""
+                      ctx: Optional[Context] = None, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """PropagatePolychromatic (polychromatic.go:18-44); `out` (float64 (ny, nx)) may be supplied."""
         wl = np.ascontiguousarray(wavelengths, dtype=np.float64)
         w = np.ascontiguousarray(weights, dtype=np.float64)
-        out = np.zeros((f.ny, f.nx))
+        out = _out_array(out, (f.ny, f.nx), np.float64)
         d = CDiag()
         cc = ctx.c() if ctx is not None else None
         _check(lib().wos_polychromatic(self.h, C.byref(f.c()), z, _ptr(wl), _ptr(w), wl.size, METHODS[method],
@@ -409,11 +418,12 @@ class GPU:
             ctx.absorb(d)
         return out
 
-    def volume(self, f: Field, zs, method: str = "asm", ctx: Optional[Context] = None) -> np.ndarray:
-        """Propagate3D (volume.go:8-18): (nz, ncomp, ny, nx) complex128."""
+    def volume(self, f: Field, zs, method: str = "asm", ctx: Optional[Context] = None,
+               out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Propagate3D (volume.go:8-18): (nz, ncomp, ny, nx) complex128; `out` may be supplied."""
         zz = np.ascontiguousarray(zs, dtype=np.float64)
         ncomp = 2 if f.polarized else 1
-        out = np.zeros((zz.size, ncomp, f.ny, f.nx), dtype=np.complex128)
+        out = _out_array(out, (zz.size, ncomp, f.ny, f.nx), np.complex128)
         d = CDiag()
         cc = ctx.c() if ctx is not None else None
         _check(lib().wos_volume(self.h, C.byref(f.c()), _ptr(zz), zz.size, METHODS[method],
@@ -431,11 +441,12 @@ class GPU:
         return out
 
     def partially_coherent(self, n: int, dx: float, width: float, coherence: float, noise: np.ndarray,
-                           z: float, method: str = "asm", ctx: Optional[Context] = None) -> np.ndarray:
-        """PropagatePartiallyCoherent (coherence.go:105-116)."""
+                           z: float, method: str = "asm", ctx: Optional[Context] = None,
+                           out: Optional[np.ndarray] = None) -> np.ndarray:
+        """PropagatePartiallyCoherent (coherence.go:105-116); `out` (float64 (n, n)) may be supplied."""
         noise = np.ascontiguousarray(noise, dtype=np.complex128)
         m = noise.shape[0]
-        out = np.zeros((n, n))
+        out = _out_array(out, (n, n), np.float64)
         d = CDiag()
         cc = ctx.c() if ctx is not None else None
         _check(lib().wos_partially_coherent(self.h, n, dx, width, coherence, m, _ptr(noise), z, METHODS[method],
