@@ -196,10 +196,21 @@ cudaError_t prof_cols(wos_ctx c, int fp64, const ColArgs& a) {
 
 int get_axis(wos_ctx c, int n, int fp64, Axis** out);
 
+bool mixed_radix_ok(int n) {
+    if (n < 4 || (n & 1)) return false;
+    int m = n;
+    for (int f : {2, 3, 5})
+        while (m % f == 0) m /= f;
+    return m == 1 && !is_pow2(n);
+}
+
 int build_axis(wos_ctx c, int n, int fp64, Axis& ax) {
     const size_t cs = fp64 ? 16 : 8;
     ax.n = n;
-    ax.blue = is_pow2(n) ? 0 : 1;
+    // power-of-two lines and 2^a 3^b 5^c lines (a >= 1, a mixed-radix plan)
+    // are transformed directly; any other length through Bluestein's chirp
+    // convolution on a power-of-two length M >= 2n - 1
+    ax.blue = (is_pow2(n) || mixed_radix_ok(n)) ? 0 : 1;
     ax.L = ax.blue ? next_pow2(2 * n - 1) : n;
     if (n < 2) return fail(WOS_UNSUPPORTED_SIZE, "line length must be >= 2");
     if (ax.L > (fp64 ? kMaxL64 : kMaxL32))

@@ -138,12 +138,62 @@ __device__ __forceinline__ void dft16(C* v) {
     for (int i = 0; i < 8; i++) { v[i] = cadd(e[i], o[i]); v[i + 8] = csub(e[i], o[i]); }
 }
 
+// Radix 3 and 5 (mixed-radix lines): the DFT sums written with the real and
+// imaginary parts of the roots of unity, w = exp(-2 pi i / R) forward.
+template <typename C> struct K35;
+template <> struct K35<float2> {
+    static constexpr float S3 = 0.86602540378443864676f;  // sin(2 pi / 3)
+    static constexpr float C51 = 0.30901699437494742410f; // cos(2 pi / 5)
+    static constexpr float C52 = -0.80901699437494742410f;
+    static constexpr float S51 = 0.95105651629515357212f;
+    static constexpr float S52 = 0.58778525229247312917f;
+};
+template <> struct K35<double2> {
+    static constexpr double S3 = 0.86602540378443864676;
+    static constexpr double C51 = 0.30901699437494742410;
+    static constexpr double C52 = -0.80901699437494742410;
+    static constexpr double S51 = 0.95105651629515357212;
+    static constexpr double S52 = 0.58778525229247312917;
+};
+
+template <bool INV, typename C>
+__device__ __forceinline__ void dft3(C* v) {
+    using T = decltype(C::x);
+    const C s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+    const C m = mkc<C>(v[0].x - (T)0.5 * s.x, v[0].y - (T)0.5 * s.y);
+    const T k = INV ? -K35<C>::S3 : K35<C>::S3;  // forward: -i sin(2pi/3) (v1 - v2)
+    v[0] = cadd(v[0], s);
+    v[1] = mkc<C>(m.x + k * d.y, m.y - k * d.x);
+    v[2] = mkc<C>(m.x - k * d.y, m.y + k * d.x);
+}
+
+template <bool INV, typename C>
+__device__ __forceinline__ void dft5(C* v) {
+    using T = decltype(C::x);
+    const C a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]);
+    const C a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+    const T c1 = K35<C>::C51, c2 = K35<C>::C52;
+    const T s1 = INV ? -K35<C>::S51 : K35<C>::S51, s2 = INV ? -K35<C>::S52 : K35<C>::S52;
+    // y_k = v0 + sum_r v_r w^{rk}: real parts from a, -i sin parts from b
+    const C m1 = mkc<C>(v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y);
+    const C m2 = mkc<C>(v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y);
+    const C n1 = mkc<C>(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y);  // y1: -i * n1
+    const C n2 = mkc<C>(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y);  // y2: -i * n2
+    v[0] = mkc<C>(v[0].x + a1.x + a2.x, v[0].y + a1.y + a2.y);
+    v[1] = mkc<C>(m1.x + n1.y, m1.y - n1.x);
+    v[4] = mkc<C>(m1.x - n1.y, m1.y + n1.x);
+    v[2] = mkc<C>(m2.x + n2.y, m2.y - n2.x);
+    v[3] = mkc<C>(m2.x - n2.y, m2.y + n2.x);
+}
+
 template <int R, bool INV, typename C>
 __device__ __forceinline__ void dft(C* v) {
     if (R == 2) dft2<INV>(v[0], v[1]);
     else if (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
     else if (R == 8) dft8<INV>(v);
     else if (R == 16) dft16<INV>(v);
+    else if (R == 3) dft3<INV>(v);
+    else if (R == 5) dft5<INV>(v);
 }
 
 // ------------------------------------------------------------- shared layouts
@@ -229,17 +279,24 @@ __device__ __forceinline__ int pass_radix(bool inv, int p, int P, int rs, int E)
 
 // Plan of a line transform: number of passes and the small radix.
 struct LinePlan {
-    int L;    // length (power of two)
+    int L;    // length (power of two, or 2^a 3^b 5^c for a mixed-radix line)
     int P;    // passes
     int rs;   // small radix (1 if none)
+    int mixed;  // 1: radix 16/8/4/2/3/5 passes through shared memory (mixed_line_fft)
 };
 __host__ __device__ inline LinePlan make_line_plan(int L, int E) {
+    LinePlan p;
+    p.L = L;
+    p.mixed = (L & (L - 1)) != 0;
+    if (p.mixed) {  // registers hold positions tt + s*T on entry and exit
+        p.P = 0;
+        p.rs = 1;
+        return p;
+    }
     int lg = 0;
     while ((1 << lg) < L) lg++;
     int le = 0;
     while ((1 << le) < E) le++;
-    LinePlan p;
-    p.L = L;
     p.P = lg / le + ((lg % le) ? 1 : 0);
     p.rs = (lg % le) ? (1 << (lg % le)) : 1;
     return p;
@@ -270,6 +327,84 @@ __device__ __forceinline__ void line_fft(C* v, C* sm, const IDX& ix, int line, i
         }
         Ns *= R;
     }
+}
+
+// One Stockham pass of a mixed-radix line held in shared memory: butterfly
+// j < L/R (sub-transform length NS, k = j mod NS) reads x[j + r L/R], takes
+// the twiddles W_L^{r k L/(NS R)} from the L-point table, and writes
+// positions (j - k) R + k + r NS.  A thread stages its ceil(E/R) butterflies
+// in registers between the two barriers, so the pass works in place.
+template <int R, int E, bool INV, typename C, typename IDX>
+__device__ __forceinline__ void mixed_pass(C* sm, const IDX& ix, int line, int tt, int T, int L, int NS,
+                                           const C* __restrict__ tw) {
+    constexpr int NB = (E + R - 1) / R;
+    const int nbf = L / R, LR = L / R;
+    C x[NB][R];
+#pragma unroll
+    for (int i = 0; i < NB; i++) {
+        const int j = tt + i * T;
+        if (j < nbf) {
+#pragma unroll
+            for (int r = 0; r < R; r++) x[i][r] = sm[ix(line, j + r * LR)];
+        }
+    }
+    __syncthreads();
+    const int step = L / (NS * R);
+#pragma unroll
+    for (int i = 0; i < NB; i++) {
+        const int j = tt + i * T;
+        if (j < nbf) {
+            const int k = j % NS;
+            if (NS > 1) {
+#pragma unroll
+                for (int r = 1; r < R; r++) {
+                    C w = ldg_c(tw + r * k * step);
+                    if (INV) w.y = -w.y;
+                    x[i][r] = cmul(x[i][r], w);
+                }
+            }
+            dft<R, INV>(x[i]);
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; r++) sm[ix(line, base + r * NS)] = x[i][r];
+        }
+    }
+    __syncthreads();
+}
+
+// Mixed-radix line transform (L = 2^a 3^b 5^c, a >= 1): registers (positions
+// tt + s*T) to shared memory, radix 16 / 8 / 4 / 2 then 3 then 5 passes in
+// place, back to the same registers.  Must be called by every thread of the
+// CTA (it synchronises).
+template <int E, bool INV, typename C, typename IDX>
+__device__ __forceinline__ void mixed_line_fft(C* v, C* sm, const IDX& ix, int line, int tt, int T, int L,
+                                               const C* __restrict__ tw) {
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < E; s++) sm[ix(line, tt + s * T)] = v[s];
+    __syncthreads();
+    int rem = L, NS = 1;
+    while (rem > 1) {
+        int R;
+        if (rem % 16 == 0) R = 16;
+        else if (rem % 8 == 0) R = 8;
+        else if (rem % 4 == 0) R = 4;
+        else if (rem % 2 == 0) R = 2;
+        else if (rem % 3 == 0) R = 3;
+        else R = 5;
+        switch (R) {
+        case 16: mixed_pass<16, E, INV>(sm, ix, line, tt, T, L, NS, tw); break;
+        case 8: mixed_pass<8, E, INV>(sm, ix, line, tt, T, L, NS, tw); break;
+        case 4: mixed_pass<4, E, INV>(sm, ix, line, tt, T, L, NS, tw); break;
+        case 2: mixed_pass<2, E, INV>(sm, ix, line, tt, T, L, NS, tw); break;
+        case 3: mixed_pass<3, E, INV>(sm, ix, line, tt, T, L, NS, tw); break;
+        default: mixed_pass<5, E, INV>(sm, ix, line, tt, T, L, NS, tw); break;
+        }
+        NS *= R;
+        rem /= R;
+    }
+#pragma unroll
+    for (int s = 0; s < E; s++) v[s] = sm[ix(line, tt + s * T)];
 }
 
 // Position held by register slot s (= b*R + r) under the natural mapping of radix R.

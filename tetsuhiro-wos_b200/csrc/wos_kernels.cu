@@ -258,9 +258,14 @@ __device__ __forceinline__ int in_radix(const LinePlan& lp, bool inv, bool blue,
 __device__ __forceinline__ int out_radix(const LinePlan& lp, bool inv, bool blue, int E) {
     return (blue || inv) ? last_radix(lp, true, E) : E;
 }
-template <int E, typename C, typename IDX>
+template <int E, bool MIX, typename C, typename IDX>
 __device__ __forceinline__ void xform(C* v, C* sm, const IDX& ix, int line, int tt, int T, const LinePlan& lp,
                                       const C* __restrict__ tw, bool inv, const C* __restrict__ bhat) {
+    if constexpr (MIX) {  // kernels launched for mixed-radix lines only
+        if (inv) mixed_line_fft<E, true>(v, sm, ix, line, tt, T, lp.L, tw);
+        else mixed_line_fft<E, false>(v, sm, ix, line, tt, T, lp.L, tw);
+        return;
+    }
     if (!bhat) {
         if (inv) line_fft<E, true>(v, sm, ix, line, tt, T, lp, tw);
         else line_fft<E, false>(v, sm, ix, line, tt, T, lp, tw);
@@ -276,7 +281,7 @@ __device__ __forceinline__ void xform(C* v, C* sm, const IDX& ix, int line, int 
 template <typename Real, int E> struct MaxT { static constexpr int v = (E >= 16 || sizeof(Real) == 8) ? 512 : 1024; };
 
 // ------------------------------------------------------------------ k_rows
-template <typename Real, int E>
+template <typename Real, int E, bool MIX>
 __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows(const RowArgs a) {
     using C = typename CT<Real>::t;
     using T_ = Real;
@@ -347,7 +352,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows(const RowArgs a) {
         }
 
         // ---- transform(s)
-        xform<E>(v, sm, ix, line, tt, T, lp, tw, !fwd_first, fwd_first ? bhf : bhi);
+        xform<E, MIX>(v, sm, ix, line, tt, T, lp, tw, !fwd_first, fwd_first ? bhf : bhi);
         Rout = out_radix(lp, !fwd_first, blue, E);
         if (a.mode == ROW_INV_FWD) {
             // real-space screen between the inverse and the next forward row
@@ -362,7 +367,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows(const RowArgs a) {
                     v[s] = mkc<C>(0, 0);
                 }
             }
-            xform<E>(v, sm, ix, line, tt, T, lp, tw, false, bhf);
+            xform<E, MIX>(v, sm, ix, line, tt, T, lp, tw, false, bhf);
             Rout = out_radix(lp, false, blue, E);
             if (blue) {
 #pragma unroll
@@ -447,7 +452,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows(const RowArgs a) {
 }
 
 // ------------------------------------------------------------------ k_cols
-template <typename Real, int E>
+template <typename Real, int E, bool MIX>
 __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
     using C = typename CT<Real>::t;
     using T_ = Real;
@@ -493,7 +498,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
     }
 
     // first column transform
-    xform<E>(v, sm, ix, w, tt, T, lp, tw, inv_first, inv_first ? bhi : bhf);
+    xform<E, MIX>(v, sm, ix, w, tt, T, lp, tw, inv_first, inv_first ? bhi : bhf);
     int Rm = out_radix(lp, inv_first, blue, E);
     if (blue && (a.mode == COL_FRAUNHOFER || a.mode == COL_FFT)) {
         // the chirp of the Bluestein output has unit modulus: applied only
@@ -595,7 +600,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
     }
 
     if (a.mode == COL_FUSED) {
-        xform<E>(v, sm, ix, w, tt, T, lp, tw, true, bhi);
+        xform<E, MIX>(v, sm, ix, w, tt, T, lp, tw, true, bhi);
         Rm = out_radix(lp, true, blue, E);
         if (blue) {
 #pragma unroll
@@ -763,6 +768,7 @@ __global__ void k_scale_copy(const double2* src, C* dst, long long n, double sre
 int pick_E(int fp64, int L) {
     int e = fp64 ? (L >= 8192 ? 16 : 8) : 16;
     while (e > L) e >>= 1;
+    while (e > 2 && L % e != 0) e >>= 1;  // a mixed-radix line: E divides L
     return e;
 }
 int max_threads_for(int fp64, int E) { return (E >= 16 || fp64) ? 512 : 1024; }
@@ -782,13 +788,15 @@ static cudaError_t launch_rows_t(const RowArgs& a, cudaStream_t st) {
     while (lines * 2 * T <= 256 && lines * 2 <= a.rows) lines *= 2;
     while (lines * T < 32) lines *= 2;  // whole warps (idle lines are inactive)
     const size_t smem = (size_t)row_line_stride(a.L) * lines * sizeof(typename CT<Real>::t);
+    const bool mix = (a.L & (a.L - 1)) != 0;
+    auto kern = mix ? k_rows<Real, E, true> : k_rows<Real, E, false>;
     if (smem > kSmemNoOptIn) {
-        cudaError_t e = cudaFuncSetAttribute(k_rows<Real, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     const int nbat = (a.mode == ROW_INV_ACC) ? 1 : (a.batch > 0 ? a.batch : 1);
     dim3 grid((a.rows + lines - 1) / lines, nbat);
-    k_rows<Real, E><<<grid, lines * T, smem, st>>>(a);
+    kern<<<grid, lines * T, smem, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -801,12 +809,14 @@ static cudaError_t launch_cols_t(const ColArgs& a, cudaStream_t st) {
     while (b.W > 1 && b.W * T > maxt) b.W /= 2;
     if (b.W * T > maxt) return cudaErrorInvalidConfiguration;
     const size_t smem = (size_t)col_tile_elems(b.L, b.W) * sizeof(typename CT<Real>::t);
+    const bool mix = (b.L & (b.L - 1)) != 0;
+    auto kern = mix ? k_cols<Real, E, true> : k_cols<Real, E, false>;
     if (smem > kSmemNoOptIn) {
-        cudaError_t e = cudaFuncSetAttribute(k_cols<Real, E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     dim3 grid((b.ncols + b.W - 1) / b.W, b.batch > 0 ? b.batch : 1);
-    k_cols<Real, E><<<grid, b.W * T, smem, st>>>(b);
+    kern<<<grid, b.W * T, smem, st>>>(b);
     return cudaGetLastError();
 }
 
