@@ -39,7 +39,9 @@ def is_pow2(n: int) -> bool:
 
 
 def tol_case(precision, method: str, ny: int, nx: int) -> float:
-    """Parity tolerance of one propagation case (see the floors above)."""
+    """Parity tolerance of one propagation case (see the floors above; lengths
+    that are not powers of two take the Bluestein floor, which also covers the
+    mixed-radix 2/3/5 transforms)."""
     if precision != wos.FP64:
         return TOL_FP32
     t = TOL_FP64

@@ -110,6 +110,7 @@ CASES = [
     (48, 80, 1e-6, 532e-9, 2e-4, "random"),
     (64, 64, 0.25e-6, 1e-6, 1e-6, "random"),     # evanescent bins present
     (96, 60, 3e-6, 633e-9, -4e-3, "lens"),       # backward
+    (98, 70, 2e-6, 632.8e-9, 5e-3, "lens"),      # factors of 7: Bluestein lines
 ]
 
 

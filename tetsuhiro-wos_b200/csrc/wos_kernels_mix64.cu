@@ -1,0 +1,11 @@
+// wos_kernels_mix64.cu -- the general sweeps instantiated in FP64 for
+// mixed-radix (2^a 3^b 5^c) lines, compiled apart from the power-of-two ones.
+#define WOS_DEFINE_MIX_LAUNCHERS
+#include "wos_kernels_dev.cuh"
+
+namespace wos {
+WOS_MIX_INST(double, 2)
+WOS_MIX_INST(double, 4)
+WOS_MIX_INST(double, 8)
+WOS_MIX_INST(double, 16)
+}  // namespace wos
