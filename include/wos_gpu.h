@@ -255,6 +255,36 @@ WOS_API int wos_apply_grating(wos_ctx ctx, wos_field* f, int kind, double period
                       double duty, double blaze_depth, double rotation, double offset);
 WOS_API int wos_apply_phase_mask(wos_ctx ctx, wos_field* f, const double* phi, double amp);
 
+/* ---- field operations (optics/field.go:109-168,199-228,264-294), host Field in
+ *      place.  Element arithmetic is FP64 whatever the context precision; the
+ *      FFT filters (bandlimit, shift, diffuser correlation) run in it. ---- */
+/* Field.ApplyJones (field.go:109-131): [[a b] [c d]] at every pixel.  A scalar
+ * field with a non-diagonal or non-uniform matrix becomes polarized (Ey = c Ex;
+ * f->ey must hold ny*nx elements and f->polarized is set to 1). */
+WOS_API int wos_apply_jones(wos_ctx ctx, wos_field* f, wos_c128 a, wos_c128 b, wos_c128 c, wos_c128 d);
+/* Field.ScaleAmplitude (field.go:134-148). */
+WOS_API int wos_scale_amplitude(wos_ctx ctx, wos_field* f, wos_c128 s);
+/* Field.ApplyTilt (field.go:151-168): exp(i k (sin(tx) x + sin(ty) y)), the
+ * row phase accumulated pixel by pixel exactly as the reference sums it. */
+WOS_API int wos_apply_tilt(wos_ctx ctx, wos_field* f, double tx, double ty, double wavelength);
+/* Field.ApplyBandlimit (field.go:264-294): fraction / sigma of Nyquist;
+ * fraction outside (0, 1) leaves the field unchanged. */
+WOS_API int wos_apply_bandlimit(wos_ctx ctx, wos_field* f, double fraction, double sigma);
+/* Field.ShiftField (field.go:199-228): G(x, y) = F(x - du, y - dv) by a Fourier ramp. */
+WOS_API int wos_shift_field(wos_ctx ctx, wos_field* f, double du, double dv);
+/* diffuserEl.Apply (elements.go:722-783): hashNoise01 phase screen on the lab
+ * lattice, Gaussian correlation filter (correlation > 0), rescaled to standard
+ * deviation sigma, transmission amplitude * exp(i phase). */
+WOS_API int wos_apply_diffuser(wos_ctx ctx, wos_field* f, double sigma, double correlation, double amplitude,
+                               long long seed, double x0, double y0);
+
+/* ---- Propagate1D (optics/propagate.go:718-738): a[n] complex128 in place,
+ *      pixel dx, distance z, wavelength wl (the Context's wavelength is not
+ *      used).  diag (may be NULL): p_in / p_out are sum |a|^2 without a dx
+ *      factor (sum1DSq) and evanescent_filtered is the only warning. ---- */
+WOS_API int wos_propagate1d(wos_ctx ctx, int n, wos_c128* a, double dx, double z, double wavelength,
+                            const wos_context* c, wos_diag* diag);
+
 /* ---- inverse design (no counterpart in the reference): ASM forward / adjoint.
  *      u = ASM_z(a * exp(i phi)), L = sum (|u|^2 - T)^2, grad = dL/dphi. ---- */
 WOS_API int wos_asm_forward_loss(wos_ctx ctx, int ny, int nx, double dx, double z, const wos_context* c,
@@ -270,6 +300,27 @@ WOS_API int wos_asm_loss_grad(wos_ctx ctx, int ny, int nx, double dx, double z, 
 WOS_API int wos_asm_loss_grad_dev(wos_ctx ctx, int ny, int nx, double dx, double z, const wos_context* c,
                                   const void* a, const double* phi, const double* target, double* loss,
                                   double* grad);
+/* ---- diffractive stack (no counterpart in the reference): nlayers phase masks,
+ *      each followed by a split-step BPM segment of `steps` slices over zseg
+ *      through the parametric medium n (PropagateSplitStep, optics/medium.go:22-45):
+ *      u = a; for l: u = BPM(u * exp(i phis[l])); L = sum (|u|^2 - T)^2;
+ *      grads[l] = dL/dphis[l] by the exact adjoint chain.  Host arrays:
+ *      a [ny][nx] complex128, phis / grads [nlayers][ny][nx], target [ny][nx]
+ *      FP64; grads may be NULL (loss only). ---- */
+WOS_API int wos_bpm_stack_loss_grad(wos_ctx ctx, int ny, int nx, double dx, int nlayers, const wos_c128* a,
+                                    const double* phis, const double* target, double zseg,
+                                    const wos_index_desc* n, int steps, const wos_context* c, double* loss,
+                                    double* grads);
+/* Device-resident form: a of the context's complex type, phis / target /
+ * grads FP64 device arrays; the loss is returned to the host. */
+WOS_API int wos_bpm_stack_loss_grad_dev(wos_ctx ctx, int ny, int nx, double dx, int nlayers, const void* a,
+                                        const double* phis, const double* target, double zseg,
+                                        const wos_index_desc* n, int steps, const wos_context* c, double* loss,
+                                        double* grads);
+/* Adjoint of wos_splitstep_dev (conj transfer functions and screens, slices
+ * in reverse order), device field in place, no diagnostics. */
+WOS_API int wos_splitstep_adjoint_dev(wos_ctx ctx, int ny, int nx, double dx, int ncomp, void* field, double z,
+                                      const wos_index_desc* n, int steps, const wos_context* c);
 /* Adjoint operator A^H = F^-1 diag(conj H) F of an ASM step, host field in place. */
 WOS_API int wos_asm_adjoint(wos_ctx ctx, wos_field* f, double z, const wos_context* c);
 

@@ -10,6 +10,10 @@
 //   Propagate3D                 optics/volume.go:8-18
 //   GenerateSchellRealizations, PropagatePartiallyCoherent
 //                               optics/coherence.go:22-116
+//   Propagate1D                 optics/propagate.go:718-738
+//   Field.ApplyJones / ScaleAmplitude / ApplyTilt / ShiftField / ApplyBandlimit
+//                               optics/field.go:109-168,199-228,264-294
+//   ApplyDiffuser               optics/elements.go:722-783 (diffuserEl.Apply)
 //   SetGPU / GPUEnabled / GPUAvailable / GPUBackendInfo
 //                               optics/gpu.go:106-143 (WOS_GPU=1 enables)
 //
@@ -293,6 +297,50 @@ inline std::vector<double> PropagatePartiallyCoherent(Backend& b, int n, double 
                                  &d));
     ctx->absorb(d);
     return out;
+}
+
+// Propagate1D: a line of n = a.size() samples in place (wl apart from ctx).
+inline void Propagate1D(Backend& b, std::vector<cplx>& a, double dx, double z, double wl, Context* ctx) {
+    Context local;
+    if (!ctx) ctx = &local;
+    wos_diag d{};
+    wos_context cc = ctx->c();
+    check(wos_propagate1d(b.handle(), (int)a.size(), reinterpret_cast<wos_c128*>(a.data()), dx, z, wl, &cc, &d));
+    ctx->absorb(d);
+}
+
+inline wos_c128 c128(cplx v) { return wos_c128{v.real(), v.imag()}; }
+
+// Field methods of the reference, as free functions over a Backend.
+inline void ApplyJones(Backend& b, Field& f, cplx a, cplx bb, cplx c, cplx d) {
+    wos_field cf = f.c();
+    check(wos_apply_jones(b.handle(), &cf, c128(a), c128(bb), c128(c), c128(d)));
+    f.Polarized = cf.polarized != 0;
+}
+inline void ScaleAmplitude(Backend& b, Field& f, cplx s) {
+    wos_field cf = f.c();
+    check(wos_scale_amplitude(b.handle(), &cf, c128(s)));
+}
+inline void ApplyTilt(Backend& b, Field& f, double tx, double ty, double wl) {
+    wos_field cf = f.c();
+    check(wos_apply_tilt(b.handle(), &cf, tx, ty, wl));
+}
+inline void ShiftField(Backend& b, Field& f, double du, double dv) {
+    wos_field cf = f.c();
+    check(wos_shift_field(b.handle(), &cf, du, dv));
+}
+struct BandlimitOpts {
+    double Fraction = 0, Sigma = 0;
+};
+inline void ApplyBandlimit(Backend& b, Field& f, const BandlimitOpts* bl) {
+    if (!bl) return;
+    wos_field cf = f.c();
+    check(wos_apply_bandlimit(b.handle(), &cf, bl->Fraction, bl->Sigma));
+}
+inline void ApplyDiffuser(Backend& b, Field& f, double sigma, double correlation, double amplitude, long long seed,
+                          double x0, double y0) {
+    wos_field cf = f.c();
+    check(wos_apply_diffuser(b.handle(), &cf, sigma, correlation, amplitude, seed, x0, y0));
 }
 
 }  // namespace optics

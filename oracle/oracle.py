@@ -38,6 +38,15 @@ class _Context(C.Structure):
     ]
 
 
+class _C128(C.Structure):
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
+def _c128(v) -> _C128:
+    v = complex(v)
+    return _C128(v.real, v.imag)
+
+
 class _Field(C.Structure):
     _fields_ = [
         ("ny", C.c_int), ("nx", C.c_int), ("dx", C.c_double), ("polarized", C.c_int),
@@ -97,11 +106,15 @@ def lib():
         L.or_apply_diffuser.argtypes = [vp, d, d, d, C.c_longlong, d, d]
         L.or_apply_phase_mask.argtypes = [vp, vp, d]
         L.or_apply_tilt.argtypes = [vp, d, d, d]
+        L.or_apply_jones.argtypes = [vp, _C128, _C128, _C128, _C128]
+        L.or_scale_amplitude.argtypes = [vp, _C128]
         L.or_apply_bandlimit.argtypes = [vp, d, d]
         L.or_shift_field.argtypes = [vp, d, d]
         L.or_index_eval.argtypes = [vp, i, i, d, i, i, d, d, d, vp, vp]
         L.or_asm_phase_loss_grad.argtypes = [i, i, d, d, vp, vp, vp, vp, vp]
         L.or_asm_phase_loss_grad.restype = d
+        L.or_bpm_stack_loss_grad.argtypes = [i, i, d, i, vp, vp, vp, d, i, vp, vp, vp]
+        L.or_bpm_stack_loss_grad.restype = d
         L.or_set_threads.argtypes = [i]
         L.or_get_threads.restype = i
         _lib = L
@@ -339,6 +352,16 @@ def apply_phase_mask(f: Field, phi: np.ndarray, amp=1.0):
     lib().or_apply_phase_mask(C.byref(f._c()), _ptr(phi), amp)
 
 
+def apply_jones(f: Field, a, b, c, d):
+    cf = f._c()
+    lib().or_apply_jones(C.byref(cf), _c128(a), _c128(b), _c128(c), _c128(d))
+    f._sync(cf)
+
+
+def scale_amplitude(f: Field, s):
+    lib().or_scale_amplitude(C.byref(f._c()), _c128(s))
+
+
 def apply_tilt(f: Field, tx, ty, wl):
     lib().or_apply_tilt(C.byref(f._c()), tx, ty, wl)
 
@@ -362,6 +385,21 @@ def asm_phase_loss_grad(a: np.ndarray, phi: np.ndarray, target: np.ndarray, dx: 
     loss = lib().or_asm_phase_loss_grad(ny, nx, dx, z, C.byref(cc), _ptr(a), _ptr(phi),
                                         _ptr(target), _ptr(grad) if want_grad else None)
     return loss, grad
+
+
+def bpm_stack_loss_grad(a: np.ndarray, phis: np.ndarray, target: np.ndarray, dx: float, zseg: float,
+                        steps: int, desc: IndexDesc, ctx: Context, want_grad: bool = True):
+    """Diffractive stack (masks phis[l] with a BPM segment of `steps` slices
+    over zseg after each): loss sum (|u|^2 - T)^2 and dL/dphi per layer."""
+    a = np.ascontiguousarray(a, dtype=np.complex128)
+    phis = np.ascontiguousarray(phis, dtype=np.float64)
+    target = np.ascontiguousarray(target, dtype=np.float64)
+    nl, ny, nx = phis.shape
+    grads = np.zeros((nl, ny, nx)) if want_grad else None
+    cc = ctx._to_c()
+    loss = lib().or_bpm_stack_loss_grad(ny, nx, dx, nl, _ptr(a), _ptr(phis), _ptr(target), zseg, steps,
+                                        C.byref(desc), C.byref(cc), _ptr(grads) if want_grad else None)
+    return loss, grads
 
 
 def set_threads(p: int) -> None:

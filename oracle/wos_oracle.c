@@ -1181,3 +1181,94 @@ double or_asm_phase_loss_grad(int ny, int nx, double dx, double z, const or_cont
     free(u); free(t);
     return loss;
 }
+
+/* ------------------------------------------------------------------ */
+/* Diffractive stack: phase masks with split-step BPM segments between */
+/* them (no reference counterpart).                                     */
+/* ------------------------------------------------------------------ */
+/* Adjoint of one Propagate(z) step of the plain ASM: F^-1 diag(conj H) F. */
+static void asm_adjoint_arr(oc128 *a, int ny, int nx, double dx, double z, const or_context *ctx) {
+    tf_spec tf = {0};
+    tf.kind = 0; tf.wl = ctx->wavelength; tf.z = z;
+    ev_policy(ctx, z, &tf.zero, &tf.reg, &tf.alpha, &tf.limit);
+    or_fft2d(a, ny, nx, 0);
+    for (int j = 0; j < ny; j++) {
+        double fy = freq_n(j, ny, dx);
+        for (int i = 0; i < nx; i++) {
+            size_t idx = (size_t)j * nx + i;
+            oc128 h = tf_eval(&tf, freq_n(i, nx, dx), fy);
+            h.im = -h.im;
+            a[idx] = cmul(a[idx], h);
+        }
+    }
+    or_fft2d(a, ny, nx, 1);
+}
+
+/* Adjoint of splitstep_core with a parametric medium: the slices in reverse
+ * order, each A(dz/2)^H M_s^H A(dz/2)^H with M_s^H = conj of the screen. */
+static void splitstep_adjoint(oc128 *a, int ny, int nx, double dx, double z, const or_index_desc *d, int steps,
+                              const or_context *ctx) {
+    if (z == 0) return;
+    if (steps <= 0) steps = 1;
+    double dz = z / (double)steps;
+    double k = 2 * M_PI / ctx->wavelength;
+    for (int s = steps - 1; s >= 0; s--) {
+        double zc = z * (double)s / (double)steps + dz / 2;
+        asm_adjoint_arr(a, ny, nx, dx, dz / 2, ctx);
+        for (int j = 0; j < ny; j++) {
+            double y = ((double)j - (double)ny / 2) * dx;
+            for (int i = 0; i < nx; i++) {
+                size_t idx = (size_t)j * nx + i;
+                double nr, ni;
+                or_index_eval(d, ny, nx, dx, i, j, ((double)i - (double)nx / 2) * dx, y, zc, &nr, &ni);
+                double ph = k * (nr - 1) * dz;
+                oc128 t = cmul(cmk(exp(-k * ni * dz), 0), cexpi(-ph));
+                a[idx] = cmul(a[idx], t);
+            }
+        }
+        asm_adjoint_arr(a, ny, nx, dx, dz / 2, ctx);
+    }
+}
+
+double or_bpm_stack_loss_grad(int ny, int nx, double dx, int nl, const oc128 *a, const double *phis,
+                              const double *target, double zseg, int steps, const or_index_desc *d,
+                              const or_context *ctx_in, double *grads) {
+    size_t n = (size_t)ny * nx;
+    or_context ctx = *ctx_in;
+    ctx.has_warnings = 0;
+    oc128 *u = (oc128 *)malloc(sizeof(oc128) * n);
+    oc128 *ey = (oc128 *)calloc(n, sizeof(oc128));
+    oc128 *V = (oc128 *)malloc(sizeof(oc128) * n * (size_t)(nl > 0 ? nl : 1));
+    memcpy(u, a, sizeof(oc128) * n);
+    or_field f = {ny, nx, dx, 0, u, ey};
+    for (int l = 0; l < nl; l++) {
+        const double *phi = phis + (size_t)l * n;
+        for (size_t i = 0; i < n; i++) u[i] = cmul(u[i], cexpi(phi[i]));
+        memcpy(V + (size_t)l * n, u, sizeof(oc128) * n);
+        or_splitstep(&f, zseg, d, steps, &ctx);
+    }
+    double loss = 0;
+    for (size_t i = 0; i < n; i++) {
+        double dd = cabs2(u[i]) - target[i];
+        loss += dd * dd;
+        u[i] = cmul(cmk(4 * dd, 0), u[i]); /* r = dL/du* */
+    }
+    if (grads) {
+        for (int l = nl - 1; l >= 0; l--) {
+            const double *phi = phis + (size_t)l * n;
+            const oc128 *v = V + (size_t)l * n;
+            double *g = grads + (size_t)l * n;
+            splitstep_adjoint(u, ny, nx, dx, zseg, d, steps, &ctx);
+            for (size_t i = 0; i < n; i++) {
+                /* g = Re(conj(b) * i * v), v = field just after mask l */
+                oc128 iv = cmul(cmk(0, 1), v[i]);
+                oc128 cb = cmk(u[i].re, -u[i].im);
+                g[i] = cmul(cb, iv).re;
+                oc128 t = cexpi(phi[i]);
+                u[i] = cmul(u[i], cmk(t.re, -t.im));
+            }
+        }
+    }
+    free(u); free(ey); free(V);
+    return loss;
+}

@@ -145,6 +145,14 @@ double or_asm_phase_loss_grad(int ny, int nx, double dx, double z, const or_cont
                               const oc128 *a, const double *phi, const double *target,
                               double *grad /* may be NULL */);
 
+/* Diffractive stack: u_0 = a; for each layer l: u = BPM_zseg(u * exp(i phi_l))
+ * (split-step, `steps` slices, parametric medium d); L = sum (|u|^2 - T)^2;
+ * grads[l] = dL/dphi_l by the exact adjoint (conj transfer functions and
+ * screens, slices in reverse order). */
+double or_bpm_stack_loss_grad(int ny, int nx, double dx, int nl, const oc128 *a, const double *phis,
+                              const double *target, double zseg, int steps, const or_index_desc *d,
+                              const or_context *ctx, double *grads /* may be NULL */);
+
 #ifdef __cplusplus
 }
 #endif

@@ -548,3 +548,62 @@ def test_hash_noise01_known_values():
         h ^= h >> 27; h = (h * 0x94D049BB133111EB) & M
         h ^= h >> 31
         assert O.hash_noise01(x, y, s) == (h >> 11) / float(1 << 53)
+
+
+def test_tilt_follows_the_running_sum():
+    """The oracle's tilt phase is the reference's running sum, which differs
+    from a direct evaluation k (sx x + sy y) in the last bits: the GPU test
+    above therefore pins the accumulation order, not just the physics."""
+    ny, nx, dx, wl = 4, 2500, 1e-6, 532e-9
+    tx = np.deg2rad(3.0)
+    f = O.Field(np.ones((ny, nx), complex), dx)
+    O.apply_tilt(f, tx, 0.0, wl)
+    k = 2 * np.pi / wl
+    direct = np.exp(1j * k * np.sin(tx) * f.x(np.arange(nx)))[None, :]
+    err = np.max(np.abs(f.ex - direct))
+    assert 0 < err < 1e-9
+
+
+def _stack_case(n=32, nl=2, seed=5):
+    rng = np.random.default_rng(seed)
+    a = np.exp(-(((np.arange(n) - n / 2)[None, :] ** 2 + (np.arange(n) - n / 2)[:, None] ** 2) / (n / 3) ** 2))
+    a = a.astype(complex)
+    phis = rng.uniform(0, 2 * np.pi, (nl, n, n))
+    T = rng.uniform(0, 1, (n, n))
+    d = O.IndexDesc()
+    d.re_bg, d.im_bg = 1.5, 1e-6
+    d.core_dn, d.core_w = 0.01, 8e-6
+    d.border_px, d.border_order, d.border_strength = 4, 2, 5e-3
+    return a, phis, T, d
+
+
+def test_oracle_bpm_stack_gradient_matches_finite_differences():
+    """The stack adjoint (conjugate transfer functions and screens, slices
+    reversed) is the exact gradient of the forward loss."""
+    a, phis, T, d = _stack_case()
+    dx, zseg, steps = 1e-6, 20e-6, 3
+    ctx = O.Context(wavelength=633e-9)
+    loss, g = O.bpm_stack_loss_grad(a, phis, T, dx, zseg, steps, d, ctx)
+    rng = np.random.default_rng(9)
+    h = 1e-6
+    for _ in range(6):
+        l, j, i = rng.integers(0, phis.shape[0]), rng.integers(0, 32), rng.integers(0, 32)
+        p = phis.copy(); p[l, j, i] += h
+        lp, _ = O.bpm_stack_loss_grad(a, p, T, dx, zseg, steps, d, ctx, want_grad=False)
+        p[l, j, i] -= 2 * h
+        lm, _ = O.bpm_stack_loss_grad(a, p, T, dx, zseg, steps, d, ctx, want_grad=False)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[l, j, i]) <= 1e-6 * np.max(np.abs(g)), (l, j, i, fd, g[l, j, i])
+
+
+def test_oracle_bpm_stack_forward_is_masks_and_splitstep():
+    a, phis, T, d = _stack_case(n=16, nl=2)
+    dx, zseg, steps = 1e-6, 10e-6, 2
+    ctx = O.Context(wavelength=633e-9)
+    f = O.Field(a.copy(), dx)
+    for l in range(2):
+        f.ex *= np.exp(1j * phis[l])
+        O.splitstep(f, zseg, d, steps, O.Context(wavelength=633e-9))
+    want = np.sum((np.abs(f.ex) ** 2 - T) ** 2)
+    loss, _ = O.bpm_stack_loss_grad(a, phis, T, dx, zseg, steps, d, ctx, want_grad=False)
+    assert abs(loss - want) <= 1e-12 * abs(want)

@@ -1690,9 +1690,12 @@ void fill_screen(ScreenArgs& s, const ScreenSrc& src, int slice, long long np, d
 // parametric medium factorises as c_s * border(d) * exp(i p_s gx(x) gy(y)):
 // the slice constants c_s = exp(-k dz Im n0) exp(i k dz (Re n0 - 1)) are
 // multiplied in FP64 on the host and applied once in the last sweep.
-// Returns -1 when the case is not eligible (the general path then runs).
+// adjoint: the adjoint operator (conj transfer functions and screens, slices
+// in reverse order).  Returns -1 when the case is not eligible (the general
+// path then runs).
 int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* in, int in_c128, void* out,
-                       int out_c128, double z, const ScreenSrc& src, int steps, const wos_context& cc, bool diag) {
+                       int out_c128, double z, const ScreenSrc& src, int steps, const wos_context& cc, bool diag,
+                       bool adjoint) {
     if (diag || c->no_fast || src.kind != 1 || !is_pow2(nx) || !is_pow2(ny) || !(z > 0)) return -1;
     const double dz = z / (double)steps, hz = dz / 2;
     const double k = 2 * M_PI / cc.wavelength;
@@ -1760,6 +1763,8 @@ int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const vo
     kc.scale = 1.0 / ((double)nx * (double)ny);
     kc.zero_ev = pol.zero;
     kc.precise_phase = 1;
+    kc.conj = adjoint;
+    const double sgn = adjoint ? -1.0 : 1.0;
     FastRows m = r;
     m.in = S;
     m.in_c128 = 0;
@@ -1778,7 +1783,8 @@ int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const vo
         kc.krev = kc.kz / (2 * M_PI);
         CK(timed_launch(c, 4, [&] { return sweep_cols(c, ny, t.colE, kc, &nb); }));
         if (s < steps) {
-            const double zc = z * (double)s / (double)steps + dz / 2;
+            const int sl = adjoint ? steps - 1 - s : s;
+            const double zc = z * (double)sl / (double)steps + dz / 2;
             double r0 = d.re_bg, i0 = d.im_bg;
             for (int q = 0; q < d.n_layers && q < 8; q++)
                 if (zc < d.layer_z[q]) {
@@ -1788,8 +1794,8 @@ int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const vo
                 }
             double mod = 1;
             if (d.zmod_amp != 0) mod = 1.0 + d.zmod_amp * std::sin(2 * M_PI * zc / d.zmod_period + d.zmod_phase);
-            m.bpm_phase = k * d.core_dn * mod * dz;
-            c_phase += k * (r0 - 1.0) * dz;
+            m.bpm_phase = sgn * (k * d.core_dn * mod * dz);
+            c_phase += sgn * (k * (r0 - 1.0) * dz);
             c_logamp += -k * i0 * dz;
             CK(timed_launch(c, 0, [&] { return fast_rows_bpm(c->fp64, nx, t.rowE, m, c->st, &nb); }));
         }
@@ -1808,7 +1814,8 @@ int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const vo
 }
 
 int run_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* in, int in_c128, void* out,
-                  int out_c128, double z, const ScreenSrc& src, int steps, const wos_context& cc, wos_diag* d) {
+                  int out_c128, double z, const ScreenSrc& src, int steps, const wos_context& cc, wos_diag* d,
+                  bool adjoint = false) {
     if (d) {
         std::memset(d, 0, sizeof(*d));
         d->dx_out = dx;
@@ -1823,7 +1830,7 @@ int run_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* i
     if (steps <= 0) steps = 1;
     {
         const int rc = try_fast_splitstep(c, ny, nx, dx, ncomp, in, in_c128, out, out_c128, z, src, steps, cc,
-                                          d != nullptr);
+                                          d != nullptr, adjoint);
         if (rc != -1) return rc;
     }
     const double dz = z / (double)steps;
@@ -1888,6 +1895,7 @@ int run_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* i
         a.out_n = ny;
         a.h = asm_h(c, cc, hz, pol, dx, nx, ny);
         a.h.kind = (s == 0 || s == steps) ? H_ASM : H_ASM_HALF2;
+        a.h.conj = adjoint;
         a.batch = ncomp;
         if (diag) {
             a.red = red_region(c, 1);
@@ -1918,8 +1926,10 @@ int run_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* i
             q.out_bstride = np;
             q.out_n = nx;
             q.batch = ncomp;
-            const double zc = z * (double)s / (double)steps + dz / 2;
-            fill_screen(q.scr, src, s, np, k, dz, zc);
+            const int sl = adjoint ? steps - 1 - s : s;
+            const double zc = z * (double)sl / (double)steps + dz / 2;
+            fill_screen(q.scr, src, sl, np, k, dz, zc);
+            q.scr.conj = adjoint;
             CK(prof_rows(c, c->fp64, q));
         }
     }
@@ -2499,6 +2509,53 @@ int asm_loss_grad_impl(wos_ctx c, int ny, int nx, double dx, double z, const wos
     return WOS_OK;
 }
 
+// Diffractive stack (no reference counterpart): u = a; for each layer l,
+// v_l = u exp(i phi_l) and u = BPM_zseg(v_l); L = sum (|u|^2 - T)^2.  The
+// gradient runs the adjoint chain b = BPM^H(r) from r = dL/du* = 4 (|u|^2 - T) u:
+// dL/dphi_l = Re(conj(b_l) i v_l), then b <- exp(-i phi_l) b.  The BPM is
+// linear in the field, so its adjoint needs no forward state inside a
+// segment: the only stored states are the nl fields v_l at the masks.
+// a: complex128 when a_c128, else the context's type; phis [nl][ny][nx],
+// target, grads: FP64 device arrays (grads null: loss only).
+int bpm_stack_impl(wos_ctx c, int ny, int nx, double dx, int nl, const void* a, int a_c128, const double* phis,
+                   const double* T, double zseg, int steps, const wos_index_desc& medium, const wos_context& cc,
+                   double* loss, double* grads) {
+    if (nl < 1 || steps < 1 || ny < 2 || nx < 2 || !(dx > 0) || !a || !phis || !T || !loss)
+        return fail(WOS_INVALID_ARG, "bpm stack arguments");
+    if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    const long long np = (long long)ny * nx;
+    const size_t fb = (size_t)np * c->csz();
+    TRY(ensure(c->scratch2, fb));
+    TRY(ensure(c->vol, fb * (size_t)nl));
+    TRY(red_prepare(c, (size_t)((np + 255) / 256)));
+    void* U = c->scratch2.p;
+    char* V = reinterpret_cast<char*>(c->vol.p);
+    if (a_c128 && !c->fp64) CK(launch_convert(0, a, U, np, c->st));
+    else CK(cudaMemcpyAsync(U, a, fb, cudaMemcpyDeviceToDevice, c->st));
+    ScreenSrc src;
+    src.kind = 1;
+    src.desc = medium;
+    for (int l = 0; l < nl; l++) {
+        CK(launch_mask_phase(c->fp64, U, phis + (size_t)l * np, np, 0, c->st));
+        CK(cudaMemcpyAsync(V + (size_t)l * fb, U, fb, cudaMemcpyDeviceToDevice, c->st));
+        TRY(run_splitstep(c, ny, nx, dx, 1, U, 0, U, 0, zseg, src, steps, cc, nullptr, false));
+    }
+    int nb = 0;
+    CK(launch_residual(c->fp64, U, T, U, np, red_region(c, 0), &nb, c->st));
+    CK(launch_reduce_finish(red_region(c, 0), nb, 1, RS_P, 1, redout_region(c, 0), c->st));
+    if (grads) {
+        for (int l = nl - 1; l >= 0; l--) {
+            TRY(run_splitstep(c, ny, nx, dx, 1, U, 0, U, 0, zseg, src, steps, cc, nullptr, true));
+            CK(launch_grad_v(c->fp64, U, V + (size_t)l * fb, grads + (size_t)l * np, np, c->st));
+            if (l > 0) CK(launch_mask_phase(c->fp64, U, phis + (size_t)l * np, np, 1, c->st));
+        }
+    }
+    CK(cudaMemcpyAsync(c->err_host, c->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+    TRY(fetch_red(c, 1));
+    *loss = c->hred[RS_P];
+    return check_err_word(c);
+}
+
 }  // namespace
 
 extern "C" {
@@ -2784,6 +2841,222 @@ int wos_apply_phase_mask(wos_ctx c, wos_field* f, const double* phi, double amp)
     CK(launch_phase_mask(stage_ex(c), stage_ey(c, f), f->polarized, np, reinterpret_cast<double*>(c->maps.p), amp,
                          c->st));
     return stage_out(c, f, f->polarized ? 2 : 1);
+}
+
+namespace {
+double2 d2(wos_c128 v) { return make_double2(v.re, v.im); }
+
+// FFT -> multiply by a filter H(fx, fy) -> inverse FFT of `ncomp` complex128
+// device planes in place, on the three-sweep propagator (context precision).
+int spectral_filter(wos_ctx c, int ny, int nx, double dx, int ncomp, void* planes, int kind, double p0,
+                    double p1) {
+    Prop p{ny, nx, dx, ncomp, planes, 1, planes, 1, 0.0, 0, default_context(), nullptr};
+    Sweep3 s;
+    s.h.kind = kind;
+    s.h.exact = c->fp64;
+    s.h.dx = dx;
+    s.h.lfx = nx;
+    s.h.lfy = ny;
+    s.h.scale = 1.0 / ((double)nx * (double)ny);
+    s.h.c_re = 1.0;
+    s.h.p0 = p0;
+    s.h.p1 = p1;
+    return run_sweep3(c, p, s);
+}
+}  // namespace
+
+int wos_apply_jones(wos_ctx c, wos_field* f, wos_c128 a, wos_c128 b, wos_c128 cc, wos_c128 d) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    int mode = 2;
+    if (f && !f->polarized) {
+        const bool diag = b.re == 0 && b.im == 0 && cc.re == 0 && cc.im == 0 && d.re == a.re && d.im == a.im;
+        mode = diag ? 0 : 1;
+        if (mode == 1 && !f->ey) return fail(WOS_INVALID_ARG, "jones: the field needs an Ey buffer");
+    }
+    TRY(check_field(f));
+    TRY(set_device(c));
+    TRY(stage_in(c, f, mode == 0 ? 1 : 2));
+    const long long np = (long long)f->ny * f->nx;
+    CK(launch_jones(stage_ex(c), stage_ey(c, f), np, mode, d2(a), d2(b), d2(cc), d2(d), c->st));
+    if (mode == 1) f->polarized = 1;
+    return stage_out(c, f, mode == 0 ? 1 : 2);
+}
+
+int wos_scale_amplitude(wos_ctx c, wos_field* f, wos_c128 s) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(element_begin(c, f));
+    CK(launch_scale(stage_ex(c), stage_ey(c, f), f->polarized, (long long)f->ny * f->nx, d2(s), c->st));
+    return stage_out(c, f, f->polarized ? 2 : 1);
+}
+
+int wos_apply_tilt(wos_ctx c, wos_field* f, double tx, double ty, double wavelength) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    if (!(wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(element_begin(c, f));
+    const double k = 2 * M_PI / wavelength;
+    CK(launch_tilt(stage_ex(c), stage_ey(c, f), f->polarized, f->ny, f->nx, f->dx, k, std::sin(tx), std::sin(ty),
+                   c->st));
+    return stage_out(c, f, f->polarized ? 2 : 1);
+}
+
+int wos_apply_bandlimit(wos_ctx c, wos_field* f, double fraction, double sigma) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(check_field(f));
+    if (fraction >= 1 || fraction <= 0) return WOS_OK;  // nil or disabled options (field.go:266-268)
+    TRY(element_begin(c, f));
+    const double fnyq = 1 / (2 * f->dx);
+    const double f0 = fraction * fnyq;
+    double sig = sigma * fnyq;
+    if (sig <= 0) sig = fnyq * 0.01;
+    TRY(spectral_filter(c, f->ny, f->nx, f->dx, f->polarized ? 2 : 1, c->stage.p, H_BANDLIMIT, f0, sig));
+    return stage_out(c, f, f->polarized ? 2 : 1);
+}
+
+int wos_shift_field(wos_ctx c, wos_field* f, double du, double dv) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(check_field(f));
+    if (du == 0 && dv == 0) return WOS_OK;
+    TRY(element_begin(c, f));
+    TRY(spectral_filter(c, f->ny, f->nx, f->dx, f->polarized ? 2 : 1, c->stage.p, H_SHIFT, du, dv));
+    return stage_out(c, f, f->polarized ? 2 : 1);
+}
+
+int wos_apply_diffuser(wos_ctx c, wos_field* f, double sigma, double correlation, double amplitude,
+                       long long seed, double x0, double y0) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(element_begin(c, f));
+    const long long np = (long long)f->ny * f->nx;
+    TRY(ensure(c->aux, (size_t)np * sizeof(double2)));
+    double2* zp = reinterpret_cast<double2*>(c->aux.p);
+    const double cell = f->dx > 0 ? f->dx : 1.0;
+    CK(launch_diffuser_noise(zp, f->ny, f->nx, f->dx, cell, x0, y0, seed, c->st));
+    if (correlation > 0) {
+        const double neg_two_pi_sq = -19.739208802178716;  // -2 pi^2 rounded once, as a Go constant
+        TRY(spectral_filter(c, f->ny, f->nx, f->dx, 1, zp, H_GAUSS, neg_two_pi_sq * correlation * correlation, 0));
+    }
+    const int nb = sum_re2_blocks(np);
+    TRY(red_prepare(c, (size_t)nb));
+    CK(launch_sum_re2(zp, np, red_region(c, 0), c->st));
+    CK(launch_reduce_finish(red_region(c, 0), nb, 1, 0, 2, redout_region(c, 0), c->st));
+    CK(launch_diffuser_apply(stage_ex(c), stage_ey(c, f), f->polarized, np, zp, redout_region(c, 0), sigma,
+                             amplitude, c->st));
+    return stage_out(c, f, f->polarized ? 2 : 1);
+}
+
+int wos_propagate1d(wos_ctx c, int n, wos_c128* a, double dx, double z, double wavelength, const wos_context* cci,
+                    wos_diag* d) {
+    if (!c || !a) return fail(WOS_INVALID_ARG, "null argument");
+    if (n < 2 || !(dx > 0)) return fail(WOS_INVALID_ARG, "propagate1d: n >= 2 and dx > 0 required");
+    if (!(wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    if (d) {
+        std::memset(d, 0, sizeof(*d));
+        d->dx_out = dx;
+    }
+    wos_context cc = cci ? *cci : default_context();
+    cc.wavelength = wavelength;  // Propagate1D takes wl apart from the Context
+    const Policy pol = ev_policy(cc, z);
+    Axis* ax;
+    TRY(get_axis(c, n, c->fp64, &ax));
+    TRY(ensure(c->stage, (size_t)n * 16));
+    TRY(ensure(c->scratch, (size_t)n * c->csz()));
+    CK(cudaMemcpyAsync(c->stage.p, a, (size_t)n * 16, cudaMemcpyHostToDevice, c->st));
+    TRY(red_prepare(c, 64));
+    RowArgs r = row_defaults(1, n, dx);
+    r.mode = ROW_FWD;
+    r.rows = 1;
+    fill_axis(r, ax);
+    r.in = c->stage.p;
+    r.in_c128 = 1;
+    r.in_ld = n;
+    r.in_n = n;
+    r.out = c->scratch.p;
+    r.out_ld = n;
+    r.out_n = n;
+    r.red = red_region(c, 0);
+    r.red_pre = 1;
+    CK(prof_rows(c, c->fp64, r));
+    CK(launch_reduce_finish(r.red, 1, 1, RS_P, 1, redout_region(c, 0), c->st));
+    HArgs h = asm_h(c, cc, z, pol, dx, n, 1);
+    h.scale = 1.0 / (double)n;
+    int nb = 0;
+    CK(launch_asm1d_h(c->fp64, c->scratch.p, n, h, red_region(c, 1), &nb, c->st));
+    CK(launch_reduce_finish(red_region(c, 1), nb, 1, RS_SW, 2, redout_region(c, 1), c->st));
+    RowArgs q = r;
+    q.mode = ROW_INV;
+    q.in = c->scratch.p;
+    q.in_c128 = 0;
+    q.out = c->stage.p;
+    q.out_c128 = 1;
+    q.red = nullptr;
+    q.red_pre = 0;
+    CK(prof_rows(c, c->fp64, q));
+    CK(cudaMemcpyAsync(a, c->stage.p, (size_t)n * 16, cudaMemcpyDeviceToHost, c->st));
+    TRY(fetch_red(c, 2));
+    // sum1DSq before and after (no dx factor); the loss fraction comes from
+    // the spectral sums, free of the cancellation of pIn - pOut
+    const double pin = c->hred[RS_P];
+    const double p0 = c->hred[RS_COUNT + RS_SW], l1 = c->hred[RS_COUNT + RS_SW + 1];
+    const double pout = pin - pin * (p0 > 0 ? l1 / p0 : 0.0);
+    if (d) {
+        d->p_in = pin;
+        d->p_out = pout;
+        if (pin > 0 && pout < pin * (1 - 1e-8) && z > 0)
+            warn_add(d, WOS_W_EVANESCENT_FILTERED, (pin - pout) / pin);
+    }
+    return WOS_OK;
+}
+
+int wos_splitstep_adjoint_dev(wos_ctx c, int ny, int nx, double dx, int ncomp, void* field, double z,
+                              const wos_index_desc* n, int steps, const wos_context* cc) {
+    if (!c || !n || !cc) return fail(WOS_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    ScreenSrc src;
+    src.kind = 1;
+    src.desc = *n;
+    return run_splitstep(c, ny, nx, dx, ncomp, field, 0, field, 0, z, src, steps, *cc, nullptr, true);
+}
+
+int wos_bpm_stack_loss_grad_dev(wos_ctx c, int ny, int nx, double dx, int nlayers, const void* a, const double* phis,
+                                const double* target, double zseg, const wos_index_desc* n, int steps,
+                                const wos_context* cc, double* loss, double* grads) {
+    if (!c || !n || !cc) return fail(WOS_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    return bpm_stack_impl(c, ny, nx, dx, nlayers, a, 0, phis, target, zseg, steps, *n, *cc, loss, grads);
+}
+
+int wos_bpm_stack_loss_grad(wos_ctx c, int ny, int nx, double dx, int nlayers, const wos_c128* a, const double* phis,
+                            const double* target, double zseg, const wos_index_desc* n, int steps,
+                            const wos_context* cc, double* loss, double* grads) {
+    if (!c || !n || !cc || !a || !phis || !target || nlayers < 1 || ny < 2 || nx < 2)
+        return fail(WOS_INVALID_ARG, "bpm stack arguments");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const long long np = (long long)ny * nx;
+    TRY(ensure(c->stage, (size_t)np * 16));
+    TRY(ensure(c->maps, sizeof(double) * (size_t)np * (2 * (size_t)nlayers + 1)));
+    double* phid = reinterpret_cast<double*>(c->maps.p);
+    double* Td = phid + (size_t)np * nlayers;
+    double* gd = Td + np;
+    CK(cudaMemcpyAsync(c->stage.p, a, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(phid, phis, sizeof(double) * (size_t)np * nlayers, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(Td, target, sizeof(double) * (size_t)np, cudaMemcpyHostToDevice, c->st));
+    TRY(bpm_stack_impl(c, ny, nx, dx, nlayers, c->stage.p, 1, phid, Td, zseg, steps, *n, *cc, loss,
+                       grads ? gd : nullptr));
+    if (grads) {
+        CK(cudaMemcpyAsync(grads, gd, sizeof(double) * (size_t)np * nlayers, cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+    }
+    return WOS_OK;
 }
 
 int wos_asm_forward_loss(wos_ctx c, int ny, int nx, double dx, double z, const wos_context* cc, const wos_c128* a,

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
+#include <algorithm>
+
 #include "wos_fft.cuh"
 #include "wos_kernels.cuh"
 
@@ -103,6 +105,131 @@ __global__ void k_phase_mask(double2* ex, double2* ey, int pol, long long n, con
     apply2(ex, ey, pol, idx, gmul(make_double2(amp, 0), gexpi(phi[idx])));
 }
 
+// ---- Field operations (optics/field.go:109-168)
+// ApplyJones: mode 0 scalar field, diagonal matrix a*I (Ex *= a); mode 1
+// scalar -> polarized transition (Ex = a Ex, Ey = c Ex); mode 2 full 2x2.
+__global__ void k_jones(double2* ex, double2* ey, long long n, int mode, double2 a, double2 b, double2 c,
+                        double2 d) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    const double2 x = ex[idx];
+    if (mode == 0) {
+        ex[idx] = gmul(x, a);
+    } else if (mode == 1) {
+        ex[idx] = gmul(a, x);
+        ey[idx] = gmul(c, x);
+    } else {
+        const double2 y = ey[idx];
+        const double2 p = gmul(a, x), q = gmul(b, y), r = gmul(c, x), t = gmul(d, y);
+        ex[idx] = make_double2(da(p.x, q.x), da(p.y, q.y));
+        ey[idx] = make_double2(da(r.x, t.x), da(r.y, t.y));
+    }
+}
+
+// ScaleAmplitude
+__global__ void k_scale(double2* ex, double2* ey, int pol, long long n, double2 s) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    apply2(ex, ey, pol, idx, s);
+}
+
+// ApplyTilt: the phase along a row is accumulated sequentially from its
+// first pixel (ph += k sx dx), so every pixel carries exactly the rounding of
+// the reference's running sum.  One CTA per row: thread 0 runs the sum for a
+// chunk of pixels into shared memory, then all threads apply exp(i ph).
+constexpr int kTiltChunk = 1024;
+__global__ void k_tilt(double2* ex, double2* ey, int pol, int ny, int nx, double dx, double k, double sx,
+                       double sy) {
+    __shared__ double ph_s[kTiltChunk];
+    __shared__ double carry;
+    const int j = blockIdx.x;
+    const double step = dm(dm(k, sx), dx);
+    if (threadIdx.x == 0) carry = dm(k, da(dm(sx, coord(0, nx, dx)), dm(sy, coord(j, ny, dx))));
+    for (int i0 = 0; i0 < nx; i0 += kTiltChunk) {
+        const int m = min(kTiltChunk, nx - i0);
+        __syncthreads();  // the previous chunk has been applied
+        if (threadIdx.x == 0) {
+            double ph = carry;
+            for (int i = 0; i < m; i++) {
+                ph_s[i] = ph;
+                ph = da(ph, step);
+            }
+            carry = ph;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+            const long long idx = (long long)j * nx + i0 + i;
+            const double2 t = gexpi(ph_s[i]);
+            ex[idx] = gmul(ex[idx], t);
+            if (pol) ey[idx] = gmul(ey[idx], t);
+        }
+    }
+}
+
+// ---- Diffuser (optics/elements.go:710-783)
+// hashNoise01: splitmix-style finaliser of the lab cell and the seed.
+__device__ __forceinline__ double hash_noise01(long long x, long long y, long long seed) {
+    unsigned long long h = (unsigned long long)seed * 0x9E3779B97F4A7C15ULL ^
+                           (unsigned long long)x * 0xC2B2AE3D27D4EB4FULL ^
+                           (unsigned long long)y * 0x165667B19E3779F9ULL;
+    h ^= h >> 30;
+    h *= 0xBF58476D1CE4E5B9ULL;
+    h ^= h >> 27;
+    h *= 0x94D049BB133111EBULL;
+    h ^= h >> 31;
+    return (double)(h >> 11) / 9007199254740992.0;  // / 2^53
+}
+// White phase noise on the lab lattice, as a complex128 plane (phase, 0).
+__global__ void k_diffuser_noise(double2* z, int ny, int nx, double dx, double cell, double x0, double y0,
+                                 long long seed) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)ny * nx) return;
+    const int j = (int)(idx / nx), i = (int)(idx % nx);
+    const long long gy = (long long)round(dd(da(coord(j, ny, dx), y0), cell));
+    const long long gx = (long long)round(dd(da(coord(i, nx, dx), x0), cell));
+    z[idx] = make_double2(ds(dm(dm(hash_noise01(gx, gy, seed), 2.0), M_PI), M_PI), 0);
+}
+// Per-CTA sums of Re z and (Re z)^2 into partials[block * RS_COUNT + {0, 1}].
+__global__ void k_sum_re2(const double2* z, long long n, double* partials) {
+    __shared__ double sm[2][32];
+    double s1 = 0, s2 = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double v = z[i].x;
+        s1 += v;
+        s2 += v * v;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s1 += __shfl_down_sync(0xffffffffu, s1, o);
+        s2 += __shfl_down_sync(0xffffffffu, s2, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sm[0][threadIdx.x >> 5] = s1;
+        sm[1][threadIdx.x >> 5] = s2;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, b = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            a += sm[0][w];
+            b += sm[1][w];
+        }
+        partials[(long long)blockIdx.x * RS_COUNT + 0] = a;
+        partials[(long long)blockIdx.x * RS_COUNT + 1] = b;
+    }
+}
+// Rescale the phase to standard deviation sigma (sums = {sum v, sum v^2},
+// on the device) and multiply by amp exp(i phase).
+__global__ void k_diffuser_apply(double2* ex, double2* ey, int pol, long long n, const double2* z,
+                                 const double* sums, double sigma, double amp) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    const double m = dd(sums[0], (double)n);
+    const double s2 = ds(dd(sums[1], (double)n), dm(m, m));
+    double ph = z[idx].x;
+    if (s2 > 0) ph = dm(ds(ph, m), dd(sigma, __dsqrt_rn(s2)));
+    apply2(ex, ey, pol, idx, gmul(make_double2(amp, 0), gexpi(ph)));
+}
+
 // ---- Gaussian Schell-model synthesis (optics/coherence.go:32-77)
 __global__ void k_schell_mu(double2* a, int n, double dx, double coh) {
     const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -185,6 +312,28 @@ __global__ void k_grad(const C* b, const double2* a, const double* phi, double* 
     g[idx] = (double)bv.x * ir + (double)bv.y * ii;
 }
 
+// u *= exp(+-i phi) in the context precision (stack masks and their adjoint)
+template <typename C>
+__global__ void k_mask_phase(C* u, const double* phi, long long n, int conj) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    double s, c;
+    sincos(phi[idx], &s, &c);
+    if (conj) s = -s;
+    const C v = u[idx];
+    u[idx] = mkc<C>((decltype(C::x))(c * (double)v.x - s * (double)v.y),
+                    (decltype(C::x))(c * (double)v.y + s * (double)v.x));
+}
+
+// g = Re(conj(b) * i * v), v = the field just after a mask
+template <typename C>
+__global__ void k_grad_v(const C* b, const C* v, double* g, long long n) {
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    const C bv = b[idx], vv = v[idx];
+    g[idx] = (double)bv.y * vv.x - (double)bv.x * vv.y;
+}
+
 // ---------------------------------------------------------------- launchers
 static inline unsigned nblk(long long n, int b = 256) { return (unsigned)((n + b - 1) / b); }
 
@@ -208,6 +357,35 @@ cudaError_t launch_grating(double2* ex, double2* ey, int pol, int ny, int nx, do
 cudaError_t launch_phase_mask(double2* ex, double2* ey, int pol, long long n, const double* phi, double amp,
                               cudaStream_t st) {
     k_phase_mask<<<nblk(n), 256, 0, st>>>(ex, ey, pol, n, phi, amp);
+    return cudaGetLastError();
+}
+cudaError_t launch_jones(double2* ex, double2* ey, long long n, int mode, double2 a, double2 b, double2 c, double2 d,
+                         cudaStream_t st) {
+    k_jones<<<nblk(n), 256, 0, st>>>(ex, ey, n, mode, a, b, c, d);
+    return cudaGetLastError();
+}
+cudaError_t launch_scale(double2* ex, double2* ey, int pol, long long n, double2 s, cudaStream_t st) {
+    k_scale<<<nblk(n), 256, 0, st>>>(ex, ey, pol, n, s);
+    return cudaGetLastError();
+}
+cudaError_t launch_tilt(double2* ex, double2* ey, int pol, int ny, int nx, double dx, double k, double sx, double sy,
+                        cudaStream_t st) {
+    k_tilt<<<ny, 256, 0, st>>>(ex, ey, pol, ny, nx, dx, k, sx, sy);
+    return cudaGetLastError();
+}
+cudaError_t launch_diffuser_noise(double2* z, int ny, int nx, double dx, double cell, double x0, double y0,
+                                  long long seed, cudaStream_t st) {
+    k_diffuser_noise<<<nblk((long long)ny * nx), 256, 0, st>>>(z, ny, nx, dx, cell, x0, y0, seed);
+    return cudaGetLastError();
+}
+int sum_re2_blocks(long long n) { return (int)std::min<long long>(nblk(n), 1184); }
+cudaError_t launch_sum_re2(const double2* z, long long n, double* partials, cudaStream_t st) {
+    k_sum_re2<<<sum_re2_blocks(n), 256, 0, st>>>(z, n, partials);
+    return cudaGetLastError();
+}
+cudaError_t launch_diffuser_apply(double2* ex, double2* ey, int pol, long long n, const double2* z,
+                                  const double* sums, double sigma, double amp, cudaStream_t st) {
+    k_diffuser_apply<<<nblk(n), 256, 0, st>>>(ex, ey, pol, n, z, sums, sigma, amp);
     return cudaGetLastError();
 }
 cudaError_t launch_schell_mu(double2* a, int n, double dx, double coh, cudaStream_t st) {
@@ -245,6 +423,19 @@ cudaError_t launch_grad(int fp64, const void* b, const double2* a, const double*
                         cudaStream_t st) {
     if (fp64) k_grad<double2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<const double2*>(b), a, phi, g, n);
     else k_grad<float2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<const float2*>(b), a, phi, g, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mask_phase(int fp64, void* u, const double* phi, long long n, int conj, cudaStream_t st) {
+    if (fp64) k_mask_phase<double2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<double2*>(u), phi, n, conj);
+    else k_mask_phase<float2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<float2*>(u), phi, n, conj);
+    return cudaGetLastError();
+}
+cudaError_t launch_grad_v(int fp64, const void* b, const void* v, double* g, long long n, cudaStream_t st) {
+    if (fp64)
+        k_grad_v<double2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<const double2*>(b), reinterpret_cast<const double2*>(v), g, n);
+    else
+        k_grad_v<float2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<const float2*>(b), reinterpret_cast<const float2*>(v), g, n);
     return cudaGetLastError();
 }
 

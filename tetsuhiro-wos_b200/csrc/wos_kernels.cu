@@ -18,6 +18,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "wos_kernels_dev.cuh"
 
 namespace wos {
@@ -110,6 +112,43 @@ __global__ void __launch_bounds__(256) k_reduce_finish(const double* partials, i
             neumaier_add(ts, tc, ws[w][0]);
         }
         out[(long long)blockIdx.x * RS_COUNT + s0 + k] = ts + tc;
+    }
+}
+
+// 1-D angular spectrum step (asmTF1D, optics/propagate.go:680-701): rho =
+// |wl fx| is asm_tf's hypot with fy = 0.  Spectral power sums for the
+// evanescent_filtered warning, as in the 2-D column pass.
+template <typename C>
+__global__ void __launch_bounds__(256) k_asm1d_h(C* a, int n, HArgs h, double* partials) {
+    using T = decltype(C::x);
+    double p0 = 0, l1 = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double m2;
+        const C hh = asm_tf<C>(h, h.wl, h.kz, h.kaz, h.z < 0, freq_n(i, h.lfx, h.dx), 0.0, m2);
+        const C x = a[i];
+        const double pw = (double)x.x * x.x + (double)x.y * x.y;
+        p0 += pw;
+        if (m2 != 1.0) l1 += pw * (1.0 - m2);
+        a[i] = cmul(x, cscale(hh, (T)h.scale));
+    }
+    __shared__ double sm[2][8];
+    for (int o = 16; o > 0; o >>= 1) {
+        p0 += __shfl_down_sync(0xffffffffu, p0, o);
+        l1 += __shfl_down_sync(0xffffffffu, l1, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sm[0][threadIdx.x >> 5] = p0;
+        sm[1][threadIdx.x >> 5] = l1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double u = 0, v = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            u += sm[0][w];
+            v += sm[1][w];
+        }
+        partials[(long long)blockIdx.x * RS_COUNT + RS_SW] = u;
+        partials[(long long)blockIdx.x * RS_COUNT + RS_SW + 1] = v;
     }
 }
 
@@ -238,6 +277,15 @@ cudaError_t launch_cols(int fp64, const ColArgs& a, cudaStream_t st) {
     case 8: return launch_cols_t<float, 8>(a, st);
     default: return launch_cols_t<float, 16>(a, st);
     }
+}
+
+cudaError_t launch_asm1d_h(int fp64, void* a, int n, const HArgs& h, double* partials, int* nblocks,
+                           cudaStream_t st) {
+    const int g = std::min((n + 255) / 256, 64);
+    *nblocks = g;
+    if (fp64) k_asm1d_h<double2><<<g, 256, 0, st>>>(reinterpret_cast<double2*>(a), n, h, partials);
+    else k_asm1d_h<float2><<<g, 256, 0, st>>>(reinterpret_cast<float2*>(a), n, h, partials);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_twiddles(int fp64, void* tw, int L, cudaStream_t st) {

@@ -17,6 +17,9 @@ enum HKind {
     H_FRESNEL_TF = 2,  // exp(ikz) exp(-i pi lambda z f^2)
     H_TABLE_XY = 3,    // separable product tx[col] * ty[q] (Fresnel impulse response)
     H_ASM_HALF2 = 4,   // (H_asm(z))^2 evaluated as a product: merged BPM half-steps
+    H_GAUSS = 5,       // exp(p0 (fx^2+fy^2)): diffuser correlation filter (elements.go:744-754)
+    H_BANDLIMIT = 6,   // exp(-((|f|-p0)/p1)^2) for |f| > p0: ApplyBandlimit (field.go:264-294)
+    H_SHIFT = 7,       // exp(-2 pi i (fx p0 + fy p1)): ShiftField (field.go:199-228)
 };
 
 struct HArgs {
@@ -34,6 +37,7 @@ struct HArgs {
     double c_re, c_im;   // extra complex constant (Fresnel prefactors)
     const void* tx;      // H_TABLE_XY tables (C type), length lfx / lfy
     const void* ty;
+    double p0, p1;       // parameters of the spectral filters (H_GAUSS .. H_SHIFT)
 };
 
 // Reduction slots (FP64) written per CTA; finalised by k_reduce_finish.
@@ -76,6 +80,7 @@ struct ScreenArgs {
     int n_layers;
     double layer_z[8], layer_re[8], layer_im[8];
     const double* nre; const double* nim;   // maps (kind 2)
+    int conj;          // adjoint: conj(t)
 };
 
 struct RowArgs {
@@ -177,6 +182,27 @@ cudaError_t launch_grating(double2* ex, double2* ey, int pol, int ny, int nx, do
                            cudaStream_t st);
 cudaError_t launch_phase_mask(double2* ex, double2* ey, int pol, long long n, const double* phi, double amp,
                               cudaStream_t st);
+cudaError_t launch_jones(double2* ex, double2* ey, long long n, int mode, double2 a, double2 b, double2 c, double2 d,
+                         cudaStream_t st);
+cudaError_t launch_scale(double2* ex, double2* ey, int pol, long long n, double2 s, cudaStream_t st);
+// k = 2 pi / wl, sx = sin(tx), sy = sin(ty) (the running row phase of ApplyTilt)
+cudaError_t launch_tilt(double2* ex, double2* ey, int pol, int ny, int nx, double dx, double k, double sx, double sy,
+                        cudaStream_t st);
+cudaError_t launch_diffuser_noise(double2* z, int ny, int nx, double dx, double cell, double x0, double y0,
+                                  long long seed, cudaStream_t st);
+int sum_re2_blocks(long long n);
+cudaError_t launch_sum_re2(const double2* z, long long n, double* partials, cudaStream_t st);
+cudaError_t launch_diffuser_apply(double2* ex, double2* ey, int pol, long long n, const double2* z,
+                                  const double* sums, double sigma, double amp, cudaStream_t st);
+// u *= exp(i phi) (exp(-i phi) when conj), u of the context's complex type
+cudaError_t launch_mask_phase(int fp64, void* u, const double* phi, long long n, int conj, cudaStream_t st);
+// g = Re(conj(b) * i * v)
+cudaError_t launch_grad_v(int fp64, const void* b, const void* v, double* g, long long n, cudaStream_t st);
+// 1-D angular spectrum step on a forward-transformed line (asmTF1D,
+// optics/propagate.go:668-738): a[i] *= H(fx_i) / n; spectral power sums
+// (RS_SW: sum |F|^2, RS_SW+1: sum |F|^2 (1 - |H|^2)) per CTA into partials.
+cudaError_t launch_asm1d_h(int fp64, void* a, int n, const HArgs& h, double* partials, int* nblocks,
+                           cudaStream_t st);
 cudaError_t launch_schell_mu(double2* a, int n, double dx, double coh, cudaStream_t st);
 cudaError_t launch_sqrt_re(double* s, const double2* a, long long nn, cudaStream_t st);
 cudaError_t launch_mul_map(double2* a, const double* s, long long nn, int batches, cudaStream_t st);

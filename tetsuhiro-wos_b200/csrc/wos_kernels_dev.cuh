@@ -155,6 +155,24 @@ __device__ __forceinline__ C eval_h(const HArgs& h, double wl, double z, int col
         const C* ty = reinterpret_cast<const C*>(h.ty);
         r = cmul(cmul(ldg_c(tx + col), ldg_c(ty + q)), mkc<C>((T)h.c_re, (T)h.c_im));
     } break;
+    case H_GAUSS: {
+        // exp(c corr^2 f^2) with p0 = c corr^2 formed on the host, c = -2 pi^2
+        const double a = h.exact ? dmul(h.p0, dadd(dmul(fx, fx), dmul(fy, fy))) : h.p0 * (fx * fx + fy * fy);
+        r = mkc<C>((T)exp(a), 0);
+    } break;
+    case H_BANDLIMIT: {
+        const double fr = go_hypot(fx, fy);
+        r = mkc<C>(1, 0);
+        if (fr > h.p0) {
+            const double d = h.exact ? ddiv(dsub(fr, h.p0), h.p1) : (fr - h.p0) / h.p1;
+            r = mkc<C>((T)exp(h.exact ? -dmul(d, d) : -(d * d)), 0);
+        }
+    } break;
+    case H_SHIFT: {
+        const double a = h.exact ? dmul(-2 * M_PI, dadd(dmul(fx, h.p0), dmul(fy, h.p1)))
+                                 : (-2 * M_PI) * (fx * h.p0 + fy * h.p1);
+        r = cexpi<C>(a);
+    } break;
     default: r = mkc<C>(1, 0); break;
     }
     if (h.conj) r.y = -r.y;
@@ -228,6 +246,7 @@ __device__ __forceinline__ C screen_eval(const ScreenArgs& s, int i, int j, int 
     const double ph = dmul(dmul(s.k, dsub(nr, 1.0)), s.dz);
     const double amp = exp(dmul(dmul(-s.k, ni), s.dz));
     C e = cexpi<C>(ph);
+    if (s.conj) e.y = -e.y;
     return mkc<C>((T)(amp * (double)e.x), (T)(amp * (double)e.y));
 }
 

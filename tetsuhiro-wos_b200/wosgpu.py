@@ -42,6 +42,9 @@ EXPORTS = [
     "wos_asm_forward_loss", "wos_asm_loss_grad", "wos_asm_loss_grad_dev", "wos_asm_adjoint",
     "wos_propagate_batch_dev", "wos_propagate_batch",
     "wos_asm_pad_c64_noalloc",
+    "wos_apply_jones", "wos_scale_amplitude", "wos_apply_tilt", "wos_apply_bandlimit", "wos_shift_field",
+    "wos_apply_diffuser", "wos_propagate1d",
+    "wos_bpm_stack_loss_grad", "wos_bpm_stack_loss_grad_dev", "wos_splitstep_adjoint_dev",
 ]
 
 
@@ -63,6 +66,15 @@ class CDiag(C.Structure):
                 ("wrap_checked", C.c_int), ("spectral_radius", C.c_double),
                 ("rms_radius_in", C.c_double), ("dx_out", C.c_double),
                 ("warn_count", C.c_int * 7), ("warn_value", C.c_double * 7)]
+
+
+class C128(C.Structure):
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
+
+
+def _c128(v) -> C128:
+    v = complex(v)
+    return C128(v.real, v.imag)
 
 
 class CField(C.Structure):
@@ -130,6 +142,16 @@ def lib():
             "wos_propagate_batch": ([vp, i, vp, d, i, vp, vp], i),
             "wos_asm_adjoint": ([vp, vp, d, vp], i),
             "wos_asm_pad_c64_noalloc": ([vp, vp, i, i, d, d, vp, vp], i),
+            "wos_apply_jones": ([vp, vp, C128, C128, C128, C128], i),
+            "wos_scale_amplitude": ([vp, vp, C128], i),
+            "wos_apply_tilt": ([vp, vp, d, d, d], i),
+            "wos_apply_bandlimit": ([vp, vp, d, d], i),
+            "wos_shift_field": ([vp, vp, d, d], i),
+            "wos_apply_diffuser": ([vp, vp, d, d, d, C.c_longlong, d, d], i),
+            "wos_propagate1d": ([vp, i, vp, d, d, d, vp, vp], i),
+            "wos_bpm_stack_loss_grad": ([vp, i, i, d, i, vp, vp, vp, d, vp, i, vp, vp, vp], i),
+            "wos_bpm_stack_loss_grad_dev": ([vp, i, i, d, i, vp, vp, vp, d, vp, i, vp, vp, vp], i),
+            "wos_splitstep_adjoint_dev": ([vp, i, i, d, i, vp, d, vp, i, vp], i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name, None)
@@ -485,6 +507,73 @@ class GPU:
     def apply_phase_mask(self, f: Field, phi: np.ndarray, amp=1.0):
         phi = np.ascontiguousarray(phi, dtype=np.float64)
         _check(lib().wos_apply_phase_mask(self.h, C.byref(f.c()), _ptr(phi), amp))
+
+    # ---- field operations (field.go:109-168,199-228,264-294; elements.go:722-783)
+    def apply_jones(self, f: Field, a, b, c, d):
+        cf = f.c()
+        _check(lib().wos_apply_jones(self.h, C.byref(cf), _c128(a), _c128(b), _c128(c), _c128(d)))
+        f.polarized = bool(cf.polarized)
+
+    def scale_amplitude(self, f: Field, s):
+        _check(lib().wos_scale_amplitude(self.h, C.byref(f.c()), _c128(s)))
+
+    def apply_tilt(self, f: Field, tx, ty, wl):
+        _check(lib().wos_apply_tilt(self.h, C.byref(f.c()), tx, ty, wl))
+
+    def apply_bandlimit(self, f: Field, fraction, sigma):
+        _check(lib().wos_apply_bandlimit(self.h, C.byref(f.c()), fraction, sigma))
+
+    def shift_field(self, f: Field, du, dv):
+        _check(lib().wos_shift_field(self.h, C.byref(f.c()), du, dv))
+
+    def apply_diffuser(self, f: Field, sigma=np.pi, corr=2e-5, amp=1.0, seed=1, x0=0.0, y0=0.0):
+        _check(lib().wos_apply_diffuser(self.h, C.byref(f.c()), sigma, corr, amp, int(seed), x0, y0))
+
+    def propagate1d(self, a: np.ndarray, dx: float, z: float, wl: float, ctx: Optional[Context] = None,
+                    diag: bool = False):
+        """Propagate1D (propagate.go:718-738) on a copy of `a`; returns the
+        propagated line (and the CDiag when diag is set)."""
+        a = np.ascontiguousarray(a, dtype=np.complex128).copy()
+        d = CDiag()
+        cc = (ctx if ctx is not None else Context(wavelength=wl)).c()
+        _check(lib().wos_propagate1d(self.h, a.size, _ptr(a), dx, z, wl, C.byref(cc), C.byref(d)))
+        if ctx is not None:
+            ctx.absorb(d)
+        return (a, d) if diag else a
+
+    # ---- diffractive stack (masks with BPM segments between them)
+    def bpm_stack_loss_grad(self, a: np.ndarray, phis: np.ndarray, target: np.ndarray, dx: float, zseg: float,
+                            steps: int, desc: "IndexDesc", ctx: Context, want_grad: bool = True):
+        """Loss sum (|u|^2 - T)^2 of the stack and dL/dphi per layer (host arrays)."""
+        a = np.ascontiguousarray(a, dtype=np.complex128)
+        phis = np.ascontiguousarray(phis, dtype=np.float64)
+        target = np.ascontiguousarray(target, dtype=np.float64)
+        nl, ny, nx = phis.shape
+        loss = C.c_double()
+        grads = np.zeros((nl, ny, nx)) if want_grad else None
+        cc = ctx.c()
+        _check(lib().wos_bpm_stack_loss_grad(self.h, ny, nx, dx, nl, _ptr(a), _ptr(phis), _ptr(target), zseg,
+                                             C.byref(desc), steps, C.byref(cc), C.byref(loss),
+                                             _ptr(grads) if want_grad else None))
+        return loss.value, grads
+
+    def bpm_stack_loss_grad_dev(self, a_ptr: int, phis_ptr: int, target_ptr: int, grads_ptr: Optional[int],
+                                nl: int, ny: int, nx: int, dx: float, zseg: float, steps: int, desc: "IndexDesc",
+                                ctx: Context) -> float:
+        """Device-resident stack loss / gradient: pointers to device arrays
+        (a of the context's complex type; phis, target, grads FP64)."""
+        loss = C.c_double()
+        cc = ctx.c()
+        _check(lib().wos_bpm_stack_loss_grad_dev(self.h, ny, nx, dx, nl, C.c_void_p(a_ptr), C.c_void_p(phis_ptr),
+                                                 C.c_void_p(target_ptr), zseg, C.byref(desc), steps, C.byref(cc),
+                                                 C.byref(loss), C.c_void_p(grads_ptr) if grads_ptr else None))
+        return loss.value
+
+    def split_step_adjoint_dev(self, ny, nx, dx, ncomp, ptr, z, desc, steps, ctx) -> None:
+        """Adjoint of split_step_dev on a device field, in place."""
+        cc = ctx.c()
+        _check(lib().wos_splitstep_adjoint_dev(self.h, ny, nx, dx, ncomp, C.c_void_p(ptr), z, C.byref(desc), steps,
+                                               C.byref(cc)))
 
     # ---- inverse design
     def asm_loss_grad(self, a: np.ndarray, phi: np.ndarray, target: np.ndarray, dx: float, z: float,
