@@ -224,7 +224,7 @@ def time_device(g, torch, bufs, steps, warmup, batch, ctx, stream, profile=False
 
 # ---------------------------------------------------------------------------
 # Secondary configurations of the workload table (one JSON line each):
-#   python bench.py --config {cfg1,cfg2,cfg3,cfg4.1,cfg4.2,cfg4.3,cfg5}
+#   python bench.py --config {cfg1,cfg2,cfg3,cfg4.1,cfg4.2,cfg4.3,cfg5,cfg5.2}
 # Seeded synthetic inputs of the stated shapes stand in for the reference's
 # cases; timed through the library's public entry points with CUDA events on
 # the context's stream (host-buffer entry points include their H2D/D2H, with
@@ -254,7 +254,10 @@ def _algorithmic_bytes(name: str, esz: int) -> float:
     k = esz / 8
     return {"cfg1": 48 * 512 ** 2 * k, "cfg2": 2 * 104 * 1.5e6 * k, "cfg3": 803 * 16 * 1024 ** 2 * k,
             "cfg4.1": (32 + 64 * 32) * 1024 ** 2 * k, "cfg4.2": 256 * 56 * 512 ** 2 * k,
-            "cfg4.3": 32 * 768 ** 2 * 129 * k, "cfg5": 108 * 2048 ** 2 * k}[name]
+            "cfg4.3": 32 * 768 ** 2 * 129 * k, "cfg5": 108 * 2048 ** 2 * k,
+            # diffractive stack, 3 layers x 200 slices, forward + adjoint: 2 nl (2S + 3)
+            # field sweeps (R+W) plus per-layer mask / state / gradient passes and the residual
+            "cfg5.2": (2 * 3 * (2 * 200 + 3) * 16 + 3 * 72 + 24) * 2048 ** 2 * k}[name]
 
 
 def run_config(args) -> None:
@@ -410,6 +413,40 @@ def run_config(args) -> None:
                                  max(2, args.steps // 10), 1)
             if prec == wos.FP64:
                 rec_cpu = cpu(lambda: O.asm_phase_loss_grad(a, phi, tgt, dx, z, O.Context(wavelength=wl)))
+        elif name == "cfg5.2":
+            # 3 phase masks, each followed by 200 BPM slices of 5 um through a
+            # uniform n = 1.5 medium; loss and gradient of all masks
+            n, dx, wl, nl, S, dz = 2048, 4e-6, 633e-9, 3, 200, 5e-6
+            r = np.random.default_rng(1)
+            phis = r.uniform(0, 2 * np.pi, (nl, n, n))
+            x = (np.arange(n) - n / 2) * dx
+            tgt = np.zeros((n, n))
+            for cx, cy in r.uniform(-0.3, 0.3, (16, 2)) * n * dx:
+                tgt += np.exp(-((x[None, :] - cx) ** 2 + (x[:, None] - cy) ** 2) / (2 * (20e-6) ** 2))
+            a = np.ones((n, n), dtype=np.complex128)
+            desc = wos.IndexDesc()
+            desc.re_bg = 1.5
+            dt = torch.complex128 if prec == wos.FP64 else torch.complex64
+            with torch.cuda.stream(stream):
+                ad = torch.from_numpy(a).to(dt).cuda()
+                pd = torch.from_numpy(phis).cuda()
+                td = torch.from_numpy(tgt).cuda()
+                gd = torch.empty((nl, n, n), dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()
+            cx = wos.Context(wavelength=wl)
+            rec["device_s"] = timed(lambda: g.bpm_stack_loss_grad_dev(ad.data_ptr(), pd.data_ptr(), td.data_ptr(),
+                                                                      gd.data_ptr(), nl, n, n, dx, S * dz, S, desc,
+                                                                      cx),
+                                    max(2, args.steps // 10), 1)
+            pin = lambda x: torch.from_numpy(x).pin_memory().numpy()  # noqa: E731
+            ah, ph, th = pin(a), pin(phis), pin(tgt)
+            rec["e2e_s"] = timed(lambda: g.bpm_stack_loss_grad(ah, ph, th, dx, S * dz, S, desc, cx), 2, 1)
+            if prec == wos.FP64:
+                od = O.IndexDesc()
+                od.re_bg = 1.5
+                # one mask and one slice forward + adjoint, scaled to nl * S slices
+                rec_cpu = nl * S * cpu(lambda: O.bpm_stack_loss_grad(a, phis[:1], tgt, dx, dz, 1, od,
+                                                                     O.Context(wavelength=wl)))
         g.close()
         lines.append(rec)
 
@@ -438,7 +475,7 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--config", default="headline",
-                    help="headline (default) or one of cfg1 cfg2 cfg3 cfg4.1 cfg4.2 cfg4.3 cfg5")
+                    help="headline (default) or one of cfg1 cfg2 cfg3 cfg4.1 cfg4.2 cfg4.3 cfg5 cfg5.2")
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the default (or WOS_ROWE/WOS_COLE/WOS_COLW) launch configuration")
     args = ap.parse_args()
