@@ -82,6 +82,7 @@ struct Axis {
     void* bf = nullptr;
     void* bi = nullptr;
     void* ftw[2] = {nullptr, nullptr};  // per-pass twiddles of the specialised sweeps (E = 8, 16)
+    void* ptw = nullptr;                // W_L^n, n < L/2: split column tiles
 };
 
 constexpr int kMaxL32 = 8192;  // largest line held on chip (threads x elements)
@@ -109,6 +110,7 @@ struct wos_ctx_s {
     int colw = 0;
     bool no_fast = false;               // force the general sweeps (tests compare both)
     int sweep_mode = 1;                 // wos_ctx_set_fast_path: 1, 2 or 3 (0 is no_fast)
+    int col_pair = 0;                   // column tiles split over two-CTA clusters where supported
     unsigned* err_dev = nullptr;        // error word of the pipelined kernels (device)
     unsigned* err_host = nullptr;       // pinned mirror, read where the host synchronises
     // streams for independent fields of a batch (wos_propagate_batch_dev),
@@ -581,10 +583,12 @@ size_t fast_row_blocks(int L, int E, int rows, int batch) {
     while (lines * T < 32) lines *= 2;
     return (size_t)((rows + lines - 1) / lines) * std::max(batch, 1);
 }
+// (an upper bound: the split tiles of fast_cols_pair launch two CTAs per tile)
 size_t fast_col_blocks(int fp64, int L, int E, int W, int ncols, int batch) {
     W = fast_col_width(fp64, L, E, W);
     if (W < 1) W = 1;
-    return (size_t)((ncols + W - 1) / W) * std::max(batch, 1);
+    const size_t per = fast_cols_pair_case(fp64, L, E, W) ? 2 : 1;
+    return per * (size_t)((ncols + W - 1) / W) * std::max(batch, 1);
 }
 
 // Per-pass twiddle table of the specialised sweeps for a power-of-two axis.
@@ -615,7 +619,34 @@ cudaError_t sweep_rows(wos_ctx c, int L, int E, bool inv, const FastRows& a, int
     }
     return fast_rows(c->fp64, L, E, inv, a, c->st, nb);
 }
+// Tables of the split column tiles: per-pass twiddles of L/2 and W_L^n.
+bool pair_tables(wos_ctx c, int L, int E, const void** twh, const void** twp) {
+    Axis *ah, *af;
+    if (get_axis(c, L / 2, c->fp64, &ah) != WOS_OK || get_axis(c, L, c->fp64, &af) != WOS_OK) return false;
+    if (fast_tw(c, ah, E, twh) != WOS_OK) return false;
+    if (!af->ptw) {
+        if (cudaMalloc(&af->ptw, (size_t)(L / 2) * c->csz()) != cudaSuccess) {
+            cudaGetLastError();
+            af->ptw = nullptr;
+            return false;
+        }
+        if (fast_build_pair_twiddles(c->fp64, L, af->ptw, c->st) != cudaSuccess) return false;
+    }
+    *twp = af->ptw;
+    return true;
+}
+bool pair_eligible(wos_ctx c, int L, int E, const FastCols& a) {
+    return c->col_pair && !a.hist && fast_cols_pair_case(c->fp64, L, E, fast_col_width(c->fp64, L, E, a.W));
+}
+
 cudaError_t sweep_cols(wos_ctx c, int L, int E, const FastCols& a, int* nb) {
+    if (pair_eligible(c, L, E, a)) {
+        FastCols b = a;
+        if (pair_tables(c, L, E, &b.tw_half, &b.tw_pair)) {
+            const cudaError_t e = fast_cols_pair(c->fp64, L, E, b, c->st, nb);
+            if (e != cudaErrorNotSupported) return e;
+        }
+    }
     if (c->sweep_mode != 2) {
         FastCols b = a;
         b.err = c->err_dev;
@@ -1261,6 +1292,7 @@ int wos_ctx_create(int device, int precision, wos_ctx* out) {
         return fail(WOS_CUDA_ERROR, std::string("context creation: ") + cudaGetErrorString(e));
     }
     *c->err_host = 0;
+    c->col_pair = env_int("WOS_COLPAIR", 0);
     *out = c;
     return WOS_OK;
 }
@@ -1279,6 +1311,7 @@ int wos_ctx_destroy(wos_ctx c) {
                 if (kv.second.bi) cudaFree(kv.second.bi);
                 for (void* t : kv.second.ftw)
                     if (t) cudaFree(t);
+                if (kv.second.ptw) cudaFree(kv.second.ptw);
             }
         DevBuf* bufs[] = {&c->stage, &c->scratch, &c->scratch2, &c->scratch3, &c->red, &c->redout, &c->tmp,
                           &c->maps, &c->params, &c->vol, &c->accum, &c->aux};
@@ -1486,6 +1519,12 @@ int wos_propagate_batch_dev(wos_ctx c, int nfields, int ny, int nx, double dx, i
             TRY(get_axis(c, ny, c->fp64, &ay));
             TRY(fast_tw(c, ax, t.rowE, &twx));
             TRY(fast_tw(c, ay, t.colE, &twy));
+            FastCols probe{};
+            probe.W = t.colW;
+            if (pair_eligible(c, ny, t.colE, probe)) {  // shared tables of the split column tiles
+                const void *th, *tp;
+                if (!pair_tables(c, ny, t.colE, &th, &tp)) return fail(WOS_CUDA_ERROR, "split-tile tables");
+            }
             nstreams = std::max(1, std::min(wos_ctx_s::kMaxAux, env_int("WOS_STREAMS", 2)));
         }
     }

@@ -15,9 +15,13 @@
 //   k_cols_fast<Real, L, E>: W adjacent columns per CTA; forward column FFT,
 //       H(fx, fy) of asmTF (optics/propagate.go:159-181) generated on the fly
 //       from an FP64 argument, inverse column FFT, optional spectral loss sums.
+#include <cooperative_groups.h>
+
 #include "wos_fast_dev.cuh"
 
 namespace wos {
+
+namespace cg = cooperative_groups;
 
 // ------------------------------------------------------------------- rows
 template <typename Real, int L, int E, bool INV>
@@ -346,6 +350,181 @@ __global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, 
         for (int s = 0; s < E; s++) dst[(long long)fpos<RO, E, L>(s, 0) * a.ld] = v[s];
     }
     col_write_red(a, (long long)blockIdx.y * gridDim.x + blockIdx.x, p0, l1, hsm);
+}
+
+// ------------------------------------------------------------- split tiles
+// H on the half spectrum a CTA of a pair holds: local index k of rank r is the
+// frequency q = 2k + r.  The partner of q, L - q, is local LH - k (rank 0; k = 0
+// and the Nyquist row k = LH/2 pair with themselves) or LH - 1 - k (rank 1), so
+// each pair stays in one CTA and H is evaluated once for both.
+template <int L, int E, int W>
+__device__ __forceinline__ void col_tile_h_pair(float2* tile, int r, int col0, const FastCols& a, const HUnit& hu,
+                                                double& p0, double& l1) {
+    constexpr int LH = L / 2, T = LH / E;
+    const int w = threadIdx.x & (W - 1);
+    const int tt = threadIdx.x / W;
+    const int col = col0 + w;
+    if (col >= a.ncols) return;  // zero columns stay zero
+    const bool red = a.red != nullptr;
+    auto apply = [&](int k, const float2 h, double m2) {
+        float2 x = tile[k * W + w];
+        if (red) {
+            const double pp = (double)x.x * x.x + (double)x.y * x.y;
+            p0 += pp;
+            l1 += pp * (1.0 - m2);
+        }
+        tile[k * W + w] = cmul(x, h);
+    };
+    const double fx = (col <= a.ncols / 2 ? (double)col : (double)(col - a.ncols)) / ((double)a.ncols * a.dx);
+    const double ax = hu.wl * fx;
+    const double cx = fma(-ax, ax, 1.0);
+    const double g = hu.wl / ((double)L * a.dx);
+    const double tg = 2.0 * (double)T * g, ay0 = (2.0 * (double)tt + (double)r) * g;
+#pragma unroll
+    for (int i = 0; i < E / 2; i++) {
+        const int k = tt + i * T;
+        double m2;
+        const float2 h = h_f32(a, hu, cx, fma((double)i, tg, ay0), m2);
+        apply(k, h, m2);
+        if (r == 0) {
+            if (k != 0) apply(LH - k, h, m2);
+        } else {
+            apply(LH - 1 - k, h, m2);
+        }
+    }
+    if (r == 0 && tt == 0) {
+        double m2;
+        const float2 h = h_f32(a, hu, cx, (double)LH * g, m2);
+        apply(LH / 2, h, m2);
+    }
+}
+
+// Fused column sweep with a tile of W columns split over a two-CTA cluster:
+// rank r holds rows [r L/2, (r+1) L/2) of the tile, in 512 threads and 80 KB
+// of shared memory, so two CTAs are resident per SM and one's global-memory
+// phases overlap the other's transforms (a whole-column CTA needs the full
+// register file).  Forward: one radix-2 decimation-in-frequency step across
+// the pair through distributed shared memory (rank 0 keeps x[n] + x[n+L/2],
+// rank 1 (x[n] - x[n+L/2]) W_L^n), then a local L/2 transform gives the even
+// (rank 0) or odd (rank 1) frequencies.  After H, the local inverse and the
+// mirrored step: x[n] = e[n] + W_L^-n o[n] (rank 0), x[n+L/2] = e[n] -
+// W_L^-n o[n] (rank 1).  Every thread of both CTAs reaches the four cluster
+// barriers; a CTA's shared memory is read by its partner only between them.
+template <int L, int E, int W>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(W * (L / 2 / E), 2) k_cols_pair(const FastCols a) {
+    using C = float2;
+    constexpr int LH = L / 2;
+    using PL = FPlan<LH, E>;
+    constexpr int T = PL::T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cg::cluster_group cl = cg::this_cluster();
+    const int r = (int)cl.block_rank();
+    const int w = threadIdx.x & (W - 1);
+    const int tt = threadIdx.x / W;
+    C* tile = reinterpret_cast<C*>(smraw);
+    C* smb = tile + w;
+    const C* ptile = cl.map_shared_rank(tile, r ^ 1);
+    const int col0 = (int)(blockIdx.x >> 1) * W;
+    const int col = col0 + w;
+    const bool act = col < a.ncols;
+    const C* twh = reinterpret_cast<const C*>(a.tw_half);
+    const C* twl = reinterpret_cast<const C*>(a.tw_pair);
+    const long long roff = (long long)r * LH * a.ld;
+    C* base = reinterpret_cast<C*>(a.data) + (long long)blockIdx.y * a.bstride + col + roff;
+    const C* sbase =
+        a.src ? reinterpret_cast<const C*>(a.src) + (long long)blockIdx.y * a.src_bstride + col + roff : base;
+    constexpr int R1 = PL::RS;  // first forward pass (natural mapping on load)
+    constexpr int RO = PL::RS;  // last inverse pass (natural mapping on store)
+    C v[E];
+    if (act) {
+        const C* src = sbase + (long long)tt * a.ld;
+#pragma unroll
+        for (int s = 0; s < E; s++) v[s] = __ldcs(src + (long long)fpos<R1, E, LH>(s, 0) * a.ld);
+    } else {
+#pragma unroll
+        for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
+    }
+#pragma unroll
+    for (int s = 0; s < E; s++) tile[fpos<R1, E, LH>(s, tt) * W + w] = v[s];
+    cl.sync();
+#pragma unroll
+    for (int s = 0; s < E; s++) {
+        const int n = fpos<R1, E, LH>(s, tt);
+        const C y = ptile[n * W + w];
+        if (r == 0) v[s] = make_float2(v[s].x + y.x, v[s].y + y.y);
+        else v[s] = cmul(make_float2(y.x - v[s].x, y.y - v[s].y), ldg_keep(twl + n));
+    }
+    cl.sync();  // the partner has read this CTA's tile
+    fpasses<LH, E, false, 0, W>(v, smb, tt, twh);
+
+    double p0 = 0, l1 = 0;
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < E; s++) tile[(tt + s * T) * W + w] = v[s];
+    __syncthreads();
+    col_tile_h_pair<L, E, W>(tile, r, col0, a, h_unit(a, blockIdx.y), p0, l1);
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < E; s++) v[s] = tile[(tt + s * T) * W + w];
+    fpasses<LH, E, true, 0, W>(v, smb, tt, twh);
+
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < E; s++) tile[fpos<RO, E, LH>(s, tt) * W + w] = v[s];
+    cl.sync();
+#pragma unroll
+    for (int s = 0; s < E; s++) {
+        const int n = fpos<RO, E, LH>(s, tt);
+        const C y = ptile[n * W + w];
+        C t = ldg_keep(twl + n);
+        t.y = -t.y;
+        if (r == 0) {
+            const C o = cmul(t, y);
+            v[s] = make_float2(v[s].x + o.x, v[s].y + o.y);
+        } else {
+            const C o = cmul(t, v[s]);
+            v[s] = make_float2(y.x - o.x, y.y - o.y);
+        }
+    }
+    cl.sync();  // the partner has read this CTA's tile
+    if (act) {
+        C* dst = base + (long long)tt * a.ld;
+#pragma unroll
+        for (int s = 0; s < E; s++) dst[(long long)fpos<RO, E, LH>(s, 0) * a.ld] = v[s];
+    }
+    col_write_red(a, (long long)blockIdx.y * gridDim.x + blockIdx.x, p0, l1, nullptr);
+}
+
+bool fast_cols_pair_case(int fp64, int L, int E, int W) { return !fp64 && L == 2048 && E == 16 && W == 8; }
+
+cudaError_t fast_cols_pair(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks) {
+    if (!fast_cols_pair_case(fp64, L, E, fast_col_width(fp64, L, E, a.W)) || a.hist || !a.tw_half || !a.tw_pair)
+        return cudaErrorNotSupported;
+    constexpr int LL = 2048, EE = 16, WW = 8;
+    const size_t smem = (size_t)fcol_elems(LL / 2, EE, WW) * sizeof(float2);
+    cudaError_t e = cudaFuncSetAttribute(k_cols_pair<LL, EE, WW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid(2 * ((a.ncols + WW - 1) / WW), a.batch > 0 ? a.batch : 1);
+    if (nblocks) *nblocks = (int)(grid.x * grid.y);
+    k_cols_pair<LL, EE, WW><<<grid, WW * (LL / 2 / EE), smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+// W_L^n = exp(-2 pi i n / L), n < L/2
+template <typename C>
+__global__ void k_pair_twiddles(C* out, int L) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= L / 2) return;
+    double s, c;
+    sincospi(-2.0 * (double)n / (double)L, &s, &c);
+    out[n] = mkc<C>((decltype(C::x))c, (decltype(C::x))s);
+}
+cudaError_t fast_build_pair_twiddles(int fp64, int L, void* out, cudaStream_t st) {
+    const int g = (L / 2 + 255) / 256;
+    if (fp64) k_pair_twiddles<double2><<<g, 256, 0, st>>>(reinterpret_cast<double2*>(out), L);
+    else k_pair_twiddles<float2><<<g, 256, 0, st>>>(reinterpret_cast<float2*>(out), L);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ tables

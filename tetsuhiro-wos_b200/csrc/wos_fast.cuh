@@ -58,10 +58,22 @@ struct FastCols {
     const double* batch_wl;
     const double* batch_z;
     double z;
+    // split tiles (FP32, L = 2048, W = 8): a tile is held by a two-CTA cluster,
+    // half of every column per CTA; per-pass twiddles of length L/2 and the
+    // table W_L^n for n < L/2 (both null: one CTA per tile)
+    const void* tw_half;
+    const void* tw_pair;
 };
 
 cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaStream_t st, int* nblocks);
 cudaError_t fast_cols(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks);
+// The column sweep on two-CTA clusters (see FastCols::tw_half); returns
+// cudaErrorNotSupported outside its case (FP32, L = 2048, E = 16, W = 8, no
+// histogram, tables given).
+cudaError_t fast_cols_pair(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks);
+bool fast_cols_pair_case(int fp64, int L, int E, int W);
+// W_L^n (forward sign) for n < L/2 in the pipeline's precision, generated in FP64.
+cudaError_t fast_build_pair_twiddles(int fp64, int L, void* out, cudaStream_t st);
 // Inverse design on rows (ASM forward / adjoint of L = sum (|u|^2 - T)^2):
 // stage 0 loads a exp(i phi) and transforms forward; stage 1 transforms back
 // to u, forms r = 4 (|u|^2 - T) u (loss partial per CTA, slot 0 of a record of
