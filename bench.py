@@ -224,7 +224,7 @@ def time_device(g, torch, bufs, steps, warmup, batch, ctx, stream, profile=False
 
 # ---------------------------------------------------------------------------
 # Secondary configurations of the workload table (one JSON line each):
-#   python bench.py --config {cfg1,cfg2,cfg3,cfg4.1,cfg4.2,cfg4.3,cfg5,cfg5.2}
+#   python bench.py --config {cfg1,cfg2,cfg3,cfg4.1,cfg4.2,cfg4.3,cfg5,cfg5.2,train}
 # Seeded synthetic inputs of the stated shapes stand in for the reference's
 # cases; timed through the library's public entry points with CUDA events on
 # the context's stream (host-buffer entry points include their H2D/D2H, with
@@ -257,7 +257,10 @@ def _algorithmic_bytes(name: str, esz: int) -> float:
             "cfg4.3": 32 * 768 ** 2 * 129 * k, "cfg5": 108 * 2048 ** 2 * k,
             # diffractive stack, 3 layers x 200 slices, forward + adjoint: 2 nl (2S + 3)
             # field sweeps (R+W) plus per-layer mask / state / gradient passes and the residual
-            "cfg5.2": (2 * 3 * (2 * 200 + 3) * 16 + 3 * 72 + 24) * 2048 ** 2 * k}[name]
+            "cfg5.2": (2 * 3 * (2 * 200 + 3) * 16 + 3 * 72 + 24) * 2048 ** 2 * k,
+            # element train: 3 elements on the complex128 planes (32 B/px each), 3
+            # propagations (64 B/px each: complex128 in and out of the FP32 sweeps), one sensor
+            "train": (3 * 32 + 3 * 64 + 24) * 2048 ** 2}[name]
 
 
 def run_config(args) -> None:
@@ -413,6 +416,40 @@ def run_config(args) -> None:
                                  max(2, args.steps // 10), 1)
             if prec == wos.FP64:
                 rec_cpu = cpu(lambda: O.asm_phase_loss_grad(a, phi, tgt, dx, z, O.Context(wavelength=wl)))
+        elif name == "train":
+            # an element train at 2048^2: lens, 5 cm, aperture, 2 cm, grating, 1 cm, sensor
+            n, dx, wl = 2048, 2e-6, 632.8e-9
+            r = np.random.default_rng(1)
+            pin = lambda x: torch.from_numpy(x).pin_memory().numpy()  # noqa: E731
+            ex = pin(np.exp(1j * r.uniform(0, 2 * np.pi, (n, n))))
+            sensor = pin(np.zeros((n, n)))
+            ops = [("lens", wl, 0.1, 1.5e-3, 0.0, 0.0), ("propagate", 0.05, "asm"), ("aperture", 1.2e-3, 0.0, 0.0, 0.0),
+                   ("propagate", 0.02, "asm"), ("grating", "phase_sin", 40e-6, 1.0, 0.5, 0.0, 0.0, 0.0),
+                   ("propagate", 0.01, "asm"), ("intensity", sensor)]
+            f = wos.Field(ex, dx)
+            cx = wos.Context(wavelength=wl, warnings_enabled=False)
+            rec["e2e_s"] = timed(lambda: g.train(f, ops, cx), max(2, args.steps // 10), 1)
+
+            def per_call():
+                g.apply_lens(f, wl, 0.1, 1.5e-3)
+                g.propagate(f, 0.05, "asm", cx)
+                g.apply_aperture_circle(f, 1.2e-3)
+                g.propagate(f, 0.02, "asm", cx)
+                g.apply_grating(f, "phase_sin", 40e-6, 1.0, 0.5)
+                g.propagate(f, 0.01, "asm", cx)
+            rec["one_call_per_op_s"] = timed(per_call, max(2, args.steps // 10), 1)
+            if prec == wos.FP64:
+                def cpu_train():
+                    of = O.Field(ex.copy(), dx)
+                    oc = O.Context(wavelength=wl, warnings_enabled=False)
+                    O.apply_lens(of, wl, 0.1, 1.5e-3)
+                    O.propagate(of, 0.05, "asm", oc)
+                    O.apply_aperture_circle(of, 1.2e-3)
+                    O.propagate(of, 0.02, "asm", oc)
+                    O.apply_grating(of, "phase_sin", 40e-6, 1.0, 0.5)
+                    O.propagate(of, 0.01, "asm", oc)
+                    of.intensity()
+                rec_cpu = cpu(cpu_train)
         elif name == "cfg5.2":
             # 3 phase masks, each followed by 200 BPM slices of 5 um through a
             # uniform n = 1.5 medium; loss and gradient of all masks
@@ -475,7 +512,7 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--config", default="headline",
-                    help="headline (default) or one of cfg1 cfg2 cfg3 cfg4.1 cfg4.2 cfg4.3 cfg5 cfg5.2")
+                    help="headline (default) or one of cfg1 cfg2 cfg3 cfg4.1 cfg4.2 cfg4.3 cfg5 cfg5.2 train")
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the default (or WOS_ROWE/WOS_COLE/WOS_COLW) launch configuration")
     args = ap.parse_args()

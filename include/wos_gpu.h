@@ -278,6 +278,56 @@ WOS_API int wos_shift_field(wos_ctx ctx, wos_field* f, double du, double dv);
 WOS_API int wos_apply_diffuser(wos_ctx ctx, wos_field* f, double sigma, double correlation, double amplitude,
                                long long seed, double x0, double y0);
 
+/* ---- element train on the device (the element loop of trainer.runTrain,
+ *      optics/simulator.go:397-500, without beam-splitter arms): the field is
+ *      uploaded once, every op runs on the device in order, and the field is
+ *      downloaded once at the end.  After every WOS_OP_PROPAGATE the
+ *      bandlimit (fraction, sigma of Nyquist) is applied when fraction is in
+ *      (0, 1), as runTrain does when ctx.Bandlimit is set.  diag (may be NULL)
+ *      accumulates the warnings of every propagation (the shared
+ *      ctx.Warnings); dx_out is the final pitch (fraunhofer changes it, and
+ *      later ops use the new pitch).  f->polarized is updated when a Jones op
+ *      turns a scalar field into a polarized one (f->ey must then hold
+ *      ny*nx elements).  Parameters per kind, in the order of the matching
+ *      wos_apply_* call:
+ *        PROPAGATE   method = wos_method, a[0] = z
+ *        LENS        a = {wavelength, focal, aperture, x0, y0}
+ *        APERTURE    a = {radius, x0, y0, edge_sigma}
+ *        GRATING     method = grating kind, a = {period, modulation, duty, blaze_depth, rotation, offset}
+ *        PHASE_MASK  map = host phi [ny][nx], a[0] = amplitude
+ *        DIFFUSER    a = {sigma, correlation, amplitude, seed, x0, y0}
+ *        JONES       m = {a, b, c, d}
+ *        SCALE       m[0] = s
+ *        TILT        a = {tx, ty, wavelength}
+ *        SHIFT       a = {du, dv}
+ *        BANDLIMIT   a = {fraction, sigma}
+ *        INTENSITY   out = host [ny][nx] FP64, receives |Ex|^2 (+ |Ey|^2) at this
+ *                    point of the train (a sensor plane; only it crosses PCIe) ---- */
+enum wos_op_kind {
+    WOS_OP_PROPAGATE = 1,
+    WOS_OP_LENS = 2,
+    WOS_OP_APERTURE = 3,
+    WOS_OP_GRATING = 4,
+    WOS_OP_PHASE_MASK = 5,
+    WOS_OP_DIFFUSER = 6,
+    WOS_OP_JONES = 7,
+    WOS_OP_SCALE = 8,
+    WOS_OP_TILT = 9,
+    WOS_OP_SHIFT = 10,
+    WOS_OP_BANDLIMIT = 11,
+    WOS_OP_INTENSITY = 12
+};
+typedef struct {
+    int kind;
+    int method;
+    double a[8];
+    wos_c128 m[4];
+    const double* map;
+    double* out;
+} wos_op;
+WOS_API int wos_train(wos_ctx ctx, wos_field* f, const wos_op* ops, int nops, const wos_context* c,
+                      double bandlimit_fraction, double bandlimit_sigma, wos_diag* diag);
+
 /* ---- Propagate1D (optics/propagate.go:718-738): a[n] complex128 in place,
  *      pixel dx, distance z, wavelength wl (the Context's wavelength is not
  *      used).  diag (may be NULL): p_in / p_out are sum |a|^2 without a dx

@@ -3098,6 +3098,138 @@ int wos_bpm_stack_loss_grad(wos_ctx c, int ny, int nx, double dx, int nlayers, c
     return WOS_OK;
 }
 
+int wos_train(wos_ctx c, wos_field* f, const wos_op* ops, int nops, const wos_context* cci, double bl_fraction,
+              double bl_sigma, wos_diag* diag) {
+    if (!c || (nops > 0 && !ops) || nops < 0) return fail(WOS_INVALID_ARG, "train arguments");
+    TRY(check_field(f));
+    bool need_ey = f->polarized != 0;
+    for (int i = 0; i < nops; i++) {
+        const wos_op& o = ops[i];
+        if (o.kind < WOS_OP_PROPAGATE || o.kind > WOS_OP_INTENSITY) return fail(WOS_INVALID_ARG, "train: unknown op");
+        if (o.kind == WOS_OP_JONES) need_ey = true;
+        if (o.kind == WOS_OP_PROPAGATE && (o.method < WOS_ASM || o.method > WOS_FRAUNHOFER))
+            return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
+        if ((o.kind == WOS_OP_PHASE_MASK && !o.map) || (o.kind == WOS_OP_INTENSITY && !o.out))
+            return fail(WOS_INVALID_ARG, "train: null map / output");
+        if (o.kind == WOS_OP_GRATING && (o.method < 0 || o.method > 4 || !(o.a[0] > 0) || o.a[2] < 0 || o.a[2] > 1))
+            return fail(WOS_INVALID_ARG, "train: grating parameters");
+        if (o.kind == WOS_OP_LENS && (o.a[1] == 0 || !(o.a[0] > 0))) return fail(WOS_INVALID_ARG, "train: lens parameters");
+        if (o.kind == WOS_OP_TILT && !(o.a[2] > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    }
+    if (need_ey && !f->ey) return fail(WOS_INVALID_ARG, "train: a Jones op needs an Ey buffer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const wos_context cc = cci ? *cci : default_context();
+    if (diag) {
+        std::memset(diag, 0, sizeof(*diag));
+        diag->dx_out = f->dx;
+    }
+    const long long np = (long long)f->ny * f->nx;
+    int pol = f->polarized ? 1 : 0;
+    TRY(ensure(c->stage, (size_t)np * 16 * (need_ey ? 2 : 1)));
+    CK(cudaMemcpyAsync(c->stage.p, f->ex, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
+    if (pol) CK(cudaMemcpyAsync(stage_ey(c, f), f->ey, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
+    double2* ex = stage_ex(c);
+    double2* ey = stage_ey(c, f);
+    double dx = f->dx;
+    bool first_prop = true;
+    for (int i = 0; i < nops; i++) {
+        const wos_op& o = ops[i];
+        const double* a = o.a;
+        switch (o.kind) {
+        case WOS_OP_PROPAGATE: {
+            if (a[0] == 0) break;  // Propagate with z == 0 returns at once (propagate.go:66-68)
+            wos_diag d{};
+            Prop p{f->ny, f->nx, dx, pol ? 2 : 1, c->stage.p, 1, c->stage.p, 1, a[0], o.method, cc, &d};
+            if (!diag) p.diag = (o.method == WOS_FRAUNHOFER) ? &d : nullptr;
+            TRY(run_propagate(c, p));
+            if (o.method == WOS_FRAUNHOFER) dx = d.dx_out;
+            if (diag) {
+                diag_merge(diag, d);
+                if (first_prop) diag->p_in = d.p_in;
+                diag->p_out = d.p_out;
+                first_prop = false;
+            }
+            if (bl_fraction > 0 && bl_fraction < 1) {
+                const double fnyq = 1 / (2 * dx);
+                double sig = bl_sigma * fnyq;
+                if (sig <= 0) sig = fnyq * 0.01;
+                TRY(spectral_filter(c, f->ny, f->nx, dx, pol ? 2 : 1, c->stage.p, H_BANDLIMIT, bl_fraction * fnyq,
+                                    sig));
+            }
+        } break;
+        case WOS_OP_LENS: {
+            const double k = 2 * M_PI / a[0];
+            CK(launch_lens(ex, ey, pol, f->ny, f->nx, dx, -k / (2 * a[1]), a[2], a[3], a[4], c->st));
+        } break;
+        case WOS_OP_APERTURE:
+            CK(launch_aperture_circle(ex, ey, pol, f->ny, f->nx, dx, a[0], a[1], a[2], a[3], c->st));
+            break;
+        case WOS_OP_GRATING:
+            CK(launch_grating(ex, ey, pol, f->ny, f->nx, dx, o.method, a[0], a[1], a[2], a[3], a[4], a[5], c->st));
+            break;
+        case WOS_OP_PHASE_MASK: {
+            TRY(ensure(c->maps, sizeof(double) * np));
+            CK(cudaMemcpyAsync(c->maps.p, o.map, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
+            CK(launch_phase_mask(ex, ey, pol, np, reinterpret_cast<double*>(c->maps.p), a[0], c->st));
+        } break;
+        case WOS_OP_DIFFUSER: {
+            TRY(ensure(c->aux, (size_t)np * sizeof(double2)));
+            double2* zp = reinterpret_cast<double2*>(c->aux.p);
+            CK(launch_diffuser_noise(zp, f->ny, f->nx, dx, dx > 0 ? dx : 1.0, a[4], a[5], (long long)a[3], c->st));
+            if (a[1] > 0) {
+                const double neg_two_pi_sq = -19.739208802178716;
+                TRY(spectral_filter(c, f->ny, f->nx, dx, 1, zp, H_GAUSS, neg_two_pi_sq * a[1] * a[1], 0));
+            }
+            const int nb = sum_re2_blocks(np);
+            TRY(red_prepare(c, (size_t)nb));
+            CK(launch_sum_re2(zp, np, red_region(c, 0), c->st));
+            CK(launch_reduce_finish(red_region(c, 0), nb, 1, 0, 2, redout_region(c, 0), c->st));
+            CK(launch_diffuser_apply(ex, ey, pol, np, zp, redout_region(c, 0), a[0], a[2], c->st));
+        } break;
+        case WOS_OP_JONES: {
+            int mode = 2;
+            if (!pol) {
+                const bool dg = o.m[1].re == 0 && o.m[1].im == 0 && o.m[2].re == 0 && o.m[2].im == 0 &&
+                                o.m[3].re == o.m[0].re && o.m[3].im == o.m[0].im;
+                mode = dg ? 0 : 1;
+            }
+            CK(launch_jones(ex, ey, np, mode, d2(o.m[0]), d2(o.m[1]), d2(o.m[2]), d2(o.m[3]), c->st));
+            if (mode == 1) pol = 1;
+        } break;
+        case WOS_OP_SCALE:
+            CK(launch_scale(ex, ey, pol, np, d2(o.m[0]), c->st));
+            break;
+        case WOS_OP_TILT:
+            CK(launch_tilt(ex, ey, pol, f->ny, f->nx, dx, 2 * M_PI / a[2], std::sin(a[0]), std::sin(a[1]), c->st));
+            break;
+        case WOS_OP_SHIFT:
+            if (a[0] != 0 || a[1] != 0)
+                TRY(spectral_filter(c, f->ny, f->nx, dx, pol ? 2 : 1, c->stage.p, H_SHIFT, a[0], a[1]));
+            break;
+        case WOS_OP_BANDLIMIT:
+            if (a[0] > 0 && a[0] < 1) {
+                const double fnyq = 1 / (2 * dx);
+                double sig = a[1] * fnyq;
+                if (sig <= 0) sig = fnyq * 0.01;
+                TRY(spectral_filter(c, f->ny, f->nx, dx, pol ? 2 : 1, c->stage.p, H_BANDLIMIT, a[0] * fnyq, sig));
+            }
+            break;
+        case WOS_OP_INTENSITY: {
+            TRY(ensure(c->accum, sizeof(double) * np));
+            double* acc = reinterpret_cast<double*>(c->accum.p);
+            CK(cudaMemsetAsync(acc, 0, sizeof(double) * np, c->st));
+            CK(launch_accum_int(1, acc, c->stage.p, pol ? 2 : 1, np, 1.0, c->st));
+            CK(cudaMemcpyAsync(o.out, acc, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
+        } break;
+        }
+    }
+    f->polarized = pol;
+    f->dx = dx;
+    if (diag) diag->dx_out = dx;
+    return stage_out(c, f, pol ? 2 : 1);
+}
+
 int wos_asm_forward_loss(wos_ctx c, int ny, int nx, double dx, double z, const wos_context* cc, const wos_c128* a,
                          const double* phi, const double* target, double* loss) {
     if (!c) return fail(WOS_INVALID_ARG, "null ctx");

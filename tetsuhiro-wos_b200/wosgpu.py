@@ -45,6 +45,7 @@ EXPORTS = [
     "wos_apply_jones", "wos_scale_amplitude", "wos_apply_tilt", "wos_apply_bandlimit", "wos_shift_field",
     "wos_apply_diffuser", "wos_propagate1d",
     "wos_bpm_stack_loss_grad", "wos_bpm_stack_loss_grad_dev", "wos_splitstep_adjoint_dev",
+    "wos_train",
 ]
 
 
@@ -75,6 +76,15 @@ class C128(C.Structure):
 def _c128(v) -> C128:
     v = complex(v)
     return C128(v.real, v.imag)
+
+
+class COp(C.Structure):
+    _fields_ = [("kind", C.c_int), ("method", C.c_int), ("a", C.c_double * 8), ("m", C128 * 4),
+                ("map", C.c_void_p), ("out", C.c_void_p)]
+
+
+OP_KINDS = {"propagate": 1, "lens": 2, "aperture": 3, "grating": 4, "phase_mask": 5, "diffuser": 6,
+            "jones": 7, "scale": 8, "tilt": 9, "shift": 10, "bandlimit": 11, "intensity": 12}
 
 
 class CField(C.Structure):
@@ -152,6 +162,7 @@ def lib():
             "wos_bpm_stack_loss_grad": ([vp, i, i, d, i, vp, vp, vp, d, vp, i, vp, vp, vp], i),
             "wos_bpm_stack_loss_grad_dev": ([vp, i, i, d, i, vp, vp, vp, d, vp, i, vp, vp, vp], i),
             "wos_splitstep_adjoint_dev": ([vp, i, i, d, i, vp, d, vp, i, vp], i),
+            "wos_train": ([vp, vp, vp, i, vp, d, d, vp], i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name, None)
@@ -540,6 +551,56 @@ class GPU:
         if ctx is not None:
             ctx.absorb(d)
         return (a, d) if diag else a
+
+    # ---- element train on the device (trainer.runTrain, simulator.go:397-500)
+    def train(self, f: Field, ops, ctx: Optional[Context] = None, bandlimit=None, diag: bool = False):
+        """Run `ops` on the field with one upload and one download.  Each op is
+        a tuple: ("propagate", z, method), ("lens", wl, focal, aperture, x0, y0),
+        ("aperture", radius, x0, y0, edge_sigma), ("grating", kind, period,
+        modulation, duty, blaze_depth, rotation, offset), ("phase_mask", phi, amp),
+        ("diffuser", sigma, corr, amp, seed, x0, y0), ("jones", a, b, c, d),
+        ("scale", s), ("tilt", tx, ty, wl), ("shift", du, dv), ("bandlimit",
+        fraction, sigma), ("intensity", out) with out a float64 (ny, nx) array.
+        bandlimit = (fraction, sigma) is applied after every propagation."""
+        arr = (COp * max(1, len(ops)))()
+        keep = []
+        for k, op in enumerate(ops):
+            name, args = op[0], op[1:]
+            o = arr[k]
+            o.kind = OP_KINDS[name]
+            if name == "propagate":
+                o.a[0] = args[0]
+                o.method = METHODS[args[1] if len(args) > 1 else "asm"]
+            elif name == "grating":
+                o.method = GRATING_KINDS[args[0]]
+                for j, v in enumerate(args[1:]):
+                    o.a[j] = v
+            elif name == "phase_mask":
+                phi = np.ascontiguousarray(args[0], dtype=np.float64)
+                keep.append(phi)
+                o.map = phi.ctypes.data
+                o.a[0] = args[1] if len(args) > 1 else 1.0
+            elif name == "intensity":
+                out = args[0]
+                assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and out.shape == (f.ny, f.nx)
+                o.out = out.ctypes.data
+            elif name in ("jones", "scale"):
+                for j, v in enumerate(args):
+                    o.m[j] = _c128(v)
+            else:
+                for j, v in enumerate(args):
+                    o.a[j] = v
+        d = CDiag()
+        cf = f.c()
+        cc = ctx.c() if ctx is not None else None
+        fr, sg = bandlimit if bandlimit is not None else (0.0, 0.0)
+        _check(lib().wos_train(self.h, C.byref(cf), arr, len(ops), C.byref(cc) if cc is not None else None, fr, sg,
+                               C.byref(d) if (diag or ctx is not None) else None))
+        f.polarized = bool(cf.polarized)
+        f.dx = cf.dx
+        if ctx is not None:
+            ctx.absorb(d)
+        return d
 
     # ---- diffractive stack (masks with BPM segments between them)
     def bpm_stack_loss_grad(self, a: np.ndarray, phis: np.ndarray, target: np.ndarray, dx: float, zseg: float,
