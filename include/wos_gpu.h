@@ -278,6 +278,14 @@ WOS_API int wos_shift_field(wos_ctx ctx, wos_field* f, double du, double dv);
 WOS_API int wos_apply_diffuser(wos_ctx ctx, wos_field* f, double sigma, double correlation, double amplitude,
                                long long seed, double x0, double y0);
 
+/* ---- PropagateVectorial (optics/vectorial.go:14-80; Propagate with method
+ *      "vectorial", propagate.go:90-93): Ex and Ey (both used whatever
+ *      f->polarized says, as the reference uses f.Ey) propagate in place and
+ *      ez [ny][nx] complex128 receives the longitudinal component
+ *      Ez = -(kx Ex + ky Ey) / kz propagated with them.  z == 0 leaves
+ *      everything untouched (Propagate returns first). ---- */
+WOS_API int wos_propagate_vectorial(wos_ctx ctx, wos_field* f, wos_c128* ez, double z, const wos_context* c);
+
 /* ---- element train on the device (the element loop of trainer.runTrain,
  *      optics/simulator.go:397-500, without beam-splitter arms): the field is
  *      uploaded once, every op runs on the device in order, and the field is

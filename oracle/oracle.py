@@ -93,6 +93,7 @@ def lib():
         L.or_spectral_centroid.argtypes = [vp, vp, vp]
         L.or_propagate.argtypes = [vp, d, i, vp]; L.or_propagate.restype = i
         L.or_propagate1d.argtypes = [vp, i, d, d, d, vp]
+        L.or_propagate_vectorial.argtypes = [vp, vp, d, vp]
         L.or_splitstep.argtypes = [vp, d, vp, i, vp]
         L.or_polychromatic.argtypes = [vp, d, vp, vp, i, i, vp, vp]; L.or_polychromatic.restype = i
         L.or_propagate3d.argtypes = [vp, vp, i, i, vp, vp]; L.or_propagate3d.restype = i
@@ -234,6 +235,19 @@ def propagate1d(a: np.ndarray, dx: float, z: float, wl: float, ctx: Optional[Con
         lib().or_propagate1d(_ptr(a), a.size, dx, z, wl, C.byref(cc))
         ctx._from_c(cc)
     return a
+
+
+def propagate_vectorial(f: Field, z: float, ctx: Optional[Context]) -> np.ndarray:
+    """PropagateVectorial (vectorial.go:14-80): Ex, Ey in place; returns Ez."""
+    ez = np.zeros_like(f.ex)
+    cf = f._c()
+    if ctx is None:
+        lib().or_propagate_vectorial(C.byref(cf), _ptr(ez), z, None)
+    else:
+        cc = ctx._to_c()
+        lib().or_propagate_vectorial(C.byref(cf), _ptr(ez), z, C.byref(cc))
+        ctx._from_c(cc)
+    return ez
 
 
 def spectral_radius(f: Field, frac: float) -> float:

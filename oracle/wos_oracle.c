@@ -1272,3 +1272,58 @@ double or_bpm_stack_loss_grad(int ny, int nx, double dx, int nl, const oc128 *a,
     free(u); free(ey); free(V);
     return loss;
 }
+
+/* ------------------------------------------------------------------ */
+/* PropagateVectorial (vectorial.go:14-80)                              */
+/* ------------------------------------------------------------------ */
+int or_propagate_vectorial(or_field *f, oc128 *ez_out, double z, or_context *ctx) {
+    or_context local;
+    if (!ctx) { memset(&local, 0, sizeof(local)); ctx = &local; }
+    int ny = f->ny, nx = f->nx;
+    size_t n = npix(f);
+    double wl = ctx->wavelength;
+    double k = 2 * M_PI / wl;
+    double az = fabs(z);
+    int backward = z < 0;
+    int zero, reg; double alpha, limit;
+    ev_policy(ctx, z, &zero, &reg, &alpha, &limit);
+    or_fft2d(f->ex, ny, nx, 0);
+    or_fft2d(f->ey, ny, nx, 0);
+    oc128 *ez = (oc128 *)calloc(n, sizeof(oc128));
+    for (int j = 0; j < ny; j++) {
+        double fy = freq_n(j, ny, f->dx);
+        double ky = 2 * M_PI * fy;
+        for (int i = 0; i < nx; i++) {
+            double fx = freq_n(i, nx, f->dx);
+            double kx = 2 * M_PI * fx;
+            double rho = wl * go_hypot(fx, fy);
+            size_t idx = (size_t)j * nx + i;
+            oc128 H;
+            oc128 ex = f->ex[idx], ey = f->ey[idx];
+            /* -(kx Ex + ky Ey), the complex products with a real factor exact */
+            double sr = -(kx * ex.re + ky * ey.re), si = -(kx * ex.im + ky * ey.im);
+            if (rho <= 1) {
+                double kz = k * sqrt((1 - rho) * (1 + rho));
+                H = cexpi(kz * z);
+                if (kz > 0) ez[idx] = cmk(sr / kz, si / kz);
+            } else {
+                double decay = k * az * sqrt((rho - 1) * (rho + 1));
+                if (zero || (limit > 0 && decay > limit)) H = cmk(0, 0);
+                else if (backward && reg) { double a = exp(decay); H = cmk(a / (1 + alpha * alpha * a * a), 0); }
+                else if (backward) H = cmk(exp(decay), 0);
+                else H = cmk(exp(-decay), 0);
+                double kzi = k * sqrt((rho - 1) * (rho + 1));
+                if (kzi > 0) ez[idx] = cmk(si / kzi, -sr / kzi); /* s / (i kzi) */
+            }
+            f->ex[idx] = cmul(f->ex[idx], H);
+            f->ey[idx] = cmul(f->ey[idx], H);
+            ez[idx] = cmul(ez[idx], H);
+        }
+    }
+    or_fft2d(f->ex, ny, nx, 1);
+    or_fft2d(f->ey, ny, nx, 1);
+    or_fft2d(ez, ny, nx, 1);
+    memcpy(ez_out, ez, sizeof(oc128) * n);
+    free(ez);
+    return 0;
+}

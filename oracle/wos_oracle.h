@@ -101,6 +101,10 @@ void or_shift_field(or_field *f, double du, double dv);    /* field.go:199-228 *
 /* ---- propagation (optics/propagate.go) ---- */
 int or_propagate(or_field *f, double z, int method, or_context *ctx); /* propagate.go:65-102 */
 int or_propagate1d(oc128 *a, int n, double dx, double z, double wl, or_context *ctx); /* :718-738 */
+/* PropagateVectorial (vectorial.go:14-80): ex and ey (both used whatever
+ * f->polarized, as the reference uses f.Ey) propagate in place, ez_out
+ * receives the reconstructed longitudinal component. */
+int or_propagate_vectorial(or_field *f, oc128 *ez_out, double z, or_context *ctx);
 /* asmTF (propagate.go:159-181) evaluated at (fx, fy) with the policy of ctx */
 oc128 or_asm_tf(double wl, double z, int zero_ev, int reg, double alpha, double limit,
                 double fx, double fy);

@@ -607,3 +607,37 @@ def test_oracle_bpm_stack_forward_is_masks_and_splitstep():
     want = np.sum((np.abs(f.ex) ** 2 - T) ** 2)
     loss, _ = O.bpm_stack_loss_grad(a, phis, T, dx, zseg, steps, d, ctx, want_grad=False)
     assert abs(loss - want) <= 1e-12 * abs(want)
+
+
+def test_oracle_vectorial_transverse_matches_scalar_asm():
+    """The transverse components of the vector ASM are the scalar ASM step
+    (vectorial.go:14-80 and propagate.go:159-181 differ only in rounding)."""
+    n, dx, wl, z = 64, 1e-6, 633e-9, 2e-4
+    rng = np.random.default_rng(1)
+    ex = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    ey = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    fv = O.Field(ex.copy(), dx, ey.copy())
+    O.propagate_vectorial(fv, z, O.Context(wavelength=wl))
+    fs = O.Field(ex.copy(), dx, ey.copy())
+    O.propagate(fs, z, "asm", O.Context(wavelength=wl))
+    assert np.linalg.norm(fv.ex - fs.ex) <= 1e-12 * np.linalg.norm(fs.ex)
+    assert np.linalg.norm(fv.ey - fs.ey) <= 1e-12 * np.linalg.norm(fs.ey)
+
+
+def test_oracle_vectorial_field_is_divergence_free():
+    """kx Ex + ky Ey + kz Ez = 0 for every propagating plane wave."""
+    n, dx, wl, z = 64, 0.5e-6, 633e-9, 3e-6
+    rng = np.random.default_rng(2)
+    ex = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    ey = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    f = O.Field(ex.copy(), dx, ey.copy())
+    ez = O.propagate_vectorial(f, z, O.Context(wavelength=wl))
+    i = np.arange(n)
+    fx = np.where(i <= n // 2, i, i - n) / (n * dx)   # freq (field.go:297-303): +Nyquist
+    FX, FY = np.meshgrid(fx, fx)
+    rho = wl * np.hypot(FX, FY)
+    prop = rho < 1
+    kz = 2 * np.pi / wl * np.sqrt(np.clip(1 - rho ** 2, 0, None))
+    div = 2 * np.pi * FX * np.fft.fft2(f.ex) + 2 * np.pi * FY * np.fft.fft2(f.ey) + kz * np.fft.fft2(ez)
+    scale = np.abs(2 * np.pi / wl * np.fft.fft2(f.ex)).max()
+    assert np.abs(div[prop]).max() <= 1e-10 * scale

@@ -3098,6 +3098,39 @@ int wos_bpm_stack_loss_grad(wos_ctx c, int ny, int nx, double dx, int nlayers, c
     return WOS_OK;
 }
 
+int wos_propagate_vectorial(wos_ctx c, wos_field* f, wos_c128* ez, double z, const wos_context* cci) {
+    if (!c || !f || !f->ex || !f->ey || !ez || f->ny < 2 || f->nx < 2 || !(f->dx > 0))
+        return fail(WOS_INVALID_ARG, "vectorial: ex, ey and ez buffers and a valid geometry are required");
+    if (z == 0) return WOS_OK;  // Propagate returns before the vectorial step (propagate.go:66-68)
+    const wos_context cc = cci ? *cci : default_context();
+    if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const int ny = f->ny, nx = f->nx;
+    const long long np = (long long)ny * nx;
+    TRY(ensure(c->stage, (size_t)np * 16 * 3));
+    double2* st = reinterpret_cast<double2*>(c->stage.p);
+    CK(cudaMemcpyAsync(st, f->ex, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(st + np, f->ey, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
+    void* work = st;
+    if (!c->fp64) {
+        TRY(ensure(c->scratch, (size_t)np * 8 * 3));
+        work = c->scratch.p;
+        CK(launch_convert(0, st, work, 2 * np, c->st));
+    }
+    const Policy pol = ev_policy(cc, z);
+    HArgs h = asm_h(c, cc, z, pol, f->dx, nx, ny);
+    TRY(fft2d_impl(c, c->fp64, ny, nx, 2, work, 0));
+    CK(launch_vectorial(c->fp64, work, ny, nx, f->dx, h, c->st));
+    TRY(fft2d_impl(c, c->fp64, ny, nx, 3, work, 1));
+    if (!c->fp64) CK(launch_convert(1, work, st, 3 * np, c->st));
+    CK(cudaMemcpyAsync(f->ex, st, (size_t)np * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(f->ey, st + np, (size_t)np * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(ez, st + 2 * np, (size_t)np * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
 int wos_train(wos_ctx c, wos_field* f, const wos_op* ops, int nops, const wos_context* cci, double bl_fraction,
               double bl_sigma, wos_diag* diag) {
     if (!c || (nops > 0 && !ops) || nops < 0) return fail(WOS_INVALID_ARG, "train arguments");

@@ -115,6 +115,49 @@ __global__ void __launch_bounds__(256) k_reduce_finish(const double* partials, i
     }
 }
 
+// Vector angular spectrum (PropagateVectorial, optics/vectorial.go:14-80) on
+// the 2-D spectra of Ex and Ey: Ez = -(kx Ex + ky Ey) / kz (kz = i kzi for
+// evanescent bins), then all three times H; rho = wl hypot(fx, fy) and the
+// phase (k sqrt(1 - rho^2)) z in the reference's operation order.
+template <typename C>
+__global__ void k_vectorial(C* ex, C* ey, C* ez, int ny, int nx, double dx, HArgs h) {
+    using T = decltype(C::x);
+    const long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (idx >= (long long)ny * nx) return;
+    const int j = (int)(idx / nx), i = (int)(idx - (long long)j * nx);
+    const double fx = freq_n(i, nx, dx), fy = freq_n(j, ny, dx);
+    const double kx = dmul(2 * M_PI, fx), ky = dmul(2 * M_PI, fy);
+    const double rho = dmul(h.wl, go_hypot(fx, fy));
+    const C x = ex[idx], y = ey[idx];
+    const double sr = -dadd(dmul(kx, (double)x.x), dmul(ky, (double)y.x));
+    const double si = -dadd(dmul(kx, (double)x.y), dmul(ky, (double)y.y));
+    C H = mkc<C>(0, 0), zz = mkc<C>(0, 0);
+    if (rho <= 1.0) {
+        const double kz = dmul(h.k, __dsqrt_rn(dmul(dsub(1.0, rho), dadd(1.0, rho))));
+        H = cexpi<C>(dmul(kz, h.z));
+        if (kz > 0) zz = mkc<C>((T)ddiv(sr, kz), (T)ddiv(si, kz));
+    } else {
+        const double sq = __dsqrt_rn(dmul(dsub(rho, 1.0), dadd(rho, 1.0)));
+        const double decay = dmul(h.kaz, sq);
+        double a;
+        if (h.zero_ev || (h.limit > 0 && decay > h.limit)) a = 0;
+        else if (h.z < 0 && h.reg) {
+            const double e = exp(decay);
+            a = ddiv(e, dadd(1.0, dmul(dmul(dmul(h.alpha, h.alpha), e), e)));
+        } else if (h.z < 0) {
+            a = exp(decay);
+        } else {
+            a = exp(-decay);
+        }
+        H = mkc<C>((T)a, 0);
+        const double kzi = dmul(h.k, sq);
+        if (kzi > 0) zz = mkc<C>((T)ddiv(si, kzi), (T)(-ddiv(sr, kzi)));
+    }
+    ex[idx] = cmul(x, H);
+    ey[idx] = cmul(y, H);
+    ez[idx] = cmul(zz, H);
+}
+
 // 1-D angular spectrum step (asmTF1D, optics/propagate.go:680-701): rho =
 // |wl fx| is asm_tf's hypot with fy = 0.  Spectral power sums for the
 // evanescent_filtered warning, as in the 2-D column pass.
@@ -277,6 +320,19 @@ cudaError_t launch_cols(int fp64, const ColArgs& a, cudaStream_t st) {
     case 8: return launch_cols_t<float, 8>(a, st);
     default: return launch_cols_t<float, 16>(a, st);
     }
+}
+
+cudaError_t launch_vectorial(int fp64, void* planes, int ny, int nx, double dx, const HArgs& h, cudaStream_t st) {
+    const long long np = (long long)ny * nx;
+    const unsigned g = (unsigned)((np + 255) / 256);
+    if (fp64) {
+        double2* p = reinterpret_cast<double2*>(planes);
+        k_vectorial<double2><<<g, 256, 0, st>>>(p, p + np, p + 2 * np, ny, nx, dx, h);
+    } else {
+        float2* p = reinterpret_cast<float2*>(planes);
+        k_vectorial<float2><<<g, 256, 0, st>>>(p, p + np, p + 2 * np, ny, nx, dx, h);
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_asm1d_h(int fp64, void* a, int n, const HArgs& h, double* partials, int* nblocks,

@@ -198,6 +198,8 @@ cudaError_t launch_diffuser_apply(double2* ex, double2* ey, int pol, long long n
 cudaError_t launch_mask_phase(int fp64, void* u, const double* phi, long long n, int conj, cudaStream_t st);
 // g = Re(conj(b) * i * v)
 cudaError_t launch_grad_v(int fp64, const void* b, const void* v, double* g, long long n, cudaStream_t st);
+// Vector angular spectrum step on the spectra of [Ex, Ey, Ez] planes (Ez written).
+cudaError_t launch_vectorial(int fp64, void* planes, int ny, int nx, double dx, const HArgs& h, cudaStream_t st);
 // 1-D angular spectrum step on a forward-transformed line (asmTF1D,
 // optics/propagate.go:668-738): a[i] *= H(fx_i) / n; spectral power sums
 // (RS_SW: sum |F|^2, RS_SW+1: sum |F|^2 (1 - |H|^2)) per CTA into partials.

@@ -45,7 +45,7 @@ EXPORTS = [
     "wos_apply_jones", "wos_scale_amplitude", "wos_apply_tilt", "wos_apply_bandlimit", "wos_shift_field",
     "wos_apply_diffuser", "wos_propagate1d",
     "wos_bpm_stack_loss_grad", "wos_bpm_stack_loss_grad_dev", "wos_splitstep_adjoint_dev",
-    "wos_train",
+    "wos_train", "wos_propagate_vectorial",
 ]
 
 
@@ -163,6 +163,7 @@ def lib():
             "wos_bpm_stack_loss_grad_dev": ([vp, i, i, d, i, vp, vp, vp, d, vp, i, vp, vp, vp], i),
             "wos_splitstep_adjoint_dev": ([vp, i, i, d, i, vp, d, vp, i, vp], i),
             "wos_train": ([vp, vp, vp, i, vp, d, d, vp], i),
+            "wos_propagate_vectorial": ([vp, vp, vp, d, vp], i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name, None)
@@ -551,6 +552,14 @@ class GPU:
         if ctx is not None:
             ctx.absorb(d)
         return (a, d) if diag else a
+
+    def propagate_vectorial(self, f: Field, z: float, ctx: Optional[Context] = None) -> np.ndarray:
+        """PropagateVectorial (vectorial.go:14-80): Ex, Ey in place; returns Ez."""
+        ez = np.zeros_like(f.ex)
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_propagate_vectorial(self.h, C.byref(f.c()), _ptr(ez), z,
+                                             C.byref(cc) if cc is not None else None))
+        return ez
 
     # ---- element train on the device (trainer.runTrain, simulator.go:397-500)
     def train(self, f: Field, ops, ctx: Optional[Context] = None, bandlimit=None, diag: bool = False):
