@@ -286,6 +286,34 @@ WOS_API int wos_apply_diffuser(wos_ctx ctx, wos_field* f, double sigma, double c
  *      everything untouched (Propagate returns first). ---- */
 WOS_API int wos_propagate_vectorial(wos_ctx ctx, wos_field* f, wos_c128* ez, double z, const wos_context* c);
 
+/* ---- plane views in the binary plane format of the reference's server
+ *      (fmt=bin, server/server.go:582-634, server/views.go:131-258): float32
+ *      little-endian [ny][nx], row-major, no header, computed in FP64 on the
+ *      device and rounded once.  Views: TOTAL = Field.Intensity (|Ex|^2, + |Ey|^2
+ *      when polarized, + |Ez|^2 when ez is given), AMPLITUDE = sqrt(TOTAL),
+ *      EX / EY / EZ = |c|^2 of one component, PHASE_X / _Y / _Z = atan2 of one
+ *      component, NaN (0x7fc00000) where its |c|^2 < mask_cut * its peak
+ *      (mask_cut <= 0: 2e-3, the server's default) or everywhere when the
+ *      component carries no light. ---- */
+enum wos_view {
+    WOS_VIEW_TOTAL = 0,
+    WOS_VIEW_AMPLITUDE = 1,
+    WOS_VIEW_EX = 2,
+    WOS_VIEW_EY = 3,
+    WOS_VIEW_EZ = 4,
+    WOS_VIEW_PHASE_X = 5,
+    WOS_VIEW_PHASE_Y = 6,
+    WOS_VIEW_PHASE_Z = 7
+};
+/* Host field (ez may be NULL unless an Ez view is asked for; the Ey views read
+ * f->ey whatever f->polarized says, as the server reads the part's Ey). */
+WOS_API int wos_plane_view(wos_ctx ctx, const wos_field* f, const wos_c128* ez, int view, double mask_cut, float* out);
+/* Device planes of the context's complex type: planes = [ncomp][ny][nx]
+ * (ncomp 1 or 2; polarized when 2), ez null or one plane; out: device float
+ * [ny][nx]. */
+WOS_API int wos_plane_view_dev(wos_ctx ctx, int ny, int nx, int ncomp, const void* planes, const void* ez, int view,
+                               double mask_cut, void* out);
+
 /* ---- element train on the device (the element loop of trainer.runTrain,
  *      optics/simulator.go:397-500, without beam-splitter arms): the field is
  *      uploaded once, every op runs on the device in order, and the field is
@@ -310,7 +338,9 @@ WOS_API int wos_propagate_vectorial(wos_ctx ctx, wos_field* f, wos_c128* ez, dou
  *        SHIFT       a = {du, dv}
  *        BANDLIMIT   a = {fraction, sigma}
  *        INTENSITY   out = host [ny][nx] FP64, receives |Ex|^2 (+ |Ey|^2) at this
- *                    point of the train (a sensor plane; only it crosses PCIe) ---- */
+ *                    point of the train (a sensor plane; only it crosses PCIe)
+ *        VIEW        method = wos_view, a[0] = mask cut, out = host float [ny][nx]
+ *                    (the binary plane format, see wos_plane_view) ---- */
 enum wos_op_kind {
     WOS_OP_PROPAGATE = 1,
     WOS_OP_LENS = 2,
@@ -323,7 +353,8 @@ enum wos_op_kind {
     WOS_OP_TILT = 9,
     WOS_OP_SHIFT = 10,
     WOS_OP_BANDLIMIT = 11,
-    WOS_OP_INTENSITY = 12
+    WOS_OP_INTENSITY = 12,
+    WOS_OP_VIEW = 13
 };
 typedef struct {
     int kind;
@@ -331,7 +362,7 @@ typedef struct {
     double a[8];
     wos_c128 m[4];
     const double* map;
-    double* out;
+    void* out;   /* INTENSITY: double [ny][nx]; VIEW: float [ny][nx] */
 } wos_op;
 WOS_API int wos_train(wos_ctx ctx, wos_field* f, const wos_op* ops, int nops, const wos_context* c,
                       double bandlimit_fraction, double bandlimit_sigma, wos_diag* diag);

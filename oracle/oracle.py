@@ -448,3 +448,32 @@ def build_source(kind: str, n: int, width: float, wl: float, waist: float = 1e-3
     s = np.sqrt(power / cur)
     f.ex *= s
     return f
+
+
+# ---- plane views (server/views.go:131-258) in the binary plane format
+# (server/server.go:620-630: float32 little-endian, row-major, no header)
+PHASE_MASK_CUT = 2e-3  # server/views.go:48
+
+
+def plane_view(f: Field, view: str, ez: Optional[np.ndarray] = None, mask_cut: float = 0.0) -> np.ndarray:
+    """One view of a field as the server's fmt=bin array (float32, little-endian)."""
+    def n2(a):
+        return a.real * a.real + a.imag * a.imag
+    if view in ("total", "amplitude"):
+        v = n2(f.ex)
+        if f.polarized:
+            v = v + n2(f.ey)
+        if ez is not None:
+            v = v + n2(ez)
+        if view == "amplitude":
+            v = np.sqrt(v)
+    elif view in ("ex", "ey", "ez"):
+        v = n2({"ex": f.ex, "ey": f.ey, "ez": ez}[view])
+    else:
+        src = {"phase_x": f.ex, "phase_y": f.ey, "phase_z": ez}[view]
+        mc = mask_cut if mask_cut > 0 else PHASE_MASK_CUT
+        p = n2(src)
+        peak = p.max()
+        v = np.arctan2(src.imag, src.real)
+        v = np.where((peak <= 0) | (p < mc * peak), np.nan, v)
+    return np.ascontiguousarray(v.astype("<f4"))

@@ -1217,7 +1217,27 @@ int fft2d_impl(wos_ctx c, int fp64, int ny, int nx, int batch, void* a, int inve
     return WOS_OK;
 }
 
+// One plane view into the device float buffer `out` (see wos_plane_view);
+// planes of precision fp64 (complex128) or complex64.
+int plane_view_dev(wos_ctx c, int fp64, const void* ex, const void* ey, const void* ez, int pol, long long np,
+                   int view, double mask_cut, void* out) {
+    const double cut = mask_cut > 0 ? mask_cut : 2e-3;
+    const double* peak = nullptr;
+    if (view >= WOS_VIEW_PHASE_X) {
+        const int nb = norm2_max_blocks(np);
+        TRY(red_prepare(c, (size_t)(nb + RS_COUNT - 1) / RS_COUNT + 1));
+        const void* comp = view == WOS_VIEW_PHASE_X ? ex : (view == WOS_VIEW_PHASE_Y ? ey : ez);
+        double* o = redout_region(c, 0);
+        CK(launch_norm2_max(fp64, comp, np, red_region(c, 0), o, c->st));
+        peak = o;
+    }
+    CK(launch_plane_view(fp64, ex, ey, ez, pol, np, view, peak, cut, out, c->st));
+    return WOS_OK;
+}
+
 }  // namespace
+
+// ====================================================================== ABI}  // namespace
 
 // ====================================================================== ABI
 extern "C" {
@@ -3131,6 +3151,45 @@ int wos_propagate_vectorial(wos_ctx c, wos_field* f, wos_c128* ez, double z, con
     return WOS_OK;
 }
 
+int wos_plane_view(wos_ctx c, const wos_field* f, const wos_c128* ez, int view, double mask_cut, float* out) {
+    if (!c || !f || !f->ex || !out || f->ny < 1 || f->nx < 1) return fail(WOS_INVALID_ARG, "plane view arguments");
+    if (view < WOS_VIEW_TOTAL || view > WOS_VIEW_PHASE_Z) return fail(WOS_INVALID_ARG, "unknown plane view");
+    const bool need_ey = view == WOS_VIEW_EY || view == WOS_VIEW_PHASE_Y || (view <= WOS_VIEW_AMPLITUDE && f->polarized);
+    const bool need_ez = view == WOS_VIEW_EZ || view == WOS_VIEW_PHASE_Z;
+    if ((need_ey && !f->ey) || (need_ez && !ez)) return fail(WOS_INVALID_ARG, "plane view: component missing");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const long long np = (long long)f->ny * f->nx;
+    const bool use_ez = ez && (need_ez || view <= WOS_VIEW_AMPLITUDE);
+    TRY(ensure(c->stage, (size_t)np * 16 * 3));
+    double2* st = reinterpret_cast<double2*>(c->stage.p);
+    CK(cudaMemcpyAsync(st, f->ex, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
+    if (need_ey) CK(cudaMemcpyAsync(st + np, f->ey, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
+    if (use_ez) CK(cudaMemcpyAsync(st + 2 * np, ez, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
+    TRY(ensure(c->accum, sizeof(float) * np));
+    TRY(plane_view_dev(c, 1, st, need_ey ? st + np : nullptr, use_ez ? st + 2 * np : nullptr, f->polarized ? 1 : 0,
+                       np, view, mask_cut, c->accum.p));
+    CK(cudaMemcpyAsync(out, c->accum.p, sizeof(float) * np, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+int wos_plane_view_dev(wos_ctx c, int ny, int nx, int ncomp, const void* planes, const void* ez, int view,
+                       double mask_cut, void* out) {
+    if (!c || !planes || !out || ny < 1 || nx < 1 || ncomp < 1 || ncomp > 2)
+        return fail(WOS_INVALID_ARG, "plane view arguments");
+    if (view < WOS_VIEW_TOTAL || view > WOS_VIEW_PHASE_Z) return fail(WOS_INVALID_ARG, "unknown plane view");
+    if ((view == WOS_VIEW_EY || view == WOS_VIEW_PHASE_Y) && ncomp < 2)
+        return fail(WOS_INVALID_ARG, "plane view: component missing");
+    if ((view == WOS_VIEW_EZ || view == WOS_VIEW_PHASE_Z) && !ez) return fail(WOS_INVALID_ARG, "plane view: no Ez");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const long long np = (long long)ny * nx;
+    const char* p = reinterpret_cast<const char*>(planes);
+    return plane_view_dev(c, c->fp64, p, ncomp == 2 ? p + (size_t)np * c->csz() : nullptr, ez, ncomp == 2 ? 1 : 0, np,
+                          view, mask_cut, out);
+}
+
 int wos_train(wos_ctx c, wos_field* f, const wos_op* ops, int nops, const wos_context* cci, double bl_fraction,
               double bl_sigma, wos_diag* diag) {
     if (!c || (nops > 0 && !ops) || nops < 0) return fail(WOS_INVALID_ARG, "train arguments");
@@ -3138,7 +3197,10 @@ int wos_train(wos_ctx c, wos_field* f, const wos_op* ops, int nops, const wos_co
     bool need_ey = f->polarized != 0;
     for (int i = 0; i < nops; i++) {
         const wos_op& o = ops[i];
-        if (o.kind < WOS_OP_PROPAGATE || o.kind > WOS_OP_INTENSITY) return fail(WOS_INVALID_ARG, "train: unknown op");
+        if (o.kind < WOS_OP_PROPAGATE || o.kind > WOS_OP_VIEW) return fail(WOS_INVALID_ARG, "train: unknown op");
+        if (o.kind == WOS_OP_VIEW && (o.method < WOS_VIEW_TOTAL || o.method > WOS_VIEW_PHASE_Y || !o.out))
+            return fail(WOS_INVALID_ARG, "train: view kind / output");
+        if (o.kind == WOS_OP_VIEW && (o.method == WOS_VIEW_EY || o.method == WOS_VIEW_PHASE_Y)) need_ey = true;
         if (o.kind == WOS_OP_JONES) need_ey = true;
         if (o.kind == WOS_OP_PROPAGATE && (o.method < WOS_ASM || o.method > WOS_FRAUNHOFER))
             return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
@@ -3149,7 +3211,7 @@ int wos_train(wos_ctx c, wos_field* f, const wos_op* ops, int nops, const wos_co
         if (o.kind == WOS_OP_LENS && (o.a[1] == 0 || !(o.a[0] > 0))) return fail(WOS_INVALID_ARG, "train: lens parameters");
         if (o.kind == WOS_OP_TILT && !(o.a[2] > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
     }
-    if (need_ey && !f->ey) return fail(WOS_INVALID_ARG, "train: a Jones op needs an Ey buffer");
+    if (need_ey && !f->ey) return fail(WOS_INVALID_ARG, "train: a Jones op or an Ey view needs an Ey buffer");
     std::lock_guard<std::mutex> lk(c->mu);
     TRY(set_device(c));
     const wos_context cc = cci ? *cci : default_context();
@@ -3161,7 +3223,8 @@ int wos_train(wos_ctx c, wos_field* f, const wos_op* ops, int nops, const wos_co
     int pol = f->polarized ? 1 : 0;
     TRY(ensure(c->stage, (size_t)np * 16 * (need_ey ? 2 : 1)));
     CK(cudaMemcpyAsync(c->stage.p, f->ex, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
-    if (pol) CK(cudaMemcpyAsync(stage_ey(c, f), f->ey, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
+    // Ey as the reference holds it (zeros for a fresh scalar field) whenever an op can read it
+    if (need_ey) CK(cudaMemcpyAsync(stage_ey(c, f), f->ey, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
     double2* ex = stage_ex(c);
     double2* ey = stage_ey(c, f);
     double dx = f->dx;
@@ -3254,6 +3317,11 @@ int wos_train(wos_ctx c, wos_field* f, const wos_op* ops, int nops, const wos_co
             CK(cudaMemsetAsync(acc, 0, sizeof(double) * np, c->st));
             CK(launch_accum_int(1, acc, c->stage.p, pol ? 2 : 1, np, 1.0, c->st));
             CK(cudaMemcpyAsync(o.out, acc, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
+        } break;
+        case WOS_OP_VIEW: {
+            TRY(ensure(c->accum, sizeof(double) * np));
+            TRY(plane_view_dev(c, 1, ex, ey, nullptr, pol, np, o.method, a[0], c->accum.p));
+            CK(cudaMemcpyAsync(o.out, c->accum.p, sizeof(float) * np, cudaMemcpyDeviceToHost, c->st));
         } break;
         }
     }

@@ -334,6 +334,73 @@ __global__ void k_grad_v(const C* b, const C* v, double* g, long long n) {
     g[idx] = (double)bv.y * vv.x - (double)bv.x * vv.y;
 }
 
+// ---- Plane views for the binary plane format (server/views.go:131-258,
+// server/server.go:582-634): float32 little-endian [ny][nx].
+// Per-CTA maxima of |c|^2 over a plane (peak of a component for the phase mask).
+template <typename C>
+__global__ void k_norm2_max(const C* a, long long n, double* partial) {
+    __shared__ double sm[32];
+    double m = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const C v = a[i];
+        const double p = da(dm((double)v.x, (double)v.x), dm((double)v.y, (double)v.y));
+        m = fmax(m, p);
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = fmax(r, sm[w]);
+        partial[blockIdx.x] = r;
+    }
+}
+__global__ void k_max_finish(const double* partial, int nb, double* out) {
+    __shared__ double sm[32];
+    double m = 0;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) m = fmax(m, partial[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double r = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = fmax(r, sm[w]);
+        *out = r;
+    }
+}
+// view: 0 total (|Ex|^2 [+ |Ey|^2 when polarized] [+ |Ez|^2 when given], as
+// Field.Intensity), 1 amplitude (sqrt of total), 2/3/4 |Ex|^2 / |Ey|^2 / |Ez|^2,
+// 5/6/7 phase of Ex / Ey / Ez (atan2, NaN where the component's |c|^2 is below
+// cut * its peak, or everywhere when the peak is 0).  Written as float32 bits;
+// NaN as 0x7fc00000 (the quiet NaN a float32 conversion of math.NaN() gives).
+template <typename C>
+__global__ void k_plane_view(const C* ex, const C* ey, const C* ez, int pol, long long n, int view,
+                             const double* peak, double cut, unsigned* out) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    auto n2 = [](C v) { return da(dm((double)v.x, (double)v.x), dm((double)v.y, (double)v.y)); };
+    double val;
+    bool nan = false;
+    if (view <= 1) {
+        val = n2(ex[i]);
+        if (pol) val = da(val, n2(ey[i]));
+        if (ez) val = da(val, n2(ez[i]));
+        if (view == 1) val = __dsqrt_rn(val);
+    } else if (view <= 4) {
+        val = n2(view == 2 ? ex[i] : (view == 3 ? ey[i] : ez[i]));
+    } else {
+        const C v = view == 5 ? ex[i] : (view == 6 ? ey[i] : ez[i]);
+        const double pk = *peak;
+        if (pk <= 0 || n2(v) < dm(cut, pk)) {
+            nan = true;
+            val = 0;
+        } else {
+            val = atan2((double)v.y, (double)v.x);
+        }
+    }
+    out[i] = nan ? 0x7fc00000u : __float_as_uint(__double2float_rn(val));
+}
+
 // ---------------------------------------------------------------- launchers
 static inline unsigned nblk(long long n, int b = 256) { return (unsigned)((n + b - 1) / b); }
 
@@ -436,6 +503,28 @@ cudaError_t launch_grad_v(int fp64, const void* b, const void* v, double* g, lon
         k_grad_v<double2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<const double2*>(b), reinterpret_cast<const double2*>(v), g, n);
     else
         k_grad_v<float2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<const float2*>(b), reinterpret_cast<const float2*>(v), g, n);
+    return cudaGetLastError();
+}
+
+int norm2_max_blocks(long long n) { return (int)std::min<long long>(nblk(n), 1024); }
+cudaError_t launch_norm2_max(int fp64, const void* a, long long n, double* partial, double* out, cudaStream_t st) {
+    const int nb = norm2_max_blocks(n);
+    if (fp64) k_norm2_max<double2><<<nb, 256, 0, st>>>(reinterpret_cast<const double2*>(a), n, partial);
+    else k_norm2_max<float2><<<nb, 256, 0, st>>>(reinterpret_cast<const float2*>(a), n, partial);
+    k_max_finish<<<1, 1024, 0, st>>>(partial, nb, out);
+    return cudaGetLastError();
+}
+cudaError_t launch_plane_view(int fp64, const void* ex, const void* ey, const void* ez, int pol, long long n, int view,
+                              const double* peak, double cut, void* out, cudaStream_t st) {
+    unsigned* o = reinterpret_cast<unsigned*>(out);
+    if (fp64)
+        k_plane_view<double2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<const double2*>(ex),
+                                                       reinterpret_cast<const double2*>(ey),
+                                                       reinterpret_cast<const double2*>(ez), pol, n, view, peak, cut, o);
+    else
+        k_plane_view<float2><<<nblk(n), 256, 0, st>>>(reinterpret_cast<const float2*>(ex),
+                                                      reinterpret_cast<const float2*>(ey),
+                                                      reinterpret_cast<const float2*>(ez), pol, n, view, peak, cut, o);
     return cudaGetLastError();
 }
 

@@ -198,6 +198,13 @@ cudaError_t launch_diffuser_apply(double2* ex, double2* ey, int pol, long long n
 cudaError_t launch_mask_phase(int fp64, void* u, const double* phi, long long n, int conj, cudaStream_t st);
 // g = Re(conj(b) * i * v)
 cudaError_t launch_grad_v(int fp64, const void* b, const void* v, double* g, long long n, cudaStream_t st);
+// Peak |c|^2 of a plane (partial: norm2_max_blocks(n) doubles; out: one double).
+int norm2_max_blocks(long long n);
+cudaError_t launch_norm2_max(int fp64, const void* a, long long n, double* partial, double* out, cudaStream_t st);
+// One view of a plane as float32 bits (see k_plane_view); ey / ez may be null
+// when not read; peak: device double (phase views).
+cudaError_t launch_plane_view(int fp64, const void* ex, const void* ey, const void* ez, int pol, long long n, int view,
+                              const double* peak, double cut, void* out, cudaStream_t st);
 // Vector angular spectrum step on the spectra of [Ex, Ey, Ez] planes (Ez written).
 cudaError_t launch_vectorial(int fp64, void* planes, int ny, int nx, double dx, const HArgs& h, cudaStream_t st);
 // 1-D angular spectrum step on a forward-transformed line (asmTF1D,

@@ -45,7 +45,7 @@ EXPORTS = [
     "wos_apply_jones", "wos_scale_amplitude", "wos_apply_tilt", "wos_apply_bandlimit", "wos_shift_field",
     "wos_apply_diffuser", "wos_propagate1d",
     "wos_bpm_stack_loss_grad", "wos_bpm_stack_loss_grad_dev", "wos_splitstep_adjoint_dev",
-    "wos_train", "wos_propagate_vectorial",
+    "wos_train", "wos_propagate_vectorial", "wos_plane_view", "wos_plane_view_dev",
 ]
 
 
@@ -84,7 +84,8 @@ class COp(C.Structure):
 
 
 OP_KINDS = {"propagate": 1, "lens": 2, "aperture": 3, "grating": 4, "phase_mask": 5, "diffuser": 6,
-            "jones": 7, "scale": 8, "tilt": 9, "shift": 10, "bandlimit": 11, "intensity": 12}
+            "jones": 7, "scale": 8, "tilt": 9, "shift": 10, "bandlimit": 11, "intensity": 12, "view": 13}
+VIEWS = {"total": 0, "amplitude": 1, "ex": 2, "ey": 3, "ez": 4, "phase_x": 5, "phase_y": 6, "phase_z": 7}
 
 
 class CField(C.Structure):
@@ -164,6 +165,8 @@ def lib():
             "wos_splitstep_adjoint_dev": ([vp, i, i, d, i, vp, d, vp, i, vp], i),
             "wos_train": ([vp, vp, vp, i, vp, d, d, vp], i),
             "wos_propagate_vectorial": ([vp, vp, vp, d, vp], i),
+            "wos_plane_view": ([vp, vp, vp, i, d, vp], i),
+            "wos_plane_view_dev": ([vp, i, i, i, vp, vp, i, d, vp], i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name, None)
@@ -561,6 +564,22 @@ class GPU:
                                              C.byref(cc) if cc is not None else None))
         return ez
 
+    def plane_view(self, f: Field, view: str, ez: Optional[np.ndarray] = None, mask_cut: float = 0.0) -> np.ndarray:
+        """Binary plane format view (server fmt=bin): float32 (ny, nx)."""
+        out = np.empty((f.ny, f.nx), dtype=np.float32)
+        ezp = None
+        if ez is not None:
+            ez = np.ascontiguousarray(ez, dtype=np.complex128)
+            ezp = _ptr(ez)
+        _check(lib().wos_plane_view(self.h, C.byref(f.c()), ezp, VIEWS[view], mask_cut, _ptr(out)))
+        return out
+
+    def plane_view_dev(self, ny: int, nx: int, ncomp: int, planes_ptr: int, ez_ptr: Optional[int], view: str,
+                       out_ptr: int, mask_cut: float = 0.0) -> None:
+        _check(lib().wos_plane_view_dev(self.h, ny, nx, ncomp, C.c_void_p(planes_ptr),
+                                        C.c_void_p(ez_ptr) if ez_ptr else None, VIEWS[view], mask_cut,
+                                        C.c_void_p(out_ptr)))
+
     # ---- element train on the device (trainer.runTrain, simulator.go:397-500)
     def train(self, f: Field, ops, ctx: Optional[Context] = None, bandlimit=None, diag: bool = False):
         """Run `ops` on the field with one upload and one download.  Each op is
@@ -593,6 +612,12 @@ class GPU:
                 out = args[0]
                 assert out.dtype == np.float64 and out.flags["C_CONTIGUOUS"] and out.shape == (f.ny, f.nx)
                 o.out = out.ctypes.data
+            elif name == "view":
+                o.method = VIEWS[args[0]]
+                out = args[1]
+                assert out.dtype == np.float32 and out.flags["C_CONTIGUOUS"] and out.shape == (f.ny, f.nx)
+                o.out = out.ctypes.data
+                o.a[0] = args[2] if len(args) > 2 else 0.0
             elif name in ("jones", "scale"):
                 for j, v in enumerate(args):
                     o.m[j] = _c128(v)
