@@ -286,6 +286,18 @@ WOS_API int wos_apply_diffuser(wos_ctx ctx, wos_field* f, double sigma, double c
  *      everything untouched (Propagate returns first). ---- */
 WOS_API int wos_propagate_vectorial(wos_ctx ctx, wos_field* f, wos_c128* ez, double z, const wos_context* c);
 
+/* ---- anisotropic media.  PropagateUniaxial (optics/birefringent.go:19-61):
+ *      optic axis along x, Ex takes the extraordinary transfer function and Ey
+ *      (when polarized) the ordinary one; evanescent components decay.
+ *      PropagateAnisotropic (optics/berreman.go:13-272): relative permittivity
+ *      eps (row-major 3x3 complex), Berreman 4x4 method per spectral component
+ *      (two forward eigenmodes, each with its own complex kz); Ex and Ey both
+ *      used whatever f->polarized says, as the reference uses f.Ey.  Both need
+ *      the Context's wavelength > 0. ---- */
+WOS_API int wos_propagate_uniaxial(wos_ctx ctx, wos_field* f, double z, double n_o, double n_e, const wos_context* c);
+WOS_API int wos_propagate_anisotropic(wos_ctx ctx, wos_field* f, double z, const wos_c128* eps,
+                                      const wos_context* c);
+
 /* ---- plane views in the binary plane format of the reference's server
  *      (fmt=bin, server/server.go:582-634, server/views.go:131-258): float32
  *      little-endian [ny][nx], row-major, no header, computed in FP64 on the

@@ -94,6 +94,10 @@ def lib():
         L.or_propagate.argtypes = [vp, d, i, vp]; L.or_propagate.restype = i
         L.or_propagate1d.argtypes = [vp, i, d, d, d, vp]
         L.or_propagate_vectorial.argtypes = [vp, vp, d, vp]
+        L.or_propagate_uniaxial.argtypes = [vp, d, d, d, vp]
+        L.or_propagate_uniaxial.restype = i
+        L.or_propagate_anisotropic.argtypes = [vp, d, vp, vp]
+        L.or_propagate_anisotropic.restype = i
         L.or_splitstep.argtypes = [vp, d, vp, i, vp]
         L.or_polychromatic.argtypes = [vp, d, vp, vp, i, i, vp, vp]; L.or_polychromatic.restype = i
         L.or_propagate3d.argtypes = [vp, vp, i, i, vp, vp]; L.or_propagate3d.restype = i
@@ -248,6 +252,20 @@ def propagate_vectorial(f: Field, z: float, ctx: Optional[Context]) -> np.ndarra
         lib().or_propagate_vectorial(C.byref(cf), _ptr(ez), z, C.byref(cc))
         ctx._from_c(cc)
     return ez
+
+
+def propagate_uniaxial(f: Field, z: float, no: float, ne: float, ctx: Context) -> None:
+    """PropagateUniaxial (birefringent.go:19-61), in place."""
+    cc = ctx._to_c()
+    if lib().or_propagate_uniaxial(C.byref(f._c()), z, no, ne, C.byref(cc)) != 0:
+        raise ValueError("uniaxial: n_o and n_e must be > 0")
+
+
+def propagate_anisotropic(f: Field, z: float, eps: np.ndarray, ctx: Context) -> None:
+    """PropagateAnisotropic (berreman.go:13-36), Ex and Ey in place."""
+    e = np.ascontiguousarray(eps, dtype=np.complex128).reshape(3, 3)
+    cc = ctx._to_c()
+    lib().or_propagate_anisotropic(C.byref(f._c()), z, _ptr(e), C.byref(cc))
 
 
 def spectral_radius(f: Field, frac: float) -> float:

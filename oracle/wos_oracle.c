@@ -1327,3 +1327,233 @@ int or_propagate_vectorial(or_field *f, oc128 *ez_out, double z, or_context *ctx
     free(ez);
     return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* Uniaxial and anisotropic media (birefringent.go:19-61, berreman.go)  */
+/* ------------------------------------------------------------------ */
+/* Go's complex128 division: Smith's algorithm (R. L. Smith, Algorithm 116,
+ * Commun. ACM 5(8), 1962), as the Go runtime divides. */
+static inline oc128 go_cdiv(oc128 n, oc128 m) {
+    double e, f;
+    if (fabs(m.re) >= fabs(m.im)) {
+        double ratio = m.im / m.re;
+        double denom = m.re + ratio * m.im;
+        e = (n.re + n.im * ratio) / denom;
+        f = (n.im - n.re * ratio) / denom;
+    } else {
+        double ratio = m.re / m.im;
+        double denom = m.im + ratio * m.re;
+        e = (n.re * ratio + n.im) / denom;
+        f = (n.im * ratio - n.re) / denom;
+    }
+    return cmk(e, f);
+}
+static inline oc128 cneg(oc128 a) { return cmk(-a.re, -a.im); }
+
+static void uniaxial_arr(oc128 *a, int ny, int nx, double dx, double k0, double z, double no, double ne, int extra) {
+    double az = fabs(z);
+    or_fft2d(a, ny, nx, 0);
+    for (int j = 0; j < ny; j++) {
+        double fy = freq_n(j, ny, dx);
+        for (int i = 0; i < nx; i++) {
+            double fx = freq_n(i, nx, dx);
+            double arg;
+            if (!extra) {
+                arg = k0 * k0 * no * no - (2 * M_PI * fx) * (2 * M_PI * fx) - (2 * M_PI * fy) * (2 * M_PI * fy);
+            } else {
+                double kx = 2 * M_PI * fx, ky = 2 * M_PI * fy;
+                arg = k0 * k0 * ne * ne - (ne * ne / (no * no)) * kx * kx - ky * ky;
+            }
+            oc128 h = arg < 0 ? cmk(exp(-az * sqrt(-arg)), 0) : cexpi(z * sqrt(arg));
+            size_t idx = (size_t)j * nx + i;
+            a[idx] = cmul(a[idx], h);
+        }
+    }
+    or_fft2d(a, ny, nx, 1);
+}
+
+int or_propagate_uniaxial(or_field *f, double z, double no, double ne, const or_context *ctx) {
+    if (no <= 0 || ne <= 0) return -1;
+    double k0 = 2 * M_PI / ctx->wavelength;
+    uniaxial_arr(f->ex, f->ny, f->nx, f->dx, k0, z, no, ne, 1);
+    if (f->polarized) uniaxial_arr(f->ey, f->ny, f->nx, f->dx, k0, z, no, ne, 0);
+    return 0;
+}
+
+typedef struct { oc128 m[4][4]; } m4;
+
+static m4 berreman_matrix(const oc128 *eps, double xi, double eta) {
+#define E(i, j) eps[(i) * 3 + (j)]
+    oc128 one = cmk(1, 0);
+    oc128 r = go_cdiv(one, E(2, 2));
+    oc128 x = cmk(xi, 0), y = cmk(eta, 0);
+    m4 D;
+    D.m[0][0] = cmul(cmul(cneg(x), r), E(2, 0));
+    D.m[0][1] = csub(one, cmul(cmul(x, x), r));
+    D.m[0][2] = cmul(cmul(cneg(x), r), E(2, 1));
+    D.m[0][3] = cmul(cmul(cneg(x), r), y);
+    D.m[1][0] = csub(csub(E(0, 0), cmul(y, y)), cmul(cmul(E(0, 2), r), E(2, 0)));
+    D.m[1][1] = cmul(cmul(cneg(E(0, 2)), r), x);
+    D.m[1][2] = csub(cadd(E(0, 1), cmul(y, x)), cmul(cmul(E(0, 2), r), E(2, 1)));
+    D.m[1][3] = cmul(cmul(cneg(E(0, 2)), r), y);
+    D.m[2][0] = cmul(cmul(cneg(y), r), E(2, 0));
+    D.m[2][1] = cmul(cmul(cneg(y), r), x);
+    D.m[2][2] = cmul(cmul(cneg(y), r), E(2, 1));
+    D.m[2][3] = csub(one, cmul(cmul(y, y), r));
+    D.m[3][0] = csub(cadd(E(1, 0), cmul(x, y)), cmul(cmul(E(1, 2), r), E(2, 0)));
+    D.m[3][1] = cmul(cmul(cneg(E(1, 2)), r), x);
+    D.m[3][2] = csub(csub(E(1, 1), cmul(x, x)), cmul(cmul(E(1, 2), r), E(2, 1)));
+    D.m[3][3] = cmul(cmul(cneg(E(1, 2)), r), y);
+#undef E
+    return D;
+}
+
+static oc128 trace4m(const m4 *A) {
+    return cadd(cadd(cadd(A->m[0][0], A->m[1][1]), A->m[2][2]), A->m[3][3]);
+}
+/* A (B + c I): the identity scaled by c is complex(0,0)*c off the diagonal */
+static m4 mul_shift(const m4 *A, const m4 *B, oc128 c) {
+    m4 S, out;
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) S.m[i][j] = cadd(B->m[i][j], cmul(cmk(i == j ? 1 : 0, 0), c));
+    for (int i = 0; i < 4; i++)
+        for (int j = 0; j < 4; j++) {
+            oc128 s = cmk(0, 0);
+            for (int k = 0; k < 4; k++) s = cadd(s, cmul(A->m[i][k], S.m[k][j]));
+            out.m[i][j] = s;
+        }
+    return out;
+}
+/* Faddeev-LeVerrier (berreman.go:130-144) */
+static void char_poly4(const m4 *A, oc128 *c) {
+    m4 B = *A;
+    c[3] = cneg(trace4m(&B));
+    B = mul_shift(A, &B, c[3]);
+    c[2] = go_cdiv(cneg(trace4m(&B)), cmk(2, 0));
+    B = mul_shift(A, &B, c[2]);
+    c[1] = go_cdiv(cneg(trace4m(&B)), cmk(3, 0));
+    B = mul_shift(A, &B, c[1]);
+    c[0] = go_cdiv(cneg(trace4m(&B)), cmk(4, 0));
+}
+static oc128 poly4(oc128 z, const oc128 *c) {
+    oc128 z2 = cmul(z, z);
+    oc128 t = cmul(cmul(z2, z), z);
+    t = cadd(t, cmul(cmul(cmul(c[3], z), z), z));
+    t = cadd(t, cmul(cmul(c[2], z), z));
+    t = cadd(t, cmul(c[1], z));
+    return cadd(t, c[0]);
+}
+/* Durand-Kerner (berreman.go:186-214) */
+static void roots4(const oc128 *c, oc128 *z) {
+    z[0] = cmk(0.4, 0.9); z[1] = cmk(0.4, -0.9); z[2] = cmk(-0.4, 0.9); z[3] = cmk(-0.4, -0.9);
+    for (int iter = 0; iter < 300; iter++) {
+        double maxd = 0;
+        for (int i = 0; i < 4; i++) {
+            oc128 num = poly4(z[i], c);
+            oc128 den = cmk(1, 0);
+            for (int j = 0; j < 4; j++)
+                if (j != i) den = cmul(den, csub(z[i], z[j]));
+            oc128 dz = go_cdiv(num, den);
+            z[i] = csub(z[i], dz);
+            double d = go_hypot(dz.re, dz.im);
+            if (d > maxd) maxd = d;
+        }
+        if (maxd < 1e-14) break;
+    }
+}
+static int forward_mode(oc128 q) {
+    if (q.im > 1e-12) return 1;
+    if (q.im < -1e-12) return 0;
+    return q.re > 0;
+}
+static oc128 det3(oc128 m[3][3]) {
+    oc128 a = cmul(m[0][0], csub(cmul(m[1][1], m[2][2]), cmul(m[1][2], m[2][1])));
+    oc128 b = cmul(m[0][1], csub(cmul(m[1][0], m[2][2]), cmul(m[1][2], m[2][0])));
+    oc128 c = cmul(m[0][2], csub(cmul(m[1][0], m[2][1]), cmul(m[1][1], m[2][0])));
+    return cadd(csub(a, b), c);
+}
+/* largest-norm column of adj(A - qI) (berreman.go:228-272) */
+static void null_vector4(const m4 *A, oc128 q, oc128 *best) {
+    m4 M = *A;
+    for (int i = 0; i < 4; i++) M.m[i][i] = csub(M.m[i][i], q);
+    double bestn = -1;
+    for (int col = 0; col < 4; col++) {
+        oc128 v[4];
+        for (int row = 0; row < 4; row++) {
+            oc128 m[3][3];
+            int ri = 0;
+            for (int r = 0; r < 4; r++) {
+                if (r == row) continue;
+                int ci = 0;
+                for (int cc = 0; cc < 4; cc++) {
+                    if (cc == col) continue;
+                    m[ri][ci++] = M.m[r][cc];
+                }
+                ri++;
+            }
+            oc128 cof = det3(m);
+            if ((row + col) % 2 == 1) cof = cneg(cof);
+            v[row] = cof;
+        }
+        double nn = 0;
+        for (int t = 0; t < 4; t++) nn += v[t].re * v[t].re + v[t].im * v[t].im;
+        if (nn > bestn) {
+            bestn = nn;
+            for (int t = 0; t < 4; t++) best[t] = v[t];
+        }
+    }
+}
+/* anisoMode (berreman.go:41-92) */
+static void aniso_mode(const oc128 *eps, double xi, double eta, double k0, double z, oc128 *ex, oc128 *ey) {
+    m4 D = berreman_matrix(eps, xi, eta);
+    oc128 c[4], roots[4], qs[2], vs[2][4];
+    char_poly4(&D, c);
+    roots4(c, roots);
+    int cnt = 0, used[4] = {0, 0, 0, 0};
+    for (int i = 0; i < 4; i++)
+        if (forward_mode(roots[i]) && cnt < 2) {
+            qs[cnt] = roots[i];
+            null_vector4(&D, roots[i], vs[cnt]);
+            used[i] = 1;
+            cnt++;
+        }
+    while (cnt < 2) {
+        double best = -1e300;
+        int bi = -1;
+        for (int i = 0; i < 4; i++)
+            if (!used[i] && roots[i].re > best) { best = roots[i].re; bi = i; }
+        if (bi < 0) break;
+        qs[cnt] = roots[bi];
+        null_vector4(&D, roots[bi], vs[cnt]);
+        used[bi] = 1;
+        cnt++;
+    }
+    oc128 a = vs[0][0], b = vs[1][0], cc = vs[0][2], d = vs[1][2];
+    oc128 det = csub(cmul(a, d), cmul(b, cc));
+    oc128 m1 = go_cdiv(csub(cmul(d, *ex), cmul(b, *ey)), det);
+    oc128 m2 = go_cdiv(cadd(cmul(cneg(cc), *ex), cmul(a, *ey)), det);
+    oc128 p0 = cmul(cexpi(k0 * qs[0].re * z), cmk(exp(-k0 * qs[0].im * z), 0));
+    oc128 p1 = cmul(cexpi(k0 * qs[1].re * z), cmk(exp(-k0 * qs[1].im * z), 0));
+    *ex = cadd(cmul(cmul(m1, p0), a), cmul(cmul(m2, p1), b));
+    *ey = cadd(cmul(cmul(m1, p0), cc), cmul(cmul(m2, p1), d));
+}
+
+int or_propagate_anisotropic(or_field *f, double z, const oc128 *eps, const or_context *ctx) {
+    int ny = f->ny, nx = f->nx;
+    double k0 = 2 * M_PI / ctx->wavelength;
+    or_fft2d(f->ex, ny, nx, 0);
+    or_fft2d(f->ey, ny, nx, 0);
+    for (int j = 0; j < ny; j++) {
+        double fy = freq_n(j, ny, f->dx);
+        double ky = 2 * M_PI * fy;
+        for (int i = 0; i < nx; i++) {
+            double fx = freq_n(i, nx, f->dx);
+            double kx = 2 * M_PI * fx;
+            size_t idx = (size_t)j * nx + i;
+            aniso_mode(eps, kx / k0, ky / k0, k0, z, &f->ex[idx], &f->ey[idx]);
+        }
+    }
+    or_fft2d(f->ex, ny, nx, 1);
+    or_fft2d(f->ey, ny, nx, 1);
+    return 0;
+}

@@ -105,6 +105,10 @@ int or_propagate1d(oc128 *a, int n, double dx, double z, double wl, or_context *
  * f->polarized, as the reference uses f.Ey) propagate in place, ez_out
  * receives the reconstructed longitudinal component. */
 int or_propagate_vectorial(or_field *f, oc128 *ez_out, double z, or_context *ctx);
+/* PropagateUniaxial (birefringent.go:19-61): Ex extraordinary, Ey ordinary (if polarized). */
+int or_propagate_uniaxial(or_field *f, double z, double no, double ne, const or_context *ctx);
+/* PropagateAnisotropic (berreman.go:13-36): eps row-major 3x3; Ex and Ey both used. */
+int or_propagate_anisotropic(or_field *f, double z, const oc128 *eps, const or_context *ctx);
 /* asmTF (propagate.go:159-181) evaluated at (fx, fy) with the policy of ctx */
 oc128 or_asm_tf(double wl, double z, int zero_ev, int reg, double alpha, double limit,
                 double fx, double fy);

@@ -641,3 +641,34 @@ def test_oracle_vectorial_field_is_divergence_free():
     div = 2 * np.pi * FX * np.fft.fft2(f.ex) + 2 * np.pi * FY * np.fft.fft2(f.ey) + kz * np.fft.fft2(ez)
     scale = np.abs(2 * np.pi / wl * np.fft.fft2(f.ex)).max()
     assert np.abs(div[prop]).max() <= 1e-10 * scale
+
+
+def test_oracle_berreman_reduces_to_uniaxial_in_the_xz_plane():
+    """For eps = diag(ne^2, no^2, no^2) and a field constant along y (ky = 0,
+    where the uniaxial transfer functions are exact) the Berreman 4x4
+    propagation equals PropagateUniaxial (berreman.go:9-12)."""
+    n, dx, wl, z, no, ne = 64, 1e-6, 1e-6, 20e-6, 1.5, 1.7
+    rng = np.random.default_rng(5)
+    rowx = rng.normal(size=n) + 1j * rng.normal(size=n)
+    rowy = rng.normal(size=n) + 1j * rng.normal(size=n)
+    ex = np.tile(rowx, (n, 1))
+    ey = np.tile(rowy, (n, 1))
+    fb = O.Field(ex.copy(), dx, ey.copy())
+    O.propagate_anisotropic(fb, z, np.diag([ne ** 2, no ** 2, no ** 2]).astype(complex), O.Context(wavelength=wl))
+    fu = O.Field(ex.copy(), dx, ey.copy())
+    O.propagate_uniaxial(fu, z, no, ne, O.Context(wavelength=wl))
+    assert np.linalg.norm(fb.ex - fu.ex) <= 1e-9 * np.linalg.norm(fu.ex)
+    assert np.linalg.norm(fb.ey - fu.ey) <= 1e-9 * np.linalg.norm(fu.ey)
+
+
+def test_oracle_uniaxial_isotropic_is_asm_in_the_medium():
+    """n_o = n_e = n: both components take the ASM of a medium of index n,
+    i.e. the vacuum ASM at wavelength wl / n."""
+    n, dx, wl, z, nn = 64, 1e-6, 1e-6, 30e-6, 1.6
+    rng = np.random.default_rng(6)
+    ex = rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))
+    fu = O.Field(ex.copy(), dx)
+    O.propagate_uniaxial(fu, z, nn, nn, O.Context(wavelength=wl))
+    fa = O.Field(ex.copy(), dx)
+    O.propagate(fa, z, "asm", O.Context(wavelength=wl / nn))
+    assert np.linalg.norm(fu.ex - fa.ex) <= 1e-10 * np.linalg.norm(fa.ex)

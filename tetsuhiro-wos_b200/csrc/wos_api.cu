@@ -2908,7 +2908,7 @@ double2 d2(wos_c128 v) { return make_double2(v.re, v.im); }
 // FFT -> multiply by a filter H(fx, fy) -> inverse FFT of `ncomp` complex128
 // device planes in place, on the three-sweep propagator (context precision).
 int spectral_filter(wos_ctx c, int ny, int nx, double dx, int ncomp, void* planes, int kind, double p0,
-                    double p1) {
+                    double p1, double k = 0, double z = 0) {
     Prop p{ny, nx, dx, ncomp, planes, 1, planes, 1, 0.0, 0, default_context(), nullptr};
     Sweep3 s;
     s.h.kind = kind;
@@ -2920,6 +2920,8 @@ int spectral_filter(wos_ctx c, int ny, int nx, double dx, int ncomp, void* plane
     s.h.c_re = 1.0;
     s.h.p0 = p0;
     s.h.p1 = p1;
+    s.h.k = k;
+    s.h.z = z;
     return run_sweep3(c, p, s);
 }
 }  // namespace
@@ -2982,6 +2984,50 @@ int wos_shift_field(wos_ctx c, wos_field* f, double du, double dv) {
     if (du == 0 && dv == 0) return WOS_OK;
     TRY(element_begin(c, f));
     TRY(spectral_filter(c, f->ny, f->nx, f->dx, f->polarized ? 2 : 1, c->stage.p, H_SHIFT, du, dv));
+    return stage_out(c, f, f->polarized ? 2 : 1);
+}
+
+int wos_propagate_anisotropic(wos_ctx c, wos_field* f, double z, const wos_c128* eps, const wos_context* cci) {
+    if (!c || !f || !f->ex || !f->ey || !eps || f->ny < 2 || f->nx < 2 || !(f->dx > 0))
+        return fail(WOS_INVALID_ARG, "anisotropic: ex, ey, eps and a valid geometry are required");
+    const wos_context cc = cci ? *cci : default_context();
+    if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const int ny = f->ny, nx = f->nx;
+    const long long np = (long long)ny * nx;
+    TRY(ensure(c->stage, (size_t)np * 16 * 2));
+    double2* st = reinterpret_cast<double2*>(c->stage.p);
+    CK(cudaMemcpyAsync(st, f->ex, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(st + np, f->ey, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
+    void* work = st;
+    if (!c->fp64) {
+        TRY(ensure(c->scratch, (size_t)np * 8 * 2));
+        work = c->scratch.p;
+        CK(launch_convert(0, st, work, 2 * np, c->st));
+    }
+    Eps9 e;
+    for (int k = 0; k < 9; k++) e.v[k] = make_double2(eps[k].re, eps[k].im);
+    TRY(fft2d_impl(c, c->fp64, ny, nx, 2, work, 0));
+    CK(launch_aniso(c->fp64, work, ny, nx, f->dx, 2 * M_PI / cc.wavelength, z, e, c->st));
+    TRY(fft2d_impl(c, c->fp64, ny, nx, 2, work, 1));
+    if (!c->fp64) CK(launch_convert(1, work, st, 2 * np, c->st));
+    CK(cudaMemcpyAsync(f->ex, st, (size_t)np * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(f->ey, st + np, (size_t)np * 16, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+int wos_propagate_uniaxial(wos_ctx c, wos_field* f, double z, double no, double ne, const wos_context* cci) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    if (!(no > 0) || !(ne > 0)) return fail(WOS_INVALID_ARG, "uniaxial: n_o and n_e must be > 0");
+    const wos_context cc = cci ? *cci : default_context();
+    if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(element_begin(c, f));
+    const double k0 = 2 * M_PI / cc.wavelength;
+    TRY(spectral_filter(c, f->ny, f->nx, f->dx, 1, stage_ex(c), H_UNIAX_E, no, ne, k0, z));
+    if (f->polarized) TRY(spectral_filter(c, f->ny, f->nx, f->dx, 1, stage_ey(c, f), H_UNIAX_O, no, ne, k0, z));
     return stage_out(c, f, f->polarized ? 2 : 1);
 }
 

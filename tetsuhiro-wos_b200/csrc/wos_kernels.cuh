@@ -20,6 +20,8 @@ enum HKind {
     H_GAUSS = 5,       // exp(p0 (fx^2+fy^2)): diffuser correlation filter (elements.go:744-754)
     H_BANDLIMIT = 6,   // exp(-((|f|-p0)/p1)^2) for |f| > p0: ApplyBandlimit (field.go:264-294)
     H_SHIFT = 7,       // exp(-2 pi i (fx p0 + fy p1)): ShiftField (field.go:199-228)
+    H_UNIAX_O = 8,     // ordinary wave of a uniaxial crystal, n_o = p0 (birefringent.go:38-44)
+    H_UNIAX_E = 9,     // extraordinary wave, n_o = p0, n_e = p1 (birefringent.go:45-53)
 };
 
 struct HArgs {
@@ -205,6 +207,13 @@ cudaError_t launch_norm2_max(int fp64, const void* a, long long n, double* parti
 // when not read; peak: device double (phase views).
 cudaError_t launch_plane_view(int fp64, const void* ex, const void* ey, const void* ez, int pol, long long n, int view,
                               const double* peak, double cut, void* out, cudaStream_t st);
+// Relative permittivity tensor, row-major 3x3 (complex).
+struct Eps9 {
+    double2 v[9];
+};
+// Berreman 4x4 propagation on the spectra of [Ex, Ey] planes (wos_aniso.cu).
+cudaError_t launch_aniso(int fp64, void* planes, int ny, int nx, double dx, double k0, double z, const Eps9& e,
+                         cudaStream_t st);
 // Vector angular spectrum step on the spectra of [Ex, Ey, Ez] planes (Ez written).
 cudaError_t launch_vectorial(int fp64, void* planes, int ny, int nx, double dx, const HArgs& h, cudaStream_t st);
 // 1-D angular spectrum step on a forward-transformed line (asmTF1D,

@@ -173,6 +173,22 @@ __device__ __forceinline__ C eval_h(const HArgs& h, double wl, double z, int col
                                  : (-2 * M_PI) * (fx * h.p0 + fy * h.p1);
         r = cexpi<C>(a);
     } break;
+    case H_UNIAX_O:
+    case H_UNIAX_E: {
+        // arg = k0^2 n^2 - (n_e/n_o)^2 kx^2 - ky^2 (extraordinary) or
+        // k0^2 n_o^2 - kx^2 - ky^2 (ordinary), in the reference's order;
+        // evanescent components decay as exp(-|z| sqrt(-arg))
+        const double kx = dmul(2 * M_PI, fx), ky = dmul(2 * M_PI, fy);
+        double arg;
+        if (h.kind == H_UNIAX_O) {
+            arg = dsub(dsub(dmul(dmul(dmul(h.k, h.k), h.p0), h.p0), dmul(kx, kx)), dmul(ky, ky));
+        } else {
+            const double rr = ddiv(dmul(h.p1, h.p1), dmul(h.p0, h.p0));
+            arg = dsub(dsub(dmul(dmul(dmul(h.k, h.k), h.p1), h.p1), dmul(dmul(rr, kx), kx)), dmul(ky, ky));
+        }
+        if (arg < 0) r = mkc<C>((T)exp(-dmul(fabs(z), __dsqrt_rn(-arg))), 0);
+        else r = cexpi<C>(dmul(z, __dsqrt_rn(arg)));
+    } break;
     default: r = mkc<C>(1, 0); break;
     }
     if (h.conj) r.y = -r.y;

@@ -46,6 +46,7 @@ EXPORTS = [
     "wos_apply_diffuser", "wos_propagate1d",
     "wos_bpm_stack_loss_grad", "wos_bpm_stack_loss_grad_dev", "wos_splitstep_adjoint_dev",
     "wos_train", "wos_propagate_vectorial", "wos_plane_view", "wos_plane_view_dev",
+    "wos_propagate_uniaxial", "wos_propagate_anisotropic",
 ]
 
 
@@ -167,6 +168,8 @@ def lib():
             "wos_propagate_vectorial": ([vp, vp, vp, d, vp], i),
             "wos_plane_view": ([vp, vp, vp, i, d, vp], i),
             "wos_plane_view_dev": ([vp, i, i, i, vp, vp, i, d, vp], i),
+            "wos_propagate_uniaxial": ([vp, vp, d, d, d, vp], i),
+            "wos_propagate_anisotropic": ([vp, vp, d, vp, vp], i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name, None)
@@ -563,6 +566,17 @@ class GPU:
         _check(lib().wos_propagate_vectorial(self.h, C.byref(f.c()), _ptr(ez), z,
                                              C.byref(cc) if cc is not None else None))
         return ez
+
+    def propagate_uniaxial(self, f: Field, z: float, no: float, ne: float, ctx: Context) -> None:
+        """PropagateUniaxial (birefringent.go:19-61), in place."""
+        cc = ctx.c()
+        _check(lib().wos_propagate_uniaxial(self.h, C.byref(f.c()), z, no, ne, C.byref(cc)))
+
+    def propagate_anisotropic(self, f: Field, z: float, eps: np.ndarray, ctx: Context) -> None:
+        """PropagateAnisotropic (berreman.go:13-36), Ex and Ey in place."""
+        e = np.ascontiguousarray(eps, dtype=np.complex128).reshape(3, 3)
+        cc = ctx.c()
+        _check(lib().wos_propagate_anisotropic(self.h, C.byref(f.c()), z, _ptr(e), C.byref(cc)))
 
     def plane_view(self, f: Field, view: str, ez: Optional[np.ndarray] = None, mask_cut: float = 0.0) -> np.ndarray:
         """Binary plane format view (server fmt=bin): float32 (ny, nx)."""
