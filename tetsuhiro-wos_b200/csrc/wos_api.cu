@@ -111,6 +111,8 @@ struct wos_ctx_s {
     bool no_fast = false;               // force the general sweeps (tests compare both)
     int sweep_mode = 1;                 // wos_ctx_set_fast_path: 1, 2 or 3 (0 is no_fast)
     int col_pair = 0;                   // column tiles split over two-CTA clusters where supported
+    int tiled = 0;                      // three-sweep ASM through the tiled intermediate (FastRows::out_tiled)
+    int tiled_lines = 0;                // rows per row-sweep CTA on the tiled path (0: default)
     unsigned* err_dev = nullptr;        // error word of the pipelined kernels (device)
     unsigned* err_host = nullptr;       // pinned mirror, read where the host synchronises
     // streams for independent fields of a batch (wos_propagate_batch_dev),
@@ -119,6 +121,8 @@ struct wos_ctx_s {
     cudaStream_t side[kMaxAux] = {};
     cudaEvent_t fork_ev = nullptr, join_ev[kMaxAux] = {};
     int naux = 0;
+    DevBuf tsc[kMaxAux + 1];            // tiled intermediates: [0] context stream, [1 + k] side stream k
+    int cur_slot = 0;                   // which of them the current stream uses
     // copy pipeline of wos_propagate_batch: host-to-device and device-to-host
     // streams, staging slots and their events
     static constexpr int kSlots = 3;
@@ -611,7 +615,7 @@ int fast_tw(wos_ctx c, Axis* a, int E, const void** out) {
 // register-bound CTAs beat three pipelined ones), FP64 rows and all columns
 // pipelined where the tile fits two stages.
 cudaError_t sweep_rows(wos_ctx c, int L, int E, bool inv, const FastRows& a, int* nb) {
-    if (c->sweep_mode == 3 || (c->sweep_mode == 1 && c->fp64)) {
+    if ((c->sweep_mode == 3 || (c->sweep_mode == 1 && c->fp64)) && !a.in_tiled && !a.out_tiled) {
         FastRows b = a;
         b.err = c->err_dev;
         const cudaError_t e = pipe_rows(c->fp64, L, E, inv, b, c->st, nb);
@@ -636,7 +640,7 @@ bool pair_tables(wos_ctx c, int L, int E, const void** twh, const void** twp) {
     return true;
 }
 bool pair_eligible(wos_ctx c, int L, int E, const FastCols& a) {
-    return c->col_pair && !a.hist && fast_cols_pair_case(c->fp64, L, E, fast_col_width(c->fp64, L, E, a.W));
+    return c->col_pair && !a.hist && !a.tiled && fast_cols_pair_case(c->fp64, L, E, fast_col_width(c->fp64, L, E, a.W));
 }
 
 cudaError_t sweep_cols(wos_ctx c, int L, int E, const FastCols& a, int* nb) {
@@ -647,7 +651,7 @@ cudaError_t sweep_cols(wos_ctx c, int L, int E, const FastCols& a, int* nb) {
             if (e != cudaErrorNotSupported) return e;
         }
     }
-    if (c->sweep_mode != 2) {
+    if (c->sweep_mode != 2 && !a.tiled) {
         FastCols b = a;
         b.err = c->err_dev;
         const cudaError_t e = pipe_cols(c->fp64, L, E, b, c->st, nb);
@@ -669,12 +673,21 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     TRY(fast_tw(c, ax, t.rowE, &twx));
     TRY(fast_tw(c, ay, t.colE, &twy));
     const long long np = (long long)p.ny * p.nx;
+    // tiled intermediate (FP32): the column sweep reads contiguous tiles of
+    // kTileW columns; the intermediate is then a buffer of its own (the last
+    // sweep changes the layout, so it cannot run in place in the output)
+    const bool tiled = c->tiled && !c->fp64 && p.nx % kTileW == 0 && !s.hist &&
+                       fast_col_width(c->fp64, p.ny, t.colE, kTileW) == kTileW;
     void* S;
-    if (!p.out_c128) {
-        S = p.out;
-    } else {
+    if (p.out_c128) {
         TRY(ensure(c->scratch, (size_t)np * p.ncomp * c->csz()));
         S = c->scratch.p;
+    } else if (tiled) {
+        DevBuf& b = c->tsc[std::max(0, std::min(c->cur_slot, wos_ctx_s::kMaxAux))];
+        TRY(ensure(b, (size_t)np * p.ncomp * c->csz()));
+        S = b.p;
+    } else {
+        S = p.out;
     }
     const size_t nbr = fast_row_blocks(p.nx, t.rowE, p.ny, p.ncomp);
     const size_t nbc = fast_col_blocks(c->fp64, p.ny, t.colE, t.colW, p.nx, p.ncomp);
@@ -694,13 +707,17 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     r.red = s.red_pin ? red_region(c, 0) + RS_P : nullptr;
     r.red_stride = RS_COUNT;
     r.batch = p.ncomp;
+    r.out_tiled = tiled;
+    r.tile_len = p.ny;
+    r.lines = tiled ? c->tiled_lines : 0;
     CK(timed_launch(c, 0, [&] { return sweep_rows(c, p.nx, t.rowE, false, r, &nb); }));
     if (s.red_pin) CK(launch_reduce_finish(red_region(c, 0), nb, 1, RS_P, 1, redout_region(c, 0), c->st));
     FastCols k{};
     k.ncols = p.nx;
-    k.W = t.colW;
+    k.W = tiled ? kTileW : t.colW;
     k.data = S;
-    k.ld = p.nx;
+    k.ld = tiled ? kTileW : p.nx;
+    k.tiled = tiled;
     k.bstride = np;
     k.tw = twy;
     k.batch = p.ncomp;
@@ -739,6 +756,9 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     q.red = s.red_pout ? red_region(c, 2) + RS_P : nullptr;
     q.red_stride = RS_COUNT;
     q.batch = p.ncomp;
+    q.in_tiled = tiled;
+    q.tile_len = p.ny;
+    q.lines = tiled ? c->tiled_lines : 0;
     CK(timed_launch(c, 1, [&] { return sweep_rows(c, p.nx, t.rowE, true, q, &nb); }));
     if (s.red_pout) CK(launch_reduce_finish(red_region(c, 2), nb, 1, RS_P, 1, redout_region(c, 2), c->st));
     s.fast = true;
@@ -1313,6 +1333,8 @@ int wos_ctx_create(int device, int precision, wos_ctx* out) {
     }
     *c->err_host = 0;
     c->col_pair = env_int("WOS_COLPAIR", 0);
+    c->tiled = env_int("WOS_TILED", 1);
+    c->tiled_lines = env_int("WOS_TILED_LINES", 0);
     *out = c;
     return WOS_OK;
 }
@@ -1337,6 +1359,8 @@ int wos_ctx_destroy(wos_ctx c) {
                           &c->maps, &c->params, &c->vol, &c->accum, &c->aux};
         for (DevBuf* b : bufs)
             if (b->p) cudaFree(b->p);
+        for (DevBuf& b : c->tsc)
+            if (b.p) cudaFree(b.p);
         if (c->hred) cudaFreeHost(c->hred);
         if (c->err_dev) cudaFree(c->err_dev);
         if (c->err_host) cudaFreeHost(c->err_host);
@@ -1567,10 +1591,12 @@ int wos_propagate_batch_dev(wos_ctx c, int nfields, int ny, int nx, double dx, i
     int rc = WOS_OK;
     for (int i = 0; i < nfields && rc == WOS_OK; i++) {
         c->st = c->side[i % nstreams];
+        c->cur_slot = 1 + i % nstreams;
         Prop p{ny, nx, dx, ncomp, in[i], 0, out[i], 0, z, method, cc, nullptr};
         rc = run_propagate(c, p);
     }
     c->st = home;
+    c->cur_slot = 0;
     for (int k = 0; k < nstreams; k++) {
         CK(cudaEventRecord(c->join_ev[k], c->side[k]));
         CK(cudaStreamWaitEvent(c->st, c->join_ev[k], 0));

@@ -50,6 +50,15 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
                 const double2 d = in[fpos<R1, E, L>(s, 0)];
                 v[s] = mkc<C>((Real)d.x, (Real)d.y);
             }
+        } else if (INV && a.in_tiled) {
+            // x = tt + s*T (R1 == E): tile (tt / kTileW) + s * (T / kTileW), lane tt % kTileW
+            static_assert(!INV || R1 == E, "tiled loads follow the natural mapping of radix E");
+            const long long tstride = a.tile_len * kTileW;
+            const C* in = reinterpret_cast<const C*>(a.in) + (long long)blockIdx.y * a.in_bstride +
+                          (long long)r * kTileW + (long long)(tt / kTileW) * tstride + (tt % kTileW);
+            const long long step = (long long)(T / kTileW) * tstride;
+#pragma unroll
+            for (int s = 0; s < E; s++) v[s] = __ldcs(in + s * step);
         } else {
             const C* in = reinterpret_cast<const C*>(a.in) + ib + tt;
 #pragma unroll
@@ -81,6 +90,14 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
             double2* out = reinterpret_cast<double2*>(a.out) + ob + tt;
 #pragma unroll
             for (int s = 0; s < E; s++) out[fpos<RO, E, L>(s, 0)] = make_double2(v[s].x, v[s].y);
+        } else if (!INV && a.out_tiled) {
+            static_assert(INV || RO == E, "tiled stores follow the natural mapping of radix E");
+            const long long tstride = a.tile_len * kTileW;
+            C* out = reinterpret_cast<C*>(a.out) + (long long)blockIdx.y * a.out_bstride + (long long)r * kTileW +
+                     (long long)(tt / kTileW) * tstride + (tt % kTileW);
+            const long long step = (long long)(T / kTileW) * tstride;
+#pragma unroll
+            for (int s = 0; s < E; s++) out[s * step] = v[s];
         } else {
             C* out = reinterpret_cast<C*>(a.out) + ob + tt;
 #pragma unroll
@@ -321,8 +338,10 @@ __global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, 
     const int col = blockIdx.x * W + w;
     const bool act = col < a.ncols;
     const C* twp = reinterpret_cast<const C*>(a.tw);
-    C* base = reinterpret_cast<C*>(a.data) + (long long)blockIdx.y * a.bstride + col;
-    const C* sbase = a.src ? reinterpret_cast<const C*>(a.src) + (long long)blockIdx.y * a.src_bstride + col : base;
+    // strided columns, or one contiguous block per tile in the tiled layout (ld == W)
+    const long long coff = a.tiled ? (long long)blockIdx.x * L * W + w : (long long)col;
+    C* base = reinterpret_cast<C*>(a.data) + (long long)blockIdx.y * a.bstride + coff;
+    const C* sbase = a.src ? reinterpret_cast<const C*>(a.src) + (long long)blockIdx.y * a.src_bstride + coff : base;
     __shared__ double hsm[97];
     if (a.hist)
         for (int k = threadIdx.x; k < 97; k += blockDim.x) hsm[k] = 0;
@@ -572,7 +591,8 @@ template <typename Real, int L, int E, bool INV>
 static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
     int lines = 1;
-    while (lines * 2 * T <= 256 && lines * 2 <= a.rows) lines *= 2;
+    const int maxt = a.lines > 0 ? a.lines * T : 256;  // rows per CTA: 256 threads unless asked
+    while (lines * 2 * T <= maxt && lines * 2 <= a.rows && lines * 2 * T <= FMaxT<Real, E>::v) lines *= 2;
     while (lines * T < 32) lines *= 2;
     const size_t smem = (size_t)frow_stride(L, E) * lines * sizeof(typename CT<Real>::t);
     if (smem > kSmemNoOptIn) {

@@ -26,7 +26,16 @@ struct FastRows {
     const double* bpm_border; // exp(-k dz strength ((px - d)/px)^order) for edge distance d < px, or null
     int bpm_border_px;
     int bpm_nx;               // grid width (edge distance)
+    // tiled intermediate of the three-sweep ASM: columns grouped in tiles of
+    // kTileW, element (r, x) of a batch item at (x / kTileW) * tile_len *
+    // kTileW + r * kTileW + x % kTileW, so that a column tile is one
+    // contiguous block; out_tiled on the forward sweep's store, in_tiled on
+    // the inverse sweep's load (native complex type only)
+    int out_tiled, in_tiled;
+    long long tile_len;       // rows of the field (the column length)
+    int lines;                // rows per CTA of k_rows_fast (0: as many as fit 256 threads)
 };
+constexpr int kTileW = 4;
 
 struct FastCols {
     int ncols;            // columns = the frequency grid length along x
@@ -58,6 +67,7 @@ struct FastCols {
     const double* batch_wl;
     const double* batch_z;
     double z;
+    int tiled;            // data (and src) in the tiled layout of FastRows (W == kTileW, ld == kTileW)
     // split tiles (FP32, L = 2048, W = 8): a tile is held by a two-CTA cluster,
     // half of every column per CTA; per-pass twiddles of length L/2 and the
     // table W_L^n for n < L/2 (both null: one CTA per tile)
