@@ -112,7 +112,6 @@ struct wos_ctx_s {
     int sweep_mode = 1;                 // wos_ctx_set_fast_path: 1, 2 or 3 (0 is no_fast)
     int col_pair = 0;                   // column tiles split over two-CTA clusters where supported
     int tiled = 0;                      // three-sweep ASM through the tiled intermediate (FastRows::out_tiled)
-    int tiled_lines = 0;                // rows per row-sweep CTA on the tiled path (0: default)
     unsigned* err_dev = nullptr;        // error word of the pipelined kernels (device)
     unsigned* err_host = nullptr;       // pinned mirror, read where the host synchronises
     // streams for independent fields of a batch (wos_propagate_batch_dev),
@@ -709,7 +708,6 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     r.batch = p.ncomp;
     r.out_tiled = tiled;
     r.tile_len = p.ny;
-    r.lines = tiled ? c->tiled_lines : 0;
     CK(timed_launch(c, 0, [&] { return sweep_rows(c, p.nx, t.rowE, false, r, &nb); }));
     if (s.red_pin) CK(launch_reduce_finish(red_region(c, 0), nb, 1, RS_P, 1, redout_region(c, 0), c->st));
     FastCols k{};
@@ -758,7 +756,6 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     q.batch = p.ncomp;
     q.in_tiled = tiled;
     q.tile_len = p.ny;
-    q.lines = tiled ? c->tiled_lines : 0;
     CK(timed_launch(c, 1, [&] { return sweep_rows(c, p.nx, t.rowE, true, q, &nb); }));
     if (s.red_pout) CK(launch_reduce_finish(red_region(c, 2), nb, 1, RS_P, 1, redout_region(c, 2), c->st));
     s.fast = true;
@@ -1334,7 +1331,6 @@ int wos_ctx_create(int device, int precision, wos_ctx* out) {
     *c->err_host = 0;
     c->col_pair = env_int("WOS_COLPAIR", 0);
     c->tiled = env_int("WOS_TILED", 1);
-    c->tiled_lines = env_int("WOS_TILED_LINES", 0);
     *out = c;
     return WOS_OK;
 }

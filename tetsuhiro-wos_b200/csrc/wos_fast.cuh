@@ -33,7 +33,6 @@ struct FastRows {
     // the inverse sweep's load (native complex type only)
     int out_tiled, in_tiled;
     long long tile_len;       // rows of the field (the column length)
-    int lines;                // rows per CTA of k_rows_fast (0: as many as fit 256 threads)
 };
 constexpr int kTileW = 4;
 
