@@ -43,6 +43,32 @@ template <typename C> __device__ __forceinline__ C cmulc(C a, C b) {  // a * con
     return mkc<C>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 template <typename C> __device__ __forceinline__ C cscale(C a, decltype(C::x) s) { return mkc<C>(a.x * s, a.y * s); }
+// complex64 sums and differences as one paired-FP32 instruction each (sm_100:
+// add/sub.f32x2 on a 64-bit register pair, IEEE round-to-nearest per lane,
+// i.e. the same results as two scalar operations); the butterflies of every
+// line transform are made of these
+#if !defined(WOS_SCALAR_CADD)
+__device__ __forceinline__ unsigned long long f2_bits(float2 a) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2_from(unsigned long long r) {
+    float2 a;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a.x), "=f"(a.y) : "l"(r));
+    return a;
+}
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) {
+    unsigned long long d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+    return f2_from(d);
+}
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+    unsigned long long d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2_bits(a)), "l"(f2_bits(b)));
+    return f2_from(d);
+}
+#endif
 template <typename C> __device__ __forceinline__ C cconj(C a) { return mkc<C>(a.x, -a.y); }
 // multiply by -i (forward) or +i (inverse)
 template <bool INV, typename C> __device__ __forceinline__ C mul_mi(C a) {
