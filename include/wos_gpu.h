@@ -42,6 +42,7 @@ extern "C" {
 
 typedef struct { double re, im; } wos_c128;
 typedef struct wos_ctx_s* wos_ctx;
+typedef struct wos_graph_s* wos_graph;
 
 /* Status codes (replace the cufftResult / cudaError_t strings of optics/gpu.go:51-79). */
 enum wos_status {
@@ -424,6 +425,24 @@ WOS_API int wos_splitstep_adjoint_dev(wos_ctx ctx, int ny, int nx, double dx, in
                                       const wos_index_desc* n, int steps, const wos_context* c);
 /* Adjoint operator A^H = F^-1 diag(conj H) F of an ASM step, host field in place. */
 WOS_API int wos_asm_adjoint(wos_ctx ctx, wos_field* f, double z, const wos_context* c);
+
+/* ---- CUDA graphs of device-resident calls (no counterpart in the reference).
+ *      Between capture_begin and capture_end, the device-resident entry points
+ *      called on this context (wos_propagate_dev / _batch_dev / _dev_c128,
+ *      wos_splitstep_dev, wos_splitstep_adjoint_dev, wos_fft2d_dev,
+ *      wos_asm_loss_grad_dev, wos_bpm_stack_loss_grad_dev, ...) are recorded,
+ *      not run; wos_graph_launch replays the whole sequence on the context
+ *      stream with one launch, for loops that repeat it on the same device
+ *      buffers.  Each call must have run once on the same geometry before the
+ *      capture (its work space and tables are then in place: nothing is
+ *      allocated or built while capturing) and must not ask for diagnostics
+ *      or return values that need a synchronisation (a call that does fails
+ *      and the capture with it).  Replays use the buffers and parameters of
+ *      the capture. ---- */
+WOS_API int wos_graph_capture_begin(wos_ctx ctx);
+WOS_API int wos_graph_capture_end(wos_ctx ctx, wos_graph* out);
+WOS_API int wos_graph_launch(wos_ctx ctx, wos_graph g);
+WOS_API int wos_graph_destroy(wos_graph g);
 
 /* ---- zero-padded ASM that allocates no device memory (no counterpart in the
  *      reference).  For callers that cannot call cudaMalloc: processes that

@@ -1,0 +1,126 @@
+"""CUDA graphs of device-resident calls (wos_graph_capture_begin / _end,
+wos_graph_launch): a replay must give the results of the captured calls run
+directly (bit for bit: the same kernels on the same buffers), including the
+forked streams of a device batch and in-place split-step runs replayed
+repeatedly; a call that needs a synchronisation inside a capture fails cleanly
+and leaves the context usable."""
+import numpy as np
+import pytest
+
+from gpu_util import wos
+
+pytestmark = pytest.mark.gpu
+
+PRECS = [pytest.param(wos.FP64, id="fp64"), pytest.param(wos.FP32, id="fp32")]
+
+
+@pytest.fixture(scope="module", params=PRECS)
+def gpu(request):
+    g = wos.GPU(request.param)
+    yield g
+    g.close()
+
+
+def _dt(gpu):
+    import torch
+    return torch.complex128 if gpu.precision == wos.FP64 else torch.complex64
+
+
+def _fields(gpu, k, n, seed=1):
+    import torch
+    rng = np.random.default_rng(seed)
+    return [torch.from_numpy(rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))).to(_dt(gpu)).cuda()
+            for _ in range(k)]
+
+
+CTX = dict(wavelength=632.8e-9, warnings_enabled=False)
+
+
+def test_graph_replays_single_calls(gpu):
+    import torch
+    n, dx, z = 512, 2e-6, 5e-3
+    ins = _fields(gpu, 3, n)
+    outs = [torch.empty_like(t) for t in ins]
+    want = [torch.empty_like(t) for t in ins]
+    torch.cuda.synchronize()
+    for i, w in zip(ins, want):  # direct calls (also the warm-up of the capture)
+        gpu.propagate_dev(n, n, dx, 1, i.data_ptr(), w.data_ptr(), z, "asm", wos.Context(**CTX))
+    gpu.synchronize()
+    gpu.graph_capture_begin()
+    for i, o in zip(ins, outs):
+        gpu.propagate_dev(n, n, dx, 1, i.data_ptr(), o.data_ptr(), z, "asm", wos.Context(**CTX))
+    g = gpu.graph_capture_end()
+    for _ in range(2):
+        for o in outs:
+            o.zero_()
+        torch.cuda.synchronize()
+        g.launch()
+        gpu.synchronize()
+        for o, w in zip(outs, want):
+            assert torch.equal(o, w)
+    g.close()
+
+
+def test_graph_replays_a_device_batch_on_forked_streams(gpu):
+    import torch
+    n, dx, z = 1024, 2e-6, 2e-2
+    ins = _fields(gpu, 4, n, 2)
+    outs = [torch.empty_like(t) for t in ins]
+    torch.cuda.synchronize()
+    gpu.propagate_batch_dev(n, n, dx, 1, [t.data_ptr() for t in ins], [t.data_ptr() for t in outs], z, "asm",
+                            wos.Context(**CTX))
+    gpu.synchronize()
+    want = [o.clone() for o in outs]
+    gpu.graph_capture_begin()
+    gpu.propagate_batch_dev(n, n, dx, 1, [t.data_ptr() for t in ins], [t.data_ptr() for t in outs], z, "asm",
+                            wos.Context(**CTX))
+    g = gpu.graph_capture_end()
+    for o in outs:
+        o.zero_()
+    torch.cuda.synchronize()
+    g.launch()
+    gpu.synchronize()
+    for o, w in zip(outs, want):
+        assert torch.equal(o, w)
+    g.close()
+
+
+def test_graph_replays_split_step_in_place(gpu):
+    """Each replay advances the field by one captured BPM run, like a direct call."""
+    import torch
+    n, dx = 256, 0.5e-6
+    d = wos.IndexDesc()
+    d.re_bg, d.core_dn, d.core_w, d.border_px, d.border_order, d.border_strength = 1.45, 0.01, 20e-6, 8, 2, 5e-3
+    ctx = dict(wavelength=1.55e-6, warnings_enabled=False)
+    a = _fields(gpu, 1, n, 3)[0]
+    b = a.clone()
+    torch.cuda.synchronize()
+    gpu.split_step_dev(n, n, dx, 1, a.data_ptr(), 20e-6, d, 10, wos.Context(**ctx))  # warm-up, direct
+    gpu.split_step_dev(n, n, dx, 1, a.data_ptr(), 20e-6, d, 10, wos.Context(**ctx))
+    gpu.synchronize()
+    gpu.graph_capture_begin()
+    gpu.split_step_dev(n, n, dx, 1, b.data_ptr(), 20e-6, d, 10, wos.Context(**ctx))
+    g = gpu.graph_capture_end()
+    torch.cuda.synchronize()
+    g.launch()
+    g.launch()
+    gpu.synchronize()
+    assert torch.equal(a, b)
+    g.close()
+
+
+def test_graph_capture_of_a_synchronising_call_fails_cleanly(gpu):
+    import torch
+    n, dx, z = 256, 2e-6, 1e-3
+    x = _fields(gpu, 1, n, 4)[0]
+    y = torch.empty_like(x)
+    torch.cuda.synchronize()
+    gpu.graph_capture_begin()
+    with pytest.raises(wos.WosError):
+        # the carrier-shift methods read the spectral centroid back to the host
+        gpu.propagate_dev(n, n, dx, 1, x.data_ptr(), y.data_ptr(), z, "asm_shift", wos.Context(**CTX))
+    with pytest.raises(wos.WosError):
+        gpu.graph_capture_end()
+    gpu.propagate_dev(n, n, dx, 1, x.data_ptr(), y.data_ptr(), z, "asm", wos.Context(**CTX))
+    gpu.synchronize()
+    assert torch.isfinite(torch.view_as_real(y)).all()

@@ -111,6 +111,8 @@ struct wos_ctx_s {
     bool no_fast = false;               // force the general sweeps (tests compare both)
     int sweep_mode = 1;                 // wos_ctx_set_fast_path: 1, 2 or 3 (0 is no_fast)
     int col_pair = 0;                   // column tiles split over two-CTA clusters where supported
+    DevBuf bpm_tab;                     // split-step tables (core profile, border absorption) on the device
+    std::vector<double> bpm_tab_host;   // ... and their host copy, to skip identical uploads
     int tiled = 0;                      // three-sweep ASM through the tiled intermediate (FastRows::out_tiled)
     unsigned* err_dev = nullptr;        // error word of the pipelined kernels (device)
     unsigned* err_host = nullptr;       // pinned mirror, read where the host synchronises
@@ -1357,6 +1359,7 @@ int wos_ctx_destroy(wos_ctx c) {
             if (b->p) cudaFree(b->p);
         for (DevBuf& b : c->tsc)
             if (b.p) cudaFree(b.p);
+        if (c->bpm_tab.p) cudaFree(c->bpm_tab.p);
         if (c->hred) cudaFreeHost(c->hred);
         if (c->err_dev) cudaFree(c->err_dev);
         if (c->err_host) cudaFreeHost(c->err_host);
@@ -1803,7 +1806,6 @@ int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const vo
     // per-run tables: gx of the graded core and the border absorption
     const bool core = d.core_dn != 0;
     const int bpx = (d.border_px > 0 && d.border_strength != 0) ? d.border_px : 0;
-    TRY(ensure(c->params, sizeof(double) * ((size_t)nx + (size_t)bpx + 1)));
     std::vector<double> tab((size_t)nx + (size_t)bpx);
     for (int i = 0; i < nx; i++) {
         const double x = ((double)i - (double)nx / 2) * dx - d.core_x0;
@@ -1815,8 +1817,15 @@ int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const vo
         for (int o = 0; o < d.border_order; o++) p *= tq;
         tab[(size_t)nx + q] = std::exp(-k * d.border_strength * p * dz);
     }
-    CK(cudaMemcpyAsync(c->params.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, c->st));
-    const double* gx = reinterpret_cast<const double*>(c->params.p);
+    // uploaded only when they change: a repeated call issues no host copy
+    // (and can then be captured in a CUDA graph)
+    if (tab != c->bpm_tab_host || !c->bpm_tab.p) {
+        TRY(ensure(c->bpm_tab, sizeof(double) * (tab.size() + 1)));
+        // (a copy from pageable memory returns once the source has been read)
+        CK(cudaMemcpyAsync(c->bpm_tab.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, c->st));
+        c->bpm_tab_host = tab;
+    }
+    const double* gx = reinterpret_cast<const double*>(c->bpm_tab.p);
     int nb = 0;
     FastRows r{};
     r.rows = ny;
@@ -3424,6 +3433,66 @@ int wos_asm_loss_grad_dev(wos_ctx c, int ny, int nx, double dx, double z, const 
     if (rc == -1)
         return fail(WOS_UNSUPPORTED_SIZE, "device-resident inverse design needs power-of-two ny, nx (256..8192)");
     return rc;
+}
+
+struct wos_graph_s {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int device = 0;
+};
+
+int wos_graph_capture_begin(wos_ctx c) {
+    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
+    return WOS_OK;
+}
+
+int wos_graph_capture_end(wos_ctx c, wos_graph* out) {
+    if (!c || !out) return fail(WOS_INVALID_ARG, "null argument");
+    *out = nullptr;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->st, &g);
+    if (e != cudaSuccess || !g) {
+        cudaGetLastError();
+        if (g) cudaGraphDestroy(g);
+        return fail(WOS_CUDA_ERROR, std::string("graph capture failed (a call inside it synchronised or failed): ") +
+                                        cudaGetErrorString(e));
+    }
+    cudaGraphExec_t x = nullptr;
+    e = cudaGraphInstantiate(&x, g, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphDestroy(g);
+        return fail(WOS_CUDA_ERROR, std::string("graph instantiation: ") + cudaGetErrorString(e));
+    }
+    wos_graph h = new wos_graph_s();
+    h->graph = g;
+    h->exec = x;
+    h->device = c->device;
+    *out = h;
+    return WOS_OK;
+}
+
+int wos_graph_launch(wos_ctx c, wos_graph g) {
+    if (!c || !g) return fail(WOS_INVALID_ARG, "null argument");
+    if (g->device != c->device) return fail(WOS_INVALID_ARG, "graph captured on another device");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    CK(cudaGraphLaunch(g->exec, c->st));
+    return WOS_OK;
+}
+
+int wos_graph_destroy(wos_graph g) {
+    if (!g) return WOS_OK;
+    cudaSetDevice(g->device);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return WOS_OK;
 }
 
 int wos_ctx_set_fast_path(wos_ctx c, int enabled) {

@@ -47,6 +47,7 @@ EXPORTS = [
     "wos_bpm_stack_loss_grad", "wos_bpm_stack_loss_grad_dev", "wos_splitstep_adjoint_dev",
     "wos_train", "wos_propagate_vectorial", "wos_plane_view", "wos_plane_view_dev",
     "wos_propagate_uniaxial", "wos_propagate_anisotropic",
+    "wos_graph_capture_begin", "wos_graph_capture_end", "wos_graph_launch", "wos_graph_destroy",
 ]
 
 
@@ -170,6 +171,8 @@ def lib():
             "wos_plane_view_dev": ([vp, i, i, i, vp, vp, i, d, vp], i),
             "wos_propagate_uniaxial": ([vp, vp, d, d, d, vp], i),
             "wos_propagate_anisotropic": ([vp, vp, d, vp, vp], i),
+            "wos_graph_capture_begin": ([vp], i), "wos_graph_capture_end": ([vp, vp], i),
+            "wos_graph_launch": ([vp, vp], i), "wos_graph_destroy": ([vp], i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name, None)
@@ -279,6 +282,27 @@ class Field:
 
     def power(self) -> float:
         return float(self.intensity().sum() * self.dx * self.dx)
+
+
+class Graph:
+    """A captured sequence of device-resident calls (wos_graph), replayed with launch()."""
+
+    def __init__(self, gpu: "GPU", h):
+        self.gpu, self.h = gpu, h
+
+    def launch(self) -> None:
+        _check(lib().wos_graph_launch(self.gpu.h, self.h))
+
+    def close(self) -> None:
+        if self.h:
+            lib().wos_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class GPU:
@@ -566,6 +590,15 @@ class GPU:
         _check(lib().wos_propagate_vectorial(self.h, C.byref(f.c()), _ptr(ez), z,
                                              C.byref(cc) if cc is not None else None))
         return ez
+
+    # ---- CUDA graphs of device-resident calls
+    def graph_capture_begin(self) -> None:
+        _check(lib().wos_graph_capture_begin(self.h))
+
+    def graph_capture_end(self) -> "Graph":
+        h = C.c_void_p()
+        _check(lib().wos_graph_capture_end(self.h, C.byref(h)))
+        return Graph(self, h)
 
     def propagate_uniaxial(self, f: Field, z: float, no: float, ne: float, ctx: Context) -> None:
         """PropagateUniaxial (birefringent.go:19-61), in place."""
