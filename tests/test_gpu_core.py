@@ -262,3 +262,26 @@ def test_power_conservation(gpu):
         assert abs(d.p_out - d.p_in) / d.p_in <= 1e-6
         # FP32 sees the input rounded to complex64
         assert abs(d.p_in - p0) / p0 <= (1e-12 if gpu.precision == wos.FP64 else 1e-6)
+
+
+@pytest.mark.parametrize("n", [1536, 2000, 3000, 3600, 6000])
+def test_fft1d_long_mixed_radix_lines(gpu, n):
+    """2^a 3^b 5^c lines up to 6000 points (one CTA per line, passes between two
+    shared-memory buffers) against numpy's FFT; FP64 6000 takes 16 values per
+    thread so that its 375 threads fit a CTA."""
+    rng = np.random.default_rng(n)
+    a = rng.normal(size=n) + 1j * rng.normal(size=n)
+    got = gpu.fft1d(a)
+    want = np.fft.fft(a)
+    assert rel_l2(got, want) <= (1e-12 if gpu.precision == wos.FP64 else 2e-6)
+    back = gpu.fft1d(got, inverse=True)
+    assert rel_l2(back, a) <= (1e-12 if gpu.precision == wos.FP64 else 2e-6)
+
+
+def test_fft1d_line_beyond_one_cta_is_unsupported(gpu):
+    """4500 = 2^2 3^2 5^3 divides only by E = 4 (1125 threads, more than a CTA
+    holds) and its Bluestein length 16384 exceeds the on-chip limit: a clear
+    WOS_UNSUPPORTED_SIZE, not a failed launch."""
+    with pytest.raises(wos.WosError) as e:
+        gpu.fft1d(np.ones(4500, complex))
+    assert e.value.status == 2

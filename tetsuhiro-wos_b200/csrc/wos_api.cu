@@ -217,7 +217,15 @@ int build_axis(wos_ctx c, int n, int fp64, Axis& ax) {
     // power-of-two lines and 2^a 3^b 5^c lines (a >= 1, a mixed-radix plan)
     // are transformed directly; any other length through Bluestein's chirp
     // convolution on a power-of-two length M >= 2n - 1
-    ax.blue = (is_pow2(n) || mixed_radix_ok(n)) ? 0 : 1;
+    // a mixed-radix line must fit one CTA: n / E threads, and two shared-memory
+    // buffers of the line (its passes alternate between them)
+    bool mixed = mixed_radix_ok(n);
+    if (mixed) {
+        const int E = pick_E(fp64, n);
+        mixed = n % E == 0 && n / E <= max_threads_for(fp64, E) &&
+                2 * row_smem_bytes(fp64, n, E, 1) <= (size_t)227 * 1024;
+    }
+    ax.blue = (is_pow2(n) || mixed) ? 0 : 1;
     ax.L = ax.blue ? next_pow2(2 * n - 1) : n;
     if (n < 2) return fail(WOS_UNSUPPORTED_SIZE, "line length must be >= 2");
     if (ax.L > (fp64 ? kMaxL64 : kMaxL32))

@@ -355,60 +355,50 @@ __device__ __forceinline__ void line_fft(C* v, C* sm, const IDX& ix, int line, i
     }
 }
 
-// One Stockham pass of a mixed-radix line held in shared memory: butterfly
-// j < L/R (sub-transform length NS, k = j mod NS) reads x[j + r L/R], takes
-// the twiddles W_L^{r k L/(NS R)} from the L-point table, and writes
-// positions (j - k) R + k + r NS.  A thread stages its ceil(E/R) butterflies
-// in registers between the two barriers, so the pass works in place.
-template <int R, int E, bool INV, typename C, typename IDX>
-__device__ __forceinline__ void mixed_pass(C* sm, const IDX& ix, int line, int tt, int T, int L, int NS,
-                                           const C* __restrict__ tw) {
-    constexpr int NB = (E + R - 1) / R;
-    const int nbf = L / R, LR = L / R;
-    C x[NB][R];
-#pragma unroll
-    for (int i = 0; i < NB; i++) {
-        const int j = tt + i * T;
-        if (j < nbf) {
-#pragma unroll
-            for (int r = 0; r < R; r++) x[i][r] = sm[ix(line, j + r * LR)];
-        }
-    }
-    __syncthreads();
+// One Stockham pass of a mixed-radix line from src to dst (shared memory), one
+// radix-R butterfly at a time: each thread holds only the R values of its
+// current butterfly (a pass in place would have to hold all of them across a
+// barrier).  Sub-transform length NS; twiddles W_L^(r k L/(NS R)) from the
+// length-L table.
+template <int R, bool INV, typename C, typename IDX>
+__device__ __forceinline__ void mixed_pass_pp(const C* src, C* dst, const IDX& ix, int line, int tt, int T, int L,
+                                              int NS, const C* __restrict__ tw) {
+    const int LR = L / R;
     const int step = L / (NS * R);
+    for (int j = tt; j < LR; j += T) {
+        C x[R];
 #pragma unroll
-    for (int i = 0; i < NB; i++) {
-        const int j = tt + i * T;
-        if (j < nbf) {
-            const int k = j % NS;
-            if (NS > 1) {
+        for (int r = 0; r < R; r++) x[r] = src[ix(line, j + r * LR)];
+        const int k = j % NS;
+        if (NS > 1) {
 #pragma unroll
-                for (int r = 1; r < R; r++) {
-                    C w = ldg_c(tw + r * k * step);
-                    if (INV) w.y = -w.y;
-                    x[i][r] = cmul(x[i][r], w);
-                }
+            for (int r = 1; r < R; r++) {
+                C w = ldg_c(tw + r * k * step);
+                if (INV) w.y = -w.y;
+                x[r] = cmul(x[r], w);
             }
-            dft<R, INV>(x[i]);
-            const int base = (j - k) * R + k;
-#pragma unroll
-            for (int r = 0; r < R; r++) sm[ix(line, base + r * NS)] = x[i][r];
         }
+        dft<R, INV>(x);
+        const int base = (j - k) * R + k;
+#pragma unroll
+        for (int r = 0; r < R; r++) dst[ix(line, base + r * NS)] = x[r];
     }
-    __syncthreads();
 }
 
 // Mixed-radix line transform (L = 2^a 3^b 5^c, a >= 1): registers (positions
-// tt + s*T) to shared memory, radix 16 / 8 / 4 / 2 then 3 then 5 passes in
-// place, back to the same registers.  Must be called by every thread of the
-// CTA (it synchronises).
+// tt + s*T) to shared memory, radix 16 / 8 / 4 / 2 then 3 then 5 passes
+// alternating between sm and alt (two buffers of the same layout), back to
+// the same registers.  Must be called by every thread of the CTA (it
+// synchronises).
 template <int E, bool INV, typename C, typename IDX>
-__device__ __forceinline__ void mixed_line_fft(C* v, C* sm, const IDX& ix, int line, int tt, int T, int L,
+__device__ __forceinline__ void mixed_line_fft(C* v, C* sm, C* alt, const IDX& ix, int line, int tt, int T, int L,
                                                const C* __restrict__ tw) {
     __syncthreads();
 #pragma unroll
     for (int s = 0; s < E; s++) sm[ix(line, tt + s * T)] = v[s];
     __syncthreads();
+    C* src = sm;
+    C* dst = alt;
     int rem = L, NS = 1;
     while (rem > 1) {
         int R;
@@ -419,18 +409,22 @@ __device__ __forceinline__ void mixed_line_fft(C* v, C* sm, const IDX& ix, int l
         else if (rem % 3 == 0) R = 3;
         else R = 5;
         switch (R) {
-        case 16: mixed_pass<16, E, INV>(sm, ix, line, tt, T, L, NS, tw); break;
-        case 8: mixed_pass<8, E, INV>(sm, ix, line, tt, T, L, NS, tw); break;
-        case 4: mixed_pass<4, E, INV>(sm, ix, line, tt, T, L, NS, tw); break;
-        case 2: mixed_pass<2, E, INV>(sm, ix, line, tt, T, L, NS, tw); break;
-        case 3: mixed_pass<3, E, INV>(sm, ix, line, tt, T, L, NS, tw); break;
-        default: mixed_pass<5, E, INV>(sm, ix, line, tt, T, L, NS, tw); break;
+        case 16: mixed_pass_pp<16, INV>(src, dst, ix, line, tt, T, L, NS, tw); break;
+        case 8: mixed_pass_pp<8, INV>(src, dst, ix, line, tt, T, L, NS, tw); break;
+        case 4: mixed_pass_pp<4, INV>(src, dst, ix, line, tt, T, L, NS, tw); break;
+        case 2: mixed_pass_pp<2, INV>(src, dst, ix, line, tt, T, L, NS, tw); break;
+        case 3: mixed_pass_pp<3, INV>(src, dst, ix, line, tt, T, L, NS, tw); break;
+        default: mixed_pass_pp<5, INV>(src, dst, ix, line, tt, T, L, NS, tw); break;
         }
+        __syncthreads();
+        C* t = src;
+        src = dst;
+        dst = t;
         NS *= R;
         rem /= R;
     }
 #pragma unroll
-    for (int s = 0; s < E; s++) v[s] = sm[ix(line, tt + s * T)];
+    for (int s = 0; s < E; s++) v[s] = src[ix(line, tt + s * T)];
 }
 
 // Position held by register slot s (= b*R + r) under the natural mapping of radix R.

@@ -235,6 +235,8 @@ int pick_E(int fp64, int L) {
     int e = fp64 ? (L >= 8192 ? 16 : 8) : 16;
     while (e > L) e >>= 1;
     while (e > 2 && L % e != 0) e >>= 1;  // a mixed-radix line: E divides L
+    // a long line whose threads would not fit one CTA takes more values per thread
+    while (e < 16 && L / e > max_threads_for(fp64, e) && L % (2 * e) == 0) e <<= 1;
     return e;
 }
 int max_threads_for(int fp64, int E) { return (E >= 16 || fp64) ? 512 : 1024; }
@@ -256,7 +258,8 @@ static cudaError_t launch_rows_t(const RowArgs& a, cudaStream_t st) {
     const size_t smem = (size_t)row_line_stride(a.L) * lines * sizeof(typename CT<Real>::t);
     const int nbat = (a.mode == ROW_INV_ACC) ? 1 : (a.batch > 0 ? a.batch : 1);
     dim3 grid((a.rows + lines - 1) / lines, nbat);
-    if ((a.L & (a.L - 1)) != 0) return launch_rows_mix<Real, E>(a, grid, lines * T, smem, st);
+    // mixed-radix lines alternate between two shared-memory buffers
+    if ((a.L & (a.L - 1)) != 0) return launch_rows_mix<Real, E>(a, grid, lines * T, 2 * smem, st);
     if (smem > kSmemNoOptIn) {
         cudaError_t e = cudaFuncSetAttribute(k_rows<Real, E, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
@@ -276,7 +279,7 @@ static cudaError_t launch_cols_t(const ColArgs& a, cudaStream_t st) {
     if (b.W * T > maxt) return cudaErrorInvalidConfiguration;
     const size_t smem = (size_t)col_tile_elems(b.L, b.W) * sizeof(typename CT<Real>::t);
     dim3 grid((b.ncols + b.W - 1) / b.W, b.batch > 0 ? b.batch : 1);
-    if ((b.L & (b.L - 1)) != 0) return launch_cols_mix<Real, E>(b, grid, b.W * T, smem, st);
+    if ((b.L & (b.L - 1)) != 0) return launch_cols_mix<Real, E>(b, grid, b.W * T, 2 * smem, st);
     if (smem > kSmemNoOptIn) {
         cudaError_t e = cudaFuncSetAttribute(k_cols<Real, E, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);

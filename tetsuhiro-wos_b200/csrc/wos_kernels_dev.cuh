@@ -282,12 +282,15 @@ __device__ __forceinline__ int in_radix(const LinePlan& lp, bool inv, bool blue,
 __device__ __forceinline__ int out_radix(const LinePlan& lp, bool inv, bool blue, int E) {
     return (blue || inv) ? last_radix(lp, true, E) : E;
 }
+// alt: the second shared-memory buffer of the mixed-radix kernels (same
+// layout as sm, placed after it), null otherwise.
 template <int E, bool MIX, typename C, typename IDX>
-__device__ __forceinline__ void xform(C* v, C* sm, const IDX& ix, int line, int tt, int T, const LinePlan& lp,
-                                      const C* __restrict__ tw, bool inv, const C* __restrict__ bhat) {
+__device__ __forceinline__ void xform(C* v, C* sm, C* alt, const IDX& ix, int line, int tt, int T,
+                                      const LinePlan& lp, const C* __restrict__ tw, bool inv,
+                                      const C* __restrict__ bhat) {
     if constexpr (MIX) {  // kernels launched for mixed-radix lines only
-        if (inv) mixed_line_fft<E, true>(v, sm, ix, line, tt, T, lp.L, tw);
-        else mixed_line_fft<E, false>(v, sm, ix, line, tt, T, lp.L, tw);
+        if (inv) mixed_line_fft<E, true>(v, sm, alt, ix, line, tt, T, lp.L, tw);
+        else mixed_line_fft<E, false>(v, sm, alt, ix, line, tt, T, lp.L, tw);
         return;
     }
     if (!bhat) {
@@ -320,6 +323,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows(const RowArgs a) {
     const int bz = blockIdx.y;
     const int grow = a.row0 + r;  // grid row (coordinates)
     const RowIdx ix{row_line_stride(L)};
+    C* const alt = MIX ? sm + (size_t)row_line_stride(L) * lines : nullptr;  // launched with two buffers
     const LinePlan lp = make_line_plan(L, E);
     const C* tw = reinterpret_cast<const C*>(a.tw);
     const bool blue = a.blue_n > 0;
@@ -376,7 +380,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows(const RowArgs a) {
         }
 
         // ---- transform(s)
-        xform<E, MIX>(v, sm, ix, line, tt, T, lp, tw, !fwd_first, fwd_first ? bhf : bhi);
+        xform<E, MIX>(v, sm, alt, ix, line, tt, T, lp, tw, !fwd_first, fwd_first ? bhf : bhi);
         Rout = out_radix(lp, !fwd_first, blue, E);
         if (a.mode == ROW_INV_FWD) {
             // real-space screen between the inverse and the next forward row
@@ -391,7 +395,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows(const RowArgs a) {
                     v[s] = mkc<C>(0, 0);
                 }
             }
-            xform<E, MIX>(v, sm, ix, line, tt, T, lp, tw, false, bhf);
+            xform<E, MIX>(v, sm, alt, ix, line, tt, T, lp, tw, false, bhf);
             Rout = out_radix(lp, false, blue, E);
             if (blue) {
 #pragma unroll
@@ -492,6 +496,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
     const bool act = col < a.ncols;
     const int bz = blockIdx.y;
     const ColIdx ix{W};
+    C* const alt = MIX ? sm + (size_t)col_tile_elems(L, W) : nullptr;  // launched with two buffers
     const LinePlan lp = make_line_plan(L, E);
     const C* tw = reinterpret_cast<const C*>(a.tw);
     const bool blue = a.blue_n > 0;
@@ -522,7 +527,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
     }
 
     // first column transform
-    xform<E, MIX>(v, sm, ix, w, tt, T, lp, tw, inv_first, inv_first ? bhi : bhf);
+    xform<E, MIX>(v, sm, alt, ix, w, tt, T, lp, tw, inv_first, inv_first ? bhi : bhf);
     int Rm = out_radix(lp, inv_first, blue, E);
     if (blue && (a.mode == COL_FRAUNHOFER || a.mode == COL_FFT)) {
         // the chirp of the Bluestein output has unit modulus: applied only
@@ -624,7 +629,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
     }
 
     if (a.mode == COL_FUSED) {
-        xform<E, MIX>(v, sm, ix, w, tt, T, lp, tw, true, bhi);
+        xform<E, MIX>(v, sm, alt, ix, w, tt, T, lp, tw, true, bhi);
         Rm = out_radix(lp, true, blue, E);
         if (blue) {
 #pragma unroll
