@@ -419,6 +419,10 @@ WOS_API int wos_bpm_stack_loss_grad_dev(wos_ctx ctx, int ny, int nx, double dx, 
                                         const double* phis, const double* target, double zseg,
                                         const wos_index_desc* n, int steps, const wos_context* c, double* loss,
                                         double* grads);
+/* Adjoint of wos_splitstep (conj transfer functions and screens, slices in
+ * reverse order): the backward BPM operator, host field in place. */
+WOS_API int wos_splitstep_adjoint(wos_ctx ctx, wos_field* f, double z, const wos_index_desc* n, int steps,
+                                  const wos_context* c);
 /* Adjoint of wos_splitstep_dev (conj transfer functions and screens, slices
  * in reverse order), device field in place, no diagnostics. */
 WOS_API int wos_splitstep_adjoint_dev(wos_ctx ctx, int ny, int nx, double dx, int ncomp, void* field, double z,

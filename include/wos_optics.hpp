@@ -11,6 +11,7 @@
 //   GenerateSchellRealizations, PropagatePartiallyCoherent
 //                               optics/coherence.go:22-116
 //   Propagate1D                 optics/propagate.go:718-738
+//   ForwardASM / BackwardASM, ForwardBPM / BackwardBPM   (inverse design; no reference counterpart)
 //   Field.ApplyJones / ScaleAmplitude / ApplyTilt / ShiftField / ApplyBandlimit
 //                               optics/field.go:109-168,199-228,264-294
 //   ApplyDiffuser               optics/elements.go:722-783 (diffuserEl.Apply)
@@ -297,6 +298,23 @@ inline std::vector<double> PropagatePartiallyCoherent(Backend& b, int n, double 
                                  &d));
     ctx->absorb(d);
     return out;
+}
+
+// Inverse design: the forward operators and their adjoints (conj transfer
+// functions, conj screens, BPM slices in reverse order), host fields in place.
+inline void ForwardASM(Backend& b, Field& f, double z, Context* ctx) { Propagate(b, f, z, Method::ASM, ctx); }
+inline void BackwardASM(Backend& b, Field& f, double z, const Context& ctx) {
+    wos_field cf = f.c();
+    wos_context cc = ctx.c();
+    check(wos_asm_adjoint(b.handle(), &cf, z, &cc));
+}
+inline void ForwardBPM(Backend& b, Field& f, double z, const wos_index_desc& n, int steps, Context* ctx) {
+    PropagateSplitStep(b, f, z, n, steps, ctx);
+}
+inline void BackwardBPM(Backend& b, Field& f, double z, const wos_index_desc& n, int steps, const Context& ctx) {
+    wos_field cf = f.c();
+    wos_context cc = ctx.c();
+    check(wos_splitstep_adjoint(b.handle(), &cf, z, &n, steps, &cc));
 }
 
 // Propagate1D: a line of n = a.size() samples in place (wl apart from ctx).

@@ -1,7 +1,8 @@
 // Exercises the C++ host interface (include/wos_optics.hpp) on a GPU and
 // checks it against the FP64 oracle: Propagate for every method, the nil
 // context and z == 0 rules, ParseMethod errors, split-step, polychromatic,
-// volume.  Prints "ok" and returns 0 on success.
+// volume, and the inverse-design Forward / Backward pairs (adjoint identity).
+// Prints "ok" and returns 0 on success.
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -110,6 +111,43 @@ int main() {
         double ip = 0;
         for (double v : I) ip += v;
         REQUIRE(ip > 0);
+    }
+    // Inverse-design pair: BackwardBPM is the adjoint of ForwardBPM, BackwardASM of ForwardASM
+    {
+        const int m = 64;
+        Field x(m, 1e-6, false), y(m, 1e-6, false);
+        for (int i = 0; i < m * m; i++) {
+            x.Ex[i] = cplx(std::sin(0.37 * i), std::cos(0.11 * i));
+            y.Ex[i] = cplx(std::cos(0.23 * i), std::sin(0.71 * i));
+        }
+        wos_index_desc d{};
+        d.re_bg = 1.5;
+        d.core_dn = 0.01;
+        d.core_w = 15e-6;
+        d.border_px = 4;
+        d.border_order = 2;
+        d.border_strength = 3e-3;
+        Context c;
+        c.Wavelength = wl;
+        for (int op = 0; op < 2; op++) {
+            Field ax = x.Clone(), ahy = y.Clone();
+            if (op == 0) {
+                ForwardBPM(b, ax, 20e-6, d, 4, &c);
+                BackwardBPM(b, ahy, 20e-6, d, 4, c);
+            } else {
+                ForwardASM(b, ax, 30e-6, &c);
+                BackwardASM(b, ahy, 30e-6, c);
+            }
+            cplx lhs = 0, rhs = 0;
+            double nax = 0, ny = 0;
+            for (int i = 0; i < m * m; i++) {
+                lhs += std::conj(y.Ex[i]) * ax.Ex[i];
+                rhs += std::conj(ahy.Ex[i]) * x.Ex[i];
+                nax += std::norm(ax.Ex[i]);
+                ny += std::norm(y.Ex[i]);
+            }
+            REQUIRE(std::abs(lhs - rhs) <= 1e-11 * std::sqrt(nax * ny));
+        }
     }
     std::printf("ok\n");
     return 0;

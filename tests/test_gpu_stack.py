@@ -173,3 +173,23 @@ def test_bpm_stack_argument_errors(gpu):
         gpu.bpm_stack_loss_grad(a, phis, T, 1e-6, 1e-5, 0, gd, wos.Context(wavelength=WL))
     with pytest.raises(wos.WosError):
         gpu.bpm_stack_loss_grad(a, phis, T, 1e-6, 1e-5, 2, gd, wos.Context(wavelength=0.0))
+
+
+@pytest.mark.parametrize("pol", [False, True])
+def test_backward_bpm_host_entry_point_is_the_adjoint(gpu, pol):
+    """<A x, y> == <x, A^H y> through the host pair split_step / split_step_adjoint."""
+    n, dx, z, steps = 64, 1e-6, 25e-6, 5
+    rng = np.random.default_rng(12)
+    c = lambda: rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n))  # noqa: E731
+    x, y = c(), c()
+    x2, y2 = (c(), c()) if pol else (None, None)
+    _, gd = _medium()
+    ctx = wos.Context(wavelength=WL, warnings_enabled=False)
+    fx = wos.Field(x.copy(), dx, None if x2 is None else x2.copy())
+    gpu.split_step(fx, z, gd, steps, ctx)
+    fy = wos.Field(y.copy(), dx, None if y2 is None else y2.copy())
+    gpu.split_step_adjoint(fy, z, gd, steps, ctx)
+    lhs = np.vdot(y, fx.ex) + (np.vdot(y2, fx.ey) if pol else 0)
+    rhs = np.vdot(fy.ex, x) + (np.vdot(fy.ey, x2) if pol else 0)
+    scale = np.linalg.norm(fx.ex) * np.linalg.norm(y) * (2 if pol else 1)
+    assert abs(lhs - rhs) <= (1e-12 if gpu.precision == wos.FP64 else 1e-5) * scale

@@ -3158,6 +3158,20 @@ int wos_propagate1d(wos_ctx c, int n, wos_c128* a, double dx, double z, double w
     return WOS_OK;
 }
 
+int wos_splitstep_adjoint(wos_ctx c, wos_field* f, double z, const wos_index_desc* n, int steps,
+                          const wos_context* cc) {
+    if (!c || !n || !cc) return fail(WOS_INVALID_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(element_begin(c, f));
+    ScreenSrc src;
+    src.kind = 1;
+    src.desc = *n;
+    const int ncomp = f->polarized ? 2 : 1;
+    TRY(run_splitstep(c, f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, c->stage.p, 1, z, src, steps, *cc, nullptr,
+                      true));
+    return stage_out(c, f, ncomp);
+}
+
 int wos_splitstep_adjoint_dev(wos_ctx c, int ny, int nx, double dx, int ncomp, void* field, double z,
                               const wos_index_desc* n, int steps, const wos_context* cc) {
     if (!c || !n || !cc) return fail(WOS_INVALID_ARG, "null argument");

@@ -48,6 +48,7 @@ EXPORTS = [
     "wos_train", "wos_propagate_vectorial", "wos_plane_view", "wos_plane_view_dev",
     "wos_propagate_uniaxial", "wos_propagate_anisotropic",
     "wos_graph_capture_begin", "wos_graph_capture_end", "wos_graph_launch", "wos_graph_destroy",
+    "wos_splitstep_adjoint",
 ]
 
 
@@ -173,6 +174,7 @@ def lib():
             "wos_propagate_anisotropic": ([vp, vp, d, vp, vp], i),
             "wos_graph_capture_begin": ([vp], i), "wos_graph_capture_end": ([vp, vp], i),
             "wos_graph_launch": ([vp, vp], i), "wos_graph_destroy": ([vp], i),
+            "wos_splitstep_adjoint": ([vp, vp, d, vp, i, vp], i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name, None)
@@ -710,6 +712,11 @@ class GPU:
                                                  C.c_void_p(target_ptr), zseg, C.byref(desc), steps, C.byref(cc),
                                                  C.byref(loss), C.c_void_p(grads_ptr) if grads_ptr else None))
         return loss.value
+
+    def split_step_adjoint(self, f: Field, z: float, desc: "IndexDesc", steps: int, ctx: Context) -> None:
+        """Backward BPM: the adjoint of split_step on a host field, in place."""
+        cc = ctx.c()
+        _check(lib().wos_splitstep_adjoint(self.h, C.byref(f.c()), z, C.byref(desc), steps, C.byref(cc)))
 
     def split_step_adjoint_dev(self, ny, nx, dx, ncomp, ptr, z, desc, steps, ctx) -> None:
         """Adjoint of split_step_dev on a device field, in place."""
