@@ -19,6 +19,7 @@
 #include "../../include/wos_gpu.h"
 #include "wos_fast.cuh"
 #include "wos_pipe.cuh"
+#include "wos_fft.cuh"
 #include "wos_kernels.cuh"
 
 using namespace wos;
@@ -231,8 +232,11 @@ int build_axis(wos_ctx c, int n, int fp64, Axis& ax) {
     if (ax.L > (fp64 ? kMaxL64 : kMaxL32))
         return fail(WOS_UNSUPPORTED_SIZE, "line length " + std::to_string(n) + " exceeds the on-chip limit (" +
                                               std::to_string(fp64 ? kMaxL64 : kMaxL32) + " transform points)");
-    CK(cudaMalloc(&ax.tw, cs * ax.L));
+    // mixed-radix lines: the L-point table, then the per-pass tables of the plan
+    const size_t ntw = (size_t)ax.L + (mixed ? (size_t)mixed_table_len(ax.L) : 0);
+    CK(cudaMalloc(&ax.tw, cs * ntw));
     CK(launch_twiddles(fp64, ax.tw, ax.L, c->st));
+    if (mixed) CK(launch_mixed_twiddles(fp64, reinterpret_cast<char*>(ax.tw) + cs * ax.L, ax.L, c->st));
     if (!ax.blue) return WOS_OK;
     CK(cudaMalloc(&ax.chirp, cs * n));
     CK(cudaMalloc(&ax.bf, cs * ax.L));

@@ -355,25 +355,51 @@ __device__ __forceinline__ void line_fft(C* v, C* sm, const IDX& ix, int line, i
     }
 }
 
+// Radix of the next pass of a mixed-radix plan with `rem` points left to
+// factor: 16, 8, 4, 2 first, then 3, then 5 (host and device agree).
+__host__ __device__ inline int mixed_radix_of(int rem) {
+    if (rem % 16 == 0) return 16;
+    if (rem % 8 == 0) return 8;
+    if (rem % 4 == 0) return 4;
+    if (rem % 2 == 0) return 2;
+    if (rem % 3 == 0) return 3;
+    return 5;
+}
+// Entries of the per-pass twiddle tables of a mixed-radix line of L points:
+// pass p (radix R, sub-transform length NS) holds W_{NS R}^{r k} at [r-1][k].
+__host__ __device__ inline int mixed_table_len(int L) {
+    int rem = L, NS = 1, n = 0;
+    while (rem > 1) {
+        const int R = mixed_radix_of(rem);
+        n += NS * (R - 1);
+        NS *= R;
+        rem /= R;
+    }
+    return n;
+}
+
 // One Stockham pass of a mixed-radix line from src to dst (shared memory), one
 // radix-R butterfly at a time: each thread holds only the R values of its
 // current butterfly (a pass in place would have to hold all of them across a
-// barrier).  Sub-transform length NS; twiddles W_L^(r k L/(NS R)) from the
-// length-L table.
+// barrier).  Sub-transform length NS; twiddles from the pass's table ptw
+// ([r-1][k], consecutive k for consecutive threads).  k = j mod NS comes from a
+// single-precision quotient corrected by one step (exact for j < 2^23).
 template <int R, bool INV, typename C, typename IDX>
 __device__ __forceinline__ void mixed_pass_pp(const C* src, C* dst, const IDX& ix, int line, int tt, int T, int L,
-                                              int NS, const C* __restrict__ tw) {
+                                              int NS, const C* __restrict__ ptw) {
     const int LR = L / R;
-    const int step = L / (NS * R);
+    const float inv_ns = 1.0f / (float)NS;
     for (int j = tt; j < LR; j += T) {
         C x[R];
 #pragma unroll
         for (int r = 0; r < R; r++) x[r] = src[ix(line, j + r * LR)];
-        const int k = j % NS;
+        int k = j - (int)((float)j * inv_ns) * NS;
+        if (k < 0) k += NS;
+        else if (k >= NS) k -= NS;
         if (NS > 1) {
 #pragma unroll
             for (int r = 1; r < R; r++) {
-                C w = ldg_c(tw + r * k * step);
+                C w = ldg_c(ptw + (r - 1) * NS + k);
                 if (INV) w.y = -w.y;
                 x[r] = cmul(x[r], w);
             }
@@ -388,8 +414,9 @@ __device__ __forceinline__ void mixed_pass_pp(const C* src, C* dst, const IDX& i
 // Mixed-radix line transform (L = 2^a 3^b 5^c, a >= 1): registers (positions
 // tt + s*T) to shared memory, radix 16 / 8 / 4 / 2 then 3 then 5 passes
 // alternating between sm and alt (two buffers of the same layout), back to
-// the same registers.  Must be called by every thread of the CTA (it
-// synchronises).
+// the same registers.  tw: the L-point table followed by the per-pass tables
+// (mixed_table_len(L) entries).  Must be called by every thread of the CTA
+// (it synchronises).
 template <int E, bool INV, typename C, typename IDX>
 __device__ __forceinline__ void mixed_line_fft(C* v, C* sm, C* alt, const IDX& ix, int line, int tt, int T, int L,
                                                const C* __restrict__ tw) {
@@ -399,27 +426,23 @@ __device__ __forceinline__ void mixed_line_fft(C* v, C* sm, C* alt, const IDX& i
     __syncthreads();
     C* src = sm;
     C* dst = alt;
+    const C* ptw = tw + L;
     int rem = L, NS = 1;
     while (rem > 1) {
-        int R;
-        if (rem % 16 == 0) R = 16;
-        else if (rem % 8 == 0) R = 8;
-        else if (rem % 4 == 0) R = 4;
-        else if (rem % 2 == 0) R = 2;
-        else if (rem % 3 == 0) R = 3;
-        else R = 5;
+        const int R = mixed_radix_of(rem);
         switch (R) {
-        case 16: mixed_pass_pp<16, INV>(src, dst, ix, line, tt, T, L, NS, tw); break;
-        case 8: mixed_pass_pp<8, INV>(src, dst, ix, line, tt, T, L, NS, tw); break;
-        case 4: mixed_pass_pp<4, INV>(src, dst, ix, line, tt, T, L, NS, tw); break;
-        case 2: mixed_pass_pp<2, INV>(src, dst, ix, line, tt, T, L, NS, tw); break;
-        case 3: mixed_pass_pp<3, INV>(src, dst, ix, line, tt, T, L, NS, tw); break;
-        default: mixed_pass_pp<5, INV>(src, dst, ix, line, tt, T, L, NS, tw); break;
+        case 16: mixed_pass_pp<16, INV>(src, dst, ix, line, tt, T, L, NS, ptw); break;
+        case 8: mixed_pass_pp<8, INV>(src, dst, ix, line, tt, T, L, NS, ptw); break;
+        case 4: mixed_pass_pp<4, INV>(src, dst, ix, line, tt, T, L, NS, ptw); break;
+        case 2: mixed_pass_pp<2, INV>(src, dst, ix, line, tt, T, L, NS, ptw); break;
+        case 3: mixed_pass_pp<3, INV>(src, dst, ix, line, tt, T, L, NS, ptw); break;
+        default: mixed_pass_pp<5, INV>(src, dst, ix, line, tt, T, L, NS, ptw); break;
         }
         __syncthreads();
         C* t = src;
         src = dst;
         dst = t;
+        ptw += NS * (R - 1);
         NS *= R;
         rem /= R;
     }

@@ -347,6 +347,37 @@ cudaError_t launch_asm1d_h(int fp64, void* a, int n, const HArgs& h, double* par
     return cudaGetLastError();
 }
 
+// Per-pass twiddle tables of a mixed-radix line (see mixed_table_len):
+// W_{NS R}^{r k} generated in FP64, entry [off_p + (r-1) NS + k].
+template <typename C>
+__global__ void k_mixed_twiddles(C* out, int L, int total) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total) return;
+    int rem = L, NS = 1, off = 0;
+    while (rem > 1) {
+        const int R = mixed_radix_of(rem);
+        const int n = NS * (R - 1);
+        if (idx < off + n) {
+            const int t = idx - off, r = t / NS + 1, k = t % NS;
+            double s, c;
+            sincospi(-2.0 * (double)r * (double)k / ((double)NS * (double)R), &s, &c);
+            out[idx] = mkc<C>((decltype(C::x))c, (decltype(C::x))s);
+            return;
+        }
+        off += n;
+        NS *= R;
+        rem /= R;
+    }
+}
+cudaError_t launch_mixed_twiddles(int fp64, void* out, int L, cudaStream_t st) {
+    const int total = mixed_table_len(L);
+    const int b = 256, g = (total + b - 1) / b;
+    if (total == 0) return cudaSuccess;
+    if (fp64) k_mixed_twiddles<double2><<<g, b, 0, st>>>(reinterpret_cast<double2*>(out), L, total);
+    else k_mixed_twiddles<float2><<<g, b, 0, st>>>(reinterpret_cast<float2*>(out), L, total);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_twiddles(int fp64, void* tw, int L, cudaStream_t st) {
     const int b = 256, g = (L + b - 1) / b;
     if (fp64) k_twiddles<double2><<<g, b, 0, st>>>(reinterpret_cast<double2*>(tw), L);

@@ -160,6 +160,8 @@ struct ColArgs {
 cudaError_t launch_rows(int fp64, const RowArgs& a, cudaStream_t st);
 cudaError_t launch_cols(int fp64, const ColArgs& a, cudaStream_t st);
 cudaError_t launch_twiddles(int fp64, void* tw, int L, cudaStream_t st);
+// Per-pass tables of a mixed-radix line, written after its L-point table.
+cudaError_t launch_mixed_twiddles(int fp64, void* out, int L, cudaStream_t st);
 cudaError_t launch_chirp_b0(int fp64, void* chirp, double2* b0f, double2* b0i, int n, int M,
                             cudaStream_t st);
 cudaError_t launch_bhat_finish(int fp64, void* dst_f, void* dst_i, const double2* bf,

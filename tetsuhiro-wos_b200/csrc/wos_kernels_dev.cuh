@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows(const RowArgs a) {
     for (int bb = 0; bb < nb; bb++) {
         const long long ibase = (long long)(a.mode == ROW_INV_ACC ? bb : bz) * a.in_bstride + (long long)r * a.in_ld;
         // ---- load (register mapping of the first pass)
-        const int R1 = in_radix(lp, !fwd_first, blue, E);
+        const int R1 = MIX ? E : in_radix(lp, !fwd_first, blue, E);  // mixed lines: natural radix E
 #pragma unroll
         for (int s = 0; s < E; s++) {
             const int p = nat_pos(s, R1, tt, T, L);
@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows(const RowArgs a) {
 
         // ---- transform(s)
         xform<E, MIX>(v, sm, alt, ix, line, tt, T, lp, tw, !fwd_first, fwd_first ? bhf : bhi);
-        Rout = out_radix(lp, !fwd_first, blue, E);
+        Rout = MIX ? E : out_radix(lp, !fwd_first, blue, E);
         if (a.mode == ROW_INV_FWD) {
             // real-space screen between the inverse and the next forward row
             // transform; for Bluestein lines the conj(chirp) / chirp pair
@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows(const RowArgs a) {
                 }
             }
             xform<E, MIX>(v, sm, alt, ix, line, tt, T, lp, tw, false, bhf);
-            Rout = out_radix(lp, false, blue, E);
+            Rout = MIX ? E : out_radix(lp, false, blue, E);
             if (blue) {
 #pragma unroll
                 for (int s = 0; s < E; s++) {
@@ -514,7 +514,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
 
     C v[E];
     const C* src = reinterpret_cast<const C*>(a.src) + (a.src_shared ? 0 : (long long)bz * a.src_bstride);
-    const int R1 = in_radix(lp, inv_first, blue, E);
+    const int R1 = MIX ? E : in_radix(lp, inv_first, blue, E);  // mixed lines: natural radix E
 #pragma unroll
     for (int s = 0; s < E; s++) {
         const int p = nat_pos(s, R1, tt, T, L);
@@ -528,7 +528,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
 
     // first column transform
     xform<E, MIX>(v, sm, alt, ix, w, tt, T, lp, tw, inv_first, inv_first ? bhi : bhf);
-    int Rm = out_radix(lp, inv_first, blue, E);
+    int Rm = MIX ? E : out_radix(lp, inv_first, blue, E);
     if (blue && (a.mode == COL_FRAUNHOFER || a.mode == COL_FFT)) {
         // the chirp of the Bluestein output has unit modulus: applied only
         // where the phase of the spectrum leaves the kernel
@@ -630,7 +630,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
 
     if (a.mode == COL_FUSED) {
         xform<E, MIX>(v, sm, alt, ix, w, tt, T, lp, tw, true, bhi);
-        Rm = out_radix(lp, true, blue, E);
+        Rm = MIX ? E : out_radix(lp, true, blue, E);
         if (blue) {
 #pragma unroll
             for (int s = 0; s < E; s++) {
