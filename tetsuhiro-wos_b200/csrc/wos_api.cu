@@ -689,7 +689,7 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     // tiled intermediate (FP32): the column sweep reads contiguous tiles of
     // kTileW columns; the intermediate is then a buffer of its own (the last
     // sweep changes the layout, so it cannot run in place in the output)
-    const bool tiled = c->tiled && !c->fp64 && p.nx % kTileW == 0 && !s.hist &&
+    const bool tiled = c->tiled && !c->fp64 && p.nx % kTileW == 0 &&
                        fast_col_width(c->fp64, p.ny, t.colE, kTileW) == kTileW;
     void* S;
     if (p.out_c128) {

@@ -251,6 +251,7 @@ __device__ __noinline__ void col_hist_bin(const C* tile, double* hsm, int col0, 
     const double fnyq = 1.0 / (2.0 * hist_dx);
     const double den = __dmul_rn((double)L, hist_dx);
     const double dnx = __dmul_rn((double)ncols, hist_dx);
+    const float inv_dnx = (float)(1.0 / dnx), inv_den = (float)(1.0 / den), bins_per_f = (float)(96.0 / fnyq);
     for (int idx = threadIdx.x; idx < W * NJ; idx += blockDim.x) {
         const int wc = idx / NJ, j = idx - wc * NJ;
         const int c2 = col0 + wc;
@@ -263,25 +264,41 @@ __device__ __noinline__ void col_hist_bin(const C* tile, double* hsm, int col0, 
                 const C y = tile[(L - j) * W + wc];
                 pw += (double)y.x * y.x + (double)y.y * y.y;
             }
-            const double hfx = (c2 <= ncols / 2) ? __ddiv_rn((double)c2, dnx) : __ddiv_rn((double)(c2 - ncols), dnx);
-            const double fy = __ddiv_rn((double)j, den);
-            double hp = fabs(hfx), hq = fabs(fy);
-            if (hp < hq) { const double t = hp; hp = hq; hq = t; }
-            double hy = 0;
-            if (hp != 0) {
-                const double r = __ddiv_rn(hq, hp);
-                hy = __dmul_rn(hp, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(r, r))));
+            // bin from a single-precision radius (error < 1e-4 of a bin), the
+            // reference's exact FP64 sequence only within 1e-3 of a bin edge
+            const int cf = (c2 <= ncols / 2) ? c2 : c2 - ncols;
+            const float rf = sqrtf(fmaf((float)cf * inv_dnx, (float)cf * inv_dnx,
+                                        ((float)j * inv_den) * ((float)j * inv_den))) * bins_per_f;
+            const float fl = floorf(rf);
+            if (rf - fl > 1e-3f && rf - fl < 1.0f - 1e-3f) {
+                b = (int)fl;
+            } else {
+                const double hfx = __ddiv_rn((double)cf, dnx);
+                const double fy = __ddiv_rn((double)j, den);
+                double hp = fabs(hfx), hq = fabs(fy);
+                if (hp < hq) { const double t = hp; hp = hq; hq = t; }
+                double hy = 0;
+                if (hp != 0) {
+                    const double r = __ddiv_rn(hq, hp);
+                    hy = __dmul_rn(hp, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(r, r))));
+                }
+                b = (int)__dmul_rn(__ddiv_rn(hy, fnyq), 96.0);
             }
-            b = (int)__dmul_rn(__ddiv_rn(hy, fnyq), 96.0);
             b = b > 96 ? 96 : (b < 0 ? 0 : b);
         }
-        const int b0 = __shfl_sync(0xffffffffu, b, 0);
-        if (__all_sync(0xffffffffu, b == b0 || pw == 0)) {
-            for (int o = 16; o > 0; o >>= 1) pw += __shfl_down_sync(0xffffffffu, pw, o);
-            if ((threadIdx.x & 31) == 0 && pw != 0) atomicAdd(&hsm[b0], pw);
-        } else if (pw != 0) {
-            atomicAdd(&hsm[b], pw);
+        // the warp's 32 consecutive j of one column have non-decreasing bins
+        // (|fy| grows with j; lanes past L/2 take the sentinel 97), so runs of
+        // equal bins are contiguous: a segmented scan leaves each run's sum in
+        // its last lane, and one atomic per run (a few per warp) adds it
+        if (!(j <= L / 2 && c2 < ncols)) b = 97;
+        const int lane = threadIdx.x & 31;
+        for (int o = 1; o < 32; o <<= 1) {
+            const double t = __shfl_up_sync(0xffffffffu, pw, o);
+            const int bt = __shfl_up_sync(0xffffffffu, b, o);
+            if (lane >= o && bt == b) pw += t;
         }
+        const int bn = __shfl_down_sync(0xffffffffu, b, 1);
+        if ((lane == 31 || bn != b) && b < 97 && pw != 0) atomicAdd(&hsm[b], pw);
     }
 }
 
