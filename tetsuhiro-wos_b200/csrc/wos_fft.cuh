@@ -85,14 +85,27 @@ __device__ __forceinline__ void dft2(C& a, C& b) {
     b = csub(t, b);
 }
 
+// Butterfly a = e + w x, b = e - w x for w = -i (forward) or +i (inverse):
+// four scalar adds with the swap and sign folded into the operands (the
+// paired add would first have to build the swapped, negated pair).
+template <bool INV, typename C>
+__device__ __forceinline__ void bfly_mi(C& a, C& b, C e, C x) {
+    if (INV) {
+        a = mkc<C>(e.x - x.y, e.y + x.x);
+        b = mkc<C>(e.x + x.y, e.y - x.x);
+    } else {
+        a = mkc<C>(e.x + x.y, e.y - x.x);
+        b = mkc<C>(e.x - x.y, e.y + x.x);
+    }
+}
+
 template <bool INV, typename C>
 __device__ __forceinline__ void dft4(C& v0, C& v1, C& v2, C& v3) {
     C a0 = cadd(v0, v2), a1 = csub(v0, v2);
-    C a2 = cadd(v1, v3), a3 = mul_mi<INV>(csub(v1, v3));
+    C a2 = cadd(v1, v3), d = csub(v1, v3);
     v0 = cadd(a0, a2);
     v2 = csub(a0, a2);
-    v1 = cadd(a1, a3);
-    v3 = csub(a1, a3);
+    bfly_mi<INV>(v1, v3, a1, d);
 }
 
 template <typename C> struct K;
@@ -117,6 +130,45 @@ template <bool INV, typename C> __device__ __forceinline__ C w8_3(C x) {
     return INV ? mkc<C>(-(x.x + x.y) * s, (x.x - x.y) * s) : mkc<C>((x.y - x.x) * s, -(x.x + x.y) * s);
 }
 
+// Butterfly for w = w8^k (k = 1, 3): w x = sqrt(1/2) u with u the sums and
+// differences of x's parts; complex64 takes e +- sqrt(1/2) u as two paired
+// FMAs (fma.rn.f32x2, one rounding per lane), complex128 the products of
+// w8_1 / w8_3 and a sum and a difference.
+template <int k, bool INV, typename C>
+__device__ __forceinline__ void bfly_w8(C& a, C& b, C e, C x) {
+    const C t = k == 1 ? w8_1<INV>(x) : w8_3<INV>(x);
+    a = cadd(e, t);
+    b = csub(e, t);
+}
+#if !defined(WOS_SCALAR_CADD)
+__device__ __forceinline__ float2 f2_fma(float2 s, float2 u, float2 e) {
+    unsigned long long d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2_bits(s)), "l"(f2_bits(u)), "l"(f2_bits(e)));
+    return f2_from(d);
+}
+template <int k, bool INV>
+__device__ __forceinline__ void bfly_w8_f2(float2& a, float2& b, float2 e, float2 x) {
+    float2 u;
+    if (k == 1) u = INV ? make_float2(x.x - x.y, x.x + x.y) : make_float2(x.x + x.y, x.y - x.x);
+    else u = INV ? make_float2(-x.x - x.y, x.x - x.y) : make_float2(x.y - x.x, -x.x - x.y);
+    const float s = K<float2>::S2;
+    a = f2_fma(make_float2(s, s), u, e);
+    b = f2_fma(make_float2(-s, -s), u, e);
+}
+template <> __device__ __forceinline__ void bfly_w8<1, false, float2>(float2& a, float2& b, float2 e, float2 x) {
+    bfly_w8_f2<1, false>(a, b, e, x);
+}
+template <> __device__ __forceinline__ void bfly_w8<1, true, float2>(float2& a, float2& b, float2 e, float2 x) {
+    bfly_w8_f2<1, true>(a, b, e, x);
+}
+template <> __device__ __forceinline__ void bfly_w8<3, false, float2>(float2& a, float2& b, float2 e, float2 x) {
+    bfly_w8_f2<3, false>(a, b, e, x);
+}
+template <> __device__ __forceinline__ void bfly_w8<3, true, float2>(float2& a, float2& b, float2 e, float2 x) {
+    bfly_w8_f2<3, true>(a, b, e, x);
+}
+#endif
+
 template <bool INV, typename C>
 __device__ __forceinline__ void dft8(C* v) {
     // even / odd radix-4 then combine
@@ -124,13 +176,10 @@ __device__ __forceinline__ void dft8(C* v) {
     C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
     dft4<INV>(e0, e1, e2, e3);
     dft4<INV>(o0, o1, o2, o3);
-    o1 = w8_1<INV>(o1);
-    o2 = mul_mi<INV>(o2);
-    o3 = w8_3<INV>(o3);
     v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
-    v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
-    v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
-    v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+    bfly_w8<1, INV>(v[1], v[5], e1, o1);
+    bfly_mi<INV>(v[2], v[6], e2, o2);
+    bfly_w8<3, INV>(v[3], v[7], e3, o3);
 }
 
 // multiply by w16^k (forward w16 = exp(-2 pi i/16)), k = 0..7
@@ -157,11 +206,14 @@ __device__ __forceinline__ void dft16(C* v) {
     for (int i = 0; i < 8; i++) { e[i] = v[2 * i]; o[i] = v[2 * i + 1]; }
     dft8<INV>(e);
     dft8<INV>(o);
-    o[1] = w16<1, INV>(o[1]); o[2] = w16<2, INV>(o[2]); o[3] = w16<3, INV>(o[3]);
-    o[4] = w16<4, INV>(o[4]); o[5] = w16<5, INV>(o[5]); o[6] = w16<6, INV>(o[6]);
-    o[7] = w16<7, INV>(o[7]);
+    o[1] = w16<1, INV>(o[1]); o[3] = w16<3, INV>(o[3]);
+    o[5] = w16<5, INV>(o[5]); o[7] = w16<7, INV>(o[7]);
 #pragma unroll
-    for (int i = 0; i < 8; i++) { v[i] = cadd(e[i], o[i]); v[i + 8] = csub(e[i], o[i]); }
+    for (int i = 0; i < 8; i += 2) { v[i + 1] = cadd(e[i + 1], o[i + 1]); v[i + 9] = csub(e[i + 1], o[i + 1]); }
+    v[0] = cadd(e[0], o[0]); v[8] = csub(e[0], o[0]);
+    bfly_w8<1, INV>(v[2], v[10], e[2], o[2]);
+    bfly_mi<INV>(v[4], v[12], e[4], o[4]);
+    bfly_w8<3, INV>(v[6], v[14], e[6], o[6]);
 }
 
 // Radix 3 and 5 (mixed-radix lines): the DFT sums written with the real and
