@@ -275,7 +275,9 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_acc_fast(const FastR
 // inverse row transform, the screen t(x, y) = border[d] exp(i phase gx gy) at
 // the inverse's natural output positions, which are the forward transform's
 // natural input positions (radix rs both), and the forward row transform, all
-// in registers.  The screen is evaluated in FP64 in both pipelines.
+// in registers.  The screen's phase argument and Gaussian factors are FP64 in
+// both pipelines; complex64 takes sin/cos of the exactly reduced revolution
+// fraction in single precision.
 template <typename Real, int L, int E>
 __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_bpm_fast(const FastRows a) {
     using C = typename CT<Real>::t;
@@ -305,20 +307,38 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_bpm_fast(const FastR
         const double gy = a.bpm_gx ? exp(-((y - a.bpm_y0) * (y - a.bpm_y0)) / a.bpm_w2) : 0.0;
         const double pg = a.bpm_phase * gy;
         const int dr = min(r, a.rows - 1 - r);
+        // complex64: the FP64 phase in revolutions (|gx| <= 1 bounds it by
+        // |pg| / 2 pi, uniform over the row), reduced exactly and turned into
+        // sin/cos in single precision (cexp_rev); complex128, or a phase too
+        // large for the exact reduction: FP64 sincos
+        const double prev = pg * (0.5 / M_PI);
+        const bool rev = sizeof(Real) == 4 && fabs(prev) < 0x1p27;
 #pragma unroll
         for (int s = 0; s < E; s++) {
             const int q = fpos<PL::RS, E, L>(s, tt);
-            double sn = 0, cs = 1;
-            if (a.bpm_gx) sincos(pg * __ldg(a.bpm_gx + q), &sn, &cs);
+            Real sn = 0, cs = 1;
+            if (a.bpm_gx) {
+                const double g = __ldg(a.bpm_gx + q);
+                if (rev) {
+                    const float2 e = cexp_rev(prev * g, true);
+                    cs = (Real)e.x;
+                    sn = (Real)e.y;
+                } else {
+                    double sd, cd;
+                    sincos(pg * g, &sd, &cd);
+                    cs = (Real)cd;
+                    sn = (Real)sd;
+                }
+            }
             if (a.bpm_border) {
                 const int d = min(dr, min(q, a.bpm_nx - 1 - q));
                 if (d < a.bpm_border_px) {
-                    const double b = __ldg(a.bpm_border + d);
+                    const Real b = (Real)__ldg(a.bpm_border + d);
                     sn *= b;
                     cs *= b;
                 }
             }
-            v[s] = cmul(v[s], mkc<C>((Real)cs, (Real)sn));
+            v[s] = cmul(v[s], mkc<C>(cs, sn));
         }
     }
     fpasses<L, E, false, 0, 1>(v, smb, tt, twp);
