@@ -15,6 +15,8 @@
 //   k_cols_fast<Real, L, E>: W adjacent columns per CTA; forward column FFT,
 //       H(fx, fy) of asmTF (optics/propagate.go:159-181) generated on the fly
 //       from an FP64 argument, inverse column FFT, optional spectral loss sums.
+#include <stdlib.h>
+
 #include <cooperative_groups.h>
 
 #include "wos_fast_dev.cuh"
@@ -29,6 +31,8 @@ namespace cg = cooperative_groups;
 // 2048^2 sweep.)
 template <typename Real, int L, int E, bool INV>
 __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows a) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename CT<Real>::t;
     using PL = FPlan<L, E>;
     constexpr int T = PL::T;
@@ -280,6 +284,8 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_acc_fast(const FastR
 // fraction in single precision.
 template <typename Real, int L, int E>
 __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_bpm_fast(const FastRows a) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename CT<Real>::t;
     using PL = FPlan<L, E>;
     constexpr int T = PL::T;
@@ -352,6 +358,8 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_bpm_fast(const FastR
 template <typename Real, int L, int E, int W>
 __global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, E, W>::minb)
     k_cols_fast(const FastCols a) {
+    pdl_wait();
+    pdl_trigger();
     using C = typename CT<Real>::t;
     using PL = FPlan<L, E>;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -610,6 +618,33 @@ cudaError_t fast_build_twiddles(int fp64, int L, int E, void* out, cudaStream_t 
 }
 
 // ------------------------------------------------------------------ launch
+// Sweeps are launched with programmatic stream serialization (the kernels
+// call pdl_wait() before touching memory), so a sweep's CTAs are scheduled
+// while the previous sweep of the stream drains; WOS_PDL=0 launches them as
+// ordinary kernels.
+static bool pdl_enabled() {
+    static const bool on = [] {
+        const char* e = getenv("WOS_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+template <typename A>
+static cudaError_t launch_sweep(void (*k)(A), dim3 grid, int threads, size_t smem, cudaStream_t st, const A& a) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl_enabled() ? 1 : 0;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k, a);
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
 template <typename Real, int L, int E, bool INV>
 static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
@@ -625,8 +660,7 @@ static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
     }
     dim3 grid((a.rows + lines - 1) / lines, a.batch > 0 ? a.batch : 1);
     if (nblocks) *nblocks = (int)(grid.x * grid.y);
-    k_rows_fast<Real, L, E, INV><<<grid, lines * T, smem, st>>>(a);
-    return cudaGetLastError();
+    return launch_sweep(k_rows_fast<Real, L, E, INV>, grid, lines * T, smem, st, a);
 }
 
 template <typename Real, int L, int E>
@@ -643,8 +677,7 @@ static cudaError_t go_rows_bpm(const FastRows& a, cudaStream_t st, int* nblocks)
     }
     dim3 grid((a.rows + lines - 1) / lines, a.batch > 0 ? a.batch : 1);
     if (nblocks) *nblocks = (int)(grid.x * grid.y);
-    k_rows_bpm_fast<Real, L, E><<<grid, lines * T, smem, st>>>(a);
-    return cudaGetLastError();
+    return launch_sweep(k_rows_bpm_fast<Real, L, E>, grid, lines * T, smem, st, a);
 }
 
 template <typename Real, int L, int E>
@@ -706,8 +739,7 @@ static cudaError_t go_cols_w(const FastCols& a, cudaStream_t st, int* nblocks) {
         }
         dim3 grid((a.ncols + W - 1) / W, a.batch > 0 ? a.batch : 1);
         if (nblocks) *nblocks = (int)(grid.x * grid.y);
-        k_cols_fast<Real, L, E, W><<<grid, W * T, smem, st>>>(a);
-        return cudaGetLastError();
+        return launch_sweep(k_cols_fast<Real, L, E, W>, grid, W * T, smem, st, a);
     }
 }
 

@@ -10,6 +10,17 @@
 
 namespace wos {
 
+// Programmatic dependent launch.  A sweep launched with the programmatic
+// stream-serialization attribute may become resident while the kernel before
+// it in the stream is still draining; pdl_wait() blocks (in hardware, not a
+// spin loop) until that grid has completed and its writes are visible, and is
+// a no-op for an ordinary launch.  Every kernel that a launcher may start with
+// the attribute calls it before its first global-memory access.
+// pdl_trigger() then lets the next sweep of the stream be scheduled; that
+// grid's own pdl_wait() still waits for this one to complete.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 template <int N> struct Log2 { static constexpr int v = 1 + Log2<N / 2>::v; };
 template <> struct Log2<1> { static constexpr int v = 0; };
 
