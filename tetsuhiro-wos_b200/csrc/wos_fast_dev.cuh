@@ -70,7 +70,14 @@ __device__ __forceinline__ double2 ldg_keep(const double2* p) {
 }
 
 // Twiddles of one Stockham DIT pass (radix R, sub-transform length NS) for
-// this thread's E/R butterflies, [b][r-1]; none when NS == 1.
+// this thread's E/R butterflies, [b][r-1] = W^(r k); none when NS == 1.
+// Complex64 passes of radix 8 and 16 load only W^k, W^2k, W^4k (and W^8k);
+// ftw_expand forms the others as products once the loads have landed (after
+// the exchange barrier), at most three roundings deep: four global loads and
+// eleven complex products per radix-16 butterfly instead of fifteen loads.
+template <int R, typename C> struct FtwPow2 {
+    static constexpr bool v = sizeof(C) == 8 && (R == 8 || R == 16);
+};
 template <int R, int E, int L, int NS, int TWOFF, typename C>
 __device__ __forceinline__ void ftw_load(C* w, int tt, const C* __restrict__ twp) {
     constexpr int T = L / E;
@@ -79,7 +86,25 @@ __device__ __forceinline__ void ftw_load(C* w, int tt, const C* __restrict__ twp
         for (int b = 0; b < E / R; b++) {
             const C* tk = twp + TWOFF + ((tt + b * T) & (NS - 1));
 #pragma unroll
-            for (int r = 1; r < R; r++) w[b * (R - 1) + r - 1] = ldg_keep(tk + (r - 1) * NS);
+            for (int r = 1; r < R; r++)
+                if (!FtwPow2<R, C>::v || (r & (r - 1)) == 0) w[b * (R - 1) + r - 1] = ldg_keep(tk + (r - 1) * NS);
+        }
+    }
+}
+template <int R, int E, int NS, typename C>
+__device__ __forceinline__ void ftw_expand(C* w) {
+    if constexpr (NS > 1 && FtwPow2<R, C>::v) {
+#pragma unroll
+        for (int b = 0; b < E / R; b++) {
+            C* p = w + b * (R - 1);  // p[r - 1] = W^(r k)
+            p[2] = cmul(p[0], p[1]);
+            p[4] = cmul(p[0], p[3]);
+            p[5] = cmul(p[1], p[3]);
+            p[6] = cmul(p[2], p[3]);
+            if constexpr (R == 16) {
+#pragma unroll
+                for (int r = 1; r < 8; r++) p[r + 7] = cmul(p[r - 1], p[7]);
+            }
         }
     }
 }
@@ -159,6 +184,7 @@ __device__ __forceinline__ void fpasses_from(C* v, C* smb, int tt, const C* __re
             ftw_load<R2, E, L, NS2, TWOFF2>(wn, tt, twp);
             __syncthreads();
             fload<R2, E, L, SH, STR>(v, smb, tt);
+            ftw_expand<R2, E, NS2>(wn);
             fpasses_from<L, E, INV, p + 1, STR>(v, smb, tt, twp, wn);
         }
     }
