@@ -159,11 +159,26 @@ __device__ __forceinline__ void fload(C* v, const C* smb, int tt) {
     }
 }
 
+// Padding period 2^SH of the exchange after a radix-R pass.  By default the
+// storing radix (SH = log2 R), which keeps every store conflict-free.  Complex64
+// rows (STR == 1) take at least 16 positions where the pass strides allow it:
+// the next pass's loads are 16 consecutive 64-bit words per half-warp, which a
+// pad every 8 positions (radix 8) puts twice on one bank pair; with a pad every
+// 16 they land on 16 distinct pairs, and the stores of a radix 2, 4 or 8 pass
+// stay conflict-free.  (Complex128 keeps log2 R: its 16-byte slots conflict on
+// the store side with a period of 16.)
+template <int L, int R, int NS, int R2, int STR, typename C>
+__host__ __device__ constexpr int fx_shift() {
+    constexpr int s = Log2<R>::v;
+    if (sizeof(C) == 8 && STR == 1 && s < 4 && (L / R2) % 16 == 0 && (NS >= 16 || NS == 1 || NS * R >= 16)) return 4;
+    return s;
+}
+
 // All passes from p on; wcur holds pass p's twiddles.  Each exchange has its
-// own padding period, the radix of the pass that stores (SH = log2 R): for
-// every power-of-two line stride W that makes the store of each pass
-// conflict-free, and the natural-order load of the next pass stays a
-// per-thread base plus immediates.  The next pass's twiddles are requested
+// own padding period (fx_shift: the radix of the pass that stores, or 16 for
+// complex64 rows): for every power-of-two line stride W that makes the store
+// of each pass conflict-free, and the natural-order load of the next pass
+// stays a per-thread base plus immediates.  The next pass's twiddles are requested
 // once this thread's stores are issued (the data registers are free then), so
 // their latency runs under the barrier.
 template <int L, int E, bool INV, int p, int STR, typename C>
@@ -177,7 +192,7 @@ __device__ __forceinline__ void fpasses_from(C* v, C* smb, int tt, const C* __re
             constexpr int R2 = fp_radix(PL::P, PL::RS, E, INV, p + 1);
             constexpr int NS2 = fp_ns(PL::P, PL::RS, E, INV, p + 1);
             constexpr int TWOFF2 = fp_twoff(PL::P, PL::RS, E, INV, p + 1);
-            constexpr int SH = Log2<R>::v;
+            constexpr int SH = fx_shift<L, R, NS, R2, STR, C>();
             C wn[(E / R2) * (R2 - 1)];
             __syncthreads();
             fstore<R, E, L, NS, SH, STR>(v, smb, tt);
