@@ -700,7 +700,7 @@ template <typename Real, int L, int E>
 static cudaError_t go_rows_acc(const FastRows& a, const AccArgs& acc, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
     int lines = 1;
-    while (lines * 2 * T <= 256 && lines * 2 <= a.rows) lines *= 2;
+    while (lines * 2 * T <= row_cta_target(T) && lines * 2 <= a.rows) lines *= 2;
     while (lines * T < 32) lines *= 2;
     const size_t smem = (size_t)frow_stride(L, E) * lines * sizeof(typename CT<Real>::t);
     if (smem > kSmemNoOptIn) {
@@ -718,7 +718,7 @@ template <typename Real, int L, int E, int STAGE>
 static cudaError_t go_rows_design(const FastRows& a, const DesignArgs& d, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
     int lines = 1;
-    while (lines * 2 * T <= 256 && lines * 2 <= a.rows) lines *= 2;
+    while (lines * 2 * T <= row_cta_target(T) && lines * 2 <= a.rows) lines *= 2;
     while (lines * T < 32) lines *= 2;
     const size_t smem = (size_t)frow_stride(L, E) * lines * sizeof(typename CT<Real>::t);
     if (smem > kSmemNoOptIn) {
