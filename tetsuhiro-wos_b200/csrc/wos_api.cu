@@ -594,10 +594,7 @@ Tune get_tune(wos_ctx c, int ny, int nx) {
 }
 
 size_t fast_row_blocks(int L, int E, int rows, int batch) {
-    const int T = L / E;
-    int lines = 1;
-    while (lines * 2 * T <= 256 && lines * 2 <= rows) lines *= 2;
-    while (lines * T < 32) lines *= 2;
+    const int lines = fast_row_lines(L, E, rows);
     return (size_t)((rows + lines - 1) / lines) * std::max(batch, 1);
 }
 // (an upper bound: the split tiles of fast_cols_pair launch two CTAs per tile)

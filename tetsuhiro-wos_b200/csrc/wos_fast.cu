@@ -646,6 +646,17 @@ static int row_cta_target(int T) {
     return T <= 32 ? 128 : 64;
 }
 
+// Lines per CTA of the fast row sweeps: grouped up to row_cta_target
+// threads, at least one warp.  The host sizes the per-CTA reduction records
+// from this count (fast_row_blocks), so every row launcher takes it from here.
+int fast_row_lines(int L, int E, int rows) {
+    const int T = L / E;
+    int lines = 1;
+    while (lines * 2 * T <= row_cta_target(T) && lines * 2 <= rows) lines *= 2;
+    while (lines * T < 32) lines *= 2;
+    return lines;
+}
+
 template <typename A>
 static cudaError_t launch_sweep(void (*k)(A), dim3 grid, int threads, size_t smem, cudaStream_t st, const A& a) {
     cudaLaunchConfig_t cfg = {};
@@ -664,9 +675,7 @@ static cudaError_t launch_sweep(void (*k)(A), dim3 grid, int threads, size_t sme
 template <typename Real, int L, int E, bool INV>
 static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
-    int lines = 1;
-    while (lines * 2 * T <= row_cta_target(T) && lines * 2 <= a.rows) lines *= 2;
-    while (lines * T < 32) lines *= 2;
+    const int lines = fast_row_lines(L, E, a.rows);
     if (lines * T > FMaxT<Real, E>::v) return cudaErrorInvalidConfiguration;
     const size_t smem = (size_t)frow_stride(L, E) * lines * sizeof(typename CT<Real>::t);
     if (smem > kSmemNoOptIn) {
@@ -682,9 +691,7 @@ static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
 template <typename Real, int L, int E>
 static cudaError_t go_rows_bpm(const FastRows& a, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
-    int lines = 1;
-    while (lines * 2 * T <= row_cta_target(T) && lines * 2 <= a.rows) lines *= 2;
-    while (lines * T < 32) lines *= 2;
+    const int lines = fast_row_lines(L, E, a.rows);
     const size_t smem = (size_t)frow_stride(L, E) * lines * sizeof(typename CT<Real>::t);
     if (smem > kSmemNoOptIn) {
         cudaError_t e = cudaFuncSetAttribute(k_rows_bpm_fast<Real, L, E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -699,9 +706,7 @@ static cudaError_t go_rows_bpm(const FastRows& a, cudaStream_t st, int* nblocks)
 template <typename Real, int L, int E>
 static cudaError_t go_rows_acc(const FastRows& a, const AccArgs& acc, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
-    int lines = 1;
-    while (lines * 2 * T <= row_cta_target(T) && lines * 2 <= a.rows) lines *= 2;
-    while (lines * T < 32) lines *= 2;
+    const int lines = fast_row_lines(L, E, a.rows);
     const size_t smem = (size_t)frow_stride(L, E) * lines * sizeof(typename CT<Real>::t);
     if (smem > kSmemNoOptIn) {
         cudaError_t e = cudaFuncSetAttribute(k_rows_acc_fast<Real, L, E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -717,9 +722,7 @@ static cudaError_t go_rows_acc(const FastRows& a, const AccArgs& acc, cudaStream
 template <typename Real, int L, int E, int STAGE>
 static cudaError_t go_rows_design(const FastRows& a, const DesignArgs& d, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
-    int lines = 1;
-    while (lines * 2 * T <= row_cta_target(T) && lines * 2 <= a.rows) lines *= 2;
-    while (lines * T < 32) lines *= 2;
+    const int lines = fast_row_lines(L, E, a.rows);
     const size_t smem = (size_t)frow_stride(L, E) * lines * sizeof(typename CT<Real>::t);
     if (smem > kSmemNoOptIn) {
         cudaError_t e = cudaFuncSetAttribute(k_rows_design<Real, L, E, STAGE>,

@@ -124,4 +124,6 @@ int fast_table_len(int L, int E);
 cudaError_t fast_build_twiddles(int fp64, int L, int E, void* out, cudaStream_t st);
 size_t fast_col_smem(int fp64, int L, int E, int W);
 int fast_col_width(int fp64, int L, int E, int W);
+// lines per CTA of the fast row sweeps (the launchers and the record sizing share it)
+int fast_row_lines(int L, int E, int rows);
 }  // namespace wos
