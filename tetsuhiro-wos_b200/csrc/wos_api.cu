@@ -586,9 +586,9 @@ Tune get_tune(wos_ctx c, int ny, int nx) {
     auto it = c->tune.find(tune_key(c->fp64, ny, nx));
     if (it != c->tune.end()) return it->second;
     Tune t;
-    // complex64 1024-point rows: E = 8 (two threads' worth of parallelism per
-    // value; 1024^2 split-step runs 9.45 -> 8.90 ms); 512 and 2048 points are
-    // faster with E = 16 (12.3 vs 16.1 us and 20.3k vs 17.8k props/s)
+    // complex64 1024-point rows: E = 8, twice the threads per line of E = 16
+    // (1024^2 split-step runs 9.45 -> 8.89 ms); 512 and 2048 points are faster
+    // with E = 16 (12.3 vs 16.1 us per propagation, 20.3k vs 17.8k props/s)
     t.rowE = env_int("WOS_ROWE", c->fp64 ? (nx >= 8192 ? 16 : 8) : (nx == 1024 ? 8 : 16));
     t.colE = env_int("WOS_COLE", c->fp64 ? (ny >= 8192 ? 16 : 8) : 16);
     t.colW = env_int("WOS_COLW", c->fp64 ? 2 : 8);
