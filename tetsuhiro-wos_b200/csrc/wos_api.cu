@@ -83,6 +83,7 @@ struct Axis {
     void* bf = nullptr;
     void* bi = nullptr;
     void* ftw[2] = {nullptr, nullptr};  // per-pass twiddles of the specialised sweeps (E = 8, 16)
+    void* ftw_lo[2] = {nullptr, nullptr};  // their complex64 residuals (compensated split-step sweeps)
     void* ptw = nullptr;                // W_L^n, n < L/2: split column tiles
 };
 
@@ -115,6 +116,20 @@ struct wos_ctx_s {
     DevBuf bpm_tab;                     // split-step tables (core profile, border absorption) on the device
     std::vector<double> bpm_tab_host;   // ... and their host copy, to skip identical uploads
     int tiled = 0;                      // three-sweep ASM through the tiled intermediate (FastRows::out_tiled)
+    int bpm_comp = 1;                   // complex64 split-step slices on the compensated transforms (WOS_BPM_COMP=0: off)
+    // transfer-function tables of the complex64 column sweep (FastCols::htab),
+    // keyed by grid and H parameters; a few slots, reused round robin (a
+    // slot is rebuilt on the context stream, after the work that read it)
+    struct HTab {
+        bool valid = false;
+        int L = 0, ncols = 0;
+        double key[9] = {};
+        DevBuf buf;
+    };
+    static constexpr int kHTabs = 4;
+    HTab htab[kHTabs];
+    int htab_next = 0;
+    int htab_on = 1;                    // WOS_HTAB=0: evaluate H in the sweep
     unsigned* err_dev = nullptr;        // error word of the pipelined kernels (device)
     unsigned* err_host = nullptr;       // pinned mirror, read where the host synchronises
     // streams for independent fields of a batch (wos_propagate_batch_dev),
@@ -619,6 +634,51 @@ int fast_tw(wos_ctx c, Axis* a, int E, const void** out) {
     *out = a->ftw[slot];
     return WOS_OK;
 }
+// Residual table of the complex64 per-pass twiddles (compensated sweeps).
+int fast_tw_lo(wos_ctx c, Axis* a, int E, const void** out) {
+    const int slot = E == 16 ? 1 : 0;
+    if (!a->ftw_lo[slot]) {
+        CK(cudaMalloc(&a->ftw_lo[slot], (size_t)fast_table_len(a->L, E) * sizeof(float2)));
+        CK(fast_build_twiddles_lo(a->L, E, a->ftw_lo[slot], c->st));
+    }
+    *out = a->ftw_lo[slot];
+    return WOS_OK;
+}
+
+// Transfer-function table of a complex64 column sweep (FastCols::htab) for
+// columns of L points, when the sweep can use one: no loss sums, one
+// wavelength and distance, W columns per CTA dividing ncols / 2, and the table
+// rows fitting beside the tile in shared memory.  Sets k.htab / k.htab_ld
+// (left null otherwise); the entries are hi + lo pairs when the sweep runs the
+// compensated transforms (k.tw_lo set).
+int attach_htab(wos_ctx c, FastCols& k, int L, int E) {
+    if (c->fp64 || !c->htab_on || k.red || k.batch_wl || k.batch_z || L < 32) return WOS_OK;
+    const int W = fast_col_width(0, L, E, k.tiled ? kTileW : k.W);
+    const int ld = htab_ld_for(L);
+    if (W < 1 || k.ncols < 2 * W || k.ncols % (2 * W) != 0) return WOS_OK;
+    const int hilo = k.tw_lo != nullptr;
+    if (fast_col_smem_htab(L, E, W, ld, hilo) + 2048 > 227 * 1024) return WOS_OK;
+    const double key[9] = {k.wl, k.dx, k.kz, k.kaz, k.scale, k.alpha, k.limit, (double)k.zero_ev,
+                           (double)(k.reg + 2 * k.backward + 4 * hilo)};
+    for (auto& h : c->htab)
+        if (h.valid && h.L == L && h.ncols == k.ncols && std::memcmp(h.key, key, sizeof key) == 0) {
+            k.htab = reinterpret_cast<const float2*>(h.buf.p);
+            k.htab_ld = ld;
+            return WOS_OK;
+        }
+    wos_ctx_s::HTab& h = c->htab[c->htab_next];
+    c->htab_next = (c->htab_next + 1) % wos_ctx_s::kHTabs;
+    h.valid = false;
+    TRY(ensure(h.buf, (size_t)(k.ncols / 2 + 1) * ld * sizeof(float2) * (hilo ? 2 : 1)));
+    CK(fast_build_htab(k, L, reinterpret_cast<float2*>(h.buf.p), ld, hilo, c->st));
+    h.valid = true;
+    h.L = L;
+    h.ncols = k.ncols;
+    std::memcpy(h.key, key, sizeof key);
+    k.htab = reinterpret_cast<const float2*>(h.buf.p);
+    k.htab_ld = ld;
+    return WOS_OK;
+}
 
 // Plain band-limited ASM on power-of-two grids through the specialised
 // sweeps.  Returns -1 when the grid is not covered (the general sweeps run).
@@ -653,7 +713,8 @@ bool pair_tables(wos_ctx c, int L, int E, const void** twh, const void** twp) {
     return true;
 }
 bool pair_eligible(wos_ctx c, int L, int E, const FastCols& a) {
-    return c->col_pair && !a.hist && !a.tiled && fast_cols_pair_case(c->fp64, L, E, fast_col_width(c->fp64, L, E, a.W));
+    return c->col_pair && !a.hist && !a.tiled && !a.tw_lo && !a.htab &&
+           fast_cols_pair_case(c->fp64, L, E, fast_col_width(c->fp64, L, E, a.W));
 }
 
 cudaError_t sweep_cols(wos_ctx c, int L, int E, const FastCols& a, int* nb) {
@@ -664,13 +725,36 @@ cudaError_t sweep_cols(wos_ctx c, int L, int E, const FastCols& a, int* nb) {
             if (e != cudaErrorNotSupported) return e;
         }
     }
-    if (c->sweep_mode != 2 && !a.tiled) {
+    if (c->sweep_mode != 2 && !a.tiled && !a.tw_lo && !a.htab) {  // (table / compensated: one-shot kernels)
         FastCols b = a;
         b.err = c->err_dev;
         const cudaError_t e = pipe_cols(c->fp64, L, E, b, c->st, nb);
         if (e != cudaErrorNotSupported) return e;
     }
     return fast_cols(c->fp64, L, E, a, c->st, nb);
+}
+
+// The transfer-function fields of a specialised column sweep from the H of a
+// plain ASM step.
+void fill_asm_h(FastCols& k, const HArgs& h) {
+    k.wl = h.wl;
+    k.dx = h.dx;
+    k.kz = h.kz;
+    k.kaz = h.kaz;
+    k.scale = h.scale;
+    k.alpha = h.alpha;
+    k.limit = h.limit;
+    k.zero_ev = h.zero_ev;
+    k.reg = h.reg;
+    k.backward = h.z < 0;
+    k.conj = h.conj;
+    k.krev = h.kz / (2 * M_PI);
+}
+
+// Whether the three-sweep ASM of an ny x nx grid goes through the tiled
+// intermediate (complex64: contiguous column tiles of kTileW).
+bool asm_tiled(wos_ctx c, int ny, int nx, const Tune& t) {
+    return c->tiled && !c->fp64 && nx % kTileW == 0 && fast_col_width(c->fp64, ny, t.colE, kTileW) == kTileW;
 }
 
 int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
@@ -689,8 +773,7 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     // tiled intermediate (FP32): the column sweep reads contiguous tiles of
     // kTileW columns; the intermediate is then a buffer of its own (the last
     // sweep changes the layout, so it cannot run in place in the output)
-    const bool tiled = c->tiled && !c->fp64 && p.nx % kTileW == 0 &&
-                       fast_col_width(c->fp64, p.ny, t.colE, kTileW) == kTileW;
+    const bool tiled = asm_tiled(c, p.ny, p.nx, t);
     void* S;
     if (p.out_c128) {
         TRY(ensure(c->scratch, (size_t)np * p.ncomp * c->csz()));
@@ -733,24 +816,14 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     k.bstride = np;
     k.tw = twy;
     k.batch = p.ncomp;
-    k.wl = s.h.wl;
-    k.dx = s.h.dx;
-    k.kz = s.h.kz;
-    k.kaz = s.h.kaz;
-    k.scale = s.h.scale;
-    k.alpha = s.h.alpha;
-    k.limit = s.h.limit;
-    k.zero_ev = s.h.zero_ev;
-    k.reg = s.h.reg;
-    k.backward = s.h.z < 0;
-    k.conj = s.h.conj;
-    k.krev = s.h.kz / (2 * M_PI);
+    fill_asm_h(k, s.h);
     k.red = s.red_loss ? red_region(c, 1) + RS_SW : nullptr;
     k.red_stride = RS_COUNT;
     if (s.hist) {
         k.hist = red_region(c, 1) + RS_HIST;
         k.hist_dx = p.dx;
     }
+    TRY(attach_htab(c, k, p.ny, t.colE));
     CK(timed_launch(c, 4, [&] { return sweep_cols(c, p.ny, t.colE, k, &nb); }));
     if (s.red_loss) CK(launch_reduce_finish(red_region(c, 1), nb, 1, RS_SW, 2, redout_region(c, 1), c->st));
     if (s.hist) CK(launch_reduce_finish(red_region(c, 1), nb, 1, RS_HIST, 97, redout_region(c, 1), c->st));
@@ -1345,6 +1418,8 @@ int wos_ctx_create(int device, int precision, wos_ctx* out) {
     *c->err_host = 0;
     c->col_pair = env_int("WOS_COLPAIR", 0);
     c->tiled = env_int("WOS_TILED", 1);
+    c->bpm_comp = env_int("WOS_BPM_COMP", 1);
+    c->htab_on = env_int("WOS_HTAB", 1);
     *out = c;
     return WOS_OK;
 }
@@ -1363,8 +1438,12 @@ int wos_ctx_destroy(wos_ctx c) {
                 if (kv.second.bi) cudaFree(kv.second.bi);
                 for (void* t : kv.second.ftw)
                     if (t) cudaFree(t);
+                for (void* t : kv.second.ftw_lo)
+                    if (t) cudaFree(t);
                 if (kv.second.ptw) cudaFree(kv.second.ptw);
             }
+        for (auto& h : c->htab)
+            if (h.buf.p) cudaFree(h.buf.p);
         DevBuf* bufs[] = {&c->stage, &c->scratch, &c->scratch2, &c->scratch3, &c->red, &c->redout, &c->tmp,
                           &c->maps, &c->params, &c->vol, &c->accum, &c->aux};
         for (DevBuf* b : bufs)
@@ -1580,6 +1659,13 @@ int wos_propagate_batch_dev(wos_ctx c, int nfields, int ny, int nx, double dx, i
                 const void *th, *tp;
                 if (!pair_tables(c, ny, t.colE, &th, &tp)) return fail(WOS_CUDA_ERROR, "split-tile tables");
             }
+            // the transfer-function table the fields' column sweeps will look up
+            FastCols hk{};
+            hk.ncols = nx;
+            hk.W = t.colW;
+            hk.tiled = asm_tiled(c, ny, nx, t);
+            fill_asm_h(hk, asm_h(c, cc, z, ev_policy(cc, z), dx, nx, ny));
+            TRY(attach_htab(c, hk, ny, t.colE));
             nstreams = std::max(1, std::min(wos_ctx_s::kMaxAux, env_int("WOS_STREAMS", 2)));
         }
     }
@@ -1804,9 +1890,19 @@ int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const vo
     Axis *ax, *ay;
     TRY(get_axis(c, nx, c->fp64, &ax));
     TRY(get_axis(c, ny, c->fp64, &ay));
+    // complex64: the slice sweeps run the compensated transforms (hi + lo
+    // twiddles), whose error does not add up over the slices; their column
+    // sweep holds 8 values per thread (16 with the residual twiddles spill)
+    const bool comp = !c->fp64 && c->bpm_comp;
+    const int colE = (comp && t.colE == 16 && fast_supported(0, ny, 8)) ? 8 : t.colE;
     const void *twx, *twy;
     TRY(fast_tw(c, ax, t.rowE, &twx));
-    TRY(fast_tw(c, ay, t.colE, &twy));
+    TRY(fast_tw(c, ay, colE, &twy));
+    const void *twx_lo = nullptr, *twy_lo = nullptr;
+    if (comp) {
+        TRY(fast_tw_lo(c, ax, t.rowE, &twx_lo));
+        TRY(fast_tw_lo(c, ay, colE, &twy_lo));
+    }
     const long long np = (long long)ny * nx;
     void* S;
     if (!out_c128) {
@@ -1866,6 +1962,7 @@ int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const vo
     kc.zero_ev = pol.zero;
     kc.precise_phase = 1;
     kc.conj = adjoint;
+    kc.tw_lo = twy_lo;
     const double sgn = adjoint ? -1.0 : 1.0;
     FastRows m = r;
     m.in = S;
@@ -1877,13 +1974,22 @@ int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const vo
     m.bpm_border = bpx ? gx + nx : nullptr;
     m.bpm_border_px = bpx;
     m.bpm_nx = nx;
-    double c_logamp = 0, c_phase = 0;  // product of the slice constants
+    m.tw_lo = twx_lo;
+    // Product of the slice constants c_s, each formed as applyMediumPhase forms
+    // the screen of a background pixel (t = exp(-k Im n dz) cexpI(k (Re n - 1)
+    // dz), optics/medium.go:58-59) and multiplied in FP64 complex arithmetic:
+    // the rounding of every factor is then the reference's own.  (Summing the
+    // slice phases instead lets the rounding of a running sum near 10^3 rad
+    // reach ~1e-11 over 400 slices.)
+    double c_re = 1.0, c_im = 0.0;
     for (int s = 0; s <= steps; s++) {
         const double zp = (s == 0 || s == steps) ? hz : dz;
         kc.kz = k * zp;
         kc.kaz = k * zp;
         kc.krev = kc.kz / (2 * M_PI);
-        CK(timed_launch(c, 4, [&] { return sweep_cols(c, ny, t.colE, kc, &nb); }));
+        kc.htab = nullptr;
+        TRY(attach_htab(c, kc, ny, colE));  // one table for dz, one for the half steps
+        CK(timed_launch(c, 4, [&] { return sweep_cols(c, ny, colE, kc, &nb); }));
         if (s < steps) {
             const int sl = adjoint ? steps - 1 - s : s;
             const double zc = z * (double)sl / (double)steps + dz / 2;
@@ -1897,8 +2003,12 @@ int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const vo
             double mod = 1;
             if (d.zmod_amp != 0) mod = 1.0 + d.zmod_amp * std::sin(2 * M_PI * zc / d.zmod_period + d.zmod_phase);
             m.bpm_phase = sgn * (k * d.core_dn * mod * dz);
-            c_phase += sgn * (k * (r0 - 1.0) * dz);
-            c_logamp += -k * i0 * dz;
+            const double ph = k * (r0 - 1.0) * dz;
+            const double am = std::exp(-k * i0 * dz);
+            const double tr = am * std::cos(ph), ti = sgn * (am * std::sin(ph));
+            const double nr = c_re * tr - c_im * ti, ni = c_re * ti + c_im * tr;
+            c_re = nr;
+            c_im = ni;
             CK(timed_launch(c, 0, [&] { return fast_rows_bpm(c->fp64, nx, t.rowE, m, c->st, &nb); }));
         }
     }
@@ -1907,10 +2017,8 @@ int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const vo
     q.in_c128 = 0;
     q.out = out;
     q.out_c128 = out_c128;
-    const double ca = std::exp(c_logamp), cp = std::remainder(c_phase, 2 * M_PI);
-    q.out_scale = ca * std::cos(cp);
-    q.out_scale_im = ca * std::sin(cp);
-    if (q.out_scale_im == 0.0 && q.out_scale == 1.0) q.out_scale_im = 0.0;
+    q.out_scale = c_re;
+    q.out_scale_im = c_im;
     CK(timed_launch(c, 1, [&] { return fast_rows(c->fp64, nx, t.rowE, true, q, c->st, &nb); }));
     return WOS_OK;
 }

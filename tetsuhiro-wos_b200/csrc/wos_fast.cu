@@ -19,7 +19,7 @@
 
 #include <cooperative_groups.h>
 
-#include "wos_fast_dev.cuh"
+#include "wos_fast_kern.cuh"
 
 namespace wos {
 
@@ -275,133 +275,6 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_acc_fast(const FastR
     }
 }
 
-// One split-step slice on a row (optics/medium.go:50-65 for the screen): the
-// inverse row transform, the screen t(x, y) = border[d] exp(i phase gx gy) at
-// the inverse's natural output positions, which are the forward transform's
-// natural input positions (radix rs both), and the forward row transform, all
-// in registers.  The screen's phase argument and Gaussian factors are FP64 in
-// both pipelines; complex64 takes sin/cos of the exactly reduced revolution
-// fraction in single precision.
-template <typename Real, int L, int E>
-__global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_bpm_fast(const FastRows a) {
-    pdl_wait();
-    pdl_trigger();
-    using C = typename CT<Real>::t;
-    using PL = FPlan<L, E>;
-    constexpr int T = PL::T;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    const int lines = blockDim.x / T;
-    const int line = threadIdx.x / T, tt = threadIdx.x - line * T;
-    C* smb = reinterpret_cast<C*>(smraw) + line * frow_stride(L, E);
-    const int r = blockIdx.x * lines + line;
-    const bool act = r < a.rows;
-    const C* twp = reinterpret_cast<const C*>(a.tw);
-    const long long ib = (long long)blockIdx.y * a.in_bstride + (long long)r * a.in_ld;
-    const long long ob = (long long)blockIdx.y * a.out_bstride + (long long)r * a.out_ld;
-    C v[E];
-    if (act) {
-        const C* in = reinterpret_cast<const C*>(a.in) + ib + tt;
-#pragma unroll
-        for (int s = 0; s < E; s++) v[s] = __ldcs(in + fpos<E, E, L>(s, 0));
-    } else {
-#pragma unroll
-        for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
-    }
-    fpasses<L, E, true, 0, 1>(v, smb, tt, twp);
-    if (act) {
-        const double y = ((double)r - (double)a.rows / 2) * a.bpm_dx;
-        const double gy = a.bpm_gx ? exp(-((y - a.bpm_y0) * (y - a.bpm_y0)) / a.bpm_w2) : 0.0;
-        const double pg = a.bpm_phase * gy;
-        const int dr = min(r, a.rows - 1 - r);
-        // complex64: the FP64 phase in revolutions (|gx| <= 1 bounds it by
-        // |pg| / 2 pi, uniform over the row), reduced exactly and turned into
-        // sin/cos in single precision (cexp_rev); complex128, or a phase too
-        // large for the exact reduction: FP64 sincos
-        const double prev = pg * (0.5 / M_PI);
-        const bool rev = sizeof(Real) == 4 && fabs(prev) < 0x1p27;
-#pragma unroll
-        for (int s = 0; s < E; s++) {
-            const int q = fpos<PL::RS, E, L>(s, tt);
-            Real sn = 0, cs = 1;
-            if (a.bpm_gx) {
-                const double g = __ldg(a.bpm_gx + q);
-                if (rev) {
-                    const float2 e = cexp_rev(prev * g, true);
-                    cs = (Real)e.x;
-                    sn = (Real)e.y;
-                } else {
-                    double sd, cd;
-                    sincos(pg * g, &sd, &cd);
-                    cs = (Real)cd;
-                    sn = (Real)sd;
-                }
-            }
-            if (a.bpm_border) {
-                const int d = min(dr, min(q, a.bpm_nx - 1 - q));
-                if (d < a.bpm_border_px) {
-                    const Real b = (Real)__ldg(a.bpm_border + d);
-                    sn *= b;
-                    cs *= b;
-                }
-            }
-            v[s] = cmul(v[s], mkc<C>(cs, sn));
-        }
-    }
-    fpasses<L, E, false, 0, 1>(v, smb, tt, twp);
-    if (act) {
-        C* out = reinterpret_cast<C*>(a.out) + ob + tt;
-#pragma unroll
-        for (int s = 0; s < E; s++) out[fpos<E, E, L>(s, 0)] = v[s];
-    }
-}
-
-template <typename Real, int L, int E, int W>
-__global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, E, W>::minb)
-    k_cols_fast(const FastCols a) {
-    pdl_wait();
-    pdl_trigger();
-    using C = typename CT<Real>::t;
-    using PL = FPlan<L, E>;
-    extern __shared__ __align__(16) unsigned char smraw[];
-    const int w = threadIdx.x & (W - 1);
-    const int tt = threadIdx.x / W;
-    C* smb = reinterpret_cast<C*>(smraw) + w;
-    const int col = blockIdx.x * W + w;
-    const bool act = col < a.ncols;
-    const C* twp = reinterpret_cast<const C*>(a.tw);
-    // strided columns, or one contiguous block per tile in the tiled layout (ld == W)
-    const long long coff = a.tiled ? (long long)blockIdx.x * L * W + w : (long long)col;
-    C* base = reinterpret_cast<C*>(a.data) + (long long)blockIdx.y * a.bstride + coff;
-    const C* sbase = a.src ? reinterpret_cast<const C*>(a.src) + (long long)blockIdx.y * a.src_bstride + coff : base;
-    __shared__ double hsm[97];
-    if (a.hist)
-        for (int k = threadIdx.x; k < 97; k += blockDim.x) hsm[k] = 0;
-    C v[E];
-    constexpr int R1 = PL::RS;
-    if (act) {
-        const C* src = sbase + (long long)tt * a.ld;
-#pragma unroll
-        for (int s = 0; s < E; s++) v[s] = __ldcs(src + (long long)fpos<R1, E, L>(s, 0) * a.ld);
-    } else {
-#pragma unroll
-        for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
-    }
-    // interleaved tile: stride W between consecutive positions of a column
-    fpasses<L, E, false, 0, W>(v, smb, tt, twp);
-
-    double p0 = 0, l1 = 0;
-    col_spectral_stage<Real, L, E, W>(v, reinterpret_cast<C*>(smraw), hsm, blockIdx.x * W, a, h_unit(a, blockIdx.y),
-                                      p0, l1);
-    fpasses<L, E, true, 0, W>(v, smb, tt, twp);
-    if (act) {
-        constexpr int RO = PL::RS;
-        C* dst = base + (long long)tt * a.ld;
-#pragma unroll
-        for (int s = 0; s < E; s++) dst[(long long)fpos<RO, E, L>(s, 0) * a.ld] = v[s];
-    }
-    col_write_red(a, (long long)blockIdx.y * gridDim.x + blockIdx.x, p0, l1, hsm);
-}
-
 // ------------------------------------------------------------- split tiles
 // H on the half spectrum a CTA of a pair holds: local index k of rank r is the
 // frequency q = 2k + r.  The partner of q, L - q, is local LH - k (rank 0; k = 0
@@ -578,6 +451,74 @@ cudaError_t fast_build_pair_twiddles(int fp64, int L, void* out, cudaStream_t st
 }
 
 // ------------------------------------------------------------------ tables
+// Quarter-plane table of the complex64 transfer function: entry [c][q] =
+// scale * H(|fx_c|, |fy_q|) of asmTF (optics/propagate.go:159-181) evaluated
+// in FP64 in the reference's operation order (h_f64) and rounded once; hilo:
+// entries are (H_hi, H_lo) float4 pairs, H_lo = (float)(H - H_hi), for the
+// compensated sweeps.
+__global__ void k_htab_build(const FastCols a, int L, float2* out, int ld, int hilo) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cx = blockIdx.y;
+    if (q >= ld) return;
+    double2 h = make_double2(0.0, 0.0);
+    if (q <= L / 2) {
+        const HUnit hu{a.wl, a.kz, a.kaz, a.krev};
+        const double fxe = __ddiv_rn((double)cx, __dmul_rn((double)a.ncols, a.dx));
+        const double px = fabs(__dmul_rn(hu.wl, fxe));
+        const double fy = __ddiv_rn((double)q, __dmul_rn((double)L, a.dx));
+        double m2;
+        h = h_f64(a, hu, px, fy, m2);
+    }
+    const float hx = (float)h.x, hy = (float)h.y;
+    if (hilo) {
+        reinterpret_cast<float4*>(out)[(long long)cx * ld + q] =
+            make_float4(hx, hy, (float)(h.x - (double)hx), (float)(h.y - (double)hy));
+    } else {
+        out[(long long)cx * ld + q] = make_float2(hx, hy);
+    }
+}
+
+cudaError_t fast_build_htab(const FastCols& a, int L, float2* out, int ld, int hilo, cudaStream_t st) {
+    FastCols b = a;
+    b.conj = 0;
+    b.batch_wl = nullptr;
+    b.batch_z = nullptr;
+    dim3 grid((ld + 255) / 256, a.ncols / 2 + 1);
+    k_htab_build<<<grid, 256, 0, st>>>(b, L, out, ld, hilo);
+    return cudaGetLastError();
+}
+
+size_t fast_col_smem_htab(int L, int E, int W, int ld, int hilo) {
+    return fcol_htab_off(L, E, W) + (size_t)W * ld * (hilo ? 16 : 8);
+}
+
+// Residuals of the complex64 per-pass table: (float)(W - (double)(float)W).
+__global__ void k_pass_twiddles_lo(float2* out, int off, int NS, int R) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= NS * (R - 1)) return;
+    const int r = i / NS + 1, k = i % NS;
+    double s, c;
+    sincospi(-2.0 * (double)r * (double)k / ((double)NS * (double)R), &s, &c);
+    out[off + i] = make_float2((float)(c - (double)(float)c), (float)(s - (double)(float)s));
+}
+
+cudaError_t fast_build_twiddles_lo(int L, int E, void* out, cudaStream_t st) {
+    int LG = 0, LE = 0;
+    while ((1 << LG) < L) LG++;
+    while ((1 << LE) < E) LE++;
+    const int P = (LG + LE - 1) / LE;
+    const int RS = (LG % LE) ? (1 << (LG % LE)) : E;
+    for (int d = 0; d < 2; d++) {
+        const bool inv = d == 1;
+        for (int p = 1; p < P; p++) {
+            const int NS = fp_ns(P, RS, E, inv, p), R = fp_radix(P, RS, E, inv, p);
+            const int off = fp_twoff(P, RS, E, inv, p);
+            const int n = NS * (R - 1);
+            k_pass_twiddles_lo<<<(n + 255) / 256, 256, 0, st>>>(reinterpret_cast<float2*>(out), off, NS, R);
+        }
+    }
+    return cudaGetLastError();
+}
 // Per-pass twiddles W_{NS R}^{r k} (forward sign), [r-1][k], FP64 -> pipeline type.
 template <typename C>
 __global__ void k_pass_twiddles(C* out, int off, int NS, int R) {
@@ -618,18 +559,6 @@ cudaError_t fast_build_twiddles(int fp64, int L, int E, void* out, cudaStream_t 
 }
 
 // ------------------------------------------------------------------ launch
-// Sweeps are launched with programmatic stream serialization (the kernels
-// call pdl_wait() before touching memory), so a sweep's CTAs are scheduled
-// while the previous sweep of the stream drains; WOS_PDL=0 launches them as
-// ordinary kernels.
-static bool pdl_enabled() {
-    static const bool on = [] {
-        const char* e = getenv("WOS_PDL");
-        return !(e && e[0] == '0');
-    }();
-    return on;
-}
-
 // Threads per row CTA: lines of T threads are grouped up to this size.  Small
 // CTAs spread the lines of a sweep evenly over the SMs and let each CTA finish
 // on its own (1024^2 split-step slices: 9.99 ms per 400-slice run at 256
@@ -657,21 +586,6 @@ int fast_row_lines(int L, int E, int rows) {
     return lines;
 }
 
-template <typename A>
-static cudaError_t launch_sweep(void (*k)(A), dim3 grid, int threads, size_t smem, cudaStream_t st, const A& a) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = dim3(threads, 1, 1);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = pdl_enabled() ? 1 : 0;
-    cudaError_t e = cudaLaunchKernelEx(&cfg, k, a);
-    return e != cudaSuccess ? e : cudaGetLastError();
-}
 template <typename Real, int L, int E, bool INV>
 static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
@@ -686,21 +600,6 @@ static cudaError_t go_rows(const FastRows& a, cudaStream_t st, int* nblocks) {
     dim3 grid((a.rows + lines - 1) / lines, a.batch > 0 ? a.batch : 1);
     if (nblocks) *nblocks = (int)(grid.x * grid.y);
     return launch_sweep(k_rows_fast<Real, L, E, INV>, grid, lines * T, smem, st, a);
-}
-
-template <typename Real, int L, int E>
-static cudaError_t go_rows_bpm(const FastRows& a, cudaStream_t st, int* nblocks) {
-    constexpr int T = L / E;
-    const int lines = fast_row_lines(L, E, a.rows);
-    const size_t smem = (size_t)frow_stride(L, E) * lines * sizeof(typename CT<Real>::t);
-    if (smem > kSmemNoOptIn) {
-        cudaError_t e = cudaFuncSetAttribute(k_rows_bpm_fast<Real, L, E>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-    }
-    dim3 grid((a.rows + lines - 1) / lines, a.batch > 0 ? a.batch : 1);
-    if (nblocks) *nblocks = (int)(grid.x * grid.y);
-    return launch_sweep(k_rows_bpm_fast<Real, L, E>, grid, lines * T, smem, st, a);
 }
 
 template <typename Real, int L, int E>
@@ -744,24 +643,6 @@ static cudaError_t go_rows_design_s(int stage, const FastRows& a, const DesignAr
     }
 }
 
-template <typename Real, int L, int E, int W>
-static cudaError_t go_cols_w(const FastCols& a, cudaStream_t st, int* nblocks) {
-    constexpr int T = L / E;
-    if constexpr (W * T < 32 || W * T > fcol_max_threads(sizeof(Real) == 8, T)) {
-        return cudaErrorInvalidConfiguration;
-    } else {
-        const size_t smem = (size_t)fcol_elems(L, E, W) * sizeof(typename CT<Real>::t);
-        if (smem > kSmemNoOptIn) {
-            cudaError_t e = cudaFuncSetAttribute(k_cols_fast<Real, L, E, W>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-        }
-        dim3 grid((a.ncols + W - 1) / W, a.batch > 0 ? a.batch : 1);
-        if (nblocks) *nblocks = (int)(grid.x * grid.y);
-        return launch_sweep(k_cols_fast<Real, L, E, W>, grid, W * T, smem, st, a);
-    }
-}
-
 template <typename Real, int L, int E>
 static cudaError_t go_cols(const FastCols& a, cudaStream_t st, int* nblocks) {
     switch (fast_col_width(sizeof(Real) == 8, L, E, a.W)) {
@@ -802,6 +683,7 @@ cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaS
 }
 
 cudaError_t fast_cols(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks) {
+    if (!fp64 && a.tw_lo) return fast_cols_cp(L, E, a, st, nblocks);
 #define CASE_C(LL)                                                                  \
     case LL:                                                                        \
         if (fp64) {                                                                 \
@@ -836,6 +718,7 @@ int fast_col_width(int fp64, int L, int E, int W) {
 }
 
 cudaError_t fast_rows_bpm(int fp64, int L, int E, const FastRows& a, cudaStream_t st, int* nblocks) {
+    if (!fp64 && a.tw_lo) return fast_rows_bpm_cp(L, E, a, st, nblocks);
 #define CASE_B(LL)                                                                   \
     case LL:                                                                         \
         if (fp64) {                                                                  \

@@ -33,6 +33,10 @@ struct FastRows {
     // the inverse sweep's load (native complex type only)
     int out_tiled, in_tiled;
     long long tile_len;       // rows of the field (the column length)
+    // residual twiddle table of the compensated transforms (complex64
+    // split-step row sweep): same layout as tw, (float)(W - tw) from FP64; null
+    // for the plain transforms
+    const void* tw_lo;
 };
 constexpr int kTileW = 4;
 
@@ -72,7 +76,35 @@ struct FastCols {
     // table W_L^n for n < L/2 (both null: one CTA per tile)
     const void* tw_half;
     const void* tw_pair;
+    // residual twiddle table of the compensated transforms (complex64
+    // split-step column sweep), as FastRows::tw_lo; null for the plain ones
+    const void* tw_lo;
+    // quarter-plane table of the complex64 transfer function (FP64 evaluation
+    // in the reference's operation order, scale folded in, rounded once): row
+    // c = |fx index| (0 .. ncols/2) holds htab_ld entries, entry q = |fy
+    // index| (0 .. L/2; the rest zero).  When set (complex64, no loss sums,
+    // one wavelength and distance), a CTA copies the W rows of its columns
+    // into shared memory while it transforms and reads H there instead of
+    // evaluating it (conj applied on reading).  With tw_lo (compensated
+    // sweeps) an entry is the pair (H_hi, H_lo), 16 bytes, H_lo = H - H_hi.
+    const float2* htab;
+    int htab_ld;
 };
+// Table rows of the W columns from col0 (W | ncols / 2): contiguous, in order
+// below ncols / 2 and reversed above it.
+__host__ __device__ inline int htab_row0(int col0, int ncols, int W) {
+    return col0 < ncols / 2 ? col0 : ncols - col0 - (W - 1);
+}
+// Row length of the table for columns of L points (a power of two >= 32):
+// L/2 + 8 >= L/2 + 1 entries, so rows are whole 16-byte units and consecutive
+// rows start 16 shared-memory banks apart.
+inline int htab_ld_for(int L) { return L / 2 + 8; }
+// Build the table of a's transfer function for columns of L points (the FP32
+// pipeline's H arguments in a, with conj ignored); hilo: (H_hi, H_lo) pairs of
+// float2 per entry, for the compensated sweeps (which read them as such).
+cudaError_t fast_build_htab(const FastCols& a, int L, float2* out, int ld, int hilo, cudaStream_t st);
+// Shared memory of a complex64 column CTA with the table rows.
+size_t fast_col_smem_htab(int L, int E, int W, int ld, int hilo);
 
 cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaStream_t st, int* nblocks);
 cudaError_t fast_cols(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks);
@@ -122,6 +154,12 @@ namespace wos {
 // per-pass twiddle tables of the specialised sweeps (forward passes, then inverse)
 int fast_table_len(int L, int E);
 cudaError_t fast_build_twiddles(int fp64, int L, int E, void* out, cudaStream_t st);
+// Residuals of the complex64 per-pass tables: (float)(W - (float)W) with W in FP64.
+cudaError_t fast_build_twiddles_lo(int L, int E, void* out, cudaStream_t st);
+// Compensated (hi + lo) complex64 split-step sweeps (wos_fast_cp.cu); the
+// plain launchers forward to them when tw_lo is set.
+cudaError_t fast_rows_bpm_cp(int L, int E, const FastRows& a, cudaStream_t st, int* nblocks);
+cudaError_t fast_cols_cp(int L, int E, const FastCols& a, cudaStream_t st, int* nblocks);
 size_t fast_col_smem(int fp64, int L, int E, int W);
 int fast_col_width(int fp64, int L, int E, int W);
 // lines per CTA of the fast row sweeps (the launchers and the record sizing share it)

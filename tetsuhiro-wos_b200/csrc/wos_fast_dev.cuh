@@ -75,25 +75,31 @@ __device__ __forceinline__ double2 ldg_keep(const double2* p) {
 // ftw_expand forms the others as products once the loads have landed (after
 // the exchange barrier), at most three roundings deep: four global loads and
 // eleven complex products per radix-16 butterfly instead of fifteen loads.
-template <int R, typename C> struct FtwPow2 {
-    static constexpr bool v = sizeof(C) == 8 && (R == 8 || R == 16);
+template <int R, typename C, bool CP = false> struct FtwPow2 {
+    static constexpr bool v = !CP && sizeof(C) == 8 && (R == 8 || R == 16);
 };
-template <int R, int E, int L, int NS, int TWOFF, typename C>
-__device__ __forceinline__ void ftw_load(C* w, int tt, const C* __restrict__ twp) {
+// CP (compensated, complex64): every twiddle is the pair W_hi + W_lo from
+// the table and its residual table twl (same layout, (float)(W - W_hi) from
+// FP64), all loaded (no products), and applied as x W_hi + x W_lo.
+template <int R, int E, int L, int NS, int TWOFF, bool CP, typename C>
+__device__ __forceinline__ void ftw_load(C* w, C* wl, int tt, const C* __restrict__ twp, const C* __restrict__ twl) {
     constexpr int T = L / E;
     if constexpr (NS > 1) {
 #pragma unroll
         for (int b = 0; b < E / R; b++) {
-            const C* tk = twp + TWOFF + ((tt + b * T) & (NS - 1));
+            const int o = TWOFF + ((tt + b * T) & (NS - 1));
+            const C* tk = twp + o;
 #pragma unroll
-            for (int r = 1; r < R; r++)
-                if (!FtwPow2<R, C>::v || (r & (r - 1)) == 0) w[b * (R - 1) + r - 1] = ldg_keep(tk + (r - 1) * NS);
+            for (int r = 1; r < R; r++) {
+                if (!FtwPow2<R, C, CP>::v || (r & (r - 1)) == 0) w[b * (R - 1) + r - 1] = ldg_keep(tk + (r - 1) * NS);
+                if constexpr (CP) wl[b * (R - 1) + r - 1] = ldg_keep(twl + o + (r - 1) * NS);
+            }
         }
     }
 }
-template <int R, int E, int NS, typename C>
+template <int R, int E, int NS, bool CP, typename C>
 __device__ __forceinline__ void ftw_expand(C* w) {
-    if constexpr (NS > 1 && FtwPow2<R, C>::v) {
+    if constexpr (NS > 1 && FtwPow2<R, C, CP>::v) {
 #pragma unroll
         for (int b = 0; b < E / R; b++) {
             C* p = w + b * (R - 1);  // p[r - 1] = W^(r k)
@@ -109,9 +115,17 @@ __device__ __forceinline__ void ftw_expand(C* w) {
     }
 }
 
+// x (t + tl) for a twiddle t with its residual tl (complex64): the small
+// product x tl first, then the main product folded in by FMAs.
+template <typename C>
+__device__ __forceinline__ C cmul_cp(C x, C t, C tl) {
+    const C c = cmul(x, tl);
+    return mkc<C>(fma(x.x, t.x, fma(-x.y, t.y, c.x)), fma(x.x, t.y, fma(x.y, t.x, c.y)));
+}
+
 // One Stockham DIT pass on registers, its twiddles already loaded.
-template <int R, int E, int NS, bool INV, typename C>
-__device__ __forceinline__ void fpass_tw(C* v, const C* w) {
+template <int R, int E, int NS, bool INV, bool CP, typename C>
+__device__ __forceinline__ void fpass_tw(C* v, const C* w, const C* wl) {
 #pragma unroll
     for (int b = 0; b < E / R; b++) {
         if constexpr (NS > 1) {
@@ -119,10 +133,16 @@ __device__ __forceinline__ void fpass_tw(C* v, const C* w) {
             for (int r = 1; r < R; r++) {
                 C t = w[b * (R - 1) + r - 1];
                 if (INV) t.y = -t.y;
-                v[b * R + r] = cmul(v[b * R + r], t);
+                if constexpr (CP) {
+                    C tl = wl[b * (R - 1) + r - 1];
+                    if (INV) tl.y = -tl.y;
+                    v[b * R + r] = cmul_cp(v[b * R + r], t, tl);
+                } else {
+                    v[b * R + r] = cmul(v[b * R + r], t);
+                }
             }
         }
-        dft<R, INV>(v + b * R);
+        dft<R, INV, C, CP>(v + b * R);
     }
 }
 
@@ -181,35 +201,40 @@ __host__ __device__ constexpr int fx_shift() {
 // stays a per-thread base plus immediates.  The next pass's twiddles are requested
 // once this thread's stores are issued (the data registers are free then), so
 // their latency runs under the barrier.
-template <int L, int E, bool INV, int p, int STR, typename C>
-__device__ __forceinline__ void fpasses_from(C* v, C* smb, int tt, const C* __restrict__ twp, const C* wcur) {
+template <int L, int E, bool INV, int p, int STR, bool CP, typename C>
+__device__ __forceinline__ void fpasses_from(C* v, C* smb, int tt, const C* __restrict__ twp, const C* __restrict__ twl,
+                                             const C* wcur, const C* wlcur) {
     using PL = FPlan<L, E>;
     if constexpr (p < PL::P) {
         constexpr int R = fp_radix(PL::P, PL::RS, E, INV, p);
         constexpr int NS = fp_ns(PL::P, PL::RS, E, INV, p);
-        fpass_tw<R, E, NS, INV>(v, wcur);
+        fpass_tw<R, E, NS, INV, CP>(v, wcur, wlcur);
         if constexpr (p < PL::P - 1) {
             constexpr int R2 = fp_radix(PL::P, PL::RS, E, INV, p + 1);
             constexpr int NS2 = fp_ns(PL::P, PL::RS, E, INV, p + 1);
             constexpr int TWOFF2 = fp_twoff(PL::P, PL::RS, E, INV, p + 1);
             constexpr int SH = fx_shift<L, R, NS, R2, STR, C>();
             C wn[(E / R2) * (R2 - 1)];
+            C wln[CP ? (E / R2) * (R2 - 1) : 1];
             __syncthreads();
             fstore<R, E, L, NS, SH, STR>(v, smb, tt);
-            ftw_load<R2, E, L, NS2, TWOFF2>(wn, tt, twp);
+            ftw_load<R2, E, L, NS2, TWOFF2, CP>(wn, wln, tt, twp, twl);
             __syncthreads();
             fload<R2, E, L, SH, STR>(v, smb, tt);
-            ftw_expand<R2, E, NS2>(wn);
-            fpasses_from<L, E, INV, p + 1, STR>(v, smb, tt, twp, wn);
+            ftw_expand<R2, E, NS2, CP>(wn);
+            fpasses_from<L, E, INV, p + 1, STR, CP>(v, smb, tt, twp, twl, wn, wln);
         }
     }
 }
 
-// A whole line transform (the first pass has NS == 1: no twiddles).
-template <int L, int E, bool INV, int p, int STR, typename C>
-__device__ __forceinline__ void fpasses(C* v, C* smb, int tt, const C* __restrict__ twp) {
+// A whole line transform (the first pass has NS == 1: no twiddles).  twl: the
+// residual table of the compensated transform (CP), else unused.
+template <int L, int E, bool INV, int p, int STR, typename C, bool CP = false>
+__device__ __forceinline__ void fpasses(C* v, C* smb, int tt, const C* __restrict__ twp,
+                                        const C* __restrict__ twl = nullptr) {
     static_assert(p == 0, "a line transform starts at pass 0");
-    fpasses_from<L, E, INV, 0, STR>(v, smb, tt, twp, static_cast<const C*>(nullptr));
+    fpasses_from<L, E, INV, 0, STR, CP>(v, smb, tt, twp, twl, static_cast<const C*>(nullptr),
+                                        static_cast<const C*>(nullptr));
 }
 
 // padded length of a line: the largest padq over the exchanges of both directions
@@ -256,6 +281,10 @@ template <typename Real, int L, int E, int W> struct FColB {
 
 __host__ __device__ constexpr int frow_stride(int L, int E) { return fp_padded_len(L, E) + 2; }
 __host__ __device__ constexpr int fcol_elems(int L, int E, int W) { return W * fp_padded_len(L, E) + 2; }
+// byte offset of the transfer-function table rows behind a complex64 column tile
+__host__ __device__ constexpr size_t fcol_htab_off(int L, int E, int W) {
+    return ((size_t)fcol_elems(L, E, W) * 8 + 15) / 16 * 16;
+}
 
 // ------------------------------------------------------------------- cols
 // sqrt of s in [2^-100, 1] to ~1e-13 relative without FP64<->FP32 conversion
@@ -445,9 +474,9 @@ __device__ __forceinline__ double2 h_f64(const FastCols& a, const HUnit& hu, dou
 // thread with q = 0 also takes the Nyquist row L/2.  p0 += |F|^2 and
 // l1 += |F|^2 (1 - |H|^2) when the loss sums are requested.  Every thread of
 // the CTA calls this between two barriers.
-template <typename Real, int L, int E, int W, typename C>
+template <typename Real, int L, int E, int W, bool HCP, typename C>
 __device__ __forceinline__ void col_tile_h(C* tile, int col0, const FastCols& a, const HUnit& hu, double& p0,
-                                           double& l1) {
+                                           double& l1, const float2* hs) {
     constexpr int T = L / E;
     const int w = threadIdx.x & (W - 1);
     const int tt = threadIdx.x / W;
@@ -464,6 +493,41 @@ __device__ __forceinline__ void col_tile_h(C* tile, int col0, const FastCols& a,
         tile[q * W + w] = cmul(x, h);
     };
     if constexpr (sizeof(Real) == 4) {
+        if (HCP && hs) {  // hi + lo table rows (compensated sweeps): x H_hi + x H_lo
+            const int cabs = col <= a.ncols / 2 ? col : a.ncols - col;
+            const float4* hr = reinterpret_cast<const float4*>(hs) + (cabs - htab_row0(col0, a.ncols, W)) * a.htab_ld;
+            const float sg = a.conj ? -1.f : 1.f;
+            auto apply4 = [&](int q, const float4 t) {
+                tile[q * W + w] = cmul_cp(tile[q * W + w], mkc<C>(t.x, sg * t.y), mkc<C>(t.z, sg * t.w));
+            };
+#pragma unroll
+            for (int i = 0; i < E / 2; i++) {
+                const int q = tt + i * T;
+                const float4 t = hr[q];
+                apply4(q, t);
+                if (q != 0) apply4(L - q, t);
+            }
+            if (tt == 0) apply4(L / 2, hr[L / 2]);
+            return;
+        }
+        if (hs) {  // the table rows of this CTA's columns (no loss sums here)
+            const int cabs = col <= a.ncols / 2 ? col : a.ncols - col;
+            const float2* hr = hs + (cabs - htab_row0(col0, a.ncols, W)) * a.htab_ld;
+            const float sg = a.conj ? -1.f : 1.f;
+#pragma unroll
+            for (int i = 0; i < E / 2; i++) {
+                const int q = tt + i * T;
+                const float2 t = hr[q];
+                const C h = mkc<C>(t.x, sg * t.y);
+                apply(q, h, 1.0);
+                if (q != 0) apply(L - q, h, 1.0);
+            }
+            if (tt == 0) {
+                const float2 t = hr[L / 2];
+                apply(L / 2, mkc<C>(t.x, sg * t.y), 1.0);
+            }
+            return;
+        }
         const double fx = (col <= a.ncols / 2 ? (double)col : (double)(col - a.ncols)) / ((double)a.ncols * a.dx);
         const double ax = hu.wl * fx;
         const double cx = fma(-ax, ax, 1.0);
@@ -507,12 +571,35 @@ __device__ __forceinline__ void col_tile_h(C* tile, int col0, const FastCols& a,
 // forward transform is done, natural order q = tt + s*T): the spectrum goes
 // to the tile, the alias-wrap histogram and H are applied there, and v is
 // reloaded in the natural order of the inverse transform's first pass.
-template <typename Real, int L, int E, int W, typename C>
+// cp.async (16 bytes, global -> shared, bypassing L1) and its completion.
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Copy the table rows of the W columns from col0 to hs (shared memory); the
+// copies complete under the forward transform (col_spectral_stage waits).
+// HCP: entries are (H_hi, H_lo) pairs, 16 bytes.
+template <int W, bool HCP>
+__device__ __forceinline__ void htab_prefetch(float2* hs, const FastCols& a, int col0) {
+    constexpr int U = HCP ? 2 : 1;  // float2 units per entry
+    const float4* g =
+        reinterpret_cast<const float4*>(a.htab + (long long)htab_row0(col0, a.ncols, W) * a.htab_ld * U);
+    const int n16 = W * a.htab_ld * U / 2;
+    for (int i = threadIdx.x; i < n16; i += blockDim.x) cp_async16(hs + 2 * i, g + i);
+    cp_async_commit();
+}
+
+template <typename Real, int L, int E, int W, typename C, bool HCP = false>
 __device__ __forceinline__ void col_spectral_stage(C* v, C* tile, double* hsm, int col0, const FastCols& a,
-                                                   const HUnit& hu, double& p0, double& l1) {
+                                                   const HUnit& hu, double& p0, double& l1,
+                                                   const float2* hs = nullptr) {
     constexpr int T = L / E;
     const int w = threadIdx.x & (W - 1);
     const int tt = threadIdx.x / W;
+    if (hs) cp_async_wait_all();  // this thread's table copies (the barriers below publish them)
     __syncthreads();  // every thread has loaded its last forward pass
 #pragma unroll
     for (int s = 0; s < E; s++) tile[(tt + s * T) * W + w] = v[s];
@@ -521,7 +608,7 @@ __device__ __forceinline__ void col_spectral_stage(C* v, C* tile, double* hsm, i
         col_hist_bin(tile, hsm, col0, L, W, a.ncols, a.hist_dx);
         __syncthreads();
     }
-    col_tile_h<Real, L, E, W>(tile, col0, a, hu, p0, l1);
+    col_tile_h<Real, L, E, W, HCP>(tile, col0, a, hu, p0, l1, hs);
     __syncthreads();
 #pragma unroll
     for (int s = 0; s < E; s++) v[s] = tile[(tt + s * T) * W + w];

@@ -113,6 +113,12 @@ template <> struct K<float2> {
     static constexpr float S2 = 0.70710678118654752440f;
     static constexpr float C8 = 0.92387953251128675613f;
     static constexpr float S8 = 0.38268343236508977173f;
+    // residuals of the single-precision constants (value - S2 etc., rounded):
+    // with them a rotation is exact to ~2^-48 instead of 2^-25, which matters
+    // where the same transform pair runs hundreds of times (split-step slices)
+    static constexpr float S2L = (float)(0.70710678118654752440 - (double)S2);
+    static constexpr float C8L = (float)(0.92387953251128675613 - (double)C8);
+    static constexpr float S8L = (float)(0.38268343236508977173 - (double)S8);
 };
 template <> struct K<double2> {
     static constexpr double S2 = 0.70710678118654752440;
@@ -169,7 +175,32 @@ template <> __device__ __forceinline__ void bfly_w8<3, true, float2>(float2& a, 
 }
 #endif
 
-template <bool INV, typename C>
+// Compensated rotations (CP): the constant c is applied as c_hi + c_lo, the
+// small product with c_lo folded in first, so that the rotation's own error
+// is that of the data rounding only (complex64).
+#if !defined(WOS_SCALAR_CADD)
+template <int k, bool INV>
+__device__ __forceinline__ void bfly_w8_cp(float2& a, float2& b, float2 e, float2 x) {
+    float2 u;
+    if (k == 1) u = INV ? make_float2(x.x - x.y, x.x + x.y) : make_float2(x.x + x.y, x.y - x.x);
+    else u = INV ? make_float2(-x.x - x.y, x.x - x.y) : make_float2(x.y - x.x, -x.x - x.y);
+    const float s = K<float2>::S2, sl = K<float2>::S2L;
+    a = f2_fma(make_float2(s, s), u, f2_fma(make_float2(sl, sl), u, e));
+    b = f2_fma(make_float2(-s, -s), u, f2_fma(make_float2(-sl, -sl), u, e));
+}
+#endif
+template <int k, bool INV, bool CP, typename C>
+__device__ __forceinline__ void bfly_w8x(C& a, C& b, C e, C x) {
+#if !defined(WOS_SCALAR_CADD)
+    if constexpr (CP && sizeof(C) == 8) {
+        bfly_w8_cp<k, INV>(a, b, e, x);
+        return;
+    }
+#endif
+    bfly_w8<k, INV>(a, b, e, x);
+}
+
+template <bool INV, typename C, bool CP = false>
 __device__ __forceinline__ void dft8(C* v) {
     // even / odd radix-4 then combine
     C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
@@ -177,9 +208,9 @@ __device__ __forceinline__ void dft8(C* v) {
     dft4<INV>(e0, e1, e2, e3);
     dft4<INV>(o0, o1, o2, o3);
     v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
-    bfly_w8<1, INV>(v[1], v[5], e1, o1);
+    bfly_w8x<1, INV, CP>(v[1], v[5], e1, o1);
     bfly_mi<INV>(v[2], v[6], e2, o2);
-    bfly_w8<3, INV>(v[3], v[7], e3, o3);
+    bfly_w8x<3, INV, CP>(v[3], v[7], e3, o3);
 }
 
 // multiply by w16^k (forward w16 = exp(-2 pi i/16)), k = 0..7
@@ -199,21 +230,39 @@ __device__ __forceinline__ C w16(C x) {
     return mkc<C>(x.x * c + x.y * s, x.y * c - x.x * s);
 }
 
-template <bool INV, typename C>
+// w16^k x (k odd) with the constants as hi + lo pairs (complex64, CP).
+template <int k, bool INV>
+__device__ __forceinline__ float2 w16_cp(float2 x) {
+    float c, s, cl, sl;  // w = c - i s (forward)
+    if (k == 1) { c = K<float2>::C8; s = K<float2>::S8; cl = K<float2>::C8L; sl = K<float2>::S8L; }
+    else if (k == 3) { c = K<float2>::S8; s = K<float2>::C8; cl = K<float2>::S8L; sl = K<float2>::C8L; }
+    else if (k == 5) { c = -K<float2>::S8; s = K<float2>::C8; cl = -K<float2>::S8L; sl = K<float2>::C8L; }
+    else { c = -K<float2>::C8; s = K<float2>::S8; cl = -K<float2>::C8L; sl = K<float2>::S8L; }
+    if (INV) { s = -s; sl = -sl; }
+    const float tx = fmaf(x.x, cl, x.y * sl), ty = fmaf(x.y, cl, -(x.x * sl));
+    return make_float2(fmaf(x.x, c, fmaf(x.y, s, tx)), fmaf(x.y, c, fmaf(-x.x, s, ty)));
+}
+template <int k, bool INV, bool CP, typename C>
+__device__ __forceinline__ C w16x(C x) {
+    if constexpr (CP && sizeof(C) == 8) return w16_cp<k, INV>(x);
+    else return w16<k, INV>(x);
+}
+
+template <bool INV, typename C, bool CP = false>
 __device__ __forceinline__ void dft16(C* v) {
     C e[8], o[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) { e[i] = v[2 * i]; o[i] = v[2 * i + 1]; }
-    dft8<INV>(e);
-    dft8<INV>(o);
-    o[1] = w16<1, INV>(o[1]); o[3] = w16<3, INV>(o[3]);
-    o[5] = w16<5, INV>(o[5]); o[7] = w16<7, INV>(o[7]);
+    dft8<INV, C, CP>(e);
+    dft8<INV, C, CP>(o);
+    o[1] = w16x<1, INV, CP>(o[1]); o[3] = w16x<3, INV, CP>(o[3]);
+    o[5] = w16x<5, INV, CP>(o[5]); o[7] = w16x<7, INV, CP>(o[7]);
 #pragma unroll
     for (int i = 0; i < 8; i += 2) { v[i + 1] = cadd(e[i + 1], o[i + 1]); v[i + 9] = csub(e[i + 1], o[i + 1]); }
     v[0] = cadd(e[0], o[0]); v[8] = csub(e[0], o[0]);
-    bfly_w8<1, INV>(v[2], v[10], e[2], o[2]);
+    bfly_w8x<1, INV, CP>(v[2], v[10], e[2], o[2]);
     bfly_mi<INV>(v[4], v[12], e[4], o[4]);
-    bfly_w8<3, INV>(v[6], v[14], e[6], o[6]);
+    bfly_w8x<3, INV, CP>(v[6], v[14], e[6], o[6]);
 }
 
 // Radix 3 and 5 (mixed-radix lines): the DFT sums written with the real and
@@ -264,12 +313,12 @@ __device__ __forceinline__ void dft5(C* v) {
     v[3] = mkc<C>(m2.x - n2.y, m2.y + n2.x);
 }
 
-template <int R, bool INV, typename C>
+template <int R, bool INV, typename C, bool CP = false>
 __device__ __forceinline__ void dft(C* v) {
     if (R == 2) dft2<INV>(v[0], v[1]);
     else if (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
-    else if (R == 8) dft8<INV>(v);
-    else if (R == 16) dft16<INV>(v);
+    else if (R == 8) dft8<INV, C, CP>(v);
+    else if (R == 16) dft16<INV, C, CP>(v);
     else if (R == 3) dft3<INV>(v);
     else if (R == 5) dft5<INV>(v);
 }
