@@ -460,9 +460,15 @@ WOS_API int wos_graph_destroy(wos_graph g);
  *      [ny][nx] (in == out allowed); ny and nx powers of two, 4..1024, larger
  *      sizes return WOS_UNSUPPORTED_SIZE.  Work space: file-scope device arrays
  *      (a 1024 x 2048 complex64 intermediate, 16 MiB, plus 32 KiB of
- *      twiddles) that every GPU loading the library holds until exit.  The
- *      first call on a device resolves their addresses and fills the twiddles
- *      (a kernel and a synchronisation of `stream`): make that first call
+ *      twiddles); once a device holds them it keeps them until exit.  The
+ *      CUDA runtime places them when it loads their module into the device's
+ *      context: under lazy module loading (the default since CUDA 12.2) that
+ *      is the first call on the device, so a caller whose allocator reserves
+ *      the whole GPU must make the first call before reserving, or run with
+ *      CUDA_MODULE_LOADING=EAGER.  The first call on a device (and the first
+ *      after the caller re-created the device's context, e.g. by
+ *      cudaDeviceReset) resolves their addresses and fills the twiddles (a
+ *      kernel and a synchronisation of `stream`): make that first call
  *      before any stream capture.  All calls share the arrays, so calls that
  *      overlap on the GPU (different streams or threads) race; serialise them.
  *      Nothing needs clearing between calls: each call writes every scratch

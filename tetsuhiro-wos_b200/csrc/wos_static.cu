@@ -9,9 +9,16 @@
 // one keeps its workspace in file-scope __device__ arrays instead, so calling
 // it never allocates.
 //
-// The price: the arrays below exist on every GPU that loads libwosgpu.so until
-// the process exits (16 MiB + 32 KiB per device), and they bound the problem
-// size.  Every call shares them.
+// The price: the arrays below bound the problem size, every call shares them,
+// and once placed on a device they stay there until the process exits (16 MiB
+// + 32 KiB per device).  They are placed when the CUDA runtime loads this
+// file's device code into the device's context: under lazy module loading
+// (CUDA_MODULE_LOADING=LAZY, the default since CUDA 12.2) that is the first
+// call of this entry point on the device, so a caller whose allocator takes
+// the whole GPU must make that first call before reserving its memory, or run
+// with CUDA_MODULE_LOADING=EAGER (the arrays are then placed when the context
+// is created).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -40,8 +47,9 @@ __device__ __align__(256) float2 g_noalloc_twiddles[2 * kNoAllocMaxL];
 
 struct DeviceState {
     bool ready = false;
-    float2* scratch = nullptr;  // device address of g_noalloc_scratch on this device
-    float2* tw = nullptr;       // device address of g_noalloc_twiddles
+    unsigned long long ctx_id = 0;  // the context the addresses and tables belong to
+    float2* scratch = nullptr;      // device address of g_noalloc_scratch on this device
+    float2* tw = nullptr;           // device address of g_noalloc_twiddles
 };
 DeviceState g_state[kNoAllocMaxDev];
 std::mutex g_state_mu;
@@ -53,12 +61,43 @@ int err(int status, const char* msg) {
 
 bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
-// Once per device, with that device current: resolve the arrays' device
-// addresses and fill the twiddle tables (a kernel on the caller's stream,
-// then a stream synchronisation so later calls on any stream see them).
+// The unique id of the current CUDA context (cuCtxGetId, through the
+// runtime's driver entry points, so nothing links libcuda).  A context that
+// the caller destroyed and re-created (cudaDeviceReset) has a new id, and its
+// copy of the arrays starts uninitialised.
+int current_ctx_id(unsigned long long* id) {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess ||
+            q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !f1 || !f2)
+            return err(WOS_CUDA_ERROR, "no-alloc asm_pad: cuCtxGetCurrent / cuCtxGetId not available");
+        get_current = reinterpret_cast<GetCurrent>(f1);
+        get_id = reinterpret_cast<GetId>(f2);
+    }
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, id) != CUDA_SUCCESS)
+        return err(WOS_CUDA_ERROR, "no-alloc asm_pad: no current CUDA context");
+    return WOS_OK;
+}
+
+// Once per device context, with that device current: resolve the arrays'
+// device addresses and fill the twiddle tables (a kernel on the caller's
+// stream, then a stream synchronisation so later calls on any stream see
+// them).  Done again when the device's context has been re-created.
 int setup(int dev, cudaStream_t st, DeviceState** out) {
     std::lock_guard<std::mutex> lk(g_state_mu);
     DeviceState& s = g_state[dev];
+    unsigned long long id = 0;
+    const int rc = current_ctx_id(&id);
+    if (rc != WOS_OK) return rc;
+    if (s.ready && s.ctx_id != id) s.ready = false;
     if (!s.ready) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -73,6 +112,7 @@ int setup(int dev, cudaStream_t st, DeviceState** out) {
         }
         e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return err(WOS_CUDA_ERROR, cudaGetErrorString(e));
+        s.ctx_id = id;
         s.ready = true;
     }
     *out = &s;
