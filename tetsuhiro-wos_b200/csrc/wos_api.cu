@@ -5,26 +5,9 @@
 // behaviour (z == 0 early return, nil-context defaults, evanescent policy,
 // warning codes and values) follows the cited reference lines; the numerics
 // run on the device, with no CPU fallback.
-#include <cuda_runtime.h>
+#include "wos_api_internal.cuh"
 
-#include <algorithm>
-#include <cmath>
-#include <cstdio>
-#include <cstring>
-#include <map>
-#include <mutex>
-#include <string>
-#include <vector>
-
-#include "../../include/wos_gpu.h"
-#include "wos_fast.cuh"
-#include "wos_pipe.cuh"
-#include "wos_fft.cuh"
-#include "wos_kernels.cuh"
-
-using namespace wos;
-
-namespace {
+namespace wapi {
 
 thread_local std::string g_err;
 
@@ -32,26 +15,6 @@ int fail(int st, const std::string& msg) {
     g_err = msg;
     return st;
 }
-
-#define CK(call)                                                                              \
-    do {                                                                                      \
-        cudaError_t e_ = (call);                                                              \
-        if (e_ != cudaSuccess) {                                                              \
-            return fail(e_ == cudaErrorMemoryAllocation ? WOS_OOM : WOS_CUDA_ERROR,           \
-                        std::string(#call) + ": " + cudaGetErrorString(e_));                 \
-        }                                                                                     \
-    } while (0)
-
-#define TRY(x)                  \
-    do {                        \
-        int rc_ = (x);          \
-        if (rc_ != WOS_OK) return rc_; \
-    } while (0)
-
-struct DevBuf {
-    void* p = nullptr;
-    size_t n = 0;
-};
 
 int ensure(DevBuf& b, size_t bytes) {
     if (b.n >= bytes && b.p) return WOS_OK;
@@ -68,102 +31,11 @@ int ensure(DevBuf& b, size_t bytes) {
     return WOS_OK;
 }
 
-bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 int next_pow2(int n) {
     int m = 1;
     while (m < n) m <<= 1;
     return m;
 }
-
-// Everything needed to transform a line of logical length n in one precision.
-struct Axis {
-    int n = 0, L = 0, blue = 0;
-    void* tw = nullptr;
-    void* chirp = nullptr;
-    void* bf = nullptr;
-    void* bi = nullptr;
-    void* ftw[2] = {nullptr, nullptr};  // per-pass twiddles of the specialised sweeps (E = 8, 16)
-    void* ftw_lo[2] = {nullptr, nullptr};  // their complex64 residuals (compensated split-step sweeps)
-    void* ptw = nullptr;                // W_L^n, n < L/2: split column tiles
-};
-
-constexpr int kMaxL32 = 8192;  // largest line held on chip (threads x elements)
-constexpr int kMaxL64 = 8192;
-
-// Launch configuration of the specialised sweeps for one grid: elements per
-// thread of the row and column passes, columns per CTA.
-struct Tune {
-    int rowE, colE, colW;
-};
-long long tune_key(int fp64, int ny, int nx) { return ((long long)fp64 << 62) | ((long long)ny << 31) | nx; }
-
-}  // namespace
-
-struct wos_ctx_s {
-    int device = 0;
-    int fp64 = 0;
-    cudaStream_t st = nullptr;
-    bool own_stream = false;
-    std::mutex mu;
-    std::map<int, Axis> axes[2];  // [fp64][n]
-    DevBuf stage, scratch, scratch2, scratch3, red, redout, tmp, maps, params, vol, accum, aux;
-    double* hred = nullptr;  // pinned mirror of redout
-    size_t hred_n = 0;
-    int colw = 0;
-    bool no_fast = false;               // force the general sweeps (tests compare both)
-    int sweep_mode = 1;                 // wos_ctx_set_fast_path: 1, 2 or 3 (0 is no_fast)
-    int col_pair = 0;                   // column tiles split over two-CTA clusters where supported
-    DevBuf bpm_tab;                     // split-step tables (core profile, border absorption) on the device
-    std::vector<double> bpm_tab_host;   // ... and their host copy, to skip identical uploads
-    int tiled = 0;                      // three-sweep ASM through the tiled intermediate (FastRows::out_tiled)
-    int bpm_comp = 1;                   // complex64 split-step slices on the compensated transforms (WOS_BPM_COMP=0: off)
-    // transfer-function tables of the complex64 column sweep (FastCols::htab),
-    // keyed by grid and H parameters; a few slots, reused round robin (a
-    // slot is rebuilt on the context stream, after the work that read it)
-    struct HTab {
-        bool valid = false;
-        int L = 0, ncols = 0;
-        double key[9] = {};
-        DevBuf buf;
-    };
-    static constexpr int kHTabs = 4;
-    HTab htab[kHTabs];
-    int htab_next = 0;
-    int htab_on = 1;                    // WOS_HTAB=0: evaluate H in the sweep
-    unsigned* err_dev = nullptr;        // error word of the pipelined kernels (device)
-    unsigned* err_host = nullptr;       // pinned mirror, read where the host synchronises
-    // streams for independent fields of a batch (wos_propagate_batch_dev),
-    // forked from and joined back into st
-    static constexpr int kMaxAux = 4;
-    cudaStream_t side[kMaxAux] = {};
-    cudaEvent_t fork_ev = nullptr, join_ev[kMaxAux] = {};
-    int naux = 0;
-    DevBuf tsc[kMaxAux + 1];            // tiled intermediates: [0] context stream, [1 + k] side stream k
-    int cur_slot = 0;                   // which of them the current stream uses
-    // copy pipeline of wos_propagate_batch: host-to-device and device-to-host
-    // streams, staging slots and their events
-    static constexpr int kSlots = 3;
-    cudaStream_t h2d = nullptr, d2h = nullptr;
-    DevBuf slot[kSlots];
-    cudaEvent_t in_ev[kSlots] = {}, done_ev[kSlots] = {}, free_ev[kSlots] = {};
-    bool pipe_made = false;
-    std::map<long long, Tune> tune;     // autotuned launch configurations
-    size_t csz() const { return fp64 ? 16 : 8; }
-    // per-launch CUDA-event profile (wos_ctx_set_profiling): a ring of event
-    // pairs; a slot's elapsed time is folded into its kind when it is reused
-    // or read, by which time the pair has long completed.
-    static constexpr int kRing = 1024;
-    bool prof_on = false, prof_made = false;
-    cudaEvent_t ev0[kRing], ev1[kRing];
-    int ev_kind[kRing];
-    bool ev_used[kRing];
-    int ev_head = 0;
-    double prof_ms[8] = {0};
-    long long prof_n[8] = {0};
-    long long launches = 0;
-};
-
-namespace {
 
 int set_device(wos_ctx c) {
     CK(cudaSetDevice(c->device));
@@ -194,30 +66,13 @@ void prof_fold(wos_ctx c, int slot) {
     c->ev_used[slot] = false;
 }
 
-// Kinds: 0..3 row modes (fwd, inv, inv.screen.fwd, inv.accumulate), 4..7 column
-// modes (fused, fraunhofer, reduce, fft).
-template <typename F>
-cudaError_t timed_launch(wos_ctx c, int kind, F&& launch) {
-    c->launches++;
-    if (!c->prof_on) return launch();
-    const int slot = c->ev_head;
-    prof_fold(c, slot);
-    cudaEventRecord(c->ev0[slot], c->st);
-    cudaError_t e = launch();
-    cudaEventRecord(c->ev1[slot], c->st);
-    c->ev_kind[slot] = kind;
-    c->ev_used[slot] = true;
-    c->ev_head = (slot + 1) % wos_ctx_s::kRing;
-    return e;
-}
 cudaError_t prof_rows(wos_ctx c, int fp64, const RowArgs& a) {
     return timed_launch(c, a.mode & 3, [&] { return launch_rows(fp64, a, c->st); });
 }
+
 cudaError_t prof_cols(wos_ctx c, int fp64, const ColArgs& a) {
     return timed_launch(c, 4 + (a.mode & 3), [&] { return launch_cols(fp64, a, c->st); });
 }
-
-int get_axis(wos_ctx c, int n, int fp64, Axis** out);
 
 bool mixed_radix_ok(int n) {
     if (n < 4 || (n & 1)) return false;
@@ -316,6 +171,7 @@ void fill_axis(RowArgs& r, const Axis* a) {
     r.bhat_f = a->bf;
     r.bhat_i = a->bi;
 }
+
 void fill_axis(ColArgs& r, const Axis* a) {
     r.L = a->L;
     r.blue_n = a->blue ? a->n : 0;
@@ -336,6 +192,7 @@ RowArgs row_defaults(int ny, int nx, double dx) {
     r.batch = 1;
     return r;
 }
+
 ColArgs col_defaults(wos_ctx c, double dx) {
     ColArgs a{};
     a.h.scale = 1.0;
@@ -360,14 +217,8 @@ int auto_colw_p(wos_ctx c, int fp64, int L) {
     while (W > 1 && (W * T > maxt || col_smem_bytes(fp64, L, W) > 200 * 1024)) W >>= 1;
     return W;
 }
-int auto_colw(wos_ctx c, int L) { return auto_colw_p(c, c->fp64, L); }
 
-// ---- reductions: partial region r, finished into redout[r]
-constexpr int kRegions = 8;
-struct Red {
-    wos_ctx c;
-    size_t per_region = 0;  // doubles per region
-};
+int auto_colw(wos_ctx c, int L) { return auto_colw_p(c, c->fp64, L); }
 
 int red_prepare(wos_ctx c, size_t max_blocks) {
     const size_t per = max_blocks * RS_COUNT;
@@ -380,11 +231,14 @@ int red_prepare(wos_ctx c, size_t max_blocks) {
     }
     return WOS_OK;
 }
+
 double* red_region(wos_ctx c, int r) {
     const size_t per = c->red.n / sizeof(double) / kRegions;
     return reinterpret_cast<double*>(c->red.p) + per * r;
 }
+
 size_t red_region_blocks(wos_ctx c) { return c->red.n / sizeof(double) / kRegions / RS_COUNT; }
+
 double* redout_region(wos_ctx c, int r) { return reinterpret_cast<double*>(c->redout.p) + (size_t)RS_COUNT * r; }
 
 // blocks of a row launch (mirrors launch_rows_t) and of a column launch
@@ -396,6 +250,7 @@ size_t row_blocks(int fp64, int L, int rows, int batch) {
     while (lines * T < 32) lines *= 2;
     return (size_t)((rows + lines - 1) / lines) * std::max(batch, 1);
 }
+
 size_t col_blocks(int fp64, int L, int W, int ncols, int batch) {
     const int E = pick_E(fp64, L);
     const int T = L / E;
@@ -405,11 +260,6 @@ size_t col_blocks(int fp64, int L, int W, int ncols, int batch) {
     return (size_t)((ncols + W - 1) / W) * std::max(batch, 1);
 }
 
-// ---- evanescent policy (optics/propagate.go:186-199)
-struct Policy {
-    int zero = 0, reg = 0;
-    double alpha = 0, limit = 0;
-};
 Policy ev_policy(const wos_context& c, double z) {
     Policy p;
     p.limit = c.evanescent_limit;
@@ -464,6 +314,7 @@ bool wrap_needed(const wos_context& c, int ny, int nx, double dx, double z) {
     if (!c.diagnostics || z == 0 || carry <= 0) return false;
     return std::fabs(z) * c.wavelength / (2 * dx) > carry;
 }
+
 void wrap_finish(wos_diag* d, const wos_context& c, int ny, int nx, double dx, double z, const double* hist) {
     const double carry = (double)std::min(nx, ny) * dx;
     const double fsig = spectral_radius_from_hist(hist, dx, 0.90);
@@ -475,21 +326,6 @@ void wrap_finish(wos_diag* d, const wos_context& c, int ny, int nx, double dx, d
     const double walk = std::fabs(z) * c.wavelength * fsig;
     if (walk > carry) warn_add(d, WOS_W_ASM_ALIAS_WRAP, walk / carry);
 }
-
-// ---------------------------------------------------------------- pipeline
-struct Prop {
-    int ny, nx;
-    double dx;
-    int ncomp;
-    const void* in;
-    int in_c128;
-    void* out;
-    int out_c128;
-    double z;
-    int method;
-    wos_context c;
-    wos_diag* diag;
-};
 
 // Fetch finished reduction regions [0, n) to the host (one synchronisation).
 int fetch_red(wos_ctx c, int nreg) {
@@ -575,23 +411,6 @@ int spectrum_stats(wos_ctx c, const Prop& p, void* dst, bool centroid, bool hist
     return WOS_OK;
 }
 
-// The three-sweep propagator shared by asm / asm_shift / asm_pad /
-// asm_shift_pad / fresnel_tf / fresnel_ir:
-//   rows:  in (ny x nx) -> scratch rows, forward transform over mx points
-//   cols:  forward over my points, H, inverse, keep rows [offy, offy+ny)
-//   rows:  inverse over mx points, keep columns [offx, offx+nx) -> out
-// pad = 1 doubles both axes (zero-padded linear convolution,
-// optics/propagate.go:346-387); the padding is folded into addressing.
-struct Sweep3 {
-    int pad = 0;
-    int shift = 0;
-    double fxc = 0, fyc = 0;
-    HArgs h{};
-    bool red_pin = false, red_pout = false, hist = false;
-    bool red_loss = false;  // spectral power-loss sums of the H_ASM step (region 1)
-    bool fast = false;      // set when the specialised sweeps ran (no crop sums)
-};
-
 int env_int(const char* name, int def) {
     const char* v = std::getenv(name);
     return (v && *v) ? std::atoi(v) : def;
@@ -615,6 +434,7 @@ size_t fast_row_blocks(int L, int E, int rows, int batch) {
     const int lines = fast_row_lines(L, E, rows);
     return (size_t)((rows + lines - 1) / lines) * std::max(batch, 1);
 }
+
 // (an upper bound: the split tiles of fast_cols_pair launch two CTAs per tile)
 size_t fast_col_blocks(int fp64, int L, int E, int W, int ncols, int batch) {
     W = fast_col_width(fp64, L, E, W);
@@ -634,6 +454,7 @@ int fast_tw(wos_ctx c, Axis* a, int E, const void** out) {
     *out = a->ftw[slot];
     return WOS_OK;
 }
+
 // Residual table of the complex64 per-pass twiddles (compensated sweeps).
 int fast_tw_lo(wos_ctx c, Axis* a, int E, const void** out) {
     const int slot = E == 16 ? 1 : 0;
@@ -696,6 +517,7 @@ cudaError_t sweep_rows(wos_ctx c, int L, int E, bool inv, const FastRows& a, int
     }
     return fast_rows(c->fp64, L, E, inv, a, c->st, nb);
 }
+
 // Tables of the split column tiles: per-pass twiddles of L/2 and W_L^n.
 bool pair_tables(wos_ctx c, int L, int E, const void** twh, const void** twp) {
     Axis *ah, *af;
@@ -712,6 +534,7 @@ bool pair_tables(wos_ctx c, int L, int E, const void** twh, const void** twp) {
     *twp = af->ptw;
     return true;
 }
+
 bool pair_eligible(wos_ctx c, int L, int E, const FastCols& a) {
     return c->col_pair && !a.hist && !a.tiled && !a.tw_lo && !a.htab &&
            fast_cols_pair_case(c->fp64, L, E, fast_col_width(c->fp64, L, E, a.W));
@@ -1256,6 +1079,7 @@ int stage_in(wos_ctx c, const wos_field* f, int ncomp) {
         CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->stage.p) + np * 16, f->ey, np * 16, cudaMemcpyHostToDevice, c->st));
     return WOS_OK;
 }
+
 int stage_out(wos_ctx c, wos_field* f, int ncomp) {
     const size_t np = (size_t)f->ny * f->nx;
     CK(cudaMemcpyAsync(f->ex, c->stage.p, np * 16, cudaMemcpyDeviceToHost, c->st));
@@ -1339,9 +1163,15 @@ int plane_view_dev(wos_ctx c, int fp64, const void* ex, const void* ey, const vo
     return WOS_OK;
 }
 
-}  // namespace
+void diag_merge(wos_diag* into, const wos_diag& d) {
+    if (!into) return;
+    for (int b = 0; b < WOS_W_COUNT; b++) {
+        into->warn_count[b] += d.warn_count[b];
+        if (d.warn_count[b] && d.warn_value[b] != 0) into->warn_value[b] = d.warn_value[b];
+    }
+}
 
-// ====================================================================== ABI}  // namespace
+}  // namespace wapi
 
 // ====================================================================== ABI
 extern "C" {
@@ -1805,1770 +1635,6 @@ int wos_propagate(wos_ctx c, wos_field* f, double z, int method, const wos_conte
     return WOS_OK;
 }
 
-}  // extern "C"
-
-// ================================================= split-step, batches, elements
-namespace {
-
-void diag_merge(wos_diag* into, const wos_diag& d) {
-    if (!into) return;
-    for (int b = 0; b < WOS_W_COUNT; b++) {
-        into->warn_count[b] += d.warn_count[b];
-        if (d.warn_count[b] && d.warn_value[b] != 0) into->warn_value[b] = d.warn_value[b];
-    }
-}
-
-struct ScreenSrc {
-    int kind = 1;  // 1 parametric, 2 maps
-    wos_index_desc desc{};
-    const double* nre = nullptr;
-    const double* nim = nullptr;
-    int nmaps = 1;
-};
-
-void fill_screen(ScreenArgs& s, const ScreenSrc& src, int slice, long long np, double k, double dz, double zc) {
-    s = ScreenArgs{};
-    s.kind = src.kind;
-    s.k = k;
-    s.dz = dz;
-    s.zc = zc;
-    if (src.kind == 1) {
-        const wos_index_desc& d = src.desc;
-        s.re_bg = d.re_bg;
-        s.im_bg = d.im_bg;
-        s.core_dn = d.core_dn;
-        s.core_x0 = d.core_x0;
-        s.core_y0 = d.core_y0;
-        s.core_w = d.core_w;
-        s.zmod_amp = d.zmod_amp;
-        s.zmod_period = d.zmod_period;
-        s.zmod_phase = d.zmod_phase;
-        s.border_px = d.border_px;
-        s.border_order = d.border_order;
-        s.border_strength = d.border_strength;
-        s.n_layers = d.n_layers < 0 ? 0 : (d.n_layers > 8 ? 8 : d.n_layers);
-        for (int i = 0; i < 8; i++) {
-            s.layer_z[i] = d.layer_z[i];
-            s.layer_re[i] = d.layer_re[i];
-            s.layer_im[i] = d.layer_im[i];
-        }
-    } else {
-        const int m = src.nmaps == 1 ? 0 : slice;
-        s.nre = src.nre + (long long)m * np;
-        s.nim = src.nim + (long long)m * np;
-    }
-}
-
-// PropagateSplitStep (optics/medium.go:22-45) with merged half steps:
-//   rows fwd | cols H(dz/2) | rows inv.M0.fwd | cols H(dz/2)^2 | ... | rows inv.M(S-1).fwd
-//   | cols H(dz/2) | rows inv
-// The power around every ASM half step (for the evanescent_filtered /
-// backward_* warnings of each Propagate(dz/2) call) comes from Parseval sums in
-// the column pass, one finished record per pass.
-// Split-step BPM on the specialised sweeps: A(dz/2) M A(dz) M ... A(dz/2) with
-// the column sweeps of the fused ASM (the merged half steps A(dz/2)^2 are one
-// step A(dz): forward steps without an evanescent limit only) and the slice
-// screens inside the row sweeps (k_rows_bpm_fast).  The screen of a
-// parametric medium factorises as c_s * border(d) * exp(i p_s gx(x) gy(y)):
-// the slice constants c_s = exp(-k dz Im n0) exp(i k dz (Re n0 - 1)) are
-// multiplied in FP64 on the host and applied once in the last sweep.
-// adjoint: the adjoint operator (conj transfer functions and screens, slices
-// in reverse order).  Returns -1 when the case is not eligible (the general
-// path then runs).
-int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* in, int in_c128, void* out,
-                       int out_c128, double z, const ScreenSrc& src, int steps, const wos_context& cc, bool diag,
-                       bool adjoint) {
-    if (diag || c->no_fast || src.kind != 1 || !is_pow2(nx) || !is_pow2(ny) || !(z > 0)) return -1;
-    const double dz = z / (double)steps, hz = dz / 2;
-    const double k = 2 * M_PI / cc.wavelength;
-    const Policy pol = ev_policy(cc, hz);
-    if (pol.limit > 0 || pol.reg) return -1;
-    if (!c->fp64 && !(std::fabs(k * dz / (2 * M_PI)) < 268435456.0)) return -1;
-    const Tune t = get_tune(c, ny, nx);
-    if (!fast_supported(c->fp64, nx, t.rowE) || !fast_supported(c->fp64, ny, t.colE)) return -1;
-    const wos_index_desc& d = src.desc;
-    Axis *ax, *ay;
-    TRY(get_axis(c, nx, c->fp64, &ax));
-    TRY(get_axis(c, ny, c->fp64, &ay));
-    // complex64: the slice sweeps run the compensated transforms (hi + lo
-    // twiddles), whose error does not add up over the slices; their column
-    // sweep holds 8 values per thread (16 with the residual twiddles spill)
-    const bool comp = !c->fp64 && c->bpm_comp;
-    const int colE = (comp && t.colE == 16 && fast_supported(0, ny, 8)) ? 8 : t.colE;
-    const void *twx, *twy;
-    TRY(fast_tw(c, ax, t.rowE, &twx));
-    TRY(fast_tw(c, ay, colE, &twy));
-    const void *twx_lo = nullptr, *twy_lo = nullptr;
-    if (comp) {
-        TRY(fast_tw_lo(c, ax, t.rowE, &twx_lo));
-        TRY(fast_tw_lo(c, ay, colE, &twy_lo));
-    }
-    const long long np = (long long)ny * nx;
-    void* S;
-    if (!out_c128) {
-        S = out;
-    } else {
-        TRY(ensure(c->scratch, (size_t)np * ncomp * c->csz()));
-        S = c->scratch.p;
-    }
-    // per-run tables: gx of the graded core and the border absorption
-    const bool core = d.core_dn != 0;
-    const int bpx = (d.border_px > 0 && d.border_strength != 0) ? d.border_px : 0;
-    std::vector<double> tab((size_t)nx + (size_t)bpx);
-    for (int i = 0; i < nx; i++) {
-        const double x = ((double)i - (double)nx / 2) * dx - d.core_x0;
-        tab[i] = core ? std::exp(-(x * x) / (d.core_w * d.core_w)) : 0.0;
-    }
-    for (int q = 0; q < bpx; q++) {
-        double p = 1;
-        const double tq = (double)(bpx - q) / (double)bpx;
-        for (int o = 0; o < d.border_order; o++) p *= tq;
-        tab[(size_t)nx + q] = std::exp(-k * d.border_strength * p * dz);
-    }
-    // uploaded only when they change: a repeated call issues no host copy
-    // (and can then be captured in a CUDA graph)
-    if (tab != c->bpm_tab_host || !c->bpm_tab.p) {
-        TRY(ensure(c->bpm_tab, sizeof(double) * (tab.size() + 1)));
-        // (a copy from pageable memory returns once the source has been read)
-        CK(cudaMemcpyAsync(c->bpm_tab.p, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, c->st));
-        c->bpm_tab_host = tab;
-    }
-    const double* gx = reinterpret_cast<const double*>(c->bpm_tab.p);
-    int nb = 0;
-    FastRows r{};
-    r.rows = ny;
-    r.in = in;
-    r.in_c128 = in_c128;
-    r.in_ld = nx;
-    r.in_bstride = np;
-    r.out = S;
-    r.out_ld = nx;
-    r.out_bstride = np;
-    r.tw = twx;
-    r.out_scale = 1.0;
-    r.batch = ncomp;
-    CK(timed_launch(c, 0, [&] { return fast_rows(c->fp64, nx, t.rowE, false, r, c->st, &nb); }));
-    FastCols kc{};
-    kc.ncols = nx;
-    kc.W = t.colW;
-    kc.data = S;
-    kc.ld = nx;
-    kc.bstride = np;
-    kc.tw = twy;
-    kc.batch = ncomp;
-    kc.wl = cc.wavelength;
-    kc.dx = dx;
-    kc.scale = 1.0 / ((double)nx * (double)ny);
-    kc.zero_ev = pol.zero;
-    kc.precise_phase = 1;
-    kc.conj = adjoint;
-    kc.tw_lo = twy_lo;
-    const double sgn = adjoint ? -1.0 : 1.0;
-    FastRows m = r;
-    m.in = S;
-    m.in_c128 = 0;
-    m.bpm_gx = core ? gx : nullptr;
-    m.bpm_y0 = d.core_y0;
-    m.bpm_w2 = d.core_w * d.core_w;
-    m.bpm_dx = dx;
-    m.bpm_border = bpx ? gx + nx : nullptr;
-    m.bpm_border_px = bpx;
-    m.bpm_nx = nx;
-    m.tw_lo = twx_lo;
-    // Product of the slice constants c_s, each formed as applyMediumPhase forms
-    // the screen of a background pixel (t = exp(-k Im n dz) cexpI(k (Re n - 1)
-    // dz), optics/medium.go:58-59) and multiplied in FP64 complex arithmetic:
-    // the rounding of every factor is then the reference's own.  (Summing the
-    // slice phases instead lets the rounding of a running sum near 10^3 rad
-    // reach ~1e-11 over 400 slices.)
-    double c_re = 1.0, c_im = 0.0;
-    for (int s = 0; s <= steps; s++) {
-        const double zp = (s == 0 || s == steps) ? hz : dz;
-        kc.kz = k * zp;
-        kc.kaz = k * zp;
-        kc.krev = kc.kz / (2 * M_PI);
-        kc.htab = nullptr;
-        TRY(attach_htab(c, kc, ny, colE));  // one table for dz, one for the half steps
-        CK(timed_launch(c, 4, [&] { return sweep_cols(c, ny, colE, kc, &nb); }));
-        if (s < steps) {
-            const int sl = adjoint ? steps - 1 - s : s;
-            const double zc = z * (double)sl / (double)steps + dz / 2;
-            double r0 = d.re_bg, i0 = d.im_bg;
-            for (int q = 0; q < d.n_layers && q < 8; q++)
-                if (zc < d.layer_z[q]) {
-                    r0 = d.layer_re[q];
-                    i0 = d.layer_im[q];
-                    break;
-                }
-            double mod = 1;
-            if (d.zmod_amp != 0) mod = 1.0 + d.zmod_amp * std::sin(2 * M_PI * zc / d.zmod_period + d.zmod_phase);
-            m.bpm_phase = sgn * (k * d.core_dn * mod * dz);
-            const double ph = k * (r0 - 1.0) * dz;
-            const double am = std::exp(-k * i0 * dz);
-            const double tr = am * std::cos(ph), ti = sgn * (am * std::sin(ph));
-            const double nr = c_re * tr - c_im * ti, ni = c_re * ti + c_im * tr;
-            c_re = nr;
-            c_im = ni;
-            CK(timed_launch(c, 0, [&] { return fast_rows_bpm(c->fp64, nx, t.rowE, m, c->st, &nb); }));
-        }
-    }
-    FastRows q = r;
-    q.in = S;
-    q.in_c128 = 0;
-    q.out = out;
-    q.out_c128 = out_c128;
-    q.out_scale = c_re;
-    q.out_scale_im = c_im;
-    CK(timed_launch(c, 1, [&] { return fast_rows(c->fp64, nx, t.rowE, true, q, c->st, &nb); }));
-    return WOS_OK;
-}
-
-int run_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* in, int in_c128, void* out,
-                  int out_c128, double z, const ScreenSrc& src, int steps, const wos_context& cc, wos_diag* d,
-                  bool adjoint = false) {
-    if (d) {
-        std::memset(d, 0, sizeof(*d));
-        d->dx_out = dx;
-    }
-    if (ny < 2 || nx < 2 || ncomp < 1 || ncomp > 2 || !(dx > 0) || !in || !out)
-        return fail(WOS_INVALID_ARG, "invalid field geometry");
-    if (z == 0) {
-        Prop p{ny, nx, dx, ncomp, in, in_c128, out, out_c128, 0.0, WOS_ASM, cc, nullptr};
-        return copy_field(c, p);
-    }
-    if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
-    if (steps <= 0) steps = 1;
-    {
-        const int rc = try_fast_splitstep(c, ny, nx, dx, ncomp, in, in_c128, out, out_c128, z, src, steps, cc,
-                                          d != nullptr, adjoint);
-        if (rc != -1) return rc;
-    }
-    const double dz = z / (double)steps;
-    const double k = 2 * M_PI / cc.wavelength;
-    const double hz = dz / 2;
-    const Policy pol = ev_policy(cc, hz);
-    Axis *ax, *ay;
-    TRY(get_axis(c, nx, c->fp64, &ax));
-    TRY(get_axis(c, ny, c->fp64, &ay));
-    const long long np = (long long)ny * nx;
-    void* S;
-    if (!out_c128) {
-        S = out;
-    } else {
-        TRY(ensure(c->scratch, (size_t)np * ncomp * c->csz()));
-        S = c->scratch.p;
-    }
-    const int W = auto_colw(c, ay->L);
-    const size_t nbr = row_blocks(c->fp64, ax->L, ny, ncomp);
-    const size_t nbc = col_blocks(c->fp64, ay->L, W, nx, ncomp);
-    TRY(red_prepare(c, std::max(nbr, nbc)));
-    const bool diag = d != nullptr;
-    const bool wrap = wrap_needed(cc, ny, nx, dx, hz);
-    const int npass = steps + 1;
-    if (diag) TRY(ensure(c->tmp, sizeof(double) * RS_COUNT * (size_t)npass));
-    double* passes = reinterpret_cast<double*>(c->tmp.p);
-
-    RowArgs r = row_defaults(ny, nx, dx);
-    r.mode = ROW_FWD;
-    r.rows = ny;
-    fill_axis(r, ax);
-    r.in = in;
-    r.in_c128 = in_c128;
-    r.in_ld = nx;
-    r.in_bstride = np;
-    r.in_n = nx;
-    r.out = S;
-    r.out_ld = nx;
-    r.out_bstride = np;
-    r.out_n = nx;
-    r.batch = ncomp;
-    if (diag) {
-        r.red = red_region(c, 0);
-        r.red_pre = 1;
-    }
-    CK(prof_rows(c, c->fp64, r));
-    if (diag) CK(launch_reduce_finish(r.red, (int)nbr, 1, RS_P, 1, redout_region(c, 0), c->st));
-
-    for (int s = 0; s <= steps; s++) {
-        ColArgs a = col_defaults(c, dx);
-        a.mode = COL_FUSED;
-        a.ncols = nx;
-        fill_axis(a, ay);
-        a.W = W;
-        a.src = S;
-        a.src_ld = nx;
-        a.src_bstride = np;
-        a.in_n = ny;
-        a.dst = S;
-        a.dst_ld = nx;
-        a.dst_bstride = np;
-        a.out_n = ny;
-        a.h = asm_h(c, cc, hz, pol, dx, nx, ny);
-        a.h.kind = (s == 0 || s == steps) ? H_ASM : H_ASM_HALF2;
-        a.h.conj = adjoint;
-        a.batch = ncomp;
-        if (diag) {
-            a.red = red_region(c, 1);
-            a.red_bpm = 1;
-            if (wrap) {
-                a.red_hist = 1;
-                a.hist_lx = nx;
-                a.hist_ly = ny;
-                a.hist_dx = dx;
-            }
-        }
-        CK(prof_cols(c, c->fp64, a));
-        if (diag) {
-            CK(launch_reduce_finish(a.red, (int)nbc, 1, RS_SW, 3, passes + (size_t)s * RS_COUNT, c->st));
-            if (wrap) CK(launch_reduce_finish(a.red, (int)nbc, 1, RS_HIST, 97, passes + (size_t)s * RS_COUNT, c->st));
-        }
-        if (s < steps) {
-            RowArgs q = row_defaults(ny, nx, dx);
-            q.mode = ROW_INV_FWD;
-            q.rows = ny;
-            fill_axis(q, ax);
-            q.in = S;
-            q.in_ld = nx;
-            q.in_bstride = np;
-            q.in_n = nx;
-            q.out = S;
-            q.out_ld = nx;
-            q.out_bstride = np;
-            q.out_n = nx;
-            q.batch = ncomp;
-            const int sl = adjoint ? steps - 1 - s : s;
-            const double zc = z * (double)sl / (double)steps + dz / 2;
-            fill_screen(q.scr, src, sl, np, k, dz, zc);
-            q.scr.conj = adjoint;
-            CK(prof_rows(c, c->fp64, q));
-        }
-    }
-    RowArgs q = row_defaults(ny, nx, dx);
-    q.mode = ROW_INV;
-    q.rows = ny;
-    fill_axis(q, ax);
-    q.in = S;
-    q.in_ld = nx;
-    q.in_bstride = np;
-    q.in_n = nx;
-    q.out = out;
-    q.out_c128 = out_c128;
-    q.out_ld = nx;
-    q.out_bstride = np;
-    q.out_n = nx;
-    q.batch = ncomp;
-    if (diag) {
-        q.red = red_region(c, 2);
-        q.red_post = 1;
-    }
-    CK(prof_rows(c, c->fp64, q));
-    if (diag) {
-        CK(launch_reduce_finish(q.red, (int)nbr, 1, RS_P, 1, redout_region(c, 2), c->st));
-        TRY(fetch_red(c, 3));
-        d->p_in = c->hred[RS_P] * dx * dx;
-        d->p_out = c->hred[2 * RS_COUNT + RS_P] * dx * dx;
-        std::vector<double> h((size_t)npass * RS_COUNT);
-        CK(cudaMemcpy(h.data(), passes, sizeof(double) * h.size(), cudaMemcpyDeviceToHost));
-        for (int s = 0; s <= steps; s++) {
-            const double* rr = h.data() + (size_t)s * RS_COUNT;
-            const double p0 = rr[RS_SW], l1 = rr[RS_SW + 1], l2 = rr[RS_SW + 2];
-            // half step(s) of this pass: P0 -> P0-L1 and, for merged passes, P0-L1 -> P0-L1-L2
-            const int nh = (s == 0 || s == steps) ? 1 : 2;
-            for (int hh = 0; hh < nh; hh++) {
-                if (wrap) wrap_finish(d, cc, ny, nx, dx, hz, rr + RS_HIST);
-                if (hh == 0) asm_warn(d, hz, p0, p0 - l1, pol);
-                else asm_warn(d, hz, p0 - l1, (p0 - l1) - l2, pol);
-            }
-        }
-    }
-    return WOS_OK;
-}
-
-// FFT2D of a complex128 device array in FP64, whatever the context precision
-// (one-time source synthesis).
-int fft2d_fp64(wos_ctx c, int n, int batch, double2* a, int inverse) {
-    return fft2d_impl(c, 1, n, n, batch, a, inverse);
-}
-
-// GenerateSchellRealizations (optics/coherence.go:22-80) into modes (device, complex128)
-int schell_generate(wos_ctx c, int n, double dx, double width, double coh, int m, const wos_c128* noise,
-                    double2* modes) {
-    const long long nn = (long long)n * n;
-    TRY(ensure(c->aux, (size_t)nn * (16 + 8)));
-    double2* mu = reinterpret_cast<double2*>(c->aux.p);
-    double* sqs = reinterpret_cast<double*>(mu + nn);
-    CK(launch_schell_mu(mu, n, dx, coh, c->st));
-    TRY(fft2d_fp64(c, n, 1, mu, 0));
-    CK(launch_sqrt_re(sqs, mu, nn, c->st));
-    CK(cudaMemcpyAsync(modes, noise, (size_t)nn * m * 16, cudaMemcpyHostToDevice, c->st));
-    CK(launch_mul_map(modes, sqs, nn, m, c->st));
-    TRY(fft2d_fp64(c, n, m, modes, 1));
-    CK(launch_schell_env(modes, n, dx, width, m, c->st));
-    return WOS_OK;
-}
-
-// Batched ASM over units that share a geometry (polychromatic wavelengths,
-// volume distances, coherent modes): one row sweep per unit set, one column
-// launch per chunk with gridDim.y = units, then either a batched inverse row
-// sweep (planes out) or an accumulating one (intensity out).
-struct Batch {
-    int ny, nx, ncomp;
-    double dx;
-    const void* in;       // complex128 device input [ncomp or units][ny][nx]
-    long long in_unit_stride;  // elements between units of the input (0: shared input)
-    int units;
-    const double* wl_dev;  // per-unit wavelength (device) or null
-    const double* z_dev;   // per-unit z (device) or null
-    std::vector<double> wl, z;  // host copies
-    const double* w_dev;   // per-unit intensity weight (device) or null
-    double* out_int;       // device [ny][nx] FP64 intensity accumulation, or null
-    void* out_planes;      // device complex128 [units][ncomp][ny][nx], or null
-    wos_context cc;
-    wos_diag* diag;
-};
-
-// Batched ASM on the specialised sweeps (power-of-two grids): the forward row
-// sweep once per component for a shared input, then per chunk of units one
-// column sweep (gridDim.y = units, per-unit wavelength / distance, the shared
-// row spectrum as its source) and one row sweep that either accumulates the
-// weighted intensity of the chunk in registers or writes each unit's plane.
-// Diagnostics: per-unit spectral loss sums and histograms from the column
-// records, input power from the row records.  -1: not eligible.
-int try_fast_batch(wos_ctx c, Batch& b, std::vector<double>& sums, std::vector<double>& pin_unit,
-                   double& pin_total) {
-    const int ny = b.ny, nx = b.nx, ncomp = b.ncomp;
-    if (c->no_fast || !is_pow2(nx) || !is_pow2(ny)) return -1;
-    if (!c->fp64) {
-        for (int u = 0; u < b.units; u++) {
-            const double wl = b.wl.empty() ? b.cc.wavelength : b.wl[u];
-            const double z = b.z.empty() ? 0.0 : b.z[u];
-            if (!(std::fabs(z / wl) < 268435456.0)) return -1;
-        }
-    }
-    const Tune t = get_tune(c, ny, nx);
-    if (!fast_supported(c->fp64, nx, t.rowE) || !fast_supported(c->fp64, ny, t.colE)) return -1;
-    const double dx = b.dx;
-    const long long np = (long long)ny * nx;
-    const bool shared_in = b.in_unit_stride == 0;
-    const bool diag = b.diag != nullptr;
-    Axis *ax, *ay;
-    TRY(get_axis(c, nx, c->fp64, &ax));
-    TRY(get_axis(c, ny, c->fp64, &ay));
-    const void *twx, *twy;
-    TRY(fast_tw(c, ax, t.rowE, &twx));
-    TRY(fast_tw(c, ay, t.colE, &twy));
-    const size_t per = (size_t)np * c->csz();
-    int B = (int)std::max<size_t>(1, ((size_t)4 << 30) / per);
-    B = std::min(B, b.units);
-    B = std::min(B, 65535);
-    const size_t nbr = fast_row_blocks(nx, t.rowE, ny, shared_in ? 1 : B);
-    const size_t nbc = fast_col_blocks(c->fp64, ny, t.colE, t.colW, nx, 1);
-    TRY(red_prepare(c, std::max(nbr, nbc * (size_t)B)));
-    if (diag) TRY(ensure(c->tmp, sizeof(double) * RS_COUNT * (size_t)B));
-    TRY(ensure(c->scratch, (size_t)(shared_in ? 1 : B) * per));
-    TRY(ensure(c->scratch2, (size_t)B * per));
-    void* S0 = c->scratch.p;
-    void* S1 = c->scratch2.p;
-    const Policy pol = ev_policy(b.cc, b.z.empty() ? 1.0 : b.z[0]);
-    const HArgs h = asm_h(c, b.cc, b.z.empty() ? 0.0 : b.z[0], pol, dx, nx, ny);
-    double* o = reinterpret_cast<double*>(c->tmp.p);
-    int nb = 0;
-    for (int comp = 0; comp < ncomp; comp++) {
-        for (int k0 = 0; k0 < b.units; k0 += B) {
-            const int nu = std::min(B, b.units - k0);
-            if (k0 == 0 || !shared_in) {
-                FastRows r{};
-                r.rows = ny;
-                r.in = reinterpret_cast<const double2*>(b.in) +
-                       (shared_in ? comp * np : ((long long)k0 * ncomp + comp) * np);
-                r.in_c128 = 1;
-                r.in_ld = nx;
-                r.in_bstride = shared_in ? 0 : ncomp * np;
-                r.out = S0;
-                r.out_ld = nx;
-                r.out_bstride = np;
-                r.tw = twx;
-                r.out_scale = 1.0;
-                r.batch = shared_in ? 1 : nu;
-                if (diag) {
-                    r.red = red_region(c, 0) + RS_P;
-                    r.red_stride = RS_COUNT;
-                }
-                CK(timed_launch(c, 0, [&] { return fast_rows(c->fp64, nx, t.rowE, false, r, c->st, &nb); }));
-                if (diag) {
-                    const int per_unit = nb / r.batch;
-                    CK(launch_reduce_finish(red_region(c, 0), per_unit, r.batch, RS_P, 1, o, c->st));
-                    std::vector<double> hh((size_t)r.batch * RS_COUNT);
-                    CK(cudaMemcpyAsync(hh.data(), o, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost, c->st));
-                    CK(cudaStreamSynchronize(c->st));
-                    for (int u = 0; u < r.batch; u++) {
-                        const double p = hh[(size_t)u * RS_COUNT + RS_P] * dx * dx;
-                        if (shared_in) pin_total += p;
-                        else pin_unit[k0 + u] += p;
-                    }
-                }
-            }
-            FastCols k{};
-            k.ncols = nx;
-            k.W = t.colW;
-            k.data = S1;
-            k.ld = nx;
-            k.bstride = np;
-            k.src = S0;
-            k.src_bstride = shared_in ? 0 : np;
-            k.tw = twy;
-            k.batch = nu;
-            k.wl = b.cc.wavelength;
-            k.dx = dx;
-            k.z = b.z.empty() ? 0.0 : b.z[0];
-            k.kz = h.kz;
-            k.kaz = h.kaz;
-            k.krev = h.kz / (2 * M_PI);
-            k.batch_wl = b.wl_dev ? b.wl_dev + k0 : nullptr;
-            k.batch_z = b.z_dev ? b.z_dev + k0 : nullptr;
-            k.scale = h.scale;
-            k.alpha = h.alpha;
-            k.limit = h.limit;
-            k.zero_ev = h.zero_ev;
-            k.reg = h.reg;
-            k.backward = h.z < 0;
-            if (diag) {
-                k.red = red_region(c, 1) + RS_SW;
-                k.red_stride = RS_COUNT;
-                k.hist = red_region(c, 1) + RS_HIST;
-                k.hist_dx = dx;
-            }
-            CK(timed_launch(c, 4, [&] { return sweep_cols(c, ny, t.colE, k, &nb); }));
-            if (diag) {
-                const int per_unit = nb / nu;
-                CK(launch_reduce_finish(red_region(c, 1), per_unit, nu, RS_SW, 2, o, c->st));
-                CK(launch_reduce_finish(red_region(c, 1), per_unit, nu, RS_HIST, 97, o, c->st));
-                std::vector<double> hh((size_t)nu * RS_COUNT);
-                CK(cudaMemcpyAsync(hh.data(), o, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost, c->st));
-                CK(cudaStreamSynchronize(c->st));
-                for (int u = 0; u < nu; u++)
-                    for (int sl = RS_SW; sl < RS_COUNT; sl++)
-                        sums[((size_t)(k0 + u) * ncomp + comp) * RS_COUNT + sl] = hh[(size_t)u * RS_COUNT + sl];
-            }
-            FastRows q{};
-            q.rows = ny;
-            q.in = S1;
-            q.in_ld = nx;
-            q.in_bstride = np;
-            q.tw = twx;
-            q.out_scale = 1.0;
-            if (b.out_int) {
-                AccArgs acc{nu, b.w_dev ? b.w_dev + k0 : nullptr, b.out_int, 1};
-                CK(timed_launch(c, 1, [&] { return fast_rows_acc(c->fp64, nx, t.rowE, q, acc, c->st, &nb); }));
-            } else {
-                q.out = reinterpret_cast<double2*>(b.out_planes) + ((long long)k0 * ncomp + comp) * np;
-                q.out_c128 = 1;
-                q.out_ld = nx;
-                q.out_bstride = ncomp * np;
-                q.batch = nu;
-                CK(timed_launch(c, 1, [&] { return fast_rows(c->fp64, nx, t.rowE, true, q, c->st, &nb); }));
-            }
-        }
-    }
-    return WOS_OK;
-}
-
-int run_batch_asm(wos_ctx c, Batch& b) {
-    const int ny = b.ny, nx = b.nx, ncomp = b.ncomp;
-    const double dx = b.dx;
-    const long long np = (long long)ny * nx;
-    Axis *ax, *ay;
-    TRY(get_axis(c, nx, c->fp64, &ax));
-    TRY(get_axis(c, ny, c->fp64, &ay));
-    const int W = auto_colw(c, ay->L);
-    const bool shared_in = b.in_unit_stride == 0;
-    // chunk the units so the per-chunk spectra stay within ~4 GiB
-    const size_t per = (size_t)np * c->csz();
-    int B = (int)std::max<size_t>(1, ((size_t)4 << 30) / per);
-    B = std::min(B, b.units);
-    B = std::min(B, 65535);
-    const size_t nbr1 = row_blocks(c->fp64, ax->L, ny, shared_in ? 1 : B);
-    const size_t nbc1 = col_blocks(c->fp64, ay->L, W, nx, 1);
-    TRY(red_prepare(c, std::max(nbr1, nbc1 * (size_t)B)));
-    const bool diag = b.diag != nullptr;
-    // spectral sums per unit and component, plus a histogram per unit
-    std::vector<double> sums((size_t)b.units * RS_COUNT * ncomp, 0.0);
-    if (diag) TRY(ensure(c->tmp, sizeof(double) * RS_COUNT * (size_t)B));
-    TRY(ensure(c->scratch, (size_t)(shared_in ? 1 : B) * per));
-    TRY(ensure(c->scratch2, (size_t)B * per));
-    void* S0 = c->scratch.p;
-    void* S1 = c->scratch2.p;
-    const Policy pol = ev_policy(b.cc, b.z.empty() ? 1.0 : b.z[0]);
-    double pin_total = 0;
-    std::vector<double> pin_unit(b.units, 0.0);
-    const int fast = try_fast_batch(c, b, sums, pin_unit, pin_total);
-    if (fast != -1 && fast != WOS_OK) return fast;
-    for (int comp = 0; comp < ncomp && fast == -1; comp++) {
-        for (int k0 = 0; k0 < b.units; k0 += B) {
-            const int nb = std::min(B, b.units - k0);
-            // rows forward (the shared input once per component, else per unit)
-            if (k0 == 0 || !shared_in) {
-                RowArgs r = row_defaults(ny, nx, dx);
-                r.mode = ROW_FWD;
-                r.rows = ny;
-                fill_axis(r, ax);
-                r.in = reinterpret_cast<const double2*>(b.in) +
-                       (shared_in ? comp * np : ((long long)k0 * ncomp + comp) * np);
-                r.in_c128 = 1;
-                r.in_ld = nx;
-                r.in_bstride = shared_in ? 0 : ncomp * np;
-                r.in_n = nx;
-                r.out = S0;
-                r.out_ld = nx;
-                r.out_bstride = np;
-                r.out_n = nx;
-                r.batch = shared_in ? 1 : nb;
-                if (diag) {
-                    r.red = red_region(c, 0);
-                    r.red_pre = 1;
-                }
-                CK(prof_rows(c, c->fp64, r));
-                if (diag) {
-                    const int nbr = (int)row_blocks(c->fp64, ax->L, ny, 1);
-                    CK(launch_reduce_finish(r.red, nbr, r.batch, RS_P, 1, reinterpret_cast<double*>(c->tmp.p), c->st));
-                    std::vector<double> h((size_t)r.batch * RS_COUNT);
-                    CK(cudaMemcpyAsync(h.data(), c->tmp.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
-                    CK(cudaStreamSynchronize(c->st));
-                    for (int u = 0; u < r.batch; u++) {
-                        const double p = h[(size_t)u * RS_COUNT + RS_P] * dx * dx;
-                        if (shared_in) pin_total += p;
-                        else pin_unit[k0 + u] += p;
-                    }
-                }
-            }
-            ColArgs a = col_defaults(c, dx);
-            a.mode = COL_FUSED;
-            a.ncols = nx;
-            fill_axis(a, ay);
-            a.W = W;
-            a.src = S0;
-            a.src_ld = nx;
-            a.src_bstride = np;
-            a.src_shared = shared_in;
-            a.in_n = ny;
-            a.dst = S1;
-            a.dst_ld = nx;
-            a.dst_bstride = np;
-            a.out_n = ny;
-            a.h = asm_h(c, b.cc, b.z.empty() ? 0.0 : b.z[0], pol, dx, nx, ny);
-            a.h.wl = -1;  // per-unit k, k z, k |z| are formed on the device from wl and z
-            a.batch_wl = b.wl_dev ? b.wl_dev + k0 : nullptr;
-            a.batch_z = b.z_dev ? b.z_dev + k0 : nullptr;
-            if (!b.wl_dev) a.h.wl = b.cc.wavelength, a.h.k = 2 * M_PI / b.cc.wavelength;
-            a.batch = nb;
-            if (diag) {
-                a.red = red_region(c, 1);
-                a.red_bpm = 1;
-                a.red_hist = 1;
-                a.hist_lx = nx;
-                a.hist_ly = ny;
-                a.hist_dx = dx;
-            }
-            CK(prof_cols(c, c->fp64, a));
-            if (diag) {
-                double* o = reinterpret_cast<double*>(c->tmp.p);
-                CK(launch_reduce_finish(a.red, (int)nbc1, nb, RS_SW, 3, o, c->st));
-                CK(launch_reduce_finish(a.red, (int)nbc1, nb, RS_HIST, 97, o, c->st));
-                std::vector<double> h((size_t)nb * RS_COUNT);
-                CK(cudaMemcpyAsync(h.data(), o, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
-                CK(cudaStreamSynchronize(c->st));
-                for (int u = 0; u < nb; u++)
-                    for (int sl = RS_SW; sl < RS_COUNT; sl++)
-                        sums[((size_t)(k0 + u) * ncomp + comp) * RS_COUNT + sl] = h[(size_t)u * RS_COUNT + sl];
-            }
-            RowArgs q = row_defaults(ny, nx, dx);
-            q.rows = ny;
-            fill_axis(q, ax);
-            q.in = S1;
-            q.in_ld = nx;
-            q.in_bstride = np;
-            q.in_n = nx;
-            q.out_ld = nx;
-            q.out_n = nx;
-            if (b.out_int) {
-                q.mode = ROW_INV_ACC;
-                q.acc_nb = nb;
-                q.acc_weight = b.w_dev ? b.w_dev + k0 : nullptr;
-                q.acc_add = 1;
-                q.out = b.out_int;
-                q.out_accum_int = 2;
-                q.out_bstride = 0;
-                q.batch = 1;
-            } else {
-                q.mode = ROW_INV;
-                q.out = reinterpret_cast<double2*>(b.out_planes) + ((long long)k0 * ncomp + comp) * np;
-                q.out_c128 = 1;
-                q.out_bstride = ncomp * np;
-                q.batch = nb;
-            }
-            CK(prof_rows(c, c->fp64, q));
-        }
-    }
-    if (diag) {
-        // per unit, in order: asmWrapWarn then asmWarn (optics/propagate.go:325-332)
-        for (int u = 0; u < b.units; u++) {
-            wos_context cu = b.cc;
-            if (!b.wl.empty()) cu.wavelength = b.wl[u];
-            const double zu = b.z.empty() ? 0.0 : b.z[u];
-            if (zu == 0) continue;
-            double sw = 0, s1 = 0, hist[97] = {0};
-            for (int comp = 0; comp < ncomp; comp++) {
-                const double* rr = &sums[((size_t)u * ncomp + comp) * RS_COUNT];
-                sw += rr[RS_SW];
-                s1 += rr[RS_SW + 1];
-                for (int k = 0; k < 97; k++) hist[k] += rr[RS_HIST + k];
-            }
-            if (wrap_needed(cu, ny, nx, dx, zu)) wrap_finish(b.diag, cu, ny, nx, dx, zu, hist);
-            const double pin = shared_in ? pin_total : pin_unit[u];
-            const double frac = sw > 0 ? s1 / sw : 0.0;  // spectral loss fraction of the step
-            asm_warn(b.diag, zu, pin, pin - pin * frac, ev_policy(cu, zu));
-        }
-    }
-    return WOS_OK;
-}
-
-int upload_params(wos_ctx c, const std::vector<double>& a, const std::vector<double>& b2,
-                  const std::vector<double>& c3, double** pa, double** pb, double** pc) {
-    const size_t n = a.size() + b2.size() + c3.size();
-    TRY(ensure(c->params, sizeof(double) * std::max<size_t>(n, 1)));
-    double* p = reinterpret_cast<double*>(c->params.p);
-    std::vector<double> all;
-    all.insert(all.end(), a.begin(), a.end());
-    all.insert(all.end(), b2.begin(), b2.end());
-    all.insert(all.end(), c3.begin(), c3.end());
-    if (n) CK(cudaMemcpyAsync(p, all.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
-    *pa = p;
-    *pb = p + a.size();
-    *pc = p + a.size() + b2.size();
-    return WOS_OK;
-}
-
-int element_begin(wos_ctx c, wos_field* f) {
-    TRY(check_field(f));
-    TRY(set_device(c));
-    return stage_in(c, f, f->polarized ? 2 : 1);
-}
-double2* stage_ex(wos_ctx c) { return reinterpret_cast<double2*>(c->stage.p); }
-double2* stage_ey(wos_ctx c, const wos_field* f) { return stage_ex(c) + (size_t)f->ny * f->nx; }
-
-// Inverse design on the specialised sweeps (power-of-two grids): five sweeps,
-// forward ASM of a exp(i phi) | residual between the inverse and the forward
-// transform of the middle row sweep | adjoint ASM | gradient in the last row
-// sweep.  a: complex128 when a_c128, else the context's complex type; phi,
-// target, grad: FP64 device arrays (grad null: loss only).  -1: not eligible.
-int asm_design_fast(wos_ctx c, int ny, int nx, double dx, double z, const wos_context& cc, const void* a,
-                    int a_c128, const double* phi, const double* target, double* loss, double* grad) {
-    if (c->no_fast || !is_pow2(nx) || !is_pow2(ny)) return -1;
-    const double k = 2 * M_PI / cc.wavelength;
-    if (!c->fp64 && !(std::fabs(k * z / (2 * M_PI)) < 268435456.0)) return -1;
-    const Tune t = get_tune(c, ny, nx);
-    if (!fast_supported(c->fp64, nx, t.rowE) || !fast_supported(c->fp64, ny, t.colE)) return -1;
-    Axis *ax, *ay;
-    TRY(get_axis(c, nx, c->fp64, &ax));
-    TRY(get_axis(c, ny, c->fp64, &ay));
-    const void *twx, *twy;
-    TRY(fast_tw(c, ax, t.rowE, &twx));
-    TRY(fast_tw(c, ay, t.colE, &twy));
-    const long long np = (long long)ny * nx;
-    TRY(ensure(c->scratch, (size_t)np * c->csz()));
-    void* S = c->scratch.p;
-    TRY(red_prepare(c, fast_row_blocks(nx, t.rowE, ny, 1)));
-    const Policy pol = ev_policy(cc, z);
-    const HArgs h = asm_h(c, cc, z, pol, dx, nx, ny);
-    FastCols kc{};
-    kc.ncols = nx;
-    kc.W = t.colW;
-    kc.data = S;
-    kc.ld = nx;
-    kc.bstride = np;
-    kc.tw = twy;
-    kc.batch = 1;
-    kc.wl = h.wl;
-    kc.dx = h.dx;
-    kc.kz = h.kz;
-    kc.kaz = h.kaz;
-    kc.krev = h.kz / (2 * M_PI);
-    kc.scale = h.scale;
-    kc.alpha = h.alpha;
-    kc.limit = h.limit;
-    kc.zero_ev = h.zero_ev;
-    kc.reg = h.reg;
-    kc.backward = h.z < 0;
-    FastRows r{};
-    r.rows = ny;
-    r.in = S;
-    r.in_ld = nx;
-    r.in_bstride = np;
-    r.out = S;
-    r.out_ld = nx;
-    r.out_bstride = np;
-    r.tw = twx;
-    r.out_scale = 1.0;
-    r.batch = 1;
-    r.red = red_region(c, 0) + RS_P;
-    r.red_stride = RS_COUNT;
-    DesignArgs dd{phi, target, a, a_c128, grad};
-    int nb = 0;
-    CK(timed_launch(c, 0, [&] { return fast_rows_design(c->fp64, nx, t.rowE, 0, r, dd, c->st, &nb); }));
-    CK(timed_launch(c, 4, [&] { return sweep_cols(c, ny, t.colE, kc, &nb); }));
-    CK(timed_launch(c, 1, [&] { return fast_rows_design(c->fp64, nx, t.rowE, 1, r, dd, c->st, &nb); }));
-    CK(launch_reduce_finish(red_region(c, 0), nb, 1, RS_P, 1, redout_region(c, 0), c->st));
-    if (grad) {
-        kc.conj = 1;
-        CK(timed_launch(c, 4, [&] { return sweep_cols(c, ny, t.colE, kc, &nb); }));
-        CK(timed_launch(c, 1, [&] { return fast_rows_design(c->fp64, nx, t.rowE, 2, r, dd, c->st, &nb); }));
-    }
-    TRY(fetch_red(c, 1));
-    *loss = c->hred[RS_P];
-    return WOS_OK;
-}
-
-// Inverse design on a host problem: forward (and adjoint) of one ASM step.
-int asm_loss_grad_impl(wos_ctx c, int ny, int nx, double dx, double z, const wos_context* cc, const wos_c128* a,
-                       const double* phi, const double* target, double* loss, double* grad) {
-    if (!cc || !a || !phi || !target || !loss || ny < 2 || nx < 2 || !(dx > 0))
-        return fail(WOS_INVALID_ARG, "inverse-design arguments");
-    if (!(cc->wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
-    const long long np = (long long)ny * nx;
-    TRY(set_device(c));
-    TRY(ensure(c->stage, (size_t)np * 16));
-    TRY(ensure(c->maps, (size_t)np * 8 * 3));
-    TRY(ensure(c->scratch, (size_t)np * c->csz()));
-    TRY(ensure(c->scratch2, (size_t)np * c->csz()));
-    double* phid = reinterpret_cast<double*>(c->maps.p);
-    double* Td = phid + np;
-    double* gd = Td + np;
-    CK(cudaMemcpyAsync(c->stage.p, a, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(phid, phi, (size_t)np * 8, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(Td, target, (size_t)np * 8, cudaMemcpyHostToDevice, c->st));
-    {
-        const int rc = asm_design_fast(c, ny, nx, dx, z, *cc, c->stage.p, 1, phid, Td, loss, grad ? gd : nullptr);
-        if (rc != -1) {
-            if (rc == WOS_OK && grad) {
-                CK(cudaMemcpyAsync(grad, gd, (size_t)np * 8, cudaMemcpyDeviceToHost, c->st));
-                CK(cudaStreamSynchronize(c->st));
-            }
-            return rc;
-        }
-    }
-    Axis *ax, *ay;
-    TRY(get_axis(c, nx, c->fp64, &ax));
-    TRY(get_axis(c, ny, c->fp64, &ay));
-    const Policy pol = ev_policy(*cc, z);
-    const int W = auto_colw(c, ay->L);
-    void* S = c->scratch.p;
-    void* U = c->scratch2.p;
-    const int nres = (int)((np + 255) / 256);
-    TRY(red_prepare(c, (size_t)nres));
-    auto rows = [&](int mode, const void* in, int in_c128, void* out, const double* pphi) -> int {
-        RowArgs r = row_defaults(ny, nx, dx);
-        r.mode = mode;
-        r.rows = ny;
-        fill_axis(r, ax);
-        r.in = in;
-        r.in_c128 = in_c128;
-        r.in_ld = nx;
-        r.in_n = nx;
-        r.out = out;
-        r.out_ld = nx;
-        r.out_n = nx;
-        r.pre_phi = pphi;
-        CK(prof_rows(c, c->fp64, r));
-        return WOS_OK;
-    };
-    auto cols = [&](int conj) -> int {
-        ColArgs k = col_defaults(c, dx);
-        k.mode = COL_FUSED;
-        k.ncols = nx;
-        fill_axis(k, ay);
-        k.W = W;
-        k.src = S;
-        k.src_ld = nx;
-        k.in_n = ny;
-        k.dst = S;
-        k.dst_ld = nx;
-        k.out_n = ny;
-        k.h = asm_h(c, *cc, z, pol, dx, nx, ny);
-        k.h.conj = conj;
-        CK(prof_cols(c, c->fp64, k));
-        return WOS_OK;
-    };
-    // forward: u = A (a exp(i phi))
-    TRY(rows(ROW_FWD, c->stage.p, 1, S, phid));
-    TRY(cols(0));
-    TRY(rows(ROW_INV, S, 0, U, nullptr));
-    // residual r = 4 (|u|^2 - T) u, loss = sum (|u|^2 - T)^2
-    int nb = 0;
-    CK(launch_residual(c->fp64, U, Td, S, np, red_region(c, 0), &nb, c->st));
-    CK(launch_reduce_finish(red_region(c, 0), nb, 1, RS_P, 1, redout_region(c, 0), c->st));
-    if (grad) {
-        // adjoint: b = A^H r = F^-1 diag(conj H) F r; grad = Re(conj(b) i t a)
-        TRY(rows(ROW_FWD, S, 0, S, nullptr));
-        TRY(cols(1));
-        TRY(rows(ROW_INV, S, 0, S, nullptr));
-        CK(launch_grad(c->fp64, S, reinterpret_cast<const double2*>(c->stage.p), phid, gd, np, c->st));
-        CK(cudaMemcpyAsync(grad, gd, (size_t)np * 8, cudaMemcpyDeviceToHost, c->st));
-    }
-    TRY(fetch_red(c, 1));
-    *loss = c->hred[RS_P];
-    return WOS_OK;
-}
-
-// Diffractive stack (no reference counterpart): u = a; for each layer l,
-// v_l = u exp(i phi_l) and u = BPM_zseg(v_l); L = sum (|u|^2 - T)^2.  The
-// gradient runs the adjoint chain b = BPM^H(r) from r = dL/du* = 4 (|u|^2 - T) u:
-// dL/dphi_l = Re(conj(b_l) i v_l), then b <- exp(-i phi_l) b.  The BPM is
-// linear in the field, so its adjoint needs no forward state inside a
-// segment: the only stored states are the nl fields v_l at the masks.
-// a: complex128 when a_c128, else the context's type; phis [nl][ny][nx],
-// target, grads: FP64 device arrays (grads null: loss only).
-int bpm_stack_impl(wos_ctx c, int ny, int nx, double dx, int nl, const void* a, int a_c128, const double* phis,
-                   const double* T, double zseg, int steps, const wos_index_desc& medium, const wos_context& cc,
-                   double* loss, double* grads) {
-    if (nl < 1 || steps < 1 || ny < 2 || nx < 2 || !(dx > 0) || !a || !phis || !T || !loss)
-        return fail(WOS_INVALID_ARG, "bpm stack arguments");
-    if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
-    const long long np = (long long)ny * nx;
-    const size_t fb = (size_t)np * c->csz();
-    TRY(ensure(c->scratch2, fb));
-    TRY(ensure(c->vol, fb * (size_t)nl));
-    TRY(red_prepare(c, (size_t)((np + 255) / 256)));
-    void* U = c->scratch2.p;
-    char* V = reinterpret_cast<char*>(c->vol.p);
-    if (a_c128 && !c->fp64) CK(launch_convert(0, a, U, np, c->st));
-    else CK(cudaMemcpyAsync(U, a, fb, cudaMemcpyDeviceToDevice, c->st));
-    ScreenSrc src;
-    src.kind = 1;
-    src.desc = medium;
-    for (int l = 0; l < nl; l++) {
-        CK(launch_mask_phase(c->fp64, U, phis + (size_t)l * np, np, 0, c->st));
-        CK(cudaMemcpyAsync(V + (size_t)l * fb, U, fb, cudaMemcpyDeviceToDevice, c->st));
-        TRY(run_splitstep(c, ny, nx, dx, 1, U, 0, U, 0, zseg, src, steps, cc, nullptr, false));
-    }
-    int nb = 0;
-    CK(launch_residual(c->fp64, U, T, U, np, red_region(c, 0), &nb, c->st));
-    CK(launch_reduce_finish(red_region(c, 0), nb, 1, RS_P, 1, redout_region(c, 0), c->st));
-    if (grads) {
-        for (int l = nl - 1; l >= 0; l--) {
-            TRY(run_splitstep(c, ny, nx, dx, 1, U, 0, U, 0, zseg, src, steps, cc, nullptr, true));
-            CK(launch_grad_v(c->fp64, U, V + (size_t)l * fb, grads + (size_t)l * np, np, c->st));
-            if (l > 0) CK(launch_mask_phase(c->fp64, U, phis + (size_t)l * np, np, 1, c->st));
-        }
-    }
-    CK(cudaMemcpyAsync(c->err_host, c->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
-    TRY(fetch_red(c, 1));
-    *loss = c->hred[RS_P];
-    return check_err_word(c);
-}
-
-}  // namespace
-
-extern "C" {
-
-int wos_splitstep(wos_ctx c, wos_field* f, double z, const wos_index_desc* n, int steps, const wos_context* cc,
-                  wos_diag* diag) {
-    if (!c || !n) return fail(WOS_INVALID_ARG, "null argument");
-    TRY(check_field(f));
-    if (diag) {
-        std::memset(diag, 0, sizeof(*diag));
-        diag->dx_out = f->dx;
-    }
-    if (z == 0) return WOS_OK;
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const int ncomp = f->polarized ? 2 : 1;
-    TRY(stage_in(c, f, ncomp));
-    ScreenSrc src;
-    src.kind = 1;
-    src.desc = *n;
-    TRY(run_splitstep(c, f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, c->stage.p, 1, z, src, steps,
-                      cc ? *cc : default_context(), diag));
-    return stage_out(c, f, ncomp);
-}
-
-int wos_splitstep_dev(wos_ctx c, int ny, int nx, double dx, int ncomp, void* field, double z,
-                      const wos_index_desc* n, int steps, const wos_context* cc, wos_diag* diag) {
-    if (!c || !n) return fail(WOS_INVALID_ARG, "null argument");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    ScreenSrc src;
-    src.kind = 1;
-    src.desc = *n;
-    return run_splitstep(c, ny, nx, dx, ncomp, field, 0, field, 0, z, src, steps, cc ? *cc : default_context(), diag);
-}
-
-int wos_splitstep_maps(wos_ctx c, wos_field* f, double z, const double* n_re, const double* n_im, int nmaps,
-                       int steps, const wos_context* cc, wos_diag* diag) {
-    if (!c || !n_re || !n_im) return fail(WOS_INVALID_ARG, "null argument");
-    TRY(check_field(f));
-    if (diag) {
-        std::memset(diag, 0, sizeof(*diag));
-        diag->dx_out = f->dx;
-    }
-    if (z == 0) return WOS_OK;
-    const int st = steps <= 0 ? 1 : steps;
-    if (nmaps != 1 && nmaps != st) return fail(WOS_INVALID_ARG, "nmaps must be 1 or steps");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const long long np = (long long)f->ny * f->nx;
-    TRY(ensure(c->maps, sizeof(double) * 2 * np * nmaps));
-    double* re = reinterpret_cast<double*>(c->maps.p);
-    double* im = re + np * nmaps;
-    CK(cudaMemcpyAsync(re, n_re, sizeof(double) * np * nmaps, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(im, n_im, sizeof(double) * np * nmaps, cudaMemcpyHostToDevice, c->st));
-    const int ncomp = f->polarized ? 2 : 1;
-    TRY(stage_in(c, f, ncomp));
-    ScreenSrc src;
-    src.kind = 2;
-    src.nre = re;
-    src.nim = im;
-    src.nmaps = nmaps;
-    TRY(run_splitstep(c, f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, c->stage.p, 1, z, src, st,
-                      cc ? *cc : default_context(), diag));
-    return stage_out(c, f, ncomp);
-}
-
-int wos_polychromatic(wos_ctx c, const wos_field* f, double z, const double* wavelengths, const double* weights,
-                      int nsamples, int method, const wos_context* base, double* out, wos_diag* diag) {
-    if (!c || !wavelengths || !weights || !out) return fail(WOS_INVALID_ARG, "null argument");
-    TRY(check_field(f));
-    if (nsamples <= 0) return fail(WOS_INVALID_ARG, "polychromatic: no wavelength samples");
-    for (int s = 0; s < nsamples; s++)
-        if (!(wavelengths[s] > 0)) return fail(WOS_INVALID_ARG, "polychromatic: wavelength must be > 0");
-    if (method < WOS_ASM || method > WOS_FRAUNHOFER) return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
-    if (diag) {
-        std::memset(diag, 0, sizeof(*diag));
-        diag->dx_out = f->dx;
-    }
-    // a nil base context means Context{Evanescent: "decay", Warnings: &Warnings{}}
-    wos_context cc = base ? *base : default_context();
-    if (!base) cc.diagnostics = 1;
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const int ncomp = f->polarized ? 2 : 1;
-    const long long np = (long long)f->ny * f->nx;
-    TRY(stage_in(c, const_cast<wos_field*>(f), ncomp));
-    TRY(ensure(c->accum, sizeof(double) * np));
-    double* acc = reinterpret_cast<double*>(c->accum.p);
-    CK(cudaMemsetAsync(acc, 0, sizeof(double) * np, c->st));
-    wos_diag* dp = (cc.diagnostics && diag) ? diag : nullptr;
-    if (z == 0) {
-        for (int s = 0; s < nsamples; s++) CK(launch_accum_int(1, acc, c->stage.p, ncomp, np, weights[s], c->st));
-    } else if (method == WOS_ASM) {
-        std::vector<double> wl(wavelengths, wavelengths + nsamples), w(weights, weights + nsamples);
-        double *wl_d, *w_d, *unused;
-        TRY(upload_params(c, wl, w, {}, &wl_d, &w_d, &unused));
-        Batch b{f->ny, f->nx, ncomp, f->dx, c->stage.p, 0, nsamples, wl_d, nullptr, wl,
-                std::vector<double>(nsamples, z), w_d, acc, nullptr, cc, dp};
-        TRY(run_batch_asm(c, b));
-    } else {
-        TRY(ensure(c->scratch3, (size_t)np * ncomp * c->csz()));
-        void* O = c->scratch3.p;
-        for (int s = 0; s < nsamples; s++) {
-            wos_context cs = cc;
-            cs.wavelength = wavelengths[s];
-            wos_diag ds;
-            Prop p{f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, O, 0, z, method, cs, dp ? &ds : nullptr};
-            TRY(run_propagate(c, p));
-            if (dp) diag_merge(dp, ds);
-            CK(launch_accum_int(c->fp64, acc, O, ncomp, np, weights[s], c->st));
-        }
-    }
-    CK(cudaMemcpyAsync(out, acc, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    return WOS_OK;
-}
-
-int wos_volume(wos_ctx c, const wos_field* f, const double* zs, int nz, int method, const wos_context* cci,
-               wos_c128* out, wos_diag* diag) {
-    if (!c || (nz > 0 && (!zs || !out)) || nz < 0) return fail(WOS_INVALID_ARG, "null argument");
-    TRY(check_field(f));
-    if (method < WOS_ASM || method > WOS_FRAUNHOFER) return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
-    if (diag) {
-        std::memset(diag, 0, sizeof(*diag));
-        diag->dx_out = f->dx;
-    }
-    if (nz == 0) return WOS_OK;
-    const wos_context cc = cci ? *cci : default_context();
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const int ncomp = f->polarized ? 2 : 1;
-    const long long np = (long long)f->ny * f->nx;
-    TRY(stage_in(c, const_cast<wos_field*>(f), ncomp));
-    TRY(ensure(c->vol, sizeof(double2) * (size_t)np * ncomp * nz));
-    double2* O = reinterpret_cast<double2*>(c->vol.p);
-    bool batched = method == WOS_ASM;
-    std::vector<double> zb;
-    std::vector<int> idx;
-    for (int q = 0; q < nz; q++) {
-        if (zs[q] != 0) {
-            zb.push_back(zs[q]);
-            idx.push_back(q);
-            if (zs[q] < 0) batched = false;
-        }
-    }
-    wos_diag* dp = diag;
-    if (batched && !zb.empty()) {
-        // the batch writes its planes compactly, then they move to their slots
-        TRY(ensure(c->scratch3, sizeof(double2) * (size_t)np * ncomp * zb.size()));
-        double2* Ob = reinterpret_cast<double2*>(c->scratch3.p);
-        double *z_d, *u1, *u2;
-        TRY(upload_params(c, zb, {}, {}, &z_d, &u1, &u2));
-        Batch b{f->ny, f->nx, ncomp, f->dx, c->stage.p, 0, (int)zb.size(), nullptr, z_d, {}, zb, nullptr, nullptr,
-                Ob, cc, (cc.diagnostics && dp) ? dp : nullptr};
-        TRY(run_batch_asm(c, b));
-        for (size_t u = 0; u < zb.size(); u++)
-            CK(cudaMemcpyAsync(O + (size_t)idx[u] * ncomp * np, Ob + u * ncomp * np, sizeof(double2) * ncomp * np,
-                               cudaMemcpyDeviceToDevice, c->st));
-    } else {
-        for (size_t u = 0; u < zb.size(); u++) {
-            wos_diag ds;
-            Prop p{f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, O + (size_t)idx[u] * ncomp * np, 1, zb[u], method, cc,
-                   (cc.diagnostics && dp) ? &ds : nullptr};
-            TRY(run_propagate(c, p));
-            if (cc.diagnostics && dp) diag_merge(dp, ds);
-        }
-    }
-    // z == 0 returns the input unchanged (optics/propagate.go:66-68)
-    for (int q = 0; q < nz; q++)
-        if (zs[q] == 0)
-            CK(cudaMemcpyAsync(O + (size_t)q * ncomp * np, c->stage.p, sizeof(double2) * ncomp * np,
-                               cudaMemcpyDeviceToDevice, c->st));
-    CK(cudaMemcpyAsync(out, O, sizeof(double2) * (size_t)np * ncomp * nz, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    return WOS_OK;
-}
-
-int wos_schell_modes(wos_ctx c, int n, double dx, double width, double coherence, int m, const wos_c128* noise,
-                     wos_c128* modes_out) {
-    if (!c || !noise || !modes_out || n < 2 || !(dx > 0)) return fail(WOS_INVALID_ARG, "null argument");
-    if (!(width > 0) || !(coherence > 0)) return fail(WOS_INVALID_ARG, "schell: width and coherence must be > 0");
-    if (m <= 0) m = 1;
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const long long nn = (long long)n * n;
-    TRY(ensure(c->vol, sizeof(double2) * (size_t)nn * m));
-    double2* modes = reinterpret_cast<double2*>(c->vol.p);
-    TRY(schell_generate(c, n, dx, width, coherence, m, noise, modes));
-    CK(cudaMemcpyAsync(modes_out, modes, sizeof(double2) * (size_t)nn * m, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    return WOS_OK;
-}
-
-int wos_partially_coherent(wos_ctx c, int n, double dx, double width, double coherence, int m,
-                           const wos_c128* noise, double z, int method, const wos_context* cci, double* out,
-                           wos_diag* diag) {
-    if (!c || !noise || !out || n < 2 || !(dx > 0)) return fail(WOS_INVALID_ARG, "null argument");
-    if (!(width > 0) || !(coherence > 0)) return fail(WOS_INVALID_ARG, "schell: width and coherence must be > 0");
-    if (method < WOS_ASM || method > WOS_FRAUNHOFER) return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
-    if (m <= 0) m = 1;
-    if (diag) {
-        std::memset(diag, 0, sizeof(*diag));
-        diag->dx_out = dx;
-    }
-    const wos_context cc = cci ? *cci : default_context();
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const long long nn = (long long)n * n;
-    TRY(ensure(c->vol, sizeof(double2) * (size_t)nn * m));
-    double2* modes = reinterpret_cast<double2*>(c->vol.p);
-    TRY(schell_generate(c, n, dx, width, coherence, m, noise, modes));
-    TRY(ensure(c->accum, sizeof(double) * nn));
-    double* acc = reinterpret_cast<double*>(c->accum.p);
-    CK(cudaMemsetAsync(acc, 0, sizeof(double) * nn, c->st));
-    const double inv = 1 / (double)m;
-    wos_diag* dp = (cc.diagnostics && diag) ? diag : nullptr;
-    if (z == 0) {
-        for (int q = 0; q < m; q++) CK(launch_accum_int(1, acc, modes + q * nn, 1, nn, inv, c->st));
-    } else if (method == WOS_ASM) {
-        std::vector<double> w(m, inv);
-        double *w_d, *u1, *u2;
-        TRY(upload_params(c, w, {}, {}, &w_d, &u1, &u2));
-        Batch b{n, n, 1, dx, modes, nn, m, nullptr, nullptr, {}, std::vector<double>(m, z), w_d, acc, nullptr, cc, dp};
-        TRY(run_batch_asm(c, b));
-    } else {
-        TRY(ensure(c->scratch3, (size_t)nn * c->csz()));
-        void* O = c->scratch3.p;
-        for (int q = 0; q < m; q++) {
-            wos_diag ds;
-            Prop p{n, n, dx, 1, modes + q * nn, 1, O, 0, z, method, cc, dp ? &ds : nullptr};
-            TRY(run_propagate(c, p));
-            if (dp) diag_merge(dp, ds);
-            CK(launch_accum_int(c->fp64, acc, O, 1, nn, inv, c->st));
-        }
-    }
-    CK(cudaMemcpyAsync(out, acc, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    return WOS_OK;
-}
-
-int wos_apply_lens(wos_ctx c, wos_field* f, double wavelength, double focal, double aperture, double x0, double y0) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    if (focal == 0) return fail(WOS_INVALID_ARG, "lens: focal length f must be non-zero");
-    if (!(wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(element_begin(c, f));
-    const double k = 2 * M_PI / wavelength;
-    const double cc = -k / (2 * focal);
-    CK(launch_lens(stage_ex(c), stage_ey(c, f), f->polarized, f->ny, f->nx, f->dx, cc, aperture, x0, y0, c->st));
-    return stage_out(c, f, f->polarized ? 2 : 1);
-}
-
-int wos_apply_aperture_circle(wos_ctx c, wos_field* f, double radius, double x0, double y0, double edge_sigma) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(element_begin(c, f));
-    CK(launch_aperture_circle(stage_ex(c), stage_ey(c, f), f->polarized, f->ny, f->nx, f->dx, radius, x0, y0,
-                              edge_sigma, c->st));
-    return stage_out(c, f, f->polarized ? 2 : 1);
-}
-
-int wos_apply_grating(wos_ctx c, wos_field* f, int kind, double period, double modulation, double duty,
-                      double blaze_depth, double rotation, double offset) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    if (!(period > 0)) return fail(WOS_INVALID_ARG, "grating: period must be > 0");
-    if (duty < 0 || duty > 1) return fail(WOS_INVALID_ARG, "grating: duty must be in [0,1]");
-    if (kind < 0 || kind > 4) return fail(WOS_INVALID_ARG, "grating: unknown kind");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(element_begin(c, f));
-    CK(launch_grating(stage_ex(c), stage_ey(c, f), f->polarized, f->ny, f->nx, f->dx, kind, period, modulation, duty,
-                      blaze_depth, rotation, offset, c->st));
-    return stage_out(c, f, f->polarized ? 2 : 1);
-}
-
-int wos_apply_phase_mask(wos_ctx c, wos_field* f, const double* phi, double amp) {
-    if (!c || !phi) return fail(WOS_INVALID_ARG, "null argument");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(element_begin(c, f));
-    const long long np = (long long)f->ny * f->nx;
-    TRY(ensure(c->maps, sizeof(double) * np));
-    CK(cudaMemcpyAsync(c->maps.p, phi, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
-    CK(launch_phase_mask(stage_ex(c), stage_ey(c, f), f->polarized, np, reinterpret_cast<double*>(c->maps.p), amp,
-                         c->st));
-    return stage_out(c, f, f->polarized ? 2 : 1);
-}
-
-namespace {
-double2 d2(wos_c128 v) { return make_double2(v.re, v.im); }
-
-// FFT -> multiply by a filter H(fx, fy) -> inverse FFT of `ncomp` complex128
-// device planes in place, on the three-sweep propagator (context precision).
-int spectral_filter(wos_ctx c, int ny, int nx, double dx, int ncomp, void* planes, int kind, double p0,
-                    double p1, double k = 0, double z = 0) {
-    Prop p{ny, nx, dx, ncomp, planes, 1, planes, 1, 0.0, 0, default_context(), nullptr};
-    Sweep3 s;
-    s.h.kind = kind;
-    s.h.exact = c->fp64;
-    s.h.dx = dx;
-    s.h.lfx = nx;
-    s.h.lfy = ny;
-    s.h.scale = 1.0 / ((double)nx * (double)ny);
-    s.h.c_re = 1.0;
-    s.h.p0 = p0;
-    s.h.p1 = p1;
-    s.h.k = k;
-    s.h.z = z;
-    return run_sweep3(c, p, s);
-}
-}  // namespace
-
-int wos_apply_jones(wos_ctx c, wos_field* f, wos_c128 a, wos_c128 b, wos_c128 cc, wos_c128 d) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    std::lock_guard<std::mutex> lk(c->mu);
-    int mode = 2;
-    if (f && !f->polarized) {
-        const bool diag = b.re == 0 && b.im == 0 && cc.re == 0 && cc.im == 0 && d.re == a.re && d.im == a.im;
-        mode = diag ? 0 : 1;
-        if (mode == 1 && !f->ey) return fail(WOS_INVALID_ARG, "jones: the field needs an Ey buffer");
-    }
-    TRY(check_field(f));
-    TRY(set_device(c));
-    TRY(stage_in(c, f, mode == 0 ? 1 : 2));
-    const long long np = (long long)f->ny * f->nx;
-    CK(launch_jones(stage_ex(c), stage_ey(c, f), np, mode, d2(a), d2(b), d2(cc), d2(d), c->st));
-    if (mode == 1) f->polarized = 1;
-    return stage_out(c, f, mode == 0 ? 1 : 2);
-}
-
-int wos_scale_amplitude(wos_ctx c, wos_field* f, wos_c128 s) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(element_begin(c, f));
-    CK(launch_scale(stage_ex(c), stage_ey(c, f), f->polarized, (long long)f->ny * f->nx, d2(s), c->st));
-    return stage_out(c, f, f->polarized ? 2 : 1);
-}
-
-int wos_apply_tilt(wos_ctx c, wos_field* f, double tx, double ty, double wavelength) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    if (!(wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(element_begin(c, f));
-    const double k = 2 * M_PI / wavelength;
-    CK(launch_tilt(stage_ex(c), stage_ey(c, f), f->polarized, f->ny, f->nx, f->dx, k, std::sin(tx), std::sin(ty),
-                   c->st));
-    return stage_out(c, f, f->polarized ? 2 : 1);
-}
-
-int wos_apply_bandlimit(wos_ctx c, wos_field* f, double fraction, double sigma) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(check_field(f));
-    if (fraction >= 1 || fraction <= 0) return WOS_OK;  // nil or disabled options (field.go:266-268)
-    TRY(element_begin(c, f));
-    const double fnyq = 1 / (2 * f->dx);
-    const double f0 = fraction * fnyq;
-    double sig = sigma * fnyq;
-    if (sig <= 0) sig = fnyq * 0.01;
-    TRY(spectral_filter(c, f->ny, f->nx, f->dx, f->polarized ? 2 : 1, c->stage.p, H_BANDLIMIT, f0, sig));
-    return stage_out(c, f, f->polarized ? 2 : 1);
-}
-
-int wos_shift_field(wos_ctx c, wos_field* f, double du, double dv) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(check_field(f));
-    if (du == 0 && dv == 0) return WOS_OK;
-    TRY(element_begin(c, f));
-    TRY(spectral_filter(c, f->ny, f->nx, f->dx, f->polarized ? 2 : 1, c->stage.p, H_SHIFT, du, dv));
-    return stage_out(c, f, f->polarized ? 2 : 1);
-}
-
-int wos_propagate_anisotropic(wos_ctx c, wos_field* f, double z, const wos_c128* eps, const wos_context* cci) {
-    if (!c || !f || !f->ex || !f->ey || !eps || f->ny < 2 || f->nx < 2 || !(f->dx > 0))
-        return fail(WOS_INVALID_ARG, "anisotropic: ex, ey, eps and a valid geometry are required");
-    const wos_context cc = cci ? *cci : default_context();
-    if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const int ny = f->ny, nx = f->nx;
-    const long long np = (long long)ny * nx;
-    TRY(ensure(c->stage, (size_t)np * 16 * 2));
-    double2* st = reinterpret_cast<double2*>(c->stage.p);
-    CK(cudaMemcpyAsync(st, f->ex, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(st + np, f->ey, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
-    void* work = st;
-    if (!c->fp64) {
-        TRY(ensure(c->scratch, (size_t)np * 8 * 2));
-        work = c->scratch.p;
-        CK(launch_convert(0, st, work, 2 * np, c->st));
-    }
-    Eps9 e;
-    for (int k = 0; k < 9; k++) e.v[k] = make_double2(eps[k].re, eps[k].im);
-    TRY(fft2d_impl(c, c->fp64, ny, nx, 2, work, 0));
-    CK(launch_aniso(c->fp64, work, ny, nx, f->dx, 2 * M_PI / cc.wavelength, z, e, c->st));
-    TRY(fft2d_impl(c, c->fp64, ny, nx, 2, work, 1));
-    if (!c->fp64) CK(launch_convert(1, work, st, 2 * np, c->st));
-    CK(cudaMemcpyAsync(f->ex, st, (size_t)np * 16, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaMemcpyAsync(f->ey, st + np, (size_t)np * 16, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    return WOS_OK;
-}
-
-int wos_propagate_uniaxial(wos_ctx c, wos_field* f, double z, double no, double ne, const wos_context* cci) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    if (!(no > 0) || !(ne > 0)) return fail(WOS_INVALID_ARG, "uniaxial: n_o and n_e must be > 0");
-    const wos_context cc = cci ? *cci : default_context();
-    if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(element_begin(c, f));
-    const double k0 = 2 * M_PI / cc.wavelength;
-    TRY(spectral_filter(c, f->ny, f->nx, f->dx, 1, stage_ex(c), H_UNIAX_E, no, ne, k0, z));
-    if (f->polarized) TRY(spectral_filter(c, f->ny, f->nx, f->dx, 1, stage_ey(c, f), H_UNIAX_O, no, ne, k0, z));
-    return stage_out(c, f, f->polarized ? 2 : 1);
-}
-
-int wos_apply_diffuser(wos_ctx c, wos_field* f, double sigma, double correlation, double amplitude,
-                       long long seed, double x0, double y0) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(element_begin(c, f));
-    const long long np = (long long)f->ny * f->nx;
-    TRY(ensure(c->aux, (size_t)np * sizeof(double2)));
-    double2* zp = reinterpret_cast<double2*>(c->aux.p);
-    const double cell = f->dx > 0 ? f->dx : 1.0;
-    CK(launch_diffuser_noise(zp, f->ny, f->nx, f->dx, cell, x0, y0, seed, c->st));
-    if (correlation > 0) {
-        const double neg_two_pi_sq = -19.739208802178716;  // -2 pi^2 rounded once, as a Go constant
-        TRY(spectral_filter(c, f->ny, f->nx, f->dx, 1, zp, H_GAUSS, neg_two_pi_sq * correlation * correlation, 0));
-    }
-    const int nb = sum_re2_blocks(np);
-    TRY(red_prepare(c, (size_t)nb));
-    CK(launch_sum_re2(zp, np, red_region(c, 0), c->st));
-    CK(launch_reduce_finish(red_region(c, 0), nb, 1, 0, 2, redout_region(c, 0), c->st));
-    CK(launch_diffuser_apply(stage_ex(c), stage_ey(c, f), f->polarized, np, zp, redout_region(c, 0), sigma,
-                             amplitude, c->st));
-    return stage_out(c, f, f->polarized ? 2 : 1);
-}
-
-int wos_propagate1d(wos_ctx c, int n, wos_c128* a, double dx, double z, double wavelength, const wos_context* cci,
-                    wos_diag* d) {
-    if (!c || !a) return fail(WOS_INVALID_ARG, "null argument");
-    if (n < 2 || !(dx > 0)) return fail(WOS_INVALID_ARG, "propagate1d: n >= 2 and dx > 0 required");
-    if (!(wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    if (d) {
-        std::memset(d, 0, sizeof(*d));
-        d->dx_out = dx;
-    }
-    wos_context cc = cci ? *cci : default_context();
-    cc.wavelength = wavelength;  // Propagate1D takes wl apart from the Context
-    const Policy pol = ev_policy(cc, z);
-    Axis* ax;
-    TRY(get_axis(c, n, c->fp64, &ax));
-    TRY(ensure(c->stage, (size_t)n * 16));
-    TRY(ensure(c->scratch, (size_t)n * c->csz()));
-    CK(cudaMemcpyAsync(c->stage.p, a, (size_t)n * 16, cudaMemcpyHostToDevice, c->st));
-    TRY(red_prepare(c, 64));
-    RowArgs r = row_defaults(1, n, dx);
-    r.mode = ROW_FWD;
-    r.rows = 1;
-    fill_axis(r, ax);
-    r.in = c->stage.p;
-    r.in_c128 = 1;
-    r.in_ld = n;
-    r.in_n = n;
-    r.out = c->scratch.p;
-    r.out_ld = n;
-    r.out_n = n;
-    r.red = red_region(c, 0);
-    r.red_pre = 1;
-    CK(prof_rows(c, c->fp64, r));
-    CK(launch_reduce_finish(r.red, 1, 1, RS_P, 1, redout_region(c, 0), c->st));
-    HArgs h = asm_h(c, cc, z, pol, dx, n, 1);
-    h.scale = 1.0 / (double)n;
-    int nb = 0;
-    CK(launch_asm1d_h(c->fp64, c->scratch.p, n, h, red_region(c, 1), &nb, c->st));
-    CK(launch_reduce_finish(red_region(c, 1), nb, 1, RS_SW, 2, redout_region(c, 1), c->st));
-    RowArgs q = r;
-    q.mode = ROW_INV;
-    q.in = c->scratch.p;
-    q.in_c128 = 0;
-    q.out = c->stage.p;
-    q.out_c128 = 1;
-    q.red = nullptr;
-    q.red_pre = 0;
-    CK(prof_rows(c, c->fp64, q));
-    CK(cudaMemcpyAsync(a, c->stage.p, (size_t)n * 16, cudaMemcpyDeviceToHost, c->st));
-    TRY(fetch_red(c, 2));
-    // sum1DSq before and after (no dx factor); the loss fraction comes from
-    // the spectral sums, free of the cancellation of pIn - pOut
-    const double pin = c->hred[RS_P];
-    const double p0 = c->hred[RS_COUNT + RS_SW], l1 = c->hred[RS_COUNT + RS_SW + 1];
-    const double pout = pin - pin * (p0 > 0 ? l1 / p0 : 0.0);
-    if (d) {
-        d->p_in = pin;
-        d->p_out = pout;
-        if (pin > 0 && pout < pin * (1 - 1e-8) && z > 0)
-            warn_add(d, WOS_W_EVANESCENT_FILTERED, (pin - pout) / pin);
-    }
-    return WOS_OK;
-}
-
-int wos_splitstep_adjoint(wos_ctx c, wos_field* f, double z, const wos_index_desc* n, int steps,
-                          const wos_context* cc) {
-    if (!c || !n || !cc) return fail(WOS_INVALID_ARG, "null argument");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(element_begin(c, f));
-    ScreenSrc src;
-    src.kind = 1;
-    src.desc = *n;
-    const int ncomp = f->polarized ? 2 : 1;
-    TRY(run_splitstep(c, f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, c->stage.p, 1, z, src, steps, *cc, nullptr,
-                      true));
-    return stage_out(c, f, ncomp);
-}
-
-int wos_splitstep_adjoint_dev(wos_ctx c, int ny, int nx, double dx, int ncomp, void* field, double z,
-                              const wos_index_desc* n, int steps, const wos_context* cc) {
-    if (!c || !n || !cc) return fail(WOS_INVALID_ARG, "null argument");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    ScreenSrc src;
-    src.kind = 1;
-    src.desc = *n;
-    return run_splitstep(c, ny, nx, dx, ncomp, field, 0, field, 0, z, src, steps, *cc, nullptr, true);
-}
-
-int wos_bpm_stack_loss_grad_dev(wos_ctx c, int ny, int nx, double dx, int nlayers, const void* a, const double* phis,
-                                const double* target, double zseg, const wos_index_desc* n, int steps,
-                                const wos_context* cc, double* loss, double* grads) {
-    if (!c || !n || !cc) return fail(WOS_INVALID_ARG, "null argument");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    return bpm_stack_impl(c, ny, nx, dx, nlayers, a, 0, phis, target, zseg, steps, *n, *cc, loss, grads);
-}
-
-int wos_bpm_stack_loss_grad(wos_ctx c, int ny, int nx, double dx, int nlayers, const wos_c128* a, const double* phis,
-                            const double* target, double zseg, const wos_index_desc* n, int steps,
-                            const wos_context* cc, double* loss, double* grads) {
-    if (!c || !n || !cc || !a || !phis || !target || nlayers < 1 || ny < 2 || nx < 2)
-        return fail(WOS_INVALID_ARG, "bpm stack arguments");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const long long np = (long long)ny * nx;
-    TRY(ensure(c->stage, (size_t)np * 16));
-    TRY(ensure(c->maps, sizeof(double) * (size_t)np * (2 * (size_t)nlayers + 1)));
-    double* phid = reinterpret_cast<double*>(c->maps.p);
-    double* Td = phid + (size_t)np * nlayers;
-    double* gd = Td + np;
-    CK(cudaMemcpyAsync(c->stage.p, a, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(phid, phis, sizeof(double) * (size_t)np * nlayers, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(Td, target, sizeof(double) * (size_t)np, cudaMemcpyHostToDevice, c->st));
-    TRY(bpm_stack_impl(c, ny, nx, dx, nlayers, c->stage.p, 1, phid, Td, zseg, steps, *n, *cc, loss,
-                       grads ? gd : nullptr));
-    if (grads) {
-        CK(cudaMemcpyAsync(grads, gd, sizeof(double) * (size_t)np * nlayers, cudaMemcpyDeviceToHost, c->st));
-        CK(cudaStreamSynchronize(c->st));
-    }
-    return WOS_OK;
-}
-
-int wos_propagate_vectorial(wos_ctx c, wos_field* f, wos_c128* ez, double z, const wos_context* cci) {
-    if (!c || !f || !f->ex || !f->ey || !ez || f->ny < 2 || f->nx < 2 || !(f->dx > 0))
-        return fail(WOS_INVALID_ARG, "vectorial: ex, ey and ez buffers and a valid geometry are required");
-    if (z == 0) return WOS_OK;  // Propagate returns before the vectorial step (propagate.go:66-68)
-    const wos_context cc = cci ? *cci : default_context();
-    if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const int ny = f->ny, nx = f->nx;
-    const long long np = (long long)ny * nx;
-    TRY(ensure(c->stage, (size_t)np * 16 * 3));
-    double2* st = reinterpret_cast<double2*>(c->stage.p);
-    CK(cudaMemcpyAsync(st, f->ex, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemcpyAsync(st + np, f->ey, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
-    void* work = st;
-    if (!c->fp64) {
-        TRY(ensure(c->scratch, (size_t)np * 8 * 3));
-        work = c->scratch.p;
-        CK(launch_convert(0, st, work, 2 * np, c->st));
-    }
-    const Policy pol = ev_policy(cc, z);
-    HArgs h = asm_h(c, cc, z, pol, f->dx, nx, ny);
-    TRY(fft2d_impl(c, c->fp64, ny, nx, 2, work, 0));
-    CK(launch_vectorial(c->fp64, work, ny, nx, f->dx, h, c->st));
-    TRY(fft2d_impl(c, c->fp64, ny, nx, 3, work, 1));
-    if (!c->fp64) CK(launch_convert(1, work, st, 3 * np, c->st));
-    CK(cudaMemcpyAsync(f->ex, st, (size_t)np * 16, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaMemcpyAsync(f->ey, st + np, (size_t)np * 16, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaMemcpyAsync(ez, st + 2 * np, (size_t)np * 16, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    return WOS_OK;
-}
-
-int wos_plane_view(wos_ctx c, const wos_field* f, const wos_c128* ez, int view, double mask_cut, float* out) {
-    if (!c || !f || !f->ex || !out || f->ny < 1 || f->nx < 1) return fail(WOS_INVALID_ARG, "plane view arguments");
-    if (view < WOS_VIEW_TOTAL || view > WOS_VIEW_PHASE_Z) return fail(WOS_INVALID_ARG, "unknown plane view");
-    const bool need_ey = view == WOS_VIEW_EY || view == WOS_VIEW_PHASE_Y || (view <= WOS_VIEW_AMPLITUDE && f->polarized);
-    const bool need_ez = view == WOS_VIEW_EZ || view == WOS_VIEW_PHASE_Z;
-    if ((need_ey && !f->ey) || (need_ez && !ez)) return fail(WOS_INVALID_ARG, "plane view: component missing");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const long long np = (long long)f->ny * f->nx;
-    const bool use_ez = ez && (need_ez || view <= WOS_VIEW_AMPLITUDE);
-    TRY(ensure(c->stage, (size_t)np * 16 * 3));
-    double2* st = reinterpret_cast<double2*>(c->stage.p);
-    CK(cudaMemcpyAsync(st, f->ex, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
-    if (need_ey) CK(cudaMemcpyAsync(st + np, f->ey, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
-    if (use_ez) CK(cudaMemcpyAsync(st + 2 * np, ez, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
-    TRY(ensure(c->accum, sizeof(float) * np));
-    TRY(plane_view_dev(c, 1, st, need_ey ? st + np : nullptr, use_ez ? st + 2 * np : nullptr, f->polarized ? 1 : 0,
-                       np, view, mask_cut, c->accum.p));
-    CK(cudaMemcpyAsync(out, c->accum.p, sizeof(float) * np, cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    return WOS_OK;
-}
-
-int wos_plane_view_dev(wos_ctx c, int ny, int nx, int ncomp, const void* planes, const void* ez, int view,
-                       double mask_cut, void* out) {
-    if (!c || !planes || !out || ny < 1 || nx < 1 || ncomp < 1 || ncomp > 2)
-        return fail(WOS_INVALID_ARG, "plane view arguments");
-    if (view < WOS_VIEW_TOTAL || view > WOS_VIEW_PHASE_Z) return fail(WOS_INVALID_ARG, "unknown plane view");
-    if ((view == WOS_VIEW_EY || view == WOS_VIEW_PHASE_Y) && ncomp < 2)
-        return fail(WOS_INVALID_ARG, "plane view: component missing");
-    if ((view == WOS_VIEW_EZ || view == WOS_VIEW_PHASE_Z) && !ez) return fail(WOS_INVALID_ARG, "plane view: no Ez");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const long long np = (long long)ny * nx;
-    const char* p = reinterpret_cast<const char*>(planes);
-    return plane_view_dev(c, c->fp64, p, ncomp == 2 ? p + (size_t)np * c->csz() : nullptr, ez, ncomp == 2 ? 1 : 0, np,
-                          view, mask_cut, out);
-}
-
-int wos_train(wos_ctx c, wos_field* f, const wos_op* ops, int nops, const wos_context* cci, double bl_fraction,
-              double bl_sigma, wos_diag* diag) {
-    if (!c || (nops > 0 && !ops) || nops < 0) return fail(WOS_INVALID_ARG, "train arguments");
-    TRY(check_field(f));
-    bool need_ey = f->polarized != 0;
-    for (int i = 0; i < nops; i++) {
-        const wos_op& o = ops[i];
-        if (o.kind < WOS_OP_PROPAGATE || o.kind > WOS_OP_VIEW) return fail(WOS_INVALID_ARG, "train: unknown op");
-        if (o.kind == WOS_OP_VIEW && (o.method < WOS_VIEW_TOTAL || o.method > WOS_VIEW_PHASE_Y || !o.out))
-            return fail(WOS_INVALID_ARG, "train: view kind / output");
-        if (o.kind == WOS_OP_VIEW && (o.method == WOS_VIEW_EY || o.method == WOS_VIEW_PHASE_Y)) need_ey = true;
-        if (o.kind == WOS_OP_JONES) need_ey = true;
-        if (o.kind == WOS_OP_PROPAGATE && (o.method < WOS_ASM || o.method > WOS_FRAUNHOFER))
-            return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
-        if ((o.kind == WOS_OP_PHASE_MASK && !o.map) || (o.kind == WOS_OP_INTENSITY && !o.out))
-            return fail(WOS_INVALID_ARG, "train: null map / output");
-        if (o.kind == WOS_OP_GRATING && (o.method < 0 || o.method > 4 || !(o.a[0] > 0) || o.a[2] < 0 || o.a[2] > 1))
-            return fail(WOS_INVALID_ARG, "train: grating parameters");
-        if (o.kind == WOS_OP_LENS && (o.a[1] == 0 || !(o.a[0] > 0))) return fail(WOS_INVALID_ARG, "train: lens parameters");
-        if (o.kind == WOS_OP_TILT && !(o.a[2] > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
-    }
-    if (need_ey && !f->ey) return fail(WOS_INVALID_ARG, "train: a Jones op or an Ey view needs an Ey buffer");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const wos_context cc = cci ? *cci : default_context();
-    if (diag) {
-        std::memset(diag, 0, sizeof(*diag));
-        diag->dx_out = f->dx;
-    }
-    const long long np = (long long)f->ny * f->nx;
-    int pol = f->polarized ? 1 : 0;
-    TRY(ensure(c->stage, (size_t)np * 16 * (need_ey ? 2 : 1)));
-    CK(cudaMemcpyAsync(c->stage.p, f->ex, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
-    // Ey as the reference holds it (zeros for a fresh scalar field) whenever an op can read it
-    if (need_ey) CK(cudaMemcpyAsync(stage_ey(c, f), f->ey, (size_t)np * 16, cudaMemcpyHostToDevice, c->st));
-    double2* ex = stage_ex(c);
-    double2* ey = stage_ey(c, f);
-    double dx = f->dx;
-    bool first_prop = true;
-    for (int i = 0; i < nops; i++) {
-        const wos_op& o = ops[i];
-        const double* a = o.a;
-        switch (o.kind) {
-        case WOS_OP_PROPAGATE: {
-            if (a[0] == 0) break;  // Propagate with z == 0 returns at once (propagate.go:66-68)
-            wos_diag d{};
-            Prop p{f->ny, f->nx, dx, pol ? 2 : 1, c->stage.p, 1, c->stage.p, 1, a[0], o.method, cc, &d};
-            if (!diag) p.diag = (o.method == WOS_FRAUNHOFER) ? &d : nullptr;
-            TRY(run_propagate(c, p));
-            if (o.method == WOS_FRAUNHOFER) dx = d.dx_out;
-            if (diag) {
-                diag_merge(diag, d);
-                if (first_prop) diag->p_in = d.p_in;
-                diag->p_out = d.p_out;
-                first_prop = false;
-            }
-            if (bl_fraction > 0 && bl_fraction < 1) {
-                const double fnyq = 1 / (2 * dx);
-                double sig = bl_sigma * fnyq;
-                if (sig <= 0) sig = fnyq * 0.01;
-                TRY(spectral_filter(c, f->ny, f->nx, dx, pol ? 2 : 1, c->stage.p, H_BANDLIMIT, bl_fraction * fnyq,
-                                    sig));
-            }
-        } break;
-        case WOS_OP_LENS: {
-            const double k = 2 * M_PI / a[0];
-            CK(launch_lens(ex, ey, pol, f->ny, f->nx, dx, -k / (2 * a[1]), a[2], a[3], a[4], c->st));
-        } break;
-        case WOS_OP_APERTURE:
-            CK(launch_aperture_circle(ex, ey, pol, f->ny, f->nx, dx, a[0], a[1], a[2], a[3], c->st));
-            break;
-        case WOS_OP_GRATING:
-            CK(launch_grating(ex, ey, pol, f->ny, f->nx, dx, o.method, a[0], a[1], a[2], a[3], a[4], a[5], c->st));
-            break;
-        case WOS_OP_PHASE_MASK: {
-            TRY(ensure(c->maps, sizeof(double) * np));
-            CK(cudaMemcpyAsync(c->maps.p, o.map, sizeof(double) * np, cudaMemcpyHostToDevice, c->st));
-            CK(launch_phase_mask(ex, ey, pol, np, reinterpret_cast<double*>(c->maps.p), a[0], c->st));
-        } break;
-        case WOS_OP_DIFFUSER: {
-            TRY(ensure(c->aux, (size_t)np * sizeof(double2)));
-            double2* zp = reinterpret_cast<double2*>(c->aux.p);
-            CK(launch_diffuser_noise(zp, f->ny, f->nx, dx, dx > 0 ? dx : 1.0, a[4], a[5], (long long)a[3], c->st));
-            if (a[1] > 0) {
-                const double neg_two_pi_sq = -19.739208802178716;
-                TRY(spectral_filter(c, f->ny, f->nx, dx, 1, zp, H_GAUSS, neg_two_pi_sq * a[1] * a[1], 0));
-            }
-            const int nb = sum_re2_blocks(np);
-            TRY(red_prepare(c, (size_t)nb));
-            CK(launch_sum_re2(zp, np, red_region(c, 0), c->st));
-            CK(launch_reduce_finish(red_region(c, 0), nb, 1, 0, 2, redout_region(c, 0), c->st));
-            CK(launch_diffuser_apply(ex, ey, pol, np, zp, redout_region(c, 0), a[0], a[2], c->st));
-        } break;
-        case WOS_OP_JONES: {
-            int mode = 2;
-            if (!pol) {
-                const bool dg = o.m[1].re == 0 && o.m[1].im == 0 && o.m[2].re == 0 && o.m[2].im == 0 &&
-                                o.m[3].re == o.m[0].re && o.m[3].im == o.m[0].im;
-                mode = dg ? 0 : 1;
-            }
-            CK(launch_jones(ex, ey, np, mode, d2(o.m[0]), d2(o.m[1]), d2(o.m[2]), d2(o.m[3]), c->st));
-            if (mode == 1) pol = 1;
-        } break;
-        case WOS_OP_SCALE:
-            CK(launch_scale(ex, ey, pol, np, d2(o.m[0]), c->st));
-            break;
-        case WOS_OP_TILT:
-            CK(launch_tilt(ex, ey, pol, f->ny, f->nx, dx, 2 * M_PI / a[2], std::sin(a[0]), std::sin(a[1]), c->st));
-            break;
-        case WOS_OP_SHIFT:
-            if (a[0] != 0 || a[1] != 0)
-                TRY(spectral_filter(c, f->ny, f->nx, dx, pol ? 2 : 1, c->stage.p, H_SHIFT, a[0], a[1]));
-            break;
-        case WOS_OP_BANDLIMIT:
-            if (a[0] > 0 && a[0] < 1) {
-                const double fnyq = 1 / (2 * dx);
-                double sig = a[1] * fnyq;
-                if (sig <= 0) sig = fnyq * 0.01;
-                TRY(spectral_filter(c, f->ny, f->nx, dx, pol ? 2 : 1, c->stage.p, H_BANDLIMIT, a[0] * fnyq, sig));
-            }
-            break;
-        case WOS_OP_INTENSITY: {
-            TRY(ensure(c->accum, sizeof(double) * np));
-            double* acc = reinterpret_cast<double*>(c->accum.p);
-            CK(cudaMemsetAsync(acc, 0, sizeof(double) * np, c->st));
-            CK(launch_accum_int(1, acc, c->stage.p, pol ? 2 : 1, np, 1.0, c->st));
-            CK(cudaMemcpyAsync(o.out, acc, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
-        } break;
-        case WOS_OP_VIEW: {
-            TRY(ensure(c->accum, sizeof(double) * np));
-            TRY(plane_view_dev(c, 1, ex, ey, nullptr, pol, np, o.method, a[0], c->accum.p));
-            CK(cudaMemcpyAsync(o.out, c->accum.p, sizeof(float) * np, cudaMemcpyDeviceToHost, c->st));
-        } break;
-        }
-    }
-    f->polarized = pol;
-    f->dx = dx;
-    if (diag) diag->dx_out = dx;
-    return stage_out(c, f, pol ? 2 : 1);
-}
-
-int wos_asm_forward_loss(wos_ctx c, int ny, int nx, double dx, double z, const wos_context* cc, const wos_c128* a,
-                         const double* phi, const double* target, double* loss) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    std::lock_guard<std::mutex> lk(c->mu);
-    return asm_loss_grad_impl(c, ny, nx, dx, z, cc, a, phi, target, loss, nullptr);
-}
-
-int wos_asm_loss_grad(wos_ctx c, int ny, int nx, double dx, double z, const wos_context* cc, const wos_c128* a,
-                      const double* phi, const double* target, double* loss, double* grad) {
-    if (!c || !grad) return fail(WOS_INVALID_ARG, "null argument");
-    std::lock_guard<std::mutex> lk(c->mu);
-    return asm_loss_grad_impl(c, ny, nx, dx, z, cc, a, phi, target, loss, grad);
-}
-
-int wos_asm_loss_grad_dev(wos_ctx c, int ny, int nx, double dx, double z, const wos_context* cc, const void* a,
-                          const double* phi, const double* target, double* loss, double* grad) {
-    if (!c || !cc || !a || !phi || !target || !loss || ny < 2 || nx < 2 || !(dx > 0))
-        return fail(WOS_INVALID_ARG, "inverse-design arguments");
-    if (!(cc->wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const int rc = asm_design_fast(c, ny, nx, dx, z, *cc, a, 0, phi, target, loss, grad);
-    if (rc == -1)
-        return fail(WOS_UNSUPPORTED_SIZE, "device-resident inverse design needs power-of-two ny, nx (256..8192)");
-    return rc;
-}
-
 struct wos_graph_s {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -3722,23 +1788,6 @@ int wos_autotune(wos_ctx c, int ny, int nx, int* row_e, int* col_e, int* col_w) 
     const bool tiled = c->tiled && !c->fp64 && nx % kTileW == 0 && fast_col_width(c->fp64, ny, bt.colE, kTileW) == kTileW;
     if (col_w) *col_w = tiled ? kTileW : bt.colW;
     return WOS_OK;
-}
-
-int wos_asm_adjoint(wos_ctx c, wos_field* f, double z, const wos_context* cci) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    TRY(check_field(f));
-    const wos_context cc = cci ? *cci : default_context();
-    if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const int ncomp = f->polarized ? 2 : 1;
-    TRY(stage_in(c, f, ncomp));
-    Prop p{f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, c->stage.p, 1, z, WOS_ASM, cc, nullptr};
-    Sweep3 s;
-    s.h = asm_h(c, cc, z, ev_policy(cc, z), f->dx, f->nx, f->ny);
-    s.h.conj = 1;
-    TRY(run_sweep3(c, p, s));
-    return stage_out(c, f, ncomp);
 }
 
 }  // extern "C"

@@ -1,0 +1,551 @@
+// wos_batch.cu -- batches of units sharing a geometry: PropagatePolychromatic
+// (optics/polychromatic.go:18-44), Propagate3D (optics/volume.go:8-18) and
+// the Gaussian-Schell source (optics/coherence.go:22-116), on one row
+// spectrum and per-chunk column launches.
+#include "wos_api_internal.cuh"
+
+namespace wapi {
+
+// FFT2D of a complex128 device array in FP64, whatever the context precision
+// (one-time source synthesis).
+int fft2d_fp64(wos_ctx c, int n, int batch, double2* a, int inverse) {
+    return fft2d_impl(c, 1, n, n, batch, a, inverse);
+}
+
+// GenerateSchellRealizations (optics/coherence.go:22-80) into modes (device, complex128)
+int schell_generate(wos_ctx c, int n, double dx, double width, double coh, int m, const wos_c128* noise,
+                    double2* modes) {
+    const long long nn = (long long)n * n;
+    TRY(ensure(c->aux, (size_t)nn * (16 + 8)));
+    double2* mu = reinterpret_cast<double2*>(c->aux.p);
+    double* sqs = reinterpret_cast<double*>(mu + nn);
+    CK(launch_schell_mu(mu, n, dx, coh, c->st));
+    TRY(fft2d_fp64(c, n, 1, mu, 0));
+    CK(launch_sqrt_re(sqs, mu, nn, c->st));
+    CK(cudaMemcpyAsync(modes, noise, (size_t)nn * m * 16, cudaMemcpyHostToDevice, c->st));
+    CK(launch_mul_map(modes, sqs, nn, m, c->st));
+    TRY(fft2d_fp64(c, n, m, modes, 1));
+    CK(launch_schell_env(modes, n, dx, width, m, c->st));
+    return WOS_OK;
+}
+
+// Batched ASM over units that share a geometry (polychromatic wavelengths,
+// volume distances, coherent modes): one row sweep per unit set, one column
+// launch per chunk with gridDim.y = units, then either a batched inverse row
+// sweep (planes out) or an accumulating one (intensity out).
+struct Batch {
+    int ny, nx, ncomp;
+    double dx;
+    const void* in;       // complex128 device input [ncomp or units][ny][nx]
+    long long in_unit_stride;  // elements between units of the input (0: shared input)
+    int units;
+    const double* wl_dev;  // per-unit wavelength (device) or null
+    const double* z_dev;   // per-unit z (device) or null
+    std::vector<double> wl, z;  // host copies
+    const double* w_dev;   // per-unit intensity weight (device) or null
+    double* out_int;       // device [ny][nx] FP64 intensity accumulation, or null
+    void* out_planes;      // device complex128 [units][ncomp][ny][nx], or null
+    wos_context cc;
+    wos_diag* diag;
+};
+
+// Batched ASM on the specialised sweeps (power-of-two grids): the forward row
+// sweep once per component for a shared input, then per chunk of units one
+// column sweep (gridDim.y = units, per-unit wavelength / distance, the shared
+// row spectrum as its source) and one row sweep that either accumulates the
+// weighted intensity of the chunk in registers or writes each unit's plane.
+// Diagnostics: per-unit spectral loss sums and histograms from the column
+// records, input power from the row records.  -1: not eligible.
+int try_fast_batch(wos_ctx c, Batch& b, std::vector<double>& sums, std::vector<double>& pin_unit,
+                   double& pin_total) {
+    const int ny = b.ny, nx = b.nx, ncomp = b.ncomp;
+    if (c->no_fast || !is_pow2(nx) || !is_pow2(ny)) return -1;
+    if (!c->fp64) {
+        for (int u = 0; u < b.units; u++) {
+            const double wl = b.wl.empty() ? b.cc.wavelength : b.wl[u];
+            const double z = b.z.empty() ? 0.0 : b.z[u];
+            if (!(std::fabs(z / wl) < 268435456.0)) return -1;
+        }
+    }
+    const Tune t = get_tune(c, ny, nx);
+    if (!fast_supported(c->fp64, nx, t.rowE) || !fast_supported(c->fp64, ny, t.colE)) return -1;
+    const double dx = b.dx;
+    const long long np = (long long)ny * nx;
+    const bool shared_in = b.in_unit_stride == 0;
+    const bool diag = b.diag != nullptr;
+    Axis *ax, *ay;
+    TRY(get_axis(c, nx, c->fp64, &ax));
+    TRY(get_axis(c, ny, c->fp64, &ay));
+    const void *twx, *twy;
+    TRY(fast_tw(c, ax, t.rowE, &twx));
+    TRY(fast_tw(c, ay, t.colE, &twy));
+    const size_t per = (size_t)np * c->csz();
+    int B = (int)std::max<size_t>(1, ((size_t)4 << 30) / per);
+    B = std::min(B, b.units);
+    B = std::min(B, 65535);
+    const size_t nbr = fast_row_blocks(nx, t.rowE, ny, shared_in ? 1 : B);
+    const size_t nbc = fast_col_blocks(c->fp64, ny, t.colE, t.colW, nx, 1);
+    TRY(red_prepare(c, std::max(nbr, nbc * (size_t)B)));
+    if (diag) TRY(ensure(c->tmp, sizeof(double) * RS_COUNT * (size_t)B));
+    TRY(ensure(c->scratch, (size_t)(shared_in ? 1 : B) * per));
+    TRY(ensure(c->scratch2, (size_t)B * per));
+    void* S0 = c->scratch.p;
+    void* S1 = c->scratch2.p;
+    const Policy pol = ev_policy(b.cc, b.z.empty() ? 1.0 : b.z[0]);
+    const HArgs h = asm_h(c, b.cc, b.z.empty() ? 0.0 : b.z[0], pol, dx, nx, ny);
+    double* o = reinterpret_cast<double*>(c->tmp.p);
+    int nb = 0;
+    for (int comp = 0; comp < ncomp; comp++) {
+        for (int k0 = 0; k0 < b.units; k0 += B) {
+            const int nu = std::min(B, b.units - k0);
+            if (k0 == 0 || !shared_in) {
+                FastRows r{};
+                r.rows = ny;
+                r.in = reinterpret_cast<const double2*>(b.in) +
+                       (shared_in ? comp * np : ((long long)k0 * ncomp + comp) * np);
+                r.in_c128 = 1;
+                r.in_ld = nx;
+                r.in_bstride = shared_in ? 0 : ncomp * np;
+                r.out = S0;
+                r.out_ld = nx;
+                r.out_bstride = np;
+                r.tw = twx;
+                r.out_scale = 1.0;
+                r.batch = shared_in ? 1 : nu;
+                if (diag) {
+                    r.red = red_region(c, 0) + RS_P;
+                    r.red_stride = RS_COUNT;
+                }
+                CK(timed_launch(c, 0, [&] { return fast_rows(c->fp64, nx, t.rowE, false, r, c->st, &nb); }));
+                if (diag) {
+                    const int per_unit = nb / r.batch;
+                    CK(launch_reduce_finish(red_region(c, 0), per_unit, r.batch, RS_P, 1, o, c->st));
+                    std::vector<double> hh((size_t)r.batch * RS_COUNT);
+                    CK(cudaMemcpyAsync(hh.data(), o, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost, c->st));
+                    CK(cudaStreamSynchronize(c->st));
+                    for (int u = 0; u < r.batch; u++) {
+                        const double p = hh[(size_t)u * RS_COUNT + RS_P] * dx * dx;
+                        if (shared_in) pin_total += p;
+                        else pin_unit[k0 + u] += p;
+                    }
+                }
+            }
+            FastCols k{};
+            k.ncols = nx;
+            k.W = t.colW;
+            k.data = S1;
+            k.ld = nx;
+            k.bstride = np;
+            k.src = S0;
+            k.src_bstride = shared_in ? 0 : np;
+            k.tw = twy;
+            k.batch = nu;
+            k.wl = b.cc.wavelength;
+            k.dx = dx;
+            k.z = b.z.empty() ? 0.0 : b.z[0];
+            k.kz = h.kz;
+            k.kaz = h.kaz;
+            k.krev = h.kz / (2 * M_PI);
+            k.batch_wl = b.wl_dev ? b.wl_dev + k0 : nullptr;
+            k.batch_z = b.z_dev ? b.z_dev + k0 : nullptr;
+            k.scale = h.scale;
+            k.alpha = h.alpha;
+            k.limit = h.limit;
+            k.zero_ev = h.zero_ev;
+            k.reg = h.reg;
+            k.backward = h.z < 0;
+            if (diag) {
+                k.red = red_region(c, 1) + RS_SW;
+                k.red_stride = RS_COUNT;
+                k.hist = red_region(c, 1) + RS_HIST;
+                k.hist_dx = dx;
+            }
+            CK(timed_launch(c, 4, [&] { return sweep_cols(c, ny, t.colE, k, &nb); }));
+            if (diag) {
+                const int per_unit = nb / nu;
+                CK(launch_reduce_finish(red_region(c, 1), per_unit, nu, RS_SW, 2, o, c->st));
+                CK(launch_reduce_finish(red_region(c, 1), per_unit, nu, RS_HIST, 97, o, c->st));
+                std::vector<double> hh((size_t)nu * RS_COUNT);
+                CK(cudaMemcpyAsync(hh.data(), o, sizeof(double) * hh.size(), cudaMemcpyDeviceToHost, c->st));
+                CK(cudaStreamSynchronize(c->st));
+                for (int u = 0; u < nu; u++)
+                    for (int sl = RS_SW; sl < RS_COUNT; sl++)
+                        sums[((size_t)(k0 + u) * ncomp + comp) * RS_COUNT + sl] = hh[(size_t)u * RS_COUNT + sl];
+            }
+            FastRows q{};
+            q.rows = ny;
+            q.in = S1;
+            q.in_ld = nx;
+            q.in_bstride = np;
+            q.tw = twx;
+            q.out_scale = 1.0;
+            if (b.out_int) {
+                AccArgs acc{nu, b.w_dev ? b.w_dev + k0 : nullptr, b.out_int, 1};
+                CK(timed_launch(c, 1, [&] { return fast_rows_acc(c->fp64, nx, t.rowE, q, acc, c->st, &nb); }));
+            } else {
+                q.out = reinterpret_cast<double2*>(b.out_planes) + ((long long)k0 * ncomp + comp) * np;
+                q.out_c128 = 1;
+                q.out_ld = nx;
+                q.out_bstride = ncomp * np;
+                q.batch = nu;
+                CK(timed_launch(c, 1, [&] { return fast_rows(c->fp64, nx, t.rowE, true, q, c->st, &nb); }));
+            }
+        }
+    }
+    return WOS_OK;
+}
+
+int run_batch_asm(wos_ctx c, Batch& b) {
+    const int ny = b.ny, nx = b.nx, ncomp = b.ncomp;
+    const double dx = b.dx;
+    const long long np = (long long)ny * nx;
+    Axis *ax, *ay;
+    TRY(get_axis(c, nx, c->fp64, &ax));
+    TRY(get_axis(c, ny, c->fp64, &ay));
+    const int W = auto_colw(c, ay->L);
+    const bool shared_in = b.in_unit_stride == 0;
+    // chunk the units so the per-chunk spectra stay within ~4 GiB
+    const size_t per = (size_t)np * c->csz();
+    int B = (int)std::max<size_t>(1, ((size_t)4 << 30) / per);
+    B = std::min(B, b.units);
+    B = std::min(B, 65535);
+    const size_t nbr1 = row_blocks(c->fp64, ax->L, ny, shared_in ? 1 : B);
+    const size_t nbc1 = col_blocks(c->fp64, ay->L, W, nx, 1);
+    TRY(red_prepare(c, std::max(nbr1, nbc1 * (size_t)B)));
+    const bool diag = b.diag != nullptr;
+    // spectral sums per unit and component, plus a histogram per unit
+    std::vector<double> sums((size_t)b.units * RS_COUNT * ncomp, 0.0);
+    if (diag) TRY(ensure(c->tmp, sizeof(double) * RS_COUNT * (size_t)B));
+    TRY(ensure(c->scratch, (size_t)(shared_in ? 1 : B) * per));
+    TRY(ensure(c->scratch2, (size_t)B * per));
+    void* S0 = c->scratch.p;
+    void* S1 = c->scratch2.p;
+    const Policy pol = ev_policy(b.cc, b.z.empty() ? 1.0 : b.z[0]);
+    double pin_total = 0;
+    std::vector<double> pin_unit(b.units, 0.0);
+    const int fast = try_fast_batch(c, b, sums, pin_unit, pin_total);
+    if (fast != -1 && fast != WOS_OK) return fast;
+    for (int comp = 0; comp < ncomp && fast == -1; comp++) {
+        for (int k0 = 0; k0 < b.units; k0 += B) {
+            const int nb = std::min(B, b.units - k0);
+            // rows forward (the shared input once per component, else per unit)
+            if (k0 == 0 || !shared_in) {
+                RowArgs r = row_defaults(ny, nx, dx);
+                r.mode = ROW_FWD;
+                r.rows = ny;
+                fill_axis(r, ax);
+                r.in = reinterpret_cast<const double2*>(b.in) +
+                       (shared_in ? comp * np : ((long long)k0 * ncomp + comp) * np);
+                r.in_c128 = 1;
+                r.in_ld = nx;
+                r.in_bstride = shared_in ? 0 : ncomp * np;
+                r.in_n = nx;
+                r.out = S0;
+                r.out_ld = nx;
+                r.out_bstride = np;
+                r.out_n = nx;
+                r.batch = shared_in ? 1 : nb;
+                if (diag) {
+                    r.red = red_region(c, 0);
+                    r.red_pre = 1;
+                }
+                CK(prof_rows(c, c->fp64, r));
+                if (diag) {
+                    const int nbr = (int)row_blocks(c->fp64, ax->L, ny, 1);
+                    CK(launch_reduce_finish(r.red, nbr, r.batch, RS_P, 1, reinterpret_cast<double*>(c->tmp.p), c->st));
+                    std::vector<double> h((size_t)r.batch * RS_COUNT);
+                    CK(cudaMemcpyAsync(h.data(), c->tmp.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+                    CK(cudaStreamSynchronize(c->st));
+                    for (int u = 0; u < r.batch; u++) {
+                        const double p = h[(size_t)u * RS_COUNT + RS_P] * dx * dx;
+                        if (shared_in) pin_total += p;
+                        else pin_unit[k0 + u] += p;
+                    }
+                }
+            }
+            ColArgs a = col_defaults(c, dx);
+            a.mode = COL_FUSED;
+            a.ncols = nx;
+            fill_axis(a, ay);
+            a.W = W;
+            a.src = S0;
+            a.src_ld = nx;
+            a.src_bstride = np;
+            a.src_shared = shared_in;
+            a.in_n = ny;
+            a.dst = S1;
+            a.dst_ld = nx;
+            a.dst_bstride = np;
+            a.out_n = ny;
+            a.h = asm_h(c, b.cc, b.z.empty() ? 0.0 : b.z[0], pol, dx, nx, ny);
+            a.h.wl = -1;  // per-unit k, k z, k |z| are formed on the device from wl and z
+            a.batch_wl = b.wl_dev ? b.wl_dev + k0 : nullptr;
+            a.batch_z = b.z_dev ? b.z_dev + k0 : nullptr;
+            if (!b.wl_dev) a.h.wl = b.cc.wavelength, a.h.k = 2 * M_PI / b.cc.wavelength;
+            a.batch = nb;
+            if (diag) {
+                a.red = red_region(c, 1);
+                a.red_bpm = 1;
+                a.red_hist = 1;
+                a.hist_lx = nx;
+                a.hist_ly = ny;
+                a.hist_dx = dx;
+            }
+            CK(prof_cols(c, c->fp64, a));
+            if (diag) {
+                double* o = reinterpret_cast<double*>(c->tmp.p);
+                CK(launch_reduce_finish(a.red, (int)nbc1, nb, RS_SW, 3, o, c->st));
+                CK(launch_reduce_finish(a.red, (int)nbc1, nb, RS_HIST, 97, o, c->st));
+                std::vector<double> h((size_t)nb * RS_COUNT);
+                CK(cudaMemcpyAsync(h.data(), o, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->st));
+                CK(cudaStreamSynchronize(c->st));
+                for (int u = 0; u < nb; u++)
+                    for (int sl = RS_SW; sl < RS_COUNT; sl++)
+                        sums[((size_t)(k0 + u) * ncomp + comp) * RS_COUNT + sl] = h[(size_t)u * RS_COUNT + sl];
+            }
+            RowArgs q = row_defaults(ny, nx, dx);
+            q.rows = ny;
+            fill_axis(q, ax);
+            q.in = S1;
+            q.in_ld = nx;
+            q.in_bstride = np;
+            q.in_n = nx;
+            q.out_ld = nx;
+            q.out_n = nx;
+            if (b.out_int) {
+                q.mode = ROW_INV_ACC;
+                q.acc_nb = nb;
+                q.acc_weight = b.w_dev ? b.w_dev + k0 : nullptr;
+                q.acc_add = 1;
+                q.out = b.out_int;
+                q.out_accum_int = 2;
+                q.out_bstride = 0;
+                q.batch = 1;
+            } else {
+                q.mode = ROW_INV;
+                q.out = reinterpret_cast<double2*>(b.out_planes) + ((long long)k0 * ncomp + comp) * np;
+                q.out_c128 = 1;
+                q.out_bstride = ncomp * np;
+                q.batch = nb;
+            }
+            CK(prof_rows(c, c->fp64, q));
+        }
+    }
+    if (diag) {
+        // per unit, in order: asmWrapWarn then asmWarn (optics/propagate.go:325-332)
+        for (int u = 0; u < b.units; u++) {
+            wos_context cu = b.cc;
+            if (!b.wl.empty()) cu.wavelength = b.wl[u];
+            const double zu = b.z.empty() ? 0.0 : b.z[u];
+            if (zu == 0) continue;
+            double sw = 0, s1 = 0, hist[97] = {0};
+            for (int comp = 0; comp < ncomp; comp++) {
+                const double* rr = &sums[((size_t)u * ncomp + comp) * RS_COUNT];
+                sw += rr[RS_SW];
+                s1 += rr[RS_SW + 1];
+                for (int k = 0; k < 97; k++) hist[k] += rr[RS_HIST + k];
+            }
+            if (wrap_needed(cu, ny, nx, dx, zu)) wrap_finish(b.diag, cu, ny, nx, dx, zu, hist);
+            const double pin = shared_in ? pin_total : pin_unit[u];
+            const double frac = sw > 0 ? s1 / sw : 0.0;  // spectral loss fraction of the step
+            asm_warn(b.diag, zu, pin, pin - pin * frac, ev_policy(cu, zu));
+        }
+    }
+    return WOS_OK;
+}
+
+int upload_params(wos_ctx c, const std::vector<double>& a, const std::vector<double>& b2,
+                  const std::vector<double>& c3, double** pa, double** pb, double** pc) {
+    const size_t n = a.size() + b2.size() + c3.size();
+    TRY(ensure(c->params, sizeof(double) * std::max<size_t>(n, 1)));
+    double* p = reinterpret_cast<double*>(c->params.p);
+    std::vector<double> all;
+    all.insert(all.end(), a.begin(), a.end());
+    all.insert(all.end(), b2.begin(), b2.end());
+    all.insert(all.end(), c3.begin(), c3.end());
+    if (n) CK(cudaMemcpyAsync(p, all.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->st));
+    *pa = p;
+    *pb = p + a.size();
+    *pc = p + a.size() + b2.size();
+    return WOS_OK;
+}
+
+}  // namespace wapi
+
+extern "C" {
+
+int wos_polychromatic(wos_ctx c, const wos_field* f, double z, const double* wavelengths, const double* weights,
+                      int nsamples, int method, const wos_context* base, double* out, wos_diag* diag) {
+    if (!c || !wavelengths || !weights || !out) return fail(WOS_INVALID_ARG, "null argument");
+    TRY(check_field(f));
+    if (nsamples <= 0) return fail(WOS_INVALID_ARG, "polychromatic: no wavelength samples");
+    for (int s = 0; s < nsamples; s++)
+        if (!(wavelengths[s] > 0)) return fail(WOS_INVALID_ARG, "polychromatic: wavelength must be > 0");
+    if (method < WOS_ASM || method > WOS_FRAUNHOFER) return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
+    if (diag) {
+        std::memset(diag, 0, sizeof(*diag));
+        diag->dx_out = f->dx;
+    }
+    // a nil base context means Context{Evanescent: "decay", Warnings: &Warnings{}}
+    wos_context cc = base ? *base : default_context();
+    if (!base) cc.diagnostics = 1;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const int ncomp = f->polarized ? 2 : 1;
+    const long long np = (long long)f->ny * f->nx;
+    TRY(stage_in(c, const_cast<wos_field*>(f), ncomp));
+    TRY(ensure(c->accum, sizeof(double) * np));
+    double* acc = reinterpret_cast<double*>(c->accum.p);
+    CK(cudaMemsetAsync(acc, 0, sizeof(double) * np, c->st));
+    wos_diag* dp = (cc.diagnostics && diag) ? diag : nullptr;
+    if (z == 0) {
+        for (int s = 0; s < nsamples; s++) CK(launch_accum_int(1, acc, c->stage.p, ncomp, np, weights[s], c->st));
+    } else if (method == WOS_ASM) {
+        std::vector<double> wl(wavelengths, wavelengths + nsamples), w(weights, weights + nsamples);
+        double *wl_d, *w_d, *unused;
+        TRY(upload_params(c, wl, w, {}, &wl_d, &w_d, &unused));
+        Batch b{f->ny, f->nx, ncomp, f->dx, c->stage.p, 0, nsamples, wl_d, nullptr, wl,
+                std::vector<double>(nsamples, z), w_d, acc, nullptr, cc, dp};
+        TRY(run_batch_asm(c, b));
+    } else {
+        TRY(ensure(c->scratch3, (size_t)np * ncomp * c->csz()));
+        void* O = c->scratch3.p;
+        for (int s = 0; s < nsamples; s++) {
+            wos_context cs = cc;
+            cs.wavelength = wavelengths[s];
+            wos_diag ds;
+            Prop p{f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, O, 0, z, method, cs, dp ? &ds : nullptr};
+            TRY(run_propagate(c, p));
+            if (dp) diag_merge(dp, ds);
+            CK(launch_accum_int(c->fp64, acc, O, ncomp, np, weights[s], c->st));
+        }
+    }
+    CK(cudaMemcpyAsync(out, acc, sizeof(double) * np, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+int wos_volume(wos_ctx c, const wos_field* f, const double* zs, int nz, int method, const wos_context* cci,
+               wos_c128* out, wos_diag* diag) {
+    if (!c || (nz > 0 && (!zs || !out)) || nz < 0) return fail(WOS_INVALID_ARG, "null argument");
+    TRY(check_field(f));
+    if (method < WOS_ASM || method > WOS_FRAUNHOFER) return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
+    if (diag) {
+        std::memset(diag, 0, sizeof(*diag));
+        diag->dx_out = f->dx;
+    }
+    if (nz == 0) return WOS_OK;
+    const wos_context cc = cci ? *cci : default_context();
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const int ncomp = f->polarized ? 2 : 1;
+    const long long np = (long long)f->ny * f->nx;
+    TRY(stage_in(c, const_cast<wos_field*>(f), ncomp));
+    TRY(ensure(c->vol, sizeof(double2) * (size_t)np * ncomp * nz));
+    double2* O = reinterpret_cast<double2*>(c->vol.p);
+    bool batched = method == WOS_ASM;
+    std::vector<double> zb;
+    std::vector<int> idx;
+    for (int q = 0; q < nz; q++) {
+        if (zs[q] != 0) {
+            zb.push_back(zs[q]);
+            idx.push_back(q);
+            if (zs[q] < 0) batched = false;
+        }
+    }
+    wos_diag* dp = diag;
+    if (batched && !zb.empty()) {
+        // the batch writes its planes compactly, then they move to their slots
+        TRY(ensure(c->scratch3, sizeof(double2) * (size_t)np * ncomp * zb.size()));
+        double2* Ob = reinterpret_cast<double2*>(c->scratch3.p);
+        double *z_d, *u1, *u2;
+        TRY(upload_params(c, zb, {}, {}, &z_d, &u1, &u2));
+        Batch b{f->ny, f->nx, ncomp, f->dx, c->stage.p, 0, (int)zb.size(), nullptr, z_d, {}, zb, nullptr, nullptr,
+                Ob, cc, (cc.diagnostics && dp) ? dp : nullptr};
+        TRY(run_batch_asm(c, b));
+        for (size_t u = 0; u < zb.size(); u++)
+            CK(cudaMemcpyAsync(O + (size_t)idx[u] * ncomp * np, Ob + u * ncomp * np, sizeof(double2) * ncomp * np,
+                               cudaMemcpyDeviceToDevice, c->st));
+    } else {
+        for (size_t u = 0; u < zb.size(); u++) {
+            wos_diag ds;
+            Prop p{f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, O + (size_t)idx[u] * ncomp * np, 1, zb[u], method, cc,
+                   (cc.diagnostics && dp) ? &ds : nullptr};
+            TRY(run_propagate(c, p));
+            if (cc.diagnostics && dp) diag_merge(dp, ds);
+        }
+    }
+    // z == 0 returns the input unchanged (optics/propagate.go:66-68)
+    for (int q = 0; q < nz; q++)
+        if (zs[q] == 0)
+            CK(cudaMemcpyAsync(O + (size_t)q * ncomp * np, c->stage.p, sizeof(double2) * ncomp * np,
+                               cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(out, O, sizeof(double2) * (size_t)np * ncomp * nz, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+int wos_schell_modes(wos_ctx c, int n, double dx, double width, double coherence, int m, const wos_c128* noise,
+                     wos_c128* modes_out) {
+    if (!c || !noise || !modes_out || n < 2 || !(dx > 0)) return fail(WOS_INVALID_ARG, "null argument");
+    if (!(width > 0) || !(coherence > 0)) return fail(WOS_INVALID_ARG, "schell: width and coherence must be > 0");
+    if (m <= 0) m = 1;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const long long nn = (long long)n * n;
+    TRY(ensure(c->vol, sizeof(double2) * (size_t)nn * m));
+    double2* modes = reinterpret_cast<double2*>(c->vol.p);
+    TRY(schell_generate(c, n, dx, width, coherence, m, noise, modes));
+    CK(cudaMemcpyAsync(modes_out, modes, sizeof(double2) * (size_t)nn * m, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+int wos_partially_coherent(wos_ctx c, int n, double dx, double width, double coherence, int m,
+                           const wos_c128* noise, double z, int method, const wos_context* cci, double* out,
+                           wos_diag* diag) {
+    if (!c || !noise || !out || n < 2 || !(dx > 0)) return fail(WOS_INVALID_ARG, "null argument");
+    if (!(width > 0) || !(coherence > 0)) return fail(WOS_INVALID_ARG, "schell: width and coherence must be > 0");
+    if (method < WOS_ASM || method > WOS_FRAUNHOFER) return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
+    if (m <= 0) m = 1;
+    if (diag) {
+        std::memset(diag, 0, sizeof(*diag));
+        diag->dx_out = dx;
+    }
+    const wos_context cc = cci ? *cci : default_context();
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const long long nn = (long long)n * n;
+    TRY(ensure(c->vol, sizeof(double2) * (size_t)nn * m));
+    double2* modes = reinterpret_cast<double2*>(c->vol.p);
+    TRY(schell_generate(c, n, dx, width, coherence, m, noise, modes));
+    TRY(ensure(c->accum, sizeof(double) * nn));
+    double* acc = reinterpret_cast<double*>(c->accum.p);
+    CK(cudaMemsetAsync(acc, 0, sizeof(double) * nn, c->st));
+    const double inv = 1 / (double)m;
+    wos_diag* dp = (cc.diagnostics && diag) ? diag : nullptr;
+    if (z == 0) {
+        for (int q = 0; q < m; q++) CK(launch_accum_int(1, acc, modes + q * nn, 1, nn, inv, c->st));
+    } else if (method == WOS_ASM) {
+        std::vector<double> w(m, inv);
+        double *w_d, *u1, *u2;
+        TRY(upload_params(c, w, {}, {}, &w_d, &u1, &u2));
+        Batch b{n, n, 1, dx, modes, nn, m, nullptr, nullptr, {}, std::vector<double>(m, z), w_d, acc, nullptr, cc, dp};
+        TRY(run_batch_asm(c, b));
+    } else {
+        TRY(ensure(c->scratch3, (size_t)nn * c->csz()));
+        void* O = c->scratch3.p;
+        for (int q = 0; q < m; q++) {
+            wos_diag ds;
+            Prop p{n, n, dx, 1, modes + q * nn, 1, O, 0, z, method, cc, dp ? &ds : nullptr};
+            TRY(run_propagate(c, p));
+            if (dp) diag_merge(dp, ds);
+            CK(launch_accum_int(c->fp64, acc, O, 1, nn, inv, c->st));
+        }
+    }
+    CK(cudaMemcpyAsync(out, acc, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return WOS_OK;
+}
+
+}  // extern "C"
