@@ -249,6 +249,32 @@ WOS_API int wos_partially_coherent(wos_ctx ctx, int n, double dx, double width, 
                            const wos_c128* noise, double z, int method, const wos_context* c,
                            double* out, wos_diag* diag);
 
+/* ---- device-resident batches: the forms of wos_polychromatic, wos_volume and
+ *      wos_partially_coherent for callers that keep fields on the GPU (no
+ *      counterpart in the reference, whose loops at optics/polychromatic.go:29-42,
+ *      optics/volume.go:10-16 and optics/coherence.go:110-115 they replace).
+ *      Method WOS_ASM, no diagnostics; fields of the context's complex type,
+ *      intensities FP64.  The wavelength, distance and weight lists are host
+ *      arrays, copied to the device only when they differ from an earlier
+ *      call's, and nothing synchronises the host: after a first call with the
+ *      same geometry and lists, a call can be recorded between
+ *      wos_graph_capture_begin and _end.  The units of one call share the row
+ *      spectrum of the input and run in one column launch (gridDim.y = units)
+ *      and one row launch per chunk of up to 4 GiB of spectra. ---- */
+/* out: device FP64 [ny][nx], overwritten with sum_k weights[k] |U_k|^2 over
+ * the components of field (device [ncomp][ny][nx]). */
+WOS_API int wos_polychromatic_dev(wos_ctx ctx, int ny, int nx, double dx, int ncomp, const void* field, double z,
+                                  const double* wavelengths, const double* weights, int nsamples,
+                                  const wos_context* base, double* out);
+/* out: device [nz][ncomp][ny][nx] of the context's complex type; plane q is the
+ * field propagated to zs[q] (zs[q] == 0 copies the field). */
+WOS_API int wos_volume_dev(wos_ctx ctx, int ny, int nx, double dx, int ncomp, const void* field, const double* zs,
+                           int nz, const wos_context* c, void* out);
+/* noise: device complex128 [m][n][n] (the place of Go's math/rand draws, as in
+ * wos_partially_coherent); out: device FP64 [n][n], the mean of |U_k|^2. */
+WOS_API int wos_partially_coherent_dev(wos_ctx ctx, int n, double dx, double width, double coherence, int m,
+                                       const void* noise, double z, const wos_context* c, double* out);
+
 /* ---- thin-element multiply (optics/elements.go:128-141,195-221,288-313,488-532). ---- */
 WOS_API int wos_apply_lens(wos_ctx ctx, wos_field* f, double wavelength, double focal, double aperture,
                    double x0, double y0);

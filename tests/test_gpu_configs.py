@@ -203,6 +203,17 @@ def test_cfg4_1_polychromatic_matches_oracle(prec):
         got = g.polychromatic(wos.Field(d["ex"].copy(), d["dx"]), d["z"], d["wls"], d["weights"], "asm", gc)
     record("cfg4.1", prec, rel_l2(got, ref), TOL_FP64 if prec == wos.FP64 else TOL_FP32)
     check_warnings(gc, oc, prec)
+    # the device-resident form on a device field
+    import torch
+    n = d["ex"].shape[0]
+    with wos.GPU(prec) as g:
+        fd = to_dev(d["ex"][None], prec)
+        out = torch.empty((n, n), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        g.polychromatic_dev(n, n, d["dx"], 1, fd.data_ptr(), d["z"], d["wls"], d["weights"],
+                            wos.Context(wavelength=d["wls"][0]), out.data_ptr())
+        g.synchronize()
+        record("cfg4.1 device", prec, rel_l2(out.cpu().numpy(), ref), TOL_FP64 if prec == wos.FP64 else TOL_FP32)
 
 
 @pytest.fixture(scope="module")
@@ -223,6 +234,15 @@ def test_cfg4_2_partially_coherent_matches_oracle(prec, cfg4_2_ref):
         got = g.partially_coherent(d["n"], d["dx"], d["width"], d["coherence"], d["noise"], d["z"], "asm",
                                    wos.Context(wavelength=d["wl"], warnings_enabled=False))
     record("cfg4.2", prec, rel_l2(got, ref), TOL_FP64_SCHELL if prec == wos.FP64 else TOL_FP32)
+    import torch
+    with wos.GPU(prec) as g:
+        nd = torch.from_numpy(d["noise"]).cuda()
+        out = torch.empty((d["n"], d["n"]), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        g.partially_coherent_dev(d["n"], d["dx"], d["width"], d["coherence"], d["noise"].shape[0], nd.data_ptr(),
+                                 d["z"], wos.Context(wavelength=d["wl"], warnings_enabled=False), out.data_ptr())
+        g.synchronize()
+        record("cfg4.2 device", prec, rel_l2(out.cpu().numpy(), ref), TOL_FP64_SCHELL if prec == wos.FP64 else TOL_FP32)
 
 
 @pytest.fixture(scope="module")
@@ -243,6 +263,57 @@ def test_cfg4_3_volume_matches_oracle(prec, cfg4_3_ref):
     assert rel_l2(got[0, 0], d["ex"]) <= (0.0 if prec == wos.FP64 else 1e-7)  # z = 0 returns the input
     record("cfg4.3", prec, rel_l2(got, ref), tol_case(prec, "asm", n, n))
     check_warnings(gc, oc, prec)
+    del got
+    import torch
+    with wos.GPU(prec) as g:
+        fd = to_dev(d["ex"][None], prec)
+        out = torch.empty((d["zs"].size, 1, n, n), dtype=torch_dt(prec), device="cuda")
+        torch.cuda.synchronize()
+        g.volume_dev(n, n, d["dx"], 1, fd.data_ptr(), d["zs"], wos.Context(wavelength=d["wl"]), out.data_ptr())
+        g.synchronize()
+        dev = out.cpu().numpy().astype(np.complex128)
+    record("cfg4.3 device", prec, rel_l2(dev, ref), tol_case(prec, "asm", n, n))
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_cfg4_device_batches_replay_from_one_graph(prec):
+    """The three device-resident batches recorded in one CUDA graph: a replay
+    reproduces the direct calls exactly (fewer units than the benchmark, same
+    grids)."""
+    import torch
+    d1, d2, d3 = W.cfg4_1(), W.cfg4_2(16), W.cfg4_3(16)
+    n1, n2, n3 = d1["ex"].shape[0], d2["n"], d3["ex"].shape[0]
+    with wos.GPU(prec) as g:
+        f1 = to_dev(d1["ex"][None], prec)
+        f3 = to_dev(d3["ex"][None], prec)
+        nz = torch.from_numpy(d2["noise"]).cuda()
+        o1 = torch.empty((n1, n1), dtype=torch.float64, device="cuda")
+        o2 = torch.empty((n2, n2), dtype=torch.float64, device="cuda")
+        o3 = torch.empty((d3["zs"].size, 1, n3, n3), dtype=torch_dt(prec), device="cuda")
+        torch.cuda.synchronize()
+
+        def run():
+            g.polychromatic_dev(n1, n1, d1["dx"], 1, f1.data_ptr(), d1["z"], d1["wls"], d1["weights"],
+                                wos.Context(wavelength=d1["wls"][0]), o1.data_ptr())
+            g.partially_coherent_dev(n2, d2["dx"], d2["width"], d2["coherence"], 16, nz.data_ptr(), d2["z"],
+                                     wos.Context(wavelength=d2["wl"]), o2.data_ptr())
+            g.volume_dev(n3, n3, d3["dx"], 1, f3.data_ptr(), d3["zs"], wos.Context(wavelength=d3["wl"]),
+                         o3.data_ptr())
+        run()
+        g.synchronize()
+        direct = [o1.cpu().numpy(), o2.cpu().numpy(), o3.cpu().numpy()]
+        for o in (o1, o2, o3):
+            o.zero_()
+        torch.cuda.synchronize()
+        g.graph_capture_begin()
+        run()
+        gr = g.graph_capture_end()
+        gr.launch()
+        g.synchronize()
+        replay = [o1.cpu().numpy(), o2.cpu().numpy(), o3.cpu().numpy()]
+        gr.close()
+    for a, b in zip(direct, replay):
+        assert np.array_equal(a, b)
 
 
 # ------------------------------------------------------------------ cfg5

@@ -1274,6 +1274,8 @@ int wos_ctx_destroy(wos_ctx c) {
             }
         for (auto& h : c->htab)
             if (h.buf.p) cudaFree(h.buf.p);
+        for (auto& ps : c->pslot)
+            if (ps.buf.p) cudaFree(ps.buf.p);
         DevBuf* bufs[] = {&c->stage, &c->scratch, &c->scratch2, &c->scratch3, &c->red, &c->redout, &c->tmp,
                           &c->maps, &c->params, &c->vol, &c->accum, &c->aux};
         for (DevBuf* b : bufs)

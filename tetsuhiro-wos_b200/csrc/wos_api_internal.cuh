@@ -111,6 +111,16 @@ struct wos_ctx_s {
     HTab htab[kHTabs];
     int htab_next = 0;
     int htab_on = 1;                    // WOS_HTAB=0: evaluate H in the sweep
+    // device copies of the small parameter lists (wavelengths, distances,
+    // weights) of the device-resident batches, keyed by content and reused
+    // round robin: a repeated call copies nothing from the host
+    struct ParamSlot {
+        std::vector<double> host;
+        DevBuf buf;
+    };
+    static constexpr int kParamSlots = 8;
+    ParamSlot pslot[kParamSlots];
+    int pslot_next = 0;
     unsigned* err_dev = nullptr;        // error word of the pipelined kernels (device)
     unsigned* err_host = nullptr;       // pinned mirror, read where the host synchronises
     // streams for independent fields of a batch (wos_propagate_batch_dev),

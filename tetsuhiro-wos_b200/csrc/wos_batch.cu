@@ -13,7 +13,7 @@ int fft2d_fp64(wos_ctx c, int n, int batch, double2* a, int inverse) {
 }
 
 // GenerateSchellRealizations (optics/coherence.go:22-80) into modes (device, complex128)
-int schell_generate(wos_ctx c, int n, double dx, double width, double coh, int m, const wos_c128* noise,
+int schell_generate(wos_ctx c, int n, double dx, double width, double coh, int m, const void* noise, bool noise_dev,
                     double2* modes) {
     const long long nn = (long long)n * n;
     TRY(ensure(c->aux, (size_t)nn * (16 + 8)));
@@ -22,7 +22,8 @@ int schell_generate(wos_ctx c, int n, double dx, double width, double coh, int m
     CK(launch_schell_mu(mu, n, dx, coh, c->st));
     TRY(fft2d_fp64(c, n, 1, mu, 0));
     CK(launch_sqrt_re(sqs, mu, nn, c->st));
-    CK(cudaMemcpyAsync(modes, noise, (size_t)nn * m * 16, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(modes, noise, (size_t)nn * m * 16, noise_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                       c->st));
     CK(launch_mul_map(modes, sqs, nn, m, c->st));
     TRY(fft2d_fp64(c, n, m, modes, 1));
     CK(launch_schell_env(modes, n, dx, width, m, c->st));
@@ -47,6 +48,10 @@ struct Batch {
     void* out_planes;      // device complex128 [units][ncomp][ny][nx], or null
     wos_context cc;
     wos_diag* diag;
+    int in_native = 0;     // in holds the context's complex type, not complex128
+    int out_native = 0;    // out_planes of the context's complex type
+    size_t in_esz(wos_ctx c) const { return in_native ? c->csz() : 16; }
+    size_t out_esz(wos_ctx c) const { return out_native ? c->csz() : 16; }
 };
 
 // Batched ASM on the specialised sweeps (power-of-two grids): the forward row
@@ -101,9 +106,9 @@ int try_fast_batch(wos_ctx c, Batch& b, std::vector<double>& sums, std::vector<d
             if (k0 == 0 || !shared_in) {
                 FastRows r{};
                 r.rows = ny;
-                r.in = reinterpret_cast<const double2*>(b.in) +
-                       (shared_in ? comp * np : ((long long)k0 * ncomp + comp) * np);
-                r.in_c128 = 1;
+                r.in = reinterpret_cast<const char*>(b.in) +
+                       b.in_esz(c) * (shared_in ? comp * np : ((long long)k0 * ncomp + comp) * np);
+                r.in_c128 = !b.in_native;
                 r.in_ld = nx;
                 r.in_bstride = shared_in ? 0 : ncomp * np;
                 r.out = S0;
@@ -183,8 +188,8 @@ int try_fast_batch(wos_ctx c, Batch& b, std::vector<double>& sums, std::vector<d
                 AccArgs acc{nu, b.w_dev ? b.w_dev + k0 : nullptr, b.out_int, 1};
                 CK(timed_launch(c, 1, [&] { return fast_rows_acc(c->fp64, nx, t.rowE, q, acc, c->st, &nb); }));
             } else {
-                q.out = reinterpret_cast<double2*>(b.out_planes) + ((long long)k0 * ncomp + comp) * np;
-                q.out_c128 = 1;
+                q.out = reinterpret_cast<char*>(b.out_planes) + b.out_esz(c) * (((long long)k0 * ncomp + comp) * np);
+                q.out_c128 = !b.out_native;
                 q.out_ld = nx;
                 q.out_bstride = ncomp * np;
                 q.batch = nu;
@@ -234,9 +239,9 @@ int run_batch_asm(wos_ctx c, Batch& b) {
                 r.mode = ROW_FWD;
                 r.rows = ny;
                 fill_axis(r, ax);
-                r.in = reinterpret_cast<const double2*>(b.in) +
-                       (shared_in ? comp * np : ((long long)k0 * ncomp + comp) * np);
-                r.in_c128 = 1;
+                r.in = reinterpret_cast<const char*>(b.in) +
+                       b.in_esz(c) * (shared_in ? comp * np : ((long long)k0 * ncomp + comp) * np);
+                r.in_c128 = !b.in_native;
                 r.in_ld = nx;
                 r.in_bstride = shared_in ? 0 : ncomp * np;
                 r.in_n = nx;
@@ -323,8 +328,8 @@ int run_batch_asm(wos_ctx c, Batch& b) {
                 q.batch = 1;
             } else {
                 q.mode = ROW_INV;
-                q.out = reinterpret_cast<double2*>(b.out_planes) + ((long long)k0 * ncomp + comp) * np;
-                q.out_c128 = 1;
+                q.out = reinterpret_cast<char*>(b.out_planes) + b.out_esz(c) * (((long long)k0 * ncomp + comp) * np);
+                q.out_c128 = !b.out_native;
                 q.out_bstride = ncomp * np;
                 q.batch = nb;
             }
@@ -351,6 +356,31 @@ int run_batch_asm(wos_ctx c, Batch& b) {
             asm_warn(b.diag, zu, pin, pin - pin * frac, ev_policy(cu, zu));
         }
     }
+    return WOS_OK;
+}
+
+// Device copy of a small parameter list (wavelengths, distances, weights of
+// the device-resident batches): an earlier call's copy holding the same
+// values is reused, so a repeated call copies nothing from the host.
+int cached_params(wos_ctx c, const std::vector<double>& v, const double** out) {
+    for (auto& ps : c->pslot)
+        if (ps.buf.p && ps.host == v) {
+            *out = reinterpret_cast<const double*>(ps.buf.p);
+            return WOS_OK;
+        }
+    wos_ctx_s::ParamSlot& ps = c->pslot[c->pslot_next];
+    c->pslot_next = (c->pslot_next + 1) % wos_ctx_s::kParamSlots;
+    ps.host.clear();
+    TRY(ensure(ps.buf, sizeof(double) * std::max<size_t>(v.size(), 1)));
+    if (!v.empty())
+        CK(cudaMemcpyAsync(ps.buf.p, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, c->st));
+    ps.host = v;
+    *out = reinterpret_cast<const double*>(ps.buf.p);
+    return WOS_OK;
+}
+
+int check_dev_geometry(int ny, int nx, double dx, int ncomp) {
+    if (ny < 2 || nx < 2 || ncomp < 1 || ncomp > 2 || !(dx > 0)) return fail(WOS_INVALID_ARG, "invalid field geometry");
     return WOS_OK;
 }
 
@@ -495,7 +525,7 @@ int wos_schell_modes(wos_ctx c, int n, double dx, double width, double coherence
     const long long nn = (long long)n * n;
     TRY(ensure(c->vol, sizeof(double2) * (size_t)nn * m));
     double2* modes = reinterpret_cast<double2*>(c->vol.p);
-    TRY(schell_generate(c, n, dx, width, coherence, m, noise, modes));
+    TRY(schell_generate(c, n, dx, width, coherence, m, noise, false, modes));
     CK(cudaMemcpyAsync(modes_out, modes, sizeof(double2) * (size_t)nn * m, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     return WOS_OK;
@@ -518,7 +548,7 @@ int wos_partially_coherent(wos_ctx c, int n, double dx, double width, double coh
     const long long nn = (long long)n * n;
     TRY(ensure(c->vol, sizeof(double2) * (size_t)nn * m));
     double2* modes = reinterpret_cast<double2*>(c->vol.p);
-    TRY(schell_generate(c, n, dx, width, coherence, m, noise, modes));
+    TRY(schell_generate(c, n, dx, width, coherence, m, noise, false, modes));
     TRY(ensure(c->accum, sizeof(double) * nn));
     double* acc = reinterpret_cast<double*>(c->accum.p);
     CK(cudaMemsetAsync(acc, 0, sizeof(double) * nn, c->st));
@@ -546,6 +576,112 @@ int wos_partially_coherent(wos_ctx c, int n, double dx, double width, double coh
     CK(cudaMemcpyAsync(out, acc, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     return WOS_OK;
+}
+
+// ---- device-resident batches
+int wos_polychromatic_dev(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* field, double z,
+                          const double* wavelengths, const double* weights, int nsamples, const wos_context* base,
+                          double* out) {
+    if (!c || !field || !out || !wavelengths || !weights) return fail(WOS_INVALID_ARG, "null argument");
+    TRY(check_dev_geometry(ny, nx, dx, ncomp));
+    if (nsamples <= 0) return fail(WOS_INVALID_ARG, "polychromatic: no wavelength samples");
+    for (int s = 0; s < nsamples; s++)
+        if (!(wavelengths[s] > 0)) return fail(WOS_INVALID_ARG, "polychromatic: wavelength must be > 0");
+    wos_context cc = base ? *base : default_context();
+    cc.diagnostics = 0;
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const long long np = (long long)ny * nx;
+    CK(cudaMemsetAsync(out, 0, sizeof(double) * np, c->st));
+    if (z == 0) {  // every sample's Propagate returns at once (optics/propagate.go:66-68)
+        for (int s = 0; s < nsamples; s++) CK(launch_accum_int(c->fp64, out, field, ncomp, np, weights[s], c->st));
+        return WOS_OK;
+    }
+    std::vector<double> wl(wavelengths, wavelengths + nsamples), w(weights, weights + nsamples);
+    const double *wl_d, *w_d;
+    TRY(cached_params(c, wl, &wl_d));
+    TRY(cached_params(c, w, &w_d));
+    Batch b{ny, nx, ncomp, dx, field, 0, nsamples, wl_d, nullptr, wl, std::vector<double>(nsamples, z), w_d, out,
+            nullptr, cc, nullptr};
+    b.in_native = 1;
+    return run_batch_asm(c, b);
+}
+
+int wos_volume_dev(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* field, const double* zs, int nz,
+                   const wos_context* cci, void* out) {
+    if (!c || !field || nz < 0 || (nz > 0 && (!zs || !out))) return fail(WOS_INVALID_ARG, "null argument");
+    TRY(check_dev_geometry(ny, nx, dx, ncomp));
+    if (nz == 0) return WOS_OK;
+    wos_context cc = cci ? *cci : default_context();
+    cc.diagnostics = 0;
+    if (!(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const size_t plane = (size_t)ny * nx * ncomp * c->csz();
+    char* O = reinterpret_cast<char*>(out);
+    std::vector<double> zb;
+    std::vector<int> idx;
+    bool batched = true;
+    for (int q = 0; q < nz; q++)
+        if (zs[q] != 0) {
+            zb.push_back(zs[q]);
+            idx.push_back(q);
+            if (zs[q] < 0) batched = false;
+        }
+    if (!zb.empty() && batched) {
+        // all planes straight into out, or compactly then moved to their slots
+        const bool compact = (int)zb.size() != nz;
+        char* dst = O;
+        if (compact) {
+            TRY(ensure(c->scratch3, plane * zb.size()));
+            dst = reinterpret_cast<char*>(c->scratch3.p);
+        }
+        const double* z_d;
+        TRY(cached_params(c, zb, &z_d));
+        Batch b{ny, nx, ncomp, dx, field, 0, (int)zb.size(), nullptr, z_d, {}, zb, nullptr, nullptr, dst, cc, nullptr};
+        b.in_native = 1;
+        b.out_native = 1;
+        TRY(run_batch_asm(c, b));
+        if (compact)
+            for (size_t u = 0; u < zb.size(); u++)
+                CK(cudaMemcpyAsync(O + (size_t)idx[u] * plane, dst + u * plane, plane, cudaMemcpyDeviceToDevice, c->st));
+    } else {
+        for (size_t u = 0; u < zb.size(); u++) {
+            Prop p{ny, nx, dx, ncomp, field, 0, O + (size_t)idx[u] * plane, 0, zb[u], WOS_ASM, cc, nullptr};
+            TRY(run_propagate(c, p));
+        }
+    }
+    // z == 0 returns the input unchanged (optics/propagate.go:66-68)
+    for (int q = 0; q < nz; q++)
+        if (zs[q] == 0) CK(cudaMemcpyAsync(O + (size_t)q * plane, field, plane, cudaMemcpyDeviceToDevice, c->st));
+    return WOS_OK;
+}
+
+int wos_partially_coherent_dev(wos_ctx c, int n, double dx, double width, double coherence, int m, const void* noise,
+                               double z, const wos_context* cci, double* out) {
+    if (!c || !noise || !out) return fail(WOS_INVALID_ARG, "null argument");
+    TRY(check_dev_geometry(n, n, dx, 1));
+    if (!(width > 0) || !(coherence > 0)) return fail(WOS_INVALID_ARG, "schell: width and coherence must be > 0");
+    if (m <= 0) m = 1;
+    wos_context cc = cci ? *cci : default_context();
+    cc.diagnostics = 0;
+    if (z != 0 && !(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const long long nn = (long long)n * n;
+    TRY(ensure(c->vol, sizeof(double2) * (size_t)nn * m));
+    double2* modes = reinterpret_cast<double2*>(c->vol.p);
+    TRY(schell_generate(c, n, dx, width, coherence, m, noise, true, modes));
+    CK(cudaMemsetAsync(out, 0, sizeof(double) * nn, c->st));
+    const double inv = 1 / (double)m;
+    if (z == 0) {
+        for (int q = 0; q < m; q++) CK(launch_accum_int(1, out, modes + q * nn, 1, nn, inv, c->st));
+        return WOS_OK;
+    }
+    const double* w_d;
+    TRY(cached_params(c, std::vector<double>(m, inv), &w_d));
+    Batch b{n, n, 1, dx, modes, nn, m, nullptr, nullptr, {}, std::vector<double>(m, z), w_d, out, nullptr, cc, nullptr};
+    return run_batch_asm(c, b);
 }
 
 }  // extern "C"

@@ -49,6 +49,7 @@ EXPORTS = [
     "wos_propagate_uniaxial", "wos_propagate_anisotropic",
     "wos_graph_capture_begin", "wos_graph_capture_end", "wos_graph_launch", "wos_graph_destroy",
     "wos_splitstep_adjoint",
+    "wos_polychromatic_dev", "wos_volume_dev", "wos_partially_coherent_dev",
 ]
 
 
@@ -175,6 +176,9 @@ def lib():
             "wos_graph_capture_begin": ([vp], i), "wos_graph_capture_end": ([vp, vp], i),
             "wos_graph_launch": ([vp, vp], i), "wos_graph_destroy": ([vp], i),
             "wos_splitstep_adjoint": ([vp, vp, d, vp, i, vp], i),
+            "wos_polychromatic_dev": ([vp, i, i, d, i, vp, d, vp, vp, i, vp, vp], i),
+            "wos_volume_dev": ([vp, i, i, d, i, vp, vp, i, vp, vp], i),
+            "wos_partially_coherent_dev": ([vp, i, d, d, d, i, vp, d, vp, vp], i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name, None)
@@ -520,6 +524,31 @@ class GPU:
         if ctx is not None:
             ctx.absorb(d)
         return out
+
+    # ---- device-resident batches (device pointers; no diagnostics)
+    def polychromatic_dev(self, ny: int, nx: int, dx: float, ncomp: int, field_ptr: int, z: float, wavelengths,
+                          weights, ctx: Optional[Context], out_ptr: int) -> None:
+        """wos_polychromatic_dev: out (device FP64 [ny][nx]) = sum_k w_k |U_k|^2."""
+        wl = np.ascontiguousarray(wavelengths, dtype=np.float64)
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_polychromatic_dev(self.h, ny, nx, dx, ncomp, C.c_void_p(field_ptr), z, _ptr(wl), _ptr(w),
+                                           wl.size, C.byref(cc) if cc is not None else None, C.c_void_p(out_ptr)))
+
+    def volume_dev(self, ny: int, nx: int, dx: float, ncomp: int, field_ptr: int, zs, ctx: Optional[Context],
+                   out_ptr: int) -> None:
+        """wos_volume_dev: out (device [nz][ncomp][ny][nx], context type)."""
+        zz = np.ascontiguousarray(zs, dtype=np.float64)
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_volume_dev(self.h, ny, nx, dx, ncomp, C.c_void_p(field_ptr), _ptr(zz), zz.size,
+                                    C.byref(cc) if cc is not None else None, C.c_void_p(out_ptr)))
+
+    def partially_coherent_dev(self, n: int, dx: float, width: float, coherence: float, m: int, noise_ptr: int,
+                               z: float, ctx: Optional[Context], out_ptr: int) -> None:
+        """wos_partially_coherent_dev: noise device complex128 [m][n][n]; out device FP64 [n][n]."""
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_partially_coherent_dev(self.h, n, dx, width, coherence, m, C.c_void_p(noise_ptr), z,
+                                                C.byref(cc) if cc is not None else None, C.c_void_p(out_ptr)))
 
     # ---- launch configuration
     def set_fast_path(self, on) -> None:
