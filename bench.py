@@ -263,6 +263,7 @@ def _algorithmic_bytes(name: str, esz: int) -> float:
     return {"cfg1": 48 * 512 ** 2 * k, "cfg2": 2 * 104 * 1.5e6 * k, "cfg3": 803 * 16 * 1024 ** 2 * k,
             "cfg4.1": (32 + 64 * 32) * 1024 ** 2 * k, "cfg4.2": 256 * 56 * 512 ** 2 * k,
             "cfg4.3": 32 * 768 ** 2 * 129 * k, "cfg5": 108 * 2048 ** 2 * k,
+            "cfg4": ((32 + 64 * 32) * 1024 ** 2 + 256 * 56 * 512 ** 2 + 32 * 768 ** 2 * 129) * k,
             # diffractive stack, 3 layers x 200 slices, forward + adjoint: 2 nl (2S + 3)
             # field sweeps (R+W) plus per-layer mask / state / gradient passes and the residual
             "cfg5.2": (2 * 3 * (2 * 200 + 3) * 16 + 3 * 72 + 24) * 2048 ** 2 * k,
@@ -395,6 +396,51 @@ def run_config(args) -> None:
                 t0 = time.perf_counter()
                 O.polychromatic(O.Field(ex.copy(), dx), z, wls[:4], np.ones(4), "asm", O.Context(wavelength=wls[0]))
                 rec_cpu = (time.perf_counter() - t0) * 16  # 4 of 64 wavelengths, scaled
+        elif name == "cfg4":
+            # the three cfg4 parts on device buffers, recorded in one CUDA graph
+            d1, d2, d3 = WL_.cfg4_1(), WL_.cfg4_2(), WL_.cfg4_3()
+            n1, n2, n3 = d1["ex"].shape[0], d2["n"], d3["ex"].shape[0]
+            m2 = d2["noise"].shape[0]
+            dt = torch.complex128 if prec == wos.FP64 else torch.complex64
+            with torch.cuda.stream(stream):
+                f1 = torch.from_numpy(d1["ex"][None]).to(dt).cuda()
+                f3 = torch.from_numpy(d3["ex"][None]).to(dt).cuda()
+                nz = torch.from_numpy(d2["noise"]).cuda()
+                o1 = torch.empty((n1, n1), dtype=torch.float64, device="cuda")
+                o2 = torch.empty((n2, n2), dtype=torch.float64, device="cuda")
+                o3 = torch.empty((d3["zs"].size, 1, n3, n3), dtype=dt, device="cuda")
+            torch.cuda.synchronize()
+
+            def cfg4_run():
+                g.polychromatic_dev(n1, n1, d1["dx"], 1, f1.data_ptr(), d1["z"], d1["wls"], d1["weights"],
+                                    wos.Context(wavelength=d1["wls"][0]), o1.data_ptr())
+                g.partially_coherent_dev(n2, d2["dx"], d2["width"], d2["coherence"], m2, nz.data_ptr(), d2["z"],
+                                         wos.Context(wavelength=d2["wl"]), o2.data_ptr())
+                g.volume_dev(n3, n3, d3["dx"], 1, f3.data_ptr(), d3["zs"], wos.Context(wavelength=d3["wl"]),
+                             o3.data_ptr())
+            rec["device_direct_s"] = timed(cfg4_run, max(2, args.steps // 4), 1)
+            gr = _graph_of(g, cfg4_run)
+            if gr is not None:
+                rec["device_s"] = timed(gr.launch, max(2, args.steps // 4), 1)
+                rec["device_api"] = "wos_polychromatic_dev + wos_partially_coherent_dev + wos_volume_dev, one graph"
+                gr.close()
+            else:
+                rec["device_s"] = rec["device_direct_s"]
+            del nz, o3
+            torch.cuda.empty_cache()
+            if prec == wos.FP64:
+                t0 = time.perf_counter()
+                O.polychromatic(O.Field(d1["ex"].copy(), d1["dx"]), d1["z"], d1["wls"][:4], np.ones(4), "asm",
+                                O.Context(wavelength=d1["wls"][0]))
+                t1 = time.perf_counter()
+                modes = O.schell_realizations(n2, d2["dx"], d2["width"], d2["coherence"], d2["noise"][:8])
+                for k in range(8):
+                    O.propagate(O.Field(modes[k].copy(), d2["dx"]), d2["z"], "asm", O.Context(wavelength=d2["wl"]))
+                t2 = time.perf_counter()
+                O.propagate3d(O.Field(d3["ex"].copy(), d3["dx"]), d3["zs"][:4], "asm", O.Context(wavelength=d3["wl"]))
+                t3 = time.perf_counter()
+                # 4 of 64 wavelengths, 8 of 256 modes, 4 of 128 planes, each scaled
+                rec_cpu = (t1 - t0) * 16 + (t2 - t1) * m2 / 8 + (t3 - t2) * d3["zs"].size / 4
         elif name == "cfg4.2":
             n, dx, z, m = 512, 4e-6, 0.01, 256
             noise = (rng_noise := np.random.default_rng(1)).standard_normal((m, n, n)) / np.sqrt(2) + \
@@ -545,7 +591,7 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--config", default="headline",
-                    help="headline (default) or one of cfg1 cfg2 cfg3 cfg4.1 cfg4.2 cfg4.3 cfg5 cfg5.2 train")
+                    help="headline (default) or one of cfg1 cfg2 cfg3 cfg4 cfg4.1 cfg4.2 cfg4.3 cfg5 cfg5.2 train")
     ap.add_argument("--no-autotune", action="store_true",
                     help="use the default (or WOS_ROWE/WOS_COLE/WOS_COLW) launch configuration")
     args = ap.parse_args()
