@@ -275,6 +275,32 @@ WOS_API int wos_volume_dev(wos_ctx ctx, int ny, int nx, double dx, int ncomp, co
 WOS_API int wos_partially_coherent_dev(wos_ctx ctx, int n, double dx, double width, double coherence, int m,
                                        const void* noise, double z, const wos_context* c, double* out);
 
+/* ---- batches sharded over GPUs (no counterpart in the reference, whose loops
+ *      at optics/polychromatic.go:29-42, optics/coherence.go:110-115 and
+ *      optics/volume.go:10-16 run their units in sequence).  One process or
+ *      thread per GPU, each with its own context; rank 0 makes an id with
+ *      wos_comm_unique_id and hands it to the others out of band, and every
+ *      rank calls wos_comm_init with it (NCCL, loaded at the first call; a
+ *      collective: all ranks must call it).  The sharded calls are
+ *      collectives too: every rank passes the whole unit list and its own
+ *      device buffers, runs the contiguous share wos_shard_range gives it,
+ *      and receives the whole result (an FP64 all-reduce of the intensity, or
+ *      a broadcast of each rank's planes) on the context stream. ---- */
+#define WOS_COMM_ID_BYTES 128
+WOS_API int wos_comm_unique_id(unsigned char* id /* [WOS_COMM_ID_BYTES] */);
+WOS_API int wos_comm_init(wos_ctx ctx, int nranks, int rank, const unsigned char* id);
+WOS_API int wos_comm_destroy(wos_ctx ctx);
+/* Units [*begin, *end) of rank `rank` among nranks: contiguous, the first
+ * units % nranks ranks one unit more (host only, needs no GPU). */
+WOS_API int wos_shard_range(int units, int nranks, int rank, int* begin, int* end);
+WOS_API int wos_polychromatic_sharded_dev(wos_ctx ctx, int ny, int nx, double dx, int ncomp, const void* field,
+                                          double z, const double* wavelengths, const double* weights, int nsamples,
+                                          const wos_context* base, double* out);
+WOS_API int wos_partially_coherent_sharded_dev(wos_ctx ctx, int n, double dx, double width, double coherence, int m,
+                                               const void* noise, double z, const wos_context* c, double* out);
+WOS_API int wos_volume_sharded_dev(wos_ctx ctx, int ny, int nx, double dx, int ncomp, const void* field,
+                                   const double* zs, int nz, const wos_context* c, void* out);
+
 /* ---- thin-element multiply (optics/elements.go:128-141,195-221,288-313,488-532). ---- */
 WOS_API int wos_apply_lens(wos_ctx ctx, wos_field* f, double wavelength, double focal, double aperture,
                    double x0, double y0);

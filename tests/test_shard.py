@@ -98,3 +98,17 @@ def test_sharded_units_match_single_process(tmp_path, world):
         port = s.getsockname()[1]
     mp.spawn(_worker, args=(world, port, str(tmp_path)), nprocs=world, join=True)
     assert all((tmp_path / f"ok{r}").exists() for r in range(world))
+
+
+def test_c_abi_shard_range_matches_the_python_partition():
+    """wos_shard_range (the partition of the C-ABI sharded batches, host only)
+    is the same contiguous split as shard.unit_range, which the gloo tests
+    above run end to end; invalid arguments are rejected."""
+    wos = importlib.import_module("tetsuhiro-wos_b200")
+    for n in range(0, 40):
+        for world in range(1, 9):
+            for r in range(world):
+                assert wos.shard_range(n, world, r) == shard.unit_range(n, r, world)
+    for bad in ((4, 0, 0), (4, 2, 2), (-1, 2, 0), (4, 2, -1)):
+        with pytest.raises(wos.WosError):
+            wos.shard_range(*bad)

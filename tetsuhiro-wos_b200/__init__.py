@@ -6,5 +6,6 @@ reference's Go `optics` API.  Import it with
     importlib.import_module("tetsuhiro-wos_b200")
 """
 from .wosgpu import (EXPORTS, FP32, FP64, GPU, METHODS, WARN_CODES, CContext, CDiag, CField,  # noqa: F401
-                     Context, Field, IndexDesc, WosError, backend_info, device_count, lib, LIB_PATH)
+                     Context, Field, IndexDesc, WosError, backend_info, comm_unique_id, device_count, lib, LIB_PATH,
+                     shard_range)
 from .build import build  # noqa: F401

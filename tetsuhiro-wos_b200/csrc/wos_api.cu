@@ -1256,6 +1256,7 @@ int wos_ctx_create(int device, int precision, wos_ctx* out) {
 
 int wos_ctx_destroy(wos_ctx c) {
     if (!c) return WOS_OK;
+    comm_release(c);
     {
         std::lock_guard<std::mutex> lk(c->mu);
         cudaSetDevice(c->device);

@@ -121,6 +121,9 @@ struct wos_ctx_s {
     static constexpr int kParamSlots = 8;
     ParamSlot pslot[kParamSlots];
     int pslot_next = 0;
+    // communicator of the sharded batches (wos_comm_init): NCCL's ncclComm_t
+    void* comm = nullptr;
+    int comm_size = 1, comm_rank = 0;
     unsigned* err_dev = nullptr;        // error word of the pipelined kernels (device)
     unsigned* err_host = nullptr;       // pinned mirror, read where the host synchronises
     // streams for independent fields of a batch (wos_propagate_batch_dev),
@@ -279,6 +282,10 @@ cudaError_t timed_launch(wos_ctx c, int kind, F&& launch) {
 int fft2d_fp64(wos_ctx c, int n, int batch, double2* a, int inverse);
 int upload_params(wos_ctx c, const std::vector<double>& a, const std::vector<double>& b2,
                   const std::vector<double>& c3, double** pa, double** pb, double** pc);
+int schell_dev_range(wos_ctx c, int n, double dx, double width, double coherence, int m, int m0, int count,
+                     const void* noise, double z, const wos_context* cci, double* out);
+// defined in wos_comm.cu: releases the context's communicator, if any
+void comm_release(wos_ctx c);
 // defined in wos_field_ops.cu
 int element_begin(wos_ctx c, wos_field* f);
 double2* stage_ex(wos_ctx c);

@@ -384,6 +384,40 @@ int check_dev_geometry(int ny, int nx, double dx, int ncomp) {
     return WOS_OK;
 }
 
+// Modes [m0, m0 + count) of an m-mode Gaussian-Schell source (device noise
+// [m][n][n] complex128) propagated to z and averaged with weight 1/m into out
+// (device FP64 [n][n], overwritten): the whole source when m0 = 0 and count =
+// m, one rank's share of a sharded run otherwise.
+int schell_dev_range(wos_ctx c, int n, double dx, double width, double coherence, int m, int m0, int count,
+                     const void* noise, double z, const wos_context* cci, double* out) {
+    if (!c || !noise || !out) return fail(WOS_INVALID_ARG, "null argument");
+    TRY(check_dev_geometry(n, n, dx, 1));
+    if (!(width > 0) || !(coherence > 0)) return fail(WOS_INVALID_ARG, "schell: width and coherence must be > 0");
+    if (m0 < 0 || count < 0 || m0 + count > m) return fail(WOS_INVALID_ARG, "schell: mode range outside the source");
+    wos_context cc = cci ? *cci : default_context();
+    cc.diagnostics = 0;
+    if (z != 0 && !(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    const long long nn = (long long)n * n;
+    CK(cudaMemsetAsync(out, 0, sizeof(double) * nn, c->st));
+    if (count == 0) return WOS_OK;
+    TRY(ensure(c->vol, sizeof(double2) * (size_t)nn * count));
+    double2* modes = reinterpret_cast<double2*>(c->vol.p);
+    TRY(schell_generate(c, n, dx, width, coherence, count, reinterpret_cast<const double2*>(noise) + m0 * nn, true,
+                        modes));
+    const double inv = 1 / (double)m;
+    if (z == 0) {
+        for (int q = 0; q < count; q++) CK(launch_accum_int(1, out, modes + q * nn, 1, nn, inv, c->st));
+        return WOS_OK;
+    }
+    const double* w_d;
+    TRY(cached_params(c, std::vector<double>(count, inv), &w_d));
+    Batch b{n, n, 1, dx, modes, nn, count, nullptr, nullptr, {}, std::vector<double>(count, z), w_d, out, nullptr, cc,
+            nullptr};
+    return run_batch_asm(c, b);
+}
+
 int upload_params(wos_ctx c, const std::vector<double>& a, const std::vector<double>& b2,
                   const std::vector<double>& c3, double** pa, double** pb, double** pc) {
     const size_t n = a.size() + b2.size() + c3.size();
@@ -659,29 +693,8 @@ int wos_volume_dev(wos_ctx c, int ny, int nx, double dx, int ncomp, const void* 
 
 int wos_partially_coherent_dev(wos_ctx c, int n, double dx, double width, double coherence, int m, const void* noise,
                                double z, const wos_context* cci, double* out) {
-    if (!c || !noise || !out) return fail(WOS_INVALID_ARG, "null argument");
-    TRY(check_dev_geometry(n, n, dx, 1));
-    if (!(width > 0) || !(coherence > 0)) return fail(WOS_INVALID_ARG, "schell: width and coherence must be > 0");
     if (m <= 0) m = 1;
-    wos_context cc = cci ? *cci : default_context();
-    cc.diagnostics = 0;
-    if (z != 0 && !(cc.wavelength > 0)) return fail(WOS_INVALID_ARG, "wavelength must be > 0");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const long long nn = (long long)n * n;
-    TRY(ensure(c->vol, sizeof(double2) * (size_t)nn * m));
-    double2* modes = reinterpret_cast<double2*>(c->vol.p);
-    TRY(schell_generate(c, n, dx, width, coherence, m, noise, true, modes));
-    CK(cudaMemsetAsync(out, 0, sizeof(double) * nn, c->st));
-    const double inv = 1 / (double)m;
-    if (z == 0) {
-        for (int q = 0; q < m; q++) CK(launch_accum_int(1, out, modes + q * nn, 1, nn, inv, c->st));
-        return WOS_OK;
-    }
-    const double* w_d;
-    TRY(cached_params(c, std::vector<double>(m, inv), &w_d));
-    Batch b{n, n, 1, dx, modes, nn, m, nullptr, nullptr, {}, std::vector<double>(m, z), w_d, out, nullptr, cc, nullptr};
-    return run_batch_asm(c, b);
+    return schell_dev_range(c, n, dx, width, coherence, m, 0, m, noise, z, cci, out);
 }
 
 }  // extern "C"

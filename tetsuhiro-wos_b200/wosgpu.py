@@ -50,6 +50,8 @@ EXPORTS = [
     "wos_graph_capture_begin", "wos_graph_capture_end", "wos_graph_launch", "wos_graph_destroy",
     "wos_splitstep_adjoint",
     "wos_polychromatic_dev", "wos_volume_dev", "wos_partially_coherent_dev",
+    "wos_comm_unique_id", "wos_comm_init", "wos_comm_destroy", "wos_shard_range",
+    "wos_polychromatic_sharded_dev", "wos_partially_coherent_sharded_dev", "wos_volume_sharded_dev",
 ]
 
 
@@ -179,6 +181,11 @@ def lib():
             "wos_polychromatic_dev": ([vp, i, i, d, i, vp, d, vp, vp, i, vp, vp], i),
             "wos_volume_dev": ([vp, i, i, d, i, vp, vp, i, vp, vp], i),
             "wos_partially_coherent_dev": ([vp, i, d, d, d, i, vp, d, vp, vp], i),
+            "wos_comm_unique_id": ([vp], i), "wos_comm_init": ([vp, i, i, vp], i), "wos_comm_destroy": ([vp], i),
+            "wos_shard_range": ([i, i, i, P(i), P(i)], i),
+            "wos_polychromatic_sharded_dev": ([vp, i, i, d, i, vp, d, vp, vp, i, vp, vp], i),
+            "wos_partially_coherent_sharded_dev": ([vp, i, d, d, d, i, vp, d, vp, vp], i),
+            "wos_volume_sharded_dev": ([vp, i, i, d, i, vp, vp, i, vp, vp], i),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name, None)
@@ -211,6 +218,20 @@ def _out_array(out, shape, dtype):
 
 def device_count() -> int:
     return lib().wos_device_count()
+
+
+def comm_unique_id() -> bytes:
+    """wos_comm_unique_id: the id rank 0 shares with the other ranks."""
+    buf = (C.c_ubyte * 128)()
+    _check(lib().wos_comm_unique_id(buf))
+    return bytes(buf)
+
+
+def shard_range(units: int, nranks: int, rank: int) -> Tuple[int, int]:
+    """wos_shard_range: the contiguous units [begin, end) of one rank (host only)."""
+    b, e = C.c_int(), C.c_int()
+    _check(lib().wos_shard_range(units, nranks, rank, C.byref(b), C.byref(e)))
+    return b.value, e.value
 
 
 def backend_info() -> str:
@@ -549,6 +570,34 @@ class GPU:
         cc = ctx.c() if ctx is not None else None
         _check(lib().wos_partially_coherent_dev(self.h, n, dx, width, coherence, m, C.c_void_p(noise_ptr), z,
                                                 C.byref(cc) if cc is not None else None, C.c_void_p(out_ptr)))
+
+    # ---- batches sharded over GPUs (collectives over the context's communicator)
+    def comm_init(self, nranks: int, rank: int, uid: bytes) -> None:
+        """wos_comm_init with the id from comm_unique_id() on rank 0."""
+        buf = (C.c_ubyte * 128).from_buffer_copy(uid)
+        _check(lib().wos_comm_init(self.h, nranks, rank, buf))
+
+    def comm_destroy(self) -> None:
+        _check(lib().wos_comm_destroy(self.h))
+
+    def polychromatic_sharded_dev(self, ny, nx, dx, ncomp, field_ptr, z, wavelengths, weights, ctx, out_ptr):
+        wl = np.ascontiguousarray(wavelengths, dtype=np.float64)
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_polychromatic_sharded_dev(self.h, ny, nx, dx, ncomp, C.c_void_p(field_ptr), z, _ptr(wl),
+                                                   _ptr(w), wl.size, C.byref(cc) if cc is not None else None,
+                                                   C.c_void_p(out_ptr)))
+
+    def partially_coherent_sharded_dev(self, n, dx, width, coherence, m, noise_ptr, z, ctx, out_ptr):
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_partially_coherent_sharded_dev(self.h, n, dx, width, coherence, m, C.c_void_p(noise_ptr), z,
+                                                        C.byref(cc) if cc is not None else None, C.c_void_p(out_ptr)))
+
+    def volume_sharded_dev(self, ny, nx, dx, ncomp, field_ptr, zs, ctx, out_ptr):
+        zz = np.ascontiguousarray(zs, dtype=np.float64)
+        cc = ctx.c() if ctx is not None else None
+        _check(lib().wos_volume_sharded_dev(self.h, ny, nx, dx, ncomp, C.c_void_p(field_ptr), _ptr(zz), zz.size,
+                                            C.byref(cc) if cc is not None else None, C.c_void_p(out_ptr)))
 
     # ---- launch configuration
     def set_fast_path(self, on) -> None:
