@@ -467,13 +467,19 @@ int fast_tw_lo(wos_ctx c, Axis* a, int E, const void** out) {
 }
 
 // Transfer-function table of a complex64 column sweep (FastCols::htab) for
-// columns of L points, when the sweep can use one: no loss sums, one
-// wavelength and distance, W columns per CTA dividing ncols / 2, and the table
-// rows fitting beside the tile in shared memory.  Sets k.htab / k.htab_ld
-// (left null otherwise); the entries are hi + lo pairs when the sweep runs the
-// compensated transforms (k.tw_lo set).
+// columns of L points, when the sweep can use one: the split-step's column
+// sweeps (precise phase), no loss sums, one wavelength and distance, W
+// columns per CTA dividing ncols / 2, and the table rows fitting beside the
+// tile in shared memory.  Sets k.htab / k.htab_ld (left null otherwise); the
+// entries are hi + lo pairs when the sweep runs the compensated transforms
+// (k.tw_lo set).  Measured: the split-step's plain complex64 run 9.87 ->
+// 8.60 ms (1024^2, 400 slices; its H takes sin/cos to ~1 ulp); the 2048^2
+// ASM column sweep unchanged at 35.1 us, its evaluation of H running under
+// the sweep's memory latency, while the 33 KB of table rows per CTA took the
+// shared memory that the other stream's row sweeps overlap in (two-stream
+// batch 20.4k -> 17.1k props/s), so the plain ASM does not use it.
 int attach_htab(wos_ctx c, FastCols& k, int L, int E) {
-    if (c->fp64 || !c->htab_on || k.red || k.batch_wl || k.batch_z || L < 32) return WOS_OK;
+    if (c->fp64 || !c->htab_on || !k.precise_phase || k.red || k.batch_wl || k.batch_z || L < 32) return WOS_OK;
     const int W = fast_col_width(0, L, E, k.tiled ? kTileW : k.W);
     const int ld = htab_ld_for(L);
     if (W < 1 || k.ncols < 2 * W || k.ncols % (2 * W) != 0) return WOS_OK;
@@ -646,7 +652,6 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
         k.hist = red_region(c, 1) + RS_HIST;
         k.hist_dx = p.dx;
     }
-    TRY(attach_htab(c, k, p.ny, t.colE));
     CK(timed_launch(c, 4, [&] { return sweep_cols(c, p.ny, t.colE, k, &nb); }));
     if (s.red_loss) CK(launch_reduce_finish(red_region(c, 1), nb, 1, RS_SW, 2, redout_region(c, 1), c->st));
     if (s.hist) CK(launch_reduce_finish(red_region(c, 1), nb, 1, RS_HIST, 97, redout_region(c, 1), c->st));
@@ -1492,13 +1497,6 @@ int wos_propagate_batch_dev(wos_ctx c, int nfields, int ny, int nx, double dx, i
                 const void *th, *tp;
                 if (!pair_tables(c, ny, t.colE, &th, &tp)) return fail(WOS_CUDA_ERROR, "split-tile tables");
             }
-            // the transfer-function table the fields' column sweeps will look up
-            FastCols hk{};
-            hk.ncols = nx;
-            hk.W = t.colW;
-            hk.tiled = asm_tiled(c, ny, nx, t);
-            fill_asm_h(hk, asm_h(c, cc, z, ev_policy(cc, z), dx, nx, ny));
-            TRY(attach_htab(c, hk, ny, t.colE));
             nstreams = std::max(1, std::min(wos_ctx_s::kMaxAux, env_int("WOS_STREAMS", 2)));
         }
     }
