@@ -1266,6 +1266,11 @@ int wos_ctx_destroy(wos_ctx c) {
         std::lock_guard<std::mutex> lk(c->mu);
         cudaSetDevice(c->device);
         cudaStreamSynchronize(c->st);
+        if (c->pipe_made) {
+            cudaStreamSynchronize(c->h2d);
+            cudaStreamSynchronize(c->d2h);
+        }
+        host_release(c);
         for (int pr = 0; pr < 2; pr++)
             for (auto& kv : c->axes[pr]) {
                 cudaFree(kv.second.tw);
@@ -1559,6 +1564,51 @@ int wos_propagate_batch(wos_ctx c, int nfields, wos_field* fields, double z, int
         }
         c->pipe_made = true;
     }
+    bool staged = false;
+    for (int i = 0; i < nfields; i++)
+        staged = staged || host_pageable(fields[i].ex) || (fields[i].polarized && host_pageable(fields[i].ey));
+    if (staged) {
+        // pageable fields: host threads convert field i into the slot's
+        // page-locked staging (context precision), then copy, sweep and copy
+        // back; field i - kSlots is converted back when its slot comes round,
+        // so the host converts while the GPU runs the fields before it
+        const size_t esz = c->csz();
+        auto drain = [&](int j) -> int {
+            const int sl = j % wos_ctx_s::kSlots;
+            CK(cudaEventSynchronize(c->free_ev[sl]));
+            host_convert(c, fields[j], c->hst[sl], true);
+            return WOS_OK;
+        };
+        int rc = WOS_OK;
+        for (int i = 0; i < nfields && rc == WOS_OK; i++) {
+            const int sl = i % wos_ctx_s::kSlots;
+            if (i >= wos_ctx_s::kSlots && (rc = drain(i - wos_ctx_s::kSlots)) != WOS_OK) break;
+            wos_field& f = fields[i];
+            const int ncomp = f.polarized ? 2 : 1;
+            const size_t bytes = (size_t)f.ny * f.nx * ncomp * esz;
+            if ((rc = host_stage(c, sl, bytes)) != WOS_OK || (rc = ensure(c->slot[sl], bytes)) != WOS_OK) break;
+            host_convert(c, f, c->hst[sl], false);
+            CK(cudaMemcpyAsync(c->slot[sl].p, c->hst[sl], bytes, cudaMemcpyHostToDevice, c->h2d));
+            CK(cudaEventRecord(c->in_ev[sl], c->h2d));
+            CK(cudaStreamWaitEvent(c->st, c->in_ev[sl], 0));
+            wos_diag local;
+            wos_diag* d = diags ? &diags[i] : (method == WOS_FRAUNHOFER ? &local : nullptr);
+            Prop p{f.ny, f.nx, f.dx, ncomp, c->slot[sl].p, 0, c->slot[sl].p, 0, z, method, cc, d};
+            if ((rc = run_propagate(c, p)) != WOS_OK) break;
+            if (method == WOS_FRAUNHOFER) f.dx = d->dx_out;
+            CK(cudaEventRecord(c->done_ev[sl], c->st));
+            CK(cudaStreamWaitEvent(c->d2h, c->done_ev[sl], 0));
+            CK(cudaMemcpyAsync(c->hst[sl], c->slot[sl].p, bytes, cudaMemcpyDeviceToHost, c->d2h));
+            CK(cudaEventRecord(c->free_ev[sl], c->d2h));
+        }
+        for (int j = std::max(0, nfields - wos_ctx_s::kSlots); j < nfields && rc == WOS_OK; j++) rc = drain(j);
+        cudaStreamSynchronize(c->h2d);
+        cudaStreamSynchronize(c->d2h);
+        CK(cudaMemcpyAsync(c->err_host, c->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        if (rc != WOS_OK) return rc;
+        return check_err_word(c);
+    }
     // field i lives in slot i % kSlots from its upload to its download; the
     // upload of the next field is queued before field i's sweeps, so the two
     // copy directions and the sweeps overlap (the sweeps stay in order on the
@@ -1623,6 +1673,9 @@ int wos_propagate(wos_ctx c, wos_field* f, double z, int method, const wos_conte
         }
         return WOS_OK;
     }
+    // a pageable field goes through the host batch's page-locked staging
+    if (host_pageable(f->ex) || (f->polarized && host_pageable(f->ey)))
+        return wos_propagate_batch(c, 1, f, z, method, cc, diag);
     std::lock_guard<std::mutex> lk(c->mu);
     TRY(set_device(c));
     const int ncomp = f->polarized ? 2 : 1;

@@ -139,6 +139,11 @@ struct wos_ctx_s {
     static constexpr int kSlots = 3;
     cudaStream_t h2d = nullptr, d2h = nullptr;
     DevBuf slot[kSlots];
+    // page-locked host staging of the batch slots for pageable fields, and
+    // the host threads that convert into and out of it (wos_host.cu)
+    void* hst[kSlots] = {};
+    size_t hst_n[kSlots] = {};
+    void* host_pool = nullptr;
     cudaEvent_t in_ev[kSlots] = {}, done_ev[kSlots] = {}, free_ev[kSlots] = {};
     bool pipe_made = false;
     std::map<long long, Tune> tune;     // autotuned launch configurations
@@ -286,6 +291,11 @@ int schell_dev_range(wos_ctx c, int n, double dx, double width, double coherence
                      const void* noise, double z, const wos_context* cci, double* out);
 // defined in wos_comm.cu: releases the context's communicator, if any
 void comm_release(wos_ctx c);
+// defined in wos_host.cu: staging of pageable host fields
+bool host_pageable(const void* p);
+int host_stage(wos_ctx c, int slot, size_t bytes);
+void host_convert(wos_ctx c, wos_field& f, void* dst, bool to_host);
+void host_release(wos_ctx c);
 // defined in wos_field_ops.cu
 int element_begin(wos_ctx c, wos_field* f);
 double2* stage_ex(wos_ctx c);
