@@ -30,7 +30,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from gpu_util import TOL_FP32, TOL_FP64, TOL_FP64_SCHELL, rel_l2, tol_case, wos
+from gpu_util import TOL_FP32, TOL_FP64, TOL_FP64_SCHELL, rel_l2, tol_case, tol_fp32_splitstep, wos
 
 W = importlib.import_module("tetsuhiro-wos_b200.workloads")
 
@@ -186,10 +186,11 @@ def test_cfg3_bpm_400_slices_matches_oracle(prec, cfg3_ref):
         buf = to_dev(d["ex"], prec)
         g.split_step_dev(n, n, d["dx"], 1, buf.data_ptr(), d["z"], desc, d["steps"],
                          wos.Context(wavelength=d["wl"], warnings_enabled=False))
-        record("cfg3 device", prec, rel_l2(from_dev(g, buf), ref), TOL_FP64 if prec == wos.FP64 else TOL_FP32)
+        bound = TOL_FP64 if prec == wos.FP64 else tol_fp32_splitstep(d["steps"])
+        record("cfg3 device", prec, rel_l2(from_dev(g, buf), ref), bound)
         f = wos.Field(d["ex"].copy(), d["dx"])
         g.split_step(f, d["z"], desc, d["steps"], wos.Context(wavelength=d["wl"]))
-        record("cfg3 host", prec, rel_l2(f.ex, ref), TOL_FP64 if prec == wos.FP64 else TOL_FP32)
+        record("cfg3 host", prec, rel_l2(f.ex, ref), bound)
 
 
 # ------------------------------------------------------------------ cfg4
@@ -441,7 +442,8 @@ def test_cfg5_2_stack_gradient_matches_fp64_adjoint_and_fd(prec, cfg5_2_ref):
         grads = gd.cpu().numpy()
     fp64 = prec == wos.FP64
     if not fp64:
-        record("cfg5.2 loss vs FP64 GPU", prec, abs(loss - loss64) / loss64, 1e-5)
+        # 600 slices; the loss (|u|^2 - T)^2 doubles the relative field error
+        record("cfg5.2 loss vs FP64 GPU", prec, abs(loss - loss64) / loss64, 2 * tol_fp32_splitstep(600))
         record("cfg5.2 grads vs FP64 GPU adjoint", prec, rel_l2(grads, grads64), 1e-4)
     fdv = np.array([v for _, v in fd])
     gv = np.array([grads[p] for p, _ in fd])
