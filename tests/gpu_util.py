@@ -1,5 +1,7 @@
 """Helpers shared by the GPU tests: the package under test and the oracle."""
 import importlib
+import json
+import os
 
 import numpy as np
 
@@ -33,6 +35,15 @@ TOL_FP64_SCHELL = 1e-7
 # 5e-8 per slice.
 def tol_fp32_splitstep(slices: int) -> float:
     return max(TOL_FP32, 5e-8 * slices)
+
+
+def log_parity(case: str, precision, err: float, bound: float, **extra) -> None:
+    """Append one measured error to the file named by WOS_PARITY_LOG (if set)."""
+    path = os.environ.get("WOS_PARITY_LOG")
+    if path:
+        with open(path, "a") as fh:
+            fh.write(json.dumps(dict(case=case, precision="fp64" if precision == wos.FP64 else "fp32",
+                                     rel_l2=err, bound=bound, **extra)) + "\n")
 
 
 def rel_l2(a, b) -> float:

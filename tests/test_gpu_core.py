@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from gpu_util import TOL_FP32, TOL_FP64, rel_l2, tol, tol_case, wos
+from gpu_util import TOL_FP32, TOL_FP64, log_parity, rel_l2, tol, tol_case, wos
 from wos_testutil import (SimpleRNG, analytic_gaussian_fresnel, centroid_x, ref_field,
                           single_bin_plane_wave)
 
@@ -156,6 +156,7 @@ def test_propagate_matches_oracle(gpu, method, case, polarized):
     gpu.propagate(gf, z, method, gc)
     t = tol_case(gpu.precision, method, ny, nx)
     err = rel_l2(gf.ex, of.ex)
+    log_parity(f"propagate {method} {ny}x{nx} {kind}{' pol' if polarized else ''}", gpu.precision, err, t)
     assert err <= t, (err, gc.warnings, oc.warnings)
     if polarized:
         assert rel_l2(gf.ey, of.ey) <= t
@@ -285,3 +286,24 @@ def test_fft1d_line_beyond_one_cta_is_unsupported(gpu):
     with pytest.raises(wos.WosError) as e:
         gpu.fft1d(np.ones(4500, complex))
     assert e.value.status == 2
+
+
+@pytest.mark.parametrize("n", [100, 768, 1000, 1500, 2000, 3000, 2049])
+def test_fp64_lines_are_closer_to_the_exact_dft_than_the_reference(n):
+    """The complex128 transforms of lengths that are not powers of two against
+    the exact DFT (numpy's pocketfft, double precision), beside the oracle,
+    which restates the reference's Bluestein transform (optics/fft.go:159-204):
+    the reference forms the chirp angle pi k^2 / n without reducing k^2 mod
+    2n, so its error grows with n (~1.7e-16 n), while these lines reduce the
+    angle exactly (mixed radix 2/3/5 below 8192 points, else Bluestein).  This
+    is the floor that the FP64 parity of non-power-of-two grids sits on."""
+    rng = np.random.default_rng(n)
+    a = rng.normal(size=n) + 1j * rng.normal(size=n)
+    exact = np.fft.fft(a)
+    with wos.GPU(wos.FP64) as g:
+        got = g.fft1d(a.copy())
+    ref = O.fft1d(a)
+    e_gpu, e_ref = rel_l2(got, exact), rel_l2(ref, exact)
+    log_parity(f"fft1d {n} vs exact DFT", wos.FP64, e_gpu, 1e-14, reference_vs_exact=e_ref)
+    assert e_gpu <= 1e-14
+    assert e_gpu <= e_ref
