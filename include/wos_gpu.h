@@ -217,7 +217,10 @@ WOS_API int wos_propagate_batch_dev(wos_ctx ctx, int nfields, int ny, int nx, do
                                     const void* const* in, void* const* out, double z, int method,
                                     const wos_context* c);
 
-/* ---- PropagateSplitStep (optics/medium.go:22-45) with a parametric medium. ---- */
+/* ---- PropagateSplitStep (optics/medium.go:22-45) with a parametric medium.
+ *      diag receives the powers and warnings only when c->diagnostics is set
+ *      (a Context with Warnings); otherwise it is zeroed apart from dx_out and
+ *      the slices take the specialised power-of-two sweeps where they apply. ---- */
 WOS_API int wos_splitstep(wos_ctx ctx, wos_field* f, double z, const wos_index_desc* n, int steps,
                   const wos_context* c, wos_diag* diag);
 WOS_API int wos_splitstep_dev(wos_ctx ctx, int ny, int nx, double dx, int ncomp, void* field, double z,

@@ -92,6 +92,7 @@ def lib():
         L.or_spectral_radius.argtypes = [vp, d]; L.or_spectral_radius.restype = d
         L.or_spectral_centroid.argtypes = [vp, vp, vp]
         L.or_propagate.argtypes = [vp, d, i, vp]; L.or_propagate.restype = i
+        L.or_propagate_shift_at.argtypes = [vp, d, i, vp, d, d]; L.or_propagate_shift_at.restype = i
         L.or_propagate1d.argtypes = [vp, i, d, d, d, vp]
         L.or_propagate_vectorial.argtypes = [vp, vp, d, vp]
         L.or_propagate_uniaxial.argtypes = [vp, d, d, d, vp]
@@ -228,6 +229,20 @@ def propagate(f: Field, z: float, method: str, ctx: Optional[Context]) -> None:
     f._sync(cf)
     if rc != 0:
         raise ValueError(f"oracle propagate failed rc={rc}")
+
+
+def propagate_shift_at(f: Field, z: float, method: str, ctx: Optional[Context], fxc: float, fyc: float) -> None:
+    """propASMShift / propASMShiftPad (propagate.go:426-504) with the spectral
+    centroid supplied instead of summed, in place."""
+    cf = f._c()
+    cc = ctx._to_c() if ctx is not None else None
+    rc = lib().or_propagate_shift_at(C.byref(cf), z, METHODS[method], C.byref(cc) if cc is not None else None,
+                                     fxc, fyc)
+    if ctx is not None:
+        ctx._from_c(cc)
+    f._sync(cf)
+    if rc != 0:
+        raise ValueError(f"oracle propagate_shift_at failed rc={rc}")
 
 
 def propagate1d(a: np.ndarray, dx: float, z: float, wl: float, ctx: Optional[Context]) -> np.ndarray:

@@ -516,10 +516,8 @@ static void shift_ramp(or_field *f, oc128 *a, double sgn, double fxc, double fyc
     }
 }
 
-/* propASMShift (propagate.go:426-471) */
-static void prop_asm_shift(or_field *f, double z, or_context *ctx) {
-    double fxc, fyc;
-    or_spectral_centroid(f, &fxc, &fyc);
+/* propASMShift (propagate.go:426-471) after its spectralCentroid call */
+static void prop_asm_shift_at(or_field *f, double z, or_context *ctx, double fxc, double fyc) {
     double fbx = 1 / ((double)f->nx * f->dx), fby = 1 / ((double)f->ny * f->dx);
     if (fabs(fxc) < 0.5 * fbx && fabs(fyc) < 0.5 * fby) { prop_asm(f, z, ctx); return; }
     tf_spec t = {0};
@@ -536,10 +534,8 @@ static void prop_asm_shift(or_field *f, double z, or_context *ctx) {
     asm_warn(z, ctx, pin, pout, t.zero, t.reg);
 }
 
-/* propASMShiftPad (propagate.go:479-504) */
-static void prop_asm_shift_pad(or_field *f, double z, or_context *ctx) {
-    double fxc, fyc;
-    or_spectral_centroid(f, &fxc, &fyc);
+/* propASMShiftPad (propagate.go:479-504) after its spectralCentroid call */
+static void prop_asm_shift_pad_at(or_field *f, double z, or_context *ctx, double fxc, double fyc) {
     double fbx = 1 / ((double)f->nx * f->dx), fby = 1 / ((double)f->ny * f->dx);
     if (fabs(fxc) < 0.5 * fbx && fabs(fyc) < 0.5 * fby) { prop_asm_pad_core(f, z, ctx, 0, 0); return; }
     shift_ramp(f, f->ex, -1, fxc, fyc);
@@ -547,6 +543,34 @@ static void prop_asm_shift_pad(or_field *f, double z, or_context *ctx) {
     prop_asm_pad_core(f, z, ctx, fxc, fyc);
     shift_ramp(f, f->ex, +1, fxc, fyc);
     if (f->polarized) shift_ramp(f, f->ey, +1, fxc, fyc);
+}
+
+static void prop_asm_shift(or_field *f, double z, or_context *ctx) {
+    double fxc, fyc;
+    or_spectral_centroid(f, &fxc, &fyc);
+    prop_asm_shift_at(f, z, ctx, fxc, fyc);
+}
+
+static void prop_asm_shift_pad(or_field *f, double z, or_context *ctx) {
+    double fxc, fyc;
+    or_spectral_centroid(f, &fxc, &fyc);
+    prop_asm_shift_pad_at(f, z, ctx, fxc, fyc);
+}
+
+/* The carrier-shift methods with the centroid supplied by the caller (a test
+ * hook: it separates the rounding of the centroid's sequential sums from the
+ * rest of the propagation). */
+int or_propagate_shift_at(or_field *f, double z, int method, or_context *ctx, double fxc, double fyc) {
+    if (z == 0) return 0;
+    or_context local;
+    if (!ctx) {
+        memset(&local, 0, sizeof(local));
+        ctx = &local;
+    }
+    if (method == OR_ASM_SHIFT) prop_asm_shift_at(f, z, ctx, fxc, fyc);
+    else if (method == OR_ASM_SHIFT_PAD) prop_asm_shift_pad_at(f, z, ctx, fxc, fyc);
+    else return -1;
+    return 0;
 }
 
 /* propFresnelTF (propagate.go:507-519); alias bound uses min(nx,ny) */

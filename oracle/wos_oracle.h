@@ -100,6 +100,7 @@ void or_shift_field(or_field *f, double du, double dv);    /* field.go:199-228 *
 
 /* ---- propagation (optics/propagate.go) ---- */
 int or_propagate(or_field *f, double z, int method, or_context *ctx); /* propagate.go:65-102 */
+int or_propagate_shift_at(or_field *f, double z, int method, or_context *ctx, double fxc, double fyc);
 int or_propagate1d(oc128 *a, int n, double dx, double z, double wl, or_context *ctx); /* :718-738 */
 /* PropagateVectorial (vectorial.go:14-80): ex and ey (both used whatever
  * f->polarized, as the reference uses f.Ey) propagate in place, ez_out

@@ -438,8 +438,9 @@ int wos_splitstep(wos_ctx c, wos_field* f, double z, const wos_index_desc* n, in
     ScreenSrc src;
     src.kind = 1;
     src.desc = *n;
-    TRY(run_splitstep(c, f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, c->stage.p, 1, z, src, steps,
-                      cc ? *cc : default_context(), diag));
+    const wos_context ctx = cc ? *cc : default_context();
+    TRY(run_splitstep(c, f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, c->stage.p, 1, z, src, steps, ctx,
+                      ctx.diagnostics ? diag : nullptr));
     return stage_out(c, f, ncomp);
 }
 
@@ -451,7 +452,13 @@ int wos_splitstep_dev(wos_ctx c, int ny, int nx, double dx, int ncomp, void* fie
     ScreenSrc src;
     src.kind = 1;
     src.desc = *n;
-    return run_splitstep(c, ny, nx, dx, ncomp, field, 0, field, 0, z, src, steps, cc ? *cc : default_context(), diag);
+    const wos_context ctx = cc ? *cc : default_context();
+    if (diag && !ctx.diagnostics) {
+        std::memset(diag, 0, sizeof(*diag));
+        diag->dx_out = dx;
+        diag = nullptr;
+    }
+    return run_splitstep(c, ny, nx, dx, ncomp, field, 0, field, 0, z, src, steps, ctx, diag);
 }
 
 int wos_splitstep_maps(wos_ctx c, wos_field* f, double z, const double* n_re, const double* n_im, int nmaps,
@@ -480,8 +487,9 @@ int wos_splitstep_maps(wos_ctx c, wos_field* f, double z, const double* n_re, co
     src.nre = re;
     src.nim = im;
     src.nmaps = nmaps;
-    TRY(run_splitstep(c, f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, c->stage.p, 1, z, src, st,
-                      cc ? *cc : default_context(), diag));
+    const wos_context ctx = cc ? *cc : default_context();
+    TRY(run_splitstep(c, f->ny, f->nx, f->dx, ncomp, c->stage.p, 1, c->stage.p, 1, z, src, st, ctx,
+                      ctx.diagnostics ? diag : nullptr));
     return stage_out(c, f, ncomp);
 }
 
