@@ -118,3 +118,32 @@ def test_noalloc_in_place_and_smallest_grids():
         o = O.Field(ex.astype(np.complex128), dx)
         O.propagate(o, z, "asm_pad", O.Context(wavelength=wl, warnings_enabled=False))
         assert rel_l2(got, o.ex) <= TOL_FP32, ((ny, nx), rel_l2(got, o.ex))
+
+
+def test_noalloc_calls_leave_device_memory_unchanged():
+    """After one call per grid size (which loads the module and fills the
+    twiddles), further calls on every size take no device memory: the free
+    memory the driver reports is the same before and after them.  Measured
+    twice if the first reading differs, in case another process on the GPU
+    moved it."""
+    import torch
+    dx, wl, z = 1e-6, 5e-7, 2e-5
+    sizes = ((4, 4), (64, 128), (1024, 1024), (512, 256))
+    bufs = {s: (torch.zeros(s, dtype=torch.complex64, device="cuda"),
+                torch.zeros(s, dtype=torch.complex64, device="cuda")) for s in sizes}
+    for (ny, nx), (a, b) in bufs.items():
+        assert _noalloc(a.data_ptr(), b.data_ptr(), ny, nx, dx, z, wl, 0) == 0, wos.lib().wos_last_error()
+    torch.cuda.synchronize()
+
+    def free_change():
+        before = torch.cuda.mem_get_info()[0]
+        for _ in range(4):
+            for (ny, nx), (a, b) in bufs.items():
+                assert _noalloc(a.data_ptr(), b.data_ptr(), ny, nx, dx, z, wl, 0) == 0
+        torch.cuda.synchronize()
+        return before - torch.cuda.mem_get_info()[0]
+
+    d = free_change()
+    if d != 0:
+        d = free_change()
+    assert d == 0, d

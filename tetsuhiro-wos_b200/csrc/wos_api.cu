@@ -405,7 +405,10 @@ int spectrum_stats(wos_ctx c, const Prop& p, void* dst, bool centroid, bool hist
     a.batch = p.ncomp;
     CK(prof_cols(c, c->fp64, a));
     const int nb = (int)nbc;
-    if (centroid) CK(launch_reduce_finish(a.red, nb, 1, RS_SW, 3, redout_region(c, region), c->st));
+    if (centroid) {
+        CK(launch_reduce_finish(a.red, nb, 1, RS_SW, 3, redout_region(c, region), c->st));
+        CK(launch_reduce_finish(a.red, nb, 1, RS_SLO, 3, redout_region(c, region), c->st));
+    }
     if (hist) CK(launch_reduce_finish(a.red, nb, 1, RS_HIST, 97, redout_region(c, region), c->st));
     if (blocks_out) *blocks_out = nb;
     return WOS_OK;
@@ -837,11 +840,15 @@ int run_propagate(wos_ctx c, const Prop& p0) {
             const bool hist_here = wrap && p.method == WOS_ASM_SHIFT;
             TRY(spectrum_stats(c, p, c->scratch2.p, true, hist_here, 0, 0, 0, 3, nullptr));
             TRY(fetch_red(c, 4));
+            // compensated sums: the centroid is exact to the last bits (the
+            // reference accumulates it in sequence, whose rounding the
+            // carrier-shift output amplifies ~1e4-fold)
             const double* rr = c->hred + RS_COUNT * 3;
+            const double sw = rr[RS_SW] + rr[RS_SLO];
             double fxc = 0, fyc = 0;
-            if (rr[RS_SW] > 0) {
-                fxc = rr[RS_SFX] / rr[RS_SW];
-                fyc = rr[RS_SFY] / rr[RS_SW];
+            if (sw > 0) {
+                fxc = (rr[RS_SFX] + rr[RS_SLO + 1]) / sw;
+                fyc = (rr[RS_SFY] + rr[RS_SLO + 2]) / sw;
             }
             if (d) {
                 d->centroid_fx = fxc;

@@ -81,13 +81,6 @@ __global__ void k_bhat_finish(C* df, C* di, const double2* bf, const double2* bi
 // batch blockIdx.x.  Each thread keeps a Neumaier pair (sum, compensation)
 // over a fixed stride of records; the pairs are combined in a fixed tree, so
 // the result is deterministic and carries the compensation of every term.
-__device__ __forceinline__ void neumaier_add(double& s, double& c, double x) {
-    const double t = s + x;
-    if (fabs(s) >= fabs(x)) c += (s - t) + x;
-    else c += (x - t) + s;
-    s = t;
-}
-
 __global__ void __launch_bounds__(256) k_reduce_finish(const double* partials, int nblocks, int s0, double* out) {
     const int k = blockIdx.y;
     const double* p = partials + (long long)blockIdx.x * nblocks * RS_COUNT + s0 + k;

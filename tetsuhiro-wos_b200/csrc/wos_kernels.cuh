@@ -54,7 +54,8 @@ enum RedSlot {
     RS_SH1 = 7,      // spectral: sum |F H|^2 (BPM half step power)
     RS_SH2 = 8,      // spectral: sum |F H H|^2
     RS_HIST = 9,     // 97-bin radial spectral histogram
-    RS_COUNT = 9 + 97,
+    RS_SLO = 9 + 97, // low parts of RS_SW, RS_SFX, RS_SFY (compensated centroid sums)
+    RS_COUNT = RS_SLO + 3,
 };
 
 // ROW_FWD     : load (+pre ops) -> forward transform -> store
@@ -141,7 +142,7 @@ struct ColArgs {
     const double* batch_z;    // z per batch (null: h.z)
     int src_shared;           // 1: every batch reads batch 0 of src
     double* red;
-    int red_spec;             // spectral sums (SW, SFX, SFY)
+    int red_spec;             // spectral sums (SW, SFX, SFY), compensated: high parts in RS_SW.., low in RS_SLO..
     int red_hist;             // radial histogram
     int red_bpm;              // SH1 / SH2 sums
     int hist_lx, hist_ly;     // grid for the histogram / centroid frequencies

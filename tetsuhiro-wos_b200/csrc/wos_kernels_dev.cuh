@@ -196,6 +196,52 @@ __device__ __forceinline__ C eval_h(const HArgs& h, double wl, double z, int col
 }
 
 // Block-wide FP64 sum of K accumulators, written by thread 0 to out[0..K).
+// Compensated (Neumaier) addition: s + c carries the sum of everything added
+// with the rounding error of each addition kept in c.
+__device__ __forceinline__ void neumaier_add(double& s, double& c, double x) {
+    const double t = s + x;
+    if (fabs(s) >= fabs(x)) c += (s - t) + x;
+    else c += (x - t) + s;
+    s = t;
+}
+
+// Compensated block sum of K per-thread pairs (s[k] + c[k]); thread 0 writes
+// the high parts to hi[k] and the low parts to lo[k].
+template <int K>
+__device__ __forceinline__ void block_sum2_write(double (&s)[K], double (&c)[K], double* hi, double* lo) {
+    __shared__ double rsm2[32][K][2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();  // a previous reduction's readers are done with rsm2
+#pragma unroll
+    for (int k = 0; k < K; k++) {
+        double v = s[k], e = c[k];
+        for (int o = 16; o > 0; o >>= 1) {
+            const double v2 = __shfl_down_sync(0xffffffffu, v, o);
+            const double e2 = __shfl_down_sync(0xffffffffu, e, o);
+            e += e2;
+            neumaier_add(v, e, v2);
+        }
+        if (lane == 0) {
+            rsm2[warp][k][0] = v;
+            rsm2[warp][k][1] = e;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+        for (int k = 0; k < K; k++) {
+            double ts = 0, tc = 0;
+            for (int w = 0; w < nw; w++) {
+                tc += rsm2[w][k][1];
+                neumaier_add(ts, tc, rsm2[w][k][0]);
+            }
+            hi[k] = ts;
+            lo[k] = tc;
+        }
+    }
+}
+
 template <int K>
 __device__ __forceinline__ void block_sum_write(double (&acc)[K], double* out) {
     __shared__ double rsm[32][K];
@@ -573,6 +619,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
     }
 
     double acc[5] = {0, 0, 0, 0, 0};
+    double spc[3] = {0, 0, 0};  // compensation of the centroid sums
     double drop = 0;
     const double hfx = (a.red_spec || a.red_hist) ? freq_n(col, a.hist_lx, a.hist_dx) : 0.0;
     const double fnyq = 1.0 / (2.0 * a.hist_dx);
@@ -588,9 +635,9 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
             const double pw = (double)x.x * x.x + (double)x.y * x.y;
             const double fy = freq_n(q, a.hist_ly, a.hist_dx);
             if (a.red_spec) {
-                acc[0] += pw;
-                acc[1] += pw * hfx;
-                acc[2] += pw * fy;
+                neumaier_add(acc[0], spc[0], pw);
+                neumaier_add(acc[1], spc[1], pw * hfx);
+                neumaier_add(acc[2], spc[2], pw * fy);
             }
             if (a.red_hist && pw != 0) {
                 int b = (int)(dmul(ddiv(go_hypot(hfx, fy), fnyq), 96.0));
@@ -654,7 +701,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
         double* out = a.red + blk * RS_COUNT;
         if (a.red_spec) {
             double s3[3] = {acc[0], acc[1], acc[2]};
-            block_sum_write<3>(s3, out + RS_SW);
+            block_sum2_write<3>(s3, spc, out + RS_SW, out + RS_SLO);
         }
         if (a.red_bpm) {
             double s4[4] = {acc[0], acc[3], acc[4], drop};
