@@ -411,14 +411,25 @@ def run_config(args) -> None:
                 o3 = torch.empty((d3["zs"].size, 1, n3, n3), dtype=dt, device="cuda")
             torch.cuda.synchronize()
 
-            def cfg4_run():
+            def part1():
                 g.polychromatic_dev(n1, n1, d1["dx"], 1, f1.data_ptr(), d1["z"], d1["wls"], d1["weights"],
                                     wos.Context(wavelength=d1["wls"][0]), o1.data_ptr())
+
+            def part2():
                 g.partially_coherent_dev(n2, d2["dx"], d2["width"], d2["coherence"], m2, nz.data_ptr(), d2["z"],
                                          wos.Context(wavelength=d2["wl"]), o2.data_ptr())
+
+            def part3():
                 g.volume_dev(n3, n3, d3["dx"], 1, f3.data_ptr(), d3["zs"], wos.Context(wavelength=d3["wl"]),
                              o3.data_ptr())
+
+            def cfg4_run():
+                part1()
+                part2()
+                part3()
             rec["device_direct_s"] = timed(cfg4_run, max(2, args.steps // 4), 1)
+            rec["parts_direct_s"] = {k: timed(f, max(2, args.steps // 4), 1)
+                                     for k, f in (("cfg4.1", part1), ("cfg4.2", part2), ("cfg4.3", part3))}
             gr = _graph_of(g, cfg4_run)
             if gr is not None:
                 rec["device_s"] = timed(gr.launch, max(2, args.steps // 4), 1)

@@ -17,10 +17,11 @@ TOL_FP32 = 1e-5    # FP32 kernels (FP64 phase arguments)
 # is held at 5e-12.
 TOL_FP64_BLUESTEIN = 5e-12
 # The carrier-shift methods (asm_shift, asm_shift_pad) have no constant floor:
-# their output depends on the spectral centroid with a gain of ~1e4 (a
-# relative change of 5e-15 in the centroid moves the 128^2 tilted field by
-# 4.5e-11), and the reference sums the centroid sequentially.  Their tests
-# measure that floor per case (exact_centroid below) instead.
+# the last bits of the spectral centroid decide how the propagation phase
+# k z sqrt(1 - rho^2) of the shifted bins rounds (a phase of ~1e4 rad, whose
+# ulp is ~2e-12 rad): two ulps of the centroid move the 64^2 tilted field by
+# 1.3e-12, and the reference's sequential sums move the 128^2 one by 4.5e-11.
+# Their tests measure that floor per case instead (exact_centroid below).
 # Gaussian-Schell synthesis takes sqrt(max(0, S)) of a spectrum whose tail is
 # rounding noise (1414 of 4096 bins slightly negative at 64^2): the oracle and
 # an independent FP64 restatement differ by 8.7e-9.
@@ -76,11 +77,13 @@ def tol_case(precision, method: str, ny: int, nx: int) -> float:
     return t
 
 
-def exact_centroid(ex, ey, dx):
+def exact_centroid(ex, ey, dx, with_scale=False):
     """spectralCentroid (optics/propagate.go:391-416) over the oracle's own
     spectrum, with every sum exactly rounded (math.fsum) instead of
     accumulated in sequence; frequencies as the reference's freq (index i
-    <= n/2 positive)."""
+    <= n/2 positive).  with_scale: also the power-weighted mean |f| (of x and
+    y, the larger), the scale of the sums' rounding (a centroid near zero
+    comes from sums that cancel)."""
     import math
 
     import oracle as O
@@ -98,5 +101,10 @@ def exact_centroid(ex, ey, dx):
         w = w + (s.real * s.real + s.imag * s.imag)
     sw = math.fsum(w.ravel())
     if sw <= 0:
-        return 0.0, 0.0
-    return math.fsum((w * fx[None, :]).ravel()) / sw, math.fsum((w * fy[:, None]).ravel()) / sw
+        return (0.0, 0.0, 0.0) if with_scale else (0.0, 0.0)
+    cx = math.fsum((w * fx[None, :]).ravel()) / sw
+    cy = math.fsum((w * fy[:, None]).ravel()) / sw
+    if not with_scale:
+        return cx, cy
+    scale = max(float(np.sum(w * np.abs(fx)[None, :])), float(np.sum(w * np.abs(fy)[:, None]))) / sw
+    return cx, cy, scale

@@ -478,6 +478,39 @@ def test_volume_specialised_batch(gpu):
     check_warnings(gc, oc, gpu.precision == wos.FP64)
 
 
+def test_partially_coherent_fused_synthesis(gpu):
+    """Power-of-two grids of 256 points or more without diagnostics: the
+    realizations (optics/coherence.go:22-80) are synthesised inside the
+    propagation sweeps (the noise times sqrt(S) and the envelope's x factor in
+    the first row sweep, its y factor in the column sweep).  Against the
+    oracle, and against the path that synthesises them first (which a
+    Context with Warnings takes), through the host and the device entry
+    points."""
+    import torch
+    n, dx, w0, sigc, m, wl, z = 256, 1e-5, 6e-4, 5e-5, 7, 632.8e-9, 2e-2
+    noise = complex_normal(8, (m, n, n))
+    modes = O.schell_realizations(n, dx, w0, sigc, noise)
+    outs = []
+    for q in range(m):
+        f = O.Field(modes[q].copy(), dx)
+        O.propagate(f, z, "asm", O.Context(wavelength=wl))
+        outs.append(f.ex)
+    ref = O.average_intensity(np.array(outs))
+    bound = max(tol(gpu.precision), TOL_FP64_SCHELL)
+    fused = gpu.partially_coherent(n, dx, w0, sigc, noise, z, "asm", wos.Context(wavelength=wl,
+                                                                                   warnings_enabled=False))
+    staged = gpu.partially_coherent(n, dx, w0, sigc, noise, z, "asm", wos.Context(wavelength=wl))
+    assert rel_l2(fused, ref) <= bound, rel_l2(fused, ref)
+    assert rel_l2(staged, ref) <= bound
+    assert rel_l2(fused, staged) <= bound
+    nd = torch.from_numpy(noise).cuda()
+    out = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    gpu.partially_coherent_dev(n, dx, w0, sigc, m, nd.data_ptr(), z, wos.Context(wavelength=wl), out.data_ptr())
+    gpu.synchronize()
+    assert np.array_equal(out.cpu().numpy(), fused)   # the same sweeps on the same noise
+
+
 def test_partially_coherent_specialised_batch(gpu):
     n, dx, w0, sigc, m, wl, z = 256, 1e-5, 6e-4, 5e-5, 12, 632.8e-9, 2e-2
     noise = complex_normal(6, (m, n, n))

@@ -2,8 +2,9 @@
 
 Two FP64 floors sit above 1e-12 and come from the reference's own arithmetic,
 not from the GPU:
-- the carrier-shift methods depend on the spectral centroid with a gain of
-  ~1e4, and the reference sums the centroid in sequence
+- the carrier-shift methods depend on the last bits of the spectral centroid
+  (they decide how the propagation phase of the shifted bins, ~1e4 rad, rounds),
+  and the reference sums the centroid in sequence
   (optics/propagate.go:391-416);
 - the reference's Bluestein transform forms its chirp angle pi*k*k/n without
   reduction (optics/fft.go), so its error grows with the length.
@@ -56,6 +57,21 @@ def test_shift_output_amplifies_the_centroid_rounding(method):
     O.propagate_shift_at(b, z, method, O.Context(wavelength=wl), *exact_centroid(ex, None, dx))
     d = rel_l2(a.ex, b.ex)
     assert 1e-12 < d < 1e-9
+
+
+def test_shift_output_steps_with_the_centroid_bits():
+    """Moving the centroid by a few ulps changes the output in steps of
+    ~1e-12 (the rounding of the phase flips in some bins), not in proportion."""
+    n, dx, wl, z = 64, 2e-6, 632.8e-9, 5e-3
+    ex = tilted_gauss(n, dx, wl)
+    cx, cy = exact_centroid(ex, None, dx)
+    outs = []
+    for k in (0, 2, 16):
+        f = O.Field(ex.copy(), dx)
+        O.propagate_shift_at(f, z, "asm_shift", O.Context(wavelength=wl), cx + k * np.spacing(cx), cy)
+        outs.append(f.ex)
+    d2, d16 = rel_l2(outs[1], outs[0]), rel_l2(outs[2], outs[0])
+    assert 1e-13 < d2 < 1e-11 and 1e-13 < d16 < 1e-10 and d16 < 8 * d2
 
 
 @pytest.mark.parametrize("n,lo,hi", [(100, 1e-15, 1e-13), (1000, 5e-14, 1e-12), (3000, 2e-13, 2e-12)])

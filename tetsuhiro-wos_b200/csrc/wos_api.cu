@@ -481,13 +481,13 @@ int fast_tw_lo(wos_ctx c, Axis* a, int E, const void** out) {
 // the sweep's memory latency, while the 33 KB of table rows per CTA took the
 // shared memory that the other stream's row sweeps overlap in (two-stream
 // batch 20.4k -> 17.1k props/s), so the plain ASM does not use it.
-int attach_htab(wos_ctx c, FastCols& k, int L, int E) {
-    if (c->fp64 || !c->htab_on || !k.precise_phase || k.red || k.batch_wl || k.batch_z || L < 32) return WOS_OK;
-    const int W = fast_col_width(0, L, E, k.tiled ? kTileW : k.W);
+// The table of k's transfer function for columns of L points, from the
+// context's cache or built now on the context stream.  A new table is waited
+// for before returning (outside stream capture), so that sweeps on other
+// streams (the batch's side streams, a stream the caller switches to) can use
+// it at once.
+int htab_of(wos_ctx c, FastCols& k, int L, int hilo) {
     const int ld = htab_ld_for(L);
-    if (W < 1 || k.ncols < 2 * W || k.ncols % (2 * W) != 0) return WOS_OK;
-    const int hilo = k.tw_lo != nullptr;
-    if (fast_col_smem_htab(L, E, W, ld, hilo) + 2048 > 227 * 1024) return WOS_OK;
     const double key[9] = {k.wl, k.dx, k.kz, k.kaz, k.scale, k.alpha, k.limit, (double)k.zero_ev,
                            (double)(k.reg + 2 * k.backward + 4 * hilo)};
     for (auto& h : c->htab)
@@ -501,12 +501,38 @@ int attach_htab(wos_ctx c, FastCols& k, int L, int E) {
     h.valid = false;
     TRY(ensure(h.buf, (size_t)(k.ncols / 2 + 1) * ld * sizeof(float2) * (hilo ? 2 : 1)));
     CK(fast_build_htab(k, L, reinterpret_cast<float2*>(h.buf.p), ld, hilo, c->st));
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(c->st, &cs));
+    if (cs == cudaStreamCaptureStatusNone) CK(cudaStreamSynchronize(c->st));
     h.valid = true;
     h.L = L;
     h.ncols = k.ncols;
     std::memcpy(h.key, key, sizeof key);
     k.htab = reinterpret_cast<const float2*>(h.buf.p);
     k.htab_ld = ld;
+    return WOS_OK;
+}
+
+int attach_htab(wos_ctx c, FastCols& k, int L, int E) {
+    if (c->fp64 || !c->htab_on || !k.precise_phase || k.red || k.batch_wl || k.batch_z || L < 32) return WOS_OK;
+    const int W = fast_col_width(0, L, E, k.tiled ? kTileW : k.W);
+    const int ld = htab_ld_for(L);
+    if (W < 1 || k.ncols < 2 * W || k.ncols % (2 * W) != 0) return WOS_OK;
+    const int hilo = k.tw_lo != nullptr;
+    if (fast_col_smem_htab(L, E, W, ld, hilo) + 2048 > 227 * 1024) return WOS_OK;
+    return htab_of(c, k, L, hilo);
+}
+
+// The same table read from global memory into registers (FastCols::htab_global)
+// by the plain complex64 ASM column sweep on the tiled intermediate (no loss
+// sums, histogram, per-unit wavelengths or distances).  Measured at 2048^2
+// (two-stream batch): column sweep 37.2 -> 33.1 us, 19.8k -> 20.4k props/s,
+// one call per field 15.9k -> 16.8k; FP32 against the oracle 4.6e-7 -> 3.3e-7
+// (H rounded once from its FP64 value).
+int attach_htab_global(wos_ctx c, FastCols& k, int L) {
+    if (c->fp64 || !c->htab_reg || k.red || k.hist || k.batch_wl || k.batch_z || k.tw_lo || L < 32) return WOS_OK;
+    TRY(htab_of(c, k, L, 0));
+    k.htab_global = 1;
     return WOS_OK;
 }
 
@@ -655,6 +681,7 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
         k.hist = red_region(c, 1) + RS_HIST;
         k.hist_dx = p.dx;
     }
+    if (tiled) TRY(attach_htab_global(c, k, p.ny));
     CK(timed_launch(c, 4, [&] { return sweep_cols(c, p.ny, t.colE, k, &nb); }));
     if (s.red_loss) CK(launch_reduce_finish(red_region(c, 1), nb, 1, RS_SW, 2, redout_region(c, 1), c->st));
     if (s.hist) CK(launch_reduce_finish(red_region(c, 1), nb, 1, RS_HIST, 97, redout_region(c, 1), c->st));
@@ -1262,6 +1289,7 @@ int wos_ctx_create(int device, int precision, wos_ctx* out) {
     c->tiled = env_int("WOS_TILED", 1);
     c->bpm_comp = env_int("WOS_BPM_COMP", 1);
     c->htab_on = env_int("WOS_HTAB", 1);
+    c->htab_reg = env_int("WOS_HTAB_REG", 1);
     *out = c;
     return WOS_OK;
 }
@@ -1508,6 +1536,13 @@ int wos_propagate_batch_dev(wos_ctx c, int nfields, int ny, int nx, double dx, i
             if (pair_eligible(c, ny, t.colE, probe)) {  // shared tables of the split column tiles
                 const void *th, *tp;
                 if (!pair_tables(c, ny, t.colE, &th, &tp)) return fail(WOS_CUDA_ERROR, "split-tile tables");
+            }
+            // the transfer-function table the (tiled) column sweeps read
+            if (asm_tiled(c, ny, nx, t)) {
+                FastCols hk{};
+                hk.ncols = nx;
+                fill_asm_h(hk, asm_h(c, cc, z, ev_policy(cc, z), dx, nx, ny));
+                TRY(attach_htab_global(c, hk, ny));
             }
             nstreams = std::max(1, std::min(wos_ctx_s::kMaxAux, env_int("WOS_STREAMS", 2)));
         }

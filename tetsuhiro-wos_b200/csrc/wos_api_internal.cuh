@@ -110,7 +110,8 @@ struct wos_ctx_s {
     static constexpr int kHTabs = 4;
     HTab htab[kHTabs];
     int htab_next = 0;
-    int htab_on = 1;                    // WOS_HTAB=0: evaluate H in the sweep
+    int htab_on = 1;                    // WOS_HTAB=0: evaluate H in the split-step sweeps
+    int htab_reg = 1;                   // WOS_HTAB_REG=0: evaluate H in the plain ASM column sweep
     // device copies of the small parameter lists (wavelengths, distances,
     // weights) of the device-resident batches, keyed by content and reused
     // round robin: a repeated call copies nothing from the host

@@ -50,9 +50,18 @@ struct Batch {
     wos_diag* diag;
     int in_native = 0;     // in holds the context's complex type, not complex128
     int out_native = 0;    // out_planes of the context's complex type
+    // Gaussian-Schell realizations synthesised inside the sweeps: in holds the
+    // units' noise (complex128), schell_sq the map sqrt(S) and schell_g the
+    // envelope factor exp(-t^2/w^2)/n of one axis (square grid; the 1/n of
+    // each inverse axis folded in).  Only the specialised sweeps run it.
+    const double* schell_sq = nullptr;
+    const double* schell_g = nullptr;
     size_t in_esz(wos_ctx c) const { return in_native ? c->csz() : 16; }
     size_t out_esz(wos_ctx c) const { return out_native ? c->csz() : 16; }
 };
+
+// Grid sizes of the fused Gaussian-Schell sweeps (wos_schell.cu).
+bool schell_fast_size(int n) { return is_pow2(n) && n >= 256 && n <= 4096; }
 
 // Batched ASM on the specialised sweeps (power-of-two grids): the forward row
 // sweep once per component for a shared input, then per chunk of units one
@@ -78,12 +87,18 @@ int try_fast_batch(wos_ctx c, Batch& b, std::vector<double>& sums, std::vector<d
     const long long np = (long long)ny * nx;
     const bool shared_in = b.in_unit_stride == 0;
     const bool diag = b.diag != nullptr;
+    const bool schell = b.schell_sq != nullptr;
+    if (schell && (diag || shared_in || ncomp != 1 || !schell_fast_size(nx) || nx != ny)) return -1;
     Axis *ax, *ay;
     TRY(get_axis(c, nx, c->fp64, &ax));
     TRY(get_axis(c, ny, c->fp64, &ay));
-    const void *twx, *twy;
+    const void *twx, *twy, *twx8 = nullptr, *twy8 = nullptr;
     TRY(fast_tw(c, ax, t.rowE, &twx));
     TRY(fast_tw(c, ay, t.colE, &twy));
+    if (schell) {
+        TRY(fast_tw(c, ax, 8, &twx8));
+        TRY(fast_tw(c, ay, 8, &twy8));
+    }
     const size_t per = (size_t)np * c->csz();
     int B = (int)std::max<size_t>(1, ((size_t)4 << 30) / per);
     B = std::min(B, b.units);
@@ -121,7 +136,14 @@ int try_fast_batch(wos_ctx c, Batch& b, std::vector<double>& sums, std::vector<d
                     r.red = red_region(c, 0) + RS_P;
                     r.red_stride = RS_COUNT;
                 }
-                CK(timed_launch(c, 0, [&] { return fast_rows(c->fp64, nx, t.rowE, false, r, c->st, &nb); }));
+                if (schell) {
+                    r.tw = twx8;
+                    r.pre_map = b.schell_sq;
+                    r.env_x = b.schell_g;
+                    CK(timed_launch(c, 0, [&] { return fast_rows_schell(c->fp64, nx, 8, r, c->st, &nb); }));
+                } else {
+                    CK(timed_launch(c, 0, [&] { return fast_rows(c->fp64, nx, t.rowE, false, r, c->st, &nb); }));
+                }
                 if (diag) {
                     const int per_unit = nb / r.batch;
                     CK(launch_reduce_finish(red_region(c, 0), per_unit, r.batch, RS_P, 1, o, c->st));
@@ -165,7 +187,14 @@ int try_fast_batch(wos_ctx c, Batch& b, std::vector<double>& sums, std::vector<d
                 k.hist = red_region(c, 1) + RS_HIST;
                 k.hist_dx = dx;
             }
-            CK(timed_launch(c, 4, [&] { return sweep_cols(c, ny, t.colE, k, &nb); }));
+            if (schell) {
+                k.tw = twy8;
+                k.W = 4;
+                k.env_y = b.schell_g;
+                CK(timed_launch(c, 4, [&] { return fast_cols_env(c->fp64, ny, 8, k, c->st, &nb); }));
+            } else {
+                CK(timed_launch(c, 4, [&] { return sweep_cols(c, ny, t.colE, k, &nb); }));
+            }
             if (diag) {
                 const int per_unit = nb / nu;
                 CK(launch_reduce_finish(red_region(c, 1), per_unit, nu, RS_SW, 2, o, c->st));
@@ -230,6 +259,7 @@ int run_batch_asm(wos_ctx c, Batch& b) {
     std::vector<double> pin_unit(b.units, 0.0);
     const int fast = try_fast_batch(c, b, sums, pin_unit, pin_total);
     if (fast != -1 && fast != WOS_OK) return fast;
+    if (fast == -1 && b.schell_sq) return -1;  // the caller synthesises the realizations first
     for (int comp = 0; comp < ncomp && fast == -1; comp++) {
         for (int k0 = 0; k0 < b.units; k0 += B) {
             const int nb = std::min(B, b.units - k0);
@@ -388,6 +418,45 @@ int check_dev_geometry(int ny, int nx, double dx, int ncomp) {
 // [m][n][n] complex128) propagated to z and averaged with weight 1/m into out
 // (device FP64 [n][n], overwritten): the whole source when m0 = 0 and count =
 // m, one rank's share of a sharded run otherwise.
+// The Gaussian-Schell tables of the fused sweeps: sqrt(max(0, Re FFT2(mu)))
+// (FP64, [n][n], as GenerateSchellRealizations forms it) and the envelope
+// factor of one axis, g(t) = exp(-t^2/w^2) / n (sqrt(I(x, y)) = g(x) g(y) n^2
+// with I = exp(-2 (x^2 + y^2) / w^2); the 1/n of each inverse axis folded in).
+int schell_tables(wos_ctx c, int n, double dx, double width, double coh, const double** sq, const double** g) {
+    const long long nn = (long long)n * n;
+    TRY(ensure(c->aux, (size_t)nn * (16 + 8)));
+    double2* mu = reinterpret_cast<double2*>(c->aux.p);
+    double* sqs = reinterpret_cast<double*>(mu + nn);
+    CK(launch_schell_mu(mu, n, dx, coh, c->st));
+    TRY(fft2d_fp64(c, n, 1, mu, 0));
+    CK(launch_sqrt_re(sqs, mu, nn, c->st));
+    std::vector<double> gh(n);
+    for (int i = 0; i < n; i++) {
+        const double x = ((double)i - (double)n / 2) * dx;
+        gh[i] = std::exp(-(x * x) / (width * width)) / (double)n;
+    }
+    TRY(cached_params(c, gh, g));
+    *sq = sqs;
+    return WOS_OK;
+}
+
+// Realizations count of noise (device complex128 [count][n][n]) synthesised
+// inside the propagation sweeps and their weighted intensities added into out
+// (device FP64 [n][n]); -1 when the fused sweeps do not cover the case.
+int schell_fused(wos_ctx c, int n, double dx, double width, double coh, int m, int count, const double2* noise,
+                 double z, const wos_context& cc, double* out) {
+    if (c->no_fast || z == 0 || !schell_fast_size(n)) return -1;
+    const double *sq, *g, *w_d;
+    TRY(schell_tables(c, n, dx, width, coh, &sq, &g));
+    TRY(cached_params(c, std::vector<double>(count, 1 / (double)m), &w_d));
+    const long long nn = (long long)n * n;
+    Batch b{n, n, 1, dx, noise, nn, count, nullptr, nullptr, {}, std::vector<double>(count, z), w_d, out, nullptr, cc,
+            nullptr};
+    b.schell_sq = sq;
+    b.schell_g = g;
+    return run_batch_asm(c, b);
+}
+
 int schell_dev_range(wos_ctx c, int n, double dx, double width, double coherence, int m, int m0, int count,
                      const void* noise, double z, const wos_context* cci, double* out) {
     if (!c || !noise || !out) return fail(WOS_INVALID_ARG, "null argument");
@@ -402,6 +471,11 @@ int schell_dev_range(wos_ctx c, int n, double dx, double width, double coherence
     const long long nn = (long long)n * n;
     CK(cudaMemsetAsync(out, 0, sizeof(double) * nn, c->st));
     if (count == 0) return WOS_OK;
+    {
+        const int rc = schell_fused(c, n, dx, width, coherence, m, count,
+                                    reinterpret_cast<const double2*>(noise) + m0 * nn, z, cc, out);
+        if (rc != -1) return rc;
+    }
     TRY(ensure(c->vol, sizeof(double2) * (size_t)nn * count));
     double2* modes = reinterpret_cast<double2*>(c->vol.p);
     TRY(schell_generate(c, n, dx, width, coherence, count, reinterpret_cast<const double2*>(noise) + m0 * nn, true,
@@ -417,6 +491,8 @@ int schell_dev_range(wos_ctx c, int n, double dx, double width, double coherence
             nullptr};
     return run_batch_asm(c, b);
 }
+
+
 
 int upload_params(wos_ctx c, const std::vector<double>& a, const std::vector<double>& b2,
                   const std::vector<double>& c3, double** pa, double** pb, double** pc) {
@@ -582,12 +658,23 @@ int wos_partially_coherent(wos_ctx c, int n, double dx, double width, double coh
     const long long nn = (long long)n * n;
     TRY(ensure(c->vol, sizeof(double2) * (size_t)nn * m));
     double2* modes = reinterpret_cast<double2*>(c->vol.p);
-    TRY(schell_generate(c, n, dx, width, coherence, m, noise, false, modes));
     TRY(ensure(c->accum, sizeof(double) * nn));
     double* acc = reinterpret_cast<double*>(c->accum.p);
     CK(cudaMemsetAsync(acc, 0, sizeof(double) * nn, c->st));
     const double inv = 1 / (double)m;
     wos_diag* dp = (cc.diagnostics && diag) ? diag : nullptr;
+    if (z != 0 && method == WOS_ASM && !dp && schell_fast_size(n) && !c->no_fast) {
+        // the realizations synthesised inside the propagation sweeps
+        CK(cudaMemcpyAsync(modes, noise, sizeof(double2) * (size_t)nn * m, cudaMemcpyHostToDevice, c->st));
+        const int rc = schell_fused(c, n, dx, width, coherence, m, m, modes, z, cc, acc);
+        if (rc != -1) {
+            TRY(rc);
+            CK(cudaMemcpyAsync(out, acc, sizeof(double) * nn, cudaMemcpyDeviceToHost, c->st));
+            CK(cudaStreamSynchronize(c->st));
+            return WOS_OK;
+        }
+    }
+    TRY(schell_generate(c, n, dx, width, coherence, m, noise, false, modes));
     if (z == 0) {
         for (int q = 0; q < m; q++) CK(launch_accum_int(1, acc, modes + q * nn, 1, nn, inv, c->st));
     } else if (method == WOS_ASM) {

@@ -37,6 +37,12 @@ struct FastRows {
     // split-step row sweep): same layout as tw, (float)(W - tw) from FP64; null
     // for the plain transforms
     const void* tw_lo;
+    // Gaussian-Schell synthesis fused into the first row sweep
+    // (k_rows_schell_fast): the complex128 input (a realization's noise) is
+    // multiplied by pre_map[r][x] (FP64, shared by the batch) on load, inverse
+    // transformed, multiplied by env_x[x] and forward transformed
+    const double* pre_map;
+    const double* env_x;
 };
 constexpr int kTileW = 4;
 
@@ -89,6 +95,16 @@ struct FastCols {
     // sweeps) an entry is the pair (H_hi, H_lo), 16 bytes, H_lo = H - H_hi.
     const float2* htab;
     int htab_ld;
+    // 1: the plain complex64 sweep (no loss sums, histogram or compensated
+    // transforms) reads its H straight from the table in global memory (L2
+    // resident across a batch) into registers, at the positions the forward
+    // transform leaves in them, instead of staging the spectrum in shared
+    // memory to evaluate H once per (q, L - q) pair
+    int htab_global;
+    // Gaussian-Schell synthesis fused into the column sweep (instantiations
+    // with ENV): each column is inverse transformed, multiplied by env_y[y]
+    // and forward transformed before the transfer function
+    const double* env_y;
 };
 // Table rows of the W columns from col0 (W | ncols / 2): contiguous, in order
 // below ncols / 2 and reversed above it.
@@ -107,6 +123,12 @@ cudaError_t fast_build_htab(const FastCols& a, int L, float2* out, int ld, int h
 size_t fast_col_smem_htab(int L, int E, int W, int ld, int hilo);
 
 cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaStream_t st, int* nblocks);
+// Gaussian-Schell sweeps (wos_schell.cu): the first row sweep of a batch of
+// realizations (a.pre_map, a.env_x; complex128 input) and the column sweep
+// with the column envelope (a.env_y).  cudaErrorNotSupported outside E = 8,
+// L = 256 .. 4096.
+cudaError_t fast_rows_schell(int fp64, int L, int E, const FastRows& a, cudaStream_t st, int* nblocks);
+cudaError_t fast_cols_env(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks);
 cudaError_t fast_cols(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks);
 // The column sweep on two-CTA clusters (see FastCols::tw_half); returns
 // cudaErrorNotSupported outside its case (FP32, L = 2048, E = 16, W = 8, no

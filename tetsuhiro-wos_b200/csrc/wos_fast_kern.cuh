@@ -172,13 +172,72 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_bpm_fast(const FastR
     }
 }
 
+// The first row sweep of a batch of Gaussian-Schell realizations
+// (GenerateSchellRealizations, optics/coherence.go:22-80, with the
+// propagation's forward row transform): realization b = blockIdx.y, row r.
+// The noise (complex128) times sqrt(S) (pre_map, FP64) is inverse
+// transformed along x, multiplied by the x factor of the separable envelope
+// sqrt(I) = exp(-x^2/w^2) exp(-y^2/w^2) (env_x, with the generation's 1/nx
+// folded in) and transformed forward again.  The envelope's y factor and the
+// column transforms follow in the column sweep (k_cols_fast with ENV):
+// operators along different axes commute, so the realization's inverse FFT2,
+// its envelope and the propagation's forward FFT2 take one pass over the data
+// per axis.
+template <typename Real, int L, int E>
+__global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_schell_fast(const FastRows a) {
+    pdl_wait();
+    pdl_trigger();
+    using C = typename CT<Real>::t;
+    using PL = FPlan<L, E>;
+    constexpr int T = PL::T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int lines = blockDim.x / T;
+    const int line = threadIdx.x / T, tt = threadIdx.x - line * T;
+    C* smb = reinterpret_cast<C*>(smraw) + line * frow_stride(L, E);
+    const int r = blockIdx.x * lines + line;
+    const bool act = r < a.rows;
+    const C* twp = reinterpret_cast<const C*>(a.tw);
+    C v[E];
+    if (act) {
+        const double2* in = reinterpret_cast<const double2*>(a.in) + (long long)blockIdx.y * a.in_bstride +
+                            (long long)r * a.in_ld + tt;
+        const double* m = a.pre_map + (long long)r * a.in_ld + tt;
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int p = fpos<E, E, L>(s, 0);
+            const double2 x = __ldcs(in + p);
+            const double g = __ldg(m + p);
+            v[s] = mkc<C>((Real)(x.x * g), (Real)(x.y * g));
+        }
+    } else {
+#pragma unroll
+        for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
+    }
+    fpasses<L, E, true, 0, 1, C>(v, smb, tt, twp);
+#pragma unroll
+    for (int s = 0; s < E; s++) {
+        const Real g = (Real)__ldg(a.env_x + fpos<PL::RS, E, L>(s, tt));
+        v[s] = mkc<C>(v[s].x * g, v[s].y * g);
+    }
+    fpasses<L, E, false, 0, 1, C>(v, smb, tt, twp);
+    if (act) {
+        C* out = reinterpret_cast<C*>(a.out) + (long long)blockIdx.y * a.out_bstride + (long long)r * a.out_ld + tt;
+#pragma unroll
+        for (int s = 0; s < E; s++) out[fpos<E, E, L>(s, 0)] = v[s];
+    }
+}
+
 // Fused column sweep: W adjacent columns per CTA (strided, or one contiguous
 // tile in the tiled layout); forward column transform, H of asmTF
 // (optics/propagate.go:159-181) from an FP64 argument or from the table
 // (FastCols::htab), optional spectral sums and wrap histogram, inverse column
 // transform.  CP: compensated transforms (twiddle residuals from a.tw_lo) and
-// hi + lo table entries.
-template <typename Real, int L, int E, int W, bool CP = false>
+// hi + lo table entries.  ENV (Gaussian-Schell batches after
+// k_rows_schell_fast): the column is first inverse transformed, multiplied by
+// env_y and transformed forward, so H meets the realization's spectrum.
+// HG (complex64, a.htab_global): H from the table in global memory, applied
+// in registers (no shared-memory spectrum stage, no H evaluation).
+template <typename Real, int L, int E, int W, bool CP = false, bool ENV = false, bool HG = false>
 __global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, E, W>::minb)
     k_cols_fast(const FastCols a) {
     pdl_wait();
@@ -202,28 +261,62 @@ __global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, 
         for (int k = threadIdx.x; k < 97; k += blockDim.x) hsm[k] = 0;
     // transfer-function table rows of this tile, behind the exchange tile
     float2* hs = nullptr;
-    if constexpr (sizeof(Real) == 4) {
-        if (a.htab) {
+    if constexpr (sizeof(Real) == 4 && !HG) {
+        if (a.htab && !a.htab_global) {
             hs = reinterpret_cast<float2*>(smraw + fcol_htab_off(L, E, W));
             htab_prefetch<W, CP>(hs, a, blockIdx.x * W);
         }
     }
     C v[E];
-    constexpr int R1 = PL::RS;
-    if (act) {
-        const C* src = sbase + (long long)tt * a.ld;
+    if constexpr (ENV) {
+        if (act) {
+            const C* src = sbase + (long long)tt * a.ld;
 #pragma unroll
-        for (int s = 0; s < E; s++) v[s] = __ldcs(src + (long long)fpos<R1, E, L>(s, 0) * a.ld);
+            for (int s = 0; s < E; s++) v[s] = __ldcs(src + (long long)fpos<E, E, L>(s, 0) * a.ld);
+        } else {
+#pragma unroll
+            for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
+        }
+        fpasses<L, E, true, 0, W, C, CP>(v, smb, tt, twp, twl);
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const Real g = (Real)__ldg(a.env_y + fpos<PL::RS, E, L>(s, tt));
+            v[s] = mkc<C>(v[s].x * g, v[s].y * g);
+        }
     } else {
+        constexpr int R1 = PL::RS;
+        if (act) {
+            const C* src = sbase + (long long)tt * a.ld;
 #pragma unroll
-        for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
+            for (int s = 0; s < E; s++) v[s] = __ldcs(src + (long long)fpos<R1, E, L>(s, 0) * a.ld);
+        } else {
+#pragma unroll
+            for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
+        }
     }
     // interleaved tile: stride W between consecutive positions of a column
     fpasses<L, E, false, 0, W, C, CP>(v, smb, tt, twp, twl);
 
     double p0 = 0, l1 = 0;
-    col_spectral_stage<Real, L, E, W, C, CP>(v, reinterpret_cast<C*>(smraw), hsm, blockIdx.x * W, a,
-                                             h_unit(a, blockIdx.y), p0, l1, hs);
+    if constexpr (HG) {
+        // v[s] holds frequency q = tt + s*T, where the inverse transform
+        // starts: H(|fx|, |fy|) from the table row of this column
+        static_assert(sizeof(Real) == 4 && !CP, "table in registers: plain complex64 sweeps");
+        if (act) {
+            const int cabs = col <= a.ncols / 2 ? col : a.ncols - col;
+            const float2* hr = a.htab + (long long)cabs * a.htab_ld;
+            const float sg = a.conj ? -1.f : 1.f;
+#pragma unroll
+            for (int s = 0; s < E; s++) {
+                const int q = tt + s * (L / E);
+                const float2 t = __ldg(hr + (q <= L / 2 ? q : L - q));
+                v[s] = cmul(v[s], mkc<C>(t.x, sg * t.y));
+            }
+        }
+    } else {
+        col_spectral_stage<Real, L, E, W, C, CP>(v, reinterpret_cast<C*>(smraw), hsm, blockIdx.x * W, a,
+                                                 h_unit(a, blockIdx.y), p0, l1, hs);
+    }
     fpasses<L, E, true, 0, W, C, CP>(v, smb, tt, twp, twl);
     if (act) {
         constexpr int RO = PL::RS;
@@ -250,23 +343,38 @@ inline cudaError_t go_rows_bpm(const FastRows& a, cudaStream_t st, int* nblocks)
     return launch_sweep(k_rows_bpm_fast<Real, L, E, CP>, grid, lines * T, smem, st, a);
 }
 
-template <typename Real, int L, int E, int W, bool CP = false>
+template <typename Real, int L, int E>
+inline cudaError_t go_rows_schell(const FastRows& a, cudaStream_t st, int* nblocks) {
+    constexpr int T = L / E;
+    const int lines = fast_row_lines(L, E, a.rows);
+    const size_t smem = (size_t)frow_stride(L, E) * lines * sizeof(typename CT<Real>::t);
+    if (smem > kSmemNoOptIn) {
+        cudaError_t e = cudaFuncSetAttribute(k_rows_schell_fast<Real, L, E>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((a.rows + lines - 1) / lines, a.batch > 0 ? a.batch : 1);
+    if (nblocks) *nblocks = (int)(grid.x * grid.y);
+    return launch_sweep(k_rows_schell_fast<Real, L, E>, grid, lines * T, smem, st, a);
+}
+
+template <typename Real, int L, int E, int W, bool CP = false, bool ENV = false, bool HG = false>
 inline cudaError_t go_cols_w(const FastCols& a, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
     if constexpr (W * T < 32 || W * T > fcol_max_threads(sizeof(Real) == 8, T)) {
         return cudaErrorInvalidConfiguration;
     } else {
         size_t smem = (size_t)fcol_elems(L, E, W) * sizeof(typename CT<Real>::t);
-        if (sizeof(Real) == 4 && a.htab)
+        if (sizeof(Real) == 4 && a.htab && !a.htab_global && !HG)
             smem = fcol_htab_off(L, E, W) + (size_t)W * a.htab_ld * sizeof(float2) * (CP ? 2 : 1);
         if (smem > kSmemNoOptIn) {
-            cudaError_t e = cudaFuncSetAttribute(k_cols_fast<Real, L, E, W, CP>,
+            cudaError_t e = cudaFuncSetAttribute(k_cols_fast<Real, L, E, W, CP, ENV, HG>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
         dim3 grid((a.ncols + W - 1) / W, a.batch > 0 ? a.batch : 1);
         if (nblocks) *nblocks = (int)(grid.x * grid.y);
-        return launch_sweep(k_cols_fast<Real, L, E, W, CP>, grid, W * T, smem, st, a);
+        return launch_sweep(k_cols_fast<Real, L, E, W, CP, ENV, HG>, grid, W * T, smem, st, a);
     }
 }
 
