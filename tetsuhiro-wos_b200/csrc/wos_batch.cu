@@ -260,6 +260,14 @@ int run_batch_asm(wos_ctx c, Batch& b) {
     const int fast = try_fast_batch(c, b, sums, pin_unit, pin_total);
     if (fast != -1 && fast != WOS_OK) return fast;
     if (fast == -1 && b.schell_sq) return -1;  // the caller synthesises the realizations first
+    // a shared input is column-transformed once and every unit's column sweep
+    // starts from that spectrum (H, inverse), where the lines need no Bluestein
+    bool spec = false;
+    if (shared_in && !diag) {
+        ColArgs probe = col_defaults(c, dx);
+        fill_axis(probe, ay);
+        spec = probe.blue_n == 0;
+    }
     for (int comp = 0; comp < ncomp && fast == -1; comp++) {
         for (int k0 = 0; k0 < b.units; k0 += B) {
             const int nb = std::min(B, b.units - k0);
@@ -297,6 +305,20 @@ int run_batch_asm(wos_ctx c, Batch& b) {
                         else pin_unit[k0 + u] += p;
                     }
                 }
+                if (spec) {  // the shared input's column transform, once for all units
+                    ColArgs f = col_defaults(c, dx);
+                    f.mode = COL_FFT;
+                    f.ncols = nx;
+                    fill_axis(f, ay);
+                    f.W = W;
+                    f.src = S0;
+                    f.src_ld = nx;
+                    f.in_n = ny;
+                    f.dst = S0;
+                    f.dst_ld = nx;
+                    f.out_n = ny;
+                    CK(prof_cols(c, c->fp64, f));
+                }
             }
             ColArgs a = col_defaults(c, dx);
             a.mode = COL_FUSED;
@@ -318,6 +340,7 @@ int run_batch_asm(wos_ctx c, Batch& b) {
             a.batch_z = b.z_dev ? b.z_dev + k0 : nullptr;
             if (!b.wl_dev) a.h.wl = b.cc.wavelength, a.h.k = 2 * M_PI / b.cc.wavelength;
             a.batch = nb;
+            a.src_spectrum = spec;
             if (diag) {
                 a.red = red_region(c, 1);
                 a.red_bpm = 1;

@@ -155,6 +155,8 @@ struct ColArgs {
     int batch;
     int col_inverse;          // COL_FFT direction
     double out_scale;         // COL_FFT scale on store
+    int src_spectrum;         // COL_FUSED: src is already column-transformed (shared by a batch's
+                              // units), so the first transform is skipped; lines without Bluestein
 };
 
 // launchers (wos_kernels.cu)

@@ -560,7 +560,9 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
 
     C v[E];
     const C* src = reinterpret_cast<const C*>(a.src) + (a.src_shared ? 0 : (long long)bz * a.src_bstride);
-    const int R1 = MIX ? E : in_radix(lp, inv_first, blue, E);  // mixed lines: natural radix E
+    // mixed lines: natural radix E; a loaded spectrum sits where the forward transform leaves it
+    const bool spec = a.src_spectrum && !blue;
+    const int R1 = MIX ? E : (spec ? out_radix(lp, false, false, E) : in_radix(lp, inv_first, blue, E));
 #pragma unroll
     for (int s = 0; s < E; s++) {
         const int p = nat_pos(s, R1, tt, T, L);
@@ -573,7 +575,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
     }
 
     // first column transform
-    xform<E, MIX>(v, sm, alt, ix, w, tt, T, lp, tw, inv_first, inv_first ? bhi : bhf);
+    if (!spec) xform<E, MIX>(v, sm, alt, ix, w, tt, T, lp, tw, inv_first, inv_first ? bhi : bhf);
     int Rm = MIX ? E : out_radix(lp, inv_first, blue, E);
     if (blue && (a.mode == COL_FRAUNHOFER || a.mode == COL_FFT)) {
         // the chirp of the Bluestein output has unit modulus: applied only
@@ -715,6 +717,185 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols(const ColArgs a) {
 }
 
 
+// ------------------------------------------------------------------ lean mixed-radix sweeps
+// The general sweeps carry every mode inline (Bluestein, screens, carrier
+// ramps, reductions, Fraunhofer, every transfer function): 128 registers a
+// thread and code that overflows the instruction cache, which on mixed-radix
+// lines (2^a 3^b 5^c) left the batched ASM column sweep stalled on
+// instruction fetch.  These two kernels do only what an ASM step on such
+// lines needs.  k_rows_mix_lean: load (complex128 conversion, window
+// in_off/in_n, carrier ramp on load), one transform, store (window, scale,
+// carrier ramp on store) or, for ROW_INV_ACC, the weighted |E|^2 summed over
+// the batch into an FP64 map.  k_cols_mix_asm: load the source columns (or
+// their spectrum, SPEC), transform, H of asmTF with per-unit wavelength and
+// distance (formed once per thread), inverse, store.
+
+// exp(i arg), complex64 from the FP64 argument reduced to revolutions (small
+// code, about one ulp); complex128 as the general sweeps (FP64 sincos).
+template <typename C> __device__ __forceinline__ C cexpi_lean(double arg);
+template <> __device__ __forceinline__ double2 cexpi_lean<double2>(double arg) { return cexpi<double2>(arg); }
+template <> __device__ __forceinline__ float2 cexpi_lean<float2>(double arg) {
+    const double t = arg * 0.15915494309189533577;  // revolutions
+    const float f = (float)(t - rint(t));           // in [-1/2, 1/2]
+    float sn, cs;
+    sincospif(2.0f * f, &sn, &cs);
+    return make_float2(cs, sn);
+}
+
+// asmTF with the complex64 phase through cexpi_lean; complex128 as asm_tf.
+template <typename C>
+__device__ __forceinline__ C asm_tf_lean(const HArgs& h, double wl, double kz, double kaz, bool backward, double fx,
+                                         double fy, double& m2) {
+    if constexpr (sizeof(C) == 16) {
+        return asm_tf<C>(h, wl, kz, kaz, backward, fx, fy, m2);
+    } else {
+        const double ax = wl * fx, ay = wl * fy;
+        const double s = fma(-ay, ay, fma(-ax, ax, 1.0));
+        if (s >= 0) {
+            m2 = 1.0;
+            return cexpi_lean<C>(kz * sqrt(s));
+        }
+        return asm_tf<C>(h, wl, kz, kaz, backward, fx, fy, m2);
+    }
+}
+
+template <typename Real, int E, bool INV>
+__global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows_mix_lean(const RowArgs a) {
+    using C = typename CT<Real>::t;
+    using T_ = Real;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int L = a.L;
+    const int T = L / E;
+    const int lines = blockDim.x / T;
+    const int line = threadIdx.x / T, tt = threadIdx.x - line * T;
+    const int r = blockIdx.x * lines + line;
+    const bool act = r < a.rows;
+    const int bz = blockIdx.y;
+    const int grow = a.row0 + r;
+    const RowIdx ix{row_line_stride(L)};
+    C* const alt = sm + (size_t)row_line_stride(L) * lines;
+    const C* tw = reinterpret_cast<const C*>(a.tw);
+    const double yrow = gX(grow, a.ny_grid, a.dx);
+    const bool acc_mode = INV && a.mode == ROW_INV_ACC;
+    const int nb = acc_mode ? a.acc_nb : 1;
+    C v[E];
+    double iacc[E];
+    for (int bb = 0; bb < nb; bb++) {
+        const long long ibase = (long long)(acc_mode ? bb : bz) * a.in_bstride + (long long)r * a.in_ld;
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int p = tt + s * T;
+            C x = mkc<C>(0, 0);
+            if (act && p >= a.in_off && p < a.in_off + a.in_n) {
+                const int i = p - a.in_off;
+                x = load_elem<C>(a.in, a.in_c128, ibase + i);
+                if (!INV && a.pre_shift) {
+                    const double arg =
+                        dmul(dmul(-2.0, M_PI), dadd(dmul(a.fxc, gX(i, a.nx_grid, a.dx)), dmul(a.fyc, yrow)));
+                    x = cmul(x, cexpi_lean<C>(arg));
+                }
+            }
+            v[s] = x;
+        }
+        mixed_line_fft<E, INV>(v, sm, alt, ix, line, tt, T, L, tw);
+        if (acc_mode) {
+            const double wgt = a.acc_weight ? a.acc_weight[bb] : 1.0;
+#pragma unroll
+            for (int s = 0; s < E; s++) {
+                const C x = cscale(v[s], (T_)a.out_scale);
+                const double pw = wgt * ((double)x.x * x.x + (double)x.y * x.y);
+                iacc[s] = (bb == 0) ? pw : iacc[s] + pw;
+            }
+        }
+    }
+    const long long obase = (long long)bz * a.out_bstride + (long long)r * a.out_ld;
+#pragma unroll
+    for (int s = 0; s < E; s++) {
+        const int q = tt + s * T;
+        if (!act || q < a.out_off || q >= a.out_off + a.out_n) continue;
+        const int i = q - a.out_off;
+        if (acc_mode) {
+            double* o = reinterpret_cast<double*>(a.out);
+            o[obase + i] = (a.acc_add ? o[obase + i] : 0.0) + iacc[s];
+            continue;
+        }
+        C x = v[s];
+        if (a.out_scale != 1.0) x = cscale(x, (T_)a.out_scale);
+        if (a.post_shift) {
+            const double arg = dmul(dmul(2.0, M_PI), dadd(dmul(a.fxc, gX(i, a.nx_grid, a.dx)), dmul(a.fyc, yrow)));
+            x = cmul(x, cexpi_lean<C>(arg));
+        }
+        store_elem<C>(a.out, a.out_c128, obase + i, x);
+    }
+}
+
+template <typename Real, int E, bool SPEC>
+__global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols_mix_asm(const ColArgs a) {
+    using C = typename CT<Real>::t;
+    using T_ = Real;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int L = a.L;
+    const int T = L / E;
+    const int W = a.W;
+    const int w = threadIdx.x & (W - 1);
+    const int tt = threadIdx.x / W;
+    const int col = blockIdx.x * W + w;
+    const bool act = col < a.ncols;
+    const int bz = blockIdx.y;
+    const ColIdx ix{W};
+    C* const alt = sm + (size_t)col_tile_elems(L, W);
+    const C* tw = reinterpret_cast<const C*>(a.tw);
+    C v[E];
+    const C* src = reinterpret_cast<const C*>(a.src) + (a.src_shared ? 0 : (long long)bz * a.src_bstride);
+#pragma unroll
+    for (int s = 0; s < E; s++) {
+        const int p = tt + s * T;
+        C x = mkc<C>(0, 0);
+        if (act && p >= a.in_off && p < a.in_off + a.in_n) x = src[(long long)(p - a.in_off) * a.src_ld + col];
+        v[s] = x;
+    }
+    if (!SPEC) mixed_line_fft<E, false>(v, sm, alt, ix, w, tt, T, L, tw);
+
+    // asmTF (optics/propagate.go:159-181) with this unit's wavelength and distance
+    const HArgs& h = a.h;
+    const double wl = a.batch_wl ? a.batch_wl[bz] : h.wl;
+    const double z = a.batch_z ? a.batch_z[bz] : h.z;
+    const double k = (wl == h.wl) ? h.k : 2 * M_PI / wl;
+    const double kz = (wl == h.wl && z == h.z) ? h.kz : k * z;
+    const double kaz = (wl == h.wl && z == h.z) ? h.kaz : k * fabs(z);
+    const double fx = h.fxoff != 0 ? dadd(freq_n(col, h.lfx, h.dx), h.fxoff) : freq_n(col, h.lfx, h.dx);
+#pragma unroll
+    for (int s = 0; s < E; s++) {
+        const int q = tt + s * T;
+        const double fy = h.fyoff != 0 ? dadd(freq_n(q, h.lfy, h.dx), h.fyoff) : freq_n(q, h.lfy, h.dx);
+        double m2;
+        C hh = asm_tf_lean<C>(h, wl, kz, kaz, z < 0, fx, fy, m2);
+        if (h.conj) hh.y = -hh.y;
+        v[s] = cscale(cmul(v[s], hh), (T_)h.scale);
+    }
+    mixed_line_fft<E, true>(v, sm, alt, ix, w, tt, T, L, tw);
+    C* dst = reinterpret_cast<C*>(a.dst) + (long long)bz * a.dst_bstride;
+#pragma unroll
+    for (int s = 0; s < E; s++) {
+        const int q = tt + s * T;
+        if (act && q >= a.out_off && q < a.out_off + a.out_n) dst[(long long)(q - a.out_off) * a.dst_ld + col] = v[s];
+    }
+}
+
+// Whether a general launch can take the lean kernels above (mixed lines only).
+__host__ inline bool rows_mix_lean_ok(const RowArgs& a) {
+    if (a.blue_n || a.red || a.pre_phi || a.pre_phi_f || a.scr.kind) return false;
+    if (a.mode == ROW_INV_ACC) return a.out_accum_int == 2;
+    return (a.mode == ROW_FWD || a.mode == ROW_INV) && a.out_accum_int == 0 && (a.mode == ROW_FWD || !a.pre_shift) &&
+           (a.mode == ROW_INV || !a.post_shift);
+}
+__host__ inline bool cols_mix_lean_ok(const ColArgs& a) {
+    return a.mode == COL_FUSED && a.h.kind == H_ASM && !a.blue_n && !a.red && !a.red_spec && !a.red_hist &&
+           !a.red_bpm;
+}
+
 // Launchers of the mixed-radix instantiations (wos_kernels_mix*.cu).
 template <typename Real, int E>
 cudaError_t launch_rows_mix(const RowArgs& a, dim3 grid, int threads, size_t smem, cudaStream_t st);
@@ -723,8 +904,22 @@ cudaError_t launch_cols_mix(const ColArgs& a, dim3 grid, int threads, size_t sme
 
 // Definitions, included by the translation units that instantiate them.
 #ifdef WOS_DEFINE_MIX_LAUNCHERS
+template <typename K>
+cudaError_t launch_mix_kernel(K kern, dim3 grid, int threads, size_t smem, cudaStream_t st, const void* args) {
+    if (smem > kSmemNoOptIn) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    void* argv[] = {const_cast<void*>(args)};
+    return cudaLaunchKernel(reinterpret_cast<const void*>(kern), grid, dim3(threads), argv, smem, st);
+}
+
 template <typename Real, int E>
 cudaError_t launch_rows_mix(const RowArgs& a, dim3 grid, int threads, size_t smem, cudaStream_t st) {
+    if (rows_mix_lean_ok(a)) {
+        if (a.mode == ROW_FWD) return launch_mix_kernel(k_rows_mix_lean<Real, E, false>, grid, threads, smem, st, &a);
+        return launch_mix_kernel(k_rows_mix_lean<Real, E, true>, grid, threads, smem, st, &a);
+    }
     if (smem > kSmemNoOptIn) {
         cudaError_t e = cudaFuncSetAttribute(k_rows<Real, E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
@@ -736,6 +931,10 @@ cudaError_t launch_rows_mix(const RowArgs& a, dim3 grid, int threads, size_t sme
 
 template <typename Real, int E>
 cudaError_t launch_cols_mix(const ColArgs& a, dim3 grid, int threads, size_t smem, cudaStream_t st) {
+    if (cols_mix_lean_ok(a)) {
+        if (a.src_spectrum) return launch_mix_kernel(k_cols_mix_asm<Real, E, true>, grid, threads, smem, st, &a);
+        return launch_mix_kernel(k_cols_mix_asm<Real, E, false>, grid, threads, smem, st, &a);
+    }
     if (smem > kSmemNoOptIn) {
         cudaError_t e = cudaFuncSetAttribute(k_cols<Real, E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
