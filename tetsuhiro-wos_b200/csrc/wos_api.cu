@@ -213,7 +213,9 @@ int auto_colw_p(wos_ctx c, int fp64, int L) {
     const int E = pick_E(fp64, L);
     const int T = L / E;
     const int maxt = max_threads_for(fp64, E);
-    int W = fp64 ? 4 : 8;
+    // complex64 mixed-radix lines take 4 columns (the lean column sweep at
+    // 768 points: 2.21 ms with 8 for 128 planes, 2.03 ms with 4)
+    int W = (fp64 || (L & (L - 1)) != 0) ? 4 : 8;
     while (W > 1 && (W * T > maxt || col_smem_bytes(fp64, L, W) > 200 * 1024)) W >>= 1;
     return W;
 }
@@ -514,7 +516,18 @@ int htab_of(wos_ctx c, FastCols& k, int L, int hilo) {
 }
 
 int attach_htab(wos_ctx c, FastCols& k, int L, int E) {
+    k.htab_global = 0;
     if (c->fp64 || !c->htab_on || !k.precise_phase || k.red || k.batch_wl || k.batch_z || L < 32) return WOS_OK;
+    if (c->htab_reg && !k.hist) {
+        // in registers from global memory (FastCols::htab_global), at the
+        // widths that variant is built for
+        const int Wg = fast_col_width(0, L, E, k.W);
+        if (Wg == 4 || (Wg == 8 && k.tw_lo)) {
+            TRY(htab_of(c, k, L, k.tw_lo != nullptr));
+            k.htab_global = 1;
+            return WOS_OK;
+        }
+    }
     const int W = fast_col_width(0, L, E, k.tiled ? kTileW : k.W);
     const int ld = htab_ld_for(L);
     if (W < 1 || k.ncols < 2 * W || k.ncols % (2 * W) != 0) return WOS_OK;

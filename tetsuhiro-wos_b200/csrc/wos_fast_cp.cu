@@ -24,6 +24,13 @@ cudaError_t fast_rows_bpm_cp(int L, int E, const FastRows& a, cudaStream_t st, i
 
 template <int L, int E>
 static cudaError_t go_cols_cp(const FastCols& a, cudaStream_t st, int* nblocks) {
+    if (a.htab_global) {  // H (hi + lo) from the table, in registers
+        switch (fast_col_width(0, L, E, a.W)) {
+        case 4: return go_cols_w<float, L, E, 4, true, false, true>(a, st, nblocks);
+        case 8: return go_cols_w<float, L, E, 8, true, false, true>(a, st, nblocks);
+        default: break;  // other widths: H from the table rows in shared memory
+        }
+    }
     switch (fast_col_width(0, L, E, a.W)) {
     case 1: return go_cols_w<float, L, E, 1, true>(a, st, nblocks);
     case 2: return go_cols_w<float, L, E, 2, true>(a, st, nblocks);

@@ -300,17 +300,28 @@ __global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, 
     double p0 = 0, l1 = 0;
     if constexpr (HG) {
         // v[s] holds frequency q = tt + s*T, where the inverse transform
-        // starts: H(|fx|, |fy|) from the table row of this column
-        static_assert(sizeof(Real) == 4 && !CP, "table in registers: plain complex64 sweeps");
+        // starts: H(|fx|, |fy|) from the table row of this column (CP: hi + lo
+        // entries, applied as x H_hi + x H_lo)
+        static_assert(sizeof(Real) == 4, "table in registers: complex64 sweeps");
         if (act) {
             const int cabs = col <= a.ncols / 2 ? col : a.ncols - col;
-            const float2* hr = a.htab + (long long)cabs * a.htab_ld;
             const float sg = a.conj ? -1.f : 1.f;
+            if constexpr (CP) {
+                const float4* hr = reinterpret_cast<const float4*>(a.htab) + (long long)cabs * a.htab_ld;
 #pragma unroll
-            for (int s = 0; s < E; s++) {
-                const int q = tt + s * (L / E);
-                const float2 t = __ldg(hr + (q <= L / 2 ? q : L - q));
-                v[s] = cmul(v[s], mkc<C>(t.x, sg * t.y));
+                for (int s = 0; s < E; s++) {
+                    const int q = tt + s * (L / E);
+                    const float4 t = __ldg(hr + (q <= L / 2 ? q : L - q));
+                    v[s] = cmul_cp(v[s], mkc<C>(t.x, sg * t.y), mkc<C>(t.z, sg * t.w));
+                }
+            } else {
+                const float2* hr = a.htab + (long long)cabs * a.htab_ld;
+#pragma unroll
+                for (int s = 0; s < E; s++) {
+                    const int q = tt + s * (L / E);
+                    const float2 t = __ldg(hr + (q <= L / 2 ? q : L - q));
+                    v[s] = cmul(v[s], mkc<C>(t.x, sg * t.y));
+                }
             }
         }
     } else {

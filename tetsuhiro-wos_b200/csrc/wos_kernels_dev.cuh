@@ -759,8 +759,10 @@ __device__ __forceinline__ C asm_tf_lean(const HArgs& h, double wl, double kz, d
     }
 }
 
-template <typename Real, int E, bool INV>
+// MODE: 0 forward, 1 inverse, 2 inverse with the weighted |E|^2 accumulated.
+template <typename Real, int E, int MODE>
 __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows_mix_lean(const RowArgs a) {
+    constexpr bool INV = MODE != 0;
     using C = typename CT<Real>::t;
     using T_ = Real;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -777,10 +779,10 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows_mix_lean(const RowArg
     C* const alt = sm + (size_t)row_line_stride(L) * lines;
     const C* tw = reinterpret_cast<const C*>(a.tw);
     const double yrow = gX(grow, a.ny_grid, a.dx);
-    const bool acc_mode = INV && a.mode == ROW_INV_ACC;
+    constexpr bool acc_mode = MODE == 2;
     const int nb = acc_mode ? a.acc_nb : 1;
     C v[E];
-    double iacc[E];
+    double iacc[acc_mode ? E : 1];
     for (int bb = 0; bb < nb; bb++) {
         const long long ibase = (long long)(acc_mode ? bb : bz) * a.in_bstride + (long long)r * a.in_ld;
 #pragma unroll
@@ -799,7 +801,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows_mix_lean(const RowArg
             v[s] = x;
         }
         mixed_line_fft<E, INV>(v, sm, alt, ix, line, tt, T, L, tw);
-        if (acc_mode) {
+        if constexpr (acc_mode) {
             const double wgt = a.acc_weight ? a.acc_weight[bb] : 1.0;
 #pragma unroll
             for (int s = 0; s < E; s++) {
@@ -815,7 +817,7 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_rows_mix_lean(const RowArg
         const int q = tt + s * T;
         if (!act || q < a.out_off || q >= a.out_off + a.out_n) continue;
         const int i = q - a.out_off;
-        if (acc_mode) {
+        if constexpr (acc_mode) {
             double* o = reinterpret_cast<double*>(a.out);
             o[obase + i] = (a.acc_add ? o[obase + i] : 0.0) + iacc[s];
             continue;
@@ -917,8 +919,9 @@ cudaError_t launch_mix_kernel(K kern, dim3 grid, int threads, size_t smem, cudaS
 template <typename Real, int E>
 cudaError_t launch_rows_mix(const RowArgs& a, dim3 grid, int threads, size_t smem, cudaStream_t st) {
     if (rows_mix_lean_ok(a)) {
-        if (a.mode == ROW_FWD) return launch_mix_kernel(k_rows_mix_lean<Real, E, false>, grid, threads, smem, st, &a);
-        return launch_mix_kernel(k_rows_mix_lean<Real, E, true>, grid, threads, smem, st, &a);
+        if (a.mode == ROW_FWD) return launch_mix_kernel(k_rows_mix_lean<Real, E, 0>, grid, threads, smem, st, &a);
+        if (a.mode == ROW_INV) return launch_mix_kernel(k_rows_mix_lean<Real, E, 1>, grid, threads, smem, st, &a);
+        return launch_mix_kernel(k_rows_mix_lean<Real, E, 2>, grid, threads, smem, st, &a);
     }
     if (smem > kSmemNoOptIn) {
         cudaError_t e = cudaFuncSetAttribute(k_rows<Real, E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
