@@ -137,7 +137,10 @@ int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const vo
     CK(timed_launch(c, 0, [&] { return fast_rows(c->fp64, nx, t.rowE, false, r, c->st, &nb); }));
     FastCols kc{};
     kc.ncols = nx;
-    kc.W = t.colW;
+    // complex64 with H from the table in registers: 4 columns a CTA (cfg3,
+    // 1024^2 x 400 slices: 10.64 ms with the table rows in shared memory at 8
+    // columns, 10.87 ms in registers at 8, 10.24 ms in registers at 4)
+    kc.W = (!c->fp64 && c->htab_reg && c->htab_on) ? 4 : t.colW;
     kc.data = S;
     kc.ld = nx;
     kc.bstride = np;
