@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libwosgpu.so")
-SOURCES = ["wos_kernels.cu", "wos_kernels_mix32.cu", "wos_kernels_mix64.cu", "wos_fast.cu", "wos_fast_cp.cu", "wos_schell.cu", "wos_aniso.cu", "wos_pipe.cu", "wos_elem.cu", "wos_api.cu", "wos_bpm.cu", "wos_batch.cu", "wos_design.cu", "wos_field_ops.cu", "wos_comm.cu", "wos_host.cu", "wos_static.cu"]
+SOURCES = ["wos_kernels.cu", "wos_kernels_mix32.cu", "wos_kernels_mix64.cu", "wos_fast.cu", "wos_fast_cp.cu", "wos_schell.cu", "wos_aniso.cu", "wos_pipe.cu", "wos_elem.cu", "wos_api.cu", "wos_bpm.cu", "wos_batch.cu", "wos_design.cu", "wos_field_ops.cu", "wos_comm.cu", "wos_host.cu", "wos_ctx.cu", "wos_static.cu"]
 HEADERS = ["wos_fft.cuh", "wos_kernels.cuh", "wos_kernels_dev.cuh", "wos_fast.cuh", "wos_fast_dev.cuh", "wos_fast_kern.cuh", "wos_pipe.cuh", "wos_api_internal.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [

@@ -1252,198 +1252,6 @@ void set_last_error(const char* msg) { g_err = msg; }
 
 extern "C" {
 
-const char* wos_backend_info(void) { return "B200 native (sm_100a): hand-written Stockham/Bluestein FFT, fused ASM sweeps"; }
-
-int wos_device_count(void) {
-    int n = 0;
-    if (cudaGetDeviceCount(&n) != cudaSuccess) {
-        cudaGetLastError();
-        return 0;
-    }
-    return n;
-}
-
-int wos_device_name(int device, char* buf, int buflen) {
-    if (!buf || buflen <= 0) return fail(WOS_INVALID_ARG, "null buffer");
-    cudaDeviceProp prop;
-    CK(cudaGetDeviceProperties(&prop, device));
-    std::snprintf(buf, (size_t)buflen, "%s", prop.name);
-    return WOS_OK;
-}
-
-int wos_ctx_create(int device, int precision, wos_ctx* out) {
-    if (!out) return fail(WOS_INVALID_ARG, "null out");
-    *out = nullptr;
-    if (precision != WOS_FP32 && precision != WOS_FP64) return fail(WOS_INVALID_ARG, "precision");
-    int n = wos_device_count();
-    if (n <= 0) return fail(WOS_NOT_INITIALISED, "no CUDA device");
-    if (device < 0 || device >= n) return fail(WOS_INVALID_ARG, "device index");
-    wos_ctx c = new wos_ctx_s();
-    c->device = device;
-    c->fp64 = precision == WOS_FP64;
-    cudaError_t e = cudaSetDevice(device);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-        delete c;
-        return fail(WOS_CUDA_ERROR, std::string("context creation: ") + cudaGetErrorString(e));
-    }
-    c->own_stream = true;
-    e = cudaMalloc(&c->err_dev, sizeof(unsigned));
-    if (e == cudaSuccess) e = cudaMemset(c->err_dev, 0, sizeof(unsigned));
-    if (e == cudaSuccess) e = cudaMallocHost(&c->err_host, sizeof(unsigned));
-    if (e != cudaSuccess) {
-        if (c->err_dev) cudaFree(c->err_dev);
-        cudaStreamDestroy(c->st);
-        delete c;
-        return fail(WOS_CUDA_ERROR, std::string("context creation: ") + cudaGetErrorString(e));
-    }
-    *c->err_host = 0;
-    c->col_pair = env_int("WOS_COLPAIR", 0);
-    c->tiled = env_int("WOS_TILED", 1);
-    c->bpm_comp = env_int("WOS_BPM_COMP", 1);
-    c->htab_on = env_int("WOS_HTAB", 1);
-    c->htab_reg = env_int("WOS_HTAB_REG", 1);
-    *out = c;
-    return WOS_OK;
-}
-
-int wos_ctx_destroy(wos_ctx c) {
-    if (!c) return WOS_OK;
-    comm_release(c);
-    {
-        std::lock_guard<std::mutex> lk(c->mu);
-        cudaSetDevice(c->device);
-        cudaStreamSynchronize(c->st);
-        if (c->pipe_made) {
-            cudaStreamSynchronize(c->h2d);
-            cudaStreamSynchronize(c->d2h);
-        }
-        host_release(c);
-        for (int pr = 0; pr < 2; pr++)
-            for (auto& kv : c->axes[pr]) {
-                cudaFree(kv.second.tw);
-                if (kv.second.chirp) cudaFree(kv.second.chirp);
-                if (kv.second.bf) cudaFree(kv.second.bf);
-                if (kv.second.bi) cudaFree(kv.second.bi);
-                for (void* t : kv.second.ftw)
-                    if (t) cudaFree(t);
-                for (void* t : kv.second.ftw_lo)
-                    if (t) cudaFree(t);
-                if (kv.second.ptw) cudaFree(kv.second.ptw);
-            }
-        for (auto& h : c->htab)
-            if (h.buf.p) cudaFree(h.buf.p);
-        for (auto& ps : c->pslot)
-            if (ps.buf.p) cudaFree(ps.buf.p);
-        DevBuf* bufs[] = {&c->stage, &c->scratch, &c->scratch2, &c->scratch3, &c->red, &c->redout, &c->tmp,
-                          &c->maps, &c->params, &c->vol, &c->accum, &c->aux};
-        for (DevBuf* b : bufs)
-            if (b->p) cudaFree(b->p);
-        for (DevBuf& b : c->tsc)
-            if (b.p) cudaFree(b.p);
-        if (c->bpm_tab.p) cudaFree(c->bpm_tab.p);
-        if (c->hred) cudaFreeHost(c->hred);
-        if (c->err_dev) cudaFree(c->err_dev);
-        if (c->err_host) cudaFreeHost(c->err_host);
-        for (int i = 0; i < c->naux; i++) {
-            cudaStreamDestroy(c->side[i]);
-            cudaEventDestroy(c->join_ev[i]);
-        }
-        if (c->fork_ev) cudaEventDestroy(c->fork_ev);
-        if (c->pipe_made) {
-            cudaStreamDestroy(c->h2d);
-            cudaStreamDestroy(c->d2h);
-            for (int i = 0; i < wos_ctx_s::kSlots; i++) {
-                if (c->slot[i].p) cudaFree(c->slot[i].p);
-                cudaEventDestroy(c->in_ev[i]);
-                cudaEventDestroy(c->done_ev[i]);
-                cudaEventDestroy(c->free_ev[i]);
-            }
-        }
-        if (c->prof_made)
-            for (int i = 0; i < wos_ctx_s::kRing; i++) {
-                cudaEventDestroy(c->ev0[i]);
-                cudaEventDestroy(c->ev1[i]);
-            }
-        if (c->own_stream) cudaStreamDestroy(c->st);
-    }
-    delete c;
-    return WOS_OK;
-}
-
-int wos_ctx_set_stream(wos_ctx c, void* stream) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    std::lock_guard<std::mutex> lk(c->mu);
-    if (c->own_stream) {
-        cudaStreamSynchronize(c->st);
-        cudaStreamDestroy(c->st);
-        c->own_stream = false;
-    }
-    c->st = reinterpret_cast<cudaStream_t>(stream);
-    return WOS_OK;
-}
-
-void* wos_ctx_get_stream(wos_ctx c) { return c ? reinterpret_cast<void*>(c->st) : nullptr; }
-
-int wos_ctx_precision(wos_ctx c) { return c ? (c->fp64 ? WOS_FP64 : WOS_FP32) : -1; }
-
-int wos_ctx_set_col_width(wos_ctx c, int w) {
-    if (!c || w < 0 || (w > 0 && (w & (w - 1)))) return fail(WOS_INVALID_ARG, "column width must be 0 or a power of two");
-    c->colw = w;
-    return WOS_OK;
-}
-
-int wos_ctx_set_profiling(wos_ctx c, int on) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    std::lock_guard<std::mutex> lk(c->mu);
-    if (on && !c->prof_made) {
-        CK(cudaSetDevice(c->device));
-        for (int i = 0; i < wos_ctx_s::kRing; i++) {
-            CK(cudaEventCreate(&c->ev0[i]));
-            CK(cudaEventCreate(&c->ev1[i]));
-            c->ev_used[i] = false;
-        }
-        c->prof_made = true;
-    }
-    c->prof_on = on != 0;
-    return WOS_OK;
-}
-
-int wos_ctx_profile(wos_ctx c, int kind, double* total_ms, long long* launches) {
-    if (!c || kind < 0 || kind > 7) return fail(WOS_INVALID_ARG, "profile kind");
-    std::lock_guard<std::mutex> lk(c->mu);
-    if (c->prof_made)
-        for (int i = 0; i < wos_ctx_s::kRing; i++) prof_fold(c, i);
-    if (total_ms) *total_ms = c->prof_ms[kind];
-    if (launches) *launches = c->prof_n[kind];
-    return WOS_OK;
-}
-
-int wos_ctx_profile_reset(wos_ctx c) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    std::lock_guard<std::mutex> lk(c->mu);
-    if (c->prof_made)
-        for (int i = 0; i < wos_ctx_s::kRing; i++) prof_fold(c, i);
-    for (int k = 0; k < 8; k++) {
-        c->prof_ms[k] = 0;
-        c->prof_n[k] = 0;
-    }
-    c->launches = 0;
-    return WOS_OK;
-}
-
-long long wos_ctx_launch_count(wos_ctx c) { return c ? c->launches : -1; }
-
-int wos_ctx_synchronize(wos_ctx c) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    CK(cudaMemcpyAsync(c->err_host, c->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    return check_err_word(c);
-}
-
-// ---- FFTs for the remaining fft2D / fft1DAny users
 int wos_fft2d_dev(wos_ctx c, int ny, int nx, int batch, void* a, int inverse) {
     if (!c || !a || ny < 2 || nx < 2 || batch < 1) return fail(WOS_INVALID_ARG, "fft2d_dev arguments");
     std::lock_guard<std::mutex> lk(c->mu);
@@ -1592,131 +1400,6 @@ int wos_propagate_batch_dev(wos_ctx c, int nfields, int ny, int nx, double dx, i
     return rc;
 }
 
-int wos_propagate_batch(wos_ctx c, int nfields, wos_field* fields, double z, int method, const wos_context* cci,
-                        wos_diag* diags) {
-    if (!c || nfields < 0 || (nfields > 0 && !fields)) return fail(WOS_INVALID_ARG, "batch arguments");
-    if (method < WOS_ASM || method > WOS_FRAUNHOFER) return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
-    for (int i = 0; i < nfields; i++) TRY(check_field(&fields[i]));
-    if (nfields == 0) return WOS_OK;
-    const wos_context cc = cci ? *cci : default_context();
-    if (z == 0) {
-        for (int i = 0; i < nfields && diags; i++) {
-            std::memset(&diags[i], 0, sizeof(diags[i]));
-            diags[i].dx_out = fields[i].dx;
-        }
-        return WOS_OK;
-    }
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    if (!c->pipe_made) {
-        CK(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
-        CK(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
-        for (int i = 0; i < wos_ctx_s::kSlots; i++) {
-            CK(cudaEventCreateWithFlags(&c->in_ev[i], cudaEventDisableTiming));
-            CK(cudaEventCreateWithFlags(&c->done_ev[i], cudaEventDisableTiming));
-            CK(cudaEventCreateWithFlags(&c->free_ev[i], cudaEventDisableTiming));
-            CK(cudaEventRecord(c->free_ev[i], c->d2h));
-        }
-        c->pipe_made = true;
-    }
-    bool staged = false;
-    for (int i = 0; i < nfields; i++)
-        staged = staged || host_pageable(fields[i].ex) || (fields[i].polarized && host_pageable(fields[i].ey));
-    if (staged) {
-        // pageable fields: host threads convert field i into the slot's
-        // page-locked staging (context precision), then copy, sweep and copy
-        // back; field i - kSlots is converted back when its slot comes round,
-        // so the host converts while the GPU runs the fields before it
-        const size_t esz = c->csz();
-        auto drain = [&](int j) -> int {
-            const int sl = j % wos_ctx_s::kSlots;
-            CK(cudaEventSynchronize(c->free_ev[sl]));
-            host_convert(c, fields[j], c->hst[sl], true);
-            return WOS_OK;
-        };
-        int rc = WOS_OK;
-        for (int i = 0; i < nfields && rc == WOS_OK; i++) {
-            const int sl = i % wos_ctx_s::kSlots;
-            if (i >= wos_ctx_s::kSlots && (rc = drain(i - wos_ctx_s::kSlots)) != WOS_OK) break;
-            wos_field& f = fields[i];
-            const int ncomp = f.polarized ? 2 : 1;
-            const size_t bytes = (size_t)f.ny * f.nx * ncomp * esz;
-            if ((rc = host_stage(c, sl, bytes)) != WOS_OK || (rc = ensure(c->slot[sl], bytes)) != WOS_OK) break;
-            host_convert(c, f, c->hst[sl], false);
-            CK(cudaMemcpyAsync(c->slot[sl].p, c->hst[sl], bytes, cudaMemcpyHostToDevice, c->h2d));
-            CK(cudaEventRecord(c->in_ev[sl], c->h2d));
-            CK(cudaStreamWaitEvent(c->st, c->in_ev[sl], 0));
-            wos_diag local;
-            wos_diag* d = diags ? &diags[i] : (method == WOS_FRAUNHOFER ? &local : nullptr);
-            Prop p{f.ny, f.nx, f.dx, ncomp, c->slot[sl].p, 0, c->slot[sl].p, 0, z, method, cc, d};
-            if ((rc = run_propagate(c, p)) != WOS_OK) break;
-            if (method == WOS_FRAUNHOFER) f.dx = d->dx_out;
-            CK(cudaEventRecord(c->done_ev[sl], c->st));
-            CK(cudaStreamWaitEvent(c->d2h, c->done_ev[sl], 0));
-            CK(cudaMemcpyAsync(c->hst[sl], c->slot[sl].p, bytes, cudaMemcpyDeviceToHost, c->d2h));
-            CK(cudaEventRecord(c->free_ev[sl], c->d2h));
-        }
-        for (int j = std::max(0, nfields - wos_ctx_s::kSlots); j < nfields && rc == WOS_OK; j++) rc = drain(j);
-        cudaStreamSynchronize(c->h2d);
-        cudaStreamSynchronize(c->d2h);
-        CK(cudaMemcpyAsync(c->err_host, c->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
-        CK(cudaStreamSynchronize(c->st));
-        if (rc != WOS_OK) return rc;
-        return check_err_word(c);
-    }
-    // field i lives in slot i % kSlots from its upload to its download; the
-    // upload of the next field is queued before field i's sweeps, so the two
-    // copy directions and the sweeps overlap (the sweeps stay in order on the
-    // context stream and share its workspace)
-    auto bytes_of = [&](int i) {
-        return (size_t)fields[i].ny * fields[i].nx * 16 * (fields[i].polarized ? 2 : 1);
-    };
-    auto upload = [&](int i) -> int {
-        const int sl = i % wos_ctx_s::kSlots;
-        const wos_field& f = fields[i];
-        const size_t np = (size_t)f.ny * f.nx;
-        CK(cudaStreamWaitEvent(c->h2d, c->free_ev[sl], 0));
-        TRY(ensure(c->slot[sl], bytes_of(i)));
-        CK(cudaMemcpyAsync(c->slot[sl].p, f.ex, np * 16, cudaMemcpyHostToDevice, c->h2d));
-        if (f.polarized)
-            CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->slot[sl].p) + np * 16, f.ey, np * 16,
-                               cudaMemcpyHostToDevice, c->h2d));
-        CK(cudaEventRecord(c->in_ev[sl], c->h2d));
-        return WOS_OK;
-    };
-    int rc = upload(0);
-    for (int i = 0; i < nfields && rc == WOS_OK; i++) {
-        const int sl = i % wos_ctx_s::kSlots;
-        if (i + 1 < nfields) {
-            rc = upload(i + 1);
-            if (rc != WOS_OK) break;
-        }
-        wos_field& f = fields[i];
-        const size_t np = (size_t)f.ny * f.nx;
-        const int ncomp = f.polarized ? 2 : 1;
-        CK(cudaStreamWaitEvent(c->st, c->in_ev[sl], 0));
-        wos_diag local;
-        wos_diag* d = diags ? &diags[i] : (method == WOS_FRAUNHOFER ? &local : nullptr);
-        Prop p{f.ny, f.nx, f.dx, ncomp, c->slot[sl].p, 1, c->slot[sl].p, 1, z, method, cc, d};
-        rc = run_propagate(c, p);
-        if (rc != WOS_OK) break;
-        if (method == WOS_FRAUNHOFER) f.dx = d->dx_out;
-        CK(cudaEventRecord(c->done_ev[sl], c->st));
-        CK(cudaStreamWaitEvent(c->d2h, c->done_ev[sl], 0));
-        CK(cudaMemcpyAsync(f.ex, c->slot[sl].p, np * 16, cudaMemcpyDeviceToHost, c->d2h));
-        if (ncomp == 2)
-            CK(cudaMemcpyAsync(f.ey, reinterpret_cast<char*>(c->slot[sl].p) + np * 16, np * 16,
-                               cudaMemcpyDeviceToHost, c->d2h));
-        CK(cudaEventRecord(c->free_ev[sl], c->d2h));
-    }
-    cudaStreamSynchronize(c->h2d);
-    cudaStreamSynchronize(c->d2h);
-    CK(cudaMemcpyAsync(c->err_host, c->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    if (rc != WOS_OK) return rc;
-    return check_err_word(c);
-}
-
 int wos_propagate(wos_ctx c, wos_field* f, double z, int method, const wos_context* cc, wos_diag* diag) {
     if (!c) return fail(WOS_INVALID_ARG, "null ctx");
     TRY(check_field(f));
@@ -1741,161 +1424,6 @@ int wos_propagate(wos_ctx c, wos_field* f, double z, int method, const wos_conte
     TRY(run_propagate(c, p));
     TRY(stage_out(c, f, ncomp));
     if (method == WOS_FRAUNHOFER) f->dx = p.diag->dx_out;
-    return WOS_OK;
-}
-
-struct wos_graph_s {
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    int device = 0;
-};
-
-int wos_graph_capture_begin(wos_ctx c) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
-    return WOS_OK;
-}
-
-int wos_graph_capture_end(wos_ctx c, wos_graph* out) {
-    if (!c || !out) return fail(WOS_INVALID_ARG, "null argument");
-    *out = nullptr;
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    cudaGraph_t g = nullptr;
-    cudaError_t e = cudaStreamEndCapture(c->st, &g);
-    if (e != cudaSuccess || !g) {
-        cudaGetLastError();
-        if (g) cudaGraphDestroy(g);
-        return fail(WOS_CUDA_ERROR, std::string("graph capture failed (a call inside it synchronised or failed): ") +
-                                        cudaGetErrorString(e));
-    }
-    cudaGraphExec_t x = nullptr;
-    e = cudaGraphInstantiate(&x, g, 0);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        cudaGraphDestroy(g);
-        return fail(WOS_CUDA_ERROR, std::string("graph instantiation: ") + cudaGetErrorString(e));
-    }
-    wos_graph h = new wos_graph_s();
-    h->graph = g;
-    h->exec = x;
-    h->device = c->device;
-    *out = h;
-    return WOS_OK;
-}
-
-int wos_graph_launch(wos_ctx c, wos_graph g) {
-    if (!c || !g) return fail(WOS_INVALID_ARG, "null argument");
-    if (g->device != c->device) return fail(WOS_INVALID_ARG, "graph captured on another device");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    CK(cudaGraphLaunch(g->exec, c->st));
-    return WOS_OK;
-}
-
-int wos_graph_destroy(wos_graph g) {
-    if (!g) return WOS_OK;
-    cudaSetDevice(g->device);
-    if (g->exec) cudaGraphExecDestroy(g->exec);
-    if (g->graph) cudaGraphDestroy(g->graph);
-    delete g;
-    return WOS_OK;
-}
-
-int wos_ctx_set_fast_path(wos_ctx c, int enabled) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    if (enabled < 0 || enabled > 3) return fail(WOS_INVALID_ARG, "fast path mode is 0, 1, 2 or 3");
-    std::lock_guard<std::mutex> lk(c->mu);
-    c->no_fast = enabled == 0;
-    c->sweep_mode = enabled == 0 ? 1 : enabled;
-    return WOS_OK;
-}
-
-int wos_ctx_set_tune(wos_ctx c, int ny, int nx, int row_e, int col_e, int col_w) {
-    if (!c) return fail(WOS_INVALID_ARG, "null ctx");
-    if (!fast_supported(c->fp64, nx, row_e) || !fast_supported(c->fp64, ny, col_e) || col_w < 1 ||
-        (col_w & (col_w - 1)))
-        return fail(WOS_INVALID_ARG, "unsupported launch configuration");
-    std::lock_guard<std::mutex> lk(c->mu);
-    c->tune[tune_key(c->fp64, ny, nx)] = Tune{row_e, col_e, col_w};
-    return WOS_OK;
-}
-
-// Times every launch configuration of the specialised ASM sweeps for an
-// ny x nx grid on this device (in-place propagations of a scratch field,
-// CUDA events on the context stream) and keeps the fastest for the context.
-int wos_autotune(wos_ctx c, int ny, int nx, int* row_e, int* col_e, int* col_w) {
-    if (!c || ny < 2 || nx < 2) return fail(WOS_INVALID_ARG, "autotune arguments");
-    std::lock_guard<std::mutex> lk(c->mu);
-    TRY(set_device(c));
-    const long long key = tune_key(c->fp64, ny, nx);
-    c->tune.erase(key);
-    const Tune def = get_tune(c, ny, nx);
-    if (!is_pow2(nx) || !is_pow2(ny)) {
-        if (row_e) *row_e = def.rowE;
-        if (col_e) *col_e = def.colE;
-        if (col_w) *col_w = def.colW;
-        return WOS_OK;
-    }
-    const long long np = (long long)ny * nx;
-    TRY(ensure(c->aux, (size_t)np * c->csz()));
-    CK(cudaMemsetAsync(c->aux.p, 0, (size_t)np * c->csz(), c->st));
-    wos_context cc = default_context();
-    cc.wavelength = 0.5e-6;
-    Prop p{ny, nx, 1e-6, 1, c->aux.p, 0, c->aux.p, 0, 1e-3, WOS_ASM, cc, nullptr};
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    // each configuration: two warm-up propagations, then the best of three
-    // rounds of ten (single-field timings vary by a few percent from round to
-    // round); the default is kept unless another is faster by more than 2 %
-    auto time_cfg = [&](const Tune& tn, float* out) {
-        c->tune[key] = tn;
-        bool ok = true;
-        for (int it = 0; it < 2 && ok; it++) ok = run_propagate(c, p) == WOS_OK;
-        float bestr = 1e30f;
-        for (int round = 0; round < 3 && ok; round++) {
-            cudaEventRecord(e0, c->st);
-            for (int it = 0; it < 10 && ok; it++) ok = run_propagate(c, p) == WOS_OK;
-            cudaEventRecord(e1, c->st);
-            cudaEventSynchronize(e1);
-            float ms = 0;
-            cudaEventElapsedTime(&ms, e0, e1);
-            bestr = std::min(bestr, ms);
-        }
-        if (!ok) cudaGetLastError();
-        *out = bestr;
-        return ok;
-    };
-    float best = 1e30f, tdef = 1e30f;
-    Tune bt = def;
-    const int es[2] = {8, 16};
-    for (int re : es)
-        for (int ce : es)
-            for (int w = 1; w <= 16; w <<= 1) {
-                if (!fast_supported(c->fp64, nx, re) || !fast_supported(c->fp64, ny, ce)) continue;
-                if (fast_col_width(c->fp64, ny, ce, w) != w || fast_col_smem(c->fp64, ny, ce, w) > 220 * 1024) continue;
-                float ms = 0;
-                if (!time_cfg(Tune{re, ce, w}, &ms)) continue;
-                if (re == def.rowE && ce == def.colE && w == def.colW) tdef = ms;
-                if (ms < best) {
-                    best = ms;
-                    bt = Tune{re, ce, w};
-                }
-            }
-    if (tdef <= best * 1.02f) bt = def;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    c->tune[key] = bt;
-    if (row_e) *row_e = bt.rowE;
-    if (col_e) *col_e = bt.colE;
-    // the width the ASM column sweep runs with: tiles of kTileW columns when
-    // the tiled intermediate applies (the tuned width then serves the other
-    // column sweeps of this grid, such as split-step slices)
-    const bool tiled = c->tiled && !c->fp64 && nx % kTileW == 0 && fast_col_width(c->fp64, ny, bt.colE, kTileW) == kTileW;
-    if (col_w) *col_w = tiled ? kTileW : bt.colW;
     return WOS_OK;
 }
 

@@ -1,4 +1,5 @@
-// wos_host.cu -- host-side staging of pageable fields.
+// wos_host.cu -- the host-field batch (wos_propagate_batch) and the
+// host-side staging of pageable fields.
 //
 // A Go caller passes its fields as ordinary (pageable) slices.  The driver
 // copies pageable memory through its own small bounce buffer, one direction at
@@ -144,3 +145,135 @@ void host_convert(wos_ctx c, wos_field& f, void* dst, bool to_host) {
 }
 
 }  // namespace wapi
+
+extern "C" {
+
+// PropagateBatch over host fields (no counterpart in the reference, which
+// propagates one field per call): copies and sweeps of consecutive fields
+// overlap; pageable fields go through the context's page-locked staging.
+int wos_propagate_batch(wos_ctx c, int nfields, wos_field* fields, double z, int method, const wos_context* cci,
+                        wos_diag* diags) {
+    if (!c || nfields < 0 || (nfields > 0 && !fields)) return fail(WOS_INVALID_ARG, "batch arguments");
+    if (method < WOS_ASM || method > WOS_FRAUNHOFER) return fail(WOS_UNKNOWN_METHOD, "unknown propagation method");
+    for (int i = 0; i < nfields; i++) TRY(check_field(&fields[i]));
+    if (nfields == 0) return WOS_OK;
+    const wos_context cc = cci ? *cci : default_context();
+    if (z == 0) {
+        for (int i = 0; i < nfields && diags; i++) {
+            std::memset(&diags[i], 0, sizeof(diags[i]));
+            diags[i].dx_out = fields[i].dx;
+        }
+        return WOS_OK;
+    }
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    if (!c->pipe_made) {
+        CK(cudaStreamCreateWithFlags(&c->h2d, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&c->d2h, cudaStreamNonBlocking));
+        for (int i = 0; i < wos_ctx_s::kSlots; i++) {
+            CK(cudaEventCreateWithFlags(&c->in_ev[i], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&c->done_ev[i], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&c->free_ev[i], cudaEventDisableTiming));
+            CK(cudaEventRecord(c->free_ev[i], c->d2h));
+        }
+        c->pipe_made = true;
+    }
+    bool staged = false;
+    for (int i = 0; i < nfields; i++)
+        staged = staged || host_pageable(fields[i].ex) || (fields[i].polarized && host_pageable(fields[i].ey));
+    if (staged) {
+        // pageable fields: host threads convert field i into the slot's
+        // page-locked staging (context precision), then copy, sweep and copy
+        // back; field i - kSlots is converted back when its slot comes round,
+        // so the host converts while the GPU runs the fields before it
+        const size_t esz = c->csz();
+        auto drain = [&](int j) -> int {
+            const int sl = j % wos_ctx_s::kSlots;
+            CK(cudaEventSynchronize(c->free_ev[sl]));
+            host_convert(c, fields[j], c->hst[sl], true);
+            return WOS_OK;
+        };
+        int rc = WOS_OK;
+        for (int i = 0; i < nfields && rc == WOS_OK; i++) {
+            const int sl = i % wos_ctx_s::kSlots;
+            if (i >= wos_ctx_s::kSlots && (rc = drain(i - wos_ctx_s::kSlots)) != WOS_OK) break;
+            wos_field& f = fields[i];
+            const int ncomp = f.polarized ? 2 : 1;
+            const size_t bytes = (size_t)f.ny * f.nx * ncomp * esz;
+            if ((rc = host_stage(c, sl, bytes)) != WOS_OK || (rc = ensure(c->slot[sl], bytes)) != WOS_OK) break;
+            host_convert(c, f, c->hst[sl], false);
+            CK(cudaMemcpyAsync(c->slot[sl].p, c->hst[sl], bytes, cudaMemcpyHostToDevice, c->h2d));
+            CK(cudaEventRecord(c->in_ev[sl], c->h2d));
+            CK(cudaStreamWaitEvent(c->st, c->in_ev[sl], 0));
+            wos_diag local;
+            wos_diag* d = diags ? &diags[i] : (method == WOS_FRAUNHOFER ? &local : nullptr);
+            Prop p{f.ny, f.nx, f.dx, ncomp, c->slot[sl].p, 0, c->slot[sl].p, 0, z, method, cc, d};
+            if ((rc = run_propagate(c, p)) != WOS_OK) break;
+            if (method == WOS_FRAUNHOFER) f.dx = d->dx_out;
+            CK(cudaEventRecord(c->done_ev[sl], c->st));
+            CK(cudaStreamWaitEvent(c->d2h, c->done_ev[sl], 0));
+            CK(cudaMemcpyAsync(c->hst[sl], c->slot[sl].p, bytes, cudaMemcpyDeviceToHost, c->d2h));
+            CK(cudaEventRecord(c->free_ev[sl], c->d2h));
+        }
+        for (int j = std::max(0, nfields - wos_ctx_s::kSlots); j < nfields && rc == WOS_OK; j++) rc = drain(j);
+        cudaStreamSynchronize(c->h2d);
+        cudaStreamSynchronize(c->d2h);
+        CK(cudaMemcpyAsync(c->err_host, c->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        if (rc != WOS_OK) return rc;
+        return check_err_word(c);
+    }
+    // field i lives in slot i % kSlots from its upload to its download; the
+    // upload of the next field is queued before field i's sweeps, so the two
+    // copy directions and the sweeps overlap (the sweeps stay in order on the
+    // context stream and share its workspace)
+    auto bytes_of = [&](int i) {
+        return (size_t)fields[i].ny * fields[i].nx * 16 * (fields[i].polarized ? 2 : 1);
+    };
+    auto upload = [&](int i) -> int {
+        const int sl = i % wos_ctx_s::kSlots;
+        const wos_field& f = fields[i];
+        const size_t np = (size_t)f.ny * f.nx;
+        CK(cudaStreamWaitEvent(c->h2d, c->free_ev[sl], 0));
+        TRY(ensure(c->slot[sl], bytes_of(i)));
+        CK(cudaMemcpyAsync(c->slot[sl].p, f.ex, np * 16, cudaMemcpyHostToDevice, c->h2d));
+        if (f.polarized)
+            CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->slot[sl].p) + np * 16, f.ey, np * 16,
+                               cudaMemcpyHostToDevice, c->h2d));
+        CK(cudaEventRecord(c->in_ev[sl], c->h2d));
+        return WOS_OK;
+    };
+    int rc = upload(0);
+    for (int i = 0; i < nfields && rc == WOS_OK; i++) {
+        const int sl = i % wos_ctx_s::kSlots;
+        if (i + 1 < nfields) {
+            rc = upload(i + 1);
+            if (rc != WOS_OK) break;
+        }
+        wos_field& f = fields[i];
+        const size_t np = (size_t)f.ny * f.nx;
+        const int ncomp = f.polarized ? 2 : 1;
+        CK(cudaStreamWaitEvent(c->st, c->in_ev[sl], 0));
+        wos_diag local;
+        wos_diag* d = diags ? &diags[i] : (method == WOS_FRAUNHOFER ? &local : nullptr);
+        Prop p{f.ny, f.nx, f.dx, ncomp, c->slot[sl].p, 1, c->slot[sl].p, 1, z, method, cc, d};
+        rc = run_propagate(c, p);
+        if (rc != WOS_OK) break;
+        if (method == WOS_FRAUNHOFER) f.dx = d->dx_out;
+        CK(cudaEventRecord(c->done_ev[sl], c->st));
+        CK(cudaStreamWaitEvent(c->d2h, c->done_ev[sl], 0));
+        CK(cudaMemcpyAsync(f.ex, c->slot[sl].p, np * 16, cudaMemcpyDeviceToHost, c->d2h));
+        if (ncomp == 2)
+            CK(cudaMemcpyAsync(f.ey, reinterpret_cast<char*>(c->slot[sl].p) + np * 16, np * 16,
+                               cudaMemcpyDeviceToHost, c->d2h));
+        CK(cudaEventRecord(c->free_ev[sl], c->d2h));
+    }
+    cudaStreamSynchronize(c->h2d);
+    cudaStreamSynchronize(c->d2h);
+    CK(cudaMemcpyAsync(c->err_host, c->err_dev, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (rc != WOS_OK) return rc;
+    return check_err_word(c);
+}
+
+}  // extern "C"
