@@ -287,38 +287,6 @@ __host__ __device__ constexpr size_t fcol_htab_off(int L, int E, int W) {
 }
 
 // ------------------------------------------------------------------- cols
-// sqrt of s in [2^-100, 1] to ~1e-13 relative without FP64<->FP32 conversion
-// instructions: the single-precision seed is assembled from the double's bit
-// fields (exponent rebias 1023 -> 127, mantissa truncated to 23 bits), its
-// reciprocal square root is taken in single precision, widened back by the
-// same rebias, and refined by one Newton step in FP64.
-__device__ __forceinline__ double fast_sqrt_bits(double s) {
-    const int hi = __double2hiint(s), lo = __double2loint(s);
-    const float sf = __int_as_float(__funnelshift_l(lo, hi - 0x38000000, 3));
-    const int rb = __float_as_int(rsqrtf(sf));
-    const double r0 = __hiloint2double((rb >> 3) + 0x38000000, (int)((unsigned)rb << 29));
-    const double y0 = s * r0;
-    return fma(0.5 * r0, fma(-y0, y0, s), y0);
-}
-
-// exp(2 pi i t) for |t| < 2^28 revolutions in single precision.  Adding
-// 1.5 * 2^29 rounds t to a multiple of 2^-23 and leaves that multiple, modulo
-// 2^23, in the low mantissa bits; sign-extending 23 of them gives the
-// fractional part in [-1/2, 1/2) as an integer, converted exactly through the
-// 1.5 * 2^23 float pattern.  `precise` evaluates sin/cos of that exact fraction
-// to about 1 ulp (sincospif, for transfer functions applied hundreds of times,
-// whose errors add up); otherwise the hardware approximation (absolute error
-// about 2^-21) serves a single application.
-__device__ __forceinline__ float2 cexp_rev(double t, bool precise) {
-    const double u = t + 805306368.0;  // 1.5 * 2^29
-    const int s23 = (int)((unsigned)__double2loint(u) << 9) >> 9;
-    const float f = __int_as_float(0x4b400000 + s23) - 12582912.0f;
-    float sn, cs;
-    if (precise) sincospif(f * 2.384185791015625e-07f, &sn, &cs);  // 2^-22: half-revolutions
-    else __sincosf(f * 7.490140565847857e-07f, &sn, &cs);            // 2 pi / 2^23
-    return make_float2(cs, sn);
-}
-
 // Radial histogram of |F|^2 (the spectrum before H) for the alias-wrap check
 // (spectralRadius, optics/propagate.go:270-310), added into hsm (97 bins,
 // zeroed by the caller) from the W columns held dense in the tile ([q][w]):

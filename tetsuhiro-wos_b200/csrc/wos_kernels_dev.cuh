@@ -742,17 +742,22 @@ template <> __device__ __forceinline__ float2 cexpi_lean<float2>(double arg) {
     return make_float2(cs, sn);
 }
 
-// asmTF with the complex64 phase through cexpi_lean; complex128 as asm_tf.
+// asmTF, complex64: 1 - (wl fx)^2 - (wl fy)^2 in FP64 from the column's
+// cx = 1 - (wl fx)^2, its square root from the single-precision seed plus one
+// FP64 Newton step, and the phase k z sqrt(.) taken in revolutions (krev =
+// k z / 2 pi, |krev| < 2^27) and reduced exactly before sin/cos in single
+// precision; complex128 as asm_tf, in the reference's operation order.
 template <typename C>
-__device__ __forceinline__ C asm_tf_lean(const HArgs& h, double wl, double kz, double kaz, bool backward, double fx,
-                                         double fy, double& m2) {
+__device__ __forceinline__ C asm_tf_lean(const HArgs& h, double wl, double kz, double kaz, double krev, double cx,
+                                         bool backward, double fx, double fy, double& m2) {
     if constexpr (sizeof(C) == 16) {
         return asm_tf<C>(h, wl, kz, kaz, backward, fx, fy, m2);
     } else {
-        const double ax = wl * fx, ay = wl * fy;
-        const double s = fma(-ay, ay, fma(-ax, ax, 1.0));
+        const double ay = wl * fy;
+        const double s = fma(-ay, ay, cx);
         if (s >= 0) {
             m2 = 1.0;
+            if (fabs(krev) < 0x1p27) return cexp_rev(krev * (s > 0x1p-100 ? fast_sqrt_bits(s) : 0.0), true);
             return cexpi_lean<C>(kz * sqrt(s));
         }
         return asm_tf<C>(h, wl, kz, kaz, backward, fx, fy, m2);
@@ -868,12 +873,18 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols_mix_asm(const ColArgs
     const double kz = (wl == h.wl && z == h.z) ? h.kz : k * z;
     const double kaz = (wl == h.wl && z == h.z) ? h.kaz : k * fabs(z);
     const double fx = h.fxoff != 0 ? dadd(freq_n(col, h.lfx, h.dx), h.fxoff) : freq_n(col, h.lfx, h.dx);
+    const double cx = fma(-(wl * fx), wl * fx, 1.0);
+    const double krev = kz * 0.15915494309189533577;
+    const double fyu = 1.0 / ((double)h.lfy * h.dx);  // complex64: fy by one multiply
 #pragma unroll
     for (int s = 0; s < E; s++) {
         const int q = tt + s * T;
-        const double fy = h.fyoff != 0 ? dadd(freq_n(q, h.lfy, h.dx), h.fyoff) : freq_n(q, h.lfy, h.dx);
+        double fy;
+        if constexpr (sizeof(C) == 16) fy = freq_n(q, h.lfy, h.dx);
+        else fy = (double)(q <= h.lfy / 2 ? q : q - h.lfy) * fyu;
+        if (h.fyoff != 0) fy = dadd(fy, h.fyoff);
         double m2;
-        C hh = asm_tf_lean<C>(h, wl, kz, kaz, z < 0, fx, fy, m2);
+        C hh = asm_tf_lean<C>(h, wl, kz, kaz, krev, cx, z < 0, fx, fy, m2);
         if (h.conj) hh.y = -hh.y;
         v[s] = cscale(cmul(v[s], hh), (T_)h.scale);
     }
