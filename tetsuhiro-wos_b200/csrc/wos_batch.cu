@@ -89,13 +89,16 @@ int try_fast_batch(wos_ctx c, Batch& b, std::vector<double>& sums, std::vector<d
     const bool diag = b.diag != nullptr;
     const bool schell = b.schell_sq != nullptr;
     if (schell && (diag || shared_in || ncomp != 1 || !schell_fast_size(nx) || nx != ny)) return -1;
+    // a shared input is column-transformed once; every unit's column sweep
+    // then starts from that spectrum (H, inverse)
+    const bool spec = shared_in && !diag && !schell && schell_fast_size(ny);
     Axis *ax, *ay;
     TRY(get_axis(c, nx, c->fp64, &ax));
     TRY(get_axis(c, ny, c->fp64, &ay));
     const void *twx, *twy, *twx8 = nullptr, *twy8 = nullptr;
     TRY(fast_tw(c, ax, t.rowE, &twx));
     TRY(fast_tw(c, ay, t.colE, &twy));
-    if (schell) {
+    if (schell || spec) {
         TRY(fast_tw(c, ax, 8, &twx8));
         TRY(fast_tw(c, ay, 8, &twy8));
     }
@@ -143,6 +146,22 @@ int try_fast_batch(wos_ctx c, Batch& b, std::vector<double>& sums, std::vector<d
                     CK(timed_launch(c, 0, [&] { return fast_rows_schell(c->fp64, nx, 8, r, c->st, &nb); }));
                 } else {
                     CK(timed_launch(c, 0, [&] { return fast_rows(c->fp64, nx, t.rowE, false, r, c->st, &nb); }));
+                }
+                if (spec) {  // the column spectrum of the shared input, once
+                    Axis* ag;
+                    TRY(get_axis(c, ny, c->fp64, &ag));
+                    ColArgs f = col_defaults(c, dx);
+                    f.mode = COL_FFT;
+                    f.ncols = nx;
+                    fill_axis(f, ag);
+                    f.W = auto_colw(c, ag->L);
+                    f.src = S0;
+                    f.src_ld = nx;
+                    f.in_n = ny;
+                    f.dst = S0;
+                    f.dst_ld = nx;
+                    f.out_n = ny;
+                    CK(prof_cols(c, c->fp64, f));
                 }
                 if (diag) {
                     const int per_unit = nb / r.batch;
@@ -192,6 +211,10 @@ int try_fast_batch(wos_ctx c, Batch& b, std::vector<double>& sums, std::vector<d
                 k.W = 4;
                 k.env_y = b.schell_g;
                 CK(timed_launch(c, 4, [&] { return fast_cols_env(c->fp64, ny, 8, k, c->st, &nb); }));
+            } else if (spec) {
+                k.tw = twy8;
+                k.W = 4;
+                CK(timed_launch(c, 4, [&] { return fast_cols_spec(c->fp64, ny, 8, k, c->st, &nb); }));
             } else {
                 CK(timed_launch(c, 4, [&] { return sweep_cols(c, ny, t.colE, k, &nb); }));
             }

@@ -102,8 +102,8 @@ struct FastCols {
     // memory to evaluate H once per (q, L - q) pair
     int htab_global;
     // Gaussian-Schell synthesis fused into the column sweep (instantiations
-    // with ENV): each column is inverse transformed, multiplied by env_y[y]
-    // and forward transformed before the transfer function
+    // with PRE = 1): each column is inverse transformed, multiplied by
+    // env_y[y] and forward transformed before the transfer function
     const double* env_y;
 };
 // Table rows of the W columns from col0 (W | ncols / 2): contiguous, in order
@@ -129,6 +129,9 @@ cudaError_t fast_rows(int fp64, int L, int E, bool inv, const FastRows& a, cudaS
 // L = 256 .. 4096.
 cudaError_t fast_rows_schell(int fp64, int L, int E, const FastRows& a, cudaStream_t st, int* nblocks);
 cudaError_t fast_cols_env(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks);
+// The column sweep of a batch whose source (a.src, shared: src_bstride 0) is
+// already column-transformed: H and the inverse only.
+cudaError_t fast_cols_spec(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks);
 cudaError_t fast_cols(int fp64, int L, int E, const FastCols& a, cudaStream_t st, int* nblocks);
 // The column sweep on two-CTA clusters (see FastCols::tw_half); returns
 // cudaErrorNotSupported outside its case (FP32, L = 2048, E = 16, W = 8, no

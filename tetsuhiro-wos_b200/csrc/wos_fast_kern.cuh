@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_bpm_fast(const FastR
 // transformed along x, multiplied by the x factor of the separable envelope
 // sqrt(I) = exp(-x^2/w^2) exp(-y^2/w^2) (env_x, with the generation's 1/nx
 // folded in) and transformed forward again.  The envelope's y factor and the
-// column transforms follow in the column sweep (k_cols_fast with ENV):
+// column transforms follow in the column sweep (k_cols_fast, PRE = 1):
 // operators along different axes commute, so the realization's inverse FFT2,
 // its envelope and the propagation's forward FFT2 take one pass over the data
 // per axis.
@@ -232,12 +232,15 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_schell_fast(const Fa
 // (optics/propagate.go:159-181) from an FP64 argument or from the table
 // (FastCols::htab), optional spectral sums and wrap histogram, inverse column
 // transform.  CP: compensated transforms (twiddle residuals from a.tw_lo) and
-// hi + lo table entries.  ENV (Gaussian-Schell batches after
-// k_rows_schell_fast): the column is first inverse transformed, multiplied by
-// env_y and transformed forward, so H meets the realization's spectrum.
+// hi + lo table entries.  PRE, what precedes H: 0 the forward column
+// transform of the loaded columns; 1 (Gaussian-Schell batches after
+// k_rows_schell_fast) an inverse transform, the factor env_y and the forward
+// transform, so H meets the realization's spectrum; 2 nothing: the source is
+// already the column spectrum (a batch's shared input, transformed once), loaded
+// where the forward transform would leave it.
 // HG (complex64, a.htab_global): H from the table in global memory, applied
 // in registers (no shared-memory spectrum stage, no H evaluation).
-template <typename Real, int L, int E, int W, bool CP = false, bool ENV = false, bool HG = false>
+template <typename Real, int L, int E, int W, bool CP = false, int PRE = 0, bool HG = false>
 __global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, E, W>::minb)
     k_cols_fast(const FastCols a) {
     pdl_wait();
@@ -268,7 +271,16 @@ __global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, 
         }
     }
     C v[E];
-    if constexpr (ENV) {
+    if constexpr (PRE == 2) {
+        if (act) {  // (shared by the batch's units: cached loads)
+            const C* src = sbase + (long long)tt * a.ld;
+#pragma unroll
+            for (int s = 0; s < E; s++) v[s] = __ldg(src + (long long)(s * (L / E)) * a.ld);
+        } else {
+#pragma unroll
+            for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
+        }
+    } else if constexpr (PRE == 1) {
         if (act) {
             const C* src = sbase + (long long)tt * a.ld;
 #pragma unroll
@@ -286,16 +298,23 @@ __global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, 
     } else {
         constexpr int R1 = PL::RS;
         if (act) {
+            // a source shared by the batch's units (src_bstride 0) is read by
+            // every unit: cached loads; otherwise streaming
             const C* src = sbase + (long long)tt * a.ld;
+            if (a.src && a.src_bstride == 0) {
 #pragma unroll
-            for (int s = 0; s < E; s++) v[s] = __ldcs(src + (long long)fpos<R1, E, L>(s, 0) * a.ld);
+                for (int s = 0; s < E; s++) v[s] = __ldg(src + (long long)fpos<R1, E, L>(s, 0) * a.ld);
+            } else {
+#pragma unroll
+                for (int s = 0; s < E; s++) v[s] = __ldcs(src + (long long)fpos<R1, E, L>(s, 0) * a.ld);
+            }
         } else {
 #pragma unroll
             for (int s = 0; s < E; s++) v[s] = mkc<C>(0, 0);
         }
     }
     // interleaved tile: stride W between consecutive positions of a column
-    fpasses<L, E, false, 0, W, C, CP>(v, smb, tt, twp, twl);
+    if constexpr (PRE != 2) fpasses<L, E, false, 0, W, C, CP>(v, smb, tt, twp, twl);
 
     double p0 = 0, l1 = 0;
     if constexpr (HG) {
@@ -369,7 +388,7 @@ inline cudaError_t go_rows_schell(const FastRows& a, cudaStream_t st, int* nbloc
     return launch_sweep(k_rows_schell_fast<Real, L, E>, grid, lines * T, smem, st, a);
 }
 
-template <typename Real, int L, int E, int W, bool CP = false, bool ENV = false, bool HG = false>
+template <typename Real, int L, int E, int W, bool CP = false, int PRE = 0, bool HG = false>
 inline cudaError_t go_cols_w(const FastCols& a, cudaStream_t st, int* nblocks) {
     constexpr int T = L / E;
     if constexpr (W * T < 32 || W * T > fcol_max_threads(sizeof(Real) == 8, T)) {
@@ -379,13 +398,13 @@ inline cudaError_t go_cols_w(const FastCols& a, cudaStream_t st, int* nblocks) {
         if (sizeof(Real) == 4 && a.htab && !a.htab_global && !HG)
             smem = fcol_htab_off(L, E, W) + (size_t)W * a.htab_ld * sizeof(float2) * (CP ? 2 : 1);
         if (smem > kSmemNoOptIn) {
-            cudaError_t e = cudaFuncSetAttribute(k_cols_fast<Real, L, E, W, CP, ENV, HG>,
+            cudaError_t e = cudaFuncSetAttribute(k_cols_fast<Real, L, E, W, CP, PRE, HG>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
         }
         dim3 grid((a.ncols + W - 1) / W, a.batch > 0 ? a.batch : 1);
         if (nblocks) *nblocks = (int)(grid.x * grid.y);
-        return launch_sweep(k_cols_fast<Real, L, E, W, CP, ENV, HG>, grid, W * T, smem, st, a);
+        return launch_sweep(k_cols_fast<Real, L, E, W, CP, PRE, HG>, grid, W * T, smem, st, a);
     }
 }
 
