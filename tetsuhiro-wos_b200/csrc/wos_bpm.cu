@@ -137,10 +137,13 @@ int try_fast_splitstep(wos_ctx c, int ny, int nx, double dx, int ncomp, const vo
     CK(timed_launch(c, 0, [&] { return fast_rows(c->fp64, nx, t.rowE, false, r, c->st, &nb); }));
     FastCols kc{};
     kc.ncols = nx;
-    // complex64 with H from the table in registers: 4 columns a CTA (cfg3,
-    // 1024^2 x 400 slices: 10.64 ms with the table rows in shared memory at 8
-    // columns, 10.87 ms in registers at 8, 10.24 ms in registers at 4)
-    kc.W = (!c->fp64 && c->htab_reg && c->htab_on) ? 4 : t.colW;
+    // complex64 with H from the table in registers, on a field that stays in
+    // L2 from slice to slice: 4 columns a CTA (cfg3, 1024^2 x 400 slices:
+    // 10.64 ms with the table rows in shared memory at 8 columns, 10.87 ms in
+    // registers at 8, 10.24 ms in registers at 4).  Larger fields keep the
+    // tuned width, whose wider row segments the DRAM traffic needs.
+    const bool l2_field = (size_t)np * ncomp * c->csz() <= ((size_t)16 << 20);
+    kc.W = (!c->fp64 && c->htab_reg && c->htab_on && l2_field) ? 4 : t.colW;
     kc.data = S;
     kc.ld = nx;
     kc.bstride = np;
@@ -400,6 +403,16 @@ int bpm_stack_impl(wos_ctx c, int ny, int nx, double dx, int nl, const void* a, 
     ScreenSrc src;
     src.kind = 1;
     src.desc = medium;
+    // The stack's slices run the plain complex64 sweeps: the compensated ones
+    // left its FP32 loss and gradients where they were (6.2e-5 and 6.6e-5
+    // against the FP64 pipeline, 2048^2, 3 masks x 200 slices) at 98 ms
+    // instead of 69 ms.
+    struct CompOff {
+        wos_ctx c;
+        int keep;
+        explicit CompOff(wos_ctx cc) : c(cc), keep(cc->bpm_comp) { c->bpm_comp = 0; }
+        ~CompOff() { c->bpm_comp = keep; }
+    } comp_off(c);
     for (int l = 0; l < nl; l++) {
         CK(launch_mask_phase(c->fp64, U, phis + (size_t)l * np, np, 0, c->st));
         CK(cudaMemcpyAsync(V + (size_t)l * fb, U, fb, cudaMemcpyDeviceToDevice, c->st));
