@@ -84,7 +84,7 @@ def test_wrap_histogram_fast_equals_general(prec, n):
     assert res[0][0] == O.spectral_radius(o, 0.90)
 
 
-def _dev_propagate(g, prec, ex, ey, dx, z, wl, mode):
+def _dev_propagate(g, prec, ex, ey, dx, z, wl, mode, diag=True):
     """propagate_dev on device buffers of the context precision (the layout the
     pipelined sweeps take), returning the fields and the diagnostics."""
     import torch
@@ -95,9 +95,28 @@ def _dev_propagate(g, prec, ex, ey, dx, z, wl, mode):
     torch.cuda.synchronize()  # the context's stream does not wait for torch's
     ny, nx = ex.shape
     c = wos.Context(wavelength=wl)
-    d = g.propagate_dev(ny, nx, dx, len(comps), buf.data_ptr(), buf.data_ptr(), z, "asm", c, diag=True)
+    d = g.propagate_dev(ny, nx, dx, len(comps), buf.data_ptr(), buf.data_ptr(), z, "asm", c, diag=diag)
     g.synchronize()
     return buf.cpu().numpy().astype(np.complex128), d, c
+
+
+@pytest.mark.parametrize("shape", [(256, 256), (2048, 2048), (256, 1024), (1024, 256)])
+@pytest.mark.parametrize("ncomp", [1, 2])
+@pytest.mark.parametrize("z", [2e-3, -2e-3])
+def test_fp64_h_table_equals_evaluated_h(shape, ncomp, z):
+    """Without diagnostics the pipelined complex128 column sweep reads H from
+    the table of its FP64 values; the one-shot sweep (mode 2) evaluates H in
+    the reference's operation order: the fields agree element for element,
+    forward and backward."""
+    ny, nx = shape
+    dx, wl = 2e-6, 632.8e-9
+    rng = np.random.default_rng(ny + 3 * nx + ncomp)
+    ex = np.exp(1j * rng.uniform(0, 2 * np.pi, (ny, nx)))
+    ey = 0.5 * np.exp(1j * rng.uniform(0, 2 * np.pi, (ny, nx))) if ncomp == 2 else None
+    with wos.GPU(wos.FP64) as g:
+        a, _, _ = _dev_propagate(g, wos.FP64, ex, ey, dx, z, wl, 1, diag=False)
+        b, _, _ = _dev_propagate(g, wos.FP64, ex, ey, dx, z, wl, 2, diag=False)
+    assert np.array_equal(a, b)
 
 
 @pytest.mark.parametrize("prec", [wos.FP64, wos.FP32], ids=["fp64", "fp32"])

@@ -549,6 +549,17 @@ int attach_htab_global(wos_ctx c, FastCols& k, int L) {
     return WOS_OK;
 }
 
+// The complex128 table (FP64 values of H, 16-byte entries) for the pipelined
+// complex128 column sweep, which reads it into registers; its entries are the
+// values the sweep would evaluate, so the results do not change.
+int attach_htab64(wos_ctx c, FastCols& k, int L) {
+    if (!c->fp64 || !c->htab_reg || c->sweep_mode == 2 || k.red || k.hist || k.batch_wl || k.batch_z || L < 32)
+        return WOS_OK;
+    TRY(htab_of(c, k, L, 2));
+    k.htab_global = 1;
+    return WOS_OK;
+}
+
 // Plain band-limited ASM on power-of-two grids through the specialised
 // sweeps.  Returns -1 when the grid is not covered (the general sweeps run).
 // One specialised sweep: the pipelined kernel where the sweep mode asks for it
@@ -596,7 +607,9 @@ cudaError_t sweep_cols(wos_ctx c, int L, int E, const FastCols& a, int* nb) {
             if (e != cudaErrorNotSupported) return e;
         }
     }
-    if (c->sweep_mode != 2 && !a.tiled && !a.tw_lo && !a.htab) {  // (table / compensated: one-shot kernels)
+    // (complex64 table or compensated: one-shot kernels; the complex128
+    // pipelined sweep reads its table itself)
+    if (c->sweep_mode != 2 && !a.tiled && !a.tw_lo && (!a.htab || (c->fp64 && a.htab_global))) {
         FastCols b = a;
         b.err = c->err_dev;
         const cudaError_t e = pipe_cols(c->fp64, L, E, b, c->st, nb);
@@ -695,6 +708,7 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
         k.hist_dx = p.dx;
     }
     if (tiled) TRY(attach_htab_global(c, k, p.ny));
+    else TRY(attach_htab64(c, k, p.ny));
     CK(timed_launch(c, 4, [&] { return sweep_cols(c, p.ny, t.colE, k, &nb); }));
     if (s.red_loss) CK(launch_reduce_finish(red_region(c, 1), nb, 1, RS_SW, 2, redout_region(c, 1), c->st));
     if (s.hist) CK(launch_reduce_finish(red_region(c, 1), nb, 1, RS_HIST, 97, redout_region(c, 1), c->st));
@@ -1359,11 +1373,12 @@ int wos_propagate_batch_dev(wos_ctx c, int nfields, int ny, int nx, double dx, i
                 if (!pair_tables(c, ny, t.colE, &th, &tp)) return fail(WOS_CUDA_ERROR, "split-tile tables");
             }
             // the transfer-function table the (tiled) column sweeps read
-            if (asm_tiled(c, ny, nx, t)) {
+            {
                 FastCols hk{};
                 hk.ncols = nx;
                 fill_asm_h(hk, asm_h(c, cc, z, ev_policy(cc, z), dx, nx, ny));
-                TRY(attach_htab_global(c, hk, ny));
+                if (asm_tiled(c, ny, nx, t)) TRY(attach_htab_global(c, hk, ny));
+                else TRY(attach_htab64(c, hk, ny));
             }
             nstreams = std::max(1, std::min(wos_ctx_s::kMaxAux, env_int("WOS_STREAMS", 2)));
         }

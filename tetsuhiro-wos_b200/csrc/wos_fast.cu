@@ -469,6 +469,10 @@ __global__ void k_htab_build(const FastCols a, int L, float2* out, int ld, int h
         double m2;
         h = h_f64(a, hu, px, fy, m2);
     }
+    if (hilo == 2) {  // complex128 entries (the FP64 pipeline)
+        reinterpret_cast<double2*>(out)[(long long)cx * ld + q] = h;
+        return;
+    }
     const float hx = (float)h.x, hy = (float)h.y;
     if (hilo) {
         reinterpret_cast<float4*>(out)[(long long)cx * ld + q] =

@@ -115,9 +115,10 @@ __host__ __device__ inline int htab_row0(int col0, int ncols, int W) {
 // L/2 + 8 >= L/2 + 1 entries, so rows are whole 16-byte units and consecutive
 // rows start 16 shared-memory banks apart.
 inline int htab_ld_for(int L) { return L / 2 + 8; }
-// Build the table of a's transfer function for columns of L points (the FP32
-// pipeline's H arguments in a, with conj ignored); hilo: (H_hi, H_lo) pairs of
-// float2 per entry, for the compensated sweeps (which read them as such).
+// Build the table of a's transfer function for columns of L points (the H
+// arguments in a, with conj ignored); hilo 0: float2 entries, 1: (H_hi, H_lo)
+// pairs of float2 per entry, for the compensated sweeps (which read them as
+// such), 2: double2 entries, for the complex128 pipeline.
 cudaError_t fast_build_htab(const FastCols& a, int L, float2* out, int ld, int hilo, cudaStream_t st);
 // Shared memory of a complex64 column CTA with the table rows.
 size_t fast_col_smem_htab(int L, int E, int W, int ld, int hilo);

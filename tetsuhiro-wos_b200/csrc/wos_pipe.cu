@@ -265,7 +265,27 @@ __global__ void __launch_bounds__(FColB<Real, L, E, W>::threads, FColB<Real, L, 
 #pragma unroll
         for (int s = 0; s < E; s++) v[s] = stg[fpos<R1, E, L>(s, tt) * W + w];
         fpasses<L, E, false, 0, W>(v, stg + w, tt, twp);
-        col_spectral_stage<Real, L, E, W>(v, stg, hsm, c0, a, h_unit(a, b), p0, l1);
+        bool h_done = false;
+        if constexpr (sizeof(Real) == 8) {
+            if (a.htab_global) {
+                // complex128 H from the table (the same FP64 values the stage
+                // would evaluate), at the frequencies q = tt + s*T the forward
+                // transform leaves in v
+                if (act) {
+                    const int cabs = col <= a.ncols / 2 ? col : a.ncols - col;
+                    const double2* hr = reinterpret_cast<const double2*>(a.htab) + (long long)cabs * a.htab_ld;
+                    const double sg = a.conj ? -1.0 : 1.0;
+#pragma unroll
+                    for (int s = 0; s < E; s++) {
+                        const int q = tt + s * (L / E);
+                        const double2 t = __ldg(hr + (q <= L / 2 ? q : L - q));
+                        v[s] = cmul(v[s], make_double2(t.x, sg * t.y));
+                    }
+                }
+                h_done = true;
+            }
+        }
+        if (!h_done) col_spectral_stage<Real, L, E, W>(v, stg, hsm, c0, a, h_unit(a, b), p0, l1);
         fpasses<L, E, true, 0, W>(v, stg + w, tt, twp);
         if (act) {
             constexpr int RO = PL::RS;
