@@ -16,6 +16,7 @@
 // scaling) and the host loops of optics/propagate.go:132-148,339-387,426-504.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <stdlib.h>
 #include <stdint.h>
 
 #include <algorithm>
@@ -223,9 +224,19 @@ __global__ void k_scale_copy(const double2* src, C* dst, long long n, double sre
 }
 
 // ------------------------------------------------------------------ launchers
-// Elements per thread: 16 (FP32) / 8 (FP64, 16 for lines of 8192), never more than L.
+// Elements per thread: 16 (FP32) / 8 (FP64, 16 for lines of 8192), never more
+// than L; WOS_MIXE (4, 8 or 16) sets the start for mixed-radix lines.
+static int mix_e_override() {
+    static const int v = [] {
+        const char* e = getenv("WOS_MIXE");
+        const int x = e ? atoi(e) : 0;
+        return (x == 4 || x == 8 || x == 16) ? x : 0;
+    }();
+    return v;
+}
 int pick_E(int fp64, int L) {
     int e = fp64 ? (L >= 8192 ? 16 : 8) : 16;
+    if ((L & (L - 1)) != 0 && mix_e_override()) e = mix_e_override();
     while (e > L) e >>= 1;
     while (e > 2 && L % e != 0) e >>= 1;  // a mixed-radix line: E divides L
     // a long line whose threads would not fit one CTA takes more values per thread

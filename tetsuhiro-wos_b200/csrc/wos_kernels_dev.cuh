@@ -897,12 +897,61 @@ __global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols_mix_asm(const ColArgs
     }
 }
 
+// The spectral-centroid sums of mixed-radix columns (COL_REDUCE without the
+// histogram): forward transform, then |F|^2, |F|^2 fx and |F|^2 fy added with
+// compensation, as the general sweep adds them.
+template <typename Real, int E>
+__global__ void __launch_bounds__(MaxT<Real, E>::v) k_cols_mix_reduce(const ColArgs a) {
+    using C = typename CT<Real>::t;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C* sm = reinterpret_cast<C*>(smraw);
+    const int L = a.L;
+    const int T = L / E;
+    const int W = a.W;
+    const int w = threadIdx.x & (W - 1);
+    const int tt = threadIdx.x / W;
+    const int col = blockIdx.x * W + w;
+    const bool act = col < a.ncols;
+    const int bz = blockIdx.y;
+    const ColIdx ix{W};
+    C* const alt = sm + (size_t)col_tile_elems(L, W);
+    const C* tw = reinterpret_cast<const C*>(a.tw);
+    C v[E];
+    const C* src = reinterpret_cast<const C*>(a.src) + (a.src_shared ? 0 : (long long)bz * a.src_bstride);
+#pragma unroll
+    for (int s = 0; s < E; s++) {
+        const int p = tt + s * T;
+        C x = mkc<C>(0, 0);
+        if (act && p >= a.in_off && p < a.in_off + a.in_n) x = src[(long long)(p - a.in_off) * a.src_ld + col];
+        v[s] = x;
+    }
+    mixed_line_fft<E, false>(v, sm, alt, ix, w, tt, T, L, tw);
+    double acc[3] = {0, 0, 0}, spc[3] = {0, 0, 0};
+    if (act) {
+        const double hfx = freq_n(col, a.hist_lx, a.hist_dx);
+#pragma unroll
+        for (int s = 0; s < E; s++) {
+            const int q = tt + s * T;
+            const double pw = (double)v[s].x * v[s].x + (double)v[s].y * v[s].y;
+            const double fy = freq_n(q, a.hist_ly, a.hist_dx);
+            neumaier_add(acc[0], spc[0], pw);
+            neumaier_add(acc[1], spc[1], pw * hfx);
+            neumaier_add(acc[2], spc[2], pw * fy);
+        }
+    }
+    double* out = a.red + ((long long)blockIdx.y * gridDim.x + blockIdx.x) * RS_COUNT;
+    block_sum2_write<3>(acc, spc, out + RS_SW, out + RS_SLO);
+}
+
 // Whether a general launch can take the lean kernels above (mixed lines only).
 __host__ inline bool rows_mix_lean_ok(const RowArgs& a) {
     if (a.blue_n || a.red || a.pre_phi || a.pre_phi_f || a.scr.kind) return false;
     if (a.mode == ROW_INV_ACC) return a.out_accum_int == 2;
     return (a.mode == ROW_FWD || a.mode == ROW_INV) && a.out_accum_int == 0 && (a.mode == ROW_FWD || !a.pre_shift) &&
            (a.mode == ROW_INV || !a.post_shift);
+}
+__host__ inline bool cols_mix_reduce_ok(const ColArgs& a) {
+    return a.mode == COL_REDUCE && a.red && a.red_spec && !a.red_hist && !a.red_bpm && !a.blue_n;
 }
 __host__ inline bool cols_mix_lean_ok(const ColArgs& a) {
     return a.mode == COL_FUSED && a.h.kind == H_ASM && !a.blue_n && !a.red && !a.red_spec && !a.red_hist &&
@@ -949,6 +998,7 @@ cudaError_t launch_cols_mix(const ColArgs& a, dim3 grid, int threads, size_t sme
         if (a.src_spectrum) return launch_mix_kernel(k_cols_mix_asm<Real, E, true>, grid, threads, smem, st, &a);
         return launch_mix_kernel(k_cols_mix_asm<Real, E, false>, grid, threads, smem, st, &a);
     }
+    if (cols_mix_reduce_ok(a)) return launch_mix_kernel(k_cols_mix_reduce<Real, E>, grid, threads, smem, st, &a);
     if (smem > kSmemNoOptIn) {
         cudaError_t e = cudaFuncSetAttribute(k_cols<Real, E, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
