@@ -215,8 +215,11 @@ int auto_colw_p(wos_ctx c, int fp64, int L) {
     const int maxt = max_threads_for(fp64, E);
     // complex64 mixed-radix lines take 4 columns (the lean column sweep at
     // 768 points: 2.21 ms with 8 for 128 planes, 2.03 ms with 4)
-    int W = (fp64 || (L & (L - 1)) != 0) ? 4 : 8;
-    while (W > 1 && (W * T > maxt || col_smem_bytes(fp64, L, W) > 200 * 1024)) W >>= 1;
+    const bool mixed = (L & (L - 1)) != 0;
+    int W = (fp64 || mixed) ? 4 : 8;
+    // mixed-radix columns run between two tile buffers
+    const size_t bufs = mixed ? 2 : 1;
+    while (W > 1 && (W * T > maxt || bufs * col_smem_bytes(fp64, L, W) > 200 * 1024)) W >>= 1;
     return W;
 }
 

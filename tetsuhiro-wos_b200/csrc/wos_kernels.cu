@@ -224,8 +224,10 @@ __global__ void k_scale_copy(const double2* src, C* dst, long long n, double sre
 }
 
 // ------------------------------------------------------------------ launchers
-// Elements per thread: 16 (FP32) / 8 (FP64, 16 for lines of 8192), never more
-// than L; WOS_MIXE (4, 8 or 16) sets the start for mixed-radix lines.
+// Elements per thread: 16 (FP32 power-of-two lines) / 8 (FP32 mixed-radix
+// lines; FP64, 16 for lines of 8192), never more than L; WOS_MIXE (4, 8 or 16)
+// sets the start for mixed-radix lines.  (Complex64 mixed lines at 8 rather
+// than 16: 128 planes of 768^2 1.90 -> 1.78 ms, cfg2 0.527 -> 0.510 ms.)
 static int mix_e_override() {
     static const int v = [] {
         const char* e = getenv("WOS_MIXE");
@@ -235,8 +237,9 @@ static int mix_e_override() {
     return v;
 }
 int pick_E(int fp64, int L) {
-    int e = fp64 ? (L >= 8192 ? 16 : 8) : 16;
-    if ((L & (L - 1)) != 0 && mix_e_override()) e = mix_e_override();
+    const bool mixed = (L & (L - 1)) != 0;
+    int e = fp64 ? (L >= 8192 ? 16 : 8) : (mixed ? 8 : 16);
+    if (mixed && mix_e_override()) e = mix_e_override();
     while (e > L) e >>= 1;
     while (e > 2 && L % e != 0) e >>= 1;  // a mixed-radix line: E divides L
     // a long line whose threads would not fit one CTA takes more values per thread
