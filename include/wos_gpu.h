@@ -500,7 +500,10 @@ WOS_API int wos_asm_adjoint(wos_ctx ctx, wos_field* f, double z, const wos_conte
  *      allocated or built while capturing) and must not ask for diagnostics
  *      or return values that need a synchronisation (a call that does fails
  *      and the capture with it).  Replays use the buffers and parameters of
- *      the capture. ---- */
+ *      the capture: the transfer-function tables and device copies of
+ *      parameter lists a capture uses are kept as they are until the context
+ *      is destroyed (later calls with other distances or lists take other
+ *      entries). ---- */
 WOS_API int wos_graph_capture_begin(wos_ctx ctx);
 WOS_API int wos_graph_capture_end(wos_ctx ctx, wos_graph* out);
 WOS_API int wos_graph_launch(wos_ctx ctx, wos_graph g);

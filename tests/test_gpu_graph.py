@@ -36,6 +36,47 @@ def _fields(gpu, k, n, seed=1):
 CTX = dict(wavelength=632.8e-9, warnings_enabled=False)
 
 
+def test_graph_keeps_its_tables_while_other_calls_evict(gpu):
+    """A graph reads the transfer-function table and the parameter lists of its
+    capture even after later direct calls with many other distances and
+    wavelength lists have cycled the context's caches."""
+    import torch
+    n, dx, z = 512, 2e-6, 5e-3
+    (x,) = _fields(gpu, 1, n, seed=3)
+    y = torch.empty_like(x)
+    want = torch.empty_like(x)
+    wls = np.linspace(500e-9, 600e-9, 3)
+    pw = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    pw_want = torch.empty_like(pw)
+    torch.cuda.synchronize()
+
+    def calls(out, pout):
+        gpu.propagate_dev(n, n, dx, 1, x.data_ptr(), out.data_ptr(), z, "asm", wos.Context(**CTX))
+        gpu.polychromatic_dev(n, n, dx, 1, x.data_ptr(), z, wls, np.ones(3), wos.Context(**CTX), pout.data_ptr())
+
+    calls(want, pw_want)
+    gpu.synchronize()
+    gpu.graph_capture_begin()
+    calls(y, pw)
+    g = gpu.graph_capture_end()
+    scratch = torch.empty_like(x)
+    sp = torch.empty_like(pw)
+    for q in range(12):  # other distances and wavelength lists, more than either cache holds
+        gpu.propagate_dev(n, n, dx, 1, x.data_ptr(), scratch.data_ptr(), z * (1.1 + 0.1 * q), "asm",
+                          wos.Context(**CTX))
+        gpu.polychromatic_dev(n, n, dx, 1, x.data_ptr(), z, wls * (1.01 + 0.01 * q), np.ones(3),
+                              wos.Context(**CTX), sp.data_ptr())
+    gpu.synchronize()
+    y.zero_()
+    pw.zero_()
+    torch.cuda.synchronize()
+    g.launch()
+    gpu.synchronize()
+    assert torch.equal(y, want)
+    assert torch.equal(pw, pw_want)
+    g.close()
+
+
 def test_graph_replays_single_calls(gpu):
     import torch
     n, dx, z = 512, 2e-6, 5e-3

@@ -497,12 +497,23 @@ int htab_of(wos_ctx c, FastCols& k, int L, int hilo) {
                            (double)(k.reg + 2 * k.backward + 4 * hilo)};
     for (auto& h : c->htab)
         if (h.valid && h.L == L && h.ncols == k.ncols && std::memcmp(h.key, key, sizeof key) == 0) {
+            if (c->capturing) h.frozen = true;
             k.htab = reinterpret_cast<const float2*>(h.buf.p);
             k.htab_ld = ld;
             return WOS_OK;
         }
-    wos_ctx_s::HTab& h = c->htab[c->htab_next];
-    c->htab_next = (c->htab_next + 1) % wos_ctx_s::kHTabs;
+    // the next slot round robin that no captured graph reads, else a new one
+    int slot = -1;
+    for (size_t i = 0; i < c->htab.size() && slot < 0; i++) {
+        const int j = (int)((c->htab_next + i) % c->htab.size());
+        if (!c->htab[j].frozen) slot = j;
+    }
+    if (slot < 0) {
+        c->htab.emplace_back();
+        slot = (int)c->htab.size() - 1;
+    }
+    c->htab_next = (slot + 1) % (int)c->htab.size();
+    wos_ctx_s::HTab& h = c->htab[slot];
     h.valid = false;
     TRY(ensure(h.buf, (size_t)(k.ncols / 2 + 1) * ld * sizeof(float2) * (hilo ? 2 : 1)));
     CK(fast_build_htab(k, L, reinterpret_cast<float2*>(h.buf.p), ld, hilo, c->st));
@@ -510,6 +521,7 @@ int htab_of(wos_ctx c, FastCols& k, int L, int hilo) {
     CK(cudaStreamIsCapturing(c->st, &cs));
     if (cs == cudaStreamCaptureStatusNone) CK(cudaStreamSynchronize(c->st));
     h.valid = true;
+    h.frozen = c->capturing;
     h.L = L;
     h.ncols = k.ncols;
     std::memcpy(h.key, key, sizeof key);

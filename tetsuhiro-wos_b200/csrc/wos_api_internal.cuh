@@ -103,12 +103,13 @@ struct wos_ctx_s {
     // slot is rebuilt on the context stream, after the work that read it)
     struct HTab {
         bool valid = false;
+        bool frozen = false;  // read by a captured graph: never rebuilt
         int L = 0, ncols = 0;
         double key[9] = {};
         DevBuf buf;
     };
-    static constexpr int kHTabs = 4;
-    HTab htab[kHTabs];
+    static constexpr int kHTabs = 4;    // tables kept round robin (more while graphs pin some)
+    std::vector<HTab> htab = std::vector<HTab>(kHTabs);
     int htab_next = 0;
     int htab_on = 1;                    // WOS_HTAB=0: evaluate H in the split-step sweeps
     int htab_reg = 1;                   // WOS_HTAB_REG=0: evaluate H in the plain ASM column sweep
@@ -117,11 +118,13 @@ struct wos_ctx_s {
     // round robin: a repeated call copies nothing from the host
     struct ParamSlot {
         std::vector<double> host;
+        bool frozen = false;  // read by a captured graph: never rewritten
         DevBuf buf;
     };
     static constexpr int kParamSlots = 8;
-    ParamSlot pslot[kParamSlots];
+    std::vector<ParamSlot> pslot = std::vector<ParamSlot>(kParamSlots);
     int pslot_next = 0;
+    bool capturing = false;             // between wos_graph_capture_begin and _end
     // communicator of the sharded batches (wos_comm_init): NCCL's ncclComm_t
     void* comm = nullptr;
     int comm_size = 1, comm_rank = 0;

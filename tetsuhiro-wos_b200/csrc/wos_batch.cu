@@ -441,11 +441,23 @@ int run_batch_asm(wos_ctx c, Batch& b) {
 int cached_params(wos_ctx c, const std::vector<double>& v, const double** out) {
     for (auto& ps : c->pslot)
         if (ps.buf.p && ps.host == v) {
+            if (c->capturing) ps.frozen = true;
             *out = reinterpret_cast<const double*>(ps.buf.p);
             return WOS_OK;
         }
-    wos_ctx_s::ParamSlot& ps = c->pslot[c->pslot_next];
-    c->pslot_next = (c->pslot_next + 1) % wos_ctx_s::kParamSlots;
+    // the next slot round robin that no captured graph reads, else a new one
+    int slot = -1;
+    for (size_t i = 0; i < c->pslot.size() && slot < 0; i++) {
+        const int j = (int)((c->pslot_next + i) % c->pslot.size());
+        if (!c->pslot[j].frozen) slot = j;
+    }
+    if (slot < 0) {
+        c->pslot.emplace_back();
+        slot = (int)c->pslot.size() - 1;
+    }
+    c->pslot_next = (slot + 1) % (int)c->pslot.size();
+    wos_ctx_s::ParamSlot& ps = c->pslot[slot];
+    ps.frozen = c->capturing;
     ps.host.clear();
     TRY(ensure(ps.buf, sizeof(double) * std::max<size_t>(v.size(), 1)));
     if (!v.empty())

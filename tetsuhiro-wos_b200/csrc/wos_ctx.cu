@@ -210,6 +210,7 @@ int wos_graph_capture_begin(wos_ctx c) {
     std::lock_guard<std::mutex> lk(c->mu);
     TRY(set_device(c));
     CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
+    c->capturing = true;  // tables and parameter lists used from here on stay as the graph reads them
     return WOS_OK;
 }
 
@@ -219,6 +220,7 @@ int wos_graph_capture_end(wos_ctx c, wos_graph* out) {
     std::lock_guard<std::mutex> lk(c->mu);
     TRY(set_device(c));
     cudaGraph_t g = nullptr;
+    c->capturing = false;
     cudaError_t e = cudaStreamEndCapture(c->st, &g);
     if (e != cudaSuccess || !g) {
         cudaGetLastError();
