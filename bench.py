@@ -56,7 +56,8 @@ def workload_config() -> dict:
     return {"workload": f"asm {N}x{N} scalar, complex64, dx=2um, lambda=632.8nm, z=5cm",
             "grid": [N, N], "method": "asm", "evanescent": "decay",
             "warnings": "off: ctx.Warnings nil (the reference default), no wrap check or power sums",
-            "input": "unit-amplitude random phase (seed 1)",
+            "input": "unit-amplitude random phase (seed 1); the lens recipe is timed and checked beside it "
+                     "(lens_input)",
             "l2_flush": f"inputs larger than L2: {POOL} distinct {N * N * 8 >> 20} MiB fields in rotation",
             "parallelism": "replicas"}
 
@@ -706,6 +707,37 @@ def main() -> None:
     props = args.steps * args.batch * world
     value = props / (ms_max / 1e3)
 
+    # ---- the second input of the workload: the lens recipe (Gaussian clipped
+    # by an aperture, thin-lens phase), its parity and the same timed batch
+    lens = WL_.lens_beam(N)
+    lens_rec = {"input": "Gaussian w = 200 um clipped at r = 400 um, thin lens f = 0.2 m"}
+    with torch.cuda.stream(stream):
+        l32 = torch.from_numpy(lens.astype(np.complex64)).cuda()
+        l64 = torch.from_numpy(lens).cuda()
+    torch.cuda.synchronize()
+    g32.propagate_batch_dev(N, N, DX, 1, [l32.data_ptr()], [l32.data_ptr()], ZPROP, "asm", ctx)
+    g64.propagate_dev(N, N, DX, 1, l64.data_ptr(), l64.data_ptr(), ZPROP, "asm", ctx)
+    torch.cuda.synchronize()
+    if rank == 0:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O  # noqa: E402  (checker only)
+        lo = O.Field(lens.copy(), DX)
+        O.propagate(lo, ZPROP, "asm", oracle_context(O))
+        lens_rec["rel_l2_fp32_vs_oracle"] = rel(l32.cpu().numpy().astype(np.complex128), lo.ex)
+        lens_rec["rel_l2_fp64_vs_oracle"] = rel(l64.cpu().numpy(), lo.ex)
+    with torch.cuda.stream(stream):
+        lin = torch.from_numpy(lens.astype(np.complex64)).cuda()
+        for b in bufs:
+            b.copy_(lin)
+    torch.cuda.synchronize()
+    del l32, l64, lin
+    ms_l, _ = time_batch(g32, torch, bufs, args.steps, args.warmup, args.batch, ctx, stream)
+    tl = torch.tensor([ms_l], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(tl, op=dist.ReduceOp.MAX)
+    lens_rec["value"] = props / (float(tl.item()) / 1e3)
+    lens_rec["unit"] = "props/s"
+
     # roofline of the dominant kernel: algorithmic bytes per launch / mean launch time
     peak, peak_kind = measured_peaks()
     per_launch_bytes = {"row_fwd": 16 * N * N, "col_fused": 16 * N * N, "row_inv": 16 * N * N}
@@ -722,7 +754,13 @@ def main() -> None:
                 "per_kernel_us": {k: v[0] / v[1] * 1e3 for k, v in prof.items()},
                 "whole_propagation": {"algorithmic_bytes": 48 * N * N,
                                       "achieved_gbs": 48 * N * N * value / world / 1e9,
-                                      "frac": 48 * N * N * value / world / 1e9 / peak}}
+                                      "frac": 48 * N * N * value / world / 1e9 / peak},
+                # secondary byte models: the compulsory I/O of a propagation
+                # (read and write the field once) and the classic four sweeps
+                "compulsory_io": {"bytes": 16 * N * N, "achieved_gbs": 16 * N * N * value / world / 1e9,
+                                  "frac": 16 * N * N * value / world / 1e9 / peak},
+                "four_sweeps": {"bytes": 64 * N * N, "achieved_gbs": 64 * N * N * value / world / 1e9,
+                                "frac": 64 * N * N * value / world / 1e9 / peak}}
     traffic_file = os.path.join(ROOT, "profiles", "traffic_asm2048_c64.json")
     if roof and os.path.exists(traffic_file):
         try:
@@ -791,7 +829,8 @@ def main() -> None:
                          "fp32_speedup": value / world / fp64_rate},
                 "single_call": {"value": single_rate * world, "unit": "props/s",
                                 "api": "one wos_propagate_dev per field, one stream"},
-                "parity": parity}
+                "parity": parity,
+                "lens_input": lens_rec}
         print(json.dumps(line), flush=True)
     g32.close()
     g64.close()

@@ -514,11 +514,13 @@ int htab_of(wos_ctx c, FastCols& k, int L, int hilo) {
     }
     c->htab_next = (slot + 1) % (int)c->htab.size();
     wos_ctx_s::HTab& h = c->htab[slot];
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(c->st, &cs));
+    // a table being replaced may still be read by sweeps on another stream
+    if (h.valid && cs == cudaStreamCaptureStatusNone) CK(cudaDeviceSynchronize());
     h.valid = false;
     TRY(ensure(h.buf, (size_t)(k.ncols / 2 + 1) * ld * sizeof(float2) * (hilo ? 2 : 1)));
     CK(fast_build_htab(k, L, reinterpret_cast<float2*>(h.buf.p), ld, hilo, c->st));
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    CK(cudaStreamIsCapturing(c->st, &cs));
     if (cs == cudaStreamCaptureStatusNone) CK(cudaStreamSynchronize(c->st));
     h.valid = true;
     h.frozen = c->capturing;
