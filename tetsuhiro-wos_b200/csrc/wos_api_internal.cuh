@@ -251,6 +251,8 @@ size_t fast_col_blocks(int fp64, int L, int E, int W, int ncols, int batch);
 int fast_tw(wos_ctx c, Axis* a, int E, const void** out);
 int fast_tw_lo(wos_ctx c, Axis* a, int E, const void** out);
 int attach_htab(wos_ctx c, FastCols& k, int L, int E);
+int attach_htab_global(wos_ctx c, FastCols& k, int L);
+int attach_htab64(wos_ctx c, FastCols& k, int L);
 cudaError_t sweep_rows(wos_ctx c, int L, int E, bool inv, const FastRows& a, int* nb);
 bool pair_tables(wos_ctx c, int L, int E, const void** twh, const void** twp);
 bool pair_eligible(wos_ctx c, int L, int E, const FastCols& a);

@@ -48,6 +48,9 @@ int asm_design_fast(wos_ctx c, int ny, int nx, double dx, double z, const wos_co
     kc.zero_ev = h.zero_ev;
     kc.reg = h.reg;
     kc.backward = h.z < 0;
+    // H (and conj H for the adjoint) from one table
+    if (c->fp64) TRY(attach_htab64(c, kc, ny));
+    else TRY(attach_htab_global(c, kc, ny));
     FastRows r{};
     r.rows = ny;
     r.in = S;

@@ -649,9 +649,12 @@ static cudaError_t go_rows_design_s(int stage, const FastRows& a, const DesignAr
 
 template <typename Real, int L, int E>
 static cudaError_t go_cols(const FastCols& a, cudaStream_t st, int* nblocks) {
-    if constexpr (sizeof(Real) == 4) {  // H from the table, in registers: the tiled layout's width only
-        if (a.htab_global && fast_col_width(0, L, E, a.W) == kTileW)
-            return go_cols_w<float, L, E, kTileW, false, false, true>(a, st, nblocks);
+    if constexpr (sizeof(Real) == 4) {  // H from the table, in registers: widths 4 (the tiled layout) and 8
+        if (a.htab_global) {
+            const int w = fast_col_width(0, L, E, a.W);
+            if (w == kTileW) return go_cols_w<float, L, E, kTileW, false, 0, true>(a, st, nblocks);
+            if (w == 8) return go_cols_w<float, L, E, 8, false, 0, true>(a, st, nblocks);
+        }
     }
     switch (fast_col_width(sizeof(Real) == 8, L, E, a.W)) {
     case 1: return go_cols_w<Real, L, E, 1>(a, st, nblocks);
