@@ -460,9 +460,9 @@ int cached_params(wos_ctx c, const std::vector<double>& v, const double** out) {
     ps.frozen = c->capturing;
     ps.host.clear();
     TRY(ensure(ps.buf, sizeof(double) * std::max<size_t>(v.size(), 1)));
+    ps.host = v;  // the copy's source: it lives as long as the slot's contents
     if (!v.empty())
-        CK(cudaMemcpyAsync(ps.buf.p, v.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, c->st));
-    ps.host = v;
+        CK(cudaMemcpyAsync(ps.buf.p, ps.host.data(), sizeof(double) * v.size(), cudaMemcpyHostToDevice, c->st));
     *out = reinterpret_cast<const double*>(ps.buf.p);
     return WOS_OK;
 }
