@@ -745,6 +745,9 @@ int try_fast_sweep3(wos_ctx c, const Prop& p, Sweep3& s) {
     q.batch = p.ncomp;
     q.in_tiled = tiled;
     q.tile_len = p.ny;
+    // the result with evict-first stores: L2 stays with the intermediates of
+    // the fields in flight (2048^2 batch 21.2k -> 21.5k props/s)
+    q.out_stream = c->out_stream;
     CK(timed_launch(c, 1, [&] { return sweep_rows(c, p.nx, t.rowE, true, q, &nb); }));
     if (s.red_pout) CK(launch_reduce_finish(red_region(c, 2), nb, 1, RS_P, 1, redout_region(c, 2), c->st));
     s.fast = true;

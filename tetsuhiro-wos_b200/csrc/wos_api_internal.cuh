@@ -113,6 +113,7 @@ struct wos_ctx_s {
     int htab_next = 0;
     int htab_on = 1;                    // WOS_HTAB=0: evaluate H in the split-step sweeps
     int htab_reg = 1;                   // WOS_HTAB_REG=0: evaluate H in the plain ASM column sweep
+    int out_stream = 1;                 // WOS_OUT_STREAM=0: the last row sweep stores without evict-first hints
     // device copies of the small parameter lists (wavelengths, distances,
     // weights) of the device-resident batches, keyed by content and reused
     // round robin: a repeated call copies nothing from the host

@@ -63,6 +63,7 @@ int wos_ctx_create(int device, int precision, wos_ctx* out) {
     c->bpm_comp = env_int("WOS_BPM_COMP", 1);
     c->htab_on = env_int("WOS_HTAB", 1);
     c->htab_reg = env_int("WOS_HTAB_REG", 1);
+    c->out_stream = env_int("WOS_OUT_STREAM", 1);
     *out = c;
     return WOS_OK;
 }

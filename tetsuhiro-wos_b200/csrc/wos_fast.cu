@@ -105,6 +105,12 @@ __global__ void __launch_bounds__(FMaxT<Real, E>::v) k_rows_fast(const FastRows 
             const long long step = (long long)(T / kTileW) * tstride;
 #pragma unroll
             for (int s = 0; s < E; s++) out[s * step] = v[s];
+        } else if (INV && a.out_stream) {
+            // the propagation's result: streaming stores leave L2 to the
+            // intermediates of the fields still in flight
+            C* out = reinterpret_cast<C*>(a.out) + ob + tt;
+#pragma unroll
+            for (int s = 0; s < E; s++) __stcs(out + fpos<RO, E, L>(s, 0), v[s]);
         } else {
             C* out = reinterpret_cast<C*>(a.out) + ob + tt;
 #pragma unroll

@@ -43,6 +43,7 @@ struct FastRows {
     // transformed, multiplied by env_x[x] and forward transformed
     const double* pre_map;
     const double* env_x;
+    int out_stream;       // inverse sweep: the output with streaming (evict-first) stores
 };
 constexpr int kTileW = 4;
 
