@@ -102,6 +102,9 @@ int try_fast_batch(wos_ctx c, Batch& b, std::vector<double>& sums, std::vector<d
         TRY(fast_tw(c, ax, 8, &twx8));
         TRY(fast_tw(c, ay, 8, &twy8));
     }
+    // all units of a batch in one launch per sweep, up to 4 GiB of
+    // intermediates: chunks small enough to stay in L2 (16 - 64 MiB) measured
+    // slower (cfg4 3.69 -> 4.31 ms at 16 MiB): the launches lose parallelism
     const size_t per = (size_t)np * c->csz();
     int B = (int)std::max<size_t>(1, ((size_t)4 << 30) / per);
     B = std::min(B, b.units);
