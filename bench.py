@@ -412,17 +412,17 @@ def run_config(args) -> None:
                 o3 = torch.empty((d3["zs"].size, 1, n3, n3), dtype=dt, device="cuda")
             torch.cuda.synchronize()
 
-            def part1():
-                g.polychromatic_dev(n1, n1, d1["dx"], 1, f1.data_ptr(), d1["z"], d1["wls"], d1["weights"],
-                                    wos.Context(wavelength=d1["wls"][0]), o1.data_ptr())
+            def part1(gx=g):
+                gx.polychromatic_dev(n1, n1, d1["dx"], 1, f1.data_ptr(), d1["z"], d1["wls"], d1["weights"],
+                                     wos.Context(wavelength=d1["wls"][0]), o1.data_ptr())
 
-            def part2():
-                g.partially_coherent_dev(n2, d2["dx"], d2["width"], d2["coherence"], m2, nz.data_ptr(), d2["z"],
-                                         wos.Context(wavelength=d2["wl"]), o2.data_ptr())
+            def part2(gx=g):
+                gx.partially_coherent_dev(n2, d2["dx"], d2["width"], d2["coherence"], m2, nz.data_ptr(), d2["z"],
+                                          wos.Context(wavelength=d2["wl"]), o2.data_ptr())
 
-            def part3():
-                g.volume_dev(n3, n3, d3["dx"], 1, f3.data_ptr(), d3["zs"], wos.Context(wavelength=d3["wl"]),
-                             o3.data_ptr())
+            def part3(gx=g):
+                gx.volume_dev(n3, n3, d3["dx"], 1, f3.data_ptr(), d3["zs"], wos.Context(wavelength=d3["wl"]),
+                              o3.data_ptr())
 
             def cfg4_run():
                 part1()
@@ -433,11 +433,44 @@ def run_config(args) -> None:
                                      for k, f in (("cfg4.1", part1), ("cfg4.2", part2), ("cfg4.3", part3))}
             gr = _graph_of(g, cfg4_run)
             if gr is not None:
+                rec["device_sequential_graph_s"] = timed(gr.launch, max(2, args.steps // 4), 1)
+                gr.close()
+            # the three batches as concurrent branches of one graph: parts 2
+            # and 3 on contexts of their own (wos_graph_capture_fork / _join)
+            gb, gc = wos.GPU(prec), wos.GPU(prec)
+            part2(gb)
+            part3(gc)
+            gb.synchronize()
+            gc.synchronize()
+            g.synchronize()
+            gr = None
+            g.graph_capture_begin()
+            try:
+                g.graph_capture_fork(gb)
+                g.graph_capture_fork(gc)
+                part1(g)
+                part2(gb)
+                part3(gc)
+            except Exception:
+                pass
+            for gx in (gb, gc):
+                try:
+                    g.graph_capture_join(gx)
+                except Exception:
+                    pass
+            try:
+                gr = g.graph_capture_end()
+            except Exception:
+                gr = None
+            if gr is not None:
                 rec["device_s"] = timed(gr.launch, max(2, args.steps // 4), 1)
-                rec["device_api"] = "wos_polychromatic_dev + wos_partially_coherent_dev + wos_volume_dev, one graph"
+                rec["device_api"] = ("wos_polychromatic_dev, wos_partially_coherent_dev and wos_volume_dev on "
+                                     "three contexts, concurrent branches of one graph")
                 gr.close()
             else:
-                rec["device_s"] = rec["device_direct_s"]
+                rec["device_s"] = rec.get("device_sequential_graph_s", rec["device_direct_s"])
+            gb.close()
+            gc.close()
             del nz, o3
             torch.cuda.empty_cache()
             if prec == wos.FP64:

@@ -505,6 +505,18 @@ WOS_API int wos_asm_adjoint(wos_ctx ctx, wos_field* f, double z, const wos_conte
  *      is destroyed (later calls with other distances or lists take other
  *      entries). ---- */
 WOS_API int wos_graph_capture_begin(wos_ctx ctx);
+/* Concurrent branches of one capture: after wos_graph_capture_begin(ctx),
+ * wos_graph_capture_fork(ctx, other) makes another context (same device, its
+ * own stream) a branch of the capture: the device-resident calls made on
+ * `other` are recorded into ctx's graph, after what ctx recorded before the
+ * fork and concurrently with what ctx records after it.
+ * wos_graph_capture_join(ctx, other) closes the branch (ctx's later calls and
+ * the end of the graph wait for it); every branch must be joined before
+ * wos_graph_capture_end(ctx).  The same rules as for ctx apply to the calls
+ * on a branch.  Independent batches (e.g. the wavelengths, modes and planes
+ * of three jobs) replay this way as one graph whose jobs share the GPU. */
+WOS_API int wos_graph_capture_fork(wos_ctx ctx, wos_ctx other);
+WOS_API int wos_graph_capture_join(wos_ctx ctx, wos_ctx other);
 WOS_API int wos_graph_capture_end(wos_ctx ctx, wos_graph* out);
 WOS_API int wos_graph_launch(wos_ctx ctx, wos_graph g);
 WOS_API int wos_graph_destroy(wos_graph g);

@@ -1,7 +1,8 @@
 """CUDA graphs of device-resident calls (wos_graph_capture_begin / _end,
 wos_graph_launch): a replay must give the results of the captured calls run
 directly (bit for bit: the same kernels on the same buffers), including the
-forked streams of a device batch and in-place split-step runs replayed
+forked streams of a device batch, branches on other contexts
+(wos_graph_capture_fork / _join) and in-place split-step runs replayed
 repeatedly; a call that needs a synchronisation inside a capture fails cleanly
 and leaves the context usable."""
 import numpy as np
@@ -165,3 +166,62 @@ def test_graph_capture_of_a_synchronising_call_fails_cleanly(gpu):
     gpu.propagate_dev(n, n, dx, 1, x.data_ptr(), y.data_ptr(), z, "asm", wos.Context(**CTX))
     gpu.synchronize()
     assert torch.isfinite(torch.view_as_real(y)).all()
+
+
+def test_graph_branches_of_other_contexts(gpu):
+    """wos_graph_capture_fork / _join: the calls of two more contexts, recorded
+    as concurrent branches of one capture, replay with the results of the
+    direct calls (bit for bit); misuse fails without breaking the capture."""
+    import torch
+    n, dx = 512, 2e-6
+    other = [wos.GPU(gpu.precision) for _ in range(2)]
+    try:
+        ins = _fields(gpu, 3, n, 7)
+        outs = [torch.empty_like(t) for t in ins]
+        wls = np.linspace(500e-9, 600e-9, 3)
+        pw = torch.empty((n, n), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+
+        def calls():
+            gpu.propagate_dev(n, n, dx, 1, ins[0].data_ptr(), outs[0].data_ptr(), 5e-3, "asm", wos.Context(**CTX))
+            other[0].propagate_batch_dev(n, n, dx, 1, [ins[1].data_ptr(), ins[2].data_ptr()],
+                                         [outs[1].data_ptr(), outs[2].data_ptr()], 2e-3, "asm", wos.Context(**CTX))
+            other[1].polychromatic_dev(n, n, dx, 1, ins[0].data_ptr(), 1e-2, wls, np.ones(3), wos.Context(**CTX),
+                                       pw.data_ptr())
+
+        calls()  # direct, also the warm-up of the capture
+        for g in [gpu] + other:
+            g.synchronize()
+        want = [o.clone() for o in outs] + [pw.clone()]
+        with pytest.raises(wos.WosError):
+            gpu.graph_capture_fork(other[0])  # ctx is not capturing
+        gpu.graph_capture_begin()
+        gpu.graph_capture_fork(other[0])
+        gpu.graph_capture_fork(other[1])
+        with pytest.raises(wos.WosError):
+            gpu.graph_capture_fork(other[0])  # already a branch
+        calls()
+        with pytest.raises(wos.WosError):
+            gpu.graph_capture_end()  # branches still open
+        gpu.graph_capture_join(other[0])
+        gpu.graph_capture_join(other[1])
+        with pytest.raises(wos.WosError):
+            gpu.graph_capture_join(other[1])  # already joined
+        g = gpu.graph_capture_end()
+        for _ in range(2):
+            for o in outs:
+                o.zero_()
+            pw.zero_()
+            torch.cuda.synchronize()
+            g.launch()
+            gpu.synchronize()
+            for o, w in zip(outs + [pw], want):
+                assert torch.equal(o, w)
+        g.close()
+        # the branches' contexts are usable on their own again
+        other[0].propagate_dev(n, n, dx, 1, ins[1].data_ptr(), outs[1].data_ptr(), 2e-3, "asm", wos.Context(**CTX))
+        other[0].synchronize()
+        assert torch.equal(outs[1], want[1])
+    finally:
+        for g in other:
+            g.close()

@@ -111,6 +111,7 @@ int wos_ctx_destroy(wos_ctx c) {
             cudaEventDestroy(c->join_ev[i]);
         }
         if (c->fork_ev) cudaEventDestroy(c->fork_ev);
+        if (c->cap_ev) cudaEventDestroy(c->cap_ev);
         if (c->pipe_made) {
             cudaStreamDestroy(c->h2d);
             cudaStreamDestroy(c->d2h);
@@ -209,9 +210,59 @@ int wos_ctx_synchronize(wos_ctx c) {
 int wos_graph_capture_begin(wos_ctx c) {
     if (!c) return fail(WOS_INVALID_ARG, "null ctx");
     std::lock_guard<std::mutex> lk(c->mu);
+    if (c->capturing) return fail(WOS_INVALID_ARG, "capture begin: ctx is already capturing");
     TRY(set_device(c));
     CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeRelaxed));
     c->capturing = true;  // tables and parameter lists used from here on stay as the graph reads them
+    return WOS_OK;
+}
+
+// A branch of a capture: the other context's stream waits on an event of the
+// capturing stream, which makes it part of the same capture (its calls are
+// recorded as nodes that depend only on what ctx recorded before the fork);
+// the join records an event on the branch and has the capturing stream wait
+// on it.  Contexts are locked one at a time, capturing context first.
+int wos_graph_capture_fork(wos_ctx c, wos_ctx o) {
+    if (!c || !o || c == o) return fail(WOS_INVALID_ARG, "capture fork: two distinct contexts");
+    if (c->device != o->device) return fail(WOS_INVALID_ARG, "capture fork: contexts on different devices");
+    cudaStream_t cst;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        if (!c->capturing || c->cap_owner) return fail(WOS_INVALID_ARG, "capture fork: ctx is not capturing");
+        TRY(set_device(c));
+        if (!c->cap_ev) CK(cudaEventCreateWithFlags(&c->cap_ev, cudaEventDisableTiming));
+        CK(cudaEventRecord(c->cap_ev, c->st));
+        cst = c->st;
+    }
+    std::lock_guard<std::mutex> lk(o->mu);
+    if (o->capturing) return fail(WOS_INVALID_ARG, "capture fork: the other context is already capturing");
+    if (o->st == cst) return fail(WOS_INVALID_ARG, "capture fork: both contexts use one stream");
+    TRY(set_device(o));
+    CK(cudaStreamWaitEvent(o->st, c->cap_ev, 0));
+    o->capturing = true;
+    o->cap_owner = c;
+    {
+        std::lock_guard<std::mutex> lc(c->mu);
+        c->cap_branches++;
+    }
+    return WOS_OK;
+}
+
+int wos_graph_capture_join(wos_ctx c, wos_ctx o) {
+    if (!c || !o || c == o) return fail(WOS_INVALID_ARG, "capture join: two distinct contexts");
+    {
+        std::lock_guard<std::mutex> lk(o->mu);
+        if (!o->capturing || o->cap_owner != c) return fail(WOS_INVALID_ARG, "capture join: not a branch of ctx");
+        TRY(set_device(o));
+        if (!o->cap_ev) CK(cudaEventCreateWithFlags(&o->cap_ev, cudaEventDisableTiming));
+        CK(cudaEventRecord(o->cap_ev, o->st));
+        o->capturing = false;
+        o->cap_owner = nullptr;
+    }
+    std::lock_guard<std::mutex> lk(c->mu);
+    TRY(set_device(c));
+    CK(cudaStreamWaitEvent(c->st, o->cap_ev, 0));
+    c->cap_branches--;
     return WOS_OK;
 }
 
@@ -219,6 +270,8 @@ int wos_graph_capture_end(wos_ctx c, wos_graph* out) {
     if (!c || !out) return fail(WOS_INVALID_ARG, "null argument");
     *out = nullptr;
     std::lock_guard<std::mutex> lk(c->mu);
+    if (c->cap_owner) return fail(WOS_INVALID_ARG, "capture end: ctx is a branch; join it to its capture instead");
+    if (c->cap_branches) return fail(WOS_INVALID_ARG, "capture end: join every forked context first");
     TRY(set_device(c));
     cudaGraph_t g = nullptr;
     c->capturing = false;

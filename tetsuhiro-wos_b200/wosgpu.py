@@ -47,7 +47,8 @@ EXPORTS = [
     "wos_bpm_stack_loss_grad", "wos_bpm_stack_loss_grad_dev", "wos_splitstep_adjoint_dev",
     "wos_train", "wos_propagate_vectorial", "wos_plane_view", "wos_plane_view_dev",
     "wos_propagate_uniaxial", "wos_propagate_anisotropic",
-    "wos_graph_capture_begin", "wos_graph_capture_end", "wos_graph_launch", "wos_graph_destroy",
+    "wos_graph_capture_begin", "wos_graph_capture_fork", "wos_graph_capture_join", "wos_graph_capture_end",
+    "wos_graph_launch", "wos_graph_destroy",
     "wos_splitstep_adjoint",
     "wos_polychromatic_dev", "wos_volume_dev", "wos_partially_coherent_dev",
     "wos_comm_unique_id", "wos_comm_init", "wos_comm_destroy", "wos_shard_range",
@@ -176,6 +177,7 @@ def lib():
             "wos_propagate_uniaxial": ([vp, vp, d, d, d, vp], i),
             "wos_propagate_anisotropic": ([vp, vp, d, vp, vp], i),
             "wos_graph_capture_begin": ([vp], i), "wos_graph_capture_end": ([vp, vp], i),
+            "wos_graph_capture_fork": ([vp, vp], i), "wos_graph_capture_join": ([vp, vp], i),
             "wos_graph_launch": ([vp, vp], i), "wos_graph_destroy": ([vp], i),
             "wos_splitstep_adjoint": ([vp, vp, d, vp, i, vp], i),
             "wos_polychromatic_dev": ([vp, i, i, d, i, vp, d, vp, vp, i, vp, vp], i),
@@ -674,6 +676,14 @@ class GPU:
     # ---- CUDA graphs of device-resident calls
     def graph_capture_begin(self) -> None:
         _check(lib().wos_graph_capture_begin(self.h))
+
+    def graph_capture_fork(self, other: "GPU") -> None:
+        """wos_graph_capture_fork: other's calls become a concurrent branch of this capture."""
+        _check(lib().wos_graph_capture_fork(self.h, other.h))
+
+    def graph_capture_join(self, other: "GPU") -> None:
+        """wos_graph_capture_join: close the branch forked to other."""
+        _check(lib().wos_graph_capture_join(self.h, other.h))
 
     def graph_capture_end(self) -> "Graph":
         h = C.c_void_p()
