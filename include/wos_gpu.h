@@ -514,7 +514,9 @@ WOS_API int wos_graph_capture_begin(wos_ctx ctx);
  * the end of the graph wait for it); every branch must be joined before
  * wos_graph_capture_end(ctx).  The same rules as for ctx apply to the calls
  * on a branch.  Independent batches (e.g. the wavelengths, modes and planes
- * of three jobs) replay this way as one graph whose jobs share the GPU. */
+ * of three jobs) replay this way as one graph whose jobs share the GPU.
+ * Destroying a branch before its join makes ctx's capture fail at its end;
+ * destroying ctx mid-capture ends the capture and releases its branches. */
 WOS_API int wos_graph_capture_fork(wos_ctx ctx, wos_ctx other);
 WOS_API int wos_graph_capture_join(wos_ctx ctx, wos_ctx other);
 WOS_API int wos_graph_capture_end(wos_ctx ctx, wos_graph* out);

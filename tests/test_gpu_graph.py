@@ -225,3 +225,43 @@ def test_graph_branches_of_other_contexts(gpu):
     finally:
         for g in other:
             g.close()
+
+
+def test_graph_branch_destroyed_mid_capture(gpu):
+    """A context destroyed while it is a branch of a capture: the owner's
+    capture then fails at its end and the owner works on; an owner destroyed
+    with a branch open ends its capture, and the branch works on."""
+    import torch
+    n, dx, z = 256, 2e-6, 1e-3
+    x = _fields(gpu, 1, n, 9)[0]
+    y, want = torch.empty_like(x), torch.empty_like(x)
+    torch.cuda.synchronize()
+    gpu.propagate_dev(n, n, dx, 1, x.data_ptr(), want.data_ptr(), z, "asm", wos.Context(**CTX))
+    gpu.synchronize()
+    b = wos.GPU(gpu.precision)
+    b.propagate_dev(n, n, dx, 1, x.data_ptr(), y.data_ptr(), z, "asm", wos.Context(**CTX))
+    b.synchronize()
+    gpu.graph_capture_begin()
+    gpu.graph_capture_fork(b)
+    b.propagate_dev(n, n, dx, 1, x.data_ptr(), y.data_ptr(), z, "asm", wos.Context(**CTX))
+    b.close()
+    with pytest.raises(wos.WosError):
+        gpu.graph_capture_end()
+    y.zero_()
+    torch.cuda.synchronize()
+    gpu.propagate_dev(n, n, dx, 1, x.data_ptr(), y.data_ptr(), z, "asm", wos.Context(**CTX))
+    gpu.synchronize()
+    assert torch.equal(y, want)
+
+    owner, b = wos.GPU(gpu.precision), wos.GPU(gpu.precision)
+    owner.propagate_dev(n, n, dx, 1, x.data_ptr(), y.data_ptr(), z, "asm", wos.Context(**CTX))
+    owner.synchronize()
+    owner.graph_capture_begin()
+    owner.graph_capture_fork(b)
+    owner.close()
+    y.zero_()
+    torch.cuda.synchronize()
+    b.propagate_dev(n, n, dx, 1, x.data_ptr(), y.data_ptr(), z, "asm", wos.Context(**CTX))
+    b.synchronize()
+    assert torch.equal(y, want)
+    b.close()

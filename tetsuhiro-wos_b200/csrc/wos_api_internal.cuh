@@ -127,7 +127,7 @@ struct wos_ctx_s {
     int pslot_next = 0;
     bool capturing = false;             // between wos_graph_capture_begin and _end
     wos_ctx cap_owner = nullptr;        // the capturing context this one is a branch of (wos_graph_capture_fork)
-    int cap_branches = 0;               // open branches of this context's capture
+    std::vector<wos_ctx> cap_open;      // open branches of this context's capture
     cudaEvent_t cap_ev = nullptr;       // fork / join point of a capture branch
     // communicator of the sharded batches (wos_comm_init): NCCL's ncclComm_t
     void* comm = nullptr;

@@ -1,6 +1,8 @@
 // wos_ctx.cu -- contexts (device, precision, stream, workspaces), their
 // settings and profiling counters, CUDA graphs of device-resident calls and
 // the launch-configuration tuner of the specialised sweeps.
+#include <algorithm>
+
 #include "wos_api_internal.cuh"
 
 extern "C" {
@@ -68,9 +70,42 @@ int wos_ctx_create(int device, int precision, wos_ctx* out) {
     return WOS_OK;
 }
 
+// A context destroyed in the middle of a capture: a branch leaves its
+// owner's list (the owner's capture then fails at its end); an owner ends its
+// capture (discarding the graph) and releases its branches, which keep no
+// pointer to it.
+static void capture_release(wos_ctx c) {
+    wos_ctx owner = nullptr;
+    std::vector<wos_ctx> open;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        owner = c->cap_owner;
+        open.swap(c->cap_open);
+        if (c->capturing && !owner) {
+            cudaSetDevice(c->device);
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(c->st, &g);
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+        }
+        c->capturing = false;
+        c->cap_owner = nullptr;
+    }
+    if (owner) {
+        std::lock_guard<std::mutex> lk(owner->mu);
+        owner->cap_open.erase(std::remove(owner->cap_open.begin(), owner->cap_open.end(), c), owner->cap_open.end());
+    }
+    for (wos_ctx b : open) {
+        std::lock_guard<std::mutex> lk(b->mu);
+        b->capturing = false;
+        b->cap_owner = nullptr;
+    }
+}
+
 int wos_ctx_destroy(wos_ctx c) {
     if (!c) return WOS_OK;
     comm_release(c);
+    capture_release(c);
     {
         std::lock_guard<std::mutex> lk(c->mu);
         cudaSetDevice(c->device);
@@ -234,17 +269,17 @@ int wos_graph_capture_fork(wos_ctx c, wos_ctx o) {
         CK(cudaEventRecord(c->cap_ev, c->st));
         cst = c->st;
     }
-    std::lock_guard<std::mutex> lk(o->mu);
-    if (o->capturing) return fail(WOS_INVALID_ARG, "capture fork: the other context is already capturing");
-    if (o->st == cst) return fail(WOS_INVALID_ARG, "capture fork: both contexts use one stream");
-    TRY(set_device(o));
-    CK(cudaStreamWaitEvent(o->st, c->cap_ev, 0));
-    o->capturing = true;
-    o->cap_owner = c;
     {
-        std::lock_guard<std::mutex> lc(c->mu);
-        c->cap_branches++;
+        std::lock_guard<std::mutex> lk(o->mu);
+        if (o->capturing) return fail(WOS_INVALID_ARG, "capture fork: the other context is already capturing");
+        if (o->st == cst) return fail(WOS_INVALID_ARG, "capture fork: both contexts use one stream");
+        TRY(set_device(o));
+        CK(cudaStreamWaitEvent(o->st, c->cap_ev, 0));
+        o->capturing = true;
+        o->cap_owner = c;
     }
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->cap_open.push_back(o);
     return WOS_OK;
 }
 
@@ -262,7 +297,7 @@ int wos_graph_capture_join(wos_ctx c, wos_ctx o) {
     std::lock_guard<std::mutex> lk(c->mu);
     TRY(set_device(c));
     CK(cudaStreamWaitEvent(c->st, o->cap_ev, 0));
-    c->cap_branches--;
+    c->cap_open.erase(std::remove(c->cap_open.begin(), c->cap_open.end(), o), c->cap_open.end());
     return WOS_OK;
 }
 
@@ -271,7 +306,7 @@ int wos_graph_capture_end(wos_ctx c, wos_graph* out) {
     *out = nullptr;
     std::lock_guard<std::mutex> lk(c->mu);
     if (c->cap_owner) return fail(WOS_INVALID_ARG, "capture end: ctx is a branch; join it to its capture instead");
-    if (c->cap_branches) return fail(WOS_INVALID_ARG, "capture end: join every forked context first");
+    if (!c->cap_open.empty()) return fail(WOS_INVALID_ARG, "capture end: join every forked context first");
     TRY(set_device(c));
     cudaGraph_t g = nullptr;
     c->capturing = false;
