@@ -1373,7 +1373,8 @@ int wos_propagate_batch_dev(wos_ctx c, int nfields, int ny, int nx, double dx, i
     // context workspace (the sweeps run in place in each output), so they can
     // run concurrently on the context's side streams; the tables they share
     // are built first, on the context stream.  Two streams measured best at
-    // 2048^2 complex64 (two 32 MiB fields in flight stay in L2; three thrash).
+    // 2048^2 complex64 (two 32 MiB fields in flight stay in L2; three thrash),
+    // three for smaller fields.
     const bool concurrent = method == WOS_ASM && z != 0 && !c->no_fast && is_pow2(nx) && is_pow2(ny) &&
                             (c->fp64 || std::fabs(z / cc.wavelength) < 268435456.0) && nfields > 1;
     int nstreams = 0;
@@ -1400,7 +1401,12 @@ int wos_propagate_batch_dev(wos_ctx c, int nfields, int ny, int nx, double dx, i
                 if (asm_tiled(c, ny, nx, t)) TRY(attach_htab_global(c, hk, ny));
                 else TRY(attach_htab64(c, hk, ny));
             }
-            nstreams = std::max(1, std::min(wos_ctx_s::kMaxAux, env_int("WOS_STREAMS", 2)));
+            // three streams for fields up to 16 MiB (1024^2 +4-5 %, 512^2
+            // complex128 +20-30 %), two above (2048^2 complex64: 21.3k
+            // against 18.9k props/s with three)
+            const size_t fbytes = (size_t)ny * nx * ncomp * c->csz();
+            const int def_streams = fbytes <= ((size_t)16 << 20) ? 3 : 2;
+            nstreams = std::max(1, std::min(wos_ctx_s::kMaxAux, env_int("WOS_STREAMS", def_streams)));
         }
     }
     if (nstreams <= 1) {
