@@ -160,6 +160,18 @@ void widen_c64(const float2* s, wos_c128* h, size_t b, size_t e) {
     for (; i < e; i++) h[i] = wos_c128{(double)s[i].x, (double)s[i].y};
 }
 
+// complex128 [b, e) copied with streaming stores (one value per SSE2 step),
+// the complex128 pipeline's staging in both directions: like the conversions,
+// it writes memory that the DMA engine or the caller reads next
+void copy_c128(const wos_c128* src, wos_c128* dst, size_t b, size_t e) {
+    if (((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) != 0) {
+        std::memcpy(dst + b, src + b, (e - b) * sizeof(wos_c128));
+        return;
+    }
+    for (size_t i = b; i < e; i++) _mm_stream_pd(&dst[i].re, _mm_load_pd(&src[i].re));
+    _mm_sfence();
+}
+
 // Components of f, complex128, into dst in the context's complex type
 // ([ncomp][ny][nx]), or back (to_host), on the context's host threads.
 void host_convert(wos_ctx c, wos_field& f, void* dst, bool to_host) {
@@ -174,8 +186,8 @@ void host_convert(wos_ctx c, wos_field& f, void* dst, bool to_host) {
             wos_c128* h = q == 0 ? f.ex : f.ey;
             if (c->fp64) {
                 wos_c128* s = static_cast<wos_c128*>(dst) + q * np;
-                if (to_host) std::memcpy(h + b, s + b, (e - b) * sizeof(wos_c128));
-                else std::memcpy(s + b, h + b, (e - b) * sizeof(wos_c128));
+                if (to_host) copy_c128(s, h, b, e);
+                else copy_c128(h, s, b, e);
             } else {
                 float2* s = static_cast<float2*>(dst) + q * np;
                 if (to_host) widen_c64(s, h, b, e);
