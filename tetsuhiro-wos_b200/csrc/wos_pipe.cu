@@ -176,9 +176,21 @@ __global__ void __launch_bounds__(RowPipe<Real, L, E>::THREADS) k_rows_pipe(cons
 #pragma unroll
                 for (int s = 0; s < E; s++) pw += (double)v[s].x * v[s].x + (double)v[s].y * v[s].y;
             }
-            C* out = reinterpret_cast<C*>(a.out) + (long long)b * a.out_bstride + (long long)r * a.out_ld + tt;
+            if (!INV && a.out_tiled) {
+                // the tiled intermediate (FastRows::out_tiled): x = tt + s*T
+                // (RO == E) lies in tile x / kTileW, lane x % kTileW
+                static_assert(INV || RO == E, "tiled stores follow the natural mapping of radix E");
+                const long long tstride = a.tile_len * kTileW;
+                C* out = reinterpret_cast<C*>(a.out) + (long long)b * a.out_bstride + (long long)r * kTileW +
+                         (long long)(tt / kTileW) * tstride + (tt % kTileW);
+                const long long step = (long long)(T / kTileW) * tstride;
 #pragma unroll
-            for (int s = 0; s < E; s++) out[fpos<RO, E, L>(s, 0)] = v[s];
+                for (int s = 0; s < E; s++) out[s * step] = v[s];
+            } else {
+                C* out = reinterpret_cast<C*>(a.out) + (long long)b * a.out_bstride + (long long)r * a.out_ld + tt;
+#pragma unroll
+                for (int s = 0; s < E; s++) out[fpos<RO, E, L>(s, 0)] = v[s];
+            }
         }
         __syncthreads();  // every thread is done with the stage
         if (threadIdx.x == 0 && u + 2 * (long long)gridDim.x < units) {
