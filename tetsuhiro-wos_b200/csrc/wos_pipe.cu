@@ -102,10 +102,14 @@ template <typename Real, int L, int E> struct RowPipe {
     static constexpr int THREADS = LINES * T;
     static constexpr size_t STAGE = round128((size_t)LINES * frow_stride(L, E) * sizeof(C));
     static constexpr size_t SMEM = 2 * STAGE + 16;
+    // two resident CTAs (<= 128 registers a thread at 256 threads): the
+    // complex128 forward sweep of 2048 points otherwise takes 134 and runs one
+    // CTA per SM
+    static constexpr int MINB = THREADS <= 256 ? 2 : 1;
 };
 
 template <typename Real, int L, int E, bool INV>
-__global__ void __launch_bounds__(RowPipe<Real, L, E>::THREADS) k_rows_pipe(const FastRows a) {
+__global__ void __launch_bounds__(RowPipe<Real, L, E>::THREADS, RowPipe<Real, L, E>::MINB) k_rows_pipe(const FastRows a) {
     using C = typename CT<Real>::t;
     using PL = FPlan<L, E>;
     using RP = RowPipe<Real, L, E>;
