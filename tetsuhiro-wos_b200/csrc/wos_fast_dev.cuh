@@ -185,7 +185,10 @@ __device__ __forceinline__ void fload(C* v, const C* smb, int tt) {
 // the next pass's loads are 16 consecutive 64-bit words per half-warp, which a
 // pad every 8 positions (radix 8) puts twice on one bank pair; with a pad every
 // 16 they land on 16 distinct pairs, and the stores of a radix 2, 4 or 8 pass
-// stay conflict-free.  Complex128 lines take 8 after radix-2 and radix-4
+// stay conflict-free; a radix-8 pass with 1 < NS < 16 (lines of E = 8) keeps
+// 8, where a period of 16 puts two of a half-warp's stores on one bank pair
+// (and 8 leaves fewer conflicts on the load side than 16 does on the store
+// side).  Complex128 lines take 8 after radix-2 and radix-4
 // passes: a wavefront serves 8 threads' 16-byte slots, and a pad every 2 or 4
 // put two of the next pass's 8 consecutive loads on one bank group (the
 // forward 2048-point row sweep: 524K load conflicts per launch); with 8 the
@@ -194,7 +197,7 @@ __device__ __forceinline__ void fload(C* v, const C* smb, int tt) {
 template <int L, int R, int NS, int R2, int STR, typename C>
 __host__ __device__ constexpr int fx_shift() {
     constexpr int s = Log2<R>::v;
-    if (sizeof(C) == 8 && STR == 1 && s < 4 && (L / R2) % 16 == 0 && (NS >= 16 || NS == 1 || NS * R >= 16)) return 4;
+    if (sizeof(C) == 8 && STR == 1 && s < 4 && (L / R2) % 16 == 0 && (NS >= 16 || NS == 1)) return 4;
     if (sizeof(C) == 16 && STR == 1 && s < 3 && (L / R2) % 8 == 0 && (NS >= 8 || NS == 1 || NS * R >= 8)) return 3;
     return s;
 }
